@@ -1,0 +1,173 @@
+/*
+ * pgb200: PEREGRINE's right-hand side and Runge-Kutta stage on one B200.
+ *
+ * A plain C ABI: opaque handles, plain pointers and sizes, an int status on
+ * every call (0 = success), and the text of the last failure on the calling
+ * thread from pgb_last_error().  Nothing here names a torch or CUDA type; a
+ * CUDA stream crosses as a void pointer.
+ *
+ * What each entry replaces in the reference (paths inside kaschau/Peregrine):
+ *
+ *  - The reference renders every kernel per case into a C++ unit and calls its
+ *    extern "C" pg_<symbol>(const K, const pg::Tiling) entry through the CUDA
+ *    driver (peregrine/backend/device/kernels/launch.mako:5-12,
+ *    peregrine/backend/device/backend.py:33-48).  Here the kernels are compiled
+ *    once for sm_100a and selected by the case description.
+ *  - The solver-level calls (peregrine/multiblock/solver.py:246-364: rhs,
+ *    advance, step, set_prims, the arrays' get/set) map onto pgb_rhs,
+ *    pgb_step, pgb_set_prims, pgb_array_set and pgb_array_get.
+ */
+#ifndef PGB200_H
+#define PGB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; a CUDA runtime failure is PGB_ERR_CUDA with its text in
+ * pgb_last_error() (the reference maps driver codes to typed exceptions,
+ * peregrine/backend/cuda/driver.py:7-55) */
+enum {
+  PGB_OK = 0,
+  PGB_ERR_ARG = 1,       /* a bad argument: a size, a name, an index */
+  PGB_ERR_STATE = 2,     /* a call out of order: e.g. a step before finalize */
+  PGB_ERR_CUDA = 3,      /* a CUDA runtime error */
+  PGB_ERR_NOMEM = 4,     /* a device allocation refused */
+  PGB_ERR_UNSUPPORTED = 5, /* a physics choice this build does not have */
+  PGB_ERR_TIMEOUT = 6,   /* a bounded device wait gave up (status word set) */
+};
+
+/* physics selectors: the config's names (peregrine/config.py:12-98) */
+enum { PGB_EULER = 0, PGB_NAVIER_STOKES = 1 };
+enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1 };
+enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2 };
+enum { PGB_RECON_CONSTANT = 0, PGB_RECON_MUSCL = 1 };
+enum { PGB_TRANS_NONE = 0, PGB_TRANS_CONSTANT = 1, PGB_TRANS_KINETIC = 2 };
+/* the launch paths */
+enum { PGB_PATH_BATCHED = 0, PGB_PATH_PER_BLOCK = 1 };
+
+/* the per-cell and per-face arrays of a block the caller sets (metrics) or
+ * reads and writes (registers, prims): the reference's array names
+ * (peregrine/multiblock/block/grid.py:123-202) */
+enum {
+  PGB_ARR_XCC = 0,     /* cell centres, 3 */
+  PGB_ARR_DETJINV = 1, /* 1 / volume, 1 */
+  PGB_ARR_JINV = 2,    /* inverse Jacobian, 3 x 3 */
+  PGB_ARR_IS = 3, PGB_ARR_JS = 4, PGB_ARR_KS = 5,    /* face area vectors, 3 */
+  PGB_ARR_IXC = 6, PGB_ARR_JXC = 7, PGB_ARR_KXC = 8, /* face centres, 3 */
+  PGB_NMETRICS = 9
+};
+
+typedef struct pgb_case pgb_case;
+
+typedef struct {
+  int simulator;  /* PGB_EULER / PGB_NAVIER_STOKES */
+  int eos;        /* PGB_EOS_* */
+  int primary;    /* PGB_FLUX_* */
+  int recon;      /* PGB_RECON_* */
+  int limiter;    /* 0 none, 1 koren, 2 minmod, 3 mc, 4 superbee, 5 vanleer */
+  int trans;      /* PGB_TRANS_* */
+  int ns;         /* species, >= 1 */
+  int nregs;      /* Runge-Kutta registers the integrator needs, dQ included */
+  double alpha;   /* alpha-damping coefficient */
+} pgb_physics;
+
+/* One Runge-Kutta combine: out = [wout out +] sum_n w[n] X[n], dt multiplying
+ * the last term when step is set (peregrine/integrators/kernels/combine.mako).
+ * A term whose reg is -1 is the stage's right-hand side dQ.  Registers are
+ * logical (0 .. nregs-1 as the integrator names them). */
+typedef struct {
+  int out;
+  int own;        /* 1: wout * out is the first term */
+  double wout;
+  int nterms;     /* 1 .. 3 */
+  int reg[3];
+  double w[3];
+  int step;
+} pgb_combine;
+
+/* One stage: the register its right-hand side reads, the combines after it */
+typedef struct {
+  int q;
+  int dq;         /* the logical register holding dQ on the per-block path */
+  int ncombine;   /* 1 or 2 */
+  pgb_combine combine[2];
+} pgb_stage;
+
+/* library */
+const char *pgb_last_error(void);
+int pgb_version(void);
+int pgb_device_init(int ordinal);
+int pgb_device_count(int *count);
+int pgb_device_sync(void);
+/* a device's free and total memory, bytes */
+int pgb_mem_info(size_t *free_bytes, size_t *total_bytes);
+
+/* a case: physics, species tables, blocks, connectivity, then finalize */
+int pgb_case_create(const pgb_physics *phys, pgb_case **out);
+int pgb_case_destroy(pgb_case *c);
+/* a named species table of n doubles (names as the reference's mixture
+ * constants: "Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0",
+ * "kappa0", "MWqinv", "wilkepair", "lewis") */
+int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long n);
+/* a block of ni x nj x nk cells; its number is the order of the calls */
+int pgb_case_add_block(pgb_case *c, int ni, int nj, int nk, int *blk);
+/* face nface (1..6: i-low, i-high, j-low, j-high, k-low, k-high) of blk joins
+ * face nbrface of nbr, orientation "123" (the lattice meshers' only one,
+ * peregrine/mesher/base.py:117-133); nbr -1 is a boundary */
+int pgb_case_connect(pgb_case *c, int blk, int nface, int nbr, int nbrface);
+/* the integrator's stages, in order */
+int pgb_case_set_stages(pgb_case *c, const pgb_stage *stages, int nstages);
+/* allocate the device arrays, build halo tables and work lists */
+int pgb_case_finalize(pgb_case *c);
+/* the halo depth the case uses and a block's full (halo included) extents */
+int pgb_case_halo(const pgb_case *c, int *ng);
+int pgb_case_device_bytes(const pgb_case *c, size_t *bytes);
+
+/* A metric array, from the host: F order (i fastest, then j, k, components
+ * outermost; numpy's order="F" of the reference's [i, j, k, comps] host view),
+ * full extents with the case's halo (face arrays one plane more along their
+ * axis). */
+int pgb_metric_set(pgb_case *c, int blk, int which, const double *host, long count);
+
+/* A register's interior cells, host F order (i fastest, components
+ * outermost), interior only.  Logical register reg. */
+int pgb_array_set(pgb_case *c, int blk, int reg, const double *host, long count);
+int pgb_array_get(pgb_case *c, int blk, int reg, double *host, long count);
+
+/* Q of register reg from primitives p, u, v, w, T, Y... on the interior
+ * (the reference's fromprims, peregrine/simulator/euler/kernels/state/fromprims.mako) */
+int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count);
+
+/* The right-hand side dQ of logical register q into logical register dq, on
+ * the per-block path (halo exchange included).  Returns when queued. */
+int pgb_rhs(pgb_case *c, int q, int dq);
+
+/* nsteps steps of dt on the chosen path; graph 1 captures one step into a CUDA
+ * graph and replays it.  Returns when queued on the case's stream. */
+int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph);
+
+/* the stream the case queues on (a cudaStream_t) */
+int pgb_case_stream(const pgb_case *c, void **stream);
+
+/* the device time of the last pgb_step, milliseconds (CUDA events) */
+int pgb_last_step_ms(const pgb_case *c, float *ms);
+
+/* kernel launches the last pgb_step queued, per step */
+int pgb_launches_per_step(const pgb_case *c, int path, int *count);
+
+/* the tile shape the batched kernel uses for blk (set by the autotuner or the
+ * caller) */
+int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk);
+int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk);
+
+/* whether blk runs in the uniform-metric form (1) or reads its metric arrays (0) */
+int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

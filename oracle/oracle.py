@@ -1,0 +1,224 @@
+"""TEST INFRASTRUCTURE ONLY: the CPU oracle's Python side.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg import this module, as the checker of the device path; the product never
+does.  It loads ``oracle/liboracle.so`` (the C restatement in
+``pg_oracle.cpp``, built by ``oracle/build.sh``) and drives it the way the
+reference's solver drives its kernels:
+
+* the halo windows of every interface, as the reference's exchange lays them
+  out (peregrine/multiblock/collections/exchange/collection.py:63-96,
+  peregrine/launch/ranges.py:32-40): the interface plane proper, never the
+  halo's edges or corners;
+* the Runge-Kutta stages as the reference's integrators make them
+  (peregrine/integrators/rungekutta.py:9-92, peregrine/integrators/base.py:122-137):
+  one right-hand side, then each stage's combine kernels in order.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+_halo_dtype = np.dtype([(n, np.int32) for n in ("dblk", "di", "dj", "dk", "sblk", "si", "sj", "sk", "layer")])
+
+
+class OCase(ctypes.Structure):
+    _fields_ = [("simulator", ctypes.c_int), ("primary", ctypes.c_int), ("ns", ctypes.c_int),
+                ("alpha", ctypes.c_double)] + \
+               [(n, ctypes.POINTER(ctypes.c_double)) for n in
+                ("Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0", "kappa0", "MWqinv", "wilkepair", "lewis")] + \
+               [("Ru", ctypes.c_double)]
+
+
+class OBlock(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("ng", ctypes.c_int),
+                ("Q", ctypes.POINTER(ctypes.c_double)),
+                ("xcc", ctypes.POINTER(ctypes.c_double)), ("detJinv", ctypes.POINTER(ctypes.c_double)),
+                ("Jinv", ctypes.POINTER(ctypes.c_double)),
+                ("S", ctypes.POINTER(ctypes.c_double) * 3), ("xf", ctypes.POINTER(ctypes.c_double) * 3)]
+
+
+def _lib():
+    if not os.path.exists(LIB):
+        raise RuntimeError(f"{LIB} is not built; run oracle/build.sh")
+    lib = ctypes.CDLL(LIB)
+    lib.oracle_rhs.restype = ctypes.c_int
+    lib.oracle_fromprims.restype = ctypes.c_int
+    lib.oracle_combine.restype = ctypes.c_int
+    return lib
+
+
+def _ptr(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def halo_map(blocks):
+    """Every face-halo cell of every block and the neighbour cell it copies.
+
+    Identity orientation ("123"), which is what the lattice meshers make: a low
+    face's halo layer l is the neighbour's l-th cell in from its high face.
+    """
+    rows = []
+    for blk in blocks:
+        g = blk.ng
+        n = blk.cells
+        for face in blk.intfaces:
+            if face.nbr is None:
+                continue
+            a = face.axis
+            nbr = blocks[face.nbr]
+            m = nbr.cells
+            other = [d for d in range(3) if d != a]
+            grid = np.meshgrid(*[np.arange(g, g + n[d]) for d in other], indexing="ij")
+            for layer in range(g):
+                dst = [None] * 3
+                src = [None] * 3
+                for d, gd in zip(other, grid):
+                    dst[d] = gd.ravel()
+                    src[d] = gd.ravel()
+                cnt = dst[other[0]].size
+                if face.is_low:
+                    dst[a] = np.full(cnt, g - 1 - layer)
+                    src[a] = np.full(cnt, g + m[a] - 1 - layer)
+                else:
+                    dst[a] = np.full(cnt, g + n[a] + layer)
+                    src[a] = np.full(cnt, g + layer)
+                r = np.zeros(cnt, _halo_dtype)
+                r["dblk"], r["sblk"], r["layer"] = blk.nblki, face.nbr, layer
+                r["di"], r["dj"], r["dk"] = dst
+                r["si"], r["sj"], r["sk"] = src
+                rows.append(r)
+    return np.concatenate(rows) if rows else np.zeros(0, _halo_dtype)
+
+
+def stage_combines(integrator, nregs_names):
+    """Each stage's combines as (out, own weight or None, [(register, weight)], step).
+
+    The reference's combine bookkeeping (peregrine/integrators/base.py:122-137)
+    on its stage tables (peregrine/integrators/rungekutta.py:42-92).
+    """
+    def combine(out, pairs, step=True):
+        weights = {}
+        for reg, w in pairs:
+            weights[reg] = weights.get(reg, 0.0) + w
+        own = weights.pop(out, 0.0)
+        reads = [(r, w) for r, w in weights.items() if w != 0.0]
+        return (out, own if own != 0.0 else None, reads, step)
+
+    R = nregs_names
+    if integrator == "rk4":
+        start, stage, total, dQ = R
+        rows = ((0.0, 0.5, 1.0 / 6.0), (0.5, 0.5, 1.0 / 3.0), (0.5, 1.0, 1.0 / 3.0), (1.0, None, 1.0 / 6.0))
+        out = []
+        for n, (_, wdQ, wsum) in enumerate(rows):
+            own = 0.0 if n == 0 else 1.0
+            share = combine(total, [(total, own), (dQ, wsum)])
+            if wdQ is None:
+                out.append(("stage", stage if n else start, [share, combine(start, [(start, 1.0), (total, 1.0)], step=False)]))
+            else:
+                out.append(("stage", start if n == 0 else stage, [share, combine(stage, [(start, 1.0), (dQ, wdQ)])]))
+        return [(q, cs) for _, q, cs in out], dQ
+    tables = {
+        "rk1": ((0.0, 0.0, 1.0, 1.0),),
+        "rk2": ((0.0, 0.0, 1.0, 1.0), (1.0, 0.5, 0.5, 0.5)),
+        "tvd-rk3": ((0.0, 0.0, 1.0, 1.0), (1.0, 0.75, 0.25, 0.25), (0.5, 1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)),
+        "rk34": ((0.0, 0.0, 1.0, 0.5), (0.5, 0.0, 1.0, 0.5), (1.0, 2.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0), (0.5, 0.0, 1.0, 0.5)),
+    }
+    stages = tables[integrator]
+    start, stage, dQ = R[0], R[1], R[-1]
+    last = len(stages) - 1
+    out = []
+    for n, (_, wQ0, wQ, wdQ) in enumerate(stages):
+        Q = start if n == 0 else stage
+        Qout = start if n == last else stage
+        out.append((Q, [combine(Qout, [(Q, wQ), (start, wQ0), (dQ, wdQ)])]))
+    return out, dQ
+
+
+NREGS = {"rk1": 2, "rk2": 3, "tvd-rk3": 3, "rk34": 3, "rk4": 4}
+
+
+class Oracle:
+    """The reference's right-hand side and stepping, on host arrays.
+
+    ``blocks`` are mesher blocks (nodes and connectivity); ``metrics`` one dict
+    per block of the arrays ``peregrine_b200.grid.metrics`` makes.
+    """
+
+    def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0):
+        self.lib = _lib()
+        self.ns, self.ne = ns, 4 + ns
+        self.blocks = blocks
+        self.metrics = [{k: np.ascontiguousarray(v, dtype=np.float64) for k, v in m.items()} for m in metrics]
+        self.integrator = integrator
+        self._tables = {}
+        c = OCase()
+        c.simulator = 1 if simulator == "navier-stokes" else 0
+        c.primary = 0
+        c.ns = ns
+        c.alpha = alpha
+        c.Ru = float(constants["Ru"])
+        names = dict(Rsp="Rsp", cp0="cp0", h298R="h298R", MWinv="MWinv", h298="h298",
+                     mu0="mu0", kappa0="kappa0", MWqinv="MWqinv", wilkepair="wilkepair", lewis="lewis")
+        for field, key in names.items():
+            arr = np.ascontiguousarray(constants.get(key, np.ones(ns)), dtype=np.float64).ravel()
+            self._tables[field] = arr
+            setattr(c, field, _ptr(arr))
+        hp = np.ascontiguousarray(np.asarray(constants["hpoly"])[:, 0], dtype=np.float64)
+        self._tables["hpoly0"] = hp
+        c.hpoly0 = _ptr(hp)
+        self.case = c
+        self.map = halo_map(blocks)
+        self.nregs = NREGS[integrator]
+        self.regs = [[np.zeros(self._shape(b)) for b in blocks] for _ in range(self.nregs)]
+
+    def _shape(self, blk):
+        return tuple(n + 2 * blk.ng for n in blk.cells) + (self.ne,)
+
+    def _oblocks(self, Q):
+        obs = (OBlock * len(self.blocks))()
+        keep = []
+        for n, (blk, m) in enumerate(zip(self.blocks, self.metrics)):
+            o = obs[n]
+            o.nx, o.ny, o.nz = blk.cells
+            o.ng = blk.ng
+            o.Q = _ptr(Q[n])
+            o.xcc, o.detJinv, o.Jinv = _ptr(m["xcc"]), _ptr(m["detJinv"]), _ptr(m["Jinv"])
+            for a, d in enumerate("ijk"):
+                o.S[a] = _ptr(m[f"{d}S"])
+                o.xf[a] = _ptr(m[f"{d}xc"])
+            keep.append(o)
+        return obs
+
+    def set_prims(self, prims):
+        for blk, q, Q in zip(self.blocks, prims, self.regs[0]):
+            q = np.ascontiguousarray(q, dtype=np.float64)
+            assert q.shape == Q.shape
+            self.lib.oracle_fromprims(ctypes.byref(self.case), _ptr(q), _ptr(Q), ctypes.c_long(Q.size // self.ne))
+
+    def rhs(self, Q, dQ):
+        obs = self._oblocks(Q)
+        m = np.ascontiguousarray(self.map)
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(dQ))(*[_ptr(d) for d in dQ])
+        rc = self.lib.oracle_rhs(ctypes.byref(self.case), obs, len(self.blocks),
+                                 m.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(m.size), ptrs)
+        if rc:
+            raise RuntimeError(f"oracle_rhs: {rc}")
+
+    def step(self, dt):
+        names = list(range(self.nregs))
+        stages, dQ = stage_combines(self.integrator, names)
+        for Q, combines in stages:
+            self.rhs(self.regs[Q], self.regs[dQ])
+            for out, own, reads, step in combines:
+                for b, blk in enumerate(self.blocks):
+                    X = (ctypes.POINTER(ctypes.c_double) * len(reads))(*[_ptr(self.regs[r][b]) for r, _ in reads])
+                    w = (ctypes.c_double * len(reads))(*[wt for _, wt in reads])
+                    self.lib.oracle_combine(*blk.cells, blk.ng, self.ne, _ptr(self.regs[out][b]),
+                                            int(own is not None), ctypes.c_double(own or 0.0),
+                                            len(reads), X, w, int(step), ctypes.c_double(dt))

@@ -1,0 +1,495 @@
+// TEST INFRASTRUCTURE ONLY: the CPU oracle the parity tests, smoke() and the
+// bench's CPU-baseline leg check the device path against.  Nothing in the
+// product links, loads or calls it.
+//
+// A CPU restatement of PEREGRINE's right-hand side and Runge-Kutta stage for
+// the calorically perfect gas, in the reference's own structure: separate
+// passes over the blocks in the order its slot graphs run them
+// (peregrine/simulator/advec/simulator.py:57-87,
+//  peregrine/simulator/advecdiff/simulator.py:110-124), each pass the
+// reference template's arithmetic in the same operation order.  Every
+// function cites the template it follows.  Built with -ffp-contract=off so no
+// multiply-add is fused: the arithmetic is IEEE double as numpy's.
+//
+// Arrays are the reference's host views: numpy C order, [i][j][k][comp...],
+// full extents including ng halo layers (peregrine/backend/allocation.py:8-37).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+extern "C" {
+
+enum { O_EULER = 0, O_NAVSTOKES = 1 };
+enum { O_KEPAEC = 0, O_HLLC = 1, O_RUSANOV = 2 };
+
+struct OCase {
+  int simulator;   // O_EULER / O_NAVSTOKES
+  int primary;     // flux function
+  int ns;          // species
+  double alpha;    // alpha-damping coefficient (alpha-damping.mako:11)
+  // species tables, ns long (wilkepair ns*ns, row-major [n][m])
+  const double *Rsp, *cp0, *h298R, *MWinv, *hpoly0, *h298;
+  const double *mu0, *kappa0, *MWqinv, *wilkepair, *lewis;
+  double Ru;
+};
+
+struct OBlock {
+  int nx, ny, nz, ng;                       // interior cells, halo depth
+  double *Q;                                // [nx+2g][ny+2g][nz+2g][ne]
+  const double *xcc, *detJinv, *Jinv;       // cells: [..][3], [..], [..][3][3]
+  const double *S[3], *xf[3];               // faces of axis a: [..][3]
+};
+
+// one halo cell of one block filled from a cell of another (the place kernel,
+// peregrine/multiblock/collections/exchange/kernels/place.mako:11-20, on the
+// windows peregrine/multiblock/collections/exchange/collection.py:63-96 lays
+// out): dst block, dst i j k, src block, src i j k, and the halo layer
+// (0 = next to the interface), all full-array indices.
+struct OHaloEntry {
+  int32_t dblk, di, dj, dk, sblk, si, sj, sk, layer;
+};
+
+}  // extern "C"
+
+namespace {
+
+struct Dims {
+  int X, Y, Z;  // full extents
+  long at(int i, int j, int k) const { return ((long)i * Y + j) * Z + k; }
+};
+
+Dims cells(const OBlock &b) { return {b.nx + 2 * b.ng, b.ny + 2 * b.ng, b.nz + 2 * b.ng}; }
+Dims faces(const OBlock &b, int a) {
+  Dims d = cells(b);
+  if (a == 0) d.X += 1;
+  if (a == 1) d.Y += 1;
+  if (a == 2) d.Z += 1;
+  return d;
+}
+
+// EosState, simulator/mixture/eos/base.py:85-86: p, T, rhoinv, rho, e, cp, gamma, c
+struct State {
+  double p, T, rhoinv, rho, e, cp, gamma, c;
+};
+enum { NSTATE = 8 };
+
+// mixmom, simulator/mixture/eos/kernels/mixing.mako:3-30; cpg's moments are
+// R <- Rsp, cp <- cp0, h298 <- h298R (simulator/mixture/eos/cpg/__init__.py)
+struct Mom {
+  double R, cp, h298;
+};
+template <class YF> Mom mixmom(const OCase &c, YF Y) {
+  Mom m{0.0, 0.0, 0.0};
+  double Ylast = 1.0;
+  for (int n = 0; n < c.ns - 1; n++) {
+    const double Yn = Y(n);
+    Ylast -= Yn;
+    m.R += Yn * c.Rsp[n];
+    m.cp += Yn * c.cp0[n];
+    m.h298 += Yn * c.h298R[n];
+  }
+  m.R += Ylast * c.Rsp[c.ns - 1];
+  m.cp += Ylast * c.cp0[c.ns - 1];
+  m.h298 += Ylast * c.h298R[c.ns - 1];
+  return m;
+}
+
+// fromQ (simulator/euler/kernels/state/fromQ.mako:5-19), efromQ
+// (simulator/euler/kernels/solution.mako:10-12) and cpg's fromrhoE
+// (simulator/mixture/eos/cpg/kernels/eos.mako:5-15)
+State fromQ(const OCase &c, const double *Q) {
+  const double rho = Q[0], rhoinv = 1.0 / rho;
+  const double e = (Q[4] - 0.5 * ((Q[1]) * (Q[1]) + (Q[2]) * (Q[2]) + (Q[3]) * (Q[3])) * rhoinv) * rhoinv;
+  Mom mom = mixmom(c, [&](int n) { return Q[5 + n] * rhoinv; });
+  State s;
+  const double cv = mom.cp - mom.R;
+  s.rho = rho;
+  s.rhoinv = 1.0 / rho;
+  s.e = e;
+  s.T = (e - mom.h298) / cv;
+  s.p = rho * mom.R * s.T;
+  s.cp = mom.cp;
+  s.gamma = mom.cp / cv;
+  s.c = std::sqrt(s.gamma * mom.R * s.T);
+  return s;
+}
+
+// fromprims (simulator/euler/kernels/state/fromprims.mako:4-12 through
+// solution.mako:2-23 and cpg's frompT, eos.mako:17-27)
+void fromprims(const OCase &c, const double *q, double *Q) {
+  const double p = q[0], T = q[4];
+  const double u[3] = {q[1], q[2], q[3]};
+  Mom mom = mixmom(c, [&](int n) { return q[5 + n]; });
+  const double cv = mom.cp - mom.R;
+  const double rho = p / (mom.R * T);
+  const double e = cv * T + mom.h298;
+  Q[0] = rho;
+  Q[1] = rho * u[0];
+  Q[2] = rho * u[1];
+  Q[3] = rho * u[2];
+  Q[4] = rho * (e + 0.5 * ((u[0]) * (u[0]) + (u[1]) * (u[1]) + (u[2]) * (u[2])));
+  for (int n = 0; n < c.ns - 1; n++) Q[5 + n] = rho * q[5 + n];
+}
+
+// transport (simulator/navstokes/kernels/transport.mako:5-35) with constant
+// species properties (simulator/mixture/transport/kernels/constant.mako:5-16),
+// Wilke's rule (simulator/mixture/mixrule/kernels/wilke.mako:3-17), the
+// series/parallel conductivity (simulator/mixture/transport/kernels/mixing.mako:3-10),
+// Lewis diffusivities (simulator/mixture/diffusion/kernels/lewis.mako:3-8) and
+// the species enthalpies (simulator/mixture/eos/kernels/species.mako:9-36)
+void transport(const OCase &c, const double *Q, const State &st, double *tr, double *hsp) {
+  const int ns = c.ns;
+  const double rho = Q[0], rhoinv = 1.0 / rho;
+  double Ylast = 1.0;
+  for (int n = 0; n < ns - 1; n++) Ylast -= Q[5 + n] * rhoinv;
+  Ylast = std::fmax(Ylast, 0.0);
+  auto Y = [&](int n) { return n < ns - 1 ? Q[5 + n] * rhoinv : Ylast; };
+  double denom = 0.0;
+  for (int n = 0; n < ns; n++) denom += Y(n) * c.MWinv[n];
+  const double MWmix = 1.0 / denom;
+  auto X = [&](int n) { return Y(n) * c.MWinv[n] * MWmix; };
+  const double T = st.T;
+  std::vector<double> sqrtmu(ns), sinv(ns), kappasp(ns);
+  for (int n = 0; n < ns; n++) sqrtmu[n] = std::sqrt(c.mu0[n]);
+  for (int n = 0; n < ns; n++) sinv[n] = 1.0 / (sqrtmu[n] * c.MWqinv[n]);
+  double mu = 0.0;
+  for (int n = 0; n < ns; n++) {
+    const double sn = sqrtmu[n] * c.MWqinv[n];
+    double phi = 0.0;
+    for (int m = 0; m < ns; m++) {
+      const double r = 1.0 + sn * sinv[m];
+      phi += r * r * c.wilkepair[n * ns + m] * X(m);
+    }
+    mu += sqrtmu[n] * sqrtmu[n] * X(n) / phi;
+  }
+  for (int n = 0; n < ns; n++) kappasp[n] = c.kappa0[n];
+  double series = 0.0, parallel = 0.0;
+  for (int n = 0; n < ns; n++) {
+    series += X(n) * kappasp[n];
+    parallel += X(n) / kappasp[n];
+  }
+  const double kappa = 0.5 * (series + 1.0 / parallel);
+  tr[0] = mu;
+  tr[1] = kappa;
+  const double kor = kappa * rhoinv / st.cp;
+  for (int n = 0; n < ns; n++) tr[2 + n] = kor / c.lewis[n];
+  const double u = std::log(T), Tinv = 1.0 / T;
+  for (int n = 0; n < ns; n++) {
+    double hRT = 0.0;
+    hRT = hRT * u + c.hpoly0[n];
+    hRT += c.h298[n] * Tinv;
+    hsp[n] = hRT * T * c.Ru * c.MWinv[n];
+  }
+}
+
+// a face's side: the cell's state plus its velocity as Q[1..3] / Q[0]
+// (simulator/euler/kernels/flux/recon/constant.mako:3-18)
+struct Side {
+  State s;
+  double u, v, w;
+};
+Side side(const double *Q, const State &st) {
+  return Side{st, Q[1] / Q[0], Q[2] / Q[0], Q[3] / Q[0]};
+}
+
+// kepaec (simulator/euler/kernels/flux/function/kepaec.mako:2-20)
+void kepaec(const OCase &c, const Side &L, const Side &R, const double *QL, const double *QR,
+            const double *S, double *F) {
+  const double uf = 0.5 * (R.u + L.u), vf = 0.5 * (R.v + L.v), wf = 0.5 * (R.w + L.w);
+  const double U = ((S[0]) * (uf) + (S[1]) * (vf) + (S[2]) * (wf));
+  const double pf = 0.5 * (R.s.p + L.s.p);
+  const double rho = 0.5 * (R.s.rho + L.s.rho);
+  const double C = rho * U;
+  F[0] = C;
+  F[1] = C * uf + pf * S[0];
+  F[2] = C * vf + pf * S[1];
+  F[3] = C * wf + pf * S[2];
+  const double Kj = C * 0.5 * ((R.u) * (L.u) + (R.v) * (L.v) + (R.w) * (L.w));
+  const double Pj = 0.5 * (L.s.p * ((R.u) * (S[0]) + (R.v) * (S[1]) + (R.w) * (S[2])) +
+                           R.s.p * ((L.u) * (S[0]) + (L.v) * (S[1]) + (L.w) * (S[2])));
+  const double thL = L.s.cp / L.s.gamma * L.s.T, thR = R.s.cp / R.s.gamma * R.s.T;
+  const double ef = 2.0 * thL * thR / (thL + thR) + 0.5 * ((L.s.e - thL) + (R.s.e - thR));
+  F[4] = ef * C + Kj + Pj;
+  for (int n = 0; n < c.ns - 1; n++) F[5 + n] = 0.5 * (QR[5 + n] / QR[0] + QL[5 + n] / QL[0]) * C;
+}
+
+// alpha damping (simulator/navstokes/kernels/flux/alpha-damping.mako:3-92)
+void alphadamping(const OCase &c, const double *S, const double *xf, const double *xccL,
+                  const double *xccR, const double *QL, const double *QR, const State &stateL,
+                  const State &stateR, const double *trL, const double *trR, const double *hspL,
+                  const double *hspR, const double *gL, const double *gR, double *F) {
+  const int ns = c.ns;
+  const double alpha = c.alpha, bulkvisc = 0.0;
+  const double Sabs = std::sqrt(((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2]))), Sinv = 1.0 / Sabs;
+  const double nx = S[0] * Sinv, ny = S[1] * Sinv, nz = S[2] * Sinv;
+  const double mu = 0.5 * (trR[0] + trL[0]);
+  const double kappa = 0.5 * (trR[1] + trL[1]);
+  const double lambda = bulkvisc - 2.0 / 3.0 * mu;
+  const double rhoinvL = stateL.rhoinv, rhoinvR = stateR.rhoinv;
+  const double uL = QL[1] * rhoinvL, vL = QL[2] * rhoinvL, wL = QL[3] * rhoinvL;
+  const double uR = QR[1] * rhoinvR, vR = QR[2] * rhoinvR, wR = QR[3] * rhoinvR;
+  const double ex = xccR[0] - xccL[0], ey = xccR[1] - xccL[1], ez = xccR[2] - xccL[2];
+  const double en0 = ex * nx, en1 = ey * ny, en2 = ez * nz;
+  const double dampinv = alpha / std::sqrt(en0 * en0 + en1 * en1 + en2 * en2);
+  const double dampx = dampinv * nx, dampy = dampinv * ny, dampz = dampinv * nz;
+  const double xLx = xf[0] - xccL[0], xLy = xf[1] - xccL[1], xLz = xf[2] - xccL[2];
+  const double xRx = xf[0] - xccR[0], xRy = xf[1] - xccR[1], xRz = xf[2] - xccR[2];
+  auto facegrad = [&](int l, double phiL, double phiR, double &gx, double &gy, double &gz) {
+    const double gLx = gL[3 * l + 0], gLy = gL[3 * l + 1], gLz = gL[3 * l + 2];
+    const double gRx = gR[3 * l + 0], gRy = gR[3 * l + 1], gRz = gR[3 * l + 2];
+    const double wl = phiL + gLx * xLx + gLy * xLy + gLz * xLz;
+    const double wr = phiR + gRx * xRx + gRy * xRy + gRz * xRz;
+    const double jump = wr - wl;
+    gx = 0.5 * (gRx + gLx) + dampx * jump;
+    gy = 0.5 * (gRy + gLy) + dampy * jump;
+    gz = 0.5 * (gRz + gLz) + dampz * jump;
+  };
+  double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
+  facegrad(0, uL, uR, dudx, dudy, dudz);
+  facegrad(1, vL, vR, dvdx, dvdy, dvdz);
+  facegrad(2, wL, wR, dwdx, dwdy, dwdz);
+  const double div = dudx + dvdy + dwdz;
+  const double txx = -2.0 * mu * dudx - lambda * div;
+  const double txy = -mu * (dvdx + dudy);
+  const double txz = -mu * (dwdx + dudz);
+  const double tyy = -2.0 * mu * dvdy - lambda * div;
+  const double tyz = -mu * (dwdy + dvdz);
+  const double tzz = -2.0 * mu * dwdz - lambda * div;
+  F[1] += txx * S[0] + txy * S[1] + txz * S[2];
+  F[2] += txy * S[0] + tyy * S[1] + tyz * S[2];
+  F[3] += txz * S[0] + tyz * S[1] + tzz * S[2];
+  double dTx, dTy, dTz;
+  facegrad(3, stateL.T, stateR.T, dTx, dTy, dTz);
+  const double heatflux = -kappa * (dTx * S[0] + dTy * S[1] + dTz * S[2]);
+  const double uf = 0.5 * (uR + uL), vf = 0.5 * (vR + vL), wf = 0.5 * (wR + wL);
+  double f4 = (uf * txx + vf * txy + wf * txz) * S[0] + (uf * txy + vf * tyy + wf * tyz) * S[1] +
+              (uf * txz + vf * tyz + wf * tzz) * S[2] + heatflux;
+  double YlastL = 1.0, YlastR = 1.0;
+  for (int n = 0; n < ns - 1; n++) {
+    YlastL -= QL[5 + n] * rhoinvL;
+    YlastR -= QR[5 + n] * rhoinvR;
+  }
+  auto YL = [&](int n) { return n < ns - 1 ? QL[5 + n] * rhoinvL : YlastL; };
+  auto YR = [&](int n) { return n < ns - 1 ? QR[5 + n] * rhoinvR : YlastR; };
+  double Dk, Vc = 0.0, gradYns = 0.0, sumYh = 0.0, Yns = 1.0;
+  const double rho = 0.5 * (QR[0] + QL[0]);
+  for (int n = 0; n < ns - 1; n++) {
+    Dk = 0.5 * (trR[2 + n] + trL[2 + n]);
+    double dYx, dYy, dYz;
+    facegrad(4 + n, YL(n), YR(n), dYx, dYy, dYz);
+    const double gradYk = dYx * S[0] + dYy * S[1] + dYz * S[2];
+    gradYns -= gradYk;
+    Vc += Dk * gradYk;
+    const double Jk = -rho * Dk * gradYk;
+    const double hk = 0.5 * (hspR[n] + hspL[n]);
+    const double Yk = 0.5 * (YR(n) + YL(n));
+    Yns -= Yk;
+    sumYh += Yk * hk;
+    F[5 + n] += Jk;
+    f4 += Jk * hk;
+  }
+  Dk = 0.5 * (trR[2 + ns - 1] + trL[2 + ns - 1]);
+  Vc += Dk * gradYns;
+  const double corr = rho * Vc;
+  for (int n = 0; n < ns - 1; n++) F[5 + n] += 0.5 * (YR(n) + YL(n)) * corr;
+  f4 += corr * sumYh;
+  const double hns = 0.5 * (hspR[ns - 1] + hspL[ns - 1]);
+  f4 += (-rho * Dk * gradYns + Yns * corr) * hns;
+  F[4] += f4;
+}
+
+// the per-block scratch one right-hand side fills, as the reference's arrays
+struct Scratch {
+  std::vector<double> state, tr, hsp, grads, F[3];
+};
+
+void halo_fill(std::vector<OBlock> &blks, const OHaloEntry *map, long nmap, int maxlayer, int comps,
+               double *(*arr)(OBlock &, std::vector<Scratch> &, int), std::vector<Scratch> &scr) {
+  for (long m = 0; m < nmap; m++) {
+    const OHaloEntry &h = map[m];
+    if (h.layer >= maxlayer) continue;
+    OBlock &d = blks[h.dblk];
+    OBlock &s = blks[h.sblk];
+    double *dp = arr(d, scr, h.dblk) + cells(d).at(h.di, h.dj, h.dk) * comps;
+    const double *sp = arr(s, scr, h.sblk) + cells(s).at(h.si, h.sj, h.sk) * comps;
+    std::memcpy(dp, sp, sizeof(double) * comps);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// The right-hand side of every block: dQ = the flux divergence of Q.
+// prerhs: Q's halo exchanged, fromQ everywhere it is read, transport on the
+// interior and first halo layer; rhs: gradients on the interior and their
+// one-plane exchange, advective then diffusive face fluxes on the interior
+// faces, applyflux (simulator/advec/kernels/applyflux.mako:2-11).
+int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *map, long nmap,
+               double **dQ) {
+  const OCase &c = *cp;
+  const int ns = c.ns, ne = 4 + ns, ngrad = ne - 1;
+  const bool visc = c.simulator == O_NAVSTOKES;
+  std::vector<OBlock> blks(blocks, blocks + nblocks);
+  std::vector<Scratch> scr(nblocks);
+  // Q's halo: every layer (simulator/advec/simulator.py:57-63)
+  halo_fill(blks, map, nmap, 1 << 30, ne, [](OBlock &b, std::vector<Scratch> &, int) { return b.Q; }, scr);
+  for (int b = 0; b < nblocks; b++) {
+    OBlock &B = blks[b];
+    const Dims d = cells(B);
+    const long N = (long)d.X * d.Y * d.Z;
+    Scratch &s = scr[b];
+    s.state.assign(N * NSTATE, 0.0);
+    s.tr.assign(N * (2 + ns), 0.0);
+    s.hsp.assign(N * ns, 0.0);
+    s.grads.assign(N * ngrad * 3, 0.0);
+    // the state wherever Q is set: interior and the face halos (edges and
+    // corners of the halo hold no density and are never read)
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int i = 0; i < d.X; i++)
+      for (int j = 0; j < d.Y; j++)
+        for (int k = 0; k < d.Z; k++) {
+          const int out = (i < B.ng || i >= d.X - B.ng) + (j < B.ng || j >= d.Y - B.ng) +
+                          (k < B.ng || k >= d.Z - B.ng);
+          if (out > 1) continue;
+          const long at = d.at(i, j, k);
+          State st = fromQ(c, B.Q + at * ne);
+          std::memcpy(&s.state[at * NSTATE], &st, sizeof(State));
+          if (visc) {
+            // the shallow range: interior plus one halo layer
+            const int deep = (i < B.ng - 1 || i > d.X - B.ng) + (j < B.ng - 1 || j > d.Y - B.ng) +
+                             (k < B.ng - 1 || k > d.Z - B.ng);
+            if (!deep) transport(c, B.Q + at * ne, st, &s.tr[at * (2 + ns)], &s.hsp[at * ns]);
+          }
+        }
+    if (visc) {
+      // dqdxyz (simulator/navstokes/kernels/dqdxyz.mako:16-41) on the interior
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int i = B.ng; i < d.X - B.ng; i++)
+        for (int j = B.ng; j < d.Y - B.ng; j++)
+          for (int k = B.ng; k < d.Z - B.ng; k++) {
+            const long at = d.at(i, j, k);
+            const double *QpI = B.Q + d.at(i + 1, j, k) * ne, *QmI = B.Q + d.at(i - 1, j, k) * ne;
+            const double *QpJ = B.Q + d.at(i, j + 1, k) * ne, *QmJ = B.Q + d.at(i, j - 1, k) * ne;
+            const double *QpK = B.Q + d.at(i, j, k + 1) * ne, *QmK = B.Q + d.at(i, j, k - 1) * ne;
+            const double TpI = s.state[d.at(i + 1, j, k) * NSTATE + 1], TmI = s.state[d.at(i - 1, j, k) * NSTATE + 1];
+            const double TpJ = s.state[d.at(i, j + 1, k) * NSTATE + 1], TmJ = s.state[d.at(i, j - 1, k) * NSTATE + 1];
+            const double TpK = s.state[d.at(i, j, k + 1) * NSTATE + 1], TmK = s.state[d.at(i, j, k - 1) * NSTATE + 1];
+            const double *J = B.Jinv + at * 9;
+            double *g = &s.grads[at * ngrad * 3];
+            const double rIp = QpI[0], rIm = QmI[0], invI = 1.0 / (rIp * rIm);
+            const double rJp = QpJ[0], rJm = QmJ[0], invJ = 1.0 / (rJp * rJm);
+            const double rKp = QpK[0], rKm = QmK[0], invK = 1.0 / (rKp * rKm);
+            auto phys = [&](int l, const double *dd) {
+              for (int e = 0; e < 3; e++) g[3 * l + e] = dd[0] * J[0 * 3 + e] + dd[1] * J[1 * 3 + e] + dd[2] * J[2 * 3 + e];
+            };
+            for (int l = 0; l < ngrad; l++) {
+              if (l == 3) {
+                const double dd[3] = {0.5 * (TpI - TmI), 0.5 * (TpJ - TmJ), 0.5 * (TpK - TmK)};
+                phys(l, dd);
+                continue;
+              }
+              const int m = l + 1;
+              const double dd[3] = {0.5 * (QpI[m] * rIm - QmI[m] * rIp) * invI,
+                                    0.5 * (QpJ[m] * rJm - QmJ[m] * rJp) * invJ,
+                                    0.5 * (QpK[m] * rKm - QmK[m] * rKp) * invK};
+              phys(l, dd);
+            }
+          }
+    }
+  }
+  if (visc) {
+    // grads: one halo plane (simulator/advecdiff/simulator.py:11-14, 116-117)
+    halo_fill(blks, map, nmap, 1, ngrad * 3,
+              [](OBlock &, std::vector<Scratch> &s, int b) { return s[b].grads.data(); }, scr);
+  }
+  for (int b = 0; b < nblocks; b++) {
+    OBlock &B = blks[b];
+    const Dims d = cells(B);
+    Scratch &s = scr[b];
+    const int g = B.ng;
+    for (int a = 0; a < 3; a++) {
+      const Dims f = faces(B, a);
+      s.F[a].assign((long)f.X * f.Y * f.Z * ne, 0.0);
+      const int hi[3] = {B.nx + (a == 0), B.ny + (a == 1), B.nz + (a == 2)};
+      // the interior faces of axis a: a face is indexed like the cell to its right
+      // (peregrine/launch/policy.py:78-86)
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int i = g; i < g + hi[0]; i++)
+        for (int j = g; j < g + hi[1]; j++)
+          for (int k = g; k < g + hi[2]; k++) {
+            const long at = f.at(i, j, k);
+            const long R = d.at(i, j, k);
+            const long L = d.at(i - (a == 0), j - (a == 1), k - (a == 2));
+            const double *QL = B.Q + L * ne, *QR = B.Q + R * ne;
+            const State &sL = *reinterpret_cast<const State *>(&s.state[L * NSTATE]);
+            const State &sR = *reinterpret_cast<const State *>(&s.state[R * NSTATE]);
+            double *F = &s.F[a][at * ne];
+            const double *S = B.S[a] + at * 3;
+            kepaec(c, side(QL, sL), side(QR, sR), QL, QR, S, F);
+            if (visc)
+              alphadamping(c, S, B.xf[a] + at * 3, B.xcc + L * 3, B.xcc + R * 3, QL, QR, sL, sR,
+                           &s.tr[L * (2 + ns)], &s.tr[R * (2 + ns)], &s.hsp[L * ns], &s.hsp[R * ns],
+                           &s.grads[L * ngrad * 3], &s.grads[R * ngrad * 3], F);
+          }
+    }
+    const Dims fi = faces(B, 0), fj = faces(B, 1), fk = faces(B, 2);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int i = g; i < g + B.nx; i++)
+      for (int j = g; j < g + B.ny; j++)
+        for (int k = g; k < g + B.nz; k++) {
+          const double *iFl = &s.F[0][fi.at(i, j, k) * ne], *iFh = &s.F[0][fi.at(i + 1, j, k) * ne];
+          const double *jFl = &s.F[1][fj.at(i, j, k) * ne], *jFh = &s.F[1][fj.at(i, j + 1, k) * ne];
+          const double *kFl = &s.F[2][fk.at(i, j, k) * ne], *kFh = &s.F[2][fk.at(i, j, k + 1) * ne];
+          const long at = d.at(i, j, k);
+          const double detJinv = B.detJinv[at];
+          for (int l = 0; l < ne; l++)
+            dQ[b][at * ne + l] = (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
+        }
+  }
+  return 0;
+}
+
+// fromprims over every cell a block has (interior and halos)
+int oracle_fromprims(const OCase *cp, const double *q, double *Q, long ncells) {
+  const int ne = 4 + cp->ns;
+#pragma omp parallel for schedule(static)
+  for (long n = 0; n < ncells; n++) fromprims(*cp, q + n * ne, Q + n * ne);
+  return 0;
+}
+
+// One stage's combine (peregrine/integrators/kernels/combine.mako:1-13) on a
+// block's interior: out = wout out + sum_n w_n X_n, dt on the last term when
+// step is set, summed left to right as the rendered expression is.  own says
+// whether wout out is a term at all.
+int oracle_combine(int nx, int ny, int nz, int ng, int ne, double *out, int own, double wout,
+                   int nterms, const double *const *X, const double *w, int step, double dt) {
+  const Dims d{nx + 2 * ng, ny + 2 * ng, nz + 2 * ng};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = ng; i < ng + nx; i++)
+    for (int j = ng; j < ng + ny; j++)
+      for (int k = ng; k < ng + nz; k++) {
+        const long at = d.at(i, j, k) * ne;
+        for (int l = 0; l < ne; l++) {
+          auto term = [&](int n) {
+            return (step && n == nterms - 1) ? w[n] * dt * X[n][at + l] : w[n] * X[n][at + l];
+          };
+          double acc;
+          int n0;
+          if (own) {
+            acc = wout * out[at + l];
+            n0 = 0;
+          } else {
+            acc = term(0);
+            n0 = 1;
+          }
+          for (int n = n0; n < nterms; n++) acc = acc + term(n);
+          out[at + l] = acc;
+        }
+      }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,60 @@
+// Device layout of a case's arrays.
+//
+// Every register (Q, Q1, ... in the reference's naming,
+// peregrine/launch/arrays.py:37-39) is one allocation holding every block.
+// With cv[b] the cells of the blocks before b and C components per cell,
+// block b's component c starts at C * cv[b] + c * vol[b] doubles, and its cell
+// (i, j, k), counted from the first halo layer, sits at i + X * (j + Y * k)
+// inside that.  i runs fastest, components outermost: the reference's device
+// F order (peregrine/backend/device/backend.py:57-58), with the blocks laid
+// end to end.  The metric arrays share the layout, 31 components per cell.
+// A face array of axis a keeps face f at the index of the cell on its high
+// side (the reference indexes a face like the cell to its right,
+// peregrine/launch/policy.py:78-86), so faces use the cell layout too.
+#pragma once
+#include <cstdint>
+
+namespace pgb {
+
+constexpr int NG = 2;  // halo layers: the fused stage's stencil reaches two cells
+
+// metric components inside the metric allocation
+enum {
+  M_XCC = 0, M_DETJINV = 3, M_JINV = 4, M_S = 13, M_XF = 22, M_NCOMP = 31
+};
+
+struct BlockDev {
+  int nx, ny, nz;     // interior cells
+  int X, Y, Z;        // full extents, nx + 2 NG ...
+  long long vol;      // X * Y * Z
+  long long cv;       // cells of the blocks before this one
+  int uniform;        // 1: the metrics are the per-axis constants below
+  // uniform form, every value read off the block's own metric arrays
+  double S[3];        // the area vector's normal component of an a-face
+  double detJinv;
+  double Jd[3];       // inverse Jacobian diagonal
+  double ex[3];       // xcc(R) - xcc(L) along a
+  double xL[3];       // xf - xcc(L) along a
+  double xR[3];       // xf - xcc(R) along a
+  // per-axis face geometry alpha damping forms, precomputed from the above
+  double damp[3];     // alpha / |e . n| for an a-face (the normal is the axis)
+};
+
+__host__ __device__ __forceinline__ long long cell_index(const BlockDev &b, int fi, int fj, int fk) {
+  return (long long)fi + (long long)b.X * ((long long)fj + (long long)b.Y * fk);
+}
+
+// one cell of a halo filled from another cell: each side's block start in
+// cells (cv), its cell index inside the block and its component stride (vol)
+struct HaloEntry {
+  long long dcv, scv;
+  int didx, sidx, dvol, svol;
+};
+
+// a fused work item: a column of tw x th cells of one block over k0 .. k1 - 1
+struct TileDev {
+  int blk;
+  short i0, j0, tw, th, k0, k1;
+};
+
+}  // namespace pgb

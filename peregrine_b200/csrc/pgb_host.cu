@@ -1,0 +1,1058 @@
+// The host side of pgb200: cases, device arrays, halo tables, the stage plans
+// and the launches, behind the C ABI of include/pgb200.h.
+#include "pgb200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fused.cuh"
+#include "layout.cuh"
+#include "physics.cuh"
+#include "plain.cuh"
+
+using namespace pgb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? PGB_ERR_NOMEM : PGB_ERR_CUDA,            \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+#define RET(call)             \
+  do {                        \
+    int r_ = (call);          \
+    if (r_ != PGB_OK) return r_; \
+  } while (0)
+
+__global__ void k_setscalar(double *p, double v) { *p = v; }
+
+struct HostBlock {
+  int nx, ny, nz;
+  int nbr[6] = {-1, -1, -1, -1, -1, -1};
+  int nbrface[6] = {0, 0, 0, 0, 0, 0};
+  int tw = 0, th = 0, kchunk = 0;
+  bool metrics_set[PGB_NMETRICS] = {};
+  BlockDev dev{};
+};
+
+// a stage's launch plan on the fused path, physical registers resolved
+struct FusedStagePlan {
+  int qin;
+  int ncomb;
+  FusedCombine comb[2];
+};
+
+}  // namespace
+
+struct pgb_case {
+  pgb_physics phys{};
+  Species sp{};
+  std::map<std::string, std::vector<double>> tables;
+  std::vector<HostBlock> blocks;
+  std::vector<pgb_stage> stages;
+  bool finalized = false;
+  int ne = 5;
+  long long cells = 0;  // total cells, halo included
+  // device
+  cudaStream_t stream = nullptr;
+  BlockDev *d_blks = nullptr;
+  double *d_reg[MAXREGS] = {};
+  double *d_met = nullptr;
+  double *d_dt = nullptr;
+  HaloEntry *d_halo = nullptr;
+  long long nhalo = 0, nhalo_l0 = 0;  // all entries; face layer 0 only (first)
+  // per-block path scratch
+  double *d_state = nullptr, *d_tr = nullptr, *d_hsp = nullptr, *d_grads = nullptr, *d_F[3] = {};
+  double *d_prims = nullptr;
+  long long prims_cap = 0;
+  // fused path
+  TileDev *d_tiles = nullptr;
+  int ntiles = 0;
+  unsigned int *d_counter = nullptr;
+  size_t fused_smem = 0;
+  bool tiles_dirty = true;
+  bool uniform_done = false;
+  // register mapping: logical -> physical
+  std::vector<int> phys_of, canonical;
+  int period = 1, phase = 0;
+  std::vector<std::vector<FusedStagePlan>> plans;  // [phase][stage]
+  std::vector<std::vector<int>> maps;              // mapping at the start of each phase
+  // graphs
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  std::vector<int> graph_map[2];  // the mapping a graph was captured under
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.0f;
+  int launches[2] = {0, 0};
+};
+
+namespace {
+
+bool fused_capable(const pgb_case *c) {
+  const pgb_physics &p = c->phys;
+  return p.eos == PGB_EOS_CPG && p.primary == PGB_FLUX_KEPAEC && p.recon == PGB_RECON_CONSTANT && p.ns == 1 &&
+         (p.simulator == PGB_EULER || p.trans == PGB_TRANS_CONSTANT);
+}
+
+const double *table(const pgb_case *c, const char *name) {
+  auto it = c->tables.find(name);
+  return it == c->tables.end() ? nullptr : it->second.data();
+}
+
+// the species tables into the constant struct, and the single-species
+// shortcuts by the same operations the per-cell formulas take for Y = 1
+int build_species(pgb_case *c) {
+  Species &s = c->sp;
+  const int ns = c->phys.ns;
+  s.ns = ns;
+  s.alpha = c->phys.alpha;
+  s.Ru = 8314.46261815324;
+  struct T {
+    const char *name;
+    double *dst;
+    bool need;
+  } list[] = {{"Rsp", s.Rsp, true},        {"cp0", s.cp0, true},          {"h298R", s.h298R, true},
+              {"MWinv", s.MWinv, true},    {"hpoly0", s.hpoly0, false},   {"h298", s.h298, false},
+              {"mu0", s.mu0, false},       {"kappa0", s.kappa0, false},   {"MWqinv", s.MWqinv, false},
+              {"lewis", s.lewis, false}};
+  for (auto &t : list) {
+    const double *v = table(c, t.name);
+    if (!v) {
+      if (t.need) return fail(PGB_ERR_ARG, std::string("species table ") + t.name + " not set");
+      for (int n = 0; n < ns; n++) t.dst[n] = 1.0;
+      continue;
+    }
+    if ((long)c->tables[t.name].size() < ns) return fail(PGB_ERR_ARG, std::string("species table ") + t.name + " short");
+    for (int n = 0; n < ns; n++) t.dst[n] = v[n];
+  }
+  const double *wp = table(c, "wilkepair");
+  for (int n = 0; n < ns; n++)
+    for (int m = 0; m < ns; m++) s.wilkepair[n * MAXNS + m] = wp ? wp[n * ns + m] : 0.25;
+  if (c->phys.trans == PGB_TRANS_CONSTANT && (!table(c, "mu0") || !table(c, "kappa0")))
+    return fail(PGB_ERR_ARG, "constant transport needs mu0 and kappa0");
+  // one species: mixmom gives R = 0 + 1 Rsp exactly, likewise cp and h298
+  s.R1 = 0.0 + 1.0 * s.Rsp[0];
+  s.cp1 = 0.0 + 1.0 * s.cp0[0];
+  s.h2981 = 0.0 + 1.0 * s.h298R[0];
+  s.cv1 = s.cp1 - s.R1;
+  s.cvinv1 = 1.0 / s.cv1;
+  s.gamma1 = s.cp1 / s.cv1;
+  s.th1 = s.cp1 / s.gamma1;
+  if (ns == 1 && c->phys.trans == PGB_TRANS_CONSTANT) {
+    // transport.mako with Y = 1: X = MWinv / MWinv, then Wilke and the conductivity mean
+    volatile double Y = 1.0;
+    const double denom = 0.0 + Y * s.MWinv[0];
+    const double MWmix = 1.0 / denom;
+    const double X = Y * s.MWinv[0] * MWmix;
+    const double sqrtmu = std::sqrt(s.mu0[0]);
+    const double sinv = 1.0 / (sqrtmu * s.MWqinv[0]);
+    const double sn = sqrtmu * s.MWqinv[0];
+    const double r = 1.0 + sn * sinv;
+    const double phi = 0.0 + r * r * s.wilkepair[0] * X;
+    s.mu1 = 0.0 + sqrtmu * sqrtmu * X / phi;
+    const double series = 0.0 + X * s.kappa0[0];
+    const double parallel = 0.0 + X / s.kappa0[0];
+    s.kappa1 = 0.5 * (series + 1.0 / parallel);
+  }
+  return PGB_OK;
+}
+
+int set_current(pgb_case *c) {
+  CK(cudaMemcpyToSymbolAsync(kSp, &c->sp, sizeof(Species), 0, cudaMemcpyHostToDevice, c->stream));
+  return PGB_OK;
+}
+
+// where a cell outside a block lies: step across faces one axis at a time
+// (orientation "123", a conforming lattice); false at a boundary
+bool locate(const pgb_case *c, int b, int ijk[3], int &sb) {
+  sb = b;
+  for (int a = 0; a < 3; a++) {
+    const HostBlock &B = c->blocks[sb];
+    const int n[3] = {B.nx, B.ny, B.nz};
+    if (ijk[a] < 0) {
+      const int nb = B.nbr[2 * a];
+      if (nb < 0) return false;
+      const HostBlock &N = c->blocks[nb];
+      const int m[3] = {N.nx, N.ny, N.nz};
+      ijk[a] += m[a];
+      sb = nb;
+    } else if (ijk[a] >= n[a]) {
+      const int nb = B.nbr[2 * a + 1];
+      if (nb < 0) return false;
+      ijk[a] -= n[a];
+      sb = nb;
+    }
+  }
+  const HostBlock &S = c->blocks[sb];
+  const int n[3] = {S.nx, S.ny, S.nz};
+  for (int a = 0; a < 3; a++)
+    if (ijk[a] < 0 || ijk[a] >= n[a]) return false;
+  return true;
+}
+
+// every halo cell a stage reads: the face halos two deep (layer 0 of every
+// face first, as the gradients' one-plane exchange reads only those), then
+// the edge cells one deep in both axes
+void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0) {
+  out.clear();
+  auto add = [&](int b, int i, int j, int k) {
+    int ijk[3] = {i, j, k};
+    int sb;
+    if (!locate(c, b, ijk, sb)) return;
+    const BlockDev &D = c->blocks[b].dev, &S = c->blocks[sb].dev;
+    HaloEntry h;
+    h.dcv = D.cv, h.scv = S.cv;
+    h.didx = (int)cell_index(D, i + NG, j + NG, k + NG);
+    h.sidx = (int)cell_index(S, ijk[0] + NG, ijk[1] + NG, ijk[2] + NG);
+    h.dvol = (int)D.vol, h.svol = (int)S.vol;
+    out.push_back(h);
+  };
+  for (int layer = 0; layer < NG; layer++) {
+    for (int b = 0; b < (int)c->blocks.size(); b++) {
+      const HostBlock &B = c->blocks[b];
+      const int n[3] = {B.nx, B.ny, B.nz};
+      for (int f = 0; f < 6; f++) {
+        const int a = f / 2;
+        const bool low = f % 2 == 0;
+        const int x = low ? -1 - layer : n[a] + layer;
+        const int a1 = (a + 1) % 3, a2 = (a + 2) % 3;
+        for (int q2 = 0; q2 < n[a2]; q2++)
+          for (int q1 = 0; q1 < n[a1]; q1++) {
+            int ijk[3];
+            ijk[a] = x, ijk[a1] = q1, ijk[a2] = q2;
+            add(b, ijk[0], ijk[1], ijk[2]);
+          }
+      }
+    }
+    if (layer == 0) n_l0 = (long long)out.size();
+  }
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const HostBlock &B = c->blocks[b];
+    const int n[3] = {B.nx, B.ny, B.nz};
+    for (int a = 0; a < 3; a++) {
+      const int a1 = (a + 1) % 3, a2 = (a + 2) % 3;
+      for (int s1 = 0; s1 < 2; s1++)
+        for (int s2 = 0; s2 < 2; s2++)
+          for (int q = 0; q < n[a]; q++) {
+            int ijk[3];
+            ijk[a] = q;
+            ijk[a1] = s1 ? n[a1] : -1;
+            ijk[a2] = s2 ? n[a2] : -1;
+            add(b, ijk[0], ijk[1], ijk[2]);
+          }
+    }
+  }
+}
+
+// the default tile of a block: a width that cuts i evenly in pieces of at
+// most 32, as many rows as 128 threads allow, k cut in two runs
+void default_tile(HostBlock &B) {
+  const int pi = (B.nx + 31) / 32;
+  int tw = (B.nx + pi - 1) / pi;
+  int th = std::max(1, FUSED_THREADS / tw);
+  th = std::min(th, B.ny);
+  const int pj = (B.ny + th - 1) / th;
+  th = (B.ny + pj - 1) / pj;
+  B.tw = tw, B.th = th;
+  B.kchunk = (B.nz + 1) / 2;
+}
+
+int build_tiles(pgb_case *c) {
+  std::vector<TileDev> tiles;
+  size_t smem = 0;
+  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    HostBlock &B = c->blocks[b];
+    if (B.tw <= 0) default_tile(B);
+    if (B.tw * B.th > FUSED_THREADS) return fail(PGB_ERR_ARG, "tile larger than 128 cells");
+    smem = std::max(smem, fused_smem(B.tw, B.th, visc));
+    for (int k0 = 0; k0 < B.nz; k0 += B.kchunk)
+      for (int j0 = 0; j0 < B.ny; j0 += B.th)
+        for (int i0 = 0; i0 < B.nx; i0 += B.tw) {
+          TileDev t;
+          t.blk = b;
+          t.i0 = (short)i0, t.j0 = (short)j0;
+          t.tw = (short)std::min(B.tw, B.nx - i0);
+          t.th = (short)std::min(B.th, B.ny - j0);
+          t.k0 = (short)k0, t.k1 = (short)std::min(B.nz, k0 + B.kchunk);
+          tiles.push_back(t);
+        }
+  }
+  // largest first, so the queue's tail is the small tiles
+  std::stable_sort(tiles.begin(), tiles.end(), [](const TileDev &x, const TileDev &y) {
+    return (long)x.tw * x.th * (x.k1 - x.k0) > (long)y.tw * y.th * (y.k1 - y.k0);
+  });
+  if (smem > 227 * 1024) return fail(PGB_ERR_ARG, "tile needs more shared memory than a CTA has");
+  if (c->d_tiles) cudaFree(c->d_tiles);
+  c->d_tiles = nullptr;
+  CK(cudaMalloc(&c->d_tiles, sizeof(TileDev) * std::max<size_t>(1, tiles.size())));
+  CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(TileDev) * tiles.size(), cudaMemcpyHostToDevice));
+  c->ntiles = (int)tiles.size();
+  c->fused_smem = smem;
+  c->tiles_dirty = false;
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
+  return PGB_OK;
+}
+
+// Each block's uniform form when its metrics allow it: every area vector along
+// its axis alone and equal, the inverse Jacobian diagonal and equal, the cell
+// centres evenly spaced; the representative values are the block's own.
+int detect_uniform(pgb_case *c, bool allow) {
+  const int nb = (int)c->blocks.size();
+  std::vector<double> h;
+  for (int b = 0; b < nb; b++) {
+    HostBlock &HB = c->blocks[b];
+    BlockDev &D = HB.dev;
+    D.uniform = 0;
+    if (!allow) continue;
+    bool ok = true;
+    for (int m = 0; m < PGB_NMETRICS; m++) ok = ok && HB.metrics_set[m];
+    if (!ok) continue;
+    h.resize((size_t)M_NCOMP * D.vol);
+    CK(cudaMemcpy(h.data(), c->d_met + (long long)M_NCOMP * D.cv, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+    auto at = [&](int comp, int i, int j, int k) { return h[(size_t)comp * D.vol + cell_index(D, i + NG, j + NG, k + NG)]; };
+    const int n[3] = {D.nx, D.ny, D.nz};
+    auto close = [](double x, double ref, double tol) { return std::fabs(x - ref) <= tol * std::fabs(ref); };
+    double S[3], Jd[3], ex[3], xL[3], xR[3];
+    const double dJ = at(M_DETJINV, 0, 0, 0);
+    for (int a = 0; a < 3; a++) {
+      S[a] = at(M_S + 3 * a + a, 0, 0, 0);
+      Jd[a] = at(M_JINV + 4 * a, 0, 0, 0);
+      int o[3] = {0, 0, 0};
+      o[a] = -1;
+      ex[a] = at(M_XCC + a, 0, 0, 0) - at(M_XCC + a, o[0], o[1], o[2]);
+      xL[a] = at(M_XF + 3 * a + a, 0, 0, 0) - at(M_XCC + a, o[0], o[1], o[2]);
+      xR[a] = at(M_XF + 3 * a + a, 0, 0, 0) - at(M_XCC + a, 0, 0, 0);
+    }
+    // every interior cell and its faces; the inverse Jacobian on the first halo layer too
+    for (int k = -1; k <= n[2] && ok; k++)
+      for (int j = -1; j <= n[1] && ok; j++)
+        for (int i = -1; i <= n[0] && ok; i++) {
+          const int out = (i < 0 || i >= n[0]) + (j < 0 || j >= n[1]) + (k < 0 || k >= n[2]);
+          if (out > 1) continue;
+          for (int a = 0; a < 3 && ok; a++)
+            for (int e = 0; e < 3; e++) {
+              const double J = at(M_JINV + 3 * a + e, i, j, k);
+              ok = ok && (a == e ? close(J, Jd[a], 1e-12) : J == 0.0);
+            }
+          if (out) continue;
+          ok = ok && close(at(M_DETJINV, i, j, k), dJ, 1e-12);
+          for (int a = 0; a < 3 && ok; a++) {
+            int o[3] = {0, 0, 0};
+            o[a] = -1;
+            for (int e = 0; e < 3; e++) {
+              const double s = at(M_S + 3 * a + e, i, j, k);
+              ok = ok && (a == e ? close(s, S[a], 1e-12) : s == 0.0);
+              const double d = at(M_XCC + e, i, j, k) - at(M_XCC + e, i + o[0], j + o[1], k + o[2]);
+              ok = ok && (a == e ? close(d, ex[a], 1e-9) : std::fabs(d) <= 1e-12 * std::fabs(ex[a]));
+            }
+          }
+        }
+    if (!ok) continue;
+    D.uniform = 1;
+    D.detJinv = dJ;
+    for (int a = 0; a < 3; a++) {
+      D.S[a] = S[a], D.Jd[a] = Jd[a], D.ex[a] = ex[a], D.xL[a] = xL[a], D.xR[a] = xR[a];
+      // alpha-damping.mako:13-25 on an area vector along axis a
+      const double Sabs = std::sqrt(S[a] * S[a]), Sinv = 1.0 / Sabs;
+      const double nrm = S[a] * Sinv;
+      const double en = ex[a] * nrm;
+      const double dampinv = c->phys.alpha / std::sqrt(en * en);
+      D.damp[a] = dampinv * nrm;
+    }
+  }
+  std::vector<BlockDev> devs;
+  for (auto &B : c->blocks) devs.push_back(B.dev);
+  CK(cudaMemcpy(c->d_blks, devs.data(), sizeof(BlockDev) * devs.size(), cudaMemcpyHostToDevice));
+  c->uniform_done = true;
+  return PGB_OK;
+}
+
+// The fused path's physical registers: a stage may not write the register its
+// stencil reads, so such a write goes to a free buffer and the mapping moves;
+// a pure write goes back to the register's own buffer when that is free.
+// Stepping from the identity mapping, the mappings fall into a cycle; the
+// case starts on the cycle (its buffers are still empty then) and the plan is
+// the cycle's steps, `period` of them.  A store is dropped when the register's
+// next access, going round the stages, is a pure write.
+int plan_step(pgb_case *c, std::vector<int> &map, std::vector<FusedStagePlan> &plan) {
+  const int nr = c->phys.nregs;
+  const int ns = (int)c->stages.size();
+  const int dq = c->stages[0].dq;
+  auto reads_of = [&](const pgb_combine &cb, int r) {
+    if (cb.own && cb.out == r) return true;
+    for (int n = 0; n < cb.nterms; n++)
+      if (cb.reg[n] == r) return true;
+    return false;
+  };
+  auto live = [&](int s, int r) {
+    for (int q = 1; q <= ns; q++) {
+      const pgb_stage &st = c->stages[(s + q) % ns];
+      if (st.q == r) return true;
+      for (int mm = 0; mm < st.ncombine; mm++) {
+        if (reads_of(st.combine[mm], r)) return true;
+        if (st.combine[mm].out == r) return false;
+      }
+    }
+    return true;
+  };
+  plan.clear();
+  for (int s = 0; s < ns; s++) {
+    const pgb_stage &st = c->stages[s];
+    FusedStagePlan p{};
+    p.qin = map[st.q];
+    p.ncomb = st.ncombine;
+    int written0 = -1;
+    for (int m = 0; m < st.ncombine; m++) {
+      const pgb_combine &cb = st.combine[m];
+      FusedCombine &f = p.comb[m];
+      f.step = cb.step;
+      f.nterms = 0;
+      if (cb.own) f.src[f.nterms] = cb.out == written0 ? -2 : map[cb.out], f.w[f.nterms++] = cb.wout;
+      for (int n = 0; n < cb.nterms; n++) {
+        const int r = cb.reg[n];
+        f.src[f.nterms] = (r == -1 || r == dq) ? -1 : (r == written0 ? -2 : map[r]);
+        f.w[f.nterms++] = cb.w[n];
+      }
+      auto in_use = [&](int buf) {
+        for (int r = 0; r < nr; r++)
+          if (r != cb.out && r != dq && map[r] == buf) return true;
+        return buf == p.qin;
+      };
+      int dst;
+      if (!cb.own && !in_use(c->canonical[cb.out])) {
+        dst = c->canonical[cb.out];
+      } else if (map[cb.out] != p.qin) {
+        dst = map[cb.out];
+      } else {
+        dst = -1;
+        for (int buf = 0; buf < nr; buf++)
+          if (!in_use(buf) && buf != map[cb.out]) {
+            dst = buf;
+            break;
+          }
+        if (dst < 0) return fail(PGB_ERR_STATE, "no free register for a stage's output");
+      }
+      f.out = dst;
+      f.write = live(s, cb.out) ? 1 : 0;
+      map[cb.out] = dst;
+      if (m == 0) written0 = cb.out;
+    }
+    // dQ's logical register names the one buffer no other register holds
+    for (int buf = 0; buf < nr; buf++) {
+      bool used = false;
+      for (int r = 0; r < nr; r++)
+        if (r != dq && map[r] == buf) used = true;
+      if (!used) map[dq] = buf;
+    }
+    plan.push_back(p);
+  }
+  return PGB_OK;
+}
+
+int build_plans(pgb_case *c) {
+  const int nr = c->phys.nregs;
+  if (c->stages.empty()) return fail(PGB_ERR_STATE, "no stages set");
+  c->canonical.resize(nr);
+  for (int r = 0; r < nr; r++) c->canonical[r] = r;
+  std::vector<std::vector<int>> states{c->canonical};
+  std::vector<std::vector<FusedStagePlan>> plans;
+  for (int t = 0; t < 8; t++) {
+    std::vector<int> map = states.back();
+    std::vector<FusedStagePlan> plan;
+    RET(plan_step(c, map, plan));
+    plans.push_back(plan);
+    for (int s = 0; s <= t; s++) {
+      if (states[s] != map) continue;
+      // steps s .. t repeat
+      c->period = t + 1 - s;
+      c->plans.assign(plans.begin() + s, plans.end());
+      c->maps.assign(states.begin() + s, states.end());
+      c->phase = 0;
+      c->phys_of = c->maps[0];
+      return PGB_OK;
+    }
+    states.push_back(map);
+  }
+  return fail(PGB_ERR_STATE, "the register plan does not repeat within eight steps");
+}
+
+int grid_for(long long n, int threads) { return (int)std::max<long long>(1, (n + threads - 1) / threads); }
+
+// one stage of the fused path
+int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &count) {
+  FusedArgs a{};
+  a.blks = c->d_blks;
+  a.tiles = c->d_tiles;
+  a.ntiles = c->ntiles;
+  a.counter = c->d_counter + stage_index;
+  a.met = c->d_met;
+  for (int r = 0; r < c->phys.nregs; r++) a.R[r] = c->d_reg[r];
+  a.qin = p.qin;
+  a.ncomb = p.ncomb;
+  a.comb[0] = p.comb[0];
+  a.comb[1] = p.comb[1];
+  a.dt = c->d_dt;
+  // the stencil register's halo first
+  k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne);
+  count++;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  bool any_general = false;
+  for (auto &B : c->blocks) any_general = any_general || !B.dev.uniform;
+  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  const int grid = std::min(c->ntiles, sms * 2);
+  const size_t sm = c->fused_smem;
+  if (visc) {
+    if (any_general) k_fused1<true, false><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
+    else k_fused1<true, true><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
+  } else {
+    if (any_general) k_fused1<false, false><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
+    else k_fused1<false, true><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
+  }
+  count++;
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int fused_attrs(pgb_case *c) {
+  const int sm = (int)c->fused_smem;
+  CK(cudaFuncSetAttribute(k_fused1<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_fused1<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_fused1<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_fused1<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  return PGB_OK;
+}
+
+// one step of the fused path at the current phase
+int step_fused(pgb_case *c, int &count) {
+  const auto &plan = c->plans[c->phase];
+  CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int) * plan.size(), c->stream));
+  for (int s = 0; s < (int)plan.size(); s++) RET(launch_fused(c, plan[s], s, count));
+  c->phase = (c->phase + 1) % c->period;
+  c->phys_of = c->maps[c->phase];
+  return PGB_OK;
+}
+
+int ensure_scratch(pgb_case *c) {
+  if (c->d_state) return PGB_OK;
+  const int ns = c->phys.ns, ne = c->ne, ngrad = ne - 1;
+  const size_t n = (size_t)c->cells;
+  CK(cudaMalloc(&c->d_state, sizeof(double) * 8 * n));
+  CK(cudaMalloc(&c->d_tr, sizeof(double) * (2 + ns) * n));
+  CK(cudaMalloc(&c->d_hsp, sizeof(double) * ns * n));
+  CK(cudaMalloc(&c->d_grads, sizeof(double) * 3 * ngrad * n));
+  for (int a = 0; a < 3; a++) CK(cudaMalloc(&c->d_F[a], sizeof(double) * ne * n));
+  CK(cudaMemsetAsync(c->d_state, 0, sizeof(double) * 8 * n, c->stream));
+  CK(cudaMemsetAsync(c->d_tr, 0, sizeof(double) * (2 + ns) * n, c->stream));
+  CK(cudaMemsetAsync(c->d_hsp, 0, sizeof(double) * ns * n, c->stream));
+  CK(cudaMemsetAsync(c->d_grads, 0, sizeof(double) * 3 * ngrad * n, c->stream));
+  for (int a = 0; a < 3; a++) CK(cudaMemsetAsync(c->d_F[a], 0, sizeof(double) * ne * n, c->stream));
+  return PGB_OK;
+}
+
+template <int NS>
+int rhs_plain_ns(pgb_case *c, int qphys, int dqphys, int &count) {
+  const int TH = 256;
+  cudaStream_t s = c->stream;
+  double *Q = c->d_reg[qphys], *dQ = c->d_reg[dqphys];
+  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  constexpr int NE = 4 + NS;
+  k_halo<<<grid_for(c->nhalo, TH), TH, 0, s>>>(Q, c->d_halo, c->nhalo, NE);
+  count++;
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const BlockDev &D = c->blocks[b].dev;
+    const long long inner = (long long)D.nx * D.ny * D.nz;
+    k_fromQ<NS><<<grid_for(D.vol, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state);
+    count++;
+    if (visc) {
+      k_transport<NS><<<grid_for(D.vol, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp);
+      k_grads<NS><<<grid_for(inner, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_grads);
+      count += 2;
+    }
+  }
+  if (visc) {
+    k_halo<<<grid_for(c->nhalo_l0, TH), TH, 0, s>>>(c->d_grads, c->d_halo, c->nhalo_l0, 3 * (NE - 1));
+    count++;
+  }
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const BlockDev &D = c->blocks[b].dev;
+    const long long inner = (long long)D.nx * D.ny * D.nz;
+    const long long fx = (long long)(D.nx + 1) * D.ny * D.nz, fy = (long long)D.nx * (D.ny + 1) * D.nz,
+                    fz = (long long)D.nx * D.ny * (D.nz + 1);
+    k_advflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[0]);
+    k_advflux<NS, 1><<<grid_for(fy, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[1]);
+    k_advflux<NS, 2><<<grid_for(fz, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[2]);
+    count += 3;
+    if (visc) {
+      k_diffflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[0]);
+      k_diffflux<NS, 1><<<grid_for(fy, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[1]);
+      k_diffflux<NS, 2><<<grid_for(fz, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[2]);
+      count += 3;
+    }
+    k_applyflux<NS><<<grid_for(inner, TH), TH, 0, s>>>(c->d_blks, b, c->d_F[0], c->d_F[1], c->d_F[2], c->d_met, dQ);
+    count++;
+  }
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
+  RET(ensure_scratch(c));
+  switch (c->phys.ns) {
+    case 1: return rhs_plain_ns<1>(c, qphys, dqphys, count);
+    case 2: return rhs_plain_ns<2>(c, qphys, dqphys, count);
+    case 3: return rhs_plain_ns<3>(c, qphys, dqphys, count);
+    default: return fail(PGB_ERR_UNSUPPORTED, "the per-block path takes 1 to 3 species in this build");
+  }
+}
+
+int step_plain(pgb_case *c, int &count) {
+  const int TH = 256;
+  const auto &map = c->phys_of;
+  for (const pgb_stage &st : c->stages) {
+    RET(rhs_plain(c, map[st.q], map[st.dq], count));
+    for (int m = 0; m < st.ncombine; m++) {
+      const pgb_combine &cb = st.combine[m];
+      CombineDev cd{};
+      cd.out = c->d_reg[map[cb.out]];
+      cd.own = cb.own;
+      cd.wout = cb.wout;
+      cd.nterms = cb.nterms;
+      cd.step = cb.step;
+      for (int n = 0; n < cb.nterms; n++) {
+        const int r = cb.reg[n] < 0 ? st.dq : cb.reg[n];
+        cd.X[n] = c->d_reg[map[r]];
+        cd.w[n] = cb.w[n];
+      }
+      for (int b = 0; b < (int)c->blocks.size(); b++) {
+        const BlockDev &D = c->blocks[b].dev;
+        k_combine<<<grid_for((long long)D.nx * D.ny * D.nz, TH), TH, 0, c->stream>>>(c->d_blks, b, c->ne, cd, c->d_dt);
+        count++;
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int prepare(pgb_case *c, bool fused) {
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  RET(set_current(c));
+  if (!c->uniform_done) RET(detect_uniform(c, fused));
+  if (fused) {
+    if (c->tiles_dirty) RET(build_tiles(c));
+    RET(fused_attrs(c));
+  }
+  return PGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pgb_last_error(void) { return g_err.c_str(); }
+int pgb_version(void) { return 1; }
+
+int pgb_device_init(int ordinal) {
+  int n = 0;
+  CK(cudaGetDeviceCount(&n));
+  if (ordinal < 0 || ordinal >= n) return fail(PGB_ERR_ARG, "no such device");
+  CK(cudaSetDevice(ordinal));
+  CK(cudaFree(nullptr));
+  return PGB_OK;
+}
+
+int pgb_device_count(int *count) {
+  if (!count) return fail(PGB_ERR_ARG, "null count");
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    *count = 0;
+    cudaGetLastError();
+  }
+  return PGB_OK;
+}
+
+int pgb_device_sync(void) {
+  CK(cudaDeviceSynchronize());
+  return PGB_OK;
+}
+
+int pgb_mem_info(size_t *free_bytes, size_t *total_bytes) {
+  CK(cudaMemGetInfo(free_bytes, total_bytes));
+  return PGB_OK;
+}
+
+int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
+  if (!phys || !out) return fail(PGB_ERR_ARG, "null argument");
+  if (phys->ns < 1 || phys->ns > MAXNS) return fail(PGB_ERR_ARG, "ns out of range");
+  if (phys->nregs < 2 || phys->nregs > MAXREGS) return fail(PGB_ERR_ARG, "nregs out of range");
+  if (phys->eos != PGB_EOS_CPG) return fail(PGB_ERR_UNSUPPORTED, "this build has the calorically perfect gas only");
+  if (phys->primary != PGB_FLUX_KEPAEC || phys->recon != PGB_RECON_CONSTANT)
+    return fail(PGB_ERR_UNSUPPORTED, "this build has kepaec on the constant reconstruction only");
+  if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT)
+    return fail(PGB_ERR_UNSUPPORTED, "this build has constant transport only");
+  auto c = std::make_unique<pgb_case>();
+  c->phys = *phys;
+  c->ne = 4 + phys->ns;
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  *out = c.release();
+  return PGB_OK;
+}
+
+int pgb_case_destroy(pgb_case *c) {
+  if (!c) return PGB_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto &r : c->d_reg)
+    if (r) cudaFree(r);
+  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
+                  c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PGB_OK;
+}
+
+int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long n) {
+  if (!c || !name || (!values && n)) return fail(PGB_ERR_ARG, "null argument");
+  if (n < 0) return fail(PGB_ERR_ARG, "negative size");
+  c->tables[name] = std::vector<double>(values, values + n);
+  return PGB_OK;
+}
+
+int pgb_case_add_block(pgb_case *c, int ni, int nj, int nk, int *blk) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (ni < 2 || nj < 2 || nk < 2) return fail(PGB_ERR_ARG, "a block has at least two cells per axis");
+  if (ni > 30000 || nj > 30000 || nk > 30000) return fail(PGB_ERR_ARG, "block too large");
+  HostBlock B;
+  B.nx = ni, B.ny = nj, B.nz = nk;
+  c->blocks.push_back(B);
+  if (blk) *blk = (int)c->blocks.size() - 1;
+  return PGB_OK;
+}
+
+int pgb_case_connect(pgb_case *c, int blk, int nface, int nbr, int nbrface) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size() || nface < 1 || nface > 6)
+    return fail(PGB_ERR_ARG, "no such block face");
+  if (nbr >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such neighbour");
+  if (nbr >= 0) {
+    const int a = (nface - 1) / 2;
+    if (nbrface != (nface % 2 ? nface + 1 : nface - 1))
+      return fail(PGB_ERR_UNSUPPORTED, "only the orientation 123 (low face to high face) is built");
+    const HostBlock &B = c->blocks[blk], &N = c->blocks[nbr];
+    const int n[3] = {B.nx, B.ny, B.nz}, m[3] = {N.nx, N.ny, N.nz};
+    for (int d = 0; d < 3; d++)
+      if (d != a && n[d] != m[d]) return fail(PGB_ERR_ARG, "the two faces do not match cell for cell");
+  }
+  c->blocks[blk].nbr[nface - 1] = nbr;
+  c->blocks[blk].nbrface[nface - 1] = nbrface;
+  return PGB_OK;
+}
+
+int pgb_case_set_stages(pgb_case *c, const pgb_stage *stages, int nstages) {
+  if (!c || !stages || nstages < 1 || nstages > 8) return fail(PGB_ERR_ARG, "bad stages");
+  for (int s = 0; s < nstages; s++) {
+    const pgb_stage &st = stages[s];
+    auto okreg = [&](int r) { return r >= -1 && r < c->phys.nregs; };
+    if (!okreg(st.q) || st.q < 0 || !okreg(st.dq) || st.dq < 0 || st.ncombine < 1 || st.ncombine > 2)
+      return fail(PGB_ERR_ARG, "bad stage");
+    for (int m = 0; m < st.ncombine; m++) {
+      const pgb_combine &cb = st.combine[m];
+      if (cb.out < 0 || cb.out >= c->phys.nregs || cb.nterms < 1 || cb.nterms > 3) return fail(PGB_ERR_ARG, "bad combine");
+      for (int n = 0; n < cb.nterms; n++)
+        if (!okreg(cb.reg[n])) return fail(PGB_ERR_ARG, "bad combine register");
+    }
+  }
+  if (c->finalized) return fail(PGB_ERR_STATE, "stages are set before finalize");
+  c->stages.assign(stages, stages + nstages);
+  return PGB_OK;
+}
+
+int pgb_case_finalize(pgb_case *c) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->finalized) return PGB_OK;
+  if (c->blocks.empty()) return fail(PGB_ERR_STATE, "no blocks");
+  if (c->stages.empty()) return fail(PGB_ERR_STATE, "no stages");
+  RET(build_species(c));
+  long long cv = 0;
+  for (auto &B : c->blocks) {
+    BlockDev &D = B.dev;
+    D = BlockDev{};
+    D.nx = B.nx, D.ny = B.ny, D.nz = B.nz;
+    D.X = B.nx + 2 * NG, D.Y = B.ny + 2 * NG, D.Z = B.nz + 2 * NG;
+    D.vol = (long long)D.X * D.Y * D.Z;
+    D.cv = cv;
+    cv += D.vol;
+  }
+  c->cells = cv;
+  const size_t n = (size_t)cv;
+  for (int r = 0; r < c->phys.nregs; r++) {
+    CK(cudaMalloc(&c->d_reg[r], sizeof(double) * c->ne * n));
+    CK(cudaMemsetAsync(c->d_reg[r], 0, sizeof(double) * c->ne * n, c->stream));
+  }
+  CK(cudaMalloc(&c->d_met, sizeof(double) * M_NCOMP * n));
+  CK(cudaMemsetAsync(c->d_met, 0, sizeof(double) * M_NCOMP * n, c->stream));
+  CK(cudaMalloc(&c->d_dt, sizeof(double)));
+  CK(cudaMalloc(&c->d_counter, sizeof(unsigned int) * 16));
+  CK(cudaMalloc(&c->d_blks, sizeof(BlockDev) * c->blocks.size()));
+  std::vector<BlockDev> devs;
+  for (auto &B : c->blocks) devs.push_back(B.dev);
+  CK(cudaMemcpy(c->d_blks, devs.data(), sizeof(BlockDev) * devs.size(), cudaMemcpyHostToDevice));
+  std::vector<HaloEntry> halo;
+  build_halo(c, halo, c->nhalo_l0);
+  c->nhalo = (long long)halo.size();
+  CK(cudaMalloc(&c->d_halo, sizeof(HaloEntry) * std::max<size_t>(1, halo.size())));
+  CK(cudaMemcpy(c->d_halo, halo.data(), sizeof(HaloEntry) * halo.size(), cudaMemcpyHostToDevice));
+  CK(cudaStreamSynchronize(c->stream));
+  c->finalized = true;
+  RET(build_plans(c));
+  return PGB_OK;
+}
+
+int pgb_case_halo(const pgb_case *c, int *ng) {
+  if (!c || !ng) return fail(PGB_ERR_ARG, "null argument");
+  *ng = NG;
+  return PGB_OK;
+}
+
+int pgb_case_device_bytes(const pgb_case *c, size_t *bytes) {
+  if (!c || !bytes) return fail(PGB_ERR_ARG, "null argument");
+  const size_t n = (size_t)c->cells;
+  size_t b = sizeof(double) * n * ((size_t)c->ne * c->phys.nregs + M_NCOMP);
+  if (c->d_state) b += sizeof(double) * n * (8 + 2 + 2 * c->phys.ns + 3 * (c->ne - 1) + 3 * c->ne);
+  *bytes = b + sizeof(HaloEntry) * (size_t)c->nhalo;
+  return PGB_OK;
+}
+
+int pgb_metric_set(pgb_case *c, int blk, int which, const double *host, long count) {
+  if (!c || !host) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "finalize the case before setting metrics");
+  if (blk < 0 || blk >= (int)c->blocks.size() || which < 0 || which >= PGB_NMETRICS)
+    return fail(PGB_ERR_ARG, "no such block or metric");
+  HostBlock &B = c->blocks[blk];
+  const BlockDev &D = B.dev;
+  static const int comps[PGB_NMETRICS] = {3, 1, 9, 3, 3, 3, 3, 3, 3};
+  static const int first[PGB_NMETRICS] = {M_XCC, M_DETJINV, M_JINV, M_S, M_S + 3, M_S + 6, M_XF, M_XF + 3, M_XF + 6};
+  const int face = which >= PGB_ARR_IS ? (which - PGB_ARR_IS) % 3 : -1;
+  const int X = D.X + (face == 0), Y = D.Y + (face == 1), Z = D.Z + (face == 2);
+  const int nc = comps[which];
+  if (count != (long)X * Y * Z * nc) return fail(PGB_ERR_ARG, "metric array of the wrong size");
+  // host F order [comp][k][j][i] over the array's own extents; the face
+  // array's last plane (past the last halo cell) is never read and is dropped
+  std::vector<double> dev((size_t)nc * D.vol);
+  for (int q = 0; q < nc; q++)
+    for (int k = 0; k < D.Z; k++)
+      for (int j = 0; j < D.Y; j++)
+        for (int i = 0; i < D.X; i++)
+          dev[(size_t)q * D.vol + cell_index(D, i, j, k)] = host[(((size_t)q * Z + k) * Y + j) * X + i];
+  CK(cudaMemcpy(c->d_met + (size_t)M_NCOMP * D.cv + (size_t)first[which] * D.vol, dev.data(),
+                sizeof(double) * dev.size(), cudaMemcpyHostToDevice));
+  B.metrics_set[which] = true;
+  c->uniform_done = false;
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
+  return PGB_OK;
+}
+
+static int check_reg(pgb_case *c, int blk, int reg, long count, int comps) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
+  if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  const BlockDev &D = c->blocks[blk].dev;
+  if (count != (long)D.nx * D.ny * D.nz * comps) return fail(PGB_ERR_ARG, "host array of the wrong size");
+  return PGB_OK;
+}
+
+static int stage_host(pgb_case *c, long long n) {
+  if (n > c->prims_cap) {
+    if (c->d_prims) cudaFree(c->d_prims);
+    c->d_prims = nullptr;
+    CK(cudaMalloc(&c->d_prims, sizeof(double) * n));
+    c->prims_cap = n;
+  }
+  return PGB_OK;
+}
+
+int pgb_array_set(pgb_case *c, int blk, int reg, const double *host, long count) {
+  RET(check_reg(c, blk, reg, count, c->ne));
+  if (!host) return fail(PGB_ERR_ARG, "null host array");
+  RET(stage_host(c, count));
+  CK(cudaMemcpyAsync(c->d_prims, host, sizeof(double) * count, cudaMemcpyHostToDevice, c->stream));
+  const BlockDev &D = c->blocks[blk].dev;
+  k_unpack<<<grid_for((long long)D.nx * D.ny * D.nz, 256), 256, 0, c->stream>>>(c->d_blks, blk, c->ne, c->d_prims,
+                                                                                   c->d_reg[c->phys_of[reg]]);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_array_get(pgb_case *c, int blk, int reg, double *host, long count) {
+  RET(check_reg(c, blk, reg, count, c->ne));
+  if (!host) return fail(PGB_ERR_ARG, "null host array");
+  RET(stage_host(c, count));
+  const BlockDev &D = c->blocks[blk].dev;
+  k_pack<<<grid_for((long long)D.nx * D.ny * D.nz, 256), 256, 0, c->stream>>>(c->d_blks, blk, c->ne,
+                                                                                 c->d_reg[c->phys_of[reg]], c->d_prims);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, c->d_prims, sizeof(double) * count, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count) {
+  RET(check_reg(c, blk, reg, count, c->ne));
+  if (!host) return fail(PGB_ERR_ARG, "null host array");
+  RET(set_current(c));
+  RET(stage_host(c, count));
+  CK(cudaMemcpyAsync(c->d_prims, host, sizeof(double) * count, cudaMemcpyHostToDevice, c->stream));
+  const BlockDev &D = c->blocks[blk].dev;
+  const int g = grid_for((long long)D.nx * D.ny * D.nz, 256);
+  double *Q = c->d_reg[c->phys_of[reg]];
+  switch (c->phys.ns) {
+    case 1: k_fromprims<1><<<g, 256, 0, c->stream>>>(c->d_blks, blk, c->d_prims, Q); break;
+    case 2: k_fromprims<2><<<g, 256, 0, c->stream>>>(c->d_blks, blk, c->d_prims, Q); break;
+    case 3: k_fromprims<3><<<g, 256, 0, c->stream>>>(c->d_blks, blk, c->d_prims, Q); break;
+    default: return fail(PGB_ERR_UNSUPPORTED, "set_prims takes 1 to 3 species in this build");
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_rhs(pgb_case *c, int q, int dq) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  RET(prepare(c, false));
+  if (q < 0 || q >= c->phys.nregs || dq < 0 || dq >= c->phys.nregs || q == dq)
+    return fail(PGB_ERR_ARG, "bad registers");
+  int count = 0;
+  RET(rhs_plain(c, c->phys_of[q], c->phys_of[dq], count));
+  return PGB_OK;
+}
+
+int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (nsteps < 0) return fail(PGB_ERR_ARG, "negative step count");
+  if (path != PGB_PATH_BATCHED && path != PGB_PATH_PER_BLOCK) return fail(PGB_ERR_ARG, "no such path");
+  const bool fused = path == PGB_PATH_BATCHED;
+  if (fused && !fused_capable(c))
+    return fail(PGB_ERR_UNSUPPORTED, "the batched path takes the single-species cpg kepaec case; use the per-block path");
+  RET(prepare(c, fused));
+  if (!fused) RET(ensure_scratch(c));
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int done = 0;
+  while (done < nsteps) {
+    const int unit = fused ? c->period : 1;
+    if (graph && c->phase == 0 && nsteps - done >= unit) {
+      cudaGraphExec_t &ge = c->graph[path];
+      if (ge && c->graph_map[path] != c->phys_of) {
+        cudaGraphExecDestroy(ge);
+        ge = nullptr;
+      }
+      if (!ge) {
+        c->graph_map[path] = c->phys_of;
+        cudaGraph_t g;
+        int count = 0;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = PGB_OK;
+        for (int u = 0; u < unit && rc == PGB_OK; u++) rc = fused ? step_fused(c, count) : step_plain(c, count);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (rc != PGB_OK) return rc;
+        if (e != cudaSuccess) return fail(PGB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        CK(cudaGraphInstantiate(&ge, g, 0));
+        cudaGraphDestroy(g);
+        c->launches[path] = count / unit;
+        // the capture advanced the phase as the launches will
+        c->phase = 0;
+        c->phys_of = c->maps.empty() ? c->phys_of : c->maps[0];
+      }
+      CK(cudaGraphLaunch(ge, c->stream));
+      if (fused) {
+        c->phase = 0;
+        c->phys_of = c->maps[0];
+      }
+      done += unit;
+      continue;
+    }
+    int count = 0;
+    RET(fused ? step_fused(c, count) : step_plain(c, count));
+    c->launches[path] = count;
+    done += 1;
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  return PGB_OK;
+}
+
+int pgb_case_stream(const pgb_case *c, void **stream) {
+  if (!c || !stream) return fail(PGB_ERR_ARG, "null argument");
+  *stream = (void *)c->stream;
+  return PGB_OK;
+}
+
+int pgb_last_step_ms(const pgb_case *c, float *ms) {
+  if (!c || !ms) return fail(PGB_ERR_ARG, "null argument");
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return PGB_OK;
+}
+
+int pgb_launches_per_step(const pgb_case *c, int path, int *count) {
+  if (!c || !count || path < 0 || path > 1) return fail(PGB_ERR_ARG, "bad argument");
+  *count = c->launches[path];
+  return PGB_OK;
+}
+
+int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk) {
+  if (!c || blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
+  if (tw < 1 || th < 1 || tw * th > FUSED_THREADS || kchunk < 1) return fail(PGB_ERR_ARG, "bad tile");
+  HostBlock &B = c->blocks[blk];
+  B.tw = std::min(tw, B.nx), B.th = std::min(th, B.ny), B.kchunk = std::min(kchunk, B.nz);
+  c->tiles_dirty = true;
+  return PGB_OK;
+}
+
+int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk) {
+  if (!c || blk < 0 || blk >= (int)c->blocks.size() || !tw || !th || !kchunk) return fail(PGB_ERR_ARG, "bad argument");
+  HostBlock B = c->blocks[blk];
+  if (B.tw <= 0) default_tile(B);
+  *tw = B.tw, *th = B.th, *kchunk = B.kchunk;
+  return PGB_OK;
+}
+
+int pgb_block_uniform(const pgb_case *c, int blk, int *uniform) {
+  if (!c || blk < 0 || blk >= (int)c->blocks.size() || !uniform) return fail(PGB_ERR_ARG, "bad argument");
+  *uniform = c->blocks[blk].dev.uniform;
+  return PGB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,251 @@
+// Cell and face physics of the calorically perfect gas, device side.
+//
+// Each function is the reference template's arithmetic (cited per function),
+// on values in registers; the callers decide where the values come from
+// (global arrays on the per-block path, shared-memory planes on the fused
+// path).  nvcc contracts multiply-adds as the reference's NVRTC build does
+// (peregrine/backend/cuda/compiler.py:17).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace pgb {
+
+constexpr int MAXNS = 12;
+
+// the case's species tables, in constant memory; filled per case before its
+// launches (a case's tables are copied in when the case is made current)
+struct Species {
+  int ns;
+  double Ru;
+  double Rsp[MAXNS], cp0[MAXNS], h298R[MAXNS], MWinv[MAXNS], hpoly0[MAXNS], h298[MAXNS];
+  double mu0[MAXNS], kappa0[MAXNS], MWqinv[MAXNS], lewis[MAXNS];
+  double wilkepair[MAXNS * MAXNS];
+  double alpha;
+  // single-species shortcuts, exact copies of what the per-cell formulas give
+  // for Y = 1 (set by the host from the same operations)
+  double R1, cp1, h2981, cv1, cvinv1, gamma1, th1;  // th1 = cp / gamma
+  double mu1, kappa1;
+};
+
+__constant__ Species kSp;
+
+// EosState (peregrine/simulator/mixture/eos/base.py:85-86)
+struct State {
+  double p, T, rhoinv, rho, e, cp, gamma, c;
+};
+
+// mixmom for the cpg moments (peregrine/simulator/mixture/eos/kernels/mixing.mako:3-30)
+template <int NS, class YF>
+__device__ __forceinline__ void mixmom(YF Y, double &R, double &cp, double &h298) {
+  R = 0.0, cp = 0.0, h298 = 0.0;
+  double Ylast = 1.0;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    const double Yn = Y(n);
+    Ylast -= Yn;
+    R += Yn * kSp.Rsp[n];
+    cp += Yn * kSp.cp0[n];
+    h298 += Yn * kSp.h298R[n];
+  }
+  R += Ylast * kSp.Rsp[NS - 1];
+  cp += Ylast * kSp.cp0[NS - 1];
+  h298 += Ylast * kSp.h298R[NS - 1];
+}
+
+// fromQ + cpg fromrhoE (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19,
+// peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:5-15)
+template <int NS, class QF>
+__device__ __forceinline__ State fromQ(QF Q) {
+  const double rho = Q(0), rhoinv = 1.0 / rho;
+  const double q1 = Q(1), q2 = Q(2), q3 = Q(3);
+  const double e = (Q(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv) * rhoinv;
+  double R, cp, h298;
+  mixmom<NS>([&](int n) { return Q(5 + n) * rhoinv; }, R, cp, h298);
+  State s;
+  const double cv = cp - R;
+  s.rho = rho;
+  s.rhoinv = 1.0 / rho;
+  s.e = e;
+  s.T = (e - h298) / cv;
+  s.p = rho * R * s.T;
+  s.cp = cp;
+  s.gamma = cp / cv;
+  s.c = sqrt(s.gamma * R * s.T);
+  return s;
+}
+
+// fromprims (peregrine/simulator/euler/kernels/state/fromprims.mako:4-12,
+// peregrine/simulator/euler/kernels/solution.mako:2-23, cpg frompT eos.mako:17-27)
+template <int NS>
+__device__ __forceinline__ void fromprims(const double *q, double *Q) {
+  const double p = q[0], T = q[4];
+  double R, cp, h298;
+  mixmom<NS>([&](int n) { return q[5 + n]; }, R, cp, h298);
+  const double cv = cp - R;
+  const double rho = p / (R * T);
+  const double e = cv * T + h298;
+  Q[0] = rho;
+  Q[1] = rho * q[1];
+  Q[2] = rho * q[2];
+  Q[3] = rho * q[3];
+  Q[4] = rho * (e + 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) Q[5 + n] = rho * q[5 + n];
+}
+
+// transport with constant species properties, Wilke, series/parallel
+// conductivity, Lewis diffusivities and species enthalpies
+// (peregrine/simulator/navstokes/kernels/transport.mako:5-35,
+//  peregrine/simulator/mixture/transport/kernels/constant.mako:5-16,
+//  peregrine/simulator/mixture/mixrule/kernels/wilke.mako:3-17,
+//  peregrine/simulator/mixture/transport/kernels/mixing.mako:3-10,
+//  peregrine/simulator/mixture/diffusion/kernels/lewis.mako:3-8,
+//  peregrine/simulator/mixture/eos/kernels/species.mako:9-36)
+template <int NS, class QF>
+__device__ __forceinline__ void transport_constant(QF Q, const State &st, double *tr, double *hsp) {
+  const double rho = Q(0), rhoinv = 1.0 / rho;
+  double Ylast = 1.0;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) Ylast -= Q(5 + n) * rhoinv;
+  Ylast = fmax(Ylast, 0.0);
+  auto Y = [&](int n) { return n < NS - 1 ? Q(5 + n) * rhoinv : Ylast; };
+  double denom = 0.0;
+#pragma unroll
+  for (int n = 0; n < NS; n++) denom += Y(n) * kSp.MWinv[n];
+  const double MWmix = 1.0 / denom;
+  double X[NS];
+#pragma unroll
+  for (int n = 0; n < NS; n++) X[n] = Y(n) * kSp.MWinv[n] * MWmix;
+  double sqrtmu[NS], sinv[NS];
+#pragma unroll
+  for (int n = 0; n < NS; n++) sqrtmu[n] = sqrt(kSp.mu0[n]);
+#pragma unroll
+  for (int n = 0; n < NS; n++) sinv[n] = 1.0 / (sqrtmu[n] * kSp.MWqinv[n]);
+  double mu = 0.0;
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    const double sn = sqrtmu[n] * kSp.MWqinv[n];
+    double phi = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) {
+      const double r = 1.0 + sn * sinv[m];
+      phi += r * r * kSp.wilkepair[n * MAXNS + m] * X[m];
+    }
+    mu += sqrtmu[n] * sqrtmu[n] * X[n] / phi;
+  }
+  double series = 0.0, parallel = 0.0;
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    series += X[n] * kSp.kappa0[n];
+    parallel += X[n] / kSp.kappa0[n];
+  }
+  const double kappa = 0.5 * (series + 1.0 / parallel);
+  tr[0] = mu;
+  tr[1] = kappa;
+  const double kor = kappa * rhoinv / st.cp;
+#pragma unroll
+  for (int n = 0; n < NS; n++) tr[2 + n] = kor / kSp.lewis[n];
+  const double T = st.T, u = log(T), Tinv = 1.0 / T;
+  (void)u;
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    double hRT = kSp.hpoly0[n];
+    hRT += kSp.h298[n] * Tinv;
+    hsp[n] = hRT * T * kSp.Ru * kSp.MWinv[n];
+  }
+}
+
+// A face side for kepaec: what the two-point flux reads of a cell
+// (peregrine/simulator/euler/kernels/flux/recon/constant.mako:3-18)
+struct KSide {
+  double u, v, w, p, rho, e, th;  // th = cp / gamma * T
+};
+
+// kepaec (peregrine/simulator/euler/kernels/flux/function/kepaec.mako:2-20);
+// the species rows are added by the caller
+__device__ __forceinline__ void kepaec(const KSide &L, const KSide &R, const double S0, const double S1,
+                                       const double S2, double *F, double &C) {
+  const double uf = 0.5 * (R.u + L.u), vf = 0.5 * (R.v + L.v), wf = 0.5 * (R.w + L.w);
+  const double U = S0 * uf + S1 * vf + S2 * wf;
+  const double pf = 0.5 * (R.p + L.p);
+  const double rho = 0.5 * (R.rho + L.rho);
+  C = rho * U;
+  F[0] = C;
+  F[1] = C * uf + pf * S0;
+  F[2] = C * vf + pf * S1;
+  F[3] = C * wf + pf * S2;
+  const double Kj = C * 0.5 * (R.u * L.u + R.v * L.v + R.w * L.w);
+  const double Pj = 0.5 * (L.p * (R.u * S0 + R.v * S1 + R.w * S2) + R.p * (L.u * S0 + L.v * S1 + L.w * S2));
+  const double ef = 2.0 * L.th * R.th / (L.th + R.th) + 0.5 * ((L.e - L.th) + (R.e - R.th));
+  F[4] = ef * C + Kj + Pj;
+}
+
+// What alpha damping reads of a face's geometry, formed once per face
+// (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:13-27)
+struct FaceGeom {
+  double S0, S1, S2;           // area vector
+  double dampx, dampy, dampz;  // alpha / |e.n| along the unit normal
+  double xLx, xLy, xLz, xRx, xRy, xRz;  // face centre less each cell centre
+};
+
+__device__ __forceinline__ FaceGeom face_geom(const double S0, const double S1, const double S2,
+                                              const double *xf, const double *xL, const double *xR) {
+  FaceGeom g;
+  g.S0 = S0, g.S1 = S1, g.S2 = S2;
+  const double Sabs = sqrt(S0 * S0 + S1 * S1 + S2 * S2), Sinv = 1.0 / Sabs;
+  const double nx = S0 * Sinv, ny = S1 * Sinv, nz = S2 * Sinv;
+  const double ex = xR[0] - xL[0], ey = xR[1] - xL[1], ez = xR[2] - xL[2];
+  const double en0 = ex * nx, en1 = ey * ny, en2 = ez * nz;
+  const double dampinv = kSp.alpha / sqrt(en0 * en0 + en1 * en1 + en2 * en2);
+  g.dampx = dampinv * nx, g.dampy = dampinv * ny, g.dampz = dampinv * nz;
+  g.xLx = xf[0] - xL[0], g.xLy = xf[1] - xL[1], g.xLz = xf[2] - xL[2];
+  g.xRx = xf[0] - xR[0], g.xRy = xf[1] - xR[1], g.xRz = xf[2] - xR[2];
+  return g;
+}
+
+// the face gradient of one row (alpha-damping.mako:29-38)
+__device__ __forceinline__ void facegrad(const FaceGeom &g, const double phiL, const double phiR,
+                                         const double *gL, const double *gR, double &gx, double &gy,
+                                         double &gz) {
+  const double wl = phiL + gL[0] * g.xLx + gL[1] * g.xLy + gL[2] * g.xLz;
+  const double wr = phiR + gR[0] * g.xRx + gR[1] * g.xRy + gR[2] * g.xRz;
+  const double jump = wr - wl;
+  gx = 0.5 * (gR[0] + gL[0]) + g.dampx * jump;
+  gy = 0.5 * (gR[1] + gL[1]) + g.dampy * jump;
+  gz = 0.5 * (gR[2] + gL[2]) + g.dampz * jump;
+}
+
+// The viscous rows of a single-species face (alpha-damping.mako:39-58 and
+// :92): with one species every diffusion term of :59-91 is zero, so the
+// energy row is the stress work plus the heat flux.  Gradient rows are
+// u, v, w, T, each 3 wide.
+__device__ __forceinline__ void viscous1(const FaceGeom &g, const double mu, const double kappa,
+                                         const double uL, const double vL, const double wL,
+                                         const double TL, const double uR, const double vR,
+                                         const double wR, const double TR, const double *gL,
+                                         const double *gR, double *F) {
+  const double lambda = 0.0 - 2.0 / 3.0 * mu;
+  double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
+  facegrad(g, uL, uR, gL + 0, gR + 0, dudx, dudy, dudz);
+  facegrad(g, vL, vR, gL + 3, gR + 3, dvdx, dvdy, dvdz);
+  facegrad(g, wL, wR, gL + 6, gR + 6, dwdx, dwdy, dwdz);
+  const double div = dudx + dvdy + dwdz;
+  const double txx = -2.0 * mu * dudx - lambda * div;
+  const double txy = -mu * (dvdx + dudy);
+  const double txz = -mu * (dwdx + dudz);
+  const double tyy = -2.0 * mu * dvdy - lambda * div;
+  const double tyz = -mu * (dwdy + dvdz);
+  const double tzz = -2.0 * mu * dwdz - lambda * div;
+  F[1] += txx * g.S0 + txy * g.S1 + txz * g.S2;
+  F[2] += txy * g.S0 + tyy * g.S1 + tyz * g.S2;
+  F[3] += txz * g.S0 + tyz * g.S1 + tzz * g.S2;
+  double dTx, dTy, dTz;
+  facegrad(g, TL, TR, gL + 9, gR + 9, dTx, dTy, dTz);
+  const double heatflux = -kappa * (dTx * g.S0 + dTy * g.S1 + dTz * g.S2);
+  const double uf = 0.5 * (uR + uL), vf = 0.5 * (vR + vL), wf = 0.5 * (wR + wL);
+  const double f4 = (uf * txx + vf * txy + wf * txz) * g.S0 + (uf * txy + vf * tyy + wf * tyz) * g.S1 +
+                    (uf * txz + vf * tyz + wf * tzz) * g.S2 + heatflux;
+  F[4] += f4;
+}
+
+}  // namespace pgb

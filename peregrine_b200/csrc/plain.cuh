@@ -1,0 +1,359 @@
+// The plain per-block path: the reference's kernels one by one, one launch
+// per block and kernel, each pass a round trip through HBM as in the
+// reference's rhs graph (peregrine/simulator/advec/simulator.py:57-87,
+// peregrine/simulator/advecdiff/simulator.py:110-124).  It is the baseline
+// the fused path is measured against and the path for physics the fused
+// kernel does not take.
+#pragma once
+#include "layout.cuh"
+#include "physics.cuh"
+
+namespace pgb {
+
+// the halo fill over every block at once: comps components per entry
+// (the reference's place kernel, peregrine/multiblock/collections/exchange/kernels/place.mako:11-20)
+__global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const HaloEntry h = tab[e];
+    double *d = base + comps * h.dcv + h.didx;
+    const double *s = base + comps * h.scv + h.sidx;
+    for (int c = 0; c < comps; c++) d[(long long)c * h.dvol] = s[(long long)c * h.svol];
+  }
+}
+
+__device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi, int &fj, int &fk) {
+  fi = (int)(t % B.X);
+  const long long r = t / B.X;
+  fj = (int)(r % B.Y);
+  fk = (int)(r / B.Y);
+}
+
+// fromQ over the whole block, halo included: state[8] per cell
+// (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19)
+template <int NS>
+__global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                        double *__restrict__ stall) {
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= B.vol) return;
+  const double *Q = Qall + (4 + NS) * B.cv + t;
+  const State s = fromQ<NS>([&](int c) { return Q[c * B.vol]; });
+  double *st = stall + 8 * B.cv + t;
+  const long long v = B.vol;
+  st[0 * v] = s.p, st[1 * v] = s.T, st[2 * v] = s.rhoinv, st[3 * v] = s.rho;
+  st[4 * v] = s.e, st[5 * v] = s.cp, st[6 * v] = s.gamma, st[7 * v] = s.c;
+}
+
+__device__ __forceinline__ State load_state(const double *st, long long v) {
+  State s;
+  s.p = st[0 * v], s.T = st[1 * v], s.rhoinv = st[2 * v], s.rho = st[3 * v];
+  s.e = st[4 * v], s.cp = st[5 * v], s.gamma = st[6 * v], s.c = st[7 * v];
+  return s;
+}
+
+// transport over the whole block: trstate[2 + ns] and hsp[ns] per cell
+// (peregrine/simulator/navstokes/kernels/transport.mako:5-35)
+template <int NS>
+__global__ void k_transport(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                            const double *__restrict__ stall, double *__restrict__ trall,
+                            double *__restrict__ hall) {
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= B.vol) return;
+  const double *Q = Qall + (4 + NS) * B.cv + t;
+  const State s = load_state(stall + 8 * B.cv + t, B.vol);
+  double tr[2 + NS], h[NS];
+  transport_constant<NS>([&](int c) { return Q[c * B.vol]; }, s, tr, h);
+  double *trp = trall + (2 + NS) * B.cv + t;
+  double *hp = hall + NS * B.cv + t;
+#pragma unroll
+  for (int n = 0; n < 2 + NS; n++) trp[n * B.vol] = tr[n];
+#pragma unroll
+  for (int n = 0; n < NS; n++) hp[n * B.vol] = h[n];
+}
+
+// cell gradients of u, v, w, T, Y on the interior
+// (peregrine/simulator/navstokes/kernels/dqdxyz.mako:16-41)
+template <int NS>
+__global__ void k_grads(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                        const double *__restrict__ stall, const double *__restrict__ met,
+                        double *__restrict__ gall) {
+  constexpr int NE = 4 + NS, NGRAD = NE - 1;
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)B.nx * B.ny * B.nz;
+  if (t >= n) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k);
+  const long long sI = 1, sJ = B.X, sK = (long long)B.X * B.Y;
+  const double *Q = Qall + NE * B.cv + c;
+  const double *T = stall + 8 * B.cv + 1 * B.vol + c;
+  const double *J = met + M_NCOMP * B.cv + M_JINV * B.vol + c;
+  double *g = gall + 3 * NGRAD * B.cv + c;
+  const long long v = B.vol;
+  const double rIp = Q[sI], rIm = Q[-sI], invI = 1.0 / (rIp * rIm);
+  const double rJp = Q[sJ], rJm = Q[-sJ], invJ = 1.0 / (rJp * rJm);
+  const double rKp = Q[sK], rKm = Q[-sK], invK = 1.0 / (rKp * rKm);
+  double Jm[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) Jm[q] = J[q * v];
+#pragma unroll
+  for (int l = 0; l < NGRAD; l++) {
+    double d[3];
+    if (l == 3) {
+      d[0] = 0.5 * (T[sI] - T[-sI]);
+      d[1] = 0.5 * (T[sJ] - T[-sJ]);
+      d[2] = 0.5 * (T[sK] - T[-sK]);
+    } else {
+      const double *Qm = Q + (l + 1) * v;
+      d[0] = 0.5 * (Qm[sI] * rIm - Qm[-sI] * rIp) * invI;
+      d[1] = 0.5 * (Qm[sJ] * rJm - Qm[-sJ] * rJp) * invJ;
+      d[2] = 0.5 * (Qm[sK] * rKm - Qm[-sK] * rKp) * invK;
+    }
+#pragma unroll
+    for (int e = 0; e < 3; e++) g[(3 * l + e) * v] = d[0] * Jm[0 * 3 + e] + d[1] * Jm[1 * 3 + e] + d[2] * Jm[2 * 3 + e];
+  }
+}
+
+// the interior faces of axis A: face f between cells f - 1 and f
+template <int A>
+__device__ __forceinline__ bool face_at(const BlockDev &B, long long t, int &i, int &j, int &k) {
+  const int fx = B.nx + (A == 0), fy = B.ny + (A == 1), fz = B.nz + (A == 2);
+  if (t >= (long long)fx * fy * fz) return false;
+  i = (int)(t % fx) + NG;
+  j = (int)((t / fx) % fy) + NG;
+  k = (int)(t / ((long long)fx * fy)) + NG;
+  return true;
+}
+
+// the advective face flux, kepaec on the cells as they are
+// (peregrine/simulator/euler/kernels/flux/single.mako:4-9 with
+//  recon/constant.mako:3-18 and function/kepaec.mako:2-20)
+template <int NS, int A>
+__global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                          const double *__restrict__ stall, const double *__restrict__ met,
+                          double *__restrict__ Fall) {
+  constexpr int NE = 4 + NS;
+  const BlockDev &B = blks[b];
+  int i, j, k;
+  if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
+  const long long v = B.vol;
+  const double *Q = Qall + NE * B.cv;
+  const double *st = stall + 8 * B.cv;
+  const double *S = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
+  auto side = [&](long long c) {
+    const State s = load_state(st + c, v);
+    KSide x;
+    x.u = Q[1 * v + c] / Q[c];
+    x.v = Q[2 * v + c] / Q[c];
+    x.w = Q[3 * v + c] / Q[c];
+    x.p = s.p, x.rho = s.rho, x.e = s.e;
+    x.th = s.cp / s.gamma * s.T;
+    return x;
+  };
+  const KSide sl = side(L), sr = side(R);
+  double F[NE], C;
+  kepaec(sl, sr, S[0], S[v], S[2 * v], F, C);
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) F[5 + n] = 0.5 * (Q[(5 + n) * v + R] / Q[R] + Q[(5 + n) * v + L] / Q[L]) * C;
+  double *Fo = Fall + NE * B.cv + R;
+#pragma unroll
+  for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
+}
+
+// the diffusive face flux added to F (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:3-99)
+template <int NS, int A>
+__global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                           const double *__restrict__ stall, const double *__restrict__ trall,
+                           const double *__restrict__ hall, const double *__restrict__ gall,
+                           const double *__restrict__ met, double *__restrict__ Fall) {
+  constexpr int NE = 4 + NS, NGRAD = NE - 1;
+  const BlockDev &B = blks[b];
+  int i, j, k;
+  if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
+  const long long v = B.vol;
+  const double *Q = Qall + NE * B.cv;
+  const double *st = stall + 8 * B.cv;
+  const double *tr = trall + (2 + NS) * B.cv;
+  const double *hs = hall + NS * B.cv;
+  const double *gr = gall + 3 * NGRAD * B.cv;
+  const double *M = met + M_NCOMP * B.cv;
+  const double S[3] = {M[(M_S + 3 * A) * v + R], M[(M_S + 3 * A + 1) * v + R], M[(M_S + 3 * A + 2) * v + R]};
+  const double xf[3] = {M[(M_XF + 3 * A) * v + R], M[(M_XF + 3 * A + 1) * v + R], M[(M_XF + 3 * A + 2) * v + R]};
+  const double xL[3] = {M[(M_XCC + 0) * v + L], M[(M_XCC + 1) * v + L], M[(M_XCC + 2) * v + L]};
+  const double xR[3] = {M[(M_XCC + 0) * v + R], M[(M_XCC + 1) * v + R], M[(M_XCC + 2) * v + R]};
+  const FaceGeom g = face_geom(S[0], S[1], S[2], xf, xL, xR);
+  const State sL = load_state(st + L, v), sR = load_state(st + R, v);
+  double gL[3 * NGRAD], gRr[3 * NGRAD];
+#pragma unroll
+  for (int q = 0; q < 3 * NGRAD; q++) gL[q] = gr[q * v + L], gRr[q] = gr[q * v + R];
+  const double mu = 0.5 * (tr[0 * v + R] + tr[0 * v + L]);
+  const double kappa = 0.5 * (tr[1 * v + R] + tr[1 * v + L]);
+  const double lambda = 0.0 - 2.0 / 3.0 * mu;
+  const double rhoinvL = sL.rhoinv, rhoinvR = sR.rhoinv;
+  const double uL = Q[1 * v + L] * rhoinvL, vL = Q[2 * v + L] * rhoinvL, wL = Q[3 * v + L] * rhoinvL;
+  const double uR = Q[1 * v + R] * rhoinvR, vR = Q[2 * v + R] * rhoinvR, wR = Q[3 * v + R] * rhoinvR;
+  double F[NE];
+  double *Fo = Fall + NE * B.cv + R;
+#pragma unroll
+  for (int l = 0; l < NE; l++) F[l] = Fo[l * v];
+  double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
+  facegrad(g, uL, uR, gL + 0, gRr + 0, dudx, dudy, dudz);
+  facegrad(g, vL, vR, gL + 3, gRr + 3, dvdx, dvdy, dvdz);
+  facegrad(g, wL, wR, gL + 6, gRr + 6, dwdx, dwdy, dwdz);
+  const double div = dudx + dvdy + dwdz;
+  const double txx = -2.0 * mu * dudx - lambda * div;
+  const double txy = -mu * (dvdx + dudy);
+  const double txz = -mu * (dwdx + dudz);
+  const double tyy = -2.0 * mu * dvdy - lambda * div;
+  const double tyz = -mu * (dwdy + dvdz);
+  const double tzz = -2.0 * mu * dwdz - lambda * div;
+  F[1] += txx * g.S0 + txy * g.S1 + txz * g.S2;
+  F[2] += txy * g.S0 + tyy * g.S1 + tyz * g.S2;
+  F[3] += txz * g.S0 + tyz * g.S1 + tzz * g.S2;
+  double dTx, dTy, dTz;
+  facegrad(g, sL.T, sR.T, gL + 9, gRr + 9, dTx, dTy, dTz);
+  const double heatflux = -kappa * (dTx * g.S0 + dTy * g.S1 + dTz * g.S2);
+  const double uf = 0.5 * (uR + uL), vf = 0.5 * (vR + vL), wf = 0.5 * (wR + wL);
+  double f4 = (uf * txx + vf * txy + wf * txz) * g.S0 + (uf * txy + vf * tyy + wf * tyz) * g.S1 +
+              (uf * txz + vf * tyz + wf * tzz) * g.S2 + heatflux;
+  double YlastL = 1.0, YlastR = 1.0;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    YlastL -= Q[(5 + n) * v + L] * rhoinvL;
+    YlastR -= Q[(5 + n) * v + R] * rhoinvR;
+  }
+  auto YL = [&](int n) { return n < NS - 1 ? Q[(5 + n) * v + L] * rhoinvL : YlastL; };
+  auto YR = [&](int n) { return n < NS - 1 ? Q[(5 + n) * v + R] * rhoinvR : YlastR; };
+  double Dk, Vc = 0.0, gradYns = 0.0, sumYh = 0.0, Yns = 1.0;
+  const double rho = 0.5 * (Q[R] + Q[L]);
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    Dk = 0.5 * (tr[(2 + n) * v + R] + tr[(2 + n) * v + L]);
+    double dYx, dYy, dYz;
+    facegrad(g, YL(n), YR(n), gL + 3 * (4 + n), gRr + 3 * (4 + n), dYx, dYy, dYz);
+    const double gradYk = dYx * g.S0 + dYy * g.S1 + dYz * g.S2;
+    gradYns -= gradYk;
+    Vc += Dk * gradYk;
+    const double Jk = -rho * Dk * gradYk;
+    const double hk = 0.5 * (hs[n * v + R] + hs[n * v + L]);
+    const double Yk = 0.5 * (YR(n) + YL(n));
+    Yns -= Yk;
+    sumYh += Yk * hk;
+    F[5 + n] += Jk;
+    f4 += Jk * hk;
+  }
+  Dk = 0.5 * (tr[(2 + NS - 1) * v + R] + tr[(2 + NS - 1) * v + L]);
+  Vc += Dk * gradYns;
+  const double corr = rho * Vc;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) F[5 + n] += 0.5 * (YR(n) + YL(n)) * corr;
+  f4 += corr * sumYh;
+  const double hns = 0.5 * (hs[(NS - 1) * v + R] + hs[(NS - 1) * v + L]);
+  f4 += (-rho * Dk * gradYns + Yns * corr) * hns;
+  F[4] += f4;
+#pragma unroll
+  for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
+}
+
+// dQ = (low faces - high faces) detJinv (peregrine/simulator/advec/kernels/applyflux.mako:2-11)
+template <int NS>
+__global__ void k_applyflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Fi,
+                            const double *__restrict__ Fj, const double *__restrict__ Fk,
+                            const double *__restrict__ met, double *__restrict__ dQall) {
+  constexpr int NE = 4 + NS;
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)B.nx * B.ny * B.nz) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k), v = B.vol;
+  const long long sJ = B.X, sK = (long long)B.X * B.Y;
+  const double detJinv = met[M_NCOMP * B.cv + M_DETJINV * v + c];
+  const double *fi = Fi + NE * B.cv + c, *fj = Fj + NE * B.cv + c, *fk = Fk + NE * B.cv + c;
+  double *dQ = dQall + NE * B.cv + c;
+#pragma unroll
+  for (int l = 0; l < NE; l++)
+    dQ[l * v] = (fi[l * v] + fj[l * v] + fk[l * v] - fi[l * v + 1] - fj[l * v + sJ] - fk[l * v + sK]) * detJinv;
+}
+
+// one combine (peregrine/integrators/kernels/combine.mako:1-13) on a block's interior
+struct CombineDev {
+  double *out;
+  const double *X[3];
+  double w[3];
+  double wout;
+  int own, nterms, step;
+};
+
+__global__ void k_combine(const BlockDev *__restrict__ blks, int b, int ne, CombineDev cd, const double *__restrict__ dt) {
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)B.nx * B.ny * B.nz) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k) + ne * B.cv;
+  const double d = *dt;
+  for (int l = 0; l < ne; l++) {
+    const long long at = c + l * B.vol;
+    auto term = [&](int n) { return (cd.step && n == cd.nterms - 1) ? cd.w[n] * d * cd.X[n][at] : cd.w[n] * cd.X[n][at]; };
+    double acc;
+    int n0;
+    if (cd.own) {
+      acc = cd.wout * cd.out[at];
+      n0 = 0;
+    } else {
+      acc = term(0);
+      n0 = 1;
+    }
+    for (int n = n0; n < cd.nterms; n++) acc = acc + term(n);
+    cd.out[at] = acc;
+  }
+}
+
+// Q from primitives on the interior (the reference's fromprims)
+template <int NS>
+__global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const double *__restrict__ prims,
+                            double *__restrict__ Qall) {
+  constexpr int NE = 4 + NS;
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)B.nx * B.ny * B.nz;
+  if (t >= n) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k);
+  double q[NE], Q[NE];
+#pragma unroll
+  for (int l = 0; l < NE; l++) q[l] = prims[l * n + t];
+  fromprims<NS>(q, Q);
+  double *Qo = Qall + NE * B.cv + c;
+#pragma unroll
+  for (int l = 0; l < NE; l++) Qo[l * B.vol] = Q[l];
+}
+
+// interior cells between a packed host-order buffer [comp][k][j][i] and a register
+__global__ void k_unpack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ src,
+                         double *__restrict__ Rall) {
+  const BlockDev &B = blks[b];
+  const long long n = (long long)B.nx * B.ny * B.nz;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k) + ne * B.cv;
+  for (int l = 0; l < ne; l++) Rall[c + l * B.vol] = src[l * n + t];
+}
+
+__global__ void k_pack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ Rall,
+                       double *__restrict__ dst) {
+  const BlockDev &B = blks[b];
+  const long long n = (long long)B.nx * B.ny * B.nz;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k) + ne * B.cv;
+  for (int l = 0; l < ne; l++) dst[l * n + t] = Rall[c + l * B.vol];
+}
+
+}  // namespace pgb

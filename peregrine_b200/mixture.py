@@ -1,0 +1,73 @@
+"""The gas: per-species constants the kernels read.
+
+Each table below is the reference's, computed with the same floating-point
+operations so the kernels see the same doubles the reference writes into
+its kernels as hex literals (peregrine/codegen/constants.py:13-20):
+
+* mixture basics ``MW``, ``MWinv``, ``Rsp`` (simulator/mixture/mixture.py:54-58);
+* calorically perfect gas: ``cppoly`` = cp0 MW / Ru, ``h298`` = dHf298 / Ru -
+  Tref cppoly (simulator/mixture/caloric/constcp.py:12-21), and the moments
+  ``cp0``, ``h298R`` = h298 Rsp (simulator/mixture/eos/base.py:48-64,
+  simulator/mixture/eos/cpg/__init__.py);
+* constant transport ``mu0``, ``kappa0`` (simulator/mixture/transport/constant.py);
+* Wilke's rule ``MWqinv`` = MW^-1/4, ``wilkepair`` = 1 / sqrt(8 (1 + MW_n / MW_m))
+  (simulator/mixture/mixrule/wilke.py:8-14);
+* Lewis diffusion ``lewis``, one unless a species states its own
+  (simulator/mixture/diffusion/lewis.py).
+"""
+
+import numpy as np
+
+Ru = 8314.46261815324
+Tref = 298.15
+
+# the kernels' table ids, shared with include/pgb200.h
+TABLES = ("MW", "MWinv", "Rsp", "cp0", "h298R", "hpolyR0", "h298", "mu0", "kappa0",
+          "MWqinv", "wilkepair", "lewis")
+
+
+class Mixture:
+    def __init__(self, cfgsect):
+        species = cfgsect["species"]
+        if not isinstance(species, dict) or not species:
+            raise ValueError("mixture.species: this build takes a dict of name to data")
+        self.cfgsect = cfgsect
+        self.species = {k: dict(v) for k, v in species.items()}
+        self.spnames = list(self.species)
+        self.ns = len(self.spnames)
+        self.eos = cfgsect["eos"]
+        self.trans = cfgsect["trans"]
+        if self.eos != "cpg":
+            raise ValueError(f"mixture.eos {self.eos!r}: this gas model is not built yet")
+        for name, sp in self.species.items():
+            for need in ("MW", "cp0"):
+                if need not in sp:
+                    raise ValueError(f"cpg needs {need} for {name}")
+            if self.trans == "constant":
+                for need in ("mu0", "kappa0"):
+                    if need not in sp:
+                        raise ValueError(f"constant needs {need} for {name}")
+
+    def collect(self, key, default=None):
+        values = [sp.get(key, default) for sp in self.species.values()]
+        return np.array(values, dtype=np.float64)
+
+    def constants(self):
+        MW = self.collect("MW")
+        out = dict(Ru=np.array(Ru), MW=MW, MWinv=1.0 / MW, Rsp=Ru / MW)
+        # calorically perfect: a constant cp is its own fit, exactly
+        cp0 = self.collect("cp0")
+        cppoly = np.array([[sp["cp0"] * sp["MW"] / Ru] for sp in self.species.values()])
+        h298 = np.array([sp.get("dHf298", 0.0) / Ru - Tref * c[0]
+                         for sp, c in zip(self.species.values(), cppoly)])
+        Rsp = out["Rsp"]
+        out.update(cppoly=cppoly, hpoly=cppoly.copy(), h298=h298, cp0=cp0,
+                   cppolyR=cppoly * Rsp[:, None], hpolyR=cppoly * Rsp[:, None],
+                   h298R=h298 * Rsp)
+        if self.trans == "constant":
+            out.update(mu0=self.collect("mu0"), kappa0=self.collect("kappa0"))
+        if self.trans is not None:
+            out.update(MWqinv=MW ** -0.25,
+                       wilkepair=1.0 / np.sqrt(8.0 * (1.0 + MW[:, None] / MW[None, :])))
+            out.update(lewis=self.collect("lewis", 1.0))
+        return out

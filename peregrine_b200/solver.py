@@ -1,0 +1,263 @@
+"""The case driver: the reference's solver API over the native library.
+
+``get_backend``, ``get_solver`` and ``Solver`` keep the reference's names and
+calls (peregrine/run.py:6-8, peregrine/backend/__init__.py:8,
+peregrine/multiblock/solver.py:23-391): ``step(dt)``, ``rhs(Q=, dQ=)``,
+``set_prims``, ``regs``, ``blocks[i].<array>.get() / set()``, ``tme``,
+``nrt``, ``run()``.  The arrays, their halos, the kernels and the CUDA graphs
+live in the library (include/pgb200.h); this module fills a case from the
+config, the mixture and the mesh and forwards the calls.
+"""
+
+import ctypes
+
+import numpy as np
+
+from peregrine_b200 import native
+from peregrine_b200.config import ConfigError
+from peregrine_b200.grid import metrics as make_metrics
+from peregrine_b200.integrators import stage_records
+from peregrine_b200.mixture import Mixture
+
+NG = 2
+
+
+class Backend:
+    """One device, as the reference's device backend (peregrine/backend/device/backend.py:50-80)."""
+
+    name = "b200"
+
+    def __init__(self, config=None, device=0):
+        self.config = config
+        self.device = device
+        native.load()
+        count = ctypes.c_int(0)
+        native.call("pgb_device_count", ctypes.byref(count))
+        if count.value == 0:
+            raise native.PgbCudaError("no CUDA device: this backend runs on a B200 and has no host fallback")
+        native.call("pgb_device_init", device)
+
+    def sync(self):
+        native.call("pgb_device_sync")
+
+    def stop(self):
+        self.sync()
+
+
+def get_backend(name, config=None, device=0):
+    if name not in ("cuda", "b200"):
+        raise ValueError(f"{name!r}: this build runs on the device alone (cuda / b200)")
+    return Backend(config, device)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Array:
+    """A register of one block, on the device; get/set the reference's host shape."""
+
+    def __init__(self, solver, blk, reg):
+        self.solver, self.blk, self.reg = solver, blk, reg
+
+    @property
+    def shape(self):
+        b = self.solver.blocks[self.blk]
+        return tuple(n + 2 * NG for n in b.cells) + (self.solver.ne,)
+
+    def get(self):
+        """The full-shaped host array; halo cells are NaN (the device keeps them)."""
+        b = self.solver.blocks[self.blk]
+        inner = np.empty(b.cells + (self.solver.ne,), order="F")
+        native.call("pgb_array_get", self.solver.case, self.blk, self.reg, _fptr(inner), inner.size)
+        out = np.full(self.shape, np.nan)
+        out[b.interior] = inner
+        return out
+
+    def set(self, values):
+        b = self.solver.blocks[self.blk]
+        values = np.asarray(values, dtype=np.float64)
+        inner = values[b.interior] if values.shape == self.shape else values
+        inner = np.asfortranarray(inner)
+        native.call("pgb_array_set", self.solver.case, self.blk, self.reg, _fptr(inner), inner.size)
+
+
+class SolverBlock:
+    def __init__(self, solver, blk):
+        self.solver, self.blk = solver, blk
+        self.mesh = blk
+        for name, reg in solver.regnum.items():
+            setattr(self, name, Array(solver, blk.nblki, reg))
+
+    def __getattr__(self, name):
+        return getattr(self.mesh, name)
+
+
+class Solver:
+    def __init__(self, cfg, mesh, backend, state=None):
+        cfg.validate()
+        self.cfg, self.mesh, self.backend = cfg, mesh, backend
+        sim = cfg["simulation"]
+        self.nrt, self.tme = 0, 0.0
+        self.mixture = Mixture(cfg["mixture"])
+        self.ns = self.mixture.ns
+        self.ne = 4 + self.ns
+        self.integrator = cfg["time-integration"]["integrator"]
+        records, nregs = stage_records(self.integrator)
+        self.nregs = nregs
+        self.regs = tuple(["Q"] + [f"Q{n}" for n in range(1, nregs)])
+        self.regnum = {name: n for n, name in enumerate(self.regs)}
+        launch = cfg["backend-b200"]["launch"]
+        self.path = native.PATH_BATCHED if launch == "batched" else native.PATH_PER_BLOCK
+        self.graph = bool(cfg["backend-b200"]["graph"])
+        adv = cfg["adv-flux"]
+        phys = native.Physics()
+        phys.simulator = native.NAVIER_STOKES if sim["simulator"] == "navier-stokes" else native.EULER
+        phys.eos = native.EOS_CPG
+        phys.primary = {"kepaec": native.FLUX_KEPAEC, "hllc": native.FLUX_HLLC, "rusanov": native.FLUX_RUSANOV}[adv["primary"]]
+        phys.recon = native.RECON_CONSTANT if adv["recon"] == "constant" else native.RECON_MUSCL
+        phys.limiter = 0
+        trans = cfg["mixture"]["trans"]
+        phys.trans = {None: native.TRANS_NONE, "constant": native.TRANS_CONSTANT,
+                      "kinetic-theory": native.TRANS_KINETIC}[trans]
+        phys.ns = self.ns
+        phys.nregs = nregs
+        phys.alpha = float(cfg["diff-flux"]["values"].get("alpha", 1.0))
+        handle = ctypes.c_void_p()
+        native.call("pgb_case_create", ctypes.byref(phys), ctypes.byref(handle))
+        self.case = handle
+        try:
+            self._fill(records)
+        except Exception:
+            native.call("pgb_case_destroy", self.case)
+            self.case = None
+            raise
+        if self.path == native.PATH_BATCHED and not self.fused_capable():
+            # the batched kernel takes the single-species kepaec case; any other
+            # physics runs the per-block kernels, still on the device
+            self.path = native.PATH_PER_BLOCK
+        if state is None:
+            self._uniform_ics()
+
+    def fused_capable(self):
+        cfg = self.cfg
+        return (self.ns == 1 and cfg["adv-flux"]["primary"] == "kepaec" and cfg["adv-flux"]["recon"] == "constant"
+                and cfg["mixture"]["eos"] == "cpg")
+
+    def _fill(self, records):
+        consts = self.mixture.constants()
+        tables = dict(Rsp=consts["Rsp"], cp0=consts["cp0"], h298R=consts["h298R"], MWinv=consts["MWinv"],
+                      hpoly0=np.asarray(consts["hpoly"])[:, 0], h298=consts["h298"])
+        for key in ("mu0", "kappa0", "MWqinv", "wilkepair", "lewis"):
+            if key in consts:
+                tables[key] = consts[key]
+        for name, values in tables.items():
+            v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+            native.call("pgb_case_set_table", self.case, name.encode(), _fptr(v), v.size)
+        self.mesh_blocks = self.mesh.make_blocks(NG)
+        for blk in self.mesh_blocks:
+            out = ctypes.c_int()
+            native.call("pgb_case_add_block", self.case, *blk.cells, ctypes.byref(out))
+        for blk in self.mesh_blocks:
+            for face in blk.intfaces:
+                nbr = -1 if face.nbr is None else face.nbr
+                native.call("pgb_case_connect", self.case, blk.nblki, face.nface, nbr, face.nbrface or 0)
+        native.call("pgb_case_set_stages", self.case, records, len(records))
+        native.call("pgb_case_finalize", self.case)
+        self.metrics = []
+        for blk in self.mesh_blocks:
+            m = make_metrics(blk.nodes, NG)
+            self.metrics.append(m)
+            for name, arr in m.items():
+                a = np.asarray(arr, dtype=np.float64)
+                a = np.asfortranarray(a.reshape(a.shape[:3] + (-1,)))
+                native.call("pgb_metric_set", self.case, blk.nblki, native.METRIC_IDS[name], _fptr(a), a.size)
+        self.blocks = [SolverBlock(self, b) for b in self.mesh_blocks]
+
+    def __del__(self):
+        case = getattr(self, "case", None)
+        if case:
+            try:
+                native.call("pgb_case_destroy", case)
+            except Exception:
+                pass
+            self.case = None
+
+    # the reference's ics section: a uniform state of p, u, v, w, T, Y
+    def _uniform_ics(self):
+        ic = self.cfg["ics"]
+        names = self.mixture.spnames
+        unknown = sorted(set(ic["Y"]) - set(names))
+        if unknown:
+            raise ConfigError("ics.Y", f"names {unknown}, which are not species of this mixture: {names}.")
+        values = [ic[k] for k in ("p", "u", "v", "w", "T")] + [ic["Y"].get(n, 0.0) for n in names[:-1]]
+        prims = []
+        for b in self.mesh_blocks:
+            q = np.empty(tuple(n + 2 * NG for n in b.cells) + (self.ne,))
+            q[...] = values
+            prims.append(q)
+        self.set_prims(prims)
+
+    ###########################################################################
+    # The reference's per-step API
+    ###########################################################################
+    def set_prims(self, prims):
+        """Q from primitive arrays, one per block: p, u, v, w, T, Y... in the last axis."""
+        for b, q in zip(self.mesh_blocks, prims):
+            q = np.asarray(q, dtype=np.float64)
+            full = tuple(n + 2 * NG for n in b.cells) + (self.ne,)
+            inner = q[b.interior] if q.shape == full else q
+            if inner.shape != b.cells + (self.ne,):
+                raise ValueError(f"block {b.nblki}: primitives of shape {q.shape}")
+            inner = np.asfortranarray(inner)
+            native.call("pgb_set_prims", self.case, b.nblki, 0, _fptr(inner), inner.size)
+
+    def rhs(self, *, Q="Q", dQ=None):
+        dQ = dQ or self.regs[-1]
+        native.call("pgb_rhs", self.case, self.regnum[Q], self.regnum[dQ])
+
+    def step(self, dt, nsteps=1):
+        native.call("pgb_step", self.case, float(dt), int(nsteps), self.path, int(self.graph))
+        self.nrt += nsteps
+        self.tme += dt * nsteps
+
+    def run(self):
+        dt = self.cfg["simulation"]["dt"]
+        self.step(dt, self.cfg["simulation"]["niter"])
+        self.backend.sync()
+
+    def last_step_ms(self):
+        ms = ctypes.c_float()
+        native.call("pgb_last_step_ms", self.case, ctypes.byref(ms))
+        return ms.value
+
+    def launches_per_step(self, path=None):
+        n = ctypes.c_int()
+        native.call("pgb_launches_per_step", self.case, self.path if path is None else path, ctypes.byref(n))
+        return n.value
+
+    def set_tile(self, blk, tw, th, kchunk):
+        native.call("pgb_set_tile", self.case, blk, tw, th, kchunk)
+
+    def get_tile(self, blk):
+        v = [ctypes.c_int() for _ in range(3)]
+        native.call("pgb_get_tile", self.case, blk, *[ctypes.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
+    def uniform(self, blk):
+        u = ctypes.c_int()
+        native.call("pgb_block_uniform", self.case, blk, ctypes.byref(u))
+        return bool(u.value)
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        native.call("pgb_case_stream", self.case, ctypes.byref(s))
+        return s.value
+
+    @property
+    def ncells(self):
+        return sum(b.ncells for b in self.mesh_blocks)
+
+
+def get_solver(cfg, mesh, backend, state=None, cls=Solver):
+    return cls(cfg, mesh, backend, state)

@@ -1,0 +1,112 @@
+"""Device path against the CPU oracle: the right-hand side and whole steps.
+
+The reference's tolerance convention: a component's error is measured
+against that component's largest magnitude over the block
+(tests/simulator/test_facefluxes.py:53-56).  Bars: RHS 1e-12, state after
+steps 1e-9, conservation to rounding.
+"""
+
+import numpy as np
+import pytest
+
+from peregrine_b200 import cases
+from peregrine_b200 import native
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+STATE_TOL = 1e-9
+
+
+def rowmax_err(got, want):
+    """max |got - want| per component over the max |want| of that component."""
+    scale = np.abs(want).reshape(-1, want.shape[-1]).max(axis=0)
+    scale[scale == 0.0] = 1.0
+    return (np.abs(got - want).reshape(-1, want.shape[-1]).max(axis=0) / scale).max()
+
+
+def build(simulator="navier-stokes", integrator="rk4", cells=16, blocks=(2, 2, 1), launch="batched", seed=3,
+          low=None, high=None, jostle=False):
+    import peregrine_b200 as pg
+    from oracle.oracle import Oracle
+
+    cfg = cases.tgv_config(simulator, integrator, launch)
+    mesh = cases.tgv_mesh(cells, blocks, seed=seed, low=low, high=high)
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    prims = cases.tgv_prims(mb.mesh_blocks, mb.metrics, seed=seed, noise=1e-3)
+    mb.set_prims(prims)
+    orc = Oracle(mb.mixture.constants(), 1, simulator, mb.mesh_blocks, mb.metrics, integrator)
+    orc.set_prims(prims)
+    return mb, orc
+
+
+def interiors(mb, arrays):
+    return [a[b.interior] for a, b in zip(arrays, mb.mesh_blocks)]
+
+
+@pytest.mark.parametrize("simulator", ["euler", "navier-stokes"])
+def test_rhs_matches_oracle(simulator):
+    mb, orc = build(simulator, cells=16, blocks=(2, 2, 1))
+    dq = mb.regs[-1]
+    mb.rhs(Q="Q", dQ=dq)
+    got = [getattr(b, dq).get() for b in mb.blocks]
+    want = [np.zeros_like(r) for r in orc.regs[0]]
+    orc.rhs(orc.regs[0], want)
+    for g, w in zip(interiors(mb, got), interiors(mb, want)):
+        assert rowmax_err(g, w) < RHS_TOL
+
+
+@pytest.mark.parametrize("launch", ["batched", "per-block"])
+@pytest.mark.parametrize("integrator", ["rk4", "tvd-rk3"])
+def test_steps_match_oracle(launch, integrator):
+    mb, orc = build("navier-stokes", integrator, cells=16, blocks=(2, 1, 2), launch=launch, low=5, high=11)
+    _, g = cases.tgv_gas()
+    dt = 0.2 * (2 * np.pi / 16) / (g["U0"] + np.sqrt(g["gamma"] * g["R"] * cases.T0))
+    for _ in range(3):
+        mb.step(dt)
+        orc.step(dt)
+    got = [b.Q.get() for b in mb.blocks]
+    for gq, w in zip(interiors(mb, got), interiors(mb, orc.regs[0])):
+        assert rowmax_err(gq, w) < STATE_TOL
+
+
+def test_batched_equals_per_block():
+    a, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 2, 2), launch="batched", low=6, high=10)
+    b, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 2, 2), launch="per-block", low=6, high=10)
+    for s in (a, b):
+        s.step(1e-5, 4)
+    for x, y in zip(a.blocks, b.blocks):
+        gx, gy = x.Q.get()[x.mesh.interior], y.Q.get()[y.mesh.interior]
+        assert rowmax_err(gx, gy) < STATE_TOL
+
+
+def test_mass_is_conserved():
+    mb, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 2, 2), low=6, high=10)
+
+    def totals():
+        s = 0.0
+        for b, m in zip(mb.blocks, mb.metrics):
+            vol = 1.0 / m["detJinv"][b.mesh.interior]
+            s = s + (b.Q.get()[b.mesh.interior] * vol[..., None]).sum(axis=(0, 1, 2))
+        return s
+
+    before = totals()
+    mb.step(1e-5, 10)
+    after = totals()
+    assert abs(after[0] - before[0]) <= 1e-13 * abs(before[0])
+    assert abs(after[4] - before[4]) <= 1e-13 * abs(before[4])
+
+
+def test_uniform_blocks_are_detected():
+    mb, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 1, 1))
+    mb.step(1e-6)
+    assert all(mb.uniform(n) for n in range(len(mb.blocks)))
+
+
+def test_unsupported_physics_is_refused():
+    import peregrine_b200 as pg
+
+    cfg = cases.tgv_config()
+    cfg["mixture"]["eos"] = "tpg"
+    with pytest.raises((ValueError, native.PgbUnsupported)):
+        pg.get_solver(cfg.validate(), cases.tgv_mesh(8), pg.get_backend("cuda", cfg))
