@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""FP64 cell-stage updates/s of the RHS + Runge-Kutta step, on B200.
+
+Workload (the multiblock Taylor-Green configuration): a periodic 128^3
+cube on [0, 2 pi]^3 cut into 3 x 3 x 3 blocks whose per-axis sizes are drawn
+from a seed in [30, 56] cells, Navier-Stokes with the kepaec flux and
+alpha-damping viscous flux, calorically perfect air, constant transport at
+Re 1600, Mach 0.1, RK4, FP64; seeded synthetic initial field.  One step is
+one RK4 step (four stages) of every cell; the metric counts cells x stages.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+The b200 arm times K steps of the batched fused path replayed as a CUDA
+graph (CUDA events on the case's stream), then the same K steps with a
+CUDA event after every launch for the fused kernel's own time (the roofline
+line), the plain per-block path for comparison, an end-to-end leg with the
+state copied in from and out to pinned host memory every step, and the CPU
+oracle on a bounded sample.  With N > 1 (torchrun), every rank runs its own
+replica of the workload (the cross-GPU halo exchange is not built); the
+time is the max over ranks.  The reference arm times the reference CPU
+restatement (oracle/, OpenMP on every host core) on the same workload.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CELLS = 128
+BLOCKS = (3, 3, 3)
+CUT_LOW, CUT_HIGH = 30, 56
+SEED = 0
+NE = 5
+STAGES = 4
+# RK4 register traffic per cell and stage, 8 ne (reads + writes): stage 0
+# reads start, writes total and stage (3); stages 1, 2 read stage, total and
+# start, write total and stage (5); stage 3 reads stage, total and start,
+# writes start (4); the mean is 4.25 registers, 170 bytes
+STAGE_REGS = (3, 5, 5, 4)
+METRIC = "FP64 cell-stage updates/s, batched vs per-block, % HBM roofline; p50/p99 latency"
+WORKLOAD = "tgv-128^3-27-uneven-blocks-ns-kepaec-alpha-damping-cpg-rk4"
+
+
+def set_cells(n):
+    global CELLS
+    CELLS = n
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons while running."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and s[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_case(launch, device=0):
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases
+
+    cfg = cases.tgv_config("navier-stokes", "rk4", launch)
+    mesh = cases.tgv_mesh(CELLS, BLOCKS, seed=SEED, low=CUT_LOW, high=CUT_HIGH)
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg, device=device))
+    prims = cases.tgv_prims(mb.mesh_blocks, mb.metrics, seed=SEED)
+    mb.set_prims(prims)
+    return mb, mesh, prims
+
+
+def stable_dt():
+    from peregrine_b200 import cases
+
+    _, g = cases.tgv_gas()
+    h = 2 * np.pi / CELLS
+    return 0.3 * h / (g["U0"] + np.sqrt(g["gamma"] * g["R"] * cases.T0))
+
+
+def time_graph(mb, dt, steps):
+    mb.step(dt, steps)
+    return mb.last_step_ms()
+
+
+def fused_kernel_times(mb, dt, steps):
+    import ctypes
+
+    from peregrine_b200 import native
+
+    cap = 64 * steps
+    ms = (ctypes.c_float * cap)()
+    kind = (ctypes.c_int * cap)()
+    n = ctypes.c_int()
+    native.call("pgb_step_timed", mb.case, float(dt), int(steps), mb.path, ms, kind, cap, ctypes.byref(n))
+    rows = [(ms[q], kind[q]) for q in range(min(n.value, cap))]
+    return rows
+
+
+def e2e_leg(mb, dt, steps):
+    import ctypes
+
+    from peregrine_b200 import native
+
+    n = mb.ncells * NE
+    host = np.zeros(n)
+    native.call("pgb_host_register", host.ctypes.data_as(ctypes.c_void_p), host.nbytes)
+    ptr = host.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    try:
+        native.call("pgb_state_get", mb.case, 0, ptr, n)
+        # warm
+        native.call("pgb_state_set", mb.case, 0, ptr, n)
+        mb.step(dt)
+        native.call("pgb_state_get", mb.case, 0, ptr, n)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            native.call("pgb_state_set", mb.case, 0, ptr, n)
+            mb.step(dt)
+            native.call("pgb_state_get", mb.case, 0, ptr, n)
+        wall = time.perf_counter() - t0
+    finally:
+        native.call("pgb_host_unregister", host.ctypes.data_as(ctypes.c_void_p))
+    return wall, host.nbytes
+
+
+def cpu_baseline(mesh_blocks, metrics, prims, constants, budget_s=15.0):
+    """The oracle (reference CPU restatement, OpenMP on every core) on stages of the same grid."""
+    from oracle.oracle import Oracle
+
+    orc = Oracle(constants, 1, "navier-stokes", mesh_blocks, metrics, "rk4")
+    orc.set_prims(prims)
+    dQ = [np.zeros_like(r) for r in orc.regs[0]]
+    ncells = sum(b.ncells for b in mesh_blocks)
+    stages = 0
+    t0 = time.perf_counter()
+    while True:
+        orc.rhs(orc.regs[0], dQ)
+        stages += 1
+        if time.perf_counter() - t0 > budget_s or stages >= 8:
+            break
+    wall = time.perf_counter() - t0
+    return ncells * stages / wall, stages, wall
+
+
+def reference_arm(args):
+    """The reference CPU restatement's throughput on the same workload; rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from peregrine_b200 import cases
+    from peregrine_b200.grid import metrics as make_metrics
+    from peregrine_b200.mixture import Mixture
+    from oracle.oracle import Oracle
+
+    cfg = cases.tgv_config("navier-stokes", "rk4")
+    mesh = cases.tgv_mesh(CELLS, BLOCKS, seed=SEED, low=CUT_LOW, high=CUT_HIGH)
+    blocks = mesh.make_blocks(2)
+    mets = [make_metrics(b.nodes, b.ng) for b in blocks]
+    prims = cases.tgv_prims(blocks, mets, seed=SEED)
+    mix = Mixture(cfg["mixture"])
+    orc = Oracle(mix.constants(), 1, "navier-stokes", blocks, mets, "rk4")
+    orc.set_prims(prims)
+    dQ = [np.zeros_like(r) for r in orc.regs[0]]
+    ncells = sum(b.ncells for b in blocks)
+    for _ in range(args.warmup):
+        orc.rhs(orc.regs[0], dQ)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.rhs(orc.regs[0], dQ)
+    wall = time.perf_counter() - t0
+    value = ncells * args.steps / wall
+    cores = os.cpu_count()
+    sample = f"one RK stage (RHS) of every cell of the workload per step, {args.steps} steps"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cell-stage/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD if CELLS == 128 else f"{WORKLOAD} at {CELLS}^3", "cells": ncells, "blocks": len(blocks), "parallelism": "openmp"},
+            "cpu_baseline": {"value": value, "unit": "cell-stage/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "cell-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-extra", action="store_true", help="skip the per-block and end-to-end legs")
+    ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
+    args = ap.parse_args()
+    set_cells(args.cells)
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    mb, mesh, prims = build_case("batched", device=local)
+    dt = stable_dt()
+    ncells = mb.ncells
+    # warm-up (the first call captures the graph)
+    mb.step(dt, args.warmup)
+    mb.backend.sync()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    barrier()
+    with Clocks(local) as clk:
+        ms = time_graph(mb, dt, args.steps)
+    barrier()
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_cell_stages = ncells * STAGES * args.steps * world
+    value = total_cell_stages / (ms / 1e3)
+    launches = mb.launches_per_step()
+
+    # the fused kernel's own launches, timed by events between launches
+    rows = fused_kernel_times(mb, dt, min(args.steps, 20))
+    fused = [m for m, k in rows if k == 1]
+    halo = [m for m, k in rows if k == 0]
+    per_stage = [float(np.mean(fused[s::STAGES])) for s in range(STAGES)]
+    bytes_per_launch = [ncells * 8 * NE * r for r in STAGE_REGS]
+    achieved = float(np.mean([b / (t / 1e3) / 1e9 for b, t in zip(bytes_per_launch, per_stage)]))
+    peak, peak_kind = peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "fused_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f)
+        traffic = tr.get("bytes_per_cell_stage", None)
+        if traffic is not None:
+            traffic = traffic * ncells
+
+    from peregrine_b200 import native
+
+    per_block, e2e = None, None
+    if not args.no_extra:
+        # the plain per-block path
+        mb.path = native.PATH_PER_BLOCK
+        mb.step(dt, 2)
+        mb.backend.sync()
+        pb_steps = max(2, min(args.steps // 4, 20))
+        ms_pb = time_graph(mb, dt, pb_steps)
+        pb_launches = mb.launches_per_step()
+        mb.path = native.PATH_BATCHED
+        value_pb = ncells * STAGES * pb_steps / (ms_pb / 1e3)
+        per_block = {"value": value_pb, "ms_per_step": ms_pb / pb_steps, "launches_per_step": pb_launches,
+                     "speedup_batched": value / world / value_pb}
+        # end to end: state in from pinned host, a step, state out, every step
+        e2e_steps = max(3, min(args.steps // 4, 20))
+        wall, nbytes = e2e_leg(mb, dt, e2e_steps)
+        e2e = {"value": ncells * STAGES * e2e_steps / wall * world, "unit": "cell-stage/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, stages, cwall = cpu_baseline(mb.mesh_blocks, mb.metrics, prims, mb.mixture.constants())
+        cpu = {"value": v, "unit": "cell-stage/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{stages} RK stages (RHS) of the full workload, {cwall:.1f} s, OpenMP"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-stage/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": ncells, "blocks": len(mb.blocks), "stages_per_step": STAGES,
+                       "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "l2": "inputs larger than L2 (four registers of 2.4M cells x 5 doubles, 0.38 GB)",
+                       "path": "batched fused persistent kernel, CUDA graph per RK4 step"},
+            "per_block": per_block,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_fused1 (one RK stage)", "kernel_ms_per_stage": per_stage,
+                         "halo_ms_per_stage": float(np.mean(halo)) if halo else None,
+                         "algorithmic_bytes_per_cell_stage": 170},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -138,6 +138,14 @@ int pgb_metric_set(pgb_case *c, int blk, int which, const double *host, long cou
 int pgb_array_set(pgb_case *c, int blk, int reg, const double *host, long count);
 int pgb_array_get(pgb_case *c, int blk, int reg, double *host, long count);
 
+/* Every block's interior cells of register reg at once: the blocks' F-order
+ * interior arrays end to end, in block order (count = ne x total cells). */
+int pgb_state_set(pgb_case *c, int reg, const double *host, long count);
+int pgb_state_get(pgb_case *c, int reg, double *host, long count);
+/* page-lock a host buffer for fast copies (cudaHostRegister), and release it */
+int pgb_host_register(void *host, size_t bytes);
+int pgb_host_unregister(void *host);
+
 /* Q of register reg from primitives p, u, v, w, T, Y... on the interior
  * (the reference's fromprims, peregrine/simulator/euler/kernels/state/fromprims.mako) */
 int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count);
@@ -149,6 +157,12 @@ int pgb_rhs(pgb_case *c, int q, int dq);
 /* nsteps steps of dt on the chosen path; graph 1 captures one step into a CUDA
  * graph and replays it.  Returns when queued on the case's stream. */
 int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph);
+
+/* nsteps steps without a graph, a CUDA event between every launch; waits for
+ * them and returns each launch's device time (ms) and kind (0 halo fill,
+ * 1 fused stage, 2 per-block kernel, 3 combine) in launch order, up to cap
+ * launches; n is the number of launches. */
+int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int *kind, int cap, int *n);
 
 /* the stream the case queues on (a cudaStream_t) */
 int pgb_case_stream(const pgb_case *c, void **stream);

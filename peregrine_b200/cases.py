@@ -42,7 +42,7 @@ def tgv_config(simulator="navier-stokes", integrator="rk4", launch="batched"):
     return cfg.validate()
 
 
-def tgv_mesh(cells=32, blocks=(1, 1, 1), seed=0, low=None, high=None):
+def tgv_mesh(cells=32, blocks=(1, 1, 1), seed=0, low=None, high=None, jostle=0.0):
     """A periodic 2 pi cube of cells^3, cut into blocks; uneven cuts drawn from seed."""
     rng = np.random.default_rng(seed)
     cuts = []
@@ -54,7 +54,7 @@ def tgv_mesh(cells=32, blocks=(1, 1, 1), seed=0, low=None, high=None):
             cuts.append([base + (1 if m < cells - base * n else 0) for m in range(n)])
         else:
             cuts.append(uneven_cuts(cells, n, low, high, rng))
-    return CubeMesher(mbdims=list(blocks), cells=cuts, lengths=[2 * np.pi] * 3, periodic=[True] * 3)
+    return CubeMesher(mbdims=list(blocks), cells=cuts, lengths=[2 * np.pi] * 3, periodic=[True] * 3, jostle=jostle)
 
 
 def tgv_prims(blocks, metrics, ne=5, seed=0, noise=1e-6, mach=0.1):

@@ -49,6 +49,11 @@ struct FusedArgs {
   int qin;
   int ncomb;
   FusedCombine comb[2];
+  // the same combines with each register term as a slot of the registers
+  // the uniform kernel copies ahead (pre[slot] the physical register)
+  int npre;
+  int pre[3];
+  FusedCombine combp[2];
   const double *dt;
 };
 

@@ -1,0 +1,382 @@
+// The fused stage for blocks with uniform metrics: every face's area vector
+// along its own axis, the inverse Jacobian diagonal and the cells evenly
+// spaced (checked by the host on the block's own metric arrays).
+//
+// Same arithmetic as the general fused kernel, with the terms the uniform
+// metrics make exactly zero left out: an off-axis area component, an
+// off-diagonal of the inverse Jacobian, an off-axis damping or extrapolation
+// distance.  Each dropped term is a product with an exact zero, so only the
+// sign of a zero result can differ.  Two further choices, each a few ulp:
+// the face velocities of kepaec (Q[1..3] / Q[0]) and of the viscous flux
+// (Q[1..3] * rhoinv) are the one quotient, and the central differences of
+// the gradients are of those quotients (the reference forms
+// (Q+ rho- - Q- rho+) / (rho+ rho-), dqdxyz.mako:8-15).
+//
+// Layout of the work: a CTA of 256 threads, one thread per column of the
+// tile and its one-cell ring (R1).  A column's cell values come from a
+// shared plane; what a thread computes for its own column it keeps:
+//   step k:  i- and j-faces below its cell at plane k (its low faces) into
+//            shared; the loads of plane k+3 issued; plane k+2's values formed
+//            from the loads of the step before; the gradients of plane k+1;
+//            the k-face between k and k+1; dQ, combines and stores for the
+//            tile's cells of plane k.
+#pragma once
+#include "fused.cuh"
+
+namespace pgb {
+
+constexpr int F2_THREADS = 256;
+// cell values kept in shared memory per plane
+enum { P_RHO = 0, P_U, P_V, P_W, P_T, P_E, P_N };
+
+struct CellP {
+  double rho, u, v, w, T, e;
+};
+
+__device__ __forceinline__ CellP prim_of(const double q0, const double q1, const double q2, const double q3,
+                                         const double q4) {
+  CellP c;
+  const double ri = 1.0 / q0;
+  c.rho = q0;
+  c.e = (q4 - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * ri) * ri;
+  c.T = quot(c.e - kSp.h2981, kSp.cv1, kSp.cvinv1);
+  c.u = quot(q1, q0, ri);
+  c.v = quot(q2, q0, ri);
+  c.w = quot(q3, q0, ri);
+  return c;
+}
+
+// One face of axis AX on uniform metrics: kepaec plus, with VISC, the
+// single-species viscous rows, each with the zero-metric terms dropped.
+// gL, gR: the two cells' gradients, rows u, v, w, T, 3 wide.
+template <int AX, bool VISC>
+__device__ __forceinline__ void face_u(const BlockDev &B, const CellP &L, const CellP &R, const double *gL,
+                                       const double *gR, double *F) {
+  const double S = B.S[AX];
+  const double pL = L.rho * kSp.R1 * L.T, pR = R.rho * kSp.R1 * R.T;
+  const double thL = kSp.th1 * L.T, thR = kSp.th1 * R.T;
+  // kepaec.mako:3-17 with S = S e_AX
+  const double uf = 0.5 * (R.u + L.u), vf = 0.5 * (R.v + L.v), wf = 0.5 * (R.w + L.w);
+  const double ua = AX == 0 ? uf : AX == 1 ? vf : wf;
+  const double U = S * ua;
+  const double pf = 0.5 * (pR + pL);
+  const double rho = 0.5 * (R.rho + L.rho);
+  const double C = rho * U;
+  F[0] = C;
+  F[1] = AX == 0 ? C * uf + pf * S : C * uf;
+  F[2] = AX == 1 ? C * vf + pf * S : C * vf;
+  F[3] = AX == 2 ? C * wf + pf * S : C * wf;
+  const double Kj = C * 0.5 * (R.u * L.u + R.v * L.v + R.w * L.w);
+  const double uRa = AX == 0 ? R.u : AX == 1 ? R.v : R.w;
+  const double uLa = AX == 0 ? L.u : AX == 1 ? L.v : L.w;
+  const double Pj = 0.5 * (pL * (uRa * S) + pR * (uLa * S));
+  const double ef = 2.0 * thL * thR / (thL + thR) + 0.5 * ((L.e - thL) + (R.e - thR));
+  F[4] = ef * C + Kj + Pj;
+  if constexpr (VISC) {
+    // alpha-damping.mako:29-58 with the normal along AX
+    const double mu = kSp.mu1, kappa = kSp.kappa1;
+    const double lambda = 0.0 - 2.0 / 3.0 * mu;
+    const double damp = B.damp[AX], xL = B.xL[AX], xR = B.xR[AX];
+    // the face gradient of a row: the axis component damped toward the jump,
+    // the others the sides' mean
+    auto row = [&](const double phiL, const double phiR, const double *gl, const double *gr, double &ga, double &gb,
+                   double &gc) {
+      const double wl = phiL + gl[AX] * xL;
+      const double wr = phiR + gr[AX] * xR;
+      const double jump = wr - wl;
+      ga = 0.5 * (gr[AX] + gl[AX]) + damp * jump;
+      constexpr int B1 = (AX + 1) % 3, B2 = (AX + 2) % 3;
+      gb = 0.5 * (gr[B1] + gl[B1]);
+      gc = 0.5 * (gr[B2] + gl[B2]);
+    };
+    double d[3][3];  // d[row][direction]: du/dx ...
+    {
+      double a, b, c;
+      row(L.u, R.u, gL + 0, gR + 0, a, b, c);
+      d[0][AX] = a, d[0][(AX + 1) % 3] = b, d[0][(AX + 2) % 3] = c;
+      row(L.v, R.v, gL + 3, gR + 3, a, b, c);
+      d[1][AX] = a, d[1][(AX + 1) % 3] = b, d[1][(AX + 2) % 3] = c;
+      row(L.w, R.w, gL + 6, gR + 6, a, b, c);
+      d[2][AX] = a, d[2][(AX + 1) % 3] = b, d[2][(AX + 2) % 3] = c;
+    }
+    const double div = d[0][0] + d[1][1] + d[2][2];
+    // the stress row of the face normal: tau[AX][m]
+    double t0, t1, t2;
+    if constexpr (AX == 0) {
+      t0 = -2.0 * mu * d[0][0] - lambda * div;  // txx
+      t1 = -mu * (d[1][0] + d[0][1]);           // txy
+      t2 = -mu * (d[2][0] + d[0][2]);           // txz
+    } else if constexpr (AX == 1) {
+      t0 = -mu * (d[1][0] + d[0][1]);           // txy
+      t1 = -2.0 * mu * d[1][1] - lambda * div;  // tyy
+      t2 = -mu * (d[2][1] + d[1][2]);           // tyz
+    } else {
+      t0 = -mu * (d[2][0] + d[0][2]);           // txz
+      t1 = -mu * (d[2][1] + d[1][2]);           // tyz
+      t2 = -2.0 * mu * d[2][2] - lambda * div;  // tzz
+    }
+    F[1] += t0 * S;
+    F[2] += t1 * S;
+    F[3] += t2 * S;
+    const double wlT = L.T + gL[9 + AX] * xL;
+    const double wrT = R.T + gR[9 + AX] * xR;
+    const double dTa = 0.5 * (gR[9 + AX] + gL[9 + AX]) + damp * (wrT - wlT);
+    const double heatflux = -kappa * (dTa * S);
+    const double f4 = (uf * t0 + vf * t1 + wf * t2) * S + heatflux;
+    F[4] += f4;
+  }
+}
+
+// the gradient rows u, v, w, T of a cell from its six neighbours' values
+// (dqdxyz.mako:16-41 on a diagonal inverse Jacobian)
+__device__ __forceinline__ void grad_u(const BlockDev &B, const CellP &xm, const CellP &xp, const CellP &ym,
+                                       const CellP &yp, const CellP &zm, const CellP &zp, double *g) {
+  const double Jx = B.Jd[0], Jy = B.Jd[1], Jz = B.Jd[2];
+  g[0] = 0.5 * (xp.u - xm.u) * Jx, g[1] = 0.5 * (yp.u - ym.u) * Jy, g[2] = 0.5 * (zp.u - zm.u) * Jz;
+  g[3] = 0.5 * (xp.v - xm.v) * Jx, g[4] = 0.5 * (yp.v - ym.v) * Jy, g[5] = 0.5 * (zp.v - zm.v) * Jz;
+  g[6] = 0.5 * (xp.w - xm.w) * Jx, g[7] = 0.5 * (yp.w - ym.w) * Jy, g[8] = 0.5 * (zp.w - zm.w) * Jz;
+  g[9] = 0.5 * (xp.T - xm.T) * Jx, g[10] = 0.5 * (yp.T - ym.T) * Jy, g[11] = 0.5 * (zp.T - zm.T) * Jz;
+}
+
+// cp.async (sm_80 and later): an 8-byte copy global -> shared that does not
+// hold a register while in flight; groups complete in order
+__device__ __forceinline__ void cp8(double *dst, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <bool VISC>
+__global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
+  extern __shared__ double smem[];
+  __shared__ int s_tile;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_tile = (int)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const int t = s_tile;
+    __syncthreads();
+    if (t >= a.ntiles) return;
+    const TileDev T = a.tiles[t];
+    const BlockDev &B = a.blks[T.blk];
+    const int tw = T.tw, th = T.th;
+    const int W1 = tw + 2, H1 = th + 2, N1 = W1 * H1;
+    const int W2 = tw + 4, N2 = W2 * (th + 4);
+    // shared: P[3][P_N][N2] cell values of three planes; G[12][256]
+    // gradients of one plane; Fi[5][256], Fj[5][256] low-face fluxes;
+    // raw[2 slots][2 cells][5][256] the Q loads in flight; pre[2][3][5][256]
+    // the combines' registers for the next plane
+    double *P = smem;
+    double *G = P + 3 * P_N * N2;
+    double *Fi = G + (VISC ? 12 * F2_THREADS : 0);
+    double *Fj = Fi + 5 * F2_THREADS;
+    double *raw = Fj + 5 * F2_THREADS;
+    double *pre = raw + 2 * 2 * 5 * F2_THREADS;
+    const int v = (int)B.vol;
+    const int sJ = B.X, sK = B.X * B.Y;
+    const double *Q = a.R[a.qin] + 5 * B.cv;
+    // this thread's column in R1 coordinates (ring included), and in R2
+    const bool col = tid < N1;
+    const int ii = tid % W1, jj = tid / W1;
+    const int c2 = (ii + 1) + W2 * (jj + 1);
+    const bool tile = col && ii >= 1 && ii <= tw && jj >= 1 && jj <= th;
+    const bool ring_corner = (ii == 0 || ii == W1 - 1) && (jj == 0 || jj == H1 - 1);
+    // the second cell a thread loads: the outer ring of R2 less its corners
+    const int nring = 2 * (tw + th);
+    int r2 = -1, x2 = 0, y2 = 0;
+    if (tid < nring) {
+      int q = tid;
+      if (q < th) x2 = 0, y2 = q + 2;
+      else if ((q -= th) < th) x2 = W2 - 1, y2 = q + 2;
+      else if ((q -= th) < tw) x2 = q + 2, y2 = 0;
+      else x2 = (q - tw) + 2, y2 = th + 3;
+      r2 = x2 + W2 * y2;
+    }
+    // in-plane offsets of the two cells in the block's arrays
+    const int o1 = (T.j0 + jj + 1) * sJ + (T.i0 + ii + 1);
+    const int o2 = (T.j0 + y2) * sJ + (T.i0 + x2);
+    auto slot = [](int p) { return (p + 3) % 3; };
+    auto getP = [&](int s, int r) {
+      const double *Ps = P + s * P_N * N2;
+      CellP c;
+      c.rho = Ps[P_RHO * N2 + r], c.u = Ps[P_U * N2 + r], c.v = Ps[P_V * N2 + r];
+      c.w = Ps[P_W * N2 + r], c.T = Ps[P_T * N2 + r], c.e = Ps[P_E * N2 + r];
+      return c;
+    };
+    auto putP = [&](int s, int r, const CellP &c) {
+      double *Ps = P + s * P_N * N2;
+      Ps[P_RHO * N2 + r] = c.rho, Ps[P_U * N2 + r] = c.u, Ps[P_V * N2 + r] = c.v;
+      Ps[P_W * N2 + r] = c.w, Ps[P_T * N2 + r] = c.T, Ps[P_E * N2 + r] = c.e;
+    };
+    auto rawp = [&](int p, int which, int l) { return raw + (((p & 1) * 2 + which) * 5 + l) * F2_THREADS + tid; };
+    // the copies of plane p's Q for this thread's cells
+    auto fetch = [&](int p) {
+      const int z = (p + NG) * sK;
+      if (col) {
+#pragma unroll
+        for (int l = 0; l < 5; l++) cp8(rawp(p, 0, l), Q + l * v + z + o1);
+      }
+      if (r2 >= 0) {
+#pragma unroll
+        for (int l = 0; l < 5; l++) cp8(rawp(p, 1, l), Q + l * v + z + o2);
+      }
+    };
+    // the copies of the combines' registers at plane p for a tile cell
+    auto fetch_pre = [&](int p) {
+      if (!tile) return;
+      const long long base = 5 * B.cv + (p + NG) * sK + o1;
+      for (int m = 0; m < a.npre; m++) {
+        const double *R = a.R[a.pre[m]] + base;
+#pragma unroll
+        for (int l = 0; l < 5; l++) cp8(pre + (((p & 1) * 3 + m) * 5 + l) * F2_THREADS + tid, R + l * v);
+      }
+    };
+    auto cellof = [&](int p, int which) {
+      return prim_of(*rawp(p, which, 0), *rawp(p, which, 1), *rawp(p, which, 2), *rawp(p, which, 3), *rawp(p, which, 4));
+    };
+    auto store = [&](int p) {
+      if (col) putP(slot(p), c2, cellof(p, 0));
+      if (r2 >= 0) putP(slot(p), r2, cellof(p, 1));
+    };
+    auto grad_own = [&](int p, double *g) {
+      const int sm = slot(p - 1), s0 = slot(p), sp = slot(p + 1);
+      grad_u(B, getP(s0, c2 - 1), getP(s0, c2 + 1), getP(s0, c2 - W2), getP(s0, c2 + W2), getP(sm, c2), getP(sp, c2), g);
+    };
+    auto putG = [&](const double *g) {
+#pragma unroll
+      for (int q = 0; q < 12; q++) G[q * F2_THREADS + tid] = g[q];
+    };
+
+    const int k0 = T.k0, k1 = T.k1;
+    // prelude: planes k0-1 .. k0+1 in shared, the gradients of k0 in shared
+    // and of k0-1 in registers, the k face below k0; plane k0+2 and the
+    // combines' registers of plane k0 in flight
+    fetch(k0 - 2);
+    cp_commit();
+    cp_wait<0>();
+    const CellP below2 = col ? cellof(k0 - 2, 0) : CellP{};
+    for (int p = k0 - 1; p <= k0 + 1; p++) {
+      fetch(p);
+      cp_commit();
+      cp_wait<0>();
+      store(p);
+    }
+    fetch(k0 + 2);
+    fetch_pre(k0);
+    cp_commit();
+    __syncthreads();
+    double gbelow[12];
+    if constexpr (VISC) {
+      if (tile) {
+        const int s0 = slot(k0 - 1), sp = slot(k0);
+        grad_u(B, getP(s0, c2 - 1), getP(s0, c2 + 1), getP(s0, c2 - W2), getP(s0, c2 + W2), below2, getP(sp, c2),
+               gbelow);
+      }
+      double g[12];
+      if (col && !ring_corner) {
+        grad_own(k0, g);
+        putG(g);
+      }
+    }
+    __syncthreads();
+    double Fk[5];
+    if (tile) {
+      double gk0[12];
+#pragma unroll
+      for (int q = 0; q < 12; q++) gk0[q] = VISC ? G[q * F2_THREADS + tid] : 0.0;
+      face_u<2, VISC>(B, getP(slot(k0 - 1), c2), getP(slot(k0), c2), gbelow, gk0, Fk);
+    }
+    const double dt = *a.dt;
+
+    for (int k = k0; k < k1; k++) {
+      const int s0 = slot(k);
+      // 1. this column's low i and j faces at plane k
+      if (col && jj >= 1 && jj <= th && ii >= 1) {
+        double F[5], gl[12], gr[12];
+        if (VISC) {
+#pragma unroll
+          for (int q = 0; q < 12; q++) gl[q] = G[q * F2_THREADS + tid - 1], gr[q] = G[q * F2_THREADS + tid];
+        }
+        face_u<0, VISC>(B, getP(s0, c2 - 1), getP(s0, c2), gl, gr, F);
+#pragma unroll
+        for (int l = 0; l < 5; l++) Fi[l * F2_THREADS + tid] = F[l];
+      }
+      if (col && ii >= 1 && ii <= tw && jj >= 1) {
+        double F[5], gl[12], gr[12];
+        if (VISC) {
+#pragma unroll
+          for (int q = 0; q < 12; q++) gl[q] = G[q * F2_THREADS + tid - W1], gr[q] = G[q * F2_THREADS + tid];
+        }
+        face_u<1, VISC>(B, getP(s0, c2 - W2), getP(s0, c2), gl, gr, F);
+#pragma unroll
+        for (int l = 0; l < 5; l++) Fj[l * F2_THREADS + tid] = F[l];
+      }
+      // 2. the next copies go out; plane k+2 and plane k's combine
+      //    registers have landed; plane k+2 into shared
+      if (k + 3 <= k1 + 1) fetch(k + 3);
+      if (k + 1 < k1) fetch_pre(k + 1);
+      cp_commit();
+      cp_wait<1>();
+      store(k + 2);
+      __syncthreads();
+      // 3. the gradients of plane k+1 for this column, the k face above k
+      double gup[12];
+      if (VISC && col && !ring_corner) grad_own(k + 1, gup);
+      if (tile) {
+        double Fkh[5], gk[12];
+#pragma unroll
+        for (int q = 0; q < 12; q++) gk[q] = VISC ? G[q * F2_THREADS + tid] : 0.0;
+        face_u<2, VISC>(B, getP(s0, c2), getP(slot(k + 1), c2), gk, gup, Fkh);
+        // 4. dQ and the combines for the cell at plane k
+        const double dJ = B.detJinv;
+        double dQ[5];
+#pragma unroll
+        for (int l = 0; l < 5; l++)
+          dQ[l] = (Fi[l * F2_THREADS + tid] + Fj[l * F2_THREADS + tid] + Fk[l] - Fi[l * F2_THREADS + tid + 1] -
+                   Fj[l * F2_THREADS + tid + W1] - Fkh[l]) * dJ;
+        const long long base = 5 * B.cv + (k + NG) * sK + o1;
+        const double *pk = pre + ((k & 1) * 3) * 5 * F2_THREADS + tid;
+        double first[5];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+          if (m >= a.ncomb) break;
+          const FusedCombine &cb = a.combp[m];
+          double *out = a.R[cb.out] + base;
+#pragma unroll
+          for (int l = 0; l < 5; l++) {
+            auto val = [&](int n) {
+              const int s = cb.src[n];
+              return s == -1 ? dQ[l] : s == -2 ? first[l] : pk[(s * 5 + l) * F2_THREADS];
+            };
+            auto term = [&](int n) { return (cb.step && n == cb.nterms - 1) ? cb.w[n] * dt * val(n) : cb.w[n] * val(n); };
+            double acc = term(0);
+#pragma unroll
+            for (int n = 1; n < 4; n++)
+              if (n < cb.nterms) acc = acc + term(n);
+            if (m == 0) first[l] = acc;
+            if (cb.write) out[l * v] = acc;
+          }
+        }
+#pragma unroll
+        for (int l = 0; l < 5; l++) Fk[l] = Fkh[l];
+      }
+      __syncthreads();
+      // 5. the plane k+1 gradients replace plane k's
+      if (VISC && col && !ring_corner) putG(gup);
+      __syncthreads();
+    }
+    cp_wait<0>();
+  }
+}
+
+inline size_t fused2_smem(int tw, int th, bool visc) {
+  const int N2 = (tw + 4) * (th + 4);
+  return sizeof(double) * (size_t)(3 * P_N * N2 + (visc ? 12 : 0) * F2_THREADS + 10 * F2_THREADS +
+                                   2 * 2 * 5 * F2_THREADS + 2 * 3 * 5 * F2_THREADS);
+}
+
+}  // namespace pgb

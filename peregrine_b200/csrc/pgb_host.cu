@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "fused.cuh"
+#include "fused2.cuh"
 #include "layout.cuh"
 #include "physics.cuh"
 #include "plain.cuh"
@@ -89,6 +90,8 @@ struct pgb_case {
   size_t fused_smem = 0;
   bool tiles_dirty = true;
   bool uniform_done = false;
+  bool use_v2 = false;  // every block uniform: the uniform-metric fused kernel
+  int v2_ctas = 1;      // its resident CTAs per SM
   // register mapping: logical -> physical
   std::vector<int> phys_of, canonical;
   int period = 1, phase = 0;
@@ -100,6 +103,13 @@ struct pgb_case {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.0f;
   int launches[2] = {0, 0};
+  // per-launch timing (pgb_step_timed): an event after every launch
+  bool timing = false;
+  std::vector<cudaEvent_t> tev;
+  std::vector<int> tkind;
+  size_t tnext = 0;
+  double *d_stage = nullptr;  // whole-state staging
+  long long stage_cap = 0;
 };
 
 namespace {
@@ -273,15 +283,34 @@ void default_tile(HostBlock &B) {
   B.kchunk = (B.nz + 1) / 2;
 }
 
+// the uniform kernel's default: one thread per column of the tile and its
+// ring, 256 of them; i cut evenly in pieces of at most 30
+void default_tile2(HostBlock &B) {
+  const int pi = (B.nx + 29) / 30;
+  const int tw = (B.nx + pi - 1) / pi;
+  int th = std::max(1, F2_THREADS / (tw + 2) - 2);
+  th = std::min(th, B.ny);
+  const int pj = (B.ny + th - 1) / th;
+  th = (B.ny + pj - 1) / pj;
+  B.tw = tw, B.th = th;
+  B.kchunk = (B.nz + 1) / 2;
+}
+
+bool tile_fits(const pgb_case *c, int tw, int th) {
+  return c->use_v2 ? (tw + 2) * (th + 2) <= F2_THREADS && 2 * (tw + th) <= F2_THREADS : tw * th <= FUSED_THREADS;
+}
+
 int build_tiles(pgb_case *c) {
   std::vector<TileDev> tiles;
   size_t smem = 0;
   const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
   for (int b = 0; b < (int)c->blocks.size(); b++) {
     HostBlock &B = c->blocks[b];
-    if (B.tw <= 0) default_tile(B);
-    if (B.tw * B.th > FUSED_THREADS) return fail(PGB_ERR_ARG, "tile larger than 128 cells");
-    smem = std::max(smem, fused_smem(B.tw, B.th, visc));
+    if (B.tw <= 0 || !tile_fits(c, B.tw, B.th)) {
+      if (c->use_v2) default_tile2(B);
+      else default_tile(B);
+    }
+    smem = std::max(smem, c->use_v2 ? fused2_smem(B.tw, B.th, visc) : fused_smem(B.tw, B.th, visc));
     for (int k0 = 0; k0 < B.nz; k0 += B.kchunk)
       for (int j0 = 0; j0 < B.ny; j0 += B.th)
         for (int i0 = 0; i0 < B.nx; i0 += B.tw) {
@@ -496,6 +525,21 @@ int build_plans(pgb_case *c) {
 
 int grid_for(long long n, int threads) { return (int)std::max<long long>(1, (n + threads - 1) / threads); }
 
+enum { K_HALO = 0, K_FUSED = 1, K_BLOCK = 2, K_COMBINE = 3 };
+
+// after every launch: count it, and under pgb_step_timed record an event
+void mark(pgb_case *c, int kind, int &count) {
+  count++;
+  if (!c->timing) return;
+  if (c->tnext >= c->tev.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->tev.push_back(e);
+  }
+  cudaEventRecord(c->tev[c->tnext++], c->stream);
+  c->tkind.push_back(kind);
+}
+
 // one stage of the fused path
 int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &count) {
   FusedArgs a{};
@@ -509,18 +553,43 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
   a.ncomb = p.ncomb;
   a.comb[0] = p.comb[0];
   a.comb[1] = p.comb[1];
+  // the registers the combines read, as slots the uniform kernel fills ahead
+  a.npre = 0;
+  for (int m = 0; m < p.ncomb; m++) {
+    a.combp[m] = p.comb[m];
+    for (int n = 0; n < p.comb[m].nterms; n++) {
+      const int r = p.comb[m].src[n];
+      if (r < 0) continue;
+      int slot = -1;
+      for (int q = 0; q < a.npre; q++)
+        if (a.pre[q] == r) slot = q;
+      if (slot < 0) {
+        if (a.npre == 3) return fail(PGB_ERR_STATE, "a stage reads more than three registers");
+        slot = a.npre;
+        a.pre[a.npre++] = r;
+      }
+      a.combp[m].src[n] = slot;
+    }
+  }
   a.dt = c->d_dt;
   // the stencil register's halo first
   k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne);
-  count++;
+  mark(c, K_HALO, count);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  bool any_general = false;
-  for (auto &B : c->blocks) any_general = any_general || !B.dev.uniform;
+  const bool any_general = !c->use_v2;
   const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
-  const int grid = std::min(c->ntiles, sms * 2);
   const size_t sm = c->fused_smem;
+  if (c->use_v2) {
+    const int grid = std::min(c->ntiles, sms * c->v2_ctas);
+    if (visc) k_fused2<true><<<grid, F2_THREADS, sm, c->stream>>>(a);
+    else k_fused2<false><<<grid, F2_THREADS, sm, c->stream>>>(a);
+    mark(c, K_FUSED, count);
+    CK(cudaGetLastError());
+    return PGB_OK;
+  }
+  const int grid = std::min(c->ntiles, sms * 2);
   if (visc) {
     if (any_general) k_fused1<true, false><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
     else k_fused1<true, true><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
@@ -528,13 +597,22 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
     if (any_general) k_fused1<false, false><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
     else k_fused1<false, true><<<grid, FUSED_THREADS, sm, c->stream>>>(a);
   }
-  count++;
+  mark(c, K_FUSED, count);
   CK(cudaGetLastError());
   return PGB_OK;
 }
 
 int fused_attrs(pgb_case *c) {
   const int sm = (int)c->fused_smem;
+  CK(cudaFuncSetAttribute(k_fused2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_fused2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  if (c->use_v2) {
+    int n = 1;
+    const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, visc ? (const void *)k_fused2<true> : (const void *)k_fused2<false>,
+                                                     F2_THREADS, c->fused_smem));
+    c->v2_ctas = std::max(1, n);
+  }
   CK(cudaFuncSetAttribute(k_fused1<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_fused1<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_fused1<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -577,21 +655,22 @@ int rhs_plain_ns(pgb_case *c, int qphys, int dqphys, int &count) {
   const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
   constexpr int NE = 4 + NS;
   k_halo<<<grid_for(c->nhalo, TH), TH, 0, s>>>(Q, c->d_halo, c->nhalo, NE);
-  count++;
+  mark(c, K_HALO, count);
   for (int b = 0; b < (int)c->blocks.size(); b++) {
     const BlockDev &D = c->blocks[b].dev;
     const long long inner = (long long)D.nx * D.ny * D.nz;
     k_fromQ<NS><<<grid_for(D.vol, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state);
-    count++;
+    mark(c, K_BLOCK, count);
     if (visc) {
       k_transport<NS><<<grid_for(D.vol, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp);
+      mark(c, K_BLOCK, count);
       k_grads<NS><<<grid_for(inner, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_grads);
-      count += 2;
+      mark(c, K_BLOCK, count);
     }
   }
   if (visc) {
     k_halo<<<grid_for(c->nhalo_l0, TH), TH, 0, s>>>(c->d_grads, c->d_halo, c->nhalo_l0, 3 * (NE - 1));
-    count++;
+    mark(c, K_HALO, count);
   }
   for (int b = 0; b < (int)c->blocks.size(); b++) {
     const BlockDev &D = c->blocks[b].dev;
@@ -599,17 +678,21 @@ int rhs_plain_ns(pgb_case *c, int qphys, int dqphys, int &count) {
     const long long fx = (long long)(D.nx + 1) * D.ny * D.nz, fy = (long long)D.nx * (D.ny + 1) * D.nz,
                     fz = (long long)D.nx * D.ny * (D.nz + 1);
     k_advflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[0]);
+    mark(c, K_BLOCK, count);
     k_advflux<NS, 1><<<grid_for(fy, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[1]);
+    mark(c, K_BLOCK, count);
     k_advflux<NS, 2><<<grid_for(fz, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[2]);
-    count += 3;
+    mark(c, K_BLOCK, count);
     if (visc) {
       k_diffflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[0]);
+      mark(c, K_BLOCK, count);
       k_diffflux<NS, 1><<<grid_for(fy, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[1]);
+      mark(c, K_BLOCK, count);
       k_diffflux<NS, 2><<<grid_for(fz, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[2]);
-      count += 3;
+      mark(c, K_BLOCK, count);
     }
     k_applyflux<NS><<<grid_for(inner, TH), TH, 0, s>>>(c->d_blks, b, c->d_F[0], c->d_F[1], c->d_F[2], c->d_met, dQ);
-    count++;
+    mark(c, K_BLOCK, count);
   }
   CK(cudaGetLastError());
   return PGB_OK;
@@ -646,7 +729,7 @@ int step_plain(pgb_case *c, int &count) {
       for (int b = 0; b < (int)c->blocks.size(); b++) {
         const BlockDev &D = c->blocks[b].dev;
         k_combine<<<grid_for((long long)D.nx * D.ny * D.nz, TH), TH, 0, c->stream>>>(c->d_blks, b, c->ne, cd, c->d_dt);
-        count++;
+        mark(c, K_COMBINE, count);
       }
     }
   }
@@ -657,7 +740,13 @@ int step_plain(pgb_case *c, int &count) {
 int prepare(pgb_case *c, bool fused) {
   if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
   RET(set_current(c));
-  if (!c->uniform_done) RET(detect_uniform(c, fused));
+  if (!c->uniform_done) {
+    RET(detect_uniform(c, fused));
+    bool all = true;
+    for (auto &B : c->blocks) all = all && B.dev.uniform;
+    if (all != c->use_v2) c->tiles_dirty = true;
+    c->use_v2 = all;
+  }
   if (fused) {
     if (c->tiles_dirty) RET(build_tiles(c));
     RET(fused_attrs(c));
@@ -728,7 +817,8 @@ int pgb_case_destroy(pgb_case *c) {
   for (auto &r : c->d_reg)
     if (r) cudaFree(r);
   void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
-                  c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter};
+                  c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage};
+  for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1013,6 +1103,105 @@ int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph) {
   return PGB_OK;
 }
 
+int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int *kind, int cap, int *n) {
+  if (!c || !n || (cap > 0 && (!ms || !kind))) return fail(PGB_ERR_ARG, "null argument");
+  if (path != PGB_PATH_BATCHED && path != PGB_PATH_PER_BLOCK) return fail(PGB_ERR_ARG, "no such path");
+  const bool fused = path == PGB_PATH_BATCHED;
+  if (fused && !fused_capable(c)) return fail(PGB_ERR_UNSUPPORTED, "the batched path does not take this case");
+  RET(prepare(c, fused));
+  if (!fused) RET(ensure_scratch(c));
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
+  CK(cudaGetLastError());
+  c->timing = true;
+  c->tnext = 0;
+  c->tkind.clear();
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = PGB_OK;
+  for (int s = 0; s < nsteps && rc == PGB_OK; s++) {
+    int count = 0;
+    rc = fused ? step_fused(c, count) : step_plain(c, count);
+    c->launches[path] = count;
+  }
+  c->timing = false;
+  if (rc != PGB_OK) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  const int total = (int)c->tnext;
+  *n = total;
+  for (int q = 0; q < total && q < cap; q++) {
+    // a launch's time: from the event before it (the previous launch's, or
+    // the start) to its own; the memset nodes between steps fall in the first
+    // launch of each step
+    cudaEvent_t before = q == 0 ? c->ev0 : c->tev[q - 1];
+    CK(cudaEventElapsedTime(&ms[q], before, c->tev[q]));
+    kind[q] = c->tkind[q];
+  }
+  return PGB_OK;
+}
+
+int pgb_state_set(pgb_case *c, int reg, const double *host, long count) {
+  if (!c || !host) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  long long inner = 0;
+  for (auto &B : c->blocks) inner += (long long)B.nx * B.ny * B.nz;
+  if (count != inner * c->ne) return fail(PGB_ERR_ARG, "host state of the wrong size");
+  if (count > c->stage_cap) {
+    if (c->d_stage) cudaFree(c->d_stage);
+    c->d_stage = nullptr;
+    CK(cudaMalloc(&c->d_stage, sizeof(double) * count));
+    c->stage_cap = count;
+  }
+  CK(cudaMemcpyAsync(c->d_stage, host, sizeof(double) * count, cudaMemcpyHostToDevice, c->stream));
+  long long at = 0;
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const BlockDev &D = c->blocks[b].dev;
+    const long long n = (long long)D.nx * D.ny * D.nz;
+    k_unpack<<<grid_for(n, 256), 256, 0, c->stream>>>(c->d_blks, b, c->ne, c->d_stage + at, c->d_reg[c->phys_of[reg]]);
+    at += n * c->ne;
+  }
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int pgb_state_get(pgb_case *c, int reg, double *host, long count) {
+  if (!c || !host) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  long long inner = 0;
+  for (auto &B : c->blocks) inner += (long long)B.nx * B.ny * B.nz;
+  if (count != inner * c->ne) return fail(PGB_ERR_ARG, "host state of the wrong size");
+  if (count > c->stage_cap) {
+    if (c->d_stage) cudaFree(c->d_stage);
+    c->d_stage = nullptr;
+    CK(cudaMalloc(&c->d_stage, sizeof(double) * count));
+    c->stage_cap = count;
+  }
+  long long at = 0;
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const BlockDev &D = c->blocks[b].dev;
+    const long long n = (long long)D.nx * D.ny * D.nz;
+    k_pack<<<grid_for(n, 256), 256, 0, c->stream>>>(c->d_blks, b, c->ne, c->d_reg[c->phys_of[reg]], c->d_stage + at);
+    at += n * c->ne;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, c->d_stage, sizeof(double) * count, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_host_register(void *host, size_t bytes) {
+  if (!host || !bytes) return fail(PGB_ERR_ARG, "null argument");
+  CK(cudaHostRegister(host, bytes, cudaHostRegisterDefault));
+  return PGB_OK;
+}
+
+int pgb_host_unregister(void *host) {
+  if (!host) return fail(PGB_ERR_ARG, "null argument");
+  CK(cudaHostUnregister(host));
+  return PGB_OK;
+}
+
 int pgb_case_stream(const pgb_case *c, void **stream) {
   if (!c || !stream) return fail(PGB_ERR_ARG, "null argument");
   *stream = (void *)c->stream;
@@ -1034,7 +1223,9 @@ int pgb_launches_per_step(const pgb_case *c, int path, int *count) {
 
 int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk) {
   if (!c || blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
-  if (tw < 1 || th < 1 || tw * th > FUSED_THREADS || kchunk < 1) return fail(PGB_ERR_ARG, "bad tile");
+  if (tw < 1 || th < 1 || kchunk < 1) return fail(PGB_ERR_ARG, "bad tile");
+  if (!tile_fits(c, std::min(tw, c->blocks[blk].nx), std::min(th, c->blocks[blk].ny)))
+    return fail(PGB_ERR_ARG, "tile larger than the fused kernel takes");
   HostBlock &B = c->blocks[blk];
   B.tw = std::min(tw, B.nx), B.th = std::min(th, B.ny), B.kchunk = std::min(kchunk, B.nz);
   c->tiles_dirty = true;
@@ -1044,7 +1235,7 @@ int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk) {
 int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk) {
   if (!c || blk < 0 || blk >= (int)c->blocks.size() || !tw || !th || !kchunk) return fail(PGB_ERR_ARG, "bad argument");
   HostBlock B = c->blocks[blk];
-  if (B.tw <= 0) default_tile(B);
+  if (B.tw <= 0) c->use_v2 ? default_tile2(B) : default_tile(B);
   *tw = B.tw, *th = B.th, *kchunk = B.kchunk;
   return PGB_OK;
 }

@@ -60,7 +60,8 @@ class CubeMesher:
     name = "cube"
 
     def __init__(self, mbdims=(1, 1, 1), blkdims=None, cells=None, lengths=(1.0, 1.0, 1.0),
-                 origin=(0.0, 0.0, 0.0), periodic=(False, False, False), bcnames=None, defaultbc=None):
+                 origin=(0.0, 0.0, 0.0), periodic=(False, False, False), bcnames=None, defaultbc=None,
+                 jostle=0.0, jostle_seed=7):
         self.mbdims = [int(n) for n in mbdims]
         if cells is None:
             if blkdims is None:
@@ -75,6 +76,11 @@ class CubeMesher:
         self.periodic = [bool(p) for p in periodic]
         self.bcnames = dict(bcnames or {})
         self.defaultbc = defaultbc
+        # moves every node inside a block (not its faces) by up to jostle
+        # spacings, so no face normal is an axis (the reference's test
+        # JostledCube, tests/simulator/support.py:48-56)
+        self.jostle = float(jostle)
+        self.jostle_seed = jostle_seed
         # where each block of the lattice starts, in cells and in space
         self.starts = [np.concatenate([[0], np.cumsum(c)]) for c in self.cells]
 
@@ -106,6 +112,12 @@ class CubeMesher:
             axes.append(np.linspace(lo, hi, self.cells[a][m] + 1))
         grid = np.meshgrid(*axes, indexing="ij")
         blk.nodes[blk.interior] = np.stack(grid, axis=-1)
+        if self.jostle:
+            g = blk.ng
+            inner = np.s_[g + 1:-g - 1, g + 1:-g - 1, g + 1:-g - 1]
+            spacing = min(self.lengths[a] / self.starts[a][-1] for a in range(3))
+            rng = np.random.default_rng(self.jostle_seed + blk.nblki)
+            blk.nodes[inner] += rng.uniform(-1, 1, blk.nodes[inner].shape) * self.jostle * spacing
 
     def _connect(self, blk, nblki, ijk):
         for axis, (n, index, wraps) in enumerate(zip(self.mbdims, ijk, self.periodic)):

@@ -102,6 +102,12 @@ SIGNATURES = {
     "pgb_launches_per_step": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_set_tile": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_get_tile": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_state_set": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_state_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_host_register": ([ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    "pgb_host_unregister": ([ctypes.c_void_p], ctypes.c_int),
+    "pgb_step_timed": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                        ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_block_uniform": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
 }
 

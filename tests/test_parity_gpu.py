@@ -31,7 +31,7 @@ def build(simulator="navier-stokes", integrator="rk4", cells=16, blocks=(2, 2, 1
     from oracle.oracle import Oracle
 
     cfg = cases.tgv_config(simulator, integrator, launch)
-    mesh = cases.tgv_mesh(cells, blocks, seed=seed, low=low, high=high)
+    mesh = cases.tgv_mesh(cells, blocks, seed=seed, low=low, high=high, jostle=0.15 if jostle else 0.0)
     mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
     prims = cases.tgv_prims(mb.mesh_blocks, mb.metrics, seed=seed, noise=1e-3)
     mb.set_prims(prims)
@@ -44,9 +44,10 @@ def interiors(mb, arrays):
     return [a[b.interior] for a, b in zip(arrays, mb.mesh_blocks)]
 
 
+@pytest.mark.parametrize("jostle", [False, True])
 @pytest.mark.parametrize("simulator", ["euler", "navier-stokes"])
-def test_rhs_matches_oracle(simulator):
-    mb, orc = build(simulator, cells=16, blocks=(2, 2, 1))
+def test_rhs_matches_oracle(simulator, jostle):
+    mb, orc = build(simulator, cells=16, blocks=(2, 2, 1), jostle=jostle)
     dq = mb.regs[-1]
     mb.rhs(Q="Q", dQ=dq)
     got = [getattr(b, dq).get() for b in mb.blocks]
@@ -56,10 +57,12 @@ def test_rhs_matches_oracle(simulator):
         assert rowmax_err(g, w) < RHS_TOL
 
 
+@pytest.mark.parametrize("jostle", [False, True])
 @pytest.mark.parametrize("launch", ["batched", "per-block"])
-@pytest.mark.parametrize("integrator", ["rk4", "tvd-rk3"])
-def test_steps_match_oracle(launch, integrator):
-    mb, orc = build("navier-stokes", integrator, cells=16, blocks=(2, 1, 2), launch=launch, low=5, high=11)
+@pytest.mark.parametrize("integrator", ["rk4", "tvd-rk3", "rk1", "rk34"])
+def test_steps_match_oracle(launch, integrator, jostle):
+    mb, orc = build("navier-stokes", integrator, cells=16, blocks=(2, 1, 2), launch=launch, low=5, high=11,
+                    jostle=jostle)
     _, g = cases.tgv_gas()
     dt = 0.2 * (2 * np.pi / 16) / (g["U0"] + np.sqrt(g["gamma"] * g["R"] * cases.T0))
     for _ in range(3):
@@ -97,10 +100,22 @@ def test_mass_is_conserved():
     assert abs(after[4] - before[4]) <= 1e-13 * abs(before[4])
 
 
-def test_uniform_blocks_are_detected():
-    mb, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 1, 1))
+@pytest.mark.parametrize("jostle", [False, True])
+def test_uniform_blocks_are_detected(jostle):
+    mb, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 1, 1), jostle=jostle)
     mb.step(1e-6)
-    assert all(mb.uniform(n) for n in range(len(mb.blocks)))
+    assert all(mb.uniform(n) != jostle for n in range(len(mb.blocks)))
+
+
+@pytest.mark.parametrize("simulator", ["euler", "navier-stokes"])
+def test_batched_euler_and_ns_on_both_kernels(simulator):
+    for jostle in (False, True):
+        mb, orc = build(simulator, "rk4", cells=12, blocks=(2, 2, 2), jostle=jostle)
+        mb.step(2e-5, 2)
+        orc.step(2e-5)
+        orc.step(2e-5)
+        for b, w in zip(mb.blocks, orc.regs[0]):
+            assert rowmax_err(b.Q.get()[b.mesh.interior], w[b.mesh.interior]) < STATE_TOL
 
 
 def test_unsupported_physics_is_refused():
