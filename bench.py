@@ -240,6 +240,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-extra", action="store_true", help="skip the per-block and end-to-end legs")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape and tiles")
+    ap.add_argument("--shape", default=None, help="force the fused kernel's THREADSxMINBLOCKS (no tuning)")
+    ap.add_argument("--ksplit", type=int, default=3, help="k runs per block with --shape")
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
     args = ap.parse_args()
     set_cells(args.cells)
@@ -264,6 +267,15 @@ def main():
     mb, mesh, prims = build_case("batched", device=local)
     dt = stable_dt()
     ncells = mb.ncells
+    mb.step(dt, 1)
+    # the launch shape and tiles, picked by timing them on this case
+    from peregrine_b200 import autotune
+
+    if args.shape:
+        threads, minb = (int(x) for x in args.shape.split("x"))
+        tuned = autotune.tune(mb, dt, shapes=((threads, minb),), ksplits=(args.ksplit,))
+    else:
+        tuned = None if args.no_tune else autotune.tune(mb, dt)
     # warm-up (the first call captures the graph)
     mb.step(dt, args.warmup)
     mb.backend.sync()
@@ -338,7 +350,8 @@ def main():
             "config": {"workload": WORKLOAD, "cells": ncells, "blocks": len(mb.blocks), "stages_per_step": STAGES,
                        "parallelism": "replicas" if world > 1 else "single-gpu",
                        "l2": "inputs larger than L2 (four registers of 2.4M cells x 5 doubles, 0.38 GB)",
-                       "path": "batched fused persistent kernel, CUDA graph per RK4 step"},
+                       "path": "batched fused persistent kernel, CUDA graph per RK4 step",
+                       "tuned": tuned},
             "per_block": per_block,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,

@@ -174,9 +174,14 @@ int pgb_last_step_ms(const pgb_case *c, float *ms);
 int pgb_launches_per_step(const pgb_case *c, int path, int *count);
 
 /* the tile shape the batched kernel uses for blk (set by the autotuner or the
- * caller) */
+ * caller); tw = th = 0 goes back to the kernel's default.  A tile the case's
+ * kernel cannot take is replaced by the default when the work list is built. */
 int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk);
 int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk);
+
+/* the uniform-metric fused kernel's threads per CTA and the CTAs per SM its
+ * registers are bounded for: 256 x 1, 256 x 2, 128 x 2, 128 x 3 or 128 x 4 */
+int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks);
 
 /* whether blk runs in the uniform-metric form (1) or reads its metric arrays (0) */
 int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);

@@ -254,6 +254,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 2) k_fused1(const FusedArgs a) 
     grad_plane(k0);
     __syncthreads();
     if (mine) kface(k0 - 1, Fk);
+    // the first load of the loop takes plane k0-1's slot, which that k face read
+    __syncthreads();
 
     for (int k = k0; k < k1; k++) {
       load_plane(k + 2);

@@ -150,8 +150,22 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <bool VISC>
-__global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
+// Shared memory of the uniform kernel with NT threads on a tw x th tile:
+// P[2][P_N][N2] two planes of cell values, G[12][NT] one plane of gradients,
+// Fi[5][NT], Fj[5][NT] low-face fluxes, raw[5][NT + NR] the Q copies in
+// flight (NR the ring's second cells), pre[2][5][NT] the combines' registers.
+template <int NT>
+struct F2Layout {
+  int N2, NR;
+  double *P, *G, *Fi, *Fj, *raw, *pre;
+  __host__ __device__ static size_t doubles(int tw, int th, bool visc) {
+    const int N2 = (tw + 4) * (th + 4), NR = 2 * (tw + th);
+    return (size_t)2 * P_N * N2 + (visc ? 12 * NT : 0) + 10 * NT + 5 * (NT + NR) + 2 * 5 * NT;
+  }
+};
+
+template <bool VISC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
   extern __shared__ double smem[];
   __shared__ int s_tile;
   const int tid = threadIdx.x;
@@ -166,27 +180,23 @@ __global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
     const int tw = T.tw, th = T.th;
     const int W1 = tw + 2, H1 = th + 2, N1 = W1 * H1;
     const int W2 = tw + 4, N2 = W2 * (th + 4);
-    // shared: P[3][P_N][N2] cell values of three planes; G[12][256]
-    // gradients of one plane; Fi[5][256], Fj[5][256] low-face fluxes;
-    // raw[2 slots][2 cells][5][256] the Q loads in flight; pre[2][3][5][256]
-    // the combines' registers for the next plane
+    const int nring = 2 * (tw + th);
     double *P = smem;
-    double *G = P + 3 * P_N * N2;
-    double *Fi = G + (VISC ? 12 * F2_THREADS : 0);
-    double *Fj = Fi + 5 * F2_THREADS;
-    double *raw = Fj + 5 * F2_THREADS;
-    double *pre = raw + 2 * 2 * 5 * F2_THREADS;
+    double *G = P + 2 * P_N * N2;
+    double *Fi = G + (VISC ? 12 * NT : 0);
+    double *Fj = Fi + 5 * NT;
+    double *raw = Fj + 5 * NT;           // [5][NT] own cells, then [5][nring] ring cells
+    double *raw2 = raw + 5 * NT;
+    double *pre = raw2 + 5 * nring;      // [2][5][NT]
     const int v = (int)B.vol;
     const int sJ = B.X, sK = B.X * B.Y;
     const double *Q = a.R[a.qin] + 5 * B.cv;
-    // this thread's column in R1 coordinates (ring included), and in R2
     const bool col = tid < N1;
     const int ii = tid % W1, jj = tid / W1;
     const int c2 = (ii + 1) + W2 * (jj + 1);
     const bool tile = col && ii >= 1 && ii <= tw && jj >= 1 && jj <= th;
     const bool ring_corner = (ii == 0 || ii == W1 - 1) && (jj == 0 || jj == H1 - 1);
-    // the second cell a thread loads: the outer ring of R2 less its corners
-    const int nring = 2 * (tw + th);
+    const bool gcol = col && !ring_corner;
     int r2 = -1, x2 = 0, y2 = 0;
     if (tid < nring) {
       int q = tid;
@@ -196,10 +206,9 @@ __global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
       else x2 = (q - tw) + 2, y2 = th + 3;
       r2 = x2 + W2 * y2;
     }
-    // in-plane offsets of the two cells in the block's arrays
     const int o1 = (T.j0 + jj + 1) * sJ + (T.i0 + ii + 1);
     const int o2 = (T.j0 + y2) * sJ + (T.i0 + x2);
-    auto slot = [](int p) { return (p + 3) % 3; };
+    auto slot = [](int p) { return p & 1; };
     auto getP = [&](int s, int r) {
       const double *Ps = P + s * P_N * N2;
       CellP c;
@@ -212,134 +221,135 @@ __global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
       Ps[P_RHO * N2 + r] = c.rho, Ps[P_U * N2 + r] = c.u, Ps[P_V * N2 + r] = c.v;
       Ps[P_W * N2 + r] = c.w, Ps[P_T * N2 + r] = c.T, Ps[P_E * N2 + r] = c.e;
     };
-    auto rawp = [&](int p, int which, int l) { return raw + (((p & 1) * 2 + which) * 5 + l) * F2_THREADS + tid; };
-    // the copies of plane p's Q for this thread's cells
+    // the copies of plane p's Q for this thread's cells (one group in flight)
     auto fetch = [&](int p) {
       const int z = (p + NG) * sK;
       if (col) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(rawp(p, 0, l), Q + l * v + z + o1);
+        for (int l = 0; l < 5; l++) cp8(raw + l * NT + tid, Q + l * v + z + o1);
       }
       if (r2 >= 0) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(rawp(p, 1, l), Q + l * v + z + o2);
+        for (int l = 0; l < 5; l++) cp8(raw2 + l * nring + tid, Q + l * v + z + o2);
       }
     };
-    // the copies of the combines' registers at plane p for a tile cell
     auto fetch_pre = [&](int p) {
       if (!tile) return;
       const long long base = 5 * B.cv + (p + NG) * sK + o1;
       for (int m = 0; m < a.npre; m++) {
         const double *R = a.R[a.pre[m]] + base;
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(pre + (((p & 1) * 3 + m) * 5 + l) * F2_THREADS + tid, R + l * v);
+        for (int l = 0; l < 5; l++) cp8(pre + (m * 5 + l) * NT + tid, R + l * v);
       }
     };
-    auto cellof = [&](int p, int which) {
-      return prim_of(*rawp(p, which, 0), *rawp(p, which, 1), *rawp(p, which, 2), *rawp(p, which, 3), *rawp(p, which, 4));
+    auto own_raw = [&]() {
+      return prim_of(raw[0 * NT + tid], raw[1 * NT + tid], raw[2 * NT + tid], raw[3 * NT + tid], raw[4 * NT + tid]);
     };
-    auto store = [&](int p) {
-      if (col) putP(slot(p), c2, cellof(p, 0));
-      if (r2 >= 0) putP(slot(p), r2, cellof(p, 1));
-    };
-    auto grad_own = [&](int p, double *g) {
-      const int sm = slot(p - 1), s0 = slot(p), sp = slot(p + 1);
-      grad_u(B, getP(s0, c2 - 1), getP(s0, c2 + 1), getP(s0, c2 - W2), getP(s0, c2 + W2), getP(sm, c2), getP(sp, c2), g);
+    auto ring_raw = [&]() {
+      return prim_of(raw2[0 * nring + tid], raw2[1 * nring + tid], raw2[2 * nring + tid], raw2[3 * nring + tid],
+                     raw2[4 * nring + tid]);
     };
     auto putG = [&](const double *g) {
 #pragma unroll
-      for (int q = 0; q < 12; q++) G[q * F2_THREADS + tid] = g[q];
+      for (int q = 0; q < 12; q++) G[q * NT + tid] = g[q];
+    };
+    // gradients of this column at a plane whose neighbours are in slot s,
+    // with the column's own cells below and above given
+    auto grad_col = [&](int s, const CellP &below, const CellP &above, double *g) {
+      grad_u(B, getP(s, c2 - 1), getP(s, c2 + 1), getP(s, c2 - W2), getP(s, c2 + W2), below, above, g);
     };
 
     const int k0 = T.k0, k1 = T.k1;
-    // prelude: planes k0-1 .. k0+1 in shared, the gradients of k0 in shared
-    // and of k0-1 in registers, the k face below k0; plane k0+2 and the
-    // combines' registers of plane k0 in flight
+    // prelude: planes k0 and k0+1 in shared, the gradients of k0 in shared,
+    // the k face below k0 in registers; plane k0+2 and plane k0's combine
+    // registers in flight
+    CellP pm2{}, pm1{}, p0{}, p1{};
     fetch(k0 - 2);
     cp_commit();
     cp_wait<0>();
-    const CellP below2 = col ? cellof(k0 - 2, 0) : CellP{};
-    for (int p = k0 - 1; p <= k0 + 1; p++) {
-      fetch(p);
-      cp_commit();
-      cp_wait<0>();
-      store(p);
-    }
+    if (col) pm2 = own_raw();
+    fetch(k0 - 1);
+    cp_commit();
+    cp_wait<0>();
+    if (col) putP(slot(k0 - 1), c2, pm1 = own_raw());
+    if (r2 >= 0) putP(slot(k0 - 1), r2, ring_raw());
+    fetch(k0);
+    cp_commit();
+    cp_wait<0>();
+    if (col) putP(slot(k0), c2, p0 = own_raw());
+    if (r2 >= 0) putP(slot(k0), r2, ring_raw());
+    fetch(k0 + 1);
+    cp_commit();
+    __syncthreads();
+    double gbelow[12];
+    if (VISC && tile) grad_col(slot(k0 - 1), pm2, p0, gbelow);
+    cp_wait<0>();
+    __syncthreads();
+    if (col) putP(slot(k0 + 1), c2, p1 = own_raw());
+    if (r2 >= 0) putP(slot(k0 + 1), r2, ring_raw());
     fetch(k0 + 2);
     fetch_pre(k0);
     cp_commit();
     __syncthreads();
-    double gbelow[12];
-    if constexpr (VISC) {
-      if (tile) {
-        const int s0 = slot(k0 - 1), sp = slot(k0);
-        grad_u(B, getP(s0, c2 - 1), getP(s0, c2 + 1), getP(s0, c2 - W2), getP(s0, c2 + W2), below2, getP(sp, c2),
-               gbelow);
+    double Fk[5];
+    {
+      double g0[12];
+      if (VISC && gcol) {
+        grad_col(slot(k0), pm1, p1, g0);
+        putG(g0);
       }
-      double g[12];
-      if (col && !ring_corner) {
-        grad_own(k0, g);
-        putG(g);
-      }
+      if (tile) face_u<2, VISC>(B, pm1, p0, gbelow, g0, Fk);
     }
     __syncthreads();
-    double Fk[5];
-    if (tile) {
-      double gk0[12];
-#pragma unroll
-      for (int q = 0; q < 12; q++) gk0[q] = VISC ? G[q * F2_THREADS + tid] : 0.0;
-      face_u<2, VISC>(B, getP(slot(k0 - 1), c2), getP(slot(k0), c2), gbelow, gk0, Fk);
-    }
     const double dt = *a.dt;
 
     for (int k = k0; k < k1; k++) {
-      const int s0 = slot(k);
+      const int s0 = slot(k), s1 = slot(k + 1);
       // 1. this column's low i and j faces at plane k
       if (col && jj >= 1 && jj <= th && ii >= 1) {
         double F[5], gl[12], gr[12];
         if (VISC) {
 #pragma unroll
-          for (int q = 0; q < 12; q++) gl[q] = G[q * F2_THREADS + tid - 1], gr[q] = G[q * F2_THREADS + tid];
+          for (int q = 0; q < 12; q++) gl[q] = G[q * NT + tid - 1], gr[q] = G[q * NT + tid];
         }
         face_u<0, VISC>(B, getP(s0, c2 - 1), getP(s0, c2), gl, gr, F);
 #pragma unroll
-        for (int l = 0; l < 5; l++) Fi[l * F2_THREADS + tid] = F[l];
+        for (int l = 0; l < 5; l++) Fi[l * NT + tid] = F[l];
       }
       if (col && ii >= 1 && ii <= tw && jj >= 1) {
         double F[5], gl[12], gr[12];
         if (VISC) {
 #pragma unroll
-          for (int q = 0; q < 12; q++) gl[q] = G[q * F2_THREADS + tid - W1], gr[q] = G[q * F2_THREADS + tid];
+          for (int q = 0; q < 12; q++) gl[q] = G[q * NT + tid - W1], gr[q] = G[q * NT + tid];
         }
         face_u<1, VISC>(B, getP(s0, c2 - W2), getP(s0, c2), gl, gr, F);
 #pragma unroll
-        for (int l = 0; l < 5; l++) Fj[l * F2_THREADS + tid] = F[l];
+        for (int l = 0; l < 5; l++) Fj[l * NT + tid] = F[l];
       }
-      // 2. the next copies go out; plane k+2 and plane k's combine
-      //    registers have landed; plane k+2 into shared
-      if (k + 3 <= k1 + 1) fetch(k + 3);
-      if (k + 1 < k1) fetch_pre(k + 1);
-      cp_commit();
-      cp_wait<1>();
-      store(k + 2);
+      // 2. plane k+2 and plane k's combine registers have landed
+      cp_wait<0>();
+      CellP p2{}, p2r{};
+      if (col) p2 = own_raw();
+      if (r2 >= 0) p2r = ring_raw();
       __syncthreads();
-      // 3. the gradients of plane k+1 for this column, the k face above k
+      // 3. the next copies go out
+      if (k + 3 <= k1 + 1) fetch(k + 3);
+      // 4. the gradients of plane k+1, the k face above k, dQ and the combines
+      const CellP pk = col ? getP(s0, c2) : CellP{};
+      const CellP pk1 = col ? getP(s1, c2) : CellP{};
       double gup[12];
-      if (VISC && col && !ring_corner) grad_own(k + 1, gup);
+      if (VISC && gcol) grad_col(s1, pk, p2, gup);
       if (tile) {
         double Fkh[5], gk[12];
 #pragma unroll
-        for (int q = 0; q < 12; q++) gk[q] = VISC ? G[q * F2_THREADS + tid] : 0.0;
-        face_u<2, VISC>(B, getP(s0, c2), getP(slot(k + 1), c2), gk, gup, Fkh);
-        // 4. dQ and the combines for the cell at plane k
+        for (int q = 0; q < 12; q++) gk[q] = VISC ? G[q * NT + tid] : 0.0;
+        face_u<2, VISC>(B, pk, pk1, gk, gup, Fkh);
         const double dJ = B.detJinv;
         double dQ[5];
 #pragma unroll
         for (int l = 0; l < 5; l++)
-          dQ[l] = (Fi[l * F2_THREADS + tid] + Fj[l * F2_THREADS + tid] + Fk[l] - Fi[l * F2_THREADS + tid + 1] -
-                   Fj[l * F2_THREADS + tid + W1] - Fkh[l]) * dJ;
+          dQ[l] = (Fi[l * NT + tid] + Fj[l * NT + tid] + Fk[l] - Fi[l * NT + tid + 1] - Fj[l * NT + tid + W1] - Fkh[l]) * dJ;
         const long long base = 5 * B.cv + (k + NG) * sK + o1;
-        const double *pk = pre + ((k & 1) * 3) * 5 * F2_THREADS + tid;
         double first[5];
 #pragma unroll
         for (int m = 0; m < 2; m++) {
@@ -350,7 +360,7 @@ __global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
           for (int l = 0; l < 5; l++) {
             auto val = [&](int n) {
               const int s = cb.src[n];
-              return s == -1 ? dQ[l] : s == -2 ? first[l] : pk[(s * 5 + l) * F2_THREADS];
+              return s == -1 ? dQ[l] : s == -2 ? first[l] : pre[(s * 5 + l) * NT + tid];
             };
             auto term = [&](int n) { return (cb.step && n == cb.nterms - 1) ? cb.w[n] * dt * val(n) : cb.w[n] * val(n); };
             double acc = term(0);
@@ -364,19 +374,21 @@ __global__ void __launch_bounds__(F2_THREADS, 1) k_fused2(const FusedArgs a) {
 #pragma unroll
         for (int l = 0; l < 5; l++) Fk[l] = Fkh[l];
       }
-      __syncthreads();
-      // 5. the plane k+1 gradients replace plane k's
-      if (VISC && col && !ring_corner) putG(gup);
+      if (k + 1 < k1) fetch_pre(k + 1);
+      cp_commit();
+      // 5. plane k+2 takes plane k's slot, the k+1 gradients plane k's
+      if (col) putP(s0, c2, p2);
+      if (r2 >= 0) putP(s0, r2, p2r);
+      if (VISC && gcol) putG(gup);
       __syncthreads();
     }
     cp_wait<0>();
   }
 }
 
+template <int NT>
 inline size_t fused2_smem(int tw, int th, bool visc) {
-  const int N2 = (tw + 4) * (th + 4);
-  return sizeof(double) * (size_t)(3 * P_N * N2 + (visc ? 12 : 0) * F2_THREADS + 10 * F2_THREADS +
-                                   2 * 2 * 5 * F2_THREADS + 2 * 3 * 5 * F2_THREADS);
+  return sizeof(double) * F2Layout<NT>::doubles(tw, th, visc);
 }
 
 }  // namespace pgb

@@ -92,6 +92,7 @@ struct pgb_case {
   bool uniform_done = false;
   bool use_v2 = false;  // every block uniform: the uniform-metric fused kernel
   int v2_ctas = 1;      // its resident CTAs per SM
+  int v2_nt = 256, v2_minb = 2;  // its threads per CTA and launch-bound CTAs per SM
   // register mapping: logical -> physical
   std::vector<int> phys_of, canonical;
   int period = 1, phase = 0;
@@ -285,10 +286,11 @@ void default_tile(HostBlock &B) {
 
 // the uniform kernel's default: one thread per column of the tile and its
 // ring, 256 of them; i cut evenly in pieces of at most 30
-void default_tile2(HostBlock &B) {
-  const int pi = (B.nx + 29) / 30;
+void default_tile2(HostBlock &B, int nt) {
+  const int wmax = nt >= 256 ? 30 : 14;
+  const int pi = (B.nx + wmax - 1) / wmax;
   const int tw = (B.nx + pi - 1) / pi;
-  int th = std::max(1, F2_THREADS / (tw + 2) - 2);
+  int th = std::max(1, nt / (tw + 2) - 2);
   th = std::min(th, B.ny);
   const int pj = (B.ny + th - 1) / th;
   th = (B.ny + pj - 1) / pj;
@@ -297,7 +299,8 @@ void default_tile2(HostBlock &B) {
 }
 
 bool tile_fits(const pgb_case *c, int tw, int th) {
-  return c->use_v2 ? (tw + 2) * (th + 2) <= F2_THREADS && 2 * (tw + th) <= F2_THREADS : tw * th <= FUSED_THREADS;
+  if (!c->use_v2) return tw * th <= FUSED_THREADS;
+  return (tw + 2) * (th + 2) <= c->v2_nt && 2 * (tw + th) <= c->v2_nt;
 }
 
 int build_tiles(pgb_case *c) {
@@ -307,10 +310,12 @@ int build_tiles(pgb_case *c) {
   for (int b = 0; b < (int)c->blocks.size(); b++) {
     HostBlock &B = c->blocks[b];
     if (B.tw <= 0 || !tile_fits(c, B.tw, B.th)) {
-      if (c->use_v2) default_tile2(B);
+      if (c->use_v2) default_tile2(B, c->v2_nt);
       else default_tile(B);
     }
-    smem = std::max(smem, c->use_v2 ? fused2_smem(B.tw, B.th, visc) : fused_smem(B.tw, B.th, visc));
+    const size_t need = !c->use_v2 ? fused_smem(B.tw, B.th, visc)
+                        : c->v2_nt == 128 ? fused2_smem<128>(B.tw, B.th, visc) : fused2_smem<256>(B.tw, B.th, visc);
+    smem = std::max(smem, need);
     for (int k0 = 0; k0 < B.nz; k0 += B.kchunk)
       for (int j0 = 0; j0 < B.ny; j0 += B.th)
         for (int i0 = 0; i0 < B.nx; i0 += B.tw) {
@@ -540,6 +545,21 @@ void mark(pgb_case *c, int kind, int &count) {
   c->tkind.push_back(kind);
 }
 
+// the uniform kernel of the case's shape: threads per CTA and launch bound
+const void *v2_kernel(const pgb_case *c) {
+  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+#define PGB_V2(NT, MB)                                                                      \
+  if (c->v2_nt == NT && c->v2_minb == MB)                                                   \
+    return visc ? (const void *)k_fused2<true, NT, MB> : (const void *)k_fused2<false, NT, MB>;
+  PGB_V2(256, 1)
+  PGB_V2(256, 2)
+  PGB_V2(128, 2)
+  PGB_V2(128, 3)
+  PGB_V2(128, 4)
+#undef PGB_V2
+  return nullptr;
+}
+
 // one stage of the fused path
 int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &count) {
   FusedArgs a{};
@@ -582,11 +602,13 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
   const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
   const size_t sm = c->fused_smem;
   if (c->use_v2) {
+    if (a.npre > 2) return fail(PGB_ERR_STATE, "the uniform kernels stage at most two registers a stage reads");
     const int grid = std::min(c->ntiles, sms * c->v2_ctas);
-    if (visc) k_fused2<true><<<grid, F2_THREADS, sm, c->stream>>>(a);
-    else k_fused2<false><<<grid, F2_THREADS, sm, c->stream>>>(a);
+    const void *fn = v2_kernel(c);
+    if (!fn) return fail(PGB_ERR_ARG, "no uniform kernel of that shape");
+    void *args[] = {&a};
+    CK(cudaLaunchKernel(fn, dim3(grid), dim3(c->v2_nt), args, sm, c->stream));
     mark(c, K_FUSED, count);
-    CK(cudaGetLastError());
     return PGB_OK;
   }
   const int grid = std::min(c->ntiles, sms * 2);
@@ -604,14 +626,14 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
 
 int fused_attrs(pgb_case *c) {
   const int sm = (int)c->fused_smem;
-  CK(cudaFuncSetAttribute(k_fused2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CK(cudaFuncSetAttribute(k_fused2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   if (c->use_v2) {
+    const void *fn = v2_kernel(c);
+    if (!fn) return fail(PGB_ERR_ARG, "no uniform kernel of that shape");
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     int n = 1;
-    const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, visc ? (const void *)k_fused2<true> : (const void *)k_fused2<false>,
-                                                     F2_THREADS, c->fused_smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, c->v2_nt, c->fused_smem));
     c->v2_ctas = std::max(1, n);
+    return PGB_OK;
   }
   CK(cudaFuncSetAttribute(k_fused1<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_fused1<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -1223,20 +1245,49 @@ int pgb_launches_per_step(const pgb_case *c, int path, int *count) {
 
 int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk) {
   if (!c || blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
-  if (tw < 1 || th < 1 || kchunk < 1) return fail(PGB_ERR_ARG, "bad tile");
-  if (!tile_fits(c, std::min(tw, c->blocks[blk].nx), std::min(th, c->blocks[blk].ny)))
-    return fail(PGB_ERR_ARG, "tile larger than the fused kernel takes");
+  // a tile the fused kernel of the case cannot take is replaced by its
+  // default when the work list is built
   HostBlock &B = c->blocks[blk];
+  if (tw == 0 && th == 0) {
+    // back to the default tile of the case's kernel
+    B.tw = 0;
+    c->tiles_dirty = true;
+    for (auto &g : c->graph)
+      if (g) cudaGraphExecDestroy(g), g = nullptr;
+    return PGB_OK;
+  }
+  if (tw < 1 || th < 1 || kchunk < 1) return fail(PGB_ERR_ARG, "bad tile");
   B.tw = std::min(tw, B.nx), B.th = std::min(th, B.ny), B.kchunk = std::min(kchunk, B.nz);
   c->tiles_dirty = true;
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
   return PGB_OK;
 }
 
 int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk) {
   if (!c || blk < 0 || blk >= (int)c->blocks.size() || !tw || !th || !kchunk) return fail(PGB_ERR_ARG, "bad argument");
   HostBlock B = c->blocks[blk];
-  if (B.tw <= 0) c->use_v2 ? default_tile2(B) : default_tile(B);
+  if (B.tw <= 0) {
+    if (c->use_v2) default_tile2(B, c->v2_nt);
+    else default_tile(B);
+  }
   *tw = B.tw, *th = B.th, *kchunk = B.kchunk;
+  return PGB_OK;
+}
+
+int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  const int nt0 = c->v2_nt, mb0 = c->v2_minb;
+  c->v2_nt = threads, c->v2_minb = minblocks;
+  if (!v2_kernel(c)) {
+    c->v2_nt = nt0, c->v2_minb = mb0;
+    return fail(PGB_ERR_ARG, "threads x minblocks: 256 x 1, 256 x 2, 128 x 2, 128 x 3 or 128 x 4");
+  }
+  if (threads != nt0)
+    for (auto &B : c->blocks) B.tw = 0;
+  c->tiles_dirty = true;
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
   return PGB_OK;
 }
 

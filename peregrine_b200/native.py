@@ -108,6 +108,7 @@ SIGNATURES = {
     "pgb_host_unregister": ([ctypes.c_void_p], ctypes.c_int),
     "pgb_step_timed": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                         ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_set_fused_shape": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_block_uniform": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
 }
 

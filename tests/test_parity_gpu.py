@@ -69,8 +69,8 @@ def test_steps_match_oracle(launch, integrator, jostle):
         mb.step(dt)
         orc.step(dt)
     got = [b.Q.get() for b in mb.blocks]
-    for gq, w in zip(interiors(mb, got), interiors(mb, orc.regs[0])):
-        assert rowmax_err(gq, w) < STATE_TOL
+    errs = [rowmax_err(gq, w) for gq, w in zip(interiors(mb, got), interiors(mb, orc.regs[0]))]
+    assert max(errs) < STATE_TOL, errs
 
 
 def test_batched_equals_per_block():
