@@ -186,6 +186,34 @@ int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks);
 /* whether blk runs in the uniform-metric form (1) or reads its metric arrays (0) */
 int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);
 
+/* The right-hand side of one block without allocating device memory.  No
+ * counterpart in the reference, which always allocates its arrays through
+ * its backend.  For callers that may not call cudaMalloc or any allocating
+ * library routine (torch's allocator included): code living in another
+ * framework's memory pool or a fixed arena, or a host application that owns
+ * all device memory.  The caller passes device arrays, all F order with the
+ * case layout's halo of two cells (full extents nx+4, ny+4, nz+4, i fastest,
+ * components outermost):
+ *   Q    ne = 4 + ns components, its halo filled by the caller (two layers on
+ *        every face, the first layer of every edge);
+ *   met  31 components: xcc (3), detJinv (1), Jinv (9, row-major), iS, jS,
+ *        kS (3 each), ixc, jxc, kxc (3 each); a face of axis a is stored at
+ *        the index of the cell on its high side;
+ *   dQ   ne components; the interior is written, the halo left alone.
+ * tables: Rsp, cp0, h298R, MWinv, hpoly0, h298, mu0, kappa0, MWqinv, lewis
+ * (ns each), then wilkepair (ns x ns, row-major).  The work goes on stream (a
+ * cudaStream_t; NULL for the default stream) and is queued when the call
+ * returns.  The scratch is one static device array of 16 MiB that every GPU
+ * loading the library holds until exit; a block larger than
+ * pgb_rhs_block_noalloc_max_cells(ns) cells (halo included; 53,773 for one
+ * species, room for 32^3 interior cells) is refused with PGB_ERR_ARG.  The
+ * first call on a device looks up the array's device address, so make it
+ * before any stream capture.  Every call uses the same array: calls that
+ * overlap on the GPU race, so keep them ordered on one stream. */
+int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tables, int nx, int ny, int nz, const double *Q,
+                          const double *met, double *dQ, void *stream);
+long long pgb_rhs_block_noalloc_max_cells(int ns);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,8 +12,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = [os.path.join(HERE, "csrc", "pgb_host.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fused.cuh", "layout.cuh", "physics.cuh", "plain.cuh")] + \
+SOURCES = [os.path.join(HERE, "csrc", "pgb_host.cu"), os.path.join(HERE, "csrc", "pgb_noalloc.cu")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fused.cuh", "fused2.cuh", "layout.cuh", "physics.cuh", "plain.cuh")] + \
           [os.path.join(ROOT, "include", "pgb200.h")]
 TARGET = os.path.join(HERE, "libpgb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -42,7 +42,7 @@ int fail(int code, const std::string &msg) {
     if (r_ != PGB_OK) return r_; \
   } while (0)
 
-__global__ void k_setscalar(double *p, double v) { *p = v; }
+static __global__ void k_setscalar(double *p, double v) { *p = v; }
 
 struct HostBlock {
   int nx, ny, nz;
@@ -126,61 +126,21 @@ const double *table(const pgb_case *c, const char *name) {
   return it == c->tables.end() ? nullptr : it->second.data();
 }
 
-// the species tables into the constant struct, and the single-species
-// shortcuts by the same operations the per-cell formulas take for Y = 1
+// the case's named species tables into the constant struct
 int build_species(pgb_case *c) {
-  Species &s = c->sp;
   const int ns = c->phys.ns;
-  s.ns = ns;
-  s.alpha = c->phys.alpha;
-  s.Ru = 8314.46261815324;
-  struct T {
-    const char *name;
-    double *dst;
-    bool need;
-  } list[] = {{"Rsp", s.Rsp, true},        {"cp0", s.cp0, true},          {"h298R", s.h298R, true},
-              {"MWinv", s.MWinv, true},    {"hpoly0", s.hpoly0, false},   {"h298", s.h298, false},
-              {"mu0", s.mu0, false},       {"kappa0", s.kappa0, false},   {"MWqinv", s.MWqinv, false},
-              {"lewis", s.lewis, false}};
-  for (auto &t : list) {
-    const double *v = table(c, t.name);
-    if (!v) {
-      if (t.need) return fail(PGB_ERR_ARG, std::string("species table ") + t.name + " not set");
-      for (int n = 0; n < ns; n++) t.dst[n] = 1.0;
-      continue;
-    }
-    if ((long)c->tables[t.name].size() < ns) return fail(PGB_ERR_ARG, std::string("species table ") + t.name + " short");
-    for (int n = 0; n < ns; n++) t.dst[n] = v[n];
+  static const char *names[T_NTAB] = {"Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0", "kappa0", "MWqinv", "lewis"};
+  static const bool need[T_NTAB] = {true, true, true, true, false, false, false, false, false, false};
+  const double *tab[T_NTAB];
+  for (int q = 0; q < T_NTAB; q++) {
+    tab[q] = table(c, names[q]);
+    if (!tab[q] && need[q]) return fail(PGB_ERR_ARG, std::string("species table ") + names[q] + " not set");
+    if (tab[q] && (long)c->tables[names[q]].size() < ns)
+      return fail(PGB_ERR_ARG, std::string("species table ") + names[q] + " short");
   }
-  const double *wp = table(c, "wilkepair");
-  for (int n = 0; n < ns; n++)
-    for (int m = 0; m < ns; m++) s.wilkepair[n * MAXNS + m] = wp ? wp[n * ns + m] : 0.25;
-  if (c->phys.trans == PGB_TRANS_CONSTANT && (!table(c, "mu0") || !table(c, "kappa0")))
+  if (c->phys.trans == PGB_TRANS_CONSTANT && (!tab[T_MU0] || !tab[T_KAPPA0]))
     return fail(PGB_ERR_ARG, "constant transport needs mu0 and kappa0");
-  // one species: mixmom gives R = 0 + 1 Rsp exactly, likewise cp and h298
-  s.R1 = 0.0 + 1.0 * s.Rsp[0];
-  s.cp1 = 0.0 + 1.0 * s.cp0[0];
-  s.h2981 = 0.0 + 1.0 * s.h298R[0];
-  s.cv1 = s.cp1 - s.R1;
-  s.cvinv1 = 1.0 / s.cv1;
-  s.gamma1 = s.cp1 / s.cv1;
-  s.th1 = s.cp1 / s.gamma1;
-  if (ns == 1 && c->phys.trans == PGB_TRANS_CONSTANT) {
-    // transport.mako with Y = 1: X = MWinv / MWinv, then Wilke and the conductivity mean
-    volatile double Y = 1.0;
-    const double denom = 0.0 + Y * s.MWinv[0];
-    const double MWmix = 1.0 / denom;
-    const double X = Y * s.MWinv[0] * MWmix;
-    const double sqrtmu = std::sqrt(s.mu0[0]);
-    const double sinv = 1.0 / (sqrtmu * s.MWqinv[0]);
-    const double sn = sqrtmu * s.MWqinv[0];
-    const double r = 1.0 + sn * sinv;
-    const double phi = 0.0 + r * r * s.wilkepair[0] * X;
-    s.mu1 = 0.0 + sqrtmu * sqrtmu * X / phi;
-    const double series = 0.0 + X * s.kappa0[0];
-    const double parallel = 0.0 + X / s.kappa0[0];
-    s.kappa1 = 0.5 * (series + 1.0 / parallel);
-  }
+  species_fill(c->sp, ns, c->phys.alpha, c->phys.trans == PGB_TRANS_CONSTANT, tab, table(c, "wilkepair"));
   return PGB_OK;
 }
 
@@ -781,6 +741,10 @@ int prepare(pgb_case *c, bool fused) {
 extern "C" {
 
 const char *pgb_last_error(void) { return g_err.c_str(); }
+
+// sets the error text of pgb_last_error from the library's other files; not
+// part of the ABI
+__attribute__((visibility("hidden"))) int pgb_internal_fail(int code, const char *msg) { return fail(code, msg); }
 int pgb_version(void) { return 1; }
 
 int pgb_device_init(int ordinal) {

@@ -8,12 +8,15 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 namespace pgb {
 
 constexpr int MAXNS = 12;
 
 // the case's species tables, in constant memory; filled per case before its
-// launches (a case's tables are copied in when the case is made current)
+// launches (a case's tables are copied in when the case is made current).
+// Static: each translation unit of the library has its own copy and fills it.
 struct Species {
   int ns;
   double Ru;
@@ -27,7 +30,47 @@ struct Species {
   double mu1, kappa1;
 };
 
-__constant__ Species kSp;
+static __constant__ Species kSp;
+
+// The species tables, in the order the C ABI passes them packed, into the
+// constant struct; and the single-species shortcuts by the same operations
+// the per-cell formulas take for Y = 1 (mixmom gives R = 0 + 1 Rsp exactly,
+// likewise cp and h298; transport.mako with X = MWinv / MWinv).
+enum { T_RSP = 0, T_CP0, T_H298R, T_MWINV, T_HPOLY0, T_H298, T_MU0, T_KAPPA0, T_MWQINV, T_LEWIS, T_NTAB };
+inline void species_fill(Species &s, int ns, double alpha, bool constant_transport, const double *const tab[T_NTAB],
+                         const double *wilkepair) {
+  s.ns = ns;
+  s.alpha = alpha;
+  s.Ru = 8314.46261815324;
+  double *dst[T_NTAB] = {s.Rsp, s.cp0, s.h298R, s.MWinv, s.hpoly0, s.h298, s.mu0, s.kappa0, s.MWqinv, s.lewis};
+  for (int q = 0; q < T_NTAB; q++)
+    for (int n = 0; n < ns; n++) dst[q][n] = tab[q] ? tab[q][n] : 1.0;
+  for (int n = 0; n < ns; n++)
+    for (int m = 0; m < ns; m++) s.wilkepair[n * MAXNS + m] = wilkepair ? wilkepair[n * ns + m] : 0.25;
+  s.R1 = 0.0 + 1.0 * s.Rsp[0];
+  s.cp1 = 0.0 + 1.0 * s.cp0[0];
+  s.h2981 = 0.0 + 1.0 * s.h298R[0];
+  s.cv1 = s.cp1 - s.R1;
+  s.cvinv1 = 1.0 / s.cv1;
+  s.gamma1 = s.cp1 / s.cv1;
+  s.th1 = s.cp1 / s.gamma1;
+  s.mu1 = s.kappa1 = 0.0;
+  if (ns == 1 && constant_transport) {
+    volatile double Y = 1.0;
+    const double denom = 0.0 + Y * s.MWinv[0];
+    const double MWmix = 1.0 / denom;
+    const double X = Y * s.MWinv[0] * MWmix;
+    const double sqrtmu = std::sqrt(s.mu0[0]);
+    const double sinv = 1.0 / (sqrtmu * s.MWqinv[0]);
+    const double sn = sqrtmu * s.MWqinv[0];
+    const double r = 1.0 + sn * sinv;
+    const double phi = 0.0 + r * r * s.wilkepair[0] * X;
+    s.mu1 = 0.0 + sqrtmu * sqrtmu * X / phi;
+    const double series = 0.0 + X * s.kappa0[0];
+    const double parallel = 0.0 + X / s.kappa0[0];
+    s.kappa1 = 0.5 * (series + 1.0 / parallel);
+  }
+}
 
 // EosState (peregrine/simulator/mixture/eos/base.py:85-86)
 struct State {

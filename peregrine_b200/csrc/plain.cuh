@@ -12,7 +12,7 @@ namespace pgb {
 
 // the halo fill over every block at once: comps components per entry
 // (the reference's place kernel, peregrine/multiblock/collections/exchange/kernels/place.mako:11-20)
-__global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps) {
+static __global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const HaloEntry h = tab[e];
     double *d = base + comps * h.dcv + h.didx;
@@ -74,16 +74,21 @@ __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const doub
 
 // cell gradients of u, v, w, T, Y on the interior
 // (peregrine/simulator/navstokes/kernels/dqdxyz.mako:16-41)
+// on the interior, or with grow 1 the interior and one halo layer around it
+// (the halo's edge cells there read cells no halo fill sets; nothing reads
+// their gradients)
 template <int NS>
 __global__ void k_grads(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                         const double *__restrict__ stall, const double *__restrict__ met,
-                        double *__restrict__ gall) {
+                        double *__restrict__ gall, int grow = 0) {
   constexpr int NE = 4 + NS, NGRAD = NE - 1;
   const BlockDev &B = blks[b];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long n = (long long)B.nx * B.ny * B.nz;
+  const int gx = B.nx + 2 * grow, gy = B.ny + 2 * grow, gz = B.nz + 2 * grow;
+  const long long n = (long long)gx * gy * gz;
   if (t >= n) return;
-  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const int i = (int)(t % gx) + NG - grow, j = (int)((t / gx) % gy) + NG - grow,
+            k = (int)(t / ((long long)gx * gy)) + NG - grow;
   const long long c = cell_index(B, i, j, k);
   const long long sI = 1, sJ = B.X, sK = (long long)B.X * B.Y;
   const double *Q = Qall + NE * B.cv + c;
@@ -289,7 +294,7 @@ struct CombineDev {
   int own, nterms, step;
 };
 
-__global__ void k_combine(const BlockDev *__restrict__ blks, int b, int ne, CombineDev cd, const double *__restrict__ dt) {
+static __global__ void k_combine(const BlockDev *__restrict__ blks, int b, int ne, CombineDev cd, const double *__restrict__ dt) {
   const BlockDev &B = blks[b];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)B.nx * B.ny * B.nz) return;
@@ -334,7 +339,7 @@ __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const doub
 }
 
 // interior cells between a packed host-order buffer [comp][k][j][i] and a register
-__global__ void k_unpack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ src,
+static __global__ void k_unpack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ src,
                          double *__restrict__ Rall) {
   const BlockDev &B = blks[b];
   const long long n = (long long)B.nx * B.ny * B.nz;
@@ -345,7 +350,7 @@ __global__ void k_unpack(const BlockDev *__restrict__ blks, int b, int ne, const
   for (int l = 0; l < ne; l++) Rall[c + l * B.vol] = src[l * n + t];
 }
 
-__global__ void k_pack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ Rall,
+static __global__ void k_pack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ Rall,
                        double *__restrict__ dst) {
   const BlockDev &B = blks[b];
   const long long n = (long long)B.nx * B.ny * B.nz;
