@@ -288,14 +288,10 @@ def main():
     with Clocks(local) as clk:
         ms = time_graph(mb, dt, args.steps)
     barrier()
-    if dist is not None:
-        import torch
+    from peregrine_b200.replicas import max_over_ranks, weak_throughput
 
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    total_cell_stages = ncells * STAGES * args.steps * world
-    value = total_cell_stages / (ms / 1e3)
+    ms = max_over_ranks(ms, dist, device=f"cuda:{local}")
+    value = weak_throughput(ncells, STAGES, args.steps, ms, world)
     launches = mb.launches_per_step()
 
     # the fused kernel's own launches, timed by events between launches

@@ -31,7 +31,7 @@ class OCase(ctypes.Structure):
                 ("alpha", ctypes.c_double)] + \
                [(n, ctypes.POINTER(ctypes.c_double)) for n in
                 ("Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0", "kappa0", "MWqinv", "wilkepair", "lewis")] + \
-               [("Ru", ctypes.c_double)]
+               [("Ru", ctypes.c_double), ("skip_adv", ctypes.c_int)]
 
 
 class OBlock(ctypes.Structure):
@@ -49,6 +49,7 @@ def _lib():
     lib.oracle_rhs.restype = ctypes.c_int
     lib.oracle_fromprims.restype = ctypes.c_int
     lib.oracle_combine.restype = ctypes.c_int
+    lib.oracle_kepaec_faces.restype = ctypes.c_int
     return lib
 
 
@@ -116,13 +117,14 @@ def stage_combines(integrator, nregs_names):
         rows = ((0.0, 0.5, 1.0 / 6.0), (0.5, 0.5, 1.0 / 3.0), (0.5, 1.0, 1.0 / 3.0), (1.0, None, 1.0 / 6.0))
         out = []
         for n, (_, wdQ, wsum) in enumerate(rows):
-            own = 0.0 if n == 0 else 1.0
-            share = combine(total, [(total, own), (dQ, wsum)])
+            q = start if n == 0 else stage
+            share = combine(total, [(total, 0.0 if n == 0 else 1.0), (dQ, wsum)])
             if wdQ is None:
-                out.append(("stage", stage if n else start, [share, combine(start, [(start, 1.0), (total, 1.0)], step=False)]))
+                last = combine(start, [(start, 1.0), (total, 1.0)], step=False)
             else:
-                out.append(("stage", start if n == 0 else stage, [share, combine(stage, [(start, 1.0), (dQ, wdQ)])]))
-        return [(q, cs) for _, q, cs in out], dQ
+                last = combine(stage, [(start, 1.0), (dQ, wdQ)])
+            out.append((q, [share, last]))
+        return out, dQ
     tables = {
         "rk1": ((0.0, 0.0, 1.0, 1.0),),
         "rk2": ((0.0, 0.0, 1.0, 1.0), (1.0, 0.5, 0.5, 0.5)),
@@ -151,6 +153,7 @@ class Oracle:
     """
 
     def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0):
+        """constants: the mixture's tables; blocks/metrics may be empty for face-only use."""
         self.lib = _lib()
         self.ns, self.ne = ns, 4 + ns
         self.blocks = blocks
@@ -201,14 +204,35 @@ class Oracle:
             assert q.shape == Q.shape
             self.lib.oracle_fromprims(ctypes.byref(self.case), _ptr(q), _ptr(Q), ctypes.c_long(Q.size // self.ne))
 
-    def rhs(self, Q, dQ):
+    def rhs(self, Q, dQ, faces=False, diffusive_only=False):
+        """dQ of every block from Q; with faces, each block's [iF, jF, kF] too."""
         obs = self._oblocks(Q)
         m = np.ascontiguousarray(self.map)
         ptrs = (ctypes.POINTER(ctypes.c_double) * len(dQ))(*[_ptr(d) for d in dQ])
+        fl, fptr = None, None
+        if faces:
+            fl = []
+            for blk in self.blocks:
+                for a in range(3):
+                    shape = [n + 2 * blk.ng for n in blk.cells]
+                    shape[a] += 1
+                    fl.append(np.zeros(tuple(shape) + (self.ne,)))
+            fptr = (ctypes.POINTER(ctypes.c_double) * len(fl))(*[_ptr(f) for f in fl])
+        self.case.skip_adv = int(diffusive_only)
         rc = self.lib.oracle_rhs(ctypes.byref(self.case), obs, len(self.blocks),
-                                 m.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(m.size), ptrs)
+                                 m.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(m.size), ptrs, fptr)
+        self.case.skip_adv = 0
         if rc:
             raise RuntimeError(f"oracle_rhs: {rc}")
+        if faces:
+            return [fl[3 * b:3 * b + 3] for b in range(len(self.blocks))]
+
+    def kepaec_faces(self, QL, QR, S):
+        """kepaec on independent faces, each side's state from its Q."""
+        QL, QR, S = (np.ascontiguousarray(x, dtype=np.float64) for x in (QL, QR, S))
+        F = np.zeros_like(QL)
+        self.lib.oracle_kepaec_faces(ctypes.byref(self.case), ctypes.c_long(QL.shape[0]), _ptr(QL), _ptr(QR), _ptr(S), _ptr(F))
+        return F
 
     def step(self, dt):
         names = list(range(self.nregs))

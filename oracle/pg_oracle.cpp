@@ -33,6 +33,7 @@ struct OCase {
   const double *Rsp, *cp0, *h298R, *MWinv, *hpoly0, *h298;
   const double *mu0, *kappa0, *MWqinv, *wilkepair, *lewis;
   double Ru;
+  int skip_adv;    // 1: the face fluxes hold the diffusive flux alone (a test's view)
 };
 
 struct OBlock {
@@ -61,7 +62,7 @@ struct Dims {
 };
 
 Dims cells(const OBlock &b) { return {b.nx + 2 * b.ng, b.ny + 2 * b.ng, b.nz + 2 * b.ng}; }
-Dims faces(const OBlock &b, int a) {
+Dims face_dims(const OBlock &b, int a) {
   Dims d = cells(b);
   if (a == 0) d.X += 1;
   if (a == 1) d.Y += 1;
@@ -327,8 +328,10 @@ extern "C" {
 // interior and first halo layer; rhs: gradients on the interior and their
 // one-plane exchange, advective then diffusive face fluxes on the interior
 // faces, applyflux (simulator/advec/kernels/applyflux.mako:2-11).
+// faces, when not null, receives each block's face fluxes: faces[3 b + a] the
+// array of axis a, [X'][Y'][Z'][ne] with one plane more along a.
 int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *map, long nmap,
-               double **dQ) {
+               double **dQ, double **faces) {
   const OCase &c = *cp;
   const int ns = c.ns, ne = 4 + ns, ngrad = ne - 1;
   const bool visc = c.simulator == O_NAVSTOKES;
@@ -411,7 +414,7 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
     Scratch &s = scr[b];
     const int g = B.ng;
     for (int a = 0; a < 3; a++) {
-      const Dims f = faces(B, a);
+      const Dims f = face_dims(B, a);
       s.F[a].assign((long)f.X * f.Y * f.Z * ne, 0.0);
       const int hi[3] = {B.nx + (a == 0), B.ny + (a == 1), B.nz + (a == 2)};
       // the interior faces of axis a: a face is indexed like the cell to its right
@@ -428,14 +431,16 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
             const State &sR = *reinterpret_cast<const State *>(&s.state[R * NSTATE]);
             double *F = &s.F[a][at * ne];
             const double *S = B.S[a] + at * 3;
-            kepaec(c, side(QL, sL), side(QR, sR), QL, QR, S, F);
+            if (!c.skip_adv) kepaec(c, side(QL, sL), side(QR, sR), QL, QR, S, F);
             if (visc)
               alphadamping(c, S, B.xf[a] + at * 3, B.xcc + L * 3, B.xcc + R * 3, QL, QR, sL, sR,
                            &s.tr[L * (2 + ns)], &s.tr[R * (2 + ns)], &s.hsp[L * ns], &s.hsp[R * ns],
                            &s.grads[L * ngrad * 3], &s.grads[R * ngrad * 3], F);
           }
     }
-    const Dims fi = faces(B, 0), fj = faces(B, 1), fk = faces(B, 2);
+    if (faces)
+      for (int a = 0; a < 3; a++) std::memcpy(faces[3 * b + a], s.F[a].data(), sizeof(double) * s.F[a].size());
+    const Dims fi = face_dims(B, 0), fj = face_dims(B, 1), fk = face_dims(B, 2);
 #pragma omp parallel for collapse(2) schedule(static)
     for (int i = g; i < g + B.nx; i++)
       for (int j = g; j < g + B.ny; j++)
@@ -448,6 +453,18 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
           for (int l = 0; l < ne; l++)
             dQ[b][at * ne + l] = (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
         }
+  }
+  return 0;
+}
+
+// kepaec on n independent faces: each side's state from its Q by fromQ,
+// rows [n][ne] (the flux-function check against the reference's numpy oracle)
+int oracle_kepaec_faces(const OCase *cp, long n, const double *QL, const double *QR, const double *S, double *F) {
+  const int ne = 4 + cp->ns;
+  for (long f = 0; f < n; f++) {
+    const double *ql = QL + f * ne, *qr = QR + f * ne;
+    const State sl = fromQ(*cp, ql), sr = fromQ(*cp, qr);
+    kepaec(*cp, side(ql, sl), side(qr, sr), ql, qr, S + 3 * f, F + f * ne);
   }
   return 0;
 }

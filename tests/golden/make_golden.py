@@ -1,0 +1,197 @@
+"""Generates the golden fixtures of tests/golden from the reference itself.
+
+    python tests/golden/make_golden.py [path to the reference checkout]
+
+Run here, where the reference's Python can be imported; the fixtures it
+writes (*.npz, *.json) are committed, and nothing at test time reads the
+reference.  The reference's package imports mako, mpi4py, h5py and lxml at
+module level for its code generation, MPI and files; none of those run on the
+paths used here, so stub modules stand in for them.
+
+What it records, each from the reference's own code:
+  faces_kepaec.npz   tests/simulator/oracle.py's cpg sides (cpg) and kepaec
+                     flux on random faces, for air and a binary N2/O2 gas;
+  metrics.npz        peregrine/multiblock/block/grid.py's cell centres, face
+                     centres, area vectors, detJinv and Jinv of a jostled block;
+  constants.npz      peregrine/simulator/mixture's constants for the
+                     Taylor-Green air and a binary gas with constant transport;
+  rk_tables.json     peregrine/integrators/rungekutta.py's combine kernels per
+                     stage (registers, weights, dt placement) for every scheme.
+"""
+
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+
+
+def stub(name, **attrs):
+    m = types.ModuleType(name)
+    for k, v in attrs.items():
+        setattr(m, k, v)
+    sys.modules[name] = m
+    return m
+
+
+class _Any:
+    def __init__(self, *a, **k):
+        pass
+
+
+class _Comm:
+    rank, size = 0, 1
+
+    def Get_rank(self):
+        return 0
+
+    def Get_size(self):
+        return 1
+
+    def bcast(self, x, root=0):
+        return x
+
+    def Allreduce(self, *a, **k):
+        pass
+
+    def Barrier(self):
+        pass
+
+
+def install_stubs():
+    mako = stub("mako")
+    mako.runtime = stub("mako.runtime", capture=lambda *a, **k: "", supports_caller=lambda f: f)
+    mako.lookup = stub("mako.lookup", TemplateLookup=_Any)
+    mako.template = stub("mako.template", Template=_Any)
+    MPI = types.SimpleNamespace(COMM_WORLD=_Comm(), IN_PLACE=None, MAX=None, SUM=None, Prequest=_Any,
+                                Request=_Any, Comm=_Comm)
+    m4 = stub("mpi4py", MPI=MPI)
+    stub("mpi4py.MPI", **vars(MPI))
+    m4.util = stub("mpi4py.util")
+    m4.util.dtlib = stub("mpi4py.util.dtlib", from_numpy_dtype=lambda d: d)
+    h5 = stub("h5py", File=_Any)
+    for s in ("h5fd", "h5p", "h5s"):
+        setattr(h5, s, stub("h5py." + s))
+    lx = stub("lxml")
+    lx.etree = stub("lxml.etree")
+
+
+def air_tgv():
+    sys.path.insert(0, os.path.dirname(HERE))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from peregrine_b200.cases import tgv_gas
+
+    return tgv_gas()[0]
+
+
+BINARY = {"N2": {"MW": 28.0134, "cp0": 1040.0, "mu0": 1.8e-5, "kappa0": 0.026},
+          "O2": {"MW": 31.9988, "cp0": 918.0, "mu0": 2.0e-5, "kappa0": 0.027, "lewis": 1.3}}
+
+
+def faces(orc, gas, n, rng):
+    ns = len(gas)
+
+    def side():
+        p = rng.uniform(5e4, 2e5, n)
+        T = rng.uniform(200.0, 600.0, n)
+        Y = rng.uniform(0.1, 0.9, (n, ns - 1))
+        s = orc.cpg(gas, p, T, Y)
+        u = rng.uniform(-100.0, 100.0, (n, 3))
+        s["u"], s["v"], s["w"] = u[:, 0], u[:, 1], u[:, 2]
+        s["Y"] = Y
+        rho = s["rho"]
+        Q = np.concatenate([rho[:, None], rho[:, None] * u,
+                            (rho * (s["e"] + 0.5 * (u * u).sum(axis=1)))[:, None], rho[:, None] * Y], axis=1)
+        return s, Q
+
+    L, QL = side()
+    R, QR = side()
+    S = rng.uniform(-1.0, 1.0, (n, 3))
+    F = orc.kepaec(L, R, S)
+    return dict(QL=QL, QR=QR, S=S, F=F)
+
+
+def metrics(GridBlock, rng):
+    ng = 2
+    shape = (7 + 2 * ng, 6 + 2 * ng, 5 + 2 * ng)
+    axes = [np.linspace(0.0, 1.0, n) for n in shape]
+    nodes = np.stack(np.meshgrid(*axes, indexing="ij"), axis=-1)
+    nodes = nodes + rng.uniform(-1, 1, nodes.shape) * 0.15 / 10
+    blk = GridBlock.__new__(GridBlock)
+    blk.ng, blk.nblki = ng, 0
+    out = dict(nodes=nodes, xcc=blk._cellcenters(nodes), detJinv=blk._detJinv(nodes), Jinv=blk._Jinv(nodes))
+    for a, d in enumerate("ijk"):
+        out[f"{d}S"] = blk._areavecs(nodes, a)
+        out[f"{d}xc"] = blk._facecenters(nodes, a)
+    return out
+
+
+def constants(pg, get_mixture, gas):
+    cfg = pg.Config()
+    cfg["mixture"]["species"] = gas
+    cfg["mixture"]["trans"] = "constant"
+    mix = get_mixture(cfg)
+    return {k: np.asarray(v, dtype=np.float64) for k, v in mix.constants().items()}
+
+
+def rk_tables(integrators):
+    import peregrine.integrators.base as base
+
+    recorded = []
+
+    class Recorder:
+        def __init__(self, provider, template, options=None, **arguments):
+            recorded.append(dict(options=options, arguments=arguments))
+
+    base.Kernel = Recorder
+    out = {}
+    for cls in (integrators.RK1, integrators.RK2, integrators.RK3, integrators.RK34, integrators.RK4):
+        integ = cls.__new__(cls)
+        integ.provider = None
+        regs = [f"R{n}" for n in range(cls.nregs)]
+        stages = []
+        for n in range(len(cls.stages)):
+            recorded.clear()
+            integ.stagekerns(n, regs)
+            q = integ.stageregs(regs)[n].Q
+            combines = []
+            for r in recorded:
+                a, o = r["arguments"], r["options"]
+                terms = [(a[f"X{m}"], a[f"w{m}"]) for m in range(o["terms"])]
+                combines.append(dict(out=a["out"], own=a.get("wout") if o["own"] else None, terms=terms, step=o["step"]))
+            stages.append(dict(q=q, combines=combines))
+        out[cls.name] = dict(nregs=cls.nregs, stages=stages)
+    return out
+
+
+def main():
+    install_stubs()
+    sys.path.insert(0, REF)
+    import peregrine as pg
+    from peregrine import integrators
+    from peregrine.multiblock.block.grid import GridBlock
+    from peregrine.simulator.mixture import get_mixture
+    from tests.simulator import oracle as orc
+
+    rng = np.random.default_rng(20261203)
+    air = air_tgv()
+    np.savez(os.path.join(HERE, "faces_kepaec.npz"),
+             **{f"air_{k}": v for k, v in faces(orc, {"Air": {"MW": air["Air"]["MW"], "cp0": air["Air"]["cp0"]}}, 64, rng).items()},
+             **{f"binary_{k}": v for k, v in faces(orc, {k: dict(MW=v["MW"], cp0=v["cp0"]) for k, v in BINARY.items()}, 64, rng).items()})
+    np.savez(os.path.join(HERE, "metrics.npz"), **metrics(GridBlock, rng))
+    consts = {f"air_{k}": v for k, v in constants(pg, get_mixture, air).items()}
+    consts.update({f"binary_{k}": v for k, v in constants(pg, get_mixture, BINARY).items()})
+    np.savez(os.path.join(HERE, "constants.npz"), **consts)
+    with open(os.path.join(HERE, "rk_tables.json"), "w") as f:
+        json.dump(rk_tables(integrators), f, indent=1)
+    with open(os.path.join(HERE, "gases.json"), "w") as f:
+        json.dump(dict(air=air, binary=BINARY), f, indent=1)
+    print("wrote", sorted(p for p in os.listdir(HERE) if not p.endswith(".py")))
+
+
+if __name__ == "__main__":
+    main()

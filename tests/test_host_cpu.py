@@ -1,0 +1,129 @@
+"""Host-side logic with no GPU: the C ABI's symbols, config, meshes, halo maps,
+and the multi-rank timing over gloo."""
+
+import ctypes
+import os
+import re
+import socket
+
+import numpy as np
+import pytest
+
+from peregrine_b200 import native
+from peregrine_b200.config import Config, ConfigError
+from peregrine_b200.mesher import CubeMesher, uneven_cuts
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "pgb200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pgb_\w+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = native.load()
+    names = header_functions()
+    assert len(names) >= 30
+    for name in names:
+        assert hasattr(lib, name), name
+    # and the Python binding types every one of them
+    assert set(names) <= set(native.SIGNATURES), set(names) - set(native.SIGNATURES)
+
+
+def test_errors_carry_the_library_message():
+    lib = native.load()
+    rc = lib.pgb_case_create(None, None)
+    assert rc == native.ERR_ARG
+    assert b"null" in lib.pgb_last_error()
+    with pytest.raises(native.PgbArgumentError):
+        native.check(rc)
+
+
+def test_config_refuses_unknown_keys_and_bad_choices():
+    cfg = Config()
+    with pytest.raises(KeyError):
+        cfg["simulation"]["simulatr"] = "euler"
+    cfg["time-integration"]["integrator"] = "rk5"
+    with pytest.raises(ConfigError):
+        cfg.validate()
+    cfg = Config()
+    cfg["mixture"]["trans"] = None
+    with pytest.raises(ConfigError):
+        cfg.validate()  # navier-stokes needs a transport model
+    cfg = Config.from_dict({"simulation": {"simulator": "euler", "dt": "1e-7"}})
+    assert cfg["simulation"]["dt"] == 1e-7
+
+
+def test_uneven_cuts_are_seeded_and_bounded():
+    for seed in range(5):
+        cuts = uneven_cuts(128, 3, 30, 56, np.random.default_rng(seed))
+        assert sum(cuts) == 128 and all(30 <= c <= 56 for c in cuts)
+    a = uneven_cuts(128, 3, 30, 56, np.random.default_rng(0))
+    b = uneven_cuts(128, 3, 30, 56, np.random.default_rng(0))
+    assert a == b
+
+
+def test_lattice_connectivity_and_periodic_node_halo():
+    mesh = CubeMesher(mbdims=[3, 2, 1], cells=[[4, 5, 6], [3, 4], [5]], lengths=[1.0, 1.0, 1.0],
+                      periodic=[True, True, False])
+    blocks = mesh.make_blocks(2)
+    assert [b.cells for b in blocks][:3] == [(4, 3, 5), (5, 3, 5), (6, 3, 5)]
+    b0 = blocks[0]
+    lo, hi = b0.get_intface(1), b0.get_intface(2)
+    assert lo.nbr == 2 and lo.periodic and hi.nbr == 1 and not hi.periodic
+    assert b0.get_intface(5).nbr is None  # k is not periodic
+    # the i-low halo nodes of block 0 are block 2's nodes one in from its high face, moved down one length
+    g = b0.ng
+    x0 = b0.nodes[g - 1, g:-g, g:-g, 0]
+    x2 = blocks[2].nodes[g + blocks[2].ni - 2, g:-g, g:-g, 0]
+    assert np.allclose(x0, x2 - 1.0)
+
+
+def test_halo_map_covers_every_face_halo_cell_once():
+    from oracle.oracle import halo_map
+
+    mesh = CubeMesher(mbdims=[2, 2, 2], cells=[[3, 4], [4, 3], [2, 5]], lengths=[1.0] * 3, periodic=[True] * 3)
+    blocks = mesh.make_blocks(2)
+    m = halo_map(blocks)
+    expect = sum(2 * 2 * (b.cells[1] * b.cells[2] + b.cells[0] * b.cells[2] + b.cells[0] * b.cells[1]) for b in blocks)
+    assert m.size == expect
+    keys = set(zip(m["dblk"], m["di"], m["dj"], m["dk"]))
+    assert len(keys) == expect
+    # every source is an interior cell of its block
+    for r in m[:200]:
+        sb = blocks[r["sblk"]]
+        for a, c in enumerate((r["si"], r["sj"], r["sk"])):
+            assert 2 <= c < 2 + sb.cells[a]
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out):
+    import torch.distributed as dist
+
+    from peregrine_b200.replicas import max_over_ranks, weak_throughput
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    ms = max_over_ranks(10.0 + rank, dist, device="cpu")
+    out[rank] = (ms, weak_throughput(1000, 4, 10, ms, world))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_report_the_slowest_time_and_the_whole_job():
+    import torch.multiprocessing as mp
+
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_rank, args=(2, _free_port(), out), nprocs=2, join=True)
+    assert out[0] == out[1]
+    ms, value = out[0]
+    assert ms == 11.0
+    assert value == pytest.approx(1000 * 4 * 10 * 2 / 0.011)
