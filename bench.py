@@ -241,7 +241,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-extra", action="store_true", help="skip the per-block and end-to-end legs")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape and tiles")
-    ap.add_argument("--shape", default=None, help="force the fused kernel's THREADSxMINBLOCKS (no tuning)")
+    ap.add_argument("--shape", default=None, help="force the fused kernel's THREADSxMINBLOCKSxWIDTH (no tuning)")
     ap.add_argument("--ksplit", type=int, default=3, help="k runs per block with --shape")
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
     args = ap.parse_args()
@@ -272,8 +272,8 @@ def main():
     from peregrine_b200 import autotune
 
     if args.shape:
-        threads, minb = (int(x) for x in args.shape.split("x"))
-        tuned = autotune.tune(mb, dt, shapes=((threads, minb),), ksplits=(args.ksplit,))
+        shape = tuple(int(x) for x in args.shape.split("x"))
+        tuned = autotune.tune(mb, dt, only=(shape,), ksplits=(args.ksplit,))
     else:
         tuned = None if args.no_tune else autotune.tune(mb, dt)
     # warm-up (the first call captures the graph)

@@ -179,9 +179,12 @@ int pgb_launches_per_step(const pgb_case *c, int path, int *count);
 int pgb_set_tile(pgb_case *c, int blk, int tw, int th, int kchunk);
 int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk);
 
-/* the uniform-metric fused kernel's threads per CTA and the CTAs per SM its
- * registers are bounded for: 256 x 1, 256 x 2, 128 x 2, 128 x 3 or 128 x 4 */
-int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks);
+/* the uniform-metric fused kernel's instance: threads per CTA, the CTAs per
+ * SM its registers are bounded for, and the widest tile its shared-memory
+ * layout holds; pgb_fused_shapes lists the instances the library has, four
+ * ints each (threads, minblocks, width, height) */
+int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks, int width);
+int pgb_fused_shapes(int *shapes, int cap, int *n);
 
 /* whether blk runs in the uniform-metric form (1) or reads its metric arrays (0) */
 int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);

@@ -15,8 +15,15 @@ import numpy as np
 
 from peregrine_b200 import native
 
-SHAPES = ((256, 1), (256, 2), (128, 2), (128, 3), (128, 4))
-KSPLITS = (1, 2, 3)
+KSPLITS = (2, 3, 4)
+
+
+def shapes():
+    """The uniform kernel's instances the library has: (threads, minblocks, width, height)."""
+    buf = (ctypes.c_int * 64)()
+    n = ctypes.c_int()
+    native.call("pgb_fused_shapes", buf, 16, ctypes.byref(n))
+    return [tuple(buf[4 * q:4 * q + 4]) for q in range(n.value)]
 
 
 def _time(mb, dt, steps):
@@ -37,15 +44,18 @@ def _tiles(mb, threads, ksplit):
     return out
 
 
-def tune(mb, dt, steps=3, shapes=SHAPES, ksplits=KSPLITS, verbose=False):
+def tune(mb, dt, steps=3, only=None, ksplits=KSPLITS, verbose=False):
     """Times every candidate; leaves the fastest set on the case and returns it."""
     if mb.path != native.PATH_BATCHED:
         return None
     saved = [b.Q.get() for b in mb.blocks]
     results = []
-    for (threads, minb), ksplit in itertools.product(shapes, ksplits):
+    cands = [s[:3] for s in shapes()]
+    if only is not None:
+        cands = [c for c in cands if c in only]
+    for (threads, minb, width), ksplit in itertools.product(cands, ksplits):
         try:
-            native.call("pgb_set_fused_shape", mb.case, threads, minb)
+            native.call("pgb_set_fused_shape", mb.case, threads, minb, width)
             for n, (tw, th, kc) in enumerate(_tiles(mb, threads, ksplit)):
                 mb.set_tile(n, tw, th, kc)
             _time(mb, dt, 1)
@@ -54,16 +64,16 @@ def tune(mb, dt, steps=3, shapes=SHAPES, ksplits=KSPLITS, verbose=False):
             if verbose:
                 print(f"  {threads}x{minb} k/{ksplit}: {e}")
             continue
-        results.append((ms, threads, minb, ksplit))
+        results.append((ms, threads, minb, width, ksplit))
         if verbose:
-            print(f"  {threads}x{minb} k/{ksplit}: {ms:.4f} ms/step")
+            print(f"  {threads}x{minb} w{width} k/{ksplit}: {ms:.4f} ms/step")
     if not results:
         return None
-    ms, threads, minb, ksplit = min(results)
-    native.call("pgb_set_fused_shape", mb.case, threads, minb)
+    ms, threads, minb, width, ksplit = min(results)
+    native.call("pgb_set_fused_shape", mb.case, threads, minb, width)
     for n, (tw, th, kc) in enumerate(_tiles(mb, threads, ksplit)):
         mb.set_tile(n, tw, th, kc)
     for b, q in zip(mb.blocks, saved):
         b.Q.set(q)
-    return {"threads": threads, "minblocks": minb, "ksplit": ksplit, "ms_per_step": ms,
-            "candidates": len(results), "all": sorted((round(r[0], 4), r[1], r[2], r[3]) for r in results)}
+    return {"threads": threads, "minblocks": minb, "width": width, "ksplit": ksplit, "ms_per_step": ms,
+            "candidates": len(results), "all": sorted((round(r[0], 4),) + r[1:] for r in results)}

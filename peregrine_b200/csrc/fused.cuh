@@ -54,6 +54,16 @@ struct FusedArgs {
   int npre;
   int pre[3];
   FusedCombine combp[2];
+  // the same combines as one fixed form the uniform kernel evaluates with no
+  // branch: out0 = c[0][0] p0 + c[0][1] p1 + c[0][2] dt dQ, and
+  // out1 = c[1][0] p0 + c[1][1] p1 + c[1][2] dt dQ + c[1][3] out0, summed in
+  // that order, a missing term's weight zero (its register slot holds zeros);
+  // p0, p1 the registers the stage reads (slots 0 and 1), in the order the
+  // reference's combines name them
+  double cw[2][4];
+  double *outp[2];
+  const double *prep[2];
+  int write[2];
   const double *dt;
 };
 

@@ -150,25 +150,37 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Shared memory of the uniform kernel with NT threads on a tw x th tile:
-// P[2][P_N][N2] two planes of cell values, G[12][NT] one plane of gradients,
-// Fi[5][NT], Fj[5][NT] low-face fluxes, raw[5][NT + NR] the Q copies in
-// flight (NR the ring's second cells), pre[2][5][NT] the combines' registers.
-template <int NT>
-struct F2Layout {
-  int N2, NR;
-  double *P, *G, *Fi, *Fj, *raw, *pre;
-  __host__ __device__ static size_t doubles(int tw, int th, bool visc) {
-    const int N2 = (tw + 4) * (th + 4), NR = 2 * (tw + th);
-    return (size_t)2 * P_N * N2 + (visc ? 12 * NT : 0) + 10 * NT + 5 * (NT + NR) + 2 * 5 * NT;
+// Shared memory of the uniform kernel, laid out for tiles of at most TW x TH
+// cells (the layout's extents are compile-time, so every neighbour and field
+// offset is an immediate; a tile may be smaller): P[2][P_N][LN2] two planes of
+// cell values, G[12][LN1] one plane of gradients, Fi[5][LN1], Fj[5][LN1]
+// low-face fluxes, raw[3][5][NT + LNR] the Q copies of three planes in
+// flight, pre[3][2][5][LNT] the combines' registers of three planes.
+template <int NT, int TW, int TH>
+struct F2L {
+  static constexpr int LW1 = TW + 2, LH1 = TH + 2, LN1 = LW1 * LH1;
+  static constexpr int LW2 = TW + 4, LN2 = LW2 * (TH + 4), LNR = 2 * (TW + TH), LNT = TW * TH;
+  static constexpr int RAW = 5 * (NT + LNR), PRE = 2 * 5 * LNT;
+  static_assert(LN1 <= NT, "the tile and its ring fit the CTA");
+  static_assert(LNR <= NT, "the outer ring fits the CTA");
+  __host__ __device__ static constexpr size_t doubles(bool visc) {
+    return (size_t)2 * P_N * LN2 + (visc ? 12 * LN1 : 0) + 10 * LN1 + 3 * RAW + 3 * PRE;
   }
 };
 
-template <bool VISC, int NT, int MINB>
+template <bool VISC, int NT, int MINB, int TW, int TH>
 __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
+  using L = F2L<NT, TW, TH>;
+  constexpr int LW1 = L::LW1, LN1 = L::LN1, LW2 = L::LW2, LN2 = L::LN2, LNR = L::LNR, LNT = L::LNT;
   extern __shared__ double smem[];
   __shared__ int s_tile;
   const int tid = threadIdx.x;
+  double *P = smem;
+  double *G = P + 2 * P_N * LN2;
+  double *Fi = G + (VISC ? 12 * LN1 : 0);
+  double *Fj = Fi + 5 * LN1;
+  double *raw = Fj + 5 * LN1;  // [3][5][NT] own cells then [5][LNR] ring cells, per slot
+  double *pre = raw + 3 * L::RAW;  // [3][2][5][LNT]
   for (;;) {
     if (tid == 0) s_tile = (int)atomicAdd(a.counter, 1u);
     __syncthreads();
@@ -179,117 +191,131 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
     const BlockDev &B = a.blks[T.blk];
     const int tw = T.tw, th = T.th;
     const int W1 = tw + 2, H1 = th + 2, N1 = W1 * H1;
-    const int W2 = tw + 4, N2 = W2 * (th + 4);
     const int nring = 2 * (tw + th);
-    double *P = smem;
-    double *G = P + 2 * P_N * N2;
-    double *Fi = G + (VISC ? 12 * NT : 0);
-    double *Fj = Fi + 5 * NT;
-    double *raw = Fj + 5 * NT;           // [5][NT] own cells, then [5][nring] ring cells
-    double *raw2 = raw + 5 * NT;
-    double *pre = raw2 + 5 * nring;      // [2][5][NT]
     const int v = (int)B.vol;
     const int sJ = B.X, sK = B.X * B.Y;
     const double *Q = a.R[a.qin] + 5 * B.cv;
     const bool col = tid < N1;
     const int ii = tid % W1, jj = tid / W1;
-    const int c2 = (ii + 1) + W2 * (jj + 1);
+    const int c1 = ii + LW1 * jj;
+    const int c2 = (ii + 1) + LW2 * (jj + 1);
     const bool tile = col && ii >= 1 && ii <= tw && jj >= 1 && jj <= th;
+    const int tc = (ii - 1) + tw * (jj - 1);  // this tile cell's index, for the combine staging
     const bool ring_corner = (ii == 0 || ii == W1 - 1) && (jj == 0 || jj == H1 - 1);
     const bool gcol = col && !ring_corner;
     int r2 = -1, x2 = 0, y2 = 0;
     if (tid < nring) {
       int q = tid;
       if (q < th) x2 = 0, y2 = q + 2;
-      else if ((q -= th) < th) x2 = W2 - 1, y2 = q + 2;
+      else if ((q -= th) < th) x2 = tw + 3, y2 = q + 2;
       else if ((q -= th) < tw) x2 = q + 2, y2 = 0;
       else x2 = (q - tw) + 2, y2 = th + 3;
-      r2 = x2 + W2 * y2;
+      r2 = x2 + LW2 * y2;
     }
     const int o1 = (T.j0 + jj + 1) * sJ + (T.i0 + ii + 1);
     const int o2 = (T.j0 + y2) * sJ + (T.i0 + x2);
     auto slot = [](int p) { return p & 1; };
+    auto ring3 = [](int p) { return (p + 6) % 3; };
     auto getP = [&](int s, int r) {
-      const double *Ps = P + s * P_N * N2;
+      const double *Ps = P + s * P_N * LN2 + r;
       CellP c;
-      c.rho = Ps[P_RHO * N2 + r], c.u = Ps[P_U * N2 + r], c.v = Ps[P_V * N2 + r];
-      c.w = Ps[P_W * N2 + r], c.T = Ps[P_T * N2 + r], c.e = Ps[P_E * N2 + r];
+      c.rho = Ps[P_RHO * LN2], c.u = Ps[P_U * LN2], c.v = Ps[P_V * LN2];
+      c.w = Ps[P_W * LN2], c.T = Ps[P_T * LN2], c.e = Ps[P_E * LN2];
       return c;
     };
     auto putP = [&](int s, int r, const CellP &c) {
-      double *Ps = P + s * P_N * N2;
-      Ps[P_RHO * N2 + r] = c.rho, Ps[P_U * N2 + r] = c.u, Ps[P_V * N2 + r] = c.v;
-      Ps[P_W * N2 + r] = c.w, Ps[P_T * N2 + r] = c.T, Ps[P_E * N2 + r] = c.e;
+      double *Ps = P + s * P_N * LN2 + r;
+      Ps[P_RHO * LN2] = c.rho, Ps[P_U * LN2] = c.u, Ps[P_V * LN2] = c.v;
+      Ps[P_W * LN2] = c.w, Ps[P_T * LN2] = c.T, Ps[P_E * LN2] = c.e;
     };
-    // the copies of plane p's Q for this thread's cells (one group in flight)
+    // plane p's Q copies for this thread's cells, into raw slot p mod 3
     auto fetch = [&](int p) {
+      double *rs = raw + ring3(p) * L::RAW;
       const int z = (p + NG) * sK;
       if (col) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(raw + l * NT + tid, Q + l * v + z + o1);
+        for (int l = 0; l < 5; l++) cp8(rs + l * NT + tid, Q + l * v + z + o1);
       }
       if (r2 >= 0) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(raw2 + l * nring + tid, Q + l * v + z + o2);
+        for (int l = 0; l < 5; l++) cp8(rs + 5 * NT + l * LNR + tid, Q + l * v + z + o2);
       }
     };
+    // plane p's combine registers for a tile cell, into pre slot p mod 3
+    const long long cbase = 5 * B.cv + o1;
+    const double *pre0 = a.prep[0] ? a.prep[0] + cbase : nullptr;
+    const double *pre1 = a.prep[1] ? a.prep[1] + cbase : nullptr;
     auto fetch_pre = [&](int p) {
       if (!tile) return;
-      const long long base = 5 * B.cv + (p + NG) * sK + o1;
-      for (int m = 0; m < a.npre; m++) {
-        const double *R = a.R[a.pre[m]] + base;
+      double *ps = pre + ring3(p) * L::PRE + tc;
+      const int z = (p + NG) * sK;
+      if (pre0) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(pre + (m * 5 + l) * NT + tid, R + l * v);
+        for (int l = 0; l < 5; l++) cp8(ps + l * LNT, pre0 + z + l * v);
+      }
+      if (pre1) {
+#pragma unroll
+        for (int l = 0; l < 5; l++) cp8(ps + (5 + l) * LNT, pre1 + z + l * v);
       }
     };
-    auto own_raw = [&]() {
-      return prim_of(raw[0 * NT + tid], raw[1 * NT + tid], raw[2 * NT + tid], raw[3 * NT + tid], raw[4 * NT + tid]);
+    // a slot no register fills holds zeros, so its zero weight adds nothing
+    if (!pre1 && tile)
+      for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int l = 0; l < 5; l++) pre[q * L::PRE + (5 + l) * LNT + tc] = 0.0;
+    if (!pre0 && tile)
+      for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int l = 0; l < 5; l++) pre[q * L::PRE + l * LNT + tc] = 0.0;
+    auto own_raw = [&](int p) {
+      const double *rs = raw + ring3(p) * L::RAW + tid;
+      return prim_of(rs[0 * NT], rs[1 * NT], rs[2 * NT], rs[3 * NT], rs[4 * NT]);
     };
-    auto ring_raw = [&]() {
-      return prim_of(raw2[0 * nring + tid], raw2[1 * nring + tid], raw2[2 * nring + tid], raw2[3 * nring + tid],
-                     raw2[4 * nring + tid]);
+    auto ring_raw = [&](int p) {
+      const double *rs = raw + ring3(p) * L::RAW + 5 * NT + tid;
+      return prim_of(rs[0 * LNR], rs[1 * LNR], rs[2 * LNR], rs[3 * LNR], rs[4 * LNR]);
     };
     auto putG = [&](const double *g) {
 #pragma unroll
-      for (int q = 0; q < 12; q++) G[q * NT + tid] = g[q];
+      for (int q = 0; q < 12; q++) G[q * LN1 + c1] = g[q];
     };
-    // gradients of this column at a plane whose neighbours are in slot s,
-    // with the column's own cells below and above given
     auto grad_col = [&](int s, const CellP &below, const CellP &above, double *g) {
-      grad_u(B, getP(s, c2 - 1), getP(s, c2 + 1), getP(s, c2 - W2), getP(s, c2 + W2), below, above, g);
+      grad_u(B, getP(s, c2 - 1), getP(s, c2 + 1), getP(s, c2 - LW2), getP(s, c2 + LW2), below, above, g);
     };
 
     const int k0 = T.k0, k1 = T.k1;
-    // prelude: planes k0 and k0+1 in shared, the gradients of k0 in shared,
-    // the k face below k0 in registers; plane k0+2 and plane k0's combine
-    // registers in flight
+    // prelude: the copies of planes k0-2 .. k0 go out together; each is
+    // turned into cell values as it lands while the next copies go out
     CellP pm2{}, pm1{}, p0{}, p1{};
     fetch(k0 - 2);
     cp_commit();
-    cp_wait<0>();
-    if (col) pm2 = own_raw();
     fetch(k0 - 1);
     cp_commit();
-    cp_wait<0>();
-    if (col) putP(slot(k0 - 1), c2, pm1 = own_raw());
-    if (r2 >= 0) putP(slot(k0 - 1), r2, ring_raw());
     fetch(k0);
     cp_commit();
-    cp_wait<0>();
-    if (col) putP(slot(k0), c2, p0 = own_raw());
-    if (r2 >= 0) putP(slot(k0), r2, ring_raw());
+    cp_wait<2>();
+    if (col) pm2 = own_raw(k0 - 2);
     fetch(k0 + 1);
+    cp_commit();
+    cp_wait<2>();
+    if (col) putP(slot(k0 - 1), c2, pm1 = own_raw(k0 - 1));
+    if (r2 >= 0) putP(slot(k0 - 1), r2, ring_raw(k0 - 1));
+    fetch(k0 + 2);
+    fetch_pre(k0);
+    cp_commit();
+    cp_wait<2>();
+    if (col) putP(slot(k0), c2, p0 = own_raw(k0));
+    if (r2 >= 0) putP(slot(k0), r2, ring_raw(k0));
+    if (k0 + 3 <= k1 + 1) fetch(k0 + 3);
+    if (k0 + 1 < k1) fetch_pre(k0 + 1);
     cp_commit();
     __syncthreads();
     double gbelow[12];
     if (VISC && tile) grad_col(slot(k0 - 1), pm2, p0, gbelow);
-    cp_wait<0>();
+    cp_wait<2>();
     __syncthreads();
-    if (col) putP(slot(k0 + 1), c2, p1 = own_raw());
-    if (r2 >= 0) putP(slot(k0 + 1), r2, ring_raw());
-    fetch(k0 + 2);
-    fetch_pre(k0);
-    cp_commit();
+    if (col) putP(slot(k0 + 1), c2, p1 = own_raw(k0 + 1));
+    if (r2 >= 0) putP(slot(k0 + 1), r2, ring_raw(k0 + 1));
     __syncthreads();
     double Fk[5];
     {
@@ -302,39 +328,48 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
     }
     __syncthreads();
     const double dt = *a.dt;
+    const double c00 = a.cw[0][0], c01 = a.cw[0][1], c02 = a.cw[0][2] * dt;
+    const double c10 = a.cw[1][0], c11 = a.cw[1][1], c12 = a.cw[1][2] * dt, c13 = a.cw[1][3];
+    double *const out0 = a.outp[0], *const out1 = a.outp[1];
+    const bool wr0 = a.write[0] && out0, wr1 = a.write[1] && out1;
 
+    // in flight at the top of step k: {plane k+2, combine registers of k},
+    // {plane k+3, combine registers of k+1}
     for (int k = k0; k < k1; k++) {
       const int s0 = slot(k), s1 = slot(k + 1);
+      // 0. the copies of plane k+4 and of plane k+2's combine registers go
+      //    out: their slots held plane k+1 and k-1, used up last step
+      if (k + 4 <= k1 + 1) fetch(k + 4);
+      if (k + 2 < k1) fetch_pre(k + 2);
+      cp_commit();
       // 1. this column's low i and j faces at plane k
       if (col && jj >= 1 && jj <= th && ii >= 1) {
         double F[5], gl[12], gr[12];
         if (VISC) {
 #pragma unroll
-          for (int q = 0; q < 12; q++) gl[q] = G[q * NT + tid - 1], gr[q] = G[q * NT + tid];
+          for (int q = 0; q < 12; q++) gl[q] = G[q * LN1 + c1 - 1], gr[q] = G[q * LN1 + c1];
         }
         face_u<0, VISC>(B, getP(s0, c2 - 1), getP(s0, c2), gl, gr, F);
 #pragma unroll
-        for (int l = 0; l < 5; l++) Fi[l * NT + tid] = F[l];
+        for (int l = 0; l < 5; l++) Fi[l * LN1 + c1] = F[l];
       }
       if (col && ii >= 1 && ii <= tw && jj >= 1) {
         double F[5], gl[12], gr[12];
         if (VISC) {
 #pragma unroll
-          for (int q = 0; q < 12; q++) gl[q] = G[q * NT + tid - W1], gr[q] = G[q * NT + tid];
+          for (int q = 0; q < 12; q++) gl[q] = G[q * LN1 + c1 - LW1], gr[q] = G[q * LN1 + c1];
         }
-        face_u<1, VISC>(B, getP(s0, c2 - W2), getP(s0, c2), gl, gr, F);
+        face_u<1, VISC>(B, getP(s0, c2 - LW2), getP(s0, c2), gl, gr, F);
 #pragma unroll
-        for (int l = 0; l < 5; l++) Fj[l * NT + tid] = F[l];
+        for (int l = 0; l < 5; l++) Fj[l * LN1 + c1] = F[l];
       }
       // 2. plane k+2 and plane k's combine registers have landed
-      cp_wait<0>();
+      cp_wait<2>();
       CellP p2{}, p2r{};
-      if (col) p2 = own_raw();
-      if (r2 >= 0) p2r = ring_raw();
+      if (col) p2 = own_raw(k + 2);
+      if (r2 >= 0) p2r = ring_raw(k + 2);
       __syncthreads();
-      // 3. the next copies go out
-      if (k + 3 <= k1 + 1) fetch(k + 3);
-      // 4. the gradients of plane k+1, the k face above k, dQ and the combines
+      // 3. the gradients of plane k+1, the k face above k, dQ and the combines
       const CellP pk = col ? getP(s0, c2) : CellP{};
       const CellP pk1 = col ? getP(s1, c2) : CellP{};
       double gup[12];
@@ -342,41 +377,28 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
       if (tile) {
         double Fkh[5], gk[12];
 #pragma unroll
-        for (int q = 0; q < 12; q++) gk[q] = VISC ? G[q * NT + tid] : 0.0;
+        for (int q = 0; q < 12; q++) gk[q] = VISC ? G[q * LN1 + c1] : 0.0;
         face_u<2, VISC>(B, pk, pk1, gk, gup, Fkh);
         const double dJ = B.detJinv;
         double dQ[5];
 #pragma unroll
         for (int l = 0; l < 5; l++)
-          dQ[l] = (Fi[l * NT + tid] + Fj[l * NT + tid] + Fk[l] - Fi[l * NT + tid + 1] - Fj[l * NT + tid + W1] - Fkh[l]) * dJ;
-        const long long base = 5 * B.cv + (k + NG) * sK + o1;
-        double first[5];
+          dQ[l] = (Fi[l * LN1 + c1] + Fj[l * LN1 + c1] + Fk[l] - Fi[l * LN1 + c1 + 1] - Fj[l * LN1 + c1 + LW1] - Fkh[l]) * dJ;
+        // the combines in their fixed form (no branch, no register lookup)
+        const long long at = cbase + (k + NG) * sK;
+        const double *pk3 = pre + ring3(k) * L::PRE + tc;
 #pragma unroll
-        for (int m = 0; m < 2; m++) {
-          if (m >= a.ncomb) break;
-          const FusedCombine &cb = a.combp[m];
-          double *out = a.R[cb.out] + base;
-#pragma unroll
-          for (int l = 0; l < 5; l++) {
-            auto val = [&](int n) {
-              const int s = cb.src[n];
-              return s == -1 ? dQ[l] : s == -2 ? first[l] : pre[(s * 5 + l) * NT + tid];
-            };
-            auto term = [&](int n) { return (cb.step && n == cb.nterms - 1) ? cb.w[n] * dt * val(n) : cb.w[n] * val(n); };
-            double acc = term(0);
-#pragma unroll
-            for (int n = 1; n < 4; n++)
-              if (n < cb.nterms) acc = acc + term(n);
-            if (m == 0) first[l] = acc;
-            if (cb.write) out[l * v] = acc;
-          }
+        for (int l = 0; l < 5; l++) {
+          const double p0 = pk3[l * LNT], p1 = pk3[(5 + l) * LNT];
+          const double o0 = c00 * p0 + c01 * p1 + c02 * dQ[l];
+          const double o1v = c10 * p0 + c11 * p1 + c12 * dQ[l] + c13 * o0;
+          if (wr0) out0[at + l * v] = o0;
+          if (wr1) out1[at + l * v] = o1v;
         }
 #pragma unroll
         for (int l = 0; l < 5; l++) Fk[l] = Fkh[l];
       }
-      if (k + 1 < k1) fetch_pre(k + 1);
-      cp_commit();
-      // 5. plane k+2 takes plane k's slot, the k+1 gradients plane k's
+      // 4. plane k+2 takes plane k's slot, the k+1 gradients plane k's
       if (col) putP(s0, c2, p2);
       if (r2 >= 0) putP(s0, r2, p2r);
       if (VISC && gcol) putG(gup);
@@ -386,9 +408,9 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
   }
 }
 
-template <int NT>
-inline size_t fused2_smem(int tw, int th, bool visc) {
-  return sizeof(double) * F2Layout<NT>::doubles(tw, th, visc);
+template <int NT, int TW, int TH>
+inline size_t fused2_smem(bool visc) {
+  return sizeof(double) * F2L<NT, TW, TH>::doubles(visc);
 }
 
 }  // namespace pgb

@@ -92,7 +92,7 @@ struct pgb_case {
   bool uniform_done = false;
   bool use_v2 = false;  // every block uniform: the uniform-metric fused kernel
   int v2_ctas = 1;      // its resident CTAs per SM
-  int v2_nt = 256, v2_minb = 2;  // its threads per CTA and launch-bound CTAs per SM
+  int v2 = 0;           // its instance: threads per CTA, launch bound, tile layout
   // register mapping: logical -> physical
   std::vector<int> phys_of, canonical;
   int period = 1, phase = 0;
@@ -244,23 +244,33 @@ void default_tile(HostBlock &B) {
   B.kchunk = (B.nz + 1) / 2;
 }
 
-// the uniform kernel's default: one thread per column of the tile and its
-// ring, 256 of them; i cut evenly in pieces of at most 30
-void default_tile2(HostBlock &B, int nt) {
-  const int wmax = nt >= 256 ? 30 : 14;
-  const int pi = (B.nx + wmax - 1) / wmax;
-  const int tw = (B.nx + pi - 1) / pi;
-  int th = std::max(1, nt / (tw + 2) - 2);
-  th = std::min(th, B.ny);
-  const int pj = (B.ny + th - 1) / th;
-  th = (B.ny + pj - 1) / pj;
-  B.tw = tw, B.th = th;
-  B.kchunk = (B.nz + 1) / 2;
+// The uniform kernel's instances: threads per CTA, the CTAs per SM its
+// registers are bounded for, and the largest tile its shared layout holds.
+struct V2Inst {
+  int nt, minb, tw, th;
+  const void *fvisc, *feuler;
+  size_t smvisc, smeuler;
+};
+#define PGB_V2(NT, MB, TW, TH)                                                                    \
+  V2Inst{NT, MB, TW, TH, (const void *)k_fused2<true, NT, MB, TW, TH>,                             \
+         (const void *)k_fused2<false, NT, MB, TW, TH>, fused2_smem<NT, TW, TH>(true),             \
+         fused2_smem<NT, TW, TH>(false)}
+const V2Inst kV2[] = {PGB_V2(256, 1, 24, 7), PGB_V2(256, 1, 30, 6), PGB_V2(128, 2, 14, 6)};
+#undef PGB_V2
+constexpr int kNV2 = sizeof(kV2) / sizeof(kV2[0]);
+
+// the uniform kernel's default tile: i and j cut evenly in pieces the layout holds
+void default_tile2(HostBlock &B, const V2Inst &v) {
+  const int pi = (B.nx + v.tw - 1) / v.tw;
+  const int pj = (B.ny + v.th - 1) / v.th;
+  B.tw = (B.nx + pi - 1) / pi;
+  B.th = (B.ny + pj - 1) / pj;
+  B.kchunk = (B.nz + 2) / 3;
 }
 
 bool tile_fits(const pgb_case *c, int tw, int th) {
   if (!c->use_v2) return tw * th <= FUSED_THREADS;
-  return (tw + 2) * (th + 2) <= c->v2_nt && 2 * (tw + th) <= c->v2_nt;
+  return tw <= kV2[c->v2].tw && th <= kV2[c->v2].th;
 }
 
 int build_tiles(pgb_case *c) {
@@ -270,11 +280,10 @@ int build_tiles(pgb_case *c) {
   for (int b = 0; b < (int)c->blocks.size(); b++) {
     HostBlock &B = c->blocks[b];
     if (B.tw <= 0 || !tile_fits(c, B.tw, B.th)) {
-      if (c->use_v2) default_tile2(B, c->v2_nt);
+      if (c->use_v2) default_tile2(B, kV2[c->v2]);
       else default_tile(B);
     }
-    const size_t need = !c->use_v2 ? fused_smem(B.tw, B.th, visc)
-                        : c->v2_nt == 128 ? fused2_smem<128>(B.tw, B.th, visc) : fused2_smem<256>(B.tw, B.th, visc);
+    const size_t need = !c->use_v2 ? fused_smem(B.tw, B.th, visc) : visc ? kV2[c->v2].smvisc : kV2[c->v2].smeuler;
     smem = std::max(smem, need);
     for (int k0 = 0; k0 < B.nz; k0 += B.kchunk)
       for (int j0 = 0; j0 < B.ny; j0 += B.th)
@@ -505,19 +514,10 @@ void mark(pgb_case *c, int kind, int &count) {
   c->tkind.push_back(kind);
 }
 
-// the uniform kernel of the case's shape: threads per CTA and launch bound
+// the uniform kernel of the case's instance
 const void *v2_kernel(const pgb_case *c) {
-  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
-#define PGB_V2(NT, MB)                                                                      \
-  if (c->v2_nt == NT && c->v2_minb == MB)                                                   \
-    return visc ? (const void *)k_fused2<true, NT, MB> : (const void *)k_fused2<false, NT, MB>;
-  PGB_V2(256, 1)
-  PGB_V2(256, 2)
-  PGB_V2(128, 2)
-  PGB_V2(128, 3)
-  PGB_V2(128, 4)
-#undef PGB_V2
-  return nullptr;
+  if (c->v2 < 0 || c->v2 >= kNV2) return nullptr;
+  return c->phys.simulator == PGB_NAVIER_STOKES ? kV2[c->v2].fvisc : kV2[c->v2].feuler;
 }
 
 // one stage of the fused path
@@ -551,6 +551,31 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
       a.combp[m].src[n] = slot;
     }
   }
+  // the fixed form: each combine's terms onto (p0, p1, dt dQ, out0), in order
+  for (int m = 0; m < 2; m++) {
+    for (int q = 0; q < 4; q++) a.cw[m][q] = 0.0;
+    a.outp[m] = nullptr;
+    a.write[m] = 0;
+  }
+  for (int m = 0; m < p.ncomb; m++) {
+    const FusedCombine &cb = a.combp[m];
+    int last = -1;
+    for (int n = 0; n < cb.nterms; n++) {
+      const int sidx = cb.src[n];
+      const int q = sidx == -1 ? 2 : sidx == -2 ? 3 : sidx;
+      // the form sums p0, p1, dQ, out0 in that order: a combine whose terms
+      // come in another order, or that reads a slot twice, has no fixed form
+      if (q <= last || (q == 3 && m == 0) || (q == 2 && !(cb.step && n == cb.nterms - 1)))
+        return fail(PGB_ERR_STATE, "a stage whose combines the uniform kernel's fixed form does not take");
+      if (q < 2 && cb.step && n == cb.nterms - 1)
+        return fail(PGB_ERR_STATE, "a stage whose dt falls on a register the fixed form does not scale");
+      last = q;
+      a.cw[m][q] = cb.w[n];
+    }
+    a.outp[m] = c->d_reg[cb.out];
+    a.write[m] = cb.write;
+  }
+  for (int q = 0; q < 2; q++) a.prep[q] = q < a.npre ? c->d_reg[a.pre[q]] : nullptr;
   a.dt = c->d_dt;
   // the stencil register's halo first
   k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne);
@@ -567,7 +592,7 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
     const void *fn = v2_kernel(c);
     if (!fn) return fail(PGB_ERR_ARG, "no uniform kernel of that shape");
     void *args[] = {&a};
-    CK(cudaLaunchKernel(fn, dim3(grid), dim3(c->v2_nt), args, sm, c->stream));
+    CK(cudaLaunchKernel(fn, dim3(grid), dim3(kV2[c->v2].nt), args, sm, c->stream));
     mark(c, K_FUSED, count);
     return PGB_OK;
   }
@@ -591,7 +616,7 @@ int fused_attrs(pgb_case *c) {
     if (!fn) return fail(PGB_ERR_ARG, "no uniform kernel of that shape");
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     int n = 1;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, c->v2_nt, c->fused_smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kV2[c->v2].nt, c->fused_smem));
     c->v2_ctas = std::max(1, n);
     return PGB_OK;
   }
@@ -1232,26 +1257,40 @@ int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk) {
   if (!c || blk < 0 || blk >= (int)c->blocks.size() || !tw || !th || !kchunk) return fail(PGB_ERR_ARG, "bad argument");
   HostBlock B = c->blocks[blk];
   if (B.tw <= 0) {
-    if (c->use_v2) default_tile2(B, c->v2_nt);
+    if (c->use_v2) default_tile2(B, kV2[c->v2]);
     else default_tile(B);
   }
   *tw = B.tw, *th = B.th, *kchunk = B.kchunk;
   return PGB_OK;
 }
 
-int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks) {
+int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks, int width) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
-  const int nt0 = c->v2_nt, mb0 = c->v2_minb;
-  c->v2_nt = threads, c->v2_minb = minblocks;
-  if (!v2_kernel(c)) {
-    c->v2_nt = nt0, c->v2_minb = mb0;
-    return fail(PGB_ERR_ARG, "threads x minblocks: 256 x 1, 256 x 2, 128 x 2, 128 x 3 or 128 x 4");
+  int pick = -1;
+  for (int q = 0; q < kNV2; q++)
+    if (kV2[q].nt == threads && kV2[q].minb == minblocks && kV2[q].tw == width) pick = q;
+  if (pick < 0) {
+    std::string have;
+    for (int q = 0; q < kNV2; q++)
+      have += " " + std::to_string(kV2[q].nt) + "x" + std::to_string(kV2[q].minb) + "x" + std::to_string(kV2[q].tw);
+    return fail(PGB_ERR_ARG, "no uniform kernel of that shape; threads x minblocks x width:" + have);
   }
-  if (threads != nt0)
+  if (pick != c->v2)
     for (auto &B : c->blocks) B.tw = 0;
+  c->v2 = pick;
   c->tiles_dirty = true;
   for (auto &g : c->graph)
     if (g) cudaGraphExecDestroy(g), g = nullptr;
+  return PGB_OK;
+}
+
+int pgb_fused_shapes(int *shapes, int cap, int *n) {
+  if (!n || (cap > 0 && !shapes)) return fail(PGB_ERR_ARG, "null argument");
+  *n = kNV2;
+  for (int q = 0; q < kNV2 && q < cap; q++) {
+    shapes[4 * q] = kV2[q].nt, shapes[4 * q + 1] = kV2[q].minb;
+    shapes[4 * q + 2] = kV2[q].tw, shapes[4 * q + 3] = kV2[q].th;
+  }
   return PGB_OK;
 }
 
