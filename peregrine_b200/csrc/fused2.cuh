@@ -342,26 +342,29 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
       if (k + 4 <= k1 + 1) fetch(k + 4);
       if (k + 2 < k1) fetch_pre(k + 2);
       cp_commit();
-      // 1. this column's low i and j faces at plane k
-      if (col && jj >= 1 && jj <= th && ii >= 1) {
-        double F[5], gl[12], gr[12];
+      // 1. this column's low i and j faces at plane k, both in one straight
+      //    run so their arithmetic interleaves; a column with no such face
+      //    (the ring) computes one from its neighbour anyway and drops it
+      if (col) {
+        const int li = ii >= 1 ? 1 : 0, lj = jj >= 1 ? LW1 : 0;
+        const int li2 = ii >= 1 ? 1 : 0, lj2 = jj >= 1 ? LW2 : 0;
+        double Fa[5], Fb[5], gli[12], glj[12], gr[12];
         if (VISC) {
 #pragma unroll
-          for (int q = 0; q < 12; q++) gl[q] = G[q * LN1 + c1 - 1], gr[q] = G[q * LN1 + c1];
+          for (int q = 0; q < 12; q++)
+            gli[q] = G[q * LN1 + c1 - li], glj[q] = G[q * LN1 + c1 - lj], gr[q] = G[q * LN1 + c1];
         }
-        face_u<0, VISC>(B, getP(s0, c2 - 1), getP(s0, c2), gl, gr, F);
+        const CellP me = getP(s0, c2);
+        face_u<0, VISC>(B, getP(s0, c2 - li2), me, gli, gr, Fa);
+        face_u<1, VISC>(B, getP(s0, c2 - lj2), me, glj, gr, Fb);
+        if (jj >= 1 && jj <= th && ii >= 1) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) Fi[l * LN1 + c1] = F[l];
-      }
-      if (col && ii >= 1 && ii <= tw && jj >= 1) {
-        double F[5], gl[12], gr[12];
-        if (VISC) {
-#pragma unroll
-          for (int q = 0; q < 12; q++) gl[q] = G[q * LN1 + c1 - LW1], gr[q] = G[q * LN1 + c1];
+          for (int l = 0; l < 5; l++) Fi[l * LN1 + c1] = Fa[l];
         }
-        face_u<1, VISC>(B, getP(s0, c2 - LW2), getP(s0, c2), gl, gr, F);
+        if (ii >= 1 && ii <= tw && jj >= 1) {
 #pragma unroll
-        for (int l = 0; l < 5; l++) Fj[l * LN1 + c1] = F[l];
+          for (int l = 0; l < 5; l++) Fj[l * LN1 + c1] = Fb[l];
+        }
       }
       // 2. plane k+2 and plane k's combine registers have landed
       cp_wait<2>();
