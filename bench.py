@@ -235,7 +235,7 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
@@ -302,14 +302,15 @@ def main():
     bytes_per_launch = [ncells * 8 * NE * r for r in STAGE_REGS]
     achieved = float(np.mean([b / (t / 1e3) / 1e9 for b, t in zip(bytes_per_launch, per_stage)]))
     peak, peak_kind = peaks()
+    # the ncu-measured DRAM bytes per cell-stage of the fused kernel (profiles/),
+    # as bytes per launch of this workload
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "fused_traffic.json")
-    if os.path.exists(tpath):
+    tpath = os.path.join(ROOT, "profiles", "fused_traffic.txt")
+    if os.path.exists(tpath) and CELLS == 128:
         with open(tpath) as f:
-            tr = json.load(f)
-        traffic = tr.get("bytes_per_cell_stage", None)
-        if traffic is not None:
-            traffic = traffic * ncells
+            for line in f:
+                if line.startswith("bytes_per_cell_stage"):
+                    traffic = float(line.split()[1]) * ncells
 
     from peregrine_b200 import native
 
@@ -351,7 +352,8 @@ def main():
             "per_block": per_block,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_fused1 (one RK stage)", "kernel_ms_per_stage": per_stage,
+                         "kernel": "k_fused2 (fused RK stage, uniform metrics)" if all(mb.uniform(n) for n in range(len(mb.blocks)))
+                         else "k_fused1 (fused RK stage, metric arrays)", "kernel_ms_per_stage": per_stage,
                          "halo_ms_per_stage": float(np.mean(halo)) if halo else None,
                          "algorithmic_bytes_per_cell_stage": 170},
             "cpu_baseline": cpu,
