@@ -43,7 +43,7 @@ enum {
 /* physics selectors: the config's names (peregrine/config.py:12-98) */
 enum { PGB_EULER = 0, PGB_NAVIER_STOKES = 1 };
 enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1 };
-enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2 };
+enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2, PGB_FLUX_AUSMUP = 3 };
 enum { PGB_RECON_CONSTANT = 0, PGB_RECON_MUSCL = 1 };
 enum { PGB_TRANS_NONE = 0, PGB_TRANS_CONSTANT = 1, PGB_TRANS_KINETIC = 2 };
 /* the launch paths */
@@ -68,7 +68,7 @@ typedef struct {
   int eos;        /* PGB_EOS_* */
   int primary;    /* PGB_FLUX_* */
   int recon;      /* PGB_RECON_* */
-  int limiter;    /* 0 none, 1 koren, 2 minmod, 3 mc, 4 superbee, 5 vanleer */
+  int limiter;    /* with PGB_RECON_MUSCL: 1 koren, 2 minmod, 3 mc, 4 superbee, 5 vanleer */
   int trans;      /* PGB_TRANS_* */
   int ns;         /* species, >= 1 */
   int nregs;      /* Runge-Kutta registers the integrator needs, dQ included */

@@ -31,7 +31,7 @@ class OCase(ctypes.Structure):
                 ("alpha", ctypes.c_double)] + \
                [(n, ctypes.POINTER(ctypes.c_double)) for n in
                 ("Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0", "kappa0", "MWqinv", "wilkepair", "lewis")] + \
-               [("Ru", ctypes.c_double), ("skip_adv", ctypes.c_int)]
+               [("Ru", ctypes.c_double), ("skip_adv", ctypes.c_int), ("recon", ctypes.c_int), ("limiter", ctypes.c_int)]
 
 
 class OBlock(ctypes.Structure):
@@ -50,6 +50,7 @@ def _lib():
     lib.oracle_fromprims.restype = ctypes.c_int
     lib.oracle_combine.restype = ctypes.c_int
     lib.oracle_kepaec_faces.restype = ctypes.c_int
+    lib.oracle_advective_faces.restype = ctypes.c_int
     return lib
 
 
@@ -152,7 +153,11 @@ class Oracle:
     per block of the arrays ``peregrine_b200.grid.metrics`` makes.
     """
 
-    def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0):
+    PRIMARY = {"kepaec": 0, "hllc": 1, "rusanov": 2, "ausmup": 3}
+    LIMITERS = {None: 0, "koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
+
+    def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0, primary="kepaec",
+                 recon="constant", limiter=None):
         """constants: the mixture's tables; blocks/metrics may be empty for face-only use."""
         self.lib = _lib()
         self.ns, self.ne = ns, 4 + ns
@@ -162,7 +167,9 @@ class Oracle:
         self._tables = {}
         c = OCase()
         c.simulator = 1 if simulator == "navier-stokes" else 0
-        c.primary = 0
+        c.primary = self.PRIMARY[primary]
+        c.recon = 1 if recon == "muscl" else 0
+        c.limiter = self.LIMITERS[limiter]
         c.ns = ns
         c.alpha = alpha
         c.Ru = float(constants["Ru"])
@@ -226,6 +233,14 @@ class Oracle:
             raise RuntimeError(f"oracle_rhs: {rc}")
         if faces:
             return [fl[3 * b:3 * b + 3] for b in range(len(self.blocks))]
+
+    def advective_faces(self, QLL, QL, QR, QRR, S):
+        """The advective flux on independent faces from their four cells' Q."""
+        Q4 = np.ascontiguousarray(np.stack([QLL, QL, QR, QRR]), dtype=np.float64)
+        S = np.ascontiguousarray(S, dtype=np.float64)
+        F = np.zeros_like(Q4[0])
+        self.lib.oracle_advective_faces(ctypes.byref(self.case), ctypes.c_long(S.shape[0]), _ptr(Q4), _ptr(S), _ptr(F))
+        return F
 
     def kepaec_faces(self, QL, QR, S):
         """kepaec on independent faces, each side's state from its Q."""

@@ -22,7 +22,7 @@
 extern "C" {
 
 enum { O_EULER = 0, O_NAVSTOKES = 1 };
-enum { O_KEPAEC = 0, O_HLLC = 1, O_RUSANOV = 2 };
+enum { O_KEPAEC = 0, O_HLLC = 1, O_RUSANOV = 2, O_AUSMUP = 3 };
 
 struct OCase {
   int simulator;   // O_EULER / O_NAVSTOKES
@@ -34,6 +34,8 @@ struct OCase {
   const double *mu0, *kappa0, *MWqinv, *wilkepair, *lewis;
   double Ru;
   int skip_adv;    // 1: the face fluxes hold the diffusive flux alone (a test's view)
+  int recon;       // 0 constant, 1 muscl
+  int limiter;     // 1 koren, 2 minmod, 3 mc, 4 superbee, 5 vanleer
 };
 
 struct OBlock {
@@ -214,6 +216,185 @@ void kepaec(const OCase &c, const Side &L, const Side &R, const double *QL, cons
   const double ef = 2.0 * thL * thR / (thL + thR) + 0.5 * ((L.s.e - thL) + (R.s.e - thR));
   F[4] = ef * C + Kj + Pj;
   for (int n = 0; n < c.ns - 1; n++) F[5 + n] = 0.5 * (QR[5 + n] / QR[0] + QL[5 + n] / QL[0]) * C;
+}
+
+// cpg frompT (simulator/mixture/eos/cpg/kernels/eos.mako:17-27)
+State frompT(const OCase &c, double p, double T, const double *Y) {
+  Mom mom = mixmom(c, [&](int n) { return Y[n]; });
+  State s;
+  const double cv = mom.cp - mom.R;
+  s.p = p;
+  s.T = T;
+  s.rho = p / (mom.R * T);
+  s.rhoinv = 1.0 / s.rho;
+  s.e = cv * T + mom.h298;
+  s.cp = mom.cp;
+  s.gamma = mom.cp / cv;
+  s.c = std::sqrt(s.gamma * mom.R * T);
+  return s;
+}
+
+// b phi(a / b) of the limiters, b > 0 (simulator/euler/kernels/flux/recon/{koren,minmod,mc,superbee,vanleer}.mako)
+double limiter(int which, double a, double b) {
+  switch (which) {
+    case 1: return std::fmax(0.0, std::fmin(std::fmin(2.0 * a, (2.0 * b + a) * (1.0 / 3.0)), 2.0 * b));
+    case 2: return std::fmax(0.0, std::fmin(b, a));
+    case 3: return std::fmax(0.0, std::fmin(std::fmin(2.0 * a, (b + a) * 0.5), 2.0 * b));
+    case 4: return std::fmax(0.0, std::fmax(std::fmin(2.0 * a, b), std::fmin(a, 2.0 * b)));
+    default: return (a + std::fabs(a)) * b / (b + std::fabs(a));
+  }
+}
+
+// the limited slope across a face (simulator/euler/kernels/flux/recon/muscl.mako:5-13)
+double phi(int which, double dm, double dp) {
+  double ph = 0.0;
+  if (dp != 0.0) {
+    const double s = std::copysign(1.0, dp), a = s * dm, b = std::fabs(dp);
+    ph = s * limiter(which, a, b);
+  }
+  return ph;
+}
+
+// MUSCL sides (simulator/euler/kernels/flux/recon/muscl.mako:15-51): p, T, Y
+// and the velocity limited, each side's state from its p, T, Y by frompT
+void muscl(const OCase &c, const double *QLL, const double *QL, const double *QR, const double *QRR,
+           const State &sLL, const State &sL, const State &sR, const State &sRR, Side &L, Side &R,
+           double *YL, double *YR) {
+  const int lim = c.limiter, ns = c.ns;
+  auto left = [&](double vLL, double vL, double vR) { return vL + 0.5 * phi(lim, vL - vLL, vR - vL); };
+  auto right = [&](double vL, double vR, double vRR) { return vR - 0.5 * phi(lim, vRR - vR, vR - vL); };
+  const double riLL = sLL.rhoinv, riL = sL.rhoinv, riR = sR.rhoinv, riRR = sRR.rhoinv;
+  const double pL = left(sLL.p, sL.p, sR.p), pR = right(sL.p, sR.p, sRR.p);
+  const double TL = left(sLL.T, sL.T, sR.T), TR = right(sL.T, sR.T, sRR.T);
+  for (int n = 0; n < ns - 1; n++) {
+    YL[n] = left(QLL[5 + n] * riLL, QL[5 + n] * riL, QR[5 + n] * riR);
+    YR[n] = right(QL[5 + n] * riL, QR[5 + n] * riR, QRR[5 + n] * riRR);
+  }
+  L.s = frompT(c, pL, TL, YL);
+  L.u = left(QLL[1] * riLL, QL[1] * riL, QR[1] * riR);
+  L.v = left(QLL[2] * riLL, QL[2] * riL, QR[2] * riR);
+  L.w = left(QLL[3] * riLL, QL[3] * riL, QR[3] * riR);
+  R.s = frompT(c, pR, TR, YR);
+  R.u = right(QL[1] * riL, QR[1] * riR, QRR[1] * riRR);
+  R.v = right(QL[2] * riL, QR[2] * riR, QRR[2] * riRR);
+  R.w = right(QL[3] * riL, QR[3] * riR, QRR[3] * riRR);
+}
+
+// HLLC with Davis's outer wave speeds (simulator/euler/kernels/flux/function/hllc.mako:2-43)
+void hllc(const OCase &c, const Side &L, const Side &R, const double *YL, const double *YR, const double *S,
+          double *F) {
+  const double area = std::sqrt(((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2])));
+  const double nx = S[0] / area, ny = S[1] / area, nz = S[2] / area;
+  const double unL = ((L.u) * (S[0]) + (L.v) * (S[1]) + (L.w) * (S[2])) / area;
+  const double unR = ((R.u) * (S[0]) + (R.v) * (S[1]) + (R.w) * (S[2])) / area;
+  const double SL = unL - L.s.c, SR = unR + R.s.c;
+  const double Sstar = (R.s.p - L.s.p + L.s.rho * unL * (SL - unL) - R.s.rho * unR * (SR - unR)) /
+                       (L.s.rho * (SL - unL) - R.s.rho * (SR - unR));
+  bool left, star;
+  if (SL >= 0.0) left = true, star = false;
+  else if (Sstar >= 0.0) left = true, star = true;
+  else if (SR >= 0.0) left = false, star = true;
+  else left = false, star = false;
+  const Side &X = left ? L : R;
+  const double *Y = left ? YL : YR;
+  const double U = left ? unL : unR, SX = left ? SL : SR;
+  const double et = X.s.e + 0.5 * ((X.u) * (X.u) + (X.v) * (X.v) + (X.w) * (X.w));
+  const double mdot = U * X.s.rho * area;
+  F[0] = mdot;
+  F[1] = mdot * X.u + X.s.p * S[0];
+  F[2] = mdot * X.v + X.s.p * S[1];
+  F[3] = mdot * X.w + X.s.p * S[2];
+  F[4] = mdot * et + U * X.s.p * area;
+  for (int n = 0; n < c.ns - 1; n++) F[5 + n] = mdot * Y[n];
+  if (star) {
+    const double rhostar = X.s.rho * ((SX - U) / (SX - Sstar));
+    const double drho = rhostar - X.s.rho, dU = rhostar * (Sstar - U);
+    const double jump = SX * area;
+    F[0] += jump * drho;
+    F[1] += jump * (drho * X.u + dU * nx);
+    F[2] += jump * (drho * X.v + dU * ny);
+    F[3] += jump * (drho * X.w + dU * nz);
+    F[4] += jump * (drho * et + dU * (Sstar + X.s.p / (X.s.rho * (SX - U))));
+    for (int n = 0; n < c.ns - 1; n++) F[5 + n] += jump * drho * Y[n];
+  }
+}
+
+// Rusanov with Davis's bound on the fastest wave (simulator/euler/kernels/flux/function/rusanov.mako:2-21)
+void rusanov(const OCase &c, const Side &L, const Side &R, const double *YL, const double *YR, const double *S,
+             double *F) {
+  const double area = std::sqrt(((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2])));
+  const double unL = ((L.u) * (S[0]) + (L.v) * (S[1]) + (L.w) * (S[2])) / area;
+  const double unR = ((R.u) * (S[0]) + (R.v) * (S[1]) + (R.w) * (S[2])) / area;
+  const double lam = std::fmax(std::fabs(unL) + L.s.c, std::fabs(unR) + R.s.c) * area;
+  const double UL = unL * area, UR = unR * area;
+  const double rL = L.s.rho, rR = R.s.rho, pL = L.s.p, pR = R.s.p;
+  F[0] = 0.5 * (UR * rR + UL * rL - lam * (rR - rL));
+  F[1] = 0.5 * (UR * rR * R.u + pR * S[0] + UL * rL * L.u + pL * S[0] - lam * (rR * R.u - rL * L.u));
+  F[2] = 0.5 * (UR * rR * R.v + pR * S[1] + UL * rL * L.v + pL * S[1] - lam * (rR * R.v - rL * L.v));
+  F[3] = 0.5 * (UR * rR * R.w + pR * S[2] + UL * rL * L.w + pL * S[2] - lam * (rR * R.w - rL * L.w));
+  const double EL = rL * (L.s.e + 0.5 * ((L.u) * (L.u) + (L.v) * (L.v) + (L.w) * (L.w)));
+  const double ER = rR * (R.s.e + 0.5 * ((R.u) * (R.u) + (R.v) * (R.v) + (R.w) * (R.w)));
+  F[4] = 0.5 * (UR * (ER + pR) + UL * (EL + pL) - lam * (ER - EL));
+  for (int n = 0; n < c.ns - 1; n++) {
+    const double rhoYL = rL * YL[n], rhoYR = rR * YR[n];
+    F[5 + n] = 0.5 * (rhoYR * UR + rhoYL * UL - lam * (rhoYR - rhoYL));
+  }
+}
+
+// AUSM+-up of Liou (2006), cut-off Mach sqrt(0.1) (simulator/euler/kernels/flux/function/ausmup.mako:2-38)
+void ausmup(const OCase &c, const Side &L, const Side &R, const double *YL, const double *YR, const double *S,
+            double *F) {
+  const double area = std::sqrt(((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2]))), invarea = 1.0 / area;
+  const double UL = ((L.u) * (S[0]) + (L.v) * (S[1]) + (L.w) * (S[2])) * invarea;
+  const double UR = ((R.u) * (S[0]) + (R.v) * (S[1]) + (R.w) * (S[2])) * invarea;
+  const double a12 = 0.5 * (R.s.c + L.s.c), inva12 = 1.0 / a12;
+  const double ML = UL * inva12, MR = UR * inva12;
+  const double Mbarsq = 0.5 * (UL * UL + UR * UR) * inva12 * inva12;
+  const double Mco = 0.31622776601683794, Kp = 0.25, Ku = 0.75, sigma = 1.0, beta = 1.0 / 8.0;
+  const double Mo = std::sqrt(std::fmin(1.0, std::fmax(Mbarsq, Mco * Mco)));
+  const double fa = Mo * (2.0 - Mo);
+  const double M1p = 0.5 * (ML + std::fabs(ML)), M1m = 0.5 * (MR - std::fabs(MR));
+  const double M2pL = 0.25 * (ML + 1.0) * (ML + 1.0), M2mL = -0.25 * (ML - 1.0) * (ML - 1.0);
+  const double M2pR = 0.25 * (MR + 1.0) * (MR + 1.0), M2mR = -0.25 * (MR - 1.0) * (MR - 1.0);
+  const double M4p = std::fabs(ML) >= 1.0 ? M1p : M2pL * (1.0 - 16.0 * beta * M2mL);
+  const double M4m = std::fabs(MR) >= 1.0 ? M1m : M2mR * (1.0 + 16.0 * beta * M2pR);
+  const double alpha = 3.0 / 16.0 * (-4.0 + 5.0 * fa * fa);
+  const double p5p = std::fabs(ML) >= 1.0 ? (ML > 0.0 ? 1.0 : 0.0) : M2pL * ((2.0 - ML) - 16.0 * alpha * ML * M2mL);
+  const double p5m = std::fabs(MR) >= 1.0 ? (MR < 0.0 ? 1.0 : 0.0) : M2mR * ((-2.0 - MR) + 16.0 * alpha * MR * M2pR);
+  const double rho12 = 0.5 * (R.s.rho + L.s.rho);
+  const double M12 = M4p + M4m - Kp * std::fmax(1.0 - sigma * Mbarsq, 0.0) * (R.s.p - L.s.p) * inva12 * inva12 / (fa * rho12);
+  const double mdot = a12 * M12 * (M12 > 0.0 ? L.s.rho : R.s.rho) * area;
+  const double p12 = p5p * L.s.p + p5m * R.s.p - Ku * p5p * p5m * (R.s.rho + L.s.rho) * fa * a12 * (UR - UL);
+  const bool left = mdot > 0.0;
+  const Side &U = left ? L : R;
+  const double *Y = left ? YL : YR;
+  F[0] = mdot;
+  F[1] = mdot * U.u + p12 * S[0];
+  F[2] = mdot * U.v + p12 * S[1];
+  F[3] = mdot * U.w + p12 * S[2];
+  F[4] = mdot * (U.s.e + 0.5 * ((U.u) * (U.u) + (U.v) * (U.v) + (U.w) * (U.w)) + U.s.p / U.s.rho);
+  for (int n = 0; n < c.ns - 1; n++) F[5 + n] = mdot * Y[n];
+}
+
+// the advective flux of one face from its four cells (LL and RR read by MUSCL only):
+// the reconstruction, then the flux function (simulator/euler/kernels/flux/single.mako:4-9)
+void advective(const OCase &c, const double *QLL, const double *QL, const double *QR, const double *QRR,
+               const State &sLL, const State &sL, const State &sR, const State &sRR, const double *S, double *F) {
+  double YL[16], YR[16];
+  if (c.primary == O_KEPAEC) {
+    kepaec(c, side(QL, sL), side(QR, sR), QL, QR, S, F);
+    return;
+  }
+  Side L, R;
+  if (c.recon == 1) {
+    muscl(c, QLL, QL, QR, QRR, sLL, sL, sR, sRR, L, R, YL, YR);
+  } else {
+    L = side(QL, sL), R = side(QR, sR);
+    for (int n = 0; n < c.ns - 1; n++) YL[n] = QL[5 + n] / QL[0], YR[n] = QR[5 + n] / QR[0];
+  }
+  if (c.primary == O_HLLC) hllc(c, L, R, YL, YR, S, F);
+  else if (c.primary == O_RUSANOV) rusanov(c, L, R, YL, YR, S, F);
+  else ausmup(c, L, R, YL, YR, S, F);
 }
 
 // alpha damping (simulator/navstokes/kernels/flux/alpha-damping.mako:3-92)
@@ -426,12 +607,17 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
             const long at = f.at(i, j, k);
             const long R = d.at(i, j, k);
             const long L = d.at(i - (a == 0), j - (a == 1), k - (a == 2));
+            const long LL = d.at(i - 2 * (a == 0), j - 2 * (a == 1), k - 2 * (a == 2));
+            const long RR = d.at(i + (a == 0), j + (a == 1), k + (a == 2));
             const double *QL = B.Q + L * ne, *QR = B.Q + R * ne;
             const State &sL = *reinterpret_cast<const State *>(&s.state[L * NSTATE]);
             const State &sR = *reinterpret_cast<const State *>(&s.state[R * NSTATE]);
+            const State &sLL = *reinterpret_cast<const State *>(&s.state[LL * NSTATE]);
+            const State &sRR = *reinterpret_cast<const State *>(&s.state[RR * NSTATE]);
             double *F = &s.F[a][at * ne];
             const double *S = B.S[a] + at * 3;
-            if (!c.skip_adv) kepaec(c, side(QL, sL), side(QR, sR), QL, QR, S, F);
+            if (!c.skip_adv)
+              advective(c, B.Q + LL * ne, QL, QR, B.Q + RR * ne, sLL, sL, sR, sRR, S, F);
             if (visc)
               alphadamping(c, S, B.xf[a] + at * 3, B.xcc + L * 3, B.xcc + R * 3, QL, QR, sL, sR,
                            &s.tr[L * (2 + ns)], &s.tr[R * (2 + ns)], &s.hsp[L * ns], &s.hsp[R * ns],
@@ -465,6 +651,20 @@ int oracle_kepaec_faces(const OCase *cp, long n, const double *QL, const double 
     const double *ql = QL + f * ne, *qr = QR + f * ne;
     const State sl = fromQ(*cp, ql), sr = fromQ(*cp, qr);
     kepaec(*cp, side(ql, sl), side(qr, sr), ql, qr, S + 3 * f, F + f * ne);
+  }
+  return 0;
+}
+
+// the advective flux on n independent faces from the four cells around each,
+// Q rows [4][n][ne] in the order LL, L, R, RR (the reconstruction and flux
+// function check against the reference's numpy oracle)
+int oracle_advective_faces(const OCase *cp, long n, const double *Q4, const double *S, double *F) {
+  const int ne = 4 + cp->ns;
+  for (long f = 0; f < n; f++) {
+    const double *q[4];
+    State st[4];
+    for (int o = 0; o < 4; o++) q[o] = Q4 + ((long)o * n + f) * ne, st[o] = fromQ(*cp, q[o]);
+    advective(*cp, q[0], q[1], q[2], q[3], st[0], st[1], st[2], st[3], S + 3 * f, F + f * ne);
   }
   return 0;
 }

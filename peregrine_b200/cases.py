@@ -74,3 +74,51 @@ def tgv_prims(blocks, metrics, ne=5, seed=0, noise=1e-6, mach=0.1):
         q[..., 4] = T0 * q[..., 0] / P0
         out.append(q)
     return out
+
+
+# three species differing in weight, heat capacity, formation enthalpy, Lewis
+# number, viscosity and conductivity
+MIXED = {
+    "A": {"MW": 28.0, "cp0": 1000.0, "dHf298": 0.0, "lewis": 1.0, "mu0": 1.8e-5, "kappa0": 0.026},
+    "B": {"MW": 32.0, "cp0": 900.0, "dHf298": 1.0e7, "lewis": 1.4, "mu0": 2.0e-5, "kappa0": 0.025},
+    "C": {"MW": 16.0, "cp0": 2200.0, "dHf298": -7.5e7, "lewis": 0.7, "mu0": 1.1e-5, "kappa0": 0.034},
+}
+
+
+def mixing_config(simulator="navier-stokes", integrator="rk4", primary="hllc", recon="muscl", limiter="koren", ns=2,
+                  launch="per-block"):
+    """A gas of ns of the MIXED species through one advective scheme."""
+    cfg = Config()
+    cfg["simulation"]["simulator"] = simulator
+    cfg["mixture"]["species"] = {k: MIXED[k] for k in list(MIXED)[:ns]}
+    cfg["mixture"]["trans"] = "constant" if simulator == "navier-stokes" else None
+    cfg["time-integration"]["integrator"] = integrator
+    cfg["adv-flux"]["primary"] = primary
+    cfg["adv-flux"]["recon"] = recon
+    cfg["adv-flux"]["limiter"] = limiter if recon == "muscl" else None
+    cfg["backend-b200"]["launch"] = launch
+    return cfg.validate()
+
+
+def rough_prims(metrics, ns, seed=0, speed=420.0):
+    """Primitives p, u, v, w, T, Y[ns - 1] per block on the 2 pi cube: waves
+    with a step in pressure, temperature and composition across x = pi, so
+    the slope ratios take every sign and size and, at this speed, some faces
+    are supersonic each way."""
+    rng = np.random.default_rng(seed)
+    ph = rng.uniform(0.0, 2 * np.pi, 8)
+    out = []
+    for m in metrics:
+        x, y, z = (m["xcc"][..., d] for d in range(3))
+        step = (np.mod(x, 2 * np.pi) > np.pi).astype(float)
+        q = np.zeros(x.shape + (4 + ns,))
+        q[..., 0] = P0 * (1.0 + 0.2 * np.sin(x + ph[0]) * np.cos(y + ph[1]) + 0.5 * step)
+        q[..., 1] = speed * np.sin(x + ph[2]) * np.cos(z + ph[3])
+        q[..., 2] = 0.4 * speed * np.cos(y + ph[4])
+        q[..., 3] = 0.3 * speed * np.sin(z + ph[5]) * np.cos(x)
+        q[..., 1:4] += 5.0 * rng.standard_normal(x.shape + (3,))
+        q[..., 4] = T0 * (1.0 + 0.2 * np.cos(x + ph[6]) * np.sin(z + ph[7]) + 0.4 * step)
+        for n in range(ns - 1):
+            q[..., 5 + n] = (0.6 - 0.2 * step) / (ns - 1) * (1.0 + 0.3 * np.sin((n + 1) * x + y + ph[n]))
+        out.append(q)
+    return out

@@ -88,7 +88,7 @@ SIMULATORS = ("euler", "navier-stokes")
 INTEGRATORS = ("rk1", "rk2", "tvd-rk3", "rk34", "rk4")
 EOSES = ("cpg", "tpg")
 TRANS = (None, "constant", "kinetic-theory")
-PRIMARIES = ("kepaec", "hllc", "rusanov")
+PRIMARIES = ("kepaec", "hllc", "rusanov", "ausmup")
 RECONS = ("constant", "muscl")
 LIMITERS = (None, "koren", "minmod", "mc", "superbee", "vanleer")
 

@@ -654,6 +654,34 @@ int ensure_scratch(pgb_case *c) {
   return PGB_OK;
 }
 
+// the advective face flux of one axis of one block, by the case's flux
+// function and reconstruction
+template <int NS, int A, int FN>
+void launch_riemann(const pgb_case *c, int b, const double *Q, long long nf, int TH) {
+  const dim3 g = grid_for(nf, TH);
+  cudaStream_t s = c->stream;
+  double *F = c->d_F[A];
+  const int lim = c->phys.recon == PGB_RECON_MUSCL ? c->phys.limiter : 0;
+  switch (lim) {
+    case 0: k_riemann<NS, A, FN, 0><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
+    case LIM_KOREN: k_riemann<NS, A, FN, LIM_KOREN><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
+    case LIM_MINMOD: k_riemann<NS, A, FN, LIM_MINMOD><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
+    case LIM_MC: k_riemann<NS, A, FN, LIM_MC><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
+    case LIM_SUPERBEE: k_riemann<NS, A, FN, LIM_SUPERBEE><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
+    default: k_riemann<NS, A, FN, LIM_VANLEER><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
+  }
+}
+
+template <int NS, int A>
+void launch_advflux(const pgb_case *c, int b, const double *Q, long long nf, int TH) {
+  switch (c->phys.primary) {
+    case PGB_FLUX_HLLC: launch_riemann<NS, A, FN_HLLC>(c, b, Q, nf, TH); break;
+    case PGB_FLUX_RUSANOV: launch_riemann<NS, A, FN_RUSANOV>(c, b, Q, nf, TH); break;
+    case PGB_FLUX_AUSMUP: launch_riemann<NS, A, FN_AUSMUP>(c, b, Q, nf, TH); break;
+    default: k_advflux<NS, A><<<grid_for(nf, TH), TH, 0, c->stream>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[A]);
+  }
+}
+
 template <int NS>
 int rhs_plain_ns(pgb_case *c, int qphys, int dqphys, int &count) {
   const int TH = 256;
@@ -684,11 +712,11 @@ int rhs_plain_ns(pgb_case *c, int qphys, int dqphys, int &count) {
     const long long inner = (long long)D.nx * D.ny * D.nz;
     const long long fx = (long long)(D.nx + 1) * D.ny * D.nz, fy = (long long)D.nx * (D.ny + 1) * D.nz,
                     fz = (long long)D.nx * D.ny * (D.nz + 1);
-    k_advflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[0]);
+    launch_advflux<NS, 0>(c, b, Q, fx, TH);
     mark(c, K_BLOCK, count);
-    k_advflux<NS, 1><<<grid_for(fy, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[1]);
+    launch_advflux<NS, 1>(c, b, Q, fy, TH);
     mark(c, K_BLOCK, count);
-    k_advflux<NS, 2><<<grid_for(fz, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[2]);
+    launch_advflux<NS, 2>(c, b, Q, fz, TH);
     mark(c, K_BLOCK, count);
     if (visc) {
       k_diffflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[0]);
@@ -806,8 +834,14 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
   if (phys->ns < 1 || phys->ns > MAXNS) return fail(PGB_ERR_ARG, "ns out of range");
   if (phys->nregs < 2 || phys->nregs > MAXREGS) return fail(PGB_ERR_ARG, "nregs out of range");
   if (phys->eos != PGB_EOS_CPG) return fail(PGB_ERR_UNSUPPORTED, "this build has the calorically perfect gas only");
-  if (phys->primary != PGB_FLUX_KEPAEC || phys->recon != PGB_RECON_CONSTANT)
-    return fail(PGB_ERR_UNSUPPORTED, "this build has kepaec on the constant reconstruction only");
+  if (phys->primary < PGB_FLUX_KEPAEC || phys->primary > PGB_FLUX_AUSMUP)
+    return fail(PGB_ERR_ARG, "no such flux function");
+  if (phys->recon != PGB_RECON_CONSTANT && phys->recon != PGB_RECON_MUSCL)
+    return fail(PGB_ERR_ARG, "no such reconstruction");
+  if (phys->recon == PGB_RECON_MUSCL && (phys->limiter < 1 || phys->limiter > 5))
+    return fail(PGB_ERR_ARG, "muscl needs a limiter: koren, minmod, mc, superbee or vanleer");
+  if (phys->primary == PGB_FLUX_KEPAEC && phys->recon != PGB_RECON_CONSTANT)
+    return fail(PGB_ERR_UNSUPPORTED, "kepaec is a two-point flux of the cells as they are; it takes no muscl sides");
   if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT)
     return fail(PGB_ERR_UNSUPPORTED, "this build has constant transport only");
   auto c = std::make_unique<pgb_case>();

@@ -223,6 +223,177 @@ __device__ __forceinline__ void kepaec(const KSide &L, const KSide &R, const dou
   F[4] = ef * C + Kj + Pj;
 }
 
+// A face side for the Riemann solvers: what hllc, rusanov and ausmup read of
+// the reference's FaceState (peregrine/simulator/euler/kernels/flux/recon/constant.mako:3-18
+// for a cell as it is, recon/muscl.mako:15-51 for a reconstructed side)
+struct RSide {
+  double u, v, w, p, rho, e, c;
+};
+
+// cpg frompT onto a side (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:17-27)
+template <int NS>
+__device__ __forceinline__ void side_frompT(const double p, const double T, const double *Y, RSide &s) {
+  double R, cp, h298;
+  mixmom<NS>([&](int n) { return Y[n]; }, R, cp, h298);
+  const double cv = cp - R;
+  s.p = p;
+  s.rho = p / (R * T);
+  s.e = cv * T + h298;
+  const double gamma = cp / cv;
+  s.c = sqrt(gamma * R * T);
+}
+
+// b phi(a / b) of the five limiters, b > 0, formed without the ratio
+// (peregrine/simulator/euler/kernels/flux/recon/{koren,minmod,mc,superbee,vanleer}.mako)
+enum { LIM_KOREN = 1, LIM_MINMOD = 2, LIM_MC = 3, LIM_SUPERBEE = 4, LIM_VANLEER = 5 };
+template <int LIM>
+__device__ __forceinline__ double bphi(const double a, const double b) {
+  if (LIM == LIM_KOREN) return fmax(0.0, fmin(fmin(2.0 * a, (2.0 * b + a) * (1.0 / 3.0)), 2.0 * b));
+  if (LIM == LIM_MINMOD) return fmax(0.0, fmin(b, a));
+  if (LIM == LIM_MC) return fmax(0.0, fmin(fmin(2.0 * a, (b + a) * 0.5), 2.0 * b));
+  if (LIM == LIM_SUPERBEE) return fmax(0.0, fmax(fmin(2.0 * a, b), fmin(a, 2.0 * b)));
+  return (a + fabs(a)) * b / (b + fabs(a));
+}
+
+// the limited slope across a face: the upwind difference dm carried to the
+// sign of the difference dp across the face, limited, and the sign put back;
+// none where dp is none (recon/muscl.mako:5-13)
+template <int LIM>
+__device__ __forceinline__ double phi(const double dm, const double dp) {
+  double ph = 0.0;
+  if (dp != 0.0) {
+    const double s = copysign(1.0, dp), a = s * dm, b = fabs(dp);
+    ph = s * bphi<LIM>(a, b);
+  }
+  return ph;
+}
+template <int LIM>
+__device__ __forceinline__ double muscl_left(const double vLL, const double vL, const double vR) {
+  return vL + 0.5 * phi<LIM>(vL - vLL, vR - vL);
+}
+template <int LIM>
+__device__ __forceinline__ double muscl_right(const double vL, const double vR, const double vRR) {
+  return vR - 0.5 * phi<LIM>(vRR - vR, vR - vL);
+}
+
+// HLLC with Davis's outer wave speeds (peregrine/simulator/euler/kernels/flux/function/hllc.mako:2-43)
+template <int NS>
+__device__ __forceinline__ void hllc(const RSide &L, const RSide &R, const double *YL, const double *YR,
+                                     const double *S, double *F) {
+  const double area = sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+  const double nx = S[0] / area, ny = S[1] / area, nz = S[2] / area;
+  const double unL = (L.u * S[0] + L.v * S[1] + L.w * S[2]) / area;
+  const double unR = (R.u * S[0] + R.v * S[1] + R.w * S[2]) / area;
+  const double SL = unL - L.c, SR = unR + R.c;
+  const double Sstar = (R.p - L.p + L.rho * unL * (SL - unL) - R.rho * unR * (SR - unR)) /
+                       (L.rho * (SL - unL) - R.rho * (SR - unR));
+  bool left, star;
+  if (SL >= 0.0) {
+    left = true, star = false;
+  } else if (Sstar >= 0.0) {
+    left = true, star = true;
+  } else if (SR >= 0.0) {
+    left = false, star = true;
+  } else {
+    left = false, star = false;
+  }
+  const RSide &X = left ? L : R;
+  const double *Y = left ? YL : YR;
+  const double U = left ? unL : unR, SX = left ? SL : SR;
+  const double et = X.e + 0.5 * (X.u * X.u + X.v * X.v + X.w * X.w);
+  const double mdot = U * X.rho * area;
+  F[0] = mdot;
+  F[1] = mdot * X.u + X.p * S[0];
+  F[2] = mdot * X.v + X.p * S[1];
+  F[3] = mdot * X.w + X.p * S[2];
+  F[4] = mdot * et + U * X.p * area;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) F[5 + n] = mdot * Y[n];
+  if (star) {
+    const double rhostar = X.rho * ((SX - U) / (SX - Sstar));
+    const double drho = rhostar - X.rho, dU = rhostar * (Sstar - U);
+    const double jump = SX * area;
+    F[0] += jump * drho;
+    F[1] += jump * (drho * X.u + dU * nx);
+    F[2] += jump * (drho * X.v + dU * ny);
+    F[3] += jump * (drho * X.w + dU * nz);
+    F[4] += jump * (drho * et + dU * (Sstar + X.p / (X.rho * (SX - U))));
+#pragma unroll
+    for (int n = 0; n < NS - 1; n++) F[5 + n] += jump * drho * Y[n];
+  }
+}
+
+// Rusanov with Davis's bound on the fastest wave
+// (peregrine/simulator/euler/kernels/flux/function/rusanov.mako:2-21)
+template <int NS>
+__device__ __forceinline__ void rusanov(const RSide &L, const RSide &R, const double *YL, const double *YR,
+                                        const double *S, double *F) {
+  const double area = sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+  const double unL = (L.u * S[0] + L.v * S[1] + L.w * S[2]) / area;
+  const double unR = (R.u * S[0] + R.v * S[1] + R.w * S[2]) / area;
+  const double lam = fmax(fabs(unL) + L.c, fabs(unR) + R.c) * area;
+  const double UL = unL * area, UR = unR * area;
+  F[0] = 0.5 * (UR * R.rho + UL * L.rho - lam * (R.rho - L.rho));
+  F[1] = 0.5 * (UR * R.rho * R.u + R.p * S[0] + UL * L.rho * L.u + L.p * S[0] - lam * (R.rho * R.u - L.rho * L.u));
+  F[2] = 0.5 * (UR * R.rho * R.v + R.p * S[1] + UL * L.rho * L.v + L.p * S[1] - lam * (R.rho * R.v - L.rho * L.v));
+  F[3] = 0.5 * (UR * R.rho * R.w + R.p * S[2] + UL * L.rho * L.w + L.p * S[2] - lam * (R.rho * R.w - L.rho * L.w));
+  const double EL = L.rho * (L.e + 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w));
+  const double ER = R.rho * (R.e + 0.5 * (R.u * R.u + R.v * R.v + R.w * R.w));
+  F[4] = 0.5 * (UR * (ER + R.p) + UL * (EL + L.p) - lam * (ER - EL));
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    const double rhoYL = L.rho * YL[n], rhoYR = R.rho * YR[n];
+    F[5 + n] = 0.5 * (rhoYR * UR + rhoYL * UL - lam * (rhoYR - rhoYL));
+  }
+}
+
+// AUSM+-up of Liou (2006) with the cut-off Mach number sqrt(0.1)
+// (peregrine/simulator/euler/kernels/flux/function/ausmup.mako:2-38)
+template <int NS>
+__device__ __forceinline__ void ausmup(const RSide &L, const RSide &R, const double *YL, const double *YR,
+                                       const double *S, double *F) {
+  const double area = sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]), invarea = 1.0 / area;
+  const double UL = (L.u * S[0] + L.v * S[1] + L.w * S[2]) * invarea;
+  const double UR = (R.u * S[0] + R.v * S[1] + R.w * S[2]) * invarea;
+  const double a12 = 0.5 * (R.c + L.c), inva12 = 1.0 / a12;
+  const double ML = UL * inva12, MR = UR * inva12;
+  const double Mbarsq = 0.5 * (UL * UL + UR * UR) * inva12 * inva12;
+  const double Mco = 0.31622776601683794, Kp = 0.25, Ku = 0.75, sigma = 1.0, beta = 1.0 / 8.0;
+  const double Mo = sqrt(fmin(1.0, fmax(Mbarsq, Mco * Mco)));
+  const double fa = Mo * (2.0 - Mo);
+  const double M1p = 0.5 * (ML + fabs(ML)), M1m = 0.5 * (MR - fabs(MR));
+  const double M2pL = 0.25 * (ML + 1.0) * (ML + 1.0), M2mL = -0.25 * (ML - 1.0) * (ML - 1.0);
+  const double M2pR = 0.25 * (MR + 1.0) * (MR + 1.0), M2mR = -0.25 * (MR - 1.0) * (MR - 1.0);
+  const double M4p = fabs(ML) >= 1.0 ? M1p : M2pL * (1.0 - 16.0 * beta * M2mL);
+  const double M4m = fabs(MR) >= 1.0 ? M1m : M2mR * (1.0 + 16.0 * beta * M2pR);
+  const double alpha = 3.0 / 16.0 * (-4.0 + 5.0 * fa * fa);
+  const double p5p = fabs(ML) >= 1.0 ? (ML > 0.0 ? 1.0 : 0.0) : M2pL * ((2.0 - ML) - 16.0 * alpha * ML * M2mL);
+  const double p5m = fabs(MR) >= 1.0 ? (MR < 0.0 ? 1.0 : 0.0) : M2mR * ((-2.0 - MR) + 16.0 * alpha * MR * M2pR);
+  const double rho12 = 0.5 * (R.rho + L.rho);
+  const double M12 = M4p + M4m - Kp * fmax(1.0 - sigma * Mbarsq, 0.0) * (R.p - L.p) * inva12 * inva12 / (fa * rho12);
+  const double mdot = a12 * M12 * (M12 > 0.0 ? L.rho : R.rho) * area;
+  const double p12 = p5p * L.p + p5m * R.p - Ku * p5p * p5m * (R.rho + L.rho) * fa * a12 * (UR - UL);
+  const bool left = mdot > 0.0;
+  const RSide &U = left ? L : R;
+  const double *Y = left ? YL : YR;
+  F[0] = mdot;
+  F[1] = mdot * U.u + p12 * S[0];
+  F[2] = mdot * U.v + p12 * S[1];
+  F[3] = mdot * U.w + p12 * S[2];
+  F[4] = mdot * (U.e + 0.5 * (U.u * U.u + U.v * U.v + U.w * U.w) + U.p / U.rho);
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) F[5 + n] = mdot * Y[n];
+}
+
+enum { FN_HLLC = 1, FN_RUSANOV = 2, FN_AUSMUP = 3 };
+template <int FN, int NS>
+__device__ __forceinline__ void riemann(const RSide &L, const RSide &R, const double *YL, const double *YR,
+                                        const double *S, double *F) {
+  if (FN == FN_HLLC) hllc<NS>(L, R, YL, YR, S, F);
+  else if (FN == FN_RUSANOV) rusanov<NS>(L, R, YL, YR, S, F);
+  else ausmup<NS>(L, R, YL, YR, S, F);
+}
+
 // What alpha damping reads of a face's geometry, formed once per face
 // (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:13-27)
 struct FaceGeom {

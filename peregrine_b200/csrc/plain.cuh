@@ -168,6 +168,67 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
   for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
 }
 
+// the advective face flux of a Riemann solver FN on the cells as they are
+// (LIM 0; recon/constant.mako:3-18) or on MUSCL's sides under limiter LIM
+// (recon/muscl.mako:15-51), both sides from the four cells LL, L, R, RR
+// along the axis (peregrine/simulator/euler/kernels/flux/single.mako:4-9)
+template <int NS, int A, int FN, int LIM>
+__global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                          const double *__restrict__ stall, const double *__restrict__ met,
+                          double *__restrict__ Fall) {
+  constexpr int NE = 4 + NS, NY = NS > 1 ? NS - 1 : 1;
+  const BlockDev &B = blks[b];
+  int i, j, k;
+  if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  const long long d = A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y;
+  const long long L = R - d;
+  const long long v = B.vol;
+  const double *Q = Qall + NE * B.cv;
+  const double *st = stall + 8 * B.cv;
+  const double *Sp = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
+  const double S[3] = {Sp[0], Sp[v], Sp[2 * v]};
+  RSide sl, sr;
+  double YL[NY], YR[NY];
+  if (LIM == 0) {
+    auto cell = [&](long long c, RSide &x, double *Y) {
+      x.p = st[0 * v + c], x.rho = st[3 * v + c], x.e = st[4 * v + c], x.c = st[7 * v + c];
+      x.u = Q[1 * v + c] / Q[c];
+      x.v = Q[2 * v + c] / Q[c];
+      x.w = Q[3 * v + c] / Q[c];
+#pragma unroll
+      for (int n = 0; n < NS - 1; n++) Y[n] = Q[(5 + n) * v + c] / Q[c];
+    };
+    cell(L, sl, YL);
+    cell(R, sr, YR);
+  } else {
+    const long long LL = L - d, RR = R + d;
+    const double riLL = st[2 * v + LL], riL = st[2 * v + L], riR = st[2 * v + R], riRR = st[2 * v + RR];
+    // a row of Q over rho on each side
+    auto lft = [&](int row) {
+      return muscl_left<LIM>(Q[row * v + LL] * riLL, Q[row * v + L] * riL, Q[row * v + R] * riR);
+    };
+    auto rgt = [&](int row) {
+      return muscl_right<LIM>(Q[row * v + L] * riL, Q[row * v + R] * riR, Q[row * v + RR] * riRR);
+    };
+    // p and T from the state; Y and the velocity as Q times the cell's 1 / rho
+    const double pL = muscl_left<LIM>(st[LL], st[L], st[R]), pR = muscl_right<LIM>(st[L], st[R], st[RR]);
+    const double TL = muscl_left<LIM>(st[v + LL], st[v + L], st[v + R]);
+    const double TR = muscl_right<LIM>(st[v + L], st[v + R], st[v + RR]);
+#pragma unroll
+    for (int n = 0; n < NS - 1; n++) YL[n] = lft(5 + n), YR[n] = rgt(5 + n);
+    side_frompT<NS>(pL, TL, YL, sl);
+    side_frompT<NS>(pR, TR, YR, sr);
+    sl.u = lft(1), sl.v = lft(2), sl.w = lft(3);
+    sr.u = rgt(1), sr.v = rgt(2), sr.w = rgt(3);
+  }
+  double F[NE];
+  riemann<FN, NS>(sl, sr, YL, YR, S, F);
+  double *Fo = Fall + NE * B.cv + R;
+#pragma unroll
+  for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
+}
+
 // the diffusive face flux added to F (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:3-99)
 template <int NS, int A>
 __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,

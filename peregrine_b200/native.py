@@ -17,8 +17,9 @@ LIBPATH = os.path.join(HERE, "libpgb200.so")
 OK, ERR_ARG, ERR_STATE, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
 EULER, NAVIER_STOKES = 0, 1
 EOS_CPG, EOS_TPG = 0, 1
-FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV = 0, 1, 2
+FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV, FLUX_AUSMUP = 0, 1, 2, 3
 RECON_CONSTANT, RECON_MUSCL = 0, 1
+LIMITERS = {"koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
 TRANS_NONE, TRANS_CONSTANT, TRANS_KINETIC = 0, 1, 2
 PATH_BATCHED, PATH_PER_BLOCK = 0, 1
 ARR_XCC, ARR_DETJINV, ARR_JINV, ARR_IS, ARR_JS, ARR_KS, ARR_IXC, ARR_JXC, ARR_KXC = range(9)

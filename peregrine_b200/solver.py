@@ -114,9 +114,10 @@ class Solver:
         phys = native.Physics()
         phys.simulator = native.NAVIER_STOKES if sim["simulator"] == "navier-stokes" else native.EULER
         phys.eos = native.EOS_CPG
-        phys.primary = {"kepaec": native.FLUX_KEPAEC, "hllc": native.FLUX_HLLC, "rusanov": native.FLUX_RUSANOV}[adv["primary"]]
+        phys.primary = {"kepaec": native.FLUX_KEPAEC, "hllc": native.FLUX_HLLC, "rusanov": native.FLUX_RUSANOV,
+                        "ausmup": native.FLUX_AUSMUP}[adv["primary"]]
         phys.recon = native.RECON_CONSTANT if adv["recon"] == "constant" else native.RECON_MUSCL
-        phys.limiter = 0
+        phys.limiter = native.LIMITERS[adv["limiter"]] if adv["recon"] == "muscl" else 0
         trans = cfg["mixture"]["trans"]
         phys.trans = {None: native.TRANS_NONE, "constant": native.TRANS_CONSTANT,
                       "kinetic-theory": native.TRANS_KINETIC}[trans]

@@ -16,7 +16,11 @@ What it records, each from the reference's own code:
   constants.npz      peregrine/simulator/mixture's constants for the
                      Taylor-Green air and a binary gas with constant transport;
   rk_tables.json     peregrine/integrators/rungekutta.py's combine kernels per
-                     stage (registers, weights, dt placement) for every scheme.
+                     stage (registers, weights, dt placement) for every scheme;
+  faces_riemann.npz  tests/simulator/oracle.py's hllc, rusanov and ausmup
+                     fluxes on the two cells as they are, and on muscl's sides
+                     under each of the five limiters, for four cells LL, L, R,
+                     RR around random faces of the binary gas.
 """
 
 import json
@@ -115,6 +119,46 @@ def faces(orc, gas, n, rng):
     return dict(QL=QL, QR=QR, S=S, F=F)
 
 
+def faces4(orc, gas, n, rng):
+    """Four cells around each face: a smooth profile plus noise, so the slope
+    ratios take every sign and size the limiters distinguish; a quarter of the
+    faces carry a supersonic stream along the normal each way, so HLLC's
+    outer cases come up besides the two star cases."""
+    ns = len(gas)
+    S = rng.uniform(-1.0, 1.0, (n, 3))
+    stream = rng.choice([0.0, 0.0, 900.0, -900.0], n)[:, None] * S / np.linalg.norm(S, axis=1, keepdims=True)
+    base = dict(p=rng.uniform(5e4, 2e5, n), T=rng.uniform(200.0, 600.0, n), Y=rng.uniform(0.2, 0.8, (n, ns - 1)),
+                u=rng.uniform(-200.0, 200.0, (n, 3)))
+    slope = dict(p=rng.uniform(-2e4, 2e4, n), T=rng.uniform(-50.0, 50.0, n), Y=rng.uniform(-0.05, 0.05, (n, ns - 1)),
+                 u=rng.uniform(-60.0, 60.0, (n, 3)))
+    fields = ("p", "T", "rhoinv", "rho", "e", "cp", "gamma", "c")
+    Q, state = [], []
+    for o in (-2, -1, 0, 1):
+        x = o + 0.5
+        v = {k: base[k] + slope[k] * (x if base[k].ndim == 1 else x) for k in base}
+        noise = dict(p=2e3, T=5.0, Y=0.01, u=8.0)
+        v = {k: v[k] + rng.normal(0.0, noise[k], v[k].shape) for k in v}
+        v["u"] = v["u"] + stream
+        s = orc.cpg(gas, v["p"], v["T"], v["Y"])
+        s["rhoinv"] = 1.0 / s["rho"]
+        rho, u = s["rho"], v["u"]
+        Q.append(np.concatenate([rho[:, None], rho[:, None] * u, (rho * (s["e"] + 0.5 * (u * u).sum(axis=1)))[:, None],
+                                 rho[:, None] * v["Y"]], axis=1))
+        state.append(np.stack([s[f] for f in fields], axis=-1))
+    Q, state = np.stack(Q), np.stack(state)
+    # the numpy oracle indexes its cells by offset from the face: -2, -1, 0, 1
+    byoff = {o: Q[o + 2] for o in (-2, -1, 0, 1)}
+    stbyoff = {o: state[o + 2] for o in (-2, -1, 0, 1)}
+    out = dict(Q4=Q, S=S)
+    for fn in ("hllc", "rusanov", "ausmup"):
+        flux = orc.functions[fn]
+        out[f"{fn}_constant"] = flux(orc.cell(Q[1], state[1]), orc.cell(Q[2], state[2]), S)
+        for name, lim in orc.limiters.items():
+            L, R = orc.muscl(gas, byoff, stbyoff, lim)
+            out[f"{fn}_muscl_{name}"] = flux(L, R, S)
+    return out
+
+
 def metrics(GridBlock, rng):
     ng = 2
     shape = (7 + 2 * ng, 6 + 2 * ng, 5 + 2 * ng)
@@ -188,6 +232,8 @@ def main():
     np.savez(os.path.join(HERE, "constants.npz"), **consts)
     with open(os.path.join(HERE, "rk_tables.json"), "w") as f:
         json.dump(rk_tables(integrators), f, indent=1)
+    binary = {k: dict(MW=v["MW"], cp0=v["cp0"]) for k, v in BINARY.items()}
+    np.savez(os.path.join(HERE, "faces_riemann.npz"), **faces4(orc, binary, 256, np.random.default_rng(20261204)))
     with open(os.path.join(HERE, "gases.json"), "w") as f:
         json.dump(dict(air=air, binary=BINARY), f, indent=1)
     print("wrote", sorted(p for p in os.listdir(HERE) if not p.endswith(".py")))

@@ -50,6 +50,49 @@ def test_kepaec_matches_the_reference_numpy_oracle(gas):
     assert close_rows(got, f[f"{gas}_F"], 1e-13)
 
 
+LIMITERS = ["koren", "minmod", "mc", "superbee", "vanleer"]
+
+
+@pytest.mark.parametrize("recon", ["constant"] + [f"muscl_{name}" for name in LIMITERS])
+@pytest.mark.parametrize("primary", ["hllc", "rusanov", "ausmup"])
+def test_riemann_fluxes_match_the_reference_numpy_oracle(primary, recon):
+    f = gold("faces_riemann.npz")
+    species = gases()["binary"]
+    consts = mixture(species).constants()
+    muscl = recon != "constant"
+    orc = Oracle(consts, len(species), "euler", [], [], primary=primary, recon="muscl" if muscl else "constant",
+                 limiter=recon[6:] if muscl else None)
+    Q4 = f["Q4"]
+    got = orc.advective_faces(Q4[0], Q4[1], Q4[2], Q4[3], f["S"])
+    # the reference's bar for its kernels' face fluxes against this oracle
+    # (tests/simulator/test_facefluxes.py:53-63); the limiters here take the
+    # two differences, the numpy oracle their ratio, so the two agree to rounding
+    assert close_rows(got, f[f"{primary}_{recon}"], 1e-13)
+
+
+def test_the_fixture_exercises_every_hllc_wave_case():
+    f = gold("faces_riemann.npz")
+    Q4, S = f["Q4"], f["S"]
+    consts = mixture(gases()["binary"]).constants()
+    area = np.linalg.norm(S, axis=1)
+
+    def side(Q):
+        rho = Q[:, 0]
+        u = Q[:, 1:4] / rho[:, None]
+        Y = np.c_[Q[:, 5:] / rho[:, None], 1.0 - Q[:, 5:].sum(1) / rho]
+        R, cp = Y @ consts["Rsp"], Y @ consts["cp0"]
+        T = (Q[:, 4] / rho - 0.5 * (u * u).sum(1) - Y @ consts["h298R"]) / (cp - R)
+        return (u * S).sum(1) / area, np.sqrt(cp / (cp - R) * R * T)
+
+    (unL, cL), (unR, cR) = side(Q4[1]), side(Q4[2])
+    SL, SR = unL - cL, unR + cR
+    # the left and right outer cases, and subsonic faces whose star state is either side
+    assert (SL >= 0).sum() > 8 and (SR < 0).sum() > 8
+    sub = (SL < 0) & (SR >= 0)
+    assert (sub & (unL + unR > 0)).sum() > 8 and (sub & (unL + unR < 0)).sum() > 8
+    assert not np.array_equal(f["hllc_constant"], f["hllc_muscl_koren"])
+
+
 def test_metrics_match_the_reference_grid_bit_for_bit():
     g = gold("metrics.npz")
     mine = grid.metrics(g["nodes"], 2)
