@@ -31,7 +31,36 @@ class OCase(ctypes.Structure):
                 ("alpha", ctypes.c_double)] + \
                [(n, ctypes.POINTER(ctypes.c_double)) for n in
                 ("Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0", "kappa0", "MWqinv", "wilkepair", "lewis")] + \
-               [("Ru", ctypes.c_double), ("skip_adv", ctypes.c_int), ("recon", ctypes.c_int), ("limiter", ctypes.c_int)]
+               [("Ru", ctypes.c_double), ("skip_adv", ctypes.c_int), ("recon", ctypes.c_int), ("limiter", ctypes.c_int),
+                ("eos", ctypes.c_int), ("ncp", ctypes.c_int), ("cppolyR", ctypes.POINTER(ctypes.c_double)),
+                ("nh", ctypes.c_int), ("hpoly", ctypes.POINTER(ctypes.c_double)), ("trans", ctypes.c_int),
+                ("nmu", ctypes.c_int), ("nkappa", ctypes.c_int), ("mupoly", ctypes.POINTER(ctypes.c_double)),
+                ("kappapoly", ctypes.POINTER(ctypes.c_double)), ("mech", ctypes.c_void_p)]
+
+
+MAXSIDE = 8
+
+
+class ORxn(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("kind", "reversible", "product", "tb", "troe", "nfcent", "nfwd", "nreact",
+                                            "nprod", "nnet")] + \
+               [(n, ctypes.c_int * MAXSIDE) for n in ("fwdsp", "reactsp", "prodsp", "netsp")] + \
+               [(n, ctypes.c_double * MAXSIDE) for n in ("fwdorder", "reactnu", "prodnu", "netnu", "netnuMW")] + \
+               [(n, ctypes.c_double) for n in ("logA", "b", "EaR", "logprA", "prb", "prEaR", "nusum")]
+
+
+class OTb(ctypes.Structure):
+    _fields_ = [("defeff", ctypes.c_double), ("neff", ctypes.c_int), ("effsp", ctypes.c_int * 16),
+                ("effdev", ctypes.c_double * 16)]
+
+
+class OMech(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nr", "ntb", "nlfc", "ng")] + \
+               [("rxn", ctypes.POINTER(ORxn)), ("tb", ctypes.POINTER(OTb)),
+                ("lfcpoly", ctypes.POINTER(ctypes.c_double)), ("gpoly", ctypes.POINTER(ctypes.c_double)),
+                ("h298", ctypes.POINTER(ctypes.c_double)), ("logform", ctypes.c_int), ("product", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in ("logprefRu", "prefRu", "Rupref", "logcfloor", "maxgain", "troeuc",
+                                               "troeuhinv", "expclamp", "lfcfloor")]
 
 
 class OBlock(ctypes.Structure):
@@ -39,7 +68,67 @@ class OBlock(ctypes.Structure):
                 ("Q", ctypes.POINTER(ctypes.c_double)),
                 ("xcc", ctypes.POINTER(ctypes.c_double)), ("detJinv", ctypes.POINTER(ctypes.c_double)),
                 ("Jinv", ctypes.POINTER(ctypes.c_double)),
-                ("S", ctypes.POINTER(ctypes.c_double) * 3), ("xf", ctypes.POINTER(ctypes.c_double) * 3)]
+                ("S", ctypes.POINTER(ctypes.c_double) * 3), ("xf", ctypes.POINTER(ctypes.c_double) * 3),
+                ("Tg", ctypes.POINTER(ctypes.c_double))]
+
+
+def _side(sp, val):
+    """A padded row's real entries: those with a nonzero value (the padding is (0, 0))."""
+    return [(int(a), float(b)) for a, b in zip(sp, val) if b != 0.0]
+
+
+def build_mech(consts):
+    """The finite-rate tables of a mixture's constants as the oracle's structs
+    (the columns of FiniteRateModel.rxnconsts and its third-body sets)."""
+    import math
+
+    nr = int(consts["rxn_nr"])
+    rxns = (ORxn * max(nr, 1))()
+    for k in range(nr):
+        r = rxns[k]
+        r.kind, r.reversible, r.product = (int(consts["rxn_kind"][k]), int(consts["rxn_reversible"][k]),
+                                           int(consts["rxn_product"][k]))
+        r.tb, r.troe, r.nfcent = int(consts["rxn_tb"][k]), int(consts["rxn_troeidx"][k]), int(consts["rxn_nfcent"][k])
+        for name, sp, val in (("fwd", "rxn_fwdsp", "rxn_fwdorder"), ("react", "rxn_reactsp", "rxn_reactnu"),
+                              ("prod", "rxn_prodsp", "rxn_prodnu")):
+            row = _side(consts[sp][k], consts[val][k])
+            setattr(r, "n" + name, len(row))
+            for j, (a, b) in enumerate(row):
+                getattr(r, name + "sp")[j] = a
+                getattr(r, {"fwd": "fwdorder", "react": "reactnu", "prod": "prodnu"}[name])[j] = b
+        net = [(int(a), float(b), float(c)) for a, b, c in
+               zip(consts["rxn_netsp"][k], consts["rxn_netnu"][k], consts["rxn_netnuMW"][k]) if b != 0.0]
+        r.nnet = len(net)
+        for j, (a, b, c) in enumerate(net):
+            r.netsp[j], r.netnu[j], r.netnuMW[j] = a, b, c
+        for name in ("logA", "b", "EaR", "logprA", "prb", "prEaR", "nusum"):
+            setattr(r, name, float(consts["rxn_" + name][k]))
+    ntb = len(consts["tbdefeff"])
+    tbs = (OTb * max(ntb, 1))()
+    for j in range(ntb):
+        tbs[j].defeff = float(consts["tbdefeff"][j])
+        n = int(consts["tb_neff"][j])
+        tbs[j].neff = n
+        for i in range(n):
+            tbs[j].effsp[i] = int(consts["tb_effsp"][j][i])
+            tbs[j].effdev[i] = float(consts["tbeffdev"][j][i])
+    keep = dict(rxns=rxns, tbs=tbs, lfc=np.ascontiguousarray(consts["rxnlfcpoly"], dtype=np.float64).reshape(-1),
+                gpoly=np.ascontiguousarray(consts["gpoly"], dtype=np.float64),
+                h298=np.ascontiguousarray(consts["h298"], dtype=np.float64))
+    m = OMech()
+    m.nr, m.ntb = nr, ntb
+    m.nlfc = int(np.asarray(consts["rxnlfcpoly"]).shape[-1]) if np.asarray(consts["rxnlfcpoly"]).size else 0
+    m.ng = int(keep["gpoly"].shape[1])
+    m.rxn, m.tb = ctypes.cast(rxns, ctypes.POINTER(ORxn)), ctypes.cast(tbs, ctypes.POINTER(OTb))
+    m.lfcpoly, m.gpoly, m.h298 = _ptr(keep["lfc"]), _ptr(keep["gpoly"]), _ptr(keep["h298"])
+    product = consts["rxn_product"][:nr]
+    m.logform, m.product = int(not np.all(product == 1)), int(np.any(product == 1))
+    for name in ("logprefRu", "prefRu", "Rupref", "logcfloor", "maxgain", "troeuc", "troeuhinv"):
+        setattr(m, name, float(consts[name]))
+    m.expclamp = math.log(float(np.finfo(np.float64).max)) - math.log(2.0 * float(consts["maxgain"]))
+    m.lfcfloor = math.log(float(np.finfo(np.float64).tiny)) * 0.4342944819032518
+    keep["mech"] = m
+    return keep
 
 
 def _lib():
@@ -51,6 +140,9 @@ def _lib():
     lib.oracle_combine.restype = ctypes.c_int
     lib.oracle_kepaec_faces.restype = ctypes.c_int
     lib.oracle_advective_faces.restype = ctypes.c_int
+    for name in ("oracle_production", "oracle_gibbs", "oracle_tlog", "oracle_texp", "oracle_mathtables",
+                 "oracle_species_cph", "oracle_fromQ"):
+        getattr(lib, name).restype = ctypes.c_int
     return lib
 
 
@@ -157,8 +249,10 @@ class Oracle:
     LIMITERS = {None: 0, "koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
 
     def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0, primary="kepaec",
-                 recon="constant", limiter=None):
-        """constants: the mixture's tables; blocks/metrics may be empty for face-only use."""
+                 recon="constant", limiter=None, eos="cpg", trans="constant", chemistry=None):
+        """constants: the mixture's tables; blocks/metrics may be empty for face-only use.
+        eos "cpg" or "tpg", trans "constant" or "kinetic-theory", chemistry
+        None or "finite-rate" (coupled: the source begins dQ)."""
         self.lib = _lib()
         self.ns, self.ne = ns, 4 + ns
         self.blocks = blocks
@@ -182,10 +276,29 @@ class Oracle:
         hp = np.ascontiguousarray(np.asarray(constants["hpoly"])[:, 0], dtype=np.float64)
         self._tables["hpoly0"] = hp
         c.hpoly0 = _ptr(hp)
+        if eos == "tpg":
+            c.eos = 1
+            cpr = np.ascontiguousarray(constants["cppolyR"], dtype=np.float64)
+            hpoly = np.ascontiguousarray(constants["hpoly"], dtype=np.float64)
+            self._tables["cppolyR"], self._tables["hpoly"] = cpr, hpoly
+            c.ncp, c.cppolyR = cpr.shape[1], _ptr(cpr)
+            c.nh, c.hpoly = hpoly.shape[1], _ptr(hpoly)
+        if trans == "kinetic-theory":
+            c.trans = 1
+            mu = np.ascontiguousarray(constants["mupoly"], dtype=np.float64)
+            ka = np.ascontiguousarray(constants["kappapoly"], dtype=np.float64)
+            self._tables["mupoly"], self._tables["kappapoly"] = mu, ka
+            c.nmu, c.mupoly, c.nkappa, c.kappapoly = mu.shape[1], _ptr(mu), ka.shape[1], _ptr(ka)
+        self._mech = None
+        if chemistry == "finite-rate":
+            self._mech = build_mech(constants)
+            c.mech = ctypes.cast(ctypes.pointer(self._mech["mech"]), ctypes.c_void_p)
         self.case = c
         self.map = halo_map(blocks)
         self.nregs = NREGS[integrator]
         self.regs = [[np.zeros(self._shape(b)) for b in blocks] for _ in range(self.nregs)]
+        # each cell's last temperature, the iterative eos's starting guess
+        self.Tg = [np.zeros(self._shape(b)[:3]) for b in blocks]
 
     def _shape(self, blk):
         return tuple(n + 2 * blk.ng for n in blk.cells) + (self.ne,)
@@ -202,14 +315,43 @@ class Oracle:
             for a, d in enumerate("ijk"):
                 o.S[a] = _ptr(m[f"{d}S"])
                 o.xf[a] = _ptr(m[f"{d}xc"])
+            o.Tg = _ptr(self.Tg[n])
             keep.append(o)
         return obs
 
     def set_prims(self, prims):
-        for blk, q, Q in zip(self.blocks, prims, self.regs[0]):
+        for n, (q, Q) in enumerate(zip(prims, self.regs[0])):
             q = np.ascontiguousarray(q, dtype=np.float64)
             assert q.shape == Q.shape
-            self.lib.oracle_fromprims(ctypes.byref(self.case), _ptr(q), _ptr(Q), ctypes.c_long(Q.size // self.ne))
+            self.lib.oracle_fromprims(ctypes.byref(self.case), _ptr(q), _ptr(Q), ctypes.c_long(Q.size // self.ne),
+                                      _ptr(self.Tg[n]))
+
+    def production(self, rho, Y, T):
+        """omega[n, ns] of independent states, rho[n], Y[n, ns] every species, T[n]."""
+        rho, Y, T = (np.ascontiguousarray(x, dtype=np.float64) for x in (rho, Y, T))
+        out = np.zeros_like(Y)
+        self.lib.oracle_production(ctypes.byref(self.case), ctypes.c_long(len(T)), _ptr(rho), _ptr(Y), _ptr(T),
+                                   _ptr(out))
+        return out
+
+    def gibbs(self, T):
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        out = np.zeros((len(T), self.ns))
+        self.lib.oracle_gibbs(ctypes.byref(self.case), ctypes.c_long(len(T)), _ptr(T), _ptr(out))
+        return out
+
+    def species_cph(self, sp, T):
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        cp, h = np.zeros_like(T), np.zeros_like(T)
+        self.lib.oracle_species_cph(ctypes.byref(self.case), sp, ctypes.c_long(len(T)), _ptr(T), _ptr(cp), _ptr(h))
+        return cp, h
+
+    def fromQ(self, Q, Tguess):
+        """the state (p, T, rhoinv, rho, e, cp, gamma, c) of Q rows, each from its guess."""
+        Q, Tg = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, Tguess))
+        out = np.zeros((len(Tg), 8))
+        self.lib.oracle_fromQ(ctypes.byref(self.case), ctypes.c_long(len(Tg)), _ptr(Q), _ptr(Tg), _ptr(out))
+        return out
 
     def rhs(self, Q, dQ, faces=False, diffusive_only=False):
         """dQ of every block from Q; with faces, each block's [iF, jF, kF] too."""
@@ -242,6 +384,7 @@ class Oracle:
         self.lib.oracle_advective_faces(ctypes.byref(self.case), ctypes.c_long(S.shape[0]), _ptr(Q4), _ptr(S), _ptr(F))
         return F
 
+
     def kepaec_faces(self, QL, QR, S):
         """kepaec on independent faces, each side's state from its Q."""
         QL, QR, S = (np.ascontiguousarray(x, dtype=np.float64) for x in (QL, QR, S))
@@ -261,3 +404,23 @@ class Oracle:
                     self.lib.oracle_combine(*blk.cells, blk.ng, self.ne, _ptr(self.regs[out][b]),
                                             int(own is not None), ctypes.c_double(own or 0.0),
                                             len(reads), X, w, int(step), ctypes.c_double(dt))
+
+
+def tlog(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros_like(x)
+    _lib().oracle_tlog(ctypes.c_long(x.size), _ptr(x), _ptr(y))
+    return y
+
+
+def texp(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros_like(x)
+    _lib().oracle_texp(ctypes.c_long(x.size), _ptr(x), _ptr(y))
+    return y
+
+
+def mathtables():
+    lt, rt, et, sc = np.zeros(128), np.zeros(128), np.zeros(64), np.zeros(4)
+    _lib().oracle_mathtables(_ptr(lt), _ptr(rt), _ptr(et), _ptr(sc))
+    return lt, rt, et, sc

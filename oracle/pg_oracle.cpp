@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <cfloat>
 
 extern "C" {
 
@@ -36,6 +37,45 @@ struct OCase {
   int skip_adv;    // 1: the face fluxes hold the diffusive flux alone (a test's view)
   int recon;       // 0 constant, 1 muscl
   int limiter;     // 1 koren, 2 minmod, 3 mc, 4 superbee, 5 vanleer
+  int eos;         // 0 calorically perfect, 1 thermally perfect
+  int ncp;         // thermally perfect: terms of cppolyR, cp / R_sp in ln T times R_sp
+  const double *cppolyR;  // [ns][ncp]
+  int nh;          // terms of hpoly (0: the one term hpoly0)
+  const double *hpoly;    // [ns][nh]
+  int trans;       // 0 constant properties, 1 kinetic theory
+  int nmu, nkappa;        // kinetic theory: terms of the fits below
+  const double *mupoly, *kappapoly;  // [ns][nmu] sqrt(mu) / T^(1/4), [ns][nkappa] kappa / sqrt(T), in ln T
+  const struct OMech *mech;  // finite-rate chemistry, coupled; null for none
+};
+
+// one reaction, the columns of FiniteRateModel.rxnconsts
+// (simulator/mixture/chemistry/finiterate.py:122-160) with their counts
+enum { O_ELEMENTARY = 0, O_THREEBODY = 1, O_LINDEMANN = 2, O_TROE = 3, O_MAXSIDE = 8 };
+struct ORxn {
+  int kind, reversible, product, tb, troe, nfcent;
+  int nfwd, nreact, nprod, nnet;
+  int fwdsp[O_MAXSIDE], reactsp[O_MAXSIDE], prodsp[O_MAXSIDE], netsp[O_MAXSIDE];
+  double fwdorder[O_MAXSIDE], reactnu[O_MAXSIDE], prodnu[O_MAXSIDE], netnu[O_MAXSIDE], netnuMW[O_MAXSIDE];
+  double logA, b, EaR, logprA, prb, prEaR, nusum;
+};
+// a third-body set: default efficiency and the deviations from it
+struct OTb {
+  double defeff;
+  int neff;
+  int effsp[16];
+  double effdev[16];
+};
+struct OMech {
+  int nr, ntb, nlfc, ng;
+  const ORxn *rxn;
+  const OTb *tb;
+  const double *lfcpoly;  // [troe rows][nlfc]
+  const double *gpoly;    // [ns][ng]: g / Ru T in ln T, less h298 / T
+  const double *h298;     // [ns]
+  int logform, product;   // whether any reaction takes the log form / the product form
+  double logprefRu, prefRu, Rupref, logcfloor, maxgain, troeuc, troeuhinv;
+  double expclamp;        // ln(DBL_MAX) - ln(2 maxgain), as the host works it out
+  double lfcfloor;        // log10 of the smallest normal double, a centre without terms
 };
 
 struct OBlock {
@@ -43,6 +83,7 @@ struct OBlock {
   double *Q;                                // [nx+2g][ny+2g][nz+2g][ne]
   const double *xcc, *detJinv, *Jinv;       // cells: [..][3], [..], [..][3][3]
   const double *S[3], *xf[3];               // faces of axis a: [..][3]
+  double *Tg;                               // [..]: each cell's last T, an iterative eos's starting guess
 };
 
 // one halo cell of one block filled from a cell of another (the place kernel,
@@ -78,35 +119,90 @@ struct State {
 };
 enum { NSTATE = 8 };
 
-// mixmom, simulator/mixture/eos/kernels/mixing.mako:3-30; cpg's moments are
-// R <- Rsp, cp <- cp0, h298 <- h298R (simulator/mixture/eos/cpg/__init__.py)
+// mixmom, simulator/mixture/eos/kernels/mixing.mako:3-30: cpg's moments are
+// R <- Rsp, cp <- cp0, h298 <- h298R (simulator/mixture/eos/cpg/__init__.py),
+// tpg's R <- Rsp, cpcoeff[m] <- cppolyR[m], h298 <- h298R
+// (simulator/mixture/eos/tpg/model.py:7-9)
+enum { O_MAXTERMS = 16 };
 struct Mom {
   double R, cp, h298;
+  double cpcoeff[O_MAXTERMS];
 };
 template <class YF> Mom mixmom(const OCase &c, YF Y) {
-  Mom m{0.0, 0.0, 0.0};
+  Mom m{};
+  const bool tpg = c.eos == 1;
   double Ylast = 1.0;
   for (int n = 0; n < c.ns - 1; n++) {
     const double Yn = Y(n);
     Ylast -= Yn;
     m.R += Yn * c.Rsp[n];
-    m.cp += Yn * c.cp0[n];
+    if (tpg)
+      for (int t = 0; t < c.ncp; t++) m.cpcoeff[t] += Yn * c.cppolyR[n * c.ncp + t];
+    else
+      m.cp += Yn * c.cp0[n];
     m.h298 += Yn * c.h298R[n];
   }
-  m.R += Ylast * c.Rsp[c.ns - 1];
-  m.cp += Ylast * c.cp0[c.ns - 1];
-  m.h298 += Ylast * c.h298R[c.ns - 1];
+  const int L = c.ns - 1;
+  m.R += Ylast * c.Rsp[L];
+  if (tpg)
+    for (int t = 0; t < c.ncp; t++) m.cpcoeff[t] += Ylast * c.cppolyR[L * c.ncp + t];
+  else
+    m.cp += Ylast * c.cp0[L];
+  m.h298 += Ylast * c.h298R[L];
   return m;
 }
 
-// fromQ (simulator/euler/kernels/state/fromQ.mako:5-19), efromQ
-// (simulator/euler/kernels/solution.mako:10-12) and cpg's fromrhoE
-// (simulator/mixture/eos/cpg/kernels/eos.mako:5-15)
-State fromQ(const OCase &c, const double *Q) {
+// ideal_cph: cp and h per mass of the moments at T, h's coefficients built
+// from cp's in the same descent (simulator/mixture/caloric/tdepcp/kernels/caloric.mako:4-15)
+void ideal_cph(const OCase &c, const Mom &mom, double T, double &cp, double &h) {
+  const double u = std::log(T);
+  cp = 0.0;
+  h = 0.0;
+  double hcoeff = 0.0;
+  for (int m = c.ncp - 1; m >= 0; m--) {
+    cp = cp * u + mom.cpcoeff[m];
+    hcoeff = mom.cpcoeff[m] - (m + 1) * hcoeff;
+    h = h * u + hcoeff;
+  }
+  h = h * T + mom.h298;
+}
+
+// efromQ (simulator/euler/kernels/solution.mako:10-12)
+double efromQ(const double *Q, double rhoinv) {
+  return (Q[4] - 0.5 * ((Q[1]) * (Q[1]) + (Q[2]) * (Q[2]) + (Q[3]) * (Q[3])) * rhoinv) * rhoinv;
+}
+
+// fromQ (simulator/euler/kernels/state/fromQ.mako:5-19) with cpg's fromrhoE
+// (simulator/mixture/eos/cpg/kernels/eos.mako:5-15) or tpg's: Newton from the
+// cell's last T, 300 K below 1 K, at least three steps and at most twelve,
+// stopping once a step is within 1e5 eps of T; cp is left at the T before
+// the last step (simulator/mixture/eos/tpg/kernels/eos.mako:8-20,
+// simulator/mixture/eos/tpg/kernels/newton.mako:3-10)
+State fromQ(const OCase &c, const double *Q, double Tguess = 0.0) {
   const double rho = Q[0], rhoinv = 1.0 / rho;
-  const double e = (Q[4] - 0.5 * ((Q[1]) * (Q[1]) + (Q[2]) * (Q[2]) + (Q[3]) * (Q[3])) * rhoinv) * rhoinv;
+  const double e = efromQ(Q, rhoinv);
   Mom mom = mixmom(c, [&](int n) { return Q[5 + n] * rhoinv; });
   State s;
+  if (c.eos == 1) {
+    double T = (Tguess < 1.0) ? 300.0 : Tguess;
+    double cp = 0.0, h = 0.0;
+    const double tol = 1e5 * DBL_EPSILON;
+    for (int k = 0; k < 12; k++) {
+      ideal_cph(c, mom, T, cp, h);
+      const double dT = (e - (h - mom.R * T)) / (cp - mom.R);
+      T += dT;
+      if (k >= 2 && std::fabs(dT) <= tol * T) break;
+    }
+    s.rho = rho;
+    s.rhoinv = 1.0 / rho;
+    s.e = e;
+    s.T = T;
+    s.p = rho * mom.R * T;
+    s.cp = cp;
+    s.gamma = cp / (cp - mom.R);
+    s.c = std::sqrt(s.gamma * mom.R * T);
+    return s;
+  }
   const double cv = mom.cp - mom.R;
   s.rho = rho;
   s.rhoinv = 1.0 / rho;
@@ -119,21 +215,43 @@ State fromQ(const OCase &c, const double *Q) {
   return s;
 }
 
+// frompT: cpg (simulator/mixture/eos/cpg/kernels/eos.mako:17-27), tpg
+// (simulator/mixture/eos/tpg/kernels/eos.mako:22-32)
+State frompT(const OCase &c, double p, double T, const double *Y) {
+  Mom mom = mixmom(c, [&](int n) { return Y[n]; });
+  State s;
+  s.p = p;
+  s.T = T;
+  s.rho = p / (mom.R * T);
+  s.rhoinv = 1.0 / s.rho;
+  if (c.eos == 1) {
+    double cp, h;
+    ideal_cph(c, mom, T, cp, h);
+    s.e = h - mom.R * T;
+    s.cp = cp;
+    s.gamma = cp / (cp - mom.R);
+  } else {
+    const double cv = mom.cp - mom.R;
+    s.e = cv * T + mom.h298;
+    s.cp = mom.cp;
+    s.gamma = mom.cp / cv;
+  }
+  s.c = std::sqrt(s.gamma * mom.R * T);
+  return s;
+}
+
 // fromprims (simulator/euler/kernels/state/fromprims.mako:4-12 through
-// solution.mako:2-23 and cpg's frompT, eos.mako:17-27)
-void fromprims(const OCase &c, const double *q, double *Q) {
-  const double p = q[0], T = q[4];
+// solution.mako:2-23 and the eos's frompT); returns the stored T
+double fromprims(const OCase &c, const double *q, double *Q) {
   const double u[3] = {q[1], q[2], q[3]};
-  Mom mom = mixmom(c, [&](int n) { return q[5 + n]; });
-  const double cv = mom.cp - mom.R;
-  const double rho = p / (mom.R * T);
-  const double e = cv * T + mom.h298;
-  Q[0] = rho;
-  Q[1] = rho * u[0];
-  Q[2] = rho * u[1];
-  Q[3] = rho * u[2];
-  Q[4] = rho * (e + 0.5 * ((u[0]) * (u[0]) + (u[1]) * (u[1]) + (u[2]) * (u[2])));
-  for (int n = 0; n < c.ns - 1; n++) Q[5 + n] = rho * q[5 + n];
+  const State th = frompT(c, q[0], q[4], q + 5);
+  Q[0] = th.rho;
+  Q[1] = th.rho * u[0];
+  Q[2] = th.rho * u[1];
+  Q[3] = th.rho * u[2];
+  Q[4] = th.rho * (th.e + 0.5 * ((u[0]) * (u[0]) + (u[1]) * (u[1]) + (u[2]) * (u[2])));
+  for (int n = 0; n < c.ns - 1; n++) Q[5 + n] = th.rho * q[5 + n];
+  return th.T;
 }
 
 // transport (simulator/navstokes/kernels/transport.mako:5-35) with constant
@@ -153,9 +271,20 @@ void transport(const OCase &c, const double *Q, const State &st, double *tr, dou
   for (int n = 0; n < ns; n++) denom += Y(n) * c.MWinv[n];
   const double MWmix = 1.0 / denom;
   auto X = [&](int n) { return Y(n) * c.MWinv[n] * MWmix; };
-  const double T = st.T;
+  const double T = st.T, lnT = std::log(T);
   std::vector<double> sqrtmu(ns), sinv(ns), kappasp(ns);
-  for (int n = 0; n < ns; n++) sqrtmu[n] = std::sqrt(c.mu0[n]);
+  // dilute kinetic theory (simulator/mixture/transport/kernels/dilute.mako:5-26)
+  // or constant properties (simulator/mixture/transport/kernels/constant.mako:5-16)
+  const double sqrtT = std::sqrt(T), sqrtsqrtT = std::sqrt(sqrtT);
+  for (int n = 0; n < ns; n++) {
+    if (c.trans == 1) {
+      double fit = 0.0;
+      for (int m = c.nmu - 1; m >= 0; m--) fit = fit * lnT + c.mupoly[n * c.nmu + m];
+      sqrtmu[n] = fit * sqrtsqrtT;
+    } else {
+      sqrtmu[n] = std::sqrt(c.mu0[n]);
+    }
+  }
   for (int n = 0; n < ns; n++) sinv[n] = 1.0 / (sqrtmu[n] * c.MWqinv[n]);
   double mu = 0.0;
   for (int n = 0; n < ns; n++) {
@@ -167,7 +296,15 @@ void transport(const OCase &c, const double *Q, const State &st, double *tr, dou
     }
     mu += sqrtmu[n] * sqrtmu[n] * X(n) / phi;
   }
-  for (int n = 0; n < ns; n++) kappasp[n] = c.kappa0[n];
+  for (int n = 0; n < ns; n++) {
+    if (c.trans == 1) {
+      double fit = 0.0;
+      for (int m = c.nkappa - 1; m >= 0; m--) fit = fit * lnT + c.kappapoly[n * c.nkappa + m];
+      kappasp[n] = fit * sqrtT;
+    } else {
+      kappasp[n] = c.kappa0[n];
+    }
+  }
   double series = 0.0, parallel = 0.0;
   for (int n = 0; n < ns; n++) {
     series += X(n) * kappasp[n];
@@ -181,10 +318,222 @@ void transport(const OCase &c, const double *Q, const State &st, double *tr, dou
   const double u = std::log(T), Tinv = 1.0 / T;
   for (int n = 0; n < ns; n++) {
     double hRT = 0.0;
-    hRT = hRT * u + c.hpoly0[n];
+    if (c.nh > 0)
+      for (int m = c.nh - 1; m >= 0; m--) hRT = hRT * u + c.hpoly[n * c.nh + m];
+    else
+      hRT = hRT * u + c.hpoly0[n];
     hRT += c.h298[n] * Tinv;
     hsp[n] = hRT * T * c.Ru * c.MWinv[n];
   }
+}
+
+// tlog and texp: the reference's table log and exp
+// (peregrine/backend/base/kernels/mathfns.mako:6-53 on the tables of
+// peregrine/backend/base/mathfns.py:1-22): log x as e ln 2 + log m_k + a
+// fifth-degree series in u = m / m_k - 1 over 128 mantissa bins; exp x as
+// 2^n 2^(j/64) times a sixth-degree series in the remainder.
+struct MathTables {
+  double logtab[128], rcptab[128], exptab[64];
+  MathTables() {
+    for (int k = 0; k < 128; k++) {
+      const double m = 0.5 + (k + 0.5) / (2 * 128);
+      logtab[k] = std::log(m);
+      rcptab[k] = 1.0 / m;
+    }
+    for (int j = 0; j < 64; j++) exptab[j] = std::pow(2.0, j / 64.0);
+  }
+};
+const MathTables &mtab() {
+  static const MathTables t;
+  return t;
+}
+const double O_LN2 = 0x1.62e42fefa39efp-1;
+const double O_EXPK = 0x1.71547652b82fep+6;          // 64 / ln 2
+const double O_LN2BINS_HI = 0x1.62e42fefp-7;          // ln 2 / 64, the head's low 20 bits clear
+const double O_LN2BINS_LO = 0x1.473de6af278edp-40;    // the rest
+
+double tlog(double x) {
+  const MathTables &t = mtab();
+  long long bits;
+  std::memcpy(&bits, &x, sizeof bits);
+  const int expo = (int)((bits >> 52) & 0x7ff) - 1022;
+  const int bin = (int)((bits >> (52 - 7)) & 127);
+  bits = (bits & 0x000fffffffffffffLL) | 0x3fe0000000000000LL;
+  double mant;
+  std::memcpy(&mant, &bits, sizeof mant);
+  const double u = mant * t.rcptab[bin] - 1.0;
+  double series = 0.2;
+  series = series * u - 0.25;
+  series = series * u + 1.0 / 3.0;
+  series = series * u - 0.5;
+  series = series * u + 1.0;
+  return expo * O_LN2 + t.logtab[bin] + u * series;
+}
+
+double texp(double v) {
+  const MathTables &tb = mtab();
+  const double t = v * O_EXPK + 6755399441055744.0;
+  long long bits;
+  std::memcpy(&bits, &t, sizeof bits);
+  const int kexp = (int)bits, nexp = kexp >> 6;
+  const double kd = t - 6755399441055744.0;
+  const double r = (v - kd * O_LN2BINS_HI) - kd * O_LN2BINS_LO;
+  double series = 1.0 / 120.0;
+  series = series * r + 1.0 / 24.0;
+  series = series * r + 1.0 / 6.0;
+  series = series * r + 0.5;
+  series = series * r + 1.0;
+  series = series * r + 1.0;
+  const double m = tb.exptab[kexp & 63] * series;
+  std::memcpy(&bits, &m, sizeof bits);
+  bits += (long long)(nexp > -1022 ? nexp : -1022) << 52;
+  double y;
+  std::memcpy(&y, &bits, sizeof y);
+  return y;
+}
+
+// g / Ru T of species n at ln T u: gpoly's Horner plus h298 / T
+// (simulator/mixture/eos/kernels/species.mako:17-22)
+double gRTspecies(const OMech &m, int n, double u, double Tinv) {
+  double g = 0.0;
+  for (int t = m.ng - 1; t >= 0; t--) g = g * u + m.gpoly[n * m.ng + t];
+  return g + m.h298[n] * Tinv;
+}
+
+// a cell's rate state (simulator/mixture/chemistry/kernels/finiterate.mako:136-183)
+struct RateState {
+  double T, logT, Tinv, logprefRuT, prefRuT, prefRuTinv, ctot;
+  double logc[16], gRT[16], cG[16], logtb[16], ctb[16];
+};
+
+template <class YF>
+void ratestate(const OCase &c, RateState &s, double rho, YF Y, double T) {
+  const OMech &m = *c.mech;
+  s.T = T;
+  s.logT = tlog(T);
+  s.Tinv = 1.0 / T;
+  if (m.logform) s.logprefRuT = m.logprefRu - s.logT;
+  if (m.product) {
+    s.prefRuT = m.prefRu * s.Tinv;
+    s.prefRuTinv = m.Rupref * T;
+  }
+  s.ctot = 0.0;
+  for (int n = 0; n < c.ns; n++) {
+    const double cn = rho * Y(n) * c.MWinv[n];
+    s.ctot += cn;
+    s.gRT[n] = gRTspecies(m, n, s.logT, s.Tinv);
+    if (m.logform) s.logc[n] = std::fmax(m.logcfloor, tlog(cn));
+    if (m.product) s.cG[n] = std::fmax(cn, 0.0) * texp(s.gRT[n]);
+  }
+  for (int j = 0; j < m.ntb; j++) {
+    const OTb &tb = m.tb[j];
+    double ctbc = tb.defeff * s.ctot;
+    for (int i = 0; i < tb.neff; i++) {
+      const int sp = tb.effsp[i];
+      ctbc += tb.effdev[i] * (rho * Y(sp) * c.MWinv[sp]);
+    }
+    s.ctb[j] = ctbc;
+    s.logtb[j] = tlog(std::fmax(DBL_MIN, ctbc));
+  }
+}
+
+// Troe's broadening added to ln k (finiterate.mako:48-63)
+double troeblend(const OMech &m, const ORxn &r, const RateState &s, double logpr) {
+  const double log10e = 0.4342944819032518, ln10 = 2.302585092994046;
+  double lfc;
+  if (r.nfcent == 0) {
+    lfc = m.lfcfloor;
+  } else {
+    const double tf = (s.logT - m.troeuc) * m.troeuhinv;
+    const double *poly = m.lfcpoly + (long)r.troe * m.nlfc;
+    lfc = poly[m.nlfc - 1];
+    for (int k = m.nlfc - 2; k >= 0; k--) lfc = lfc * tf + poly[k];
+  }
+  const double C = -0.4 - 0.67 * lfc, N = 0.75 - 1.27 * lfc;
+  const double A = logpr * log10e + C, B = N - 0.14 * A, B2 = B * B;
+  return lfc * B2 / (B2 + A * A) * ln10;
+}
+
+// one reaction's net rate of progress: the product form (finiterate.mako:66-125)
+// or the log form (finiterate.mako:7-46 and the double fold, :201-214)
+double rate_of_progress(const OMech &m, const ORxn &r, const RateState &s) {
+  double lk = r.logA;
+  if (r.b != 0.0) lk += r.b * s.logT;
+  if (r.EaR != 0.0) lk -= r.EaR * s.Tinv;
+  const bool falloff = r.kind >= O_LINDEMANN, thirdbody = r.kind != O_ELEMENTARY;
+  double logpr = 0.0;
+  if (falloff) {
+    logpr = s.logtb[r.tb] + r.logprA;
+    if (r.prb != 0.0) logpr += r.prb * s.logT;
+    if (r.prEaR != 0.0) logpr -= r.prEaR * s.Tinv;
+  }
+  if (r.product) {
+    double pfac = 0.0;
+    if (falloff) {
+      const double pr = texp(std::fmin(logpr, m.expclamp));
+      pfac = pr / (1.0 + pr);
+    }
+    if (r.kind == O_TROE) lk += troeblend(m, r, s, logpr);
+    double xk = lk;
+    for (int j = 0; j < r.nreact; j++) xk -= r.reactnu[j] * s.gRT[r.reactsp[j]];
+    double K = texp(std::fmin(xk, m.expclamp));
+    if (thirdbody && !falloff) K *= s.ctb[r.tb];
+    if (falloff) K *= pfac;
+    double fwd = K;
+    for (int j = 0; j < r.nreact; j++)
+      for (int q = 0; q < (int)r.reactnu[j]; q++) fwd *= s.cG[r.reactsp[j]];
+    double rev = 0.0;
+    if (r.reversible) {
+      rev = K;
+      const int nu = (int)std::fabs(r.nusum);
+      for (int q = 0; q < nu; q++) rev *= r.nusum > 0 ? s.prefRuTinv : s.prefRuT;
+      for (int j = 0; j < r.nprod; j++)
+        for (int q = 0; q < (int)r.prodnu[j]; q++) rev *= s.cG[r.prodsp[j]];
+    }
+    return fwd - rev;
+  }
+  if (thirdbody && !falloff) lk += s.logtb[r.tb];
+  if (falloff) lk += std::fmin(logpr, 0.0) - std::log1p(texp(-std::fabs(logpr)));
+  if (r.kind == O_TROE) lk += troeblend(m, r, s, logpr);
+  double lrp = lk;
+  for (int j = 0; j < r.nfwd; j++) lrp += r.fwdorder[j] * s.logc[r.fwdsp[j]];
+  const double fwd = texp(std::fmin(lrp, m.expclamp));
+  if (!r.reversible) return fwd;
+  double diff = r.nusum != 0.0 ? r.nusum * s.logprefRuT : 0.0;
+  for (int j = 0; j < r.nnet; j++) diff -= r.netnu[j] * (s.gRT[r.netsp[j]] + s.logc[r.netsp[j]]);
+  const double rev = texp(std::fmin(lrp - diff, m.expclamp));
+  return fwd - rev;
+}
+
+// production: the net mass production rates, kg / m^3 / s (finiterate.mako:186-231)
+void production(const OCase &c, const RateState &s, double *omega) {
+  const OMech &m = *c.mech;
+  for (int n = 0; n < c.ns; n++) omega[n] = 0.0;
+  for (int k = 0; k < m.nr; k++) {
+    const ORxn &r = m.rxn[k];
+    const double rp = rate_of_progress(m, r, s);
+    for (int j = 0; j < r.nnet; j++) omega[r.netsp[j]] += r.netnuMW[j] * rp;
+  }
+}
+
+// cellrates: the clipped mass fractions (simulator/euler/kernels/solution.mako:25-38),
+// the rate state at the cell's T and the production rates
+// (simulator/chemint/kernels/cell.mako:5-12)
+void cellrates(const OCase &c, const double *Q, double T, double *omega) {
+  const int ns = c.ns;
+  const double rhoinv = 1.0 / Q[0];
+  double Ylast = 1.0, Ysum = 0.0;
+  for (int n = 0; n < ns - 1; n++) {
+    const double Yn = std::fmax(std::fmin(Q[5 + n] * rhoinv, 1.0), 0.0);
+    Ylast -= Yn;
+    Ysum += Yn;
+  }
+  const double Yscale = 1.0 / std::fmax(Ysum, 1.0);
+  Ylast = std::fmax(Ylast, 0.0);
+  auto Y = [&](int n) { return n < ns - 1 ? std::fmax(std::fmin(Q[5 + n] * rhoinv, 1.0), 0.0) * Yscale : Ylast; };
+  RateState s;
+  ratestate(c, s, Q[0], Y, T);
+  production(c, s, omega);
 }
 
 // a face's side: the cell's state plus its velocity as Q[1..3] / Q[0]
@@ -216,22 +565,6 @@ void kepaec(const OCase &c, const Side &L, const Side &R, const double *QL, cons
   const double ef = 2.0 * thL * thR / (thL + thR) + 0.5 * ((L.s.e - thL) + (R.s.e - thR));
   F[4] = ef * C + Kj + Pj;
   for (int n = 0; n < c.ns - 1; n++) F[5 + n] = 0.5 * (QR[5 + n] / QR[0] + QL[5 + n] / QL[0]) * C;
-}
-
-// cpg frompT (simulator/mixture/eos/cpg/kernels/eos.mako:17-27)
-State frompT(const OCase &c, double p, double T, const double *Y) {
-  Mom mom = mixmom(c, [&](int n) { return Y[n]; });
-  State s;
-  const double cv = mom.cp - mom.R;
-  s.p = p;
-  s.T = T;
-  s.rho = p / (mom.R * T);
-  s.rhoinv = 1.0 / s.rho;
-  s.e = cv * T + mom.h298;
-  s.cp = mom.cp;
-  s.gamma = mom.cp / cv;
-  s.c = std::sqrt(s.gamma * mom.R * T);
-  return s;
 }
 
 // b phi(a / b) of the limiters, b > 0 (simulator/euler/kernels/flux/recon/{koren,minmod,mc,superbee,vanleer}.mako)
@@ -539,7 +872,8 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
                           (k < B.ng || k >= d.Z - B.ng);
           if (out > 1) continue;
           const long at = d.at(i, j, k);
-          State st = fromQ(c, B.Q + at * ne);
+          State st = fromQ(c, B.Q + at * ne, B.Tg ? B.Tg[at] : 0.0);
+          if (B.Tg) B.Tg[at] = st.T;
           std::memcpy(&s.state[at * NSTATE], &st, sizeof(State));
           if (visc) {
             // the shallow range: interior plus one halo layer
@@ -636,8 +970,20 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
           const double *kFl = &s.F[2][fk.at(i, j, k) * ne], *kFh = &s.F[2][fk.at(i, j, k + 1) * ne];
           const long at = d.at(i, j, k);
           const double detJinv = B.detJinv[at];
-          for (int l = 0; l < ne; l++)
-            dQ[b][at * ne + l] = (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
+          if (c.mech) {
+            // coupled chemistry begins dQ with the carried species' production
+            // rates, the fluxes add to it (simulator/chemint/kernels/source.mako:3-10,
+            // cell.mako:14-19, applyflux.mako with append)
+            double omega[16], src[32];
+            cellrates(c, B.Q + at * ne, s.state[at * NSTATE + 1], omega);
+            for (int l = 0; l < 5; l++) src[l] = 0.0;
+            for (int n = 0; n < ns - 1; n++) src[5 + n] = omega[n];
+            for (int l = 0; l < ne; l++)
+              dQ[b][at * ne + l] = src[l] + (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
+          } else {
+            for (int l = 0; l < ne; l++)
+              dQ[b][at * ne + l] = (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
+          }
         }
   }
   return 0;
@@ -669,11 +1015,77 @@ int oracle_advective_faces(const OCase *cp, long n, const double *Q4, const doub
   return 0;
 }
 
-// fromprims over every cell a block has (interior and halos)
-int oracle_fromprims(const OCase *cp, const double *q, double *Q, long ncells) {
+// fromprims over every cell a block has (interior and halos); Tg, when not
+// null, receives each cell's stored T (the next fromQ's starting guess)
+int oracle_fromprims(const OCase *cp, const double *q, double *Q, long ncells, double *Tg) {
   const int ne = 4 + cp->ns;
 #pragma omp parallel for schedule(static)
-  for (long n = 0; n < ncells; n++) fromprims(*cp, q + n * ne, Q + n * ne);
+  for (long n = 0; n < ncells; n++) {
+    const double T = fromprims(*cp, q + n * ne, Q + n * ne);
+    if (Tg) Tg[n] = T;
+  }
+  return 0;
+}
+
+// the production rates of n independent states (rho, Y[ns] every species, T)
+// as the kernels form them: the rate state straight from Y, without the
+// clipping cellrates applies (the reference's numpy twin's view,
+// tests/mixture/rates.py:169-185)
+int oracle_production(const OCase *cp, long n, const double *rho, const double *Y, const double *T,
+                      double *omega) {
+  const int ns = cp->ns;
+  for (long q = 0; q < n; q++) {
+    RateState s;
+    ratestate(*cp, s, rho[q], [&](int k) { return Y[q * ns + k]; }, T[q]);
+    production(*cp, s, omega + q * ns);
+  }
+  return 0;
+}
+
+// g / Ru T of every species at n temperatures, ln T by tlog
+int oracle_gibbs(const OCase *cp, long n, const double *T, double *gRT) {
+  for (long q = 0; q < n; q++)
+    for (int k = 0; k < cp->ns; k++) gRT[q * cp->ns + k] = gRTspecies(*cp->mech, k, tlog(T[q]), 1.0 / T[q]);
+  return 0;
+}
+
+int oracle_tlog(long n, const double *x, double *y) {
+  for (long q = 0; q < n; q++) y[q] = tlog(x[q]);
+  return 0;
+}
+
+int oracle_texp(long n, const double *x, double *y) {
+  for (long q = 0; q < n; q++) y[q] = texp(x[q]);
+  return 0;
+}
+
+// the tables tlog and texp read, for a check against the reference's
+int oracle_mathtables(double *logtab, double *rcptab, double *exptab, double *scalars) {
+  const MathTables &t = mtab();
+  std::memcpy(logtab, t.logtab, sizeof t.logtab);
+  std::memcpy(rcptab, t.rcptab, sizeof t.rcptab);
+  std::memcpy(exptab, t.exptab, sizeof t.exptab);
+  scalars[0] = O_LN2, scalars[1] = O_EXPK, scalars[2] = O_LN2BINS_HI, scalars[3] = O_LN2BINS_LO;
+  return 0;
+}
+
+// cp and h of a pure species n at n temperatures by ideal_cph, per mass
+int oracle_species_cph(const OCase *cp, int sp, long n, const double *T, double *cpo, double *ho) {
+  const OCase &c = *cp;
+  for (long q = 0; q < n; q++) {
+    Mom mom = mixmom(c, [&](int k) { return k == sp ? 1.0 : 0.0; });
+    ideal_cph(c, mom, T[q], cpo[q], ho[q]);
+  }
+  return 0;
+}
+
+// the state of n cells from Q rows, each from its guess
+int oracle_fromQ(const OCase *cp, long n, const double *Q, const double *Tguess, double *state) {
+  const int ne = 4 + cp->ns;
+  for (long q = 0; q < n; q++) {
+    const State st = fromQ(*cp, Q + q * ne, Tguess[q]);
+    std::memcpy(state + q * NSTATE, &st, sizeof st);
+  }
   return 0;
 }
 

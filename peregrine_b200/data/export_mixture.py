@@ -1,0 +1,185 @@
+"""Writes a mixture's constant tables, as the reference's own mixture computes
+them, to an .npz that peregrine_b200 loads.
+
+    python -m peregrine_b200.data.export_mixture REFERENCE OUT.npz MECHANISM \\
+        [--keep H2,H,O,...] [--eos tpg] [--trans kinetic-theory] \\
+        [--chemistry finite-rate] [--trange 300 3500]
+
+The thermally perfect fits (cp, h and s in ln T), the kinetic-theory fits of
+mu and kappa, the reaction columns and the third-body sets are all worked out
+by the reference's Python (peregrine/simulator/mixture/mixture.py:54-58 and
+each model's ``constants``); this script runs that code once, offline, on a
+checkout of the reference, and stores the numbers.  The kernels then read the
+same doubles the reference would have written into its rendered kernels.
+``--keep`` restricts a Cantera-format mechanism to a species subset: its
+reactions among those species only, and third-body efficiencies of absent
+species dropped (the parser refuses them,
+peregrine/simulator/mixture/parser/base.py:46-51).
+
+The reference's package imports mako, mpi4py, h5py and lxml at module level
+for its code generation, MPI and files; none of those run on this path, so
+stub modules stand in for them.
+"""
+
+import argparse
+import os
+import re
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+# reaction kinds, shared with include/pgb200.h
+KINDS = {"elementary": 0, "three-body": 1, "lindemann": 2, "troe": 3}
+
+
+def _stub(name, **attrs):
+    m = types.ModuleType(name)
+    for k, v in attrs.items():
+        setattr(m, k, v)
+    sys.modules[name] = m
+    return m
+
+
+class _Any:
+    def __init__(self, *a, **k):
+        pass
+
+
+class _Comm:
+    rank, size = 0, 1
+
+    def Get_rank(self):
+        return 0
+
+    def Get_size(self):
+        return 1
+
+    def bcast(self, x, root=0):
+        return x
+
+    def Allreduce(self, *a, **k):
+        pass
+
+    def Barrier(self):
+        pass
+
+
+def install_stubs():
+    """Stand-ins for the modules the reference imports but this path never calls."""
+    mako = _stub("mako")
+    mako.runtime = _stub("mako.runtime", capture=lambda *a, **k: "", supports_caller=lambda f: f)
+    mako.lookup = _stub("mako.lookup", TemplateLookup=_Any)
+    mako.template = _stub("mako.template", Template=_Any)
+    MPI = types.SimpleNamespace(COMM_WORLD=_Comm(), IN_PLACE=None, MAX=None, SUM=None, Prequest=_Any,
+                                Request=_Any, Comm=_Comm)
+    m4 = _stub("mpi4py", MPI=MPI)
+    _stub("mpi4py.MPI", **vars(MPI))
+    m4.util = _stub("mpi4py.util")
+    m4.util.dtlib = _stub("mpi4py.util.dtlib", from_numpy_dtype=lambda d: d)
+    h5 = _stub("h5py", File=_Any)
+    for s in ("h5fd", "h5p", "h5s"):
+        setattr(h5, s, _stub("h5py." + s))
+    lx = _stub("lxml")
+    lx.etree = _stub("lxml.etree")
+    if "cantera" not in sys.modules:
+        _stub("cantera", add_directory=lambda *a, **k: None)
+
+
+def _species_of(equation):
+    out = []
+    for side in re.split(r"<=>|=>", equation.replace("(+M)", "")):
+        for term in side.split("+"):
+            t = re.sub(r"^[0-9.]+\s*", "", term.strip())
+            if t and t != "M":
+                out.append(t)
+    return out
+
+
+def subset(mechanism, keep, where):
+    """A Cantera-format mechanism cut to the species in keep, written under where."""
+    import yaml
+
+    with open(mechanism) as f:
+        src = yaml.safe_load(f)
+    keep = list(keep)
+    phase = dict(src["phases"][0], species=keep)
+    reactions = []
+    for r in src["reactions"]:
+        if all(s in keep for s in _species_of(r["equation"])):
+            r = dict(r)
+            if "efficiencies" in r:
+                r["efficiencies"] = {k: v for k, v in r["efficiencies"].items() if k in keep}
+            reactions.append(r)
+    out = dict(units=src["units"], phases=[phase], species=[s for s in src["species"] if s["name"] in keep],
+               reactions=reactions)
+    path = os.path.join(where, os.path.basename(mechanism))
+    with open(path, "w") as f:
+        yaml.safe_dump(out, f, sort_keys=False)
+    return path
+
+
+def reference_mixture(reference, species, eos="tpg", trans=None, chemistry=None, trange=(300.0, 3500.0)):
+    """The reference's Mixture for a config, from a checkout at reference."""
+    install_stubs()
+    if reference not in sys.path:
+        sys.path.insert(0, reference)
+    import peregrine as pg
+    from peregrine.simulator.mixture import get_mixture
+
+    cfg = pg.Config()
+    m = cfg["mixture"]
+    m["species"], m["eos"], m["trans"], m["chemistry"] = species, eos, trans, chemistry
+    m["T-range"] = tuple(trange)
+    return get_mixture(cfg)
+
+
+def tables(mix):
+    """Every table the kernels read, by the reference's names."""
+    out = {k: np.asarray(v, dtype=np.float64) for k, v in mix.constants().items()}
+    out["spnames"] = np.array(mix.spnames)
+    out["eos"] = np.array(mix.eos.name)
+    out["trans"] = np.array(mix.trans.name if mix.trans is not None else "")
+    out["ns"] = np.array(mix.ns)
+    if mix.chemistry is not None:
+        cols = mix.chemistry.rxnconsts(mix.species)
+        terms = mix.chemistry.terms(mix.species)
+        for k, v in cols.items():
+            if k == "type":
+                out["rxn_kind"] = np.array([KINDS[t] for t in v], dtype=np.int32)
+            else:
+                out["rxn_" + k] = np.asarray(v)
+        out["rxn_tb"] = np.array([-1 if r.tb is None else r.tb for r in terms.reactions], dtype=np.int32)
+        out["rxn_troeidx"] = np.array([-1 if r.troeidx is None else r.troeidx for r in terms.reactions],
+                                      dtype=np.int32)
+        out["tb_effsp"] = mix.chemistry.padded([[sp for sp, _ in t.eff] for t in terms.thirdbodies], np.int32)
+        out["tb_neff"] = np.array([len(t.eff) for t in terms.thirdbodies], dtype=np.int32)
+        out["chemistry"] = np.array(mix.chemistry.name)
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("reference")
+    ap.add_argument("out")
+    ap.add_argument("mechanism")
+    ap.add_argument("--keep", default=None)
+    ap.add_argument("--eos", default="tpg")
+    ap.add_argument("--trans", default=None)
+    ap.add_argument("--chemistry", default=None)
+    ap.add_argument("--trange", nargs=2, type=float, default=(300.0, 3500.0))
+    a = ap.parse_args(argv)
+    mech = a.mechanism
+    if not os.path.isfile(mech):
+        mech = os.path.join(a.reference, "peregrine", "simulator", "mixture", "database", "mechanisms", mech)
+    with tempfile.TemporaryDirectory() as tmp:
+        if a.keep:
+            mech = subset(mech, a.keep.split(","), tmp)
+        mix = reference_mixture(a.reference, mech, a.eos, a.trans, a.chemistry, a.trange)
+        np.savez(a.out, **tables(mix))
+    print(a.out, mix)
+
+
+if __name__ == "__main__":
+    main()

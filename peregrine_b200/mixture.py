@@ -14,7 +14,17 @@ its kernels as hex literals (peregrine/codegen/constants.py:13-20):
   (simulator/mixture/mixrule/wilke.py:8-14);
 * Lewis diffusion ``lewis``, one unless a species states its own
   (simulator/mixture/diffusion/lewis.py).
+
+A thermally perfect gas, kinetic-theory transport and finite-rate chemistry
+take tables the reference's own mixture code works out from its species
+database and mechanism files (polynomial refits in ln T, collision-integral
+fits, reaction columns).  Those are not restated here: they are read from an
+.npz that peregrine_b200/data/export_mixture.py wrote by running the
+reference's mixture once, offline.  Name such a table set (a file under
+peregrine_b200/data, or a path) as ``mixture.species``.
 """
+
+import os
 
 import numpy as np
 
@@ -26,11 +36,28 @@ TABLES = ("MW", "MWinv", "Rsp", "cp0", "h298R", "hpolyR0", "h298", "mu0", "kappa
           "MWqinv", "wilkepair", "lewis")
 
 
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+def load_tables(name):
+    """A mixture's tables as the reference's mixture wrote them: a file under
+    peregrine_b200/data by its stem, or a path to an .npz."""
+    path = name if os.path.isfile(name) else os.path.join(DATA, f"{name}.npz")
+    if not os.path.isfile(path):
+        raise FileNotFoundError(f"no mixture tables {name!r} (tried {path})")
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
 class Mixture:
     def __init__(self, cfgsect):
         species = cfgsect["species"]
+        self.tables = None
+        if isinstance(species, str):
+            self._from_tables(cfgsect, load_tables(species))
+            return
         if not isinstance(species, dict) or not species:
-            raise ValueError("mixture.species: this build takes a dict of name to data")
+            raise ValueError("mixture.species: a dict of name to data, or the name of a table set")
         self.cfgsect = cfgsect
         self.species = {k: dict(v) for k, v in species.items()}
         self.spnames = list(self.species)
@@ -48,11 +75,29 @@ class Mixture:
                     if need not in sp:
                         raise ValueError(f"constant needs {need} for {name}")
 
+    def _from_tables(self, cfgsect, tables):
+        self.cfgsect = cfgsect
+        self.tables = tables
+        self.spnames = [str(n) for n in tables["spnames"]]
+        self.ns = len(self.spnames)
+        self.species = {n: {"MW": float(m)} for n, m in zip(self.spnames, tables["MW"])}
+        self.eos, self.trans = cfgsect["eos"], cfgsect["trans"]
+        self.chemistry = cfgsect.get("chemistry")
+        made = str(tables["eos"])
+        if self.eos != made:
+            raise ValueError(f"mixture.eos {self.eos!r}: the tables were made for {made!r}")
+        if self.trans is not None and self.trans != str(tables["trans"]):
+            raise ValueError(f"mixture.trans {self.trans!r}: the tables were made for {str(tables['trans'])!r}")
+        if self.chemistry is not None and "rxn_nr" not in tables:
+            raise ValueError("mixture.chemistry: the tables carry no reactions")
+
     def collect(self, key, default=None):
         values = [sp.get(key, default) for sp in self.species.values()]
         return np.array(values, dtype=np.float64)
 
     def constants(self):
+        if self.tables is not None:
+            return dict(self.tables)
         MW = self.collect("MW")
         out = dict(Ru=np.array(Ru), MW=MW, MWinv=1.0 / MW, Rsp=Ru / MW)
         # calorically perfect: a constant cp is its own fit, exactly

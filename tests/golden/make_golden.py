@@ -20,7 +20,18 @@ What it records, each from the reference's own code:
   faces_riemann.npz  tests/simulator/oracle.py's hllc, rusanov and ausmup
                      fluxes on the two cells as they are, and on muscl's sides
                      under each of the five limiters, for four cells LL, L, R,
-                     RR around random faces of the binary gas.
+                     RR around random faces of the binary gas;
+  mathfns.npz        peregrine/backend/base/mathfns.py's tables for the table
+                     log and exp, and tests/mixture/rates.py's numpy twins of
+                     the kernels' tlog and texp on sample arguments;
+  rates_<mech>.npz   tests/mixture/rates.py's production rates (the kernels'
+                     form) on random states of the 9-species H2/O2/N2 subset of
+                     GRI-Mech 3.0 and of CH4_O2_FFCMY, with the reference's
+                     Gibbs functions, and the species' cp and h by the
+                     reference's own polynomial evaluation.
+
+The mixtures' constant tables themselves are written by
+peregrine_b200/data/export_mixture.py from the same reference code.
 """
 
 import json
@@ -67,6 +78,8 @@ class _Comm:
 
 
 def install_stubs():
+    if "cantera" not in sys.modules:
+        stub("cantera", add_directory=lambda *a, **k: None)
     mako = stub("mako")
     mako.runtime = stub("mako.runtime", capture=lambda *a, **k: "", supports_caller=lambda f: f)
     mako.lookup = stub("mako.lookup", TemplateLookup=_Any)
@@ -159,6 +172,52 @@ def faces4(orc, gas, n, rng):
     return out
 
 
+def mathfns():
+    from peregrine.backend.base import mathfns as mf
+    from tests.mixture import rates
+
+    rng = np.random.default_rng(20261205)
+    xl = np.concatenate([np.exp(rng.uniform(-700.0, 700.0, 4000)), rng.uniform(0.5, 2.0, 1000),
+                         [1.0, 2.0, 0.5, 5e-324, 2.2250738585072014e-308, 1.7976931348623157e308]])
+    xe = np.concatenate([rng.uniform(-745.0, 709.0, 4000), rng.uniform(-1.0, 1.0, 1000), [0.0, -708.4, 709.0]])
+    return dict(LOGTAB=np.array(mf.LOGTAB), RCPTAB=np.array(mf.RCPTAB), EXPTAB=np.array(mf.EXPTAB),
+                scalars=np.array([mf.LN2, mf.EXPK, mf.LN2BINS_HI, mf.LN2BINS_LO]), xlog=xl, tlog=rates.tlog(xl),
+                xexp=xe, texp=rates.texp(xe))
+
+
+def rates_of(reference, mech, keep, n, rng):
+    from peregrine_b200.data.export_mixture import reference_mixture, subset
+    from tests.mixture import rates
+    import tempfile
+
+    path = os.path.join(reference, "peregrine", "simulator", "mixture", "database", "mechanisms", mech)
+    with tempfile.TemporaryDirectory() as tmp:
+        if keep:
+            path = subset(path, keep, tmp)
+        mix = reference_mixture(reference, path, "tpg", "kinetic-theory", "finite-rate")
+    ns = mix.ns
+    rho, T, Y, omega, gRT = [], [], [], [], []
+    for trial in range(n):
+        y = rng.random(ns)
+        if trial % 4 == 3:
+            # trace and absent species: the log floor and the product form's zero concentrations
+            y[rng.random(ns) < 0.4] = 0.0
+            y[0] = max(y[0], 0.1)
+        y = y / y.sum()
+        p, t = rng.uniform(1e5, 30e5), rng.uniform(600.0, 2800.0)
+        r = rates.density(mix, y, t, p)
+        rho.append(r), T.append(t), Y.append(y)
+        omega.append(rates.production(mix, r, y, t))
+        gRT.append(mix.eos.gibbs(mix.species, [t], u=[rates.tlog(t)])[:, 0])
+    Ts = np.geomspace(300.0, 3500.0, 64)
+    ev = mix.eos.caloric.evaluate
+    sps = list(mix.species.values())
+    cpR = np.array([ev(sp["cppoly"], np.log(Ts)) for sp in sps]).T
+    hR = np.array([ev(sp["hpoly"], np.log(Ts)) * Ts + sp["h298"] for sp in sps]).T
+    return dict(rho=np.array(rho), T=np.array(T), Y=np.array(Y), omega=np.array(omega), gRT=np.array(gRT),
+                Ts=Ts, cpR=cpR, hR=hR)
+
+
 def metrics(GridBlock, rng):
     ng = 2
     shape = (7 + 2 * ng, 6 + 2 * ng, 5 + 2 * ng)
@@ -234,6 +293,12 @@ def main():
         json.dump(rk_tables(integrators), f, indent=1)
     binary = {k: dict(MW=v["MW"], cp0=v["cp0"]) for k, v in BINARY.items()}
     np.savez(os.path.join(HERE, "faces_riemann.npz"), **faces4(orc, binary, 256, np.random.default_rng(20261204)))
+    np.savez(os.path.join(HERE, "mathfns.npz"), **mathfns())
+    h2o2 = ["H2", "H", "O", "O2", "OH", "H2O", "HO2", "H2O2", "N2"]
+    np.savez(os.path.join(HERE, "rates_h2o2_gri30.npz"),
+             **rates_of(REF, "GRI30.yaml", h2o2, 96, np.random.default_rng(20261206)))
+    np.savez(os.path.join(HERE, "rates_ch4_o2_ffcmy.npz"),
+             **rates_of(REF, "CH4_O2_FFCMY.yaml", None, 96, np.random.default_rng(20261207)))
     with open(os.path.join(HERE, "gases.json"), "w") as f:
         json.dump(dict(air=air, binary=BINARY), f, indent=1)
     print("wrote", sorted(p for p in os.listdir(HERE) if not p.endswith(".py")))
