@@ -46,6 +46,9 @@ enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1 };
 enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2, PGB_FLUX_AUSMUP = 3 };
 enum { PGB_RECON_CONSTANT = 0, PGB_RECON_MUSCL = 1 };
 enum { PGB_TRANS_NONE = 0, PGB_TRANS_CONSTANT = 1, PGB_TRANS_KINETIC = 2 };
+/* chemistry: none, or finite-rate coupled into the right-hand side
+ * (peregrine/simulator/chemint/coupled.py) */
+enum { PGB_CHEM_NONE = 0, PGB_CHEM_COUPLED = 1 };
 /* the launch paths */
 enum { PGB_PATH_BATCHED = 0, PGB_PATH_PER_BLOCK = 1 };
 
@@ -73,7 +76,45 @@ typedef struct {
   int ns;         /* species, >= 1 */
   int nregs;      /* Runge-Kutta registers the integrator needs, dQ included */
   double alpha;   /* alpha-damping coefficient */
+  int chemistry;  /* PGB_CHEM_* */
 } pgb_physics;
+
+/* A finite-rate mechanism: the columns the reference's FiniteRateModel
+ * works out (peregrine/simulator/mixture/chemistry/finiterate.py:29-51,
+ * 122-160), one struct per reaction.  Species are numbered as the mixture's;
+ * a side lists its species with nonzero coefficients. */
+enum { PGB_RXN_ELEMENTARY = 0, PGB_RXN_THREEBODY = 1, PGB_RXN_LINDEMANN = 2, PGB_RXN_TROE = 3 };
+#define PGB_MAXSIDE 4
+#define PGB_MAXNET 8
+typedef struct {
+  int kind;        /* PGB_RXN_* */
+  int reversible;
+  int product;     /* 1: the product form, 0: the log form (finiterate.py:62-102) */
+  int tb;          /* third-body set, -1 for none */
+  int troe;        /* row of the Troe centre fit */
+  int nfcent;      /* terms of the Troe centre; 0 floors it */
+  int nfwd, nreact, nprod, nnet;
+  int fwdsp[PGB_MAXSIDE], reactsp[PGB_MAXSIDE], prodsp[PGB_MAXSIDE], netsp[PGB_MAXNET];
+  double fwdorder[PGB_MAXSIDE], reactnu[PGB_MAXSIDE], prodnu[PGB_MAXSIDE];
+  double netnu[PGB_MAXNET], netnuMW[PGB_MAXNET];
+  double logA, b, EaR;        /* ln k = logA + b ln T - EaR / T */
+  double logprA, prb, prEaR;  /* the falloff's pressure ratio, the same form */
+  double nusum;               /* the net stoichiometry's sum */
+} pgb_reaction;
+typedef struct {
+  double defeff;    /* default efficiency */
+  int neff;
+  int effsp[12];    /* species whose efficiency differs, and by how much */
+  double effdev[12];
+} pgb_thirdbody;
+typedef struct {
+  int nr, ntb, ntroe, nlfc, ng;
+  const pgb_reaction *rxn;   /* [nr] */
+  const pgb_thirdbody *tb;   /* [ntb] */
+  const double *lfcpoly;     /* [ntroe][nlfc]: Troe's log10 centre in (ln T - troeuc) troeuhinv */
+  const double *gpoly;       /* [ns][ng]: g / Ru T in ln T, less h298 / T (the "h298" table) */
+  double logprefRu, prefRu, Rupref, logcfloor, maxgain, troeuc, troeuhinv;
+} pgb_mechanism;
 
 /* One Runge-Kutta combine: out = [wout out +] sum_n w[n] X[n], dt multiplying
  * the last term when step is set (peregrine/integrators/kernels/combine.mako).
@@ -113,6 +154,15 @@ int pgb_case_destroy(pgb_case *c);
  * constants: "Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0",
  * "kappa0", "MWqinv", "wilkepair", "lewis") */
 int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long n);
+/* the thermally perfect gas reads "cppolyR" (cp in ln T times R_sp) and
+ * "hpoly" (h / R T), kinetic-theory transport "mupoly" and "kappapoly", each
+ * [ns][terms] with 1 to 8 terms (peregrine/simulator/mixture/eos/tpg/model.py,
+ * peregrine/simulator/mixture/transport/kinetic.py) */
+/* the case's finite-rate mechanism, copied; before finalize */
+int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m);
+/* net production rates omega[n][ns], kg / m^3 / s, of n states rho[n],
+ * Y[n][ns] (every species) and T[n], host arrays, by the device fold */
+int pgb_production(pgb_case *c, long n, const double *rho, const double *Y, const double *T, double *omega);
 /* a block of ni x nj x nk cells; its number is the order of the calls */
 int pgb_case_add_block(pgb_case *c, int ni, int nj, int nk, int *blk);
 /* face nface (1..6: i-low, i-high, j-low, j-high, k-low, k-high) of blk joins

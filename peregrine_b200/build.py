@@ -1,24 +1,40 @@
 """Builds libpgb200.so in the package directory, for sm_100a.
 
-    python -m peregrine_b200.build
+    python -m peregrine_b200.build [--force]
 
-nvcc cross-compiles without a GPU.  The library is built in-tree so it
-travels with the source to wherever it runs.
+nvcc cross-compiles without a GPU.  The host unit, the no-allocation unit
+and one per-block unit per species count (plain_tu.cu with PGB_NS = 1..12)
+compile in parallel into objects under _build/, then link into one shared
+library.  The library is built in-tree so it travels with the source to
+wherever it runs.
 """
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = [os.path.join(HERE, "csrc", "pgb_host.cu"), os.path.join(HERE, "csrc", "pgb_noalloc.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fused.cuh", "fused2.cuh", "layout.cuh", "physics.cuh", "plain.cuh")] + \
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+MAXNS = 12
+SOURCES = [os.path.join(CSRC, f) for f in ("pgb_host.cu", "pgb_noalloc.cu", "plain_tu.cu")]
+HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cuh", ".h"))] + \
           [os.path.join(ROOT, "include", "pgb200.h")]
 TARGET = os.path.join(HERE, "libpgb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-shared", f"-I{os.path.join(ROOT, 'include')}"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{os.path.join(ROOT, 'include')}"]
+
+
+def units():
+    """(source, object, extra flags) of every translation unit."""
+    out = [(os.path.join(CSRC, "pgb_host.cu"), os.path.join(OBJ, "pgb_host.o"), []),
+           (os.path.join(CSRC, "pgb_noalloc.cu"), os.path.join(OBJ, "pgb_noalloc.o"), [])]
+    for n in range(1, MAXNS + 1):
+        out.append((os.path.join(CSRC, "plain_tu.cu"), os.path.join(OBJ, f"plain_ns{n}.o"), [f"-DPGB_NS={n}"]))
+    return out
 
 
 def stale():
@@ -28,12 +44,26 @@ def stale():
     return any(os.path.getmtime(p) > built for p in SOURCES + HEADERS)
 
 
-def build(force=False, verbose=False):
+def build(force=False, verbose=False, jobs=None):
     if not force and not stale():
         return TARGET
-    cmd = [NVCC, *FLAGS, "-o", TARGET, *SOURCES]
+    os.makedirs(OBJ, exist_ok=True)
+
+    def compile_one(unit):
+        src, obj, extra = unit
+        cmd = [NVCC, *FLAGS, *extra, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(f"nvcc failed on {os.path.basename(src)} {' '.join(extra)}:\n{r.stderr}")
+        return obj
+
+    with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as pool:
+        objs = list(pool.map(compile_one, units()))
+    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", TARGET, *objs]
     if verbose:
-        print(" ".join(cmd))
+        print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     return TARGET
 

@@ -122,3 +122,93 @@ def rough_prims(metrics, ns, seed=0, speed=420.0):
             q[..., 5 + n] = (0.6 - 0.2 * step) / (ns - 1) * (1.0 + 0.3 * np.sin((n + 1) * x + y + ph[n]))
         out.append(q)
     return out
+
+
+# the reacting homogeneous field: stoichiometric H2/air (H2 : O2 : N2 = 2 : 1 : 3.76
+# by moles) at 1 atm and 1000 K, Gaussian hot spots and a divergence-free velocity
+H2O2_TABLES = "h2o2_gri30"
+
+
+def reacting_config(simulator="navier-stokes", integrator="tvd-rk3", primary="hllc", recon="muscl", limiter="koren",
+                    chemistry=True, tables=H2O2_TABLES, launch="per-block"):
+    """The 9-species H2/O2/N2 mixture (the GRI-Mech 3.0 subset, thermally
+    perfect, kinetic-theory transport, finite-rate chemistry coupled)."""
+    cfg = Config()
+    cfg["simulation"]["simulator"] = simulator
+    cfg["mixture"]["species"] = tables
+    cfg["mixture"]["eos"] = "tpg"
+    cfg["mixture"]["trans"] = "kinetic-theory" if simulator == "navier-stokes" else None
+    cfg["mixture"]["chemistry"] = "finite-rate" if chemistry else None
+    cfg["chem-integration"]["kind"] = "coupled" if chemistry else None
+    cfg["time-integration"]["integrator"] = integrator
+    cfg["adv-flux"]["primary"] = primary
+    cfg["adv-flux"]["recon"] = recon
+    cfg["adv-flux"]["limiter"] = limiter if recon == "muscl" else None
+    cfg["backend-b200"]["launch"] = launch
+    return cfg.validate()
+
+
+def stoichiometric_h2_air(spnames, MW):
+    X = np.zeros(len(spnames))
+    for name, moles in (("H2", 2.0), ("O2", 1.0), ("N2", 3.76)):
+        X[spnames.index(name)] = moles
+    Y = X * np.asarray(MW)
+    return Y / Y.sum()
+
+
+def reacting_mesh(cells=96, blocks=(1, 1, 1), length=0.01):
+    """A periodic cube of side length (m) in cells^3, evenly cut."""
+    cuts = []
+    for n in blocks:
+        base = cells // n
+        cuts.append([base + (1 if m < cells - base * n else 0) for m in range(n)])
+    return CubeMesher(mbdims=list(blocks), cells=cuts, lengths=[length] * 3, periodic=[True] * 3)
+
+
+def reacting_prims(metrics, spnames, MW, cells, length=0.01, seed=0, spots=4, dT=400.0, width=8.0, urms=10.0,
+                   T0=1000.0, p0=101325.0, radicals=0.0):
+    """Primitives of the reacting field: seeded Gaussian hot spots (peak
+    dT, standard deviation width cells, periodic images) on T0, and the curl
+    of a seeded random vector potential of a few Fourier modes scaled to
+    u_rms, so the velocity is divergence free.  radicals > 0 seeds every
+    species absent from the mixture with random mass fractions up to that,
+    taken from the last species, so every reaction runs both ways."""
+    rng = np.random.default_rng(seed)
+    ns = len(spnames)
+    Y = stoichiometric_h2_air(list(spnames), MW)
+    centres = rng.uniform(0.0, length, (spots, 3))
+    amps = rng.uniform(0.5, 1.0, spots) * dT
+    sigma = width * length / cells
+    nk = 6
+    kvec = rng.integers(1, 4, (nk, 3)) * rng.choice([-1, 1], (nk, 3))
+    avec = rng.normal(0.0, 1.0, (nk, 3))
+    phase = rng.uniform(0.0, 2 * np.pi, nk)
+    out = []
+    vel = []
+    for m in metrics:
+        x = m["xcc"]
+        T = np.full(x.shape[:3], T0)
+        for c, a in zip(centres, amps):
+            d = x - c
+            d -= length * np.round(d / length)
+            T += a * np.exp(-0.5 * (d ** 2).sum(-1) / sigma ** 2)
+        # u = curl A, A = sum_k a_k sin(2 pi k.x / L + phi_k)
+        u = np.zeros(x.shape)
+        for k, a, ph in zip(kvec, avec, phase):
+            arg = 2 * np.pi * (x @ k) / length + ph
+            grad = np.cos(arg)[..., None] * (2 * np.pi * k / length)
+            u += np.cross(grad, a)
+        vel.append(u)
+        q = np.zeros(x.shape[:3] + (4 + ns,))
+        q[..., 0] = p0
+        q[..., 4] = T
+        q[..., 5:] = Y[:-1]
+        if radicals > 0.0:
+            for n in range(ns - 1):
+                if Y[n] == 0.0:
+                    q[..., 5 + n] = radicals * rng.uniform(0.0, 1.0, x.shape[:3])
+        out.append(q)
+    rms = np.sqrt(np.mean(np.concatenate([(u ** 2).sum(-1).ravel() / 3 for u in vel])))
+    for q, u in zip(out, vel):
+        q[..., 1:4] = u * (urms / rms)
+    return out

@@ -3,6 +3,7 @@
 #include "pgb200.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -16,8 +17,30 @@
 #include "layout.cuh"
 #include "physics.cuh"
 #include "plain.cuh"
+#include "plain_api.h"
 
 using namespace pgb;
+
+PGB_PLAIN_DECL(1)
+PGB_PLAIN_DECL(2)
+PGB_PLAIN_DECL(3)
+PGB_PLAIN_DECL(4)
+PGB_PLAIN_DECL(5)
+PGB_PLAIN_DECL(6)
+PGB_PLAIN_DECL(7)
+PGB_PLAIN_DECL(8)
+PGB_PLAIN_DECL(9)
+PGB_PLAIN_DECL(10)
+PGB_PLAIN_DECL(11)
+PGB_PLAIN_DECL(12)
+
+namespace {
+#define PGB_OPS(N) {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N}
+// the per-block path of each species count, 1 to MAXNS
+const PlainOps kPlain[MAXNS] = {PGB_OPS(1), PGB_OPS(2), PGB_OPS(3), PGB_OPS(4),  PGB_OPS(5),  PGB_OPS(6),
+                                PGB_OPS(7), PGB_OPS(8), PGB_OPS(9), PGB_OPS(10), PGB_OPS(11), PGB_OPS(12)};
+#undef PGB_OPS
+}  // namespace
 
 namespace {
 
@@ -111,6 +134,10 @@ struct pgb_case {
   size_t tnext = 0;
   double *d_stage = nullptr;  // whole-state staging
   long long stage_cap = 0;
+  // finite-rate chemistry: the mechanism's device tables
+  std::unique_ptr<Mech> mech;
+  unsigned long long uid = 0;  // unique over the process, never reused
+  unsigned version = 0;        // bumped when the species or mechanism tables change
 };
 
 namespace {
@@ -141,11 +168,59 @@ int build_species(pgb_case *c) {
   if (c->phys.trans == PGB_TRANS_CONSTANT && (!tab[T_MU0] || !tab[T_KAPPA0]))
     return fail(PGB_ERR_ARG, "constant transport needs mu0 and kappa0");
   species_fill(c->sp, ns, c->phys.alpha, c->phys.trans == PGB_TRANS_CONSTANT, tab, table(c, "wilkepair"));
+  // the thermally perfect fits and the kinetic-theory fits, [ns][terms]
+  auto fit = [&](const char *name, double *dst, int &terms) -> int {
+    auto it = c->tables.find(name);
+    if (it == c->tables.end()) return fail(PGB_ERR_ARG, std::string("table ") + name + " not set");
+    const long n = (long)it->second.size();
+    if (n % ns || n / ns < 1 || n / ns > MAXT)
+      return fail(PGB_ERR_ARG, std::string("table ") + name + ": species times 1 to 8 terms");
+    fit_fill(dst, terms, it->second.data(), ns, (int)(n / ns));
+    return PGB_OK;
+  };
+  if (c->phys.eos == PGB_EOS_TPG) {
+    c->sp.tpg = 1;
+    RET(fit("cppolyR", c->sp.cppolyR, c->sp.ncp));
+    RET(fit("hpoly", c->sp.hpoly, c->sp.nh));
+  }
+  if (c->phys.trans == PGB_TRANS_KINETIC) {
+    c->sp.kinetic = 1;
+    RET(fit("mupoly", c->sp.mupoly, c->sp.nmu));
+    RET(fit("kappapoly", c->sp.kappapoly, c->sp.nkappa));
+  }
+  if (c->phys.chemistry == PGB_CHEM_COUPLED && !c->mech)
+    return fail(PGB_ERR_STATE, "finite-rate chemistry needs pgb_case_set_mechanism before finalize");
+  c->version++;
   return PGB_OK;
 }
 
+// which case's tables each species count's unit holds, so a case's repeated
+// launches upload nothing
+struct Uploaded {
+  unsigned long long uid = 0;
+  unsigned version = 0;
+  int device = -1;
+  bool same(const pgb_case *c, int dev) const { return uid == c->uid && version == c->version && device == dev; }
+  void set(const pgb_case *c, int dev) { uid = c->uid, version = c->version, device = dev; }
+};
+Uploaded g_host_up, g_plain_up[MAXNS];
+unsigned long long g_next_uid = 0;
+
 int set_current(pgb_case *c) {
-  CK(cudaMemcpyToSymbolAsync(kSp, &c->sp, sizeof(Species), 0, cudaMemcpyHostToDevice, c->stream));
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (!g_host_up.same(c, dev)) {
+    CK(cudaMemcpyToSymbolAsync(kSp, &c->sp, sizeof(Species), 0, cudaMemcpyHostToDevice, c->stream));
+    g_host_up.set(c, dev);
+  }
+  Uploaded &u = g_plain_up[c->phys.ns - 1];
+  if (!u.same(c, dev)) {
+    static MathTables mt;
+    static bool filled = false;
+    if (!filled) math_tables_fill(mt), filled = true;
+    RET(kPlain[c->phys.ns - 1].upload(&c->sp, c->mech.get(), c->mech ? &mt : nullptr, c->stream));
+    u.set(c, dev);
+  }
   return PGB_OK;
 }
 
@@ -637,16 +712,25 @@ int step_fused(pgb_case *c, int &count) {
   return PGB_OK;
 }
 
-int ensure_scratch(pgb_case *c) {
+// the per-cell state, kept between right-hand sides: an iterative eos starts
+// from each cell's last T
+int ensure_state(pgb_case *c) {
   if (c->d_state) return PGB_OK;
-  const int ns = c->phys.ns, ne = c->ne, ngrad = ne - 1;
   const size_t n = (size_t)c->cells;
   CK(cudaMalloc(&c->d_state, sizeof(double) * 8 * n));
+  CK(cudaMemsetAsync(c->d_state, 0, sizeof(double) * 8 * n, c->stream));
+  return PGB_OK;
+}
+
+int ensure_scratch(pgb_case *c) {
+  RET(ensure_state(c));
+  if (c->d_tr) return PGB_OK;
+  const int ns = c->phys.ns, ne = c->ne, ngrad = ne - 1;
+  const size_t n = (size_t)c->cells;
   CK(cudaMalloc(&c->d_tr, sizeof(double) * (2 + ns) * n));
   CK(cudaMalloc(&c->d_hsp, sizeof(double) * ns * n));
   CK(cudaMalloc(&c->d_grads, sizeof(double) * 3 * ngrad * n));
   for (int a = 0; a < 3; a++) CK(cudaMalloc(&c->d_F[a], sizeof(double) * ne * n));
-  CK(cudaMemsetAsync(c->d_state, 0, sizeof(double) * 8 * n, c->stream));
   CK(cudaMemsetAsync(c->d_tr, 0, sizeof(double) * (2 + ns) * n, c->stream));
   CK(cudaMemsetAsync(c->d_hsp, 0, sizeof(double) * ns * n, c->stream));
   CK(cudaMemsetAsync(c->d_grads, 0, sizeof(double) * 3 * ngrad * n, c->stream));
@@ -654,93 +738,43 @@ int ensure_scratch(pgb_case *c) {
   return PGB_OK;
 }
 
-// the advective face flux of one axis of one block, by the case's flux
-// function and reconstruction
-template <int NS, int A, int FN>
-void launch_riemann(const pgb_case *c, int b, const double *Q, long long nf, int TH) {
-  const dim3 g = grid_for(nf, TH);
-  cudaStream_t s = c->stream;
-  double *F = c->d_F[A];
-  const int lim = c->phys.recon == PGB_RECON_MUSCL ? c->phys.limiter : 0;
-  switch (lim) {
-    case 0: k_riemann<NS, A, FN, 0><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
-    case LIM_KOREN: k_riemann<NS, A, FN, LIM_KOREN><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
-    case LIM_MINMOD: k_riemann<NS, A, FN, LIM_MINMOD><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
-    case LIM_MC: k_riemann<NS, A, FN, LIM_MC><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
-    case LIM_SUPERBEE: k_riemann<NS, A, FN, LIM_SUPERBEE><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
-    default: k_riemann<NS, A, FN, LIM_VANLEER><<<g, TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, F); break;
-  }
+struct MarkCtx {
+  pgb_case *c;
+  int *count;
+};
+
+void mark_cb(void *ctx, int kind) {
+  MarkCtx *m = (MarkCtx *)ctx;
+  mark(m->c, kind, *m->count);
 }
 
-template <int NS, int A>
-void launch_advflux(const pgb_case *c, int b, const double *Q, long long nf, int TH) {
-  switch (c->phys.primary) {
-    case PGB_FLUX_HLLC: launch_riemann<NS, A, FN_HLLC>(c, b, Q, nf, TH); break;
-    case PGB_FLUX_RUSANOV: launch_riemann<NS, A, FN_RUSANOV>(c, b, Q, nf, TH); break;
-    case PGB_FLUX_AUSMUP: launch_riemann<NS, A, FN_AUSMUP>(c, b, Q, nf, TH); break;
-    default: k_advflux<NS, A><<<grid_for(nf, TH), TH, 0, c->stream>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_F[A]);
-  }
-}
-
-template <int NS>
-int rhs_plain_ns(pgb_case *c, int qphys, int dqphys, int &count) {
-  const int TH = 256;
-  cudaStream_t s = c->stream;
-  double *Q = c->d_reg[qphys], *dQ = c->d_reg[dqphys];
-  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
-  constexpr int NE = 4 + NS;
-  k_halo<<<grid_for(c->nhalo, TH), TH, 0, s>>>(Q, c->d_halo, c->nhalo, NE);
-  mark(c, K_HALO, count);
-  for (int b = 0; b < (int)c->blocks.size(); b++) {
-    const BlockDev &D = c->blocks[b].dev;
-    const long long inner = (long long)D.nx * D.ny * D.nz;
-    k_fromQ<NS><<<grid_for(D.vol, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state);
-    mark(c, K_BLOCK, count);
-    if (visc) {
-      k_transport<NS><<<grid_for(D.vol, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp);
-      mark(c, K_BLOCK, count);
-      k_grads<NS><<<grid_for(inner, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_met, c->d_grads);
-      mark(c, K_BLOCK, count);
-    }
-  }
-  if (visc) {
-    k_halo<<<grid_for(c->nhalo_l0, TH), TH, 0, s>>>(c->d_grads, c->d_halo, c->nhalo_l0, 3 * (NE - 1));
-    mark(c, K_HALO, count);
-  }
-  for (int b = 0; b < (int)c->blocks.size(); b++) {
-    const BlockDev &D = c->blocks[b].dev;
-    const long long inner = (long long)D.nx * D.ny * D.nz;
-    const long long fx = (long long)(D.nx + 1) * D.ny * D.nz, fy = (long long)D.nx * (D.ny + 1) * D.nz,
-                    fz = (long long)D.nx * D.ny * (D.nz + 1);
-    launch_advflux<NS, 0>(c, b, Q, fx, TH);
-    mark(c, K_BLOCK, count);
-    launch_advflux<NS, 1>(c, b, Q, fy, TH);
-    mark(c, K_BLOCK, count);
-    launch_advflux<NS, 2>(c, b, Q, fz, TH);
-    mark(c, K_BLOCK, count);
-    if (visc) {
-      k_diffflux<NS, 0><<<grid_for(fx, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[0]);
-      mark(c, K_BLOCK, count);
-      k_diffflux<NS, 1><<<grid_for(fy, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[1]);
-      mark(c, K_BLOCK, count);
-      k_diffflux<NS, 2><<<grid_for(fz, TH), TH, 0, s>>>(c->d_blks, b, Q, c->d_state, c->d_tr, c->d_hsp, c->d_grads, c->d_met, c->d_F[2]);
-      mark(c, K_BLOCK, count);
-    }
-    k_applyflux<NS><<<grid_for(inner, TH), TH, 0, s>>>(c->d_blks, b, c->d_F[0], c->d_F[1], c->d_F[2], c->d_met, dQ);
-    mark(c, K_BLOCK, count);
-  }
-  CK(cudaGetLastError());
-  return PGB_OK;
+PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
+  hb.clear();
+  for (auto &B : c->blocks) hb.push_back(B.dev);
+  PlainCase pc{};
+  pc.d_blks = c->d_blks;
+  pc.h_blks = hb.data();
+  pc.nblocks = (int)hb.size();
+  pc.state = c->d_state, pc.tr = c->d_tr, pc.hsp = c->d_hsp, pc.grads = c->d_grads;
+  for (int a = 0; a < 3; a++) pc.F[a] = c->d_F[a];
+  pc.met = c->d_met;
+  pc.halo = c->d_halo;
+  pc.nhalo = c->nhalo, pc.nhalo_l0 = c->nhalo_l0;
+  pc.visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
+  pc.chem = c->phys.chemistry == PGB_CHEM_COUPLED;
+  pc.stream = c->stream;
+  return pc;
 }
 
 int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
   RET(ensure_scratch(c));
-  switch (c->phys.ns) {
-    case 1: return rhs_plain_ns<1>(c, qphys, dqphys, count);
-    case 2: return rhs_plain_ns<2>(c, qphys, dqphys, count);
-    case 3: return rhs_plain_ns<3>(c, qphys, dqphys, count);
-    default: return fail(PGB_ERR_UNSUPPORTED, "the per-block path takes 1 to 3 species in this build");
-  }
+  std::vector<BlockDev> hb;
+  PlainCase pc = plain_case(c, hb);
+  MarkCtx mc{c, &count};
+  pc.mark = mark_cb;
+  pc.ctx = &mc;
+  return kPlain[c->phys.ns - 1].rhs(&pc, c->d_reg[qphys], c->d_reg[dqphys]);
 }
 
 int step_plain(pgb_case *c, int &count) {
@@ -833,7 +867,8 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
   if (!phys || !out) return fail(PGB_ERR_ARG, "null argument");
   if (phys->ns < 1 || phys->ns > MAXNS) return fail(PGB_ERR_ARG, "ns out of range");
   if (phys->nregs < 2 || phys->nregs > MAXREGS) return fail(PGB_ERR_ARG, "nregs out of range");
-  if (phys->eos != PGB_EOS_CPG) return fail(PGB_ERR_UNSUPPORTED, "this build has the calorically perfect gas only");
+  if (phys->eos != PGB_EOS_CPG && phys->eos != PGB_EOS_TPG)
+    return fail(PGB_ERR_UNSUPPORTED, "this build has the calorically and thermally perfect gases");
   if (phys->primary < PGB_FLUX_KEPAEC || phys->primary > PGB_FLUX_AUSMUP)
     return fail(PGB_ERR_ARG, "no such flux function");
   if (phys->recon != PGB_RECON_CONSTANT && phys->recon != PGB_RECON_MUSCL)
@@ -842,9 +877,16 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
     return fail(PGB_ERR_ARG, "muscl needs a limiter: koren, minmod, mc, superbee or vanleer");
   if (phys->primary == PGB_FLUX_KEPAEC && phys->recon != PGB_RECON_CONSTANT)
     return fail(PGB_ERR_UNSUPPORTED, "kepaec is a two-point flux of the cells as they are; it takes no muscl sides");
-  if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT)
-    return fail(PGB_ERR_UNSUPPORTED, "this build has constant transport only");
+  if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT && phys->trans != PGB_TRANS_KINETIC)
+    return fail(PGB_ERR_UNSUPPORTED, "the viscous path takes constant or kinetic-theory transport");
+  if (phys->trans == PGB_TRANS_KINETIC && phys->eos != PGB_EOS_TPG)
+    return fail(PGB_ERR_ARG, "kinetic-theory transport needs the thermally perfect gas");
+  if (phys->chemistry != PGB_CHEM_NONE && phys->chemistry != PGB_CHEM_COUPLED)
+    return fail(PGB_ERR_UNSUPPORTED, "the chemistry takes none or coupled");
+  if (phys->chemistry == PGB_CHEM_COUPLED && phys->eos != PGB_EOS_TPG)
+    return fail(PGB_ERR_ARG, "finite-rate chemistry needs the thermally perfect gas");
   auto c = std::make_unique<pgb_case>();
+  c->uid = ++g_next_uid;
   c->phys = *phys;
   c->ne = 4 + phys->ns;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -876,7 +918,112 @@ int pgb_case_destroy(pgb_case *c) {
 int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long n) {
   if (!c || !name || (!values && n)) return fail(PGB_ERR_ARG, "null argument");
   if (n < 0) return fail(PGB_ERR_ARG, "negative size");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
   c->tables[name] = std::vector<double>(values, values + n);
+  return PGB_OK;
+}
+
+int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m) {
+  if (!c || !m) return fail(PGB_ERR_ARG, "null argument");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (c->phys.chemistry != PGB_CHEM_COUPLED) return fail(PGB_ERR_STATE, "the case has no chemistry");
+  const int ns = c->phys.ns;
+  if (m->nr < 0 || m->nr > MAXRXN) return fail(PGB_ERR_UNSUPPORTED, "at most 64 reactions in this build");
+  if (m->nr && !m->rxn) return fail(PGB_ERR_ARG, "null reactions");
+  if (m->ntb < 0 || m->ntb > MAXTB || (m->ntb && !m->tb)) return fail(PGB_ERR_UNSUPPORTED, "at most 8 third-body sets");
+  if (m->ntroe < 0 || m->ntroe > MAXTROE || m->nlfc < 0 || m->nlfc > MAXLFC || (m->ntroe && !m->lfcpoly))
+    return fail(PGB_ERR_UNSUPPORTED, "at most 8 Troe reactions of 16 fit terms");
+  if (m->ng < 1 || m->ng > MAXT + 1 || !m->gpoly) return fail(PGB_ERR_ARG, "the Gibbs fits take 1 to 9 terms");
+  if (!(m->maxgain > 0.0)) return fail(PGB_ERR_ARG, "maxgain is positive");
+  auto M = std::make_unique<Mech>();
+  std::memset(M.get(), 0, sizeof(Mech));
+  M->nr = m->nr, M->ntb = m->ntb, M->nlfc = m->nlfc, M->ngp = m->ng;
+  M->logprefRu = m->logprefRu, M->prefRu = m->prefRu, M->Rupref = m->Rupref, M->logcfloor = m->logcfloor;
+  M->troeuc = m->troeuc, M->troeuhinv = m->troeuhinv;
+  // the fold's clamp and the floor of a Troe centre with no terms, as the
+  // reference works them out on the host (finiterate.mako:128-133, 50-52)
+  M->expclamp = std::log(DBL_MAX) - std::log(2.0 * m->maxgain);
+  M->lfcfloor = std::log(DBL_MIN) * 0.4342944819032518;
+  for (int j = 0; j < m->ntb; j++) {
+    const pgb_thirdbody &t = m->tb[j];
+    if (t.neff < 0 || t.neff > ns) return fail(PGB_ERR_ARG, "a third-body set's efficiencies exceed the species");
+    M->tbdefeff[j] = t.defeff;
+    M->tbneff[j] = t.neff;
+    for (int i = 0; i < t.neff; i++) {
+      if (t.effsp[i] < 0 || t.effsp[i] >= ns) return fail(PGB_ERR_ARG, "a third body names no species");
+      M->tbeffsp[j][i] = t.effsp[i];
+      M->tbeffdev[j][i] = t.effdev[i];
+    }
+  }
+  for (int k = 0; k < m->ntroe; k++)
+    for (int t = 0; t < m->nlfc; t++) M->lfcpoly[k][t] = m->lfcpoly[k * m->nlfc + t];
+  for (int n = 0; n < ns; n++)
+    for (int t = 0; t < m->ng; t++) M->gpoly[n][t] = m->gpoly[n * m->ng + t];
+  bool logform = false, product = false;
+  for (int k = 0; k < m->nr; k++) {
+    const pgb_reaction &r = m->rxn[k];
+    Rxn &d = M->rxn[k];
+    if (r.kind < PGB_RXN_ELEMENTARY || r.kind > PGB_RXN_TROE) return fail(PGB_ERR_ARG, "no such reaction kind");
+    if ((r.kind != PGB_RXN_ELEMENTARY) && (r.tb < 0 || r.tb >= m->ntb))
+      return fail(PGB_ERR_ARG, "a third-body reaction names no set");
+    if (r.kind == PGB_RXN_TROE && r.nfcent > 0 && (r.troe < 0 || r.troe >= m->ntroe))
+      return fail(PGB_ERR_ARG, "a Troe reaction names no fit");
+    if (r.nfwd < 0 || r.nfwd > PGB_MAXSIDE || r.nreact < 0 || r.nreact > PGB_MAXSIDE || r.nprod < 0 ||
+        r.nprod > PGB_MAXSIDE || r.nnet < 0 || r.nnet > PGB_MAXNET)
+      return fail(PGB_ERR_UNSUPPORTED, "a reaction's side is longer than this build takes");
+    d.kind = r.kind, d.reversible = r.reversible, d.product = r.product, d.tb = r.tb, d.troe = r.troe;
+    d.nfcent = r.nfcent, d.nfwd = r.nfwd, d.nreact = r.nreact, d.nprod = r.nprod, d.nnet = r.nnet;
+    auto sp_ok = [&](int sp) { return sp >= 0 && sp < ns; };
+    for (int j = 0; j < r.nfwd; j++) {
+      if (!sp_ok(r.fwdsp[j])) return fail(PGB_ERR_ARG, "a reaction names no species");
+      d.fwdsp[j] = r.fwdsp[j], d.fwdorder[j] = r.fwdorder[j];
+    }
+    for (int j = 0; j < r.nreact; j++) {
+      if (!sp_ok(r.reactsp[j])) return fail(PGB_ERR_ARG, "a reaction names no species");
+      d.reactsp[j] = r.reactsp[j], d.reactnu[j] = r.reactnu[j];
+    }
+    for (int j = 0; j < r.nprod; j++) {
+      if (!sp_ok(r.prodsp[j])) return fail(PGB_ERR_ARG, "a reaction names no species");
+      d.prodsp[j] = r.prodsp[j], d.prodnu[j] = r.prodnu[j];
+    }
+    for (int j = 0; j < r.nnet; j++) {
+      if (!sp_ok(r.netsp[j])) return fail(PGB_ERR_ARG, "a reaction names no species");
+      d.netsp[j] = r.netsp[j], d.netnu[j] = r.netnu[j], d.netnuMW[j] = r.netnuMW[j];
+    }
+    d.logA = r.logA, d.b = r.b, d.EaR = r.EaR, d.logprA = r.logprA, d.prb = r.prb, d.prEaR = r.prEaR;
+    d.nusum = r.nusum;
+    (r.product ? product : logform) = true;
+  }
+  M->logform = logform, M->product = product;
+  c->mech = std::move(M);
+  c->version++;
+  return PGB_OK;
+}
+
+int pgb_production(pgb_case *c, long n, const double *rho, const double *Y, const double *T, double *omega) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (!c->mech) return fail(PGB_ERR_STATE, "the case has no mechanism");
+  if (n < 0 || (n && (!rho || !Y || !T || !omega))) return fail(PGB_ERR_ARG, "null arrays");
+  if (n == 0) return PGB_OK;
+  RET(set_current(c));
+  const int ns = c->phys.ns;
+  const size_t bytes = sizeof(double) * (size_t)n * (2 + 2 * ns);
+  double *d = nullptr;
+  CK(cudaMallocAsync((void **)&d, bytes, c->stream));
+  double *drho = d, *dT = d + n, *dY = d + 2 * n, *dw = d + 2 * n + (size_t)n * ns;
+  cudaError_t e = cudaMemcpyAsync(drho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dY, Y, sizeof(double) * n * ns, cudaMemcpyHostToDevice, c->stream);
+  int rc = PGB_OK;
+  if (e == cudaSuccess) rc = kPlain[ns - 1].production(n, drho, dY, dT, dw, c->stream);
+  if (e == cudaSuccess && rc == PGB_OK)
+    e = cudaMemcpyAsync(omega, dw, sizeof(double) * n * ns, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(d, c->stream);
+  const cudaError_t s = cudaStreamSynchronize(c->stream);
+  if (rc != PGB_OK) return rc;
+  if (e != cudaSuccess) return fail(PGB_ERR_CUDA, std::string("production copies: ") + cudaGetErrorString(e));
+  if (s != cudaSuccess) return fail(PGB_ERR_CUDA, std::string("production: ") + cudaGetErrorString(s));
   return PGB_OK;
 }
 
@@ -1067,18 +1214,12 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
   RET(check_reg(c, blk, reg, count, c->ne));
   if (!host) return fail(PGB_ERR_ARG, "null host array");
   RET(set_current(c));
+  RET(ensure_state(c));
   RET(stage_host(c, count));
   CK(cudaMemcpyAsync(c->d_prims, host, sizeof(double) * count, cudaMemcpyHostToDevice, c->stream));
-  const BlockDev &D = c->blocks[blk].dev;
-  const int g = grid_for((long long)D.nx * D.ny * D.nz, 256);
-  double *Q = c->d_reg[c->phys_of[reg]];
-  switch (c->phys.ns) {
-    case 1: k_fromprims<1><<<g, 256, 0, c->stream>>>(c->d_blks, blk, c->d_prims, Q); break;
-    case 2: k_fromprims<2><<<g, 256, 0, c->stream>>>(c->d_blks, blk, c->d_prims, Q); break;
-    case 3: k_fromprims<3><<<g, 256, 0, c->stream>>>(c->d_blks, blk, c->d_prims, Q); break;
-    default: return fail(PGB_ERR_UNSUPPORTED, "set_prims takes 1 to 3 species in this build");
-  }
-  CK(cudaGetLastError());
+  std::vector<BlockDev> hb;
+  const PlainCase pc = plain_case(c, hb);
+  RET(kPlain[c->phys.ns - 1].fromprims(&pc, blk, c->d_prims, c->d_reg[c->phys_of[reg]]));
   CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
 }

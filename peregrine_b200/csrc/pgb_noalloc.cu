@@ -67,6 +67,7 @@ extern "C" int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tabl
     return fail(PGB_ERR_UNSUPPORTED, "the calorically perfect gas with kepaec on the cells as they are");
   const bool visc = phys->simulator == PGB_NAVIER_STOKES;
   if (visc && phys->trans != PGB_TRANS_CONSTANT) return fail(PGB_ERR_UNSUPPORTED, "constant transport only");
+  if (phys->chemistry != PGB_CHEM_NONE) return fail(PGB_ERR_UNSUPPORTED, "no chemistry");
   if (nx < 2 || ny < 2 || nz < 2) return fail(PGB_ERR_ARG, "a block has at least two cells per axis");
   const long long X = nx + 2 * NG, Y = ny + 2 * NG, Z = nz + 2 * NG, V = X * Y * Z;
   const int ne = 4 + ns;

@@ -13,6 +13,7 @@
 namespace pgb {
 
 constexpr int MAXNS = 12;
+constexpr int MAXT = 8;  // terms of a fit in ln T
 
 // the case's species tables, in constant memory; filled per case before its
 // launches (a case's tables are copied in when the case is made current).
@@ -28,6 +29,13 @@ struct Species {
   // for Y = 1 (set by the host from the same operations)
   double R1, cp1, h2981, cv1, cvinv1, gamma1, th1;  // th1 = cp / gamma
   double mu1, kappa1;
+  // the thermally perfect gas and kinetic-theory transport: 0 / 1 selectors,
+  // and fits in ln T, [species][term]: cp (times R_sp), h over R T, sqrt(mu)
+  // over T^(1/4), kappa over sqrt(T) (peregrine/simulator/mixture/eos/tpg/model.py:7-9,
+  // peregrine/simulator/mixture/transport/kinetic.py)
+  int tpg, kinetic;
+  int ncp, nh, nmu, nkappa;
+  double cppolyR[MAXNS * MAXT], hpoly[MAXNS * MAXT], mupoly[MAXNS * MAXT], kappapoly[MAXNS * MAXT];
 };
 
 static __constant__ Species kSp;
@@ -55,6 +63,8 @@ inline void species_fill(Species &s, int ns, double alpha, bool constant_transpo
   s.gamma1 = s.cp1 / s.cv1;
   s.th1 = s.cp1 / s.gamma1;
   s.mu1 = s.kappa1 = 0.0;
+  s.tpg = s.kinetic = 0;
+  s.ncp = s.nh = s.nmu = s.nkappa = 0;
   if (ns == 1 && constant_transport) {
     volatile double Y = 1.0;
     const double denom = 0.0 + Y * s.MWinv[0];
@@ -70,6 +80,13 @@ inline void species_fill(Species &s, int ns, double alpha, bool constant_transpo
     const double parallel = 0.0 + X / s.kappa0[0];
     s.kappa1 = 0.5 * (series + 1.0 / parallel);
   }
+}
+
+// a fit table [ns][terms] into the constant struct's [species][MAXT]
+inline void fit_fill(double *dst, int &nterms, const double *src, int ns, int terms) {
+  nterms = terms;
+  for (int n = 0; n < ns; n++)
+    for (int t = 0; t < MAXT; t++) dst[n * MAXT + t] = t < terms ? src[n * terms + t] : 0.0;
 }
 
 // EosState (peregrine/simulator/mixture/eos/base.py:85-86)
@@ -95,16 +112,88 @@ __device__ __forceinline__ void mixmom(YF Y, double &R, double &cp, double &h298
   h298 += Ylast * kSp.h298R[NS - 1];
 }
 
-// fromQ + cpg fromrhoE (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19,
-// peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:5-15)
+// the thermally perfect moments: R, h298 and cp's coefficients in ln T, each
+// Y-weighted (peregrine/simulator/mixture/eos/kernels/mixing.mako:3-30 with
+// the moments of peregrine/simulator/mixture/eos/tpg/model.py:7-9)
+template <int NS, class YF>
+__device__ __forceinline__ void mixmom_tpg(YF Y, double &R, double &h298, double *cc) {
+  R = 0.0, h298 = 0.0;
+#pragma unroll
+  for (int t = 0; t < MAXT; t++) cc[t] = 0.0;
+  double Ylast = 1.0;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    const double Yn = Y(n);
+    Ylast -= Yn;
+    R += Yn * kSp.Rsp[n];
+    h298 += Yn * kSp.h298R[n];
+#pragma unroll
+    for (int t = 0; t < MAXT; t++)
+      if (t < kSp.ncp) cc[t] += Yn * kSp.cppolyR[n * MAXT + t];
+  }
+  R += Ylast * kSp.Rsp[NS - 1];
+  h298 += Ylast * kSp.h298R[NS - 1];
+#pragma unroll
+  for (int t = 0; t < MAXT; t++)
+    if (t < kSp.ncp) cc[t] += Ylast * kSp.cppolyR[(NS - 1) * MAXT + t];
+}
+
+// ideal_cph: cp and h per mass at T from the moments, h's coefficients built
+// from cp's in the same descent
+// (peregrine/simulator/mixture/caloric/tdepcp/kernels/caloric.mako:4-15)
+__device__ __forceinline__ void ideal_cph(const double *cc, const double h298, const double T, double &cp, double &h) {
+  const double u = log(T);
+  cp = 0.0;
+  h = 0.0;
+  double hcoeff = 0.0;
+#pragma unroll
+  for (int m = MAXT - 1; m >= 0; m--) {
+    if (m < kSp.ncp) {
+      cp = cp * u + cc[m];
+      hcoeff = cc[m] - (m + 1) * hcoeff;
+      h = h * u + hcoeff;
+    }
+  }
+  h = h * T + h298;
+}
+
+// fromQ (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19) with the
+// calorically perfect fromrhoE (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:5-15)
+// or the thermally perfect one: Newton from the cell's last T (300 K below
+// 1 K), at least three steps and at most twelve, done once a step is within
+// 1e5 eps of T; cp is left at the T before the last step
+// (peregrine/simulator/mixture/eos/tpg/kernels/eos.mako:8-20,
+//  peregrine/simulator/mixture/eos/tpg/kernels/newton.mako:3-10)
 template <int NS, class QF>
-__device__ __forceinline__ State fromQ(QF Q) {
+__device__ __forceinline__ State fromQ(QF Q, const double Tguess = 0.0) {
   const double rho = Q(0), rhoinv = 1.0 / rho;
   const double q1 = Q(1), q2 = Q(2), q3 = Q(3);
   const double e = (Q(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv) * rhoinv;
+  State s;
+  if (kSp.tpg) {
+    double R, h298, cc[MAXT];
+    mixmom_tpg<NS>([&](int n) { return Q(5 + n) * rhoinv; }, R, h298, cc);
+    double T = (Tguess < 1.0) ? 300.0 : Tguess;
+    double cp = 0.0, h = 0.0;
+    const double tol = 1e5 * 2.220446049250313e-16;
+    for (int k = 0; k < 12; k++) {
+      ideal_cph(cc, h298, T, cp, h);
+      const double dT = (e - (h - R * T)) / (cp - R);
+      T += dT;
+      if (k >= 2 && fabs(dT) <= tol * T) break;
+    }
+    s.rho = rho;
+    s.rhoinv = 1.0 / rho;
+    s.e = e;
+    s.T = T;
+    s.p = rho * R * T;
+    s.cp = cp;
+    s.gamma = cp / (cp - R);
+    s.c = sqrt(s.gamma * R * T);
+    return s;
+  }
   double R, cp, h298;
   mixmom<NS>([&](int n) { return Q(5 + n) * rhoinv; }, R, cp, h298);
-  State s;
   const double cv = cp - R;
   s.rho = rho;
   s.rhoinv = 1.0 / rho;
@@ -117,23 +206,52 @@ __device__ __forceinline__ State fromQ(QF Q) {
   return s;
 }
 
-// fromprims (peregrine/simulator/euler/kernels/state/fromprims.mako:4-12,
-// peregrine/simulator/euler/kernels/solution.mako:2-23, cpg frompT eos.mako:17-27)
-template <int NS>
-__device__ __forceinline__ void fromprims(const double *q, double *Q) {
-  const double p = q[0], T = q[4];
+// frompT: the calorically perfect (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:17-27)
+// or the thermally perfect (peregrine/simulator/mixture/eos/tpg/kernels/eos.mako:22-32)
+template <int NS, class YF>
+__device__ __forceinline__ State frompT(const double p, const double T, YF Y) {
+  State s;
+  s.p = p;
+  s.T = T;
+  if (kSp.tpg) {
+    double R, h298, cc[MAXT], cp, h;
+    mixmom_tpg<NS>(Y, R, h298, cc);
+    ideal_cph(cc, h298, T, cp, h);
+    s.rho = p / (R * T);
+    s.rhoinv = 1.0 / s.rho;
+    s.e = h - R * T;
+    s.cp = cp;
+    s.gamma = cp / (cp - R);
+    s.c = sqrt(s.gamma * R * T);
+    return s;
+  }
   double R, cp, h298;
-  mixmom<NS>([&](int n) { return q[5 + n]; }, R, cp, h298);
+  mixmom<NS>(Y, R, cp, h298);
   const double cv = cp - R;
-  const double rho = p / (R * T);
-  const double e = cv * T + h298;
+  s.rho = p / (R * T);
+  s.rhoinv = 1.0 / s.rho;
+  s.e = cv * T + h298;
+  s.cp = cp;
+  s.gamma = cp / cv;
+  s.c = sqrt(s.gamma * R * T);
+  return s;
+}
+
+// fromprims (peregrine/simulator/euler/kernels/state/fromprims.mako:4-12,
+// peregrine/simulator/euler/kernels/solution.mako:2-23 through the eos's
+// frompT); the state it stores is returned
+template <int NS>
+__device__ __forceinline__ State fromprims(const double *q, double *Q) {
+  const State th = frompT<NS>(q[0], q[4], [&](int n) { return q[5 + n]; });
+  const double rho = th.rho;
   Q[0] = rho;
   Q[1] = rho * q[1];
   Q[2] = rho * q[2];
   Q[3] = rho * q[3];
-  Q[4] = rho * (e + 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
+  Q[4] = rho * (th.e + 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
 #pragma unroll
   for (int n = 0; n < NS - 1; n++) Q[5 + n] = rho * q[5 + n];
+  return th;
 }
 
 // transport with constant species properties, Wilke, series/parallel
@@ -145,7 +263,7 @@ __device__ __forceinline__ void fromprims(const double *q, double *Q) {
 //  peregrine/simulator/mixture/diffusion/kernels/lewis.mako:3-8,
 //  peregrine/simulator/mixture/eos/kernels/species.mako:9-36)
 template <int NS, class QF>
-__device__ __forceinline__ void transport_constant(QF Q, const State &st, double *tr, double *hsp) {
+__device__ __forceinline__ void transport(QF Q, const State &st, double *tr, double *hsp) {
   const double rho = Q(0), rhoinv = 1.0 / rho;
   double Ylast = 1.0;
 #pragma unroll
@@ -159,9 +277,26 @@ __device__ __forceinline__ void transport_constant(QF Q, const State &st, double
   double X[NS];
 #pragma unroll
   for (int n = 0; n < NS; n++) X[n] = Y(n) * kSp.MWinv[n] * MWmix;
-  double sqrtmu[NS], sinv[NS];
+  double sqrtmu[NS], sinv[NS], kappasp[NS];
+  const double T = st.T, lnT = log(T);
+  if (kSp.kinetic) {
+    // dilute kinetic theory (peregrine/simulator/mixture/transport/kernels/dilute.mako:5-26)
+    const double sqrtT = sqrt(T), sqrtsqrtT = sqrt(sqrtT);
 #pragma unroll
-  for (int n = 0; n < NS; n++) sqrtmu[n] = sqrt(kSp.mu0[n]);
+    for (int n = 0; n < NS; n++) {
+      double fit = 0.0, fk = 0.0;
+#pragma unroll
+      for (int m = MAXT - 1; m >= 0; m--) {
+        if (m < kSp.nmu) fit = fit * lnT + kSp.mupoly[n * MAXT + m];
+        if (m < kSp.nkappa) fk = fk * lnT + kSp.kappapoly[n * MAXT + m];
+      }
+      sqrtmu[n] = fit * sqrtsqrtT;
+      kappasp[n] = fk * sqrtT;
+    }
+  } else {
+#pragma unroll
+    for (int n = 0; n < NS; n++) sqrtmu[n] = sqrt(kSp.mu0[n]), kappasp[n] = kSp.kappa0[n];
+  }
 #pragma unroll
   for (int n = 0; n < NS; n++) sinv[n] = 1.0 / (sqrtmu[n] * kSp.MWqinv[n]);
   double mu = 0.0;
@@ -179,8 +314,8 @@ __device__ __forceinline__ void transport_constant(QF Q, const State &st, double
   double series = 0.0, parallel = 0.0;
 #pragma unroll
   for (int n = 0; n < NS; n++) {
-    series += X[n] * kSp.kappa0[n];
-    parallel += X[n] / kSp.kappa0[n];
+    series += X[n] * kappasp[n];
+    parallel += X[n] / kappasp[n];
   }
   const double kappa = 0.5 * (series + 1.0 / parallel);
   tr[0] = mu;
@@ -188,11 +323,18 @@ __device__ __forceinline__ void transport_constant(QF Q, const State &st, double
   const double kor = kappa * rhoinv / st.cp;
 #pragma unroll
   for (int n = 0; n < NS; n++) tr[2 + n] = kor / kSp.lewis[n];
-  const double T = st.T, u = log(T), Tinv = 1.0 / T;
-  (void)u;
+  // hspecies (peregrine/simulator/mixture/eos/kernels/species.mako:9-15, 31-36)
+  const double u = lnT, Tinv = 1.0 / T;
 #pragma unroll
   for (int n = 0; n < NS; n++) {
-    double hRT = kSp.hpoly0[n];
+    double hRT = 0.0;
+    if (kSp.nh > 0) {
+#pragma unroll
+      for (int m = MAXT - 1; m >= 0; m--)
+        if (m < kSp.nh) hRT = hRT * u + kSp.hpoly[n * MAXT + m];
+    } else {
+      hRT = kSp.hpoly0[n];
+    }
     hRT += kSp.h298[n] * Tinv;
     hsp[n] = hRT * T * kSp.Ru * kSp.MWinv[n];
   }
@@ -230,50 +372,46 @@ struct RSide {
   double u, v, w, p, rho, e, c;
 };
 
-// cpg frompT onto a side (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:17-27)
+// frompT onto a side (the eos's frompT)
 template <int NS>
 __device__ __forceinline__ void side_frompT(const double p, const double T, const double *Y, RSide &s) {
-  double R, cp, h298;
-  mixmom<NS>([&](int n) { return Y[n]; }, R, cp, h298);
-  const double cv = cp - R;
-  s.p = p;
-  s.rho = p / (R * T);
-  s.e = cv * T + h298;
-  const double gamma = cp / cv;
-  s.c = sqrt(gamma * R * T);
+  const State th = frompT<NS>(p, T, [&](int n) { return Y[n]; });
+  s.p = th.p;
+  s.rho = th.rho;
+  s.e = th.e;
+  s.c = th.c;
 }
 
 // b phi(a / b) of the five limiters, b > 0, formed without the ratio
-// (peregrine/simulator/euler/kernels/flux/recon/{koren,minmod,mc,superbee,vanleer}.mako)
+// (peregrine/simulator/euler/kernels/flux/recon/{koren,minmod,mc,superbee,vanleer}.mako);
+// the limiter is the case's, the same for every thread
 enum { LIM_KOREN = 1, LIM_MINMOD = 2, LIM_MC = 3, LIM_SUPERBEE = 4, LIM_VANLEER = 5 };
-template <int LIM>
-__device__ __forceinline__ double bphi(const double a, const double b) {
-  if (LIM == LIM_KOREN) return fmax(0.0, fmin(fmin(2.0 * a, (2.0 * b + a) * (1.0 / 3.0)), 2.0 * b));
-  if (LIM == LIM_MINMOD) return fmax(0.0, fmin(b, a));
-  if (LIM == LIM_MC) return fmax(0.0, fmin(fmin(2.0 * a, (b + a) * 0.5), 2.0 * b));
-  if (LIM == LIM_SUPERBEE) return fmax(0.0, fmax(fmin(2.0 * a, b), fmin(a, 2.0 * b)));
-  return (a + fabs(a)) * b / (b + fabs(a));
+__device__ __forceinline__ double bphi(const int lim, const double a, const double b) {
+  switch (lim) {
+    case LIM_KOREN: return fmax(0.0, fmin(fmin(2.0 * a, (2.0 * b + a) * (1.0 / 3.0)), 2.0 * b));
+    case LIM_MINMOD: return fmax(0.0, fmin(b, a));
+    case LIM_MC: return fmax(0.0, fmin(fmin(2.0 * a, (b + a) * 0.5), 2.0 * b));
+    case LIM_SUPERBEE: return fmax(0.0, fmax(fmin(2.0 * a, b), fmin(a, 2.0 * b)));
+    default: return (a + fabs(a)) * b / (b + fabs(a));
+  }
 }
 
 // the limited slope across a face: the upwind difference dm carried to the
 // sign of the difference dp across the face, limited, and the sign put back;
 // none where dp is none (recon/muscl.mako:5-13)
-template <int LIM>
-__device__ __forceinline__ double phi(const double dm, const double dp) {
+__device__ __forceinline__ double phi(const int lim, const double dm, const double dp) {
   double ph = 0.0;
   if (dp != 0.0) {
     const double s = copysign(1.0, dp), a = s * dm, b = fabs(dp);
-    ph = s * bphi<LIM>(a, b);
+    ph = s * bphi(lim, a, b);
   }
   return ph;
 }
-template <int LIM>
-__device__ __forceinline__ double muscl_left(const double vLL, const double vL, const double vR) {
-  return vL + 0.5 * phi<LIM>(vL - vLL, vR - vL);
+__device__ __forceinline__ double muscl_left(const int lim, const double vLL, const double vL, const double vR) {
+  return vL + 0.5 * phi(lim, vL - vLL, vR - vL);
 }
-template <int LIM>
-__device__ __forceinline__ double muscl_right(const double vL, const double vR, const double vRR) {
-  return vR - 0.5 * phi<LIM>(vRR - vR, vR - vL);
+__device__ __forceinline__ double muscl_right(const int lim, const double vL, const double vR, const double vRR) {
+  return vR - 0.5 * phi(lim, vRR - vR, vR - vL);
 }
 
 // HLLC with Davis's outer wave speeds (peregrine/simulator/euler/kernels/flux/function/hllc.mako:2-43)

@@ -28,7 +28,8 @@ __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi,
   fk = (int)(r / B.Y);
 }
 
-// fromQ over the whole block, halo included: state[8] per cell
+// fromQ over the whole block, halo included: state[8] per cell, the cell's
+// last T the starting guess of an iterative eos
 // (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19)
 template <int NS>
 __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
@@ -37,9 +38,9 @@ __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
-  const State s = fromQ<NS>([&](int c) { return Q[c * B.vol]; });
   double *st = stall + 8 * B.cv + t;
   const long long v = B.vol;
+  const State s = fromQ<NS>([&](int c) { return Q[c * B.vol]; }, st[1 * v]);
   st[0 * v] = s.p, st[1 * v] = s.T, st[2 * v] = s.rhoinv, st[3 * v] = s.rho;
   st[4 * v] = s.e, st[5 * v] = s.cp, st[6 * v] = s.gamma, st[7 * v] = s.c;
 }
@@ -63,7 +64,7 @@ __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const doub
   const double *Q = Qall + (4 + NS) * B.cv + t;
   const State s = load_state(stall + 8 * B.cv + t, B.vol);
   double tr[2 + NS], h[NS];
-  transport_constant<NS>([&](int c) { return Q[c * B.vol]; }, s, tr, h);
+  transport<NS>([&](int c) { return Q[c * B.vol]; }, s, tr, h);
   double *trp = trall + (2 + NS) * B.cv + t;
   double *hp = hall + NS * B.cv + t;
 #pragma unroll
@@ -169,13 +170,13 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
 }
 
 // the advective face flux of a Riemann solver FN on the cells as they are
-// (LIM 0; recon/constant.mako:3-18) or on MUSCL's sides under limiter LIM
+// (lim 0; recon/constant.mako:3-18) or on MUSCL's sides under limiter lim
 // (recon/muscl.mako:15-51), both sides from the four cells LL, L, R, RR
 // along the axis (peregrine/simulator/euler/kernels/flux/single.mako:4-9)
-template <int NS, int A, int FN, int LIM>
+template <int NS, int A, int FN>
 __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                           const double *__restrict__ stall, const double *__restrict__ met,
-                          double *__restrict__ Fall) {
+                          double *__restrict__ Fall, const int lim) {
   constexpr int NE = 4 + NS, NY = NS > 1 ? NS - 1 : 1;
   const BlockDev &B = blks[b];
   int i, j, k;
@@ -190,7 +191,7 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
   const double S[3] = {Sp[0], Sp[v], Sp[2 * v]};
   RSide sl, sr;
   double YL[NY], YR[NY];
-  if (LIM == 0) {
+  if (lim == 0) {
     auto cell = [&](long long c, RSide &x, double *Y) {
       x.p = st[0 * v + c], x.rho = st[3 * v + c], x.e = st[4 * v + c], x.c = st[7 * v + c];
       x.u = Q[1 * v + c] / Q[c];
@@ -206,15 +207,15 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
     const double riLL = st[2 * v + LL], riL = st[2 * v + L], riR = st[2 * v + R], riRR = st[2 * v + RR];
     // a row of Q over rho on each side
     auto lft = [&](int row) {
-      return muscl_left<LIM>(Q[row * v + LL] * riLL, Q[row * v + L] * riL, Q[row * v + R] * riR);
+      return muscl_left(lim, Q[row * v + LL] * riLL, Q[row * v + L] * riL, Q[row * v + R] * riR);
     };
     auto rgt = [&](int row) {
-      return muscl_right<LIM>(Q[row * v + L] * riL, Q[row * v + R] * riR, Q[row * v + RR] * riRR);
+      return muscl_right(lim, Q[row * v + L] * riL, Q[row * v + R] * riR, Q[row * v + RR] * riRR);
     };
     // p and T from the state; Y and the velocity as Q times the cell's 1 / rho
-    const double pL = muscl_left<LIM>(st[LL], st[L], st[R]), pR = muscl_right<LIM>(st[L], st[R], st[RR]);
-    const double TL = muscl_left<LIM>(st[v + LL], st[v + L], st[v + R]);
-    const double TR = muscl_right<LIM>(st[v + L], st[v + R], st[v + RR]);
+    const double pL = muscl_left(lim, st[LL], st[L], st[R]), pR = muscl_right(lim, st[L], st[R], st[RR]);
+    const double TL = muscl_left(lim, st[v + LL], st[v + L], st[v + R]);
+    const double TR = muscl_right(lim, st[v + L], st[v + R], st[v + RR]);
 #pragma unroll
     for (int n = 0; n < NS - 1; n++) YL[n] = lft(5 + n), YR[n] = rgt(5 + n);
     side_frompT<NS>(pL, TL, YL, sl);
@@ -330,7 +331,7 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
 template <int NS>
 __global__ void k_applyflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Fi,
                             const double *__restrict__ Fj, const double *__restrict__ Fk,
-                            const double *__restrict__ met, double *__restrict__ dQall) {
+                            const double *__restrict__ met, double *__restrict__ dQall, int append = 0) {
   constexpr int NE = 4 + NS;
   const BlockDev &B = blks[b];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -341,9 +342,12 @@ __global__ void k_applyflux(const BlockDev *__restrict__ blks, int b, const doub
   const double detJinv = met[M_NCOMP * B.cv + M_DETJINV * v + c];
   const double *fi = Fi + NE * B.cv + c, *fj = Fj + NE * B.cv + c, *fk = Fk + NE * B.cv + c;
   double *dQ = dQall + NE * B.cv + c;
+  // with append, a source began dQ and the fluxes add to it (applyflux.mako's append)
 #pragma unroll
-  for (int l = 0; l < NE; l++)
-    dQ[l * v] = (fi[l * v] + fj[l * v] + fk[l * v] - fi[l * v + 1] - fj[l * v + sJ] - fk[l * v + sK]) * detJinv;
+  for (int l = 0; l < NE; l++) {
+    const double f = (fi[l * v] + fj[l * v] + fk[l * v] - fi[l * v + 1] - fj[l * v + sJ] - fk[l * v + sK]) * detJinv;
+    dQ[l * v] = append ? dQ[l * v] + f : f;
+  }
 }
 
 // one combine (peregrine/integrators/kernels/combine.mako:1-13) on a block's interior
@@ -379,10 +383,11 @@ static __global__ void k_combine(const BlockDev *__restrict__ blks, int b, int n
   }
 }
 
-// Q from primitives on the interior (the reference's fromprims)
+// Q and the state from primitives on the interior (the reference's fromprims);
+// the stored T is the next fromQ's starting guess
 template <int NS>
 __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const double *__restrict__ prims,
-                            double *__restrict__ Qall) {
+                            double *__restrict__ Qall, double *__restrict__ stall) {
   constexpr int NE = 4 + NS;
   const BlockDev &B = blks[b];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -393,10 +398,16 @@ __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const doub
   double q[NE], Q[NE];
 #pragma unroll
   for (int l = 0; l < NE; l++) q[l] = prims[l * n + t];
-  fromprims<NS>(q, Q);
+  const State th = fromprims<NS>(q, Q);
   double *Qo = Qall + NE * B.cv + c;
 #pragma unroll
   for (int l = 0; l < NE; l++) Qo[l * B.vol] = Q[l];
+  if (stall) {
+    double *st = stall + 8 * B.cv + c;
+    const long long v = B.vol;
+    st[0 * v] = th.p, st[1 * v] = th.T, st[2 * v] = th.rhoinv, st[3 * v] = th.rho;
+    st[4 * v] = th.e, st[5 * v] = th.cp, st[6 * v] = th.gamma, st[7 * v] = th.c;
+  }
 }
 
 // interior cells between a packed host-order buffer [comp][k][j][i] and a register

@@ -1,0 +1,47 @@
+// The per-block path's entry points, one set per species count: each is
+// compiled from plain_tu.cu with PGB_NS set, so a species count's kernels
+// build in their own translation unit (and in parallel).  Internal to the
+// library (hidden visibility); the C ABI is include/pgb200.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "chem_types.h"
+#include "layout.cuh"
+#include "physics.cuh"
+
+namespace pgb {
+
+// what a right-hand side on the per-block path reads of a case
+struct PlainCase {
+  const BlockDev *d_blks;  // device descriptors
+  const BlockDev *h_blks;  // the same on the host, for the launch sizes
+  int nblocks;
+  double *state, *tr, *hsp, *grads, *F[3];
+  const double *met;
+  const HaloEntry *halo;
+  long long nhalo, nhalo_l0;  // every halo entry; the first layer's
+  int visc, primary, recon, limiter, chem;
+  cudaStream_t stream;
+  void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block
+  void *ctx;
+};
+
+struct PlainOps {
+  int (*upload)(const Species *, const Mech *, const MathTables *, cudaStream_t);
+  int (*rhs)(const PlainCase *, const double *Q, double *dQ);
+  int (*fromprims)(const PlainCase *, int blk, const double *prims, double *Q);
+  int (*production)(long long n, const double *rho, const double *Y, const double *T, double *omega, cudaStream_t);
+};
+
+}  // namespace pgb
+
+#define PGB_PLAIN_DECL(N) PGB_PLAIN_DECL_I(N)
+#define PGB_PLAIN_DECL_I(N)                                                                                      \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_upload_##N(                                     \
+      const pgb::Species *, const pgb::Mech *, const pgb::MathTables *, cudaStream_t);                           \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_rhs_##N(const pgb::PlainCase *, const double *, \
+                                                                         double *);                              \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_fromprims_##N(const pgb::PlainCase *, int,      \
+                                                                               const double *, double *);        \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_production_##N(                                 \
+      long long, const double *, const double *, const double *, double *, cudaStream_t);

@@ -20,6 +20,66 @@ EOS_CPG, EOS_TPG = 0, 1
 FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV, FLUX_AUSMUP = 0, 1, 2, 3
 RECON_CONSTANT, RECON_MUSCL = 0, 1
 LIMITERS = {"koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
+CHEM_NONE, CHEM_COUPLED = 0, 1
+
+
+def mechanism(consts):
+    """The C ABI's mechanism struct from a mixture's tables (the columns of the
+    reference's FiniteRateModel.rxnconsts and its third-body sets); returns
+    the struct and the arrays it points into, which must outlive the call."""
+    import numpy as np
+
+    def side(sp, val):
+        return [(int(a), float(b)) for a, b in zip(sp, val) if b != 0.0]
+
+    nr = int(consts["rxn_nr"])
+    rxns = (Reaction * max(nr, 1))()
+    for k in range(nr):
+        r = rxns[k]
+        r.kind, r.reversible, r.product = (int(consts["rxn_kind"][k]), int(consts["rxn_reversible"][k]),
+                                           int(consts["rxn_product"][k]))
+        r.tb, r.troe, r.nfcent = int(consts["rxn_tb"][k]), int(consts["rxn_troeidx"][k]), int(consts["rxn_nfcent"][k])
+        for name, sp, val, coef in (("fwd", "rxn_fwdsp", "rxn_fwdorder", "fwdorder"),
+                                    ("react", "rxn_reactsp", "rxn_reactnu", "reactnu"),
+                                    ("prod", "rxn_prodsp", "rxn_prodnu", "prodnu")):
+            row = side(consts[sp][k], consts[val][k])
+            if len(row) > MAXSIDE:
+                raise ValueError(f"reaction {k}: more than {MAXSIDE} species on a side")
+            setattr(r, "n" + name, len(row))
+            for j, (a, b) in enumerate(row):
+                getattr(r, name + "sp")[j] = a
+                getattr(r, coef)[j] = b
+        net = [(int(a), float(b), float(c)) for a, b, c in
+               zip(consts["rxn_netsp"][k], consts["rxn_netnu"][k], consts["rxn_netnuMW"][k]) if b != 0.0]
+        if len(net) > MAXNET:
+            raise ValueError(f"reaction {k}: more than {MAXNET} species change")
+        r.nnet = len(net)
+        for j, (a, b, c) in enumerate(net):
+            r.netsp[j], r.netnu[j], r.netnuMW[j] = a, b, c
+        for name in ("logA", "b", "EaR", "logprA", "prb", "prEaR", "nusum"):
+            setattr(r, name, float(consts["rxn_" + name][k]))
+    ntb = len(consts["tbdefeff"])
+    tbs = (ThirdBody * max(ntb, 1))()
+    for j in range(ntb):
+        tbs[j].defeff = float(consts["tbdefeff"][j])
+        n = int(consts["tb_neff"][j])
+        tbs[j].neff = n
+        for i in range(n):
+            tbs[j].effsp[i] = int(consts["tb_effsp"][j][i])
+            tbs[j].effdev[i] = float(consts["tbeffdev"][j][i])
+    lfc = np.ascontiguousarray(consts["rxnlfcpoly"], dtype=np.float64)
+    gpoly = np.ascontiguousarray(consts["gpoly"], dtype=np.float64)
+    m = Mechanism()
+    m.nr, m.ntb = nr, ntb
+    m.ntroe = int(lfc.shape[0]) if lfc.ndim == 2 else 0
+    m.nlfc = int(lfc.shape[1]) if lfc.ndim == 2 else 0
+    m.ng = int(gpoly.shape[1])
+    m.rxn, m.tb = ctypes.cast(rxns, ctypes.POINTER(Reaction)), ctypes.cast(tbs, ctypes.POINTER(ThirdBody))
+    m.lfcpoly = lfc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    m.gpoly = gpoly.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    for name in ("logprefRu", "prefRu", "Rupref", "logcfloor", "maxgain", "troeuc", "troeuhinv"):
+        setattr(m, name, float(consts[name]))
+    return m, (rxns, tbs, lfc, gpoly)
 TRANS_NONE, TRANS_CONSTANT, TRANS_KINETIC = 0, 1, 2
 PATH_BATCHED, PATH_PER_BLOCK = 0, 1
 ARR_XCC, ARR_DETJINV, ARR_JINV, ARR_IS, ARR_JS, ARR_KS, ARR_IXC, ARR_JXC, ARR_KXC = range(9)
@@ -61,7 +121,35 @@ _ERRORS = {c.code: c for c in (PgbArgumentError, PgbStateError, PgbCudaError, Pg
 class Physics(ctypes.Structure):
     _fields_ = [("simulator", ctypes.c_int), ("eos", ctypes.c_int), ("primary", ctypes.c_int),
                 ("recon", ctypes.c_int), ("limiter", ctypes.c_int), ("trans", ctypes.c_int),
-                ("ns", ctypes.c_int), ("nregs", ctypes.c_int), ("alpha", ctypes.c_double)]
+                ("ns", ctypes.c_int), ("nregs", ctypes.c_int), ("alpha", ctypes.c_double),
+                ("chemistry", ctypes.c_int)]
+
+
+MAXSIDE, MAXNET = 4, 8
+
+
+class Reaction(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("kind", "reversible", "product", "tb", "troe", "nfcent", "nfwd",
+                                            "nreact", "nprod", "nnet")] + \
+               [("fwdsp", ctypes.c_int * MAXSIDE), ("reactsp", ctypes.c_int * MAXSIDE),
+                ("prodsp", ctypes.c_int * MAXSIDE), ("netsp", ctypes.c_int * MAXNET),
+                ("fwdorder", ctypes.c_double * MAXSIDE), ("reactnu", ctypes.c_double * MAXSIDE),
+                ("prodnu", ctypes.c_double * MAXSIDE), ("netnu", ctypes.c_double * MAXNET),
+                ("netnuMW", ctypes.c_double * MAXNET)] + \
+               [(n, ctypes.c_double) for n in ("logA", "b", "EaR", "logprA", "prb", "prEaR", "nusum")]
+
+
+class ThirdBody(ctypes.Structure):
+    _fields_ = [("defeff", ctypes.c_double), ("neff", ctypes.c_int), ("effsp", ctypes.c_int * 12),
+                ("effdev", ctypes.c_double * 12)]
+
+
+class Mechanism(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nr", "ntb", "ntroe", "nlfc", "ng")] + \
+               [("rxn", ctypes.POINTER(Reaction)), ("tb", ctypes.POINTER(ThirdBody)),
+                ("lfcpoly", ctypes.POINTER(ctypes.c_double)), ("gpoly", ctypes.POINTER(ctypes.c_double))] + \
+               [(n, ctypes.c_double) for n in ("logprefRu", "prefRu", "Rupref", "logcfloor", "maxgain", "troeuc",
+                                               "troeuhinv")]
 
 
 class Combine(ctypes.Structure):
@@ -86,6 +174,8 @@ SIGNATURES = {
     "pgb_case_create": ([ctypes.POINTER(Physics), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "pgb_case_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "pgb_case_set_table": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_case_set_mechanism": ([ctypes.c_void_p, ctypes.POINTER(Mechanism)], ctypes.c_int),
+    "pgb_production": ([ctypes.c_void_p, ctypes.c_long] + [ctypes.POINTER(ctypes.c_double)] * 4, ctypes.c_int),
     "pgb_case_add_block": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_case_connect": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_case_set_stages": ([ctypes.c_void_p, ctypes.POINTER(Stage), ctypes.c_int], ctypes.c_int),

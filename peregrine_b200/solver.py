@@ -113,7 +113,7 @@ class Solver:
         adv = cfg["adv-flux"]
         phys = native.Physics()
         phys.simulator = native.NAVIER_STOKES if sim["simulator"] == "navier-stokes" else native.EULER
-        phys.eos = native.EOS_CPG
+        phys.eos = native.EOS_TPG if cfg["mixture"]["eos"] == "tpg" else native.EOS_CPG
         phys.primary = {"kepaec": native.FLUX_KEPAEC, "hllc": native.FLUX_HLLC, "rusanov": native.FLUX_RUSANOV,
                         "ausmup": native.FLUX_AUSMUP}[adv["primary"]]
         phys.recon = native.RECON_CONSTANT if adv["recon"] == "constant" else native.RECON_MUSCL
@@ -124,6 +124,8 @@ class Solver:
         phys.ns = self.ns
         phys.nregs = nregs
         phys.alpha = float(cfg["diff-flux"]["values"].get("alpha", 1.0))
+        kind = cfg["chem-integration"]["kind"]
+        phys.chemistry = native.CHEM_COUPLED if kind == "coupled" else native.CHEM_NONE
         handle = ctypes.c_void_p()
         native.call("pgb_case_create", ctypes.byref(phys), ctypes.byref(handle))
         self.case = handle
@@ -152,6 +154,10 @@ class Solver:
         for key in ("mu0", "kappa0", "MWqinv", "wilkepair", "lewis"):
             if key in consts:
                 tables[key] = consts[key]
+        if self.mixture.eos == "tpg":
+            tables.update(cppolyR=consts["cppolyR"], hpoly=consts["hpoly"])
+        if self.mixture.trans == "kinetic-theory":
+            tables.update(mupoly=consts["mupoly"], kappapoly=consts["kappapoly"])
         for name, values in tables.items():
             v = np.ascontiguousarray(values, dtype=np.float64).ravel()
             native.call("pgb_case_set_table", self.case, name.encode(), _fptr(v), v.size)
@@ -163,6 +169,9 @@ class Solver:
             for face in blk.intfaces:
                 nbr = -1 if face.nbr is None else face.nbr
                 native.call("pgb_case_connect", self.case, blk.nblki, face.nface, nbr, face.nbrface or 0)
+        if self.cfg["chem-integration"]["kind"] == "coupled":
+            mech, keep = native.mechanism(consts)
+            native.call("pgb_case_set_mechanism", self.case, ctypes.byref(mech))
         native.call("pgb_case_set_stages", self.case, records, len(records))
         native.call("pgb_case_finalize", self.case)
         self.metrics = []

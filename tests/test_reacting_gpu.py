@@ -1,0 +1,116 @@
+"""The thermally perfect gas, kinetic-theory transport and coupled
+finite-rate chemistry on the device against the CPU oracle.
+
+The 9-species H2/O2/N2 subset of GRI-Mech 3.0 with the tables the
+reference's own mixture code made (peregrine_b200/data), stoichiometric
+H2/air with hot spots.  Bars: the fold within 1e-12 of a state's largest
+rate (the reference measured 7e-13 on a GPU with its own exp and log against
+its host twin, tests/chemint/test_rates.py:34); the right-hand side 1e-12 of
+each component's largest for the gas dynamics and 1e-11 for the species rows,
+which carry the rates' difference of one-way terms; 1e-9 for the state after
+steps.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from peregrine_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rowmax(got, want):
+    scale = np.abs(want).reshape(-1, want.shape[-1]).max(axis=0)
+    scale[scale == 0.0] = 1.0
+    return np.abs(got - want).reshape(-1, want.shape[-1]).max(axis=0) / scale
+
+
+def build(simulator="navier-stokes", integrator="tvd-rk3", chemistry=True, primary="hllc", recon="muscl", cells=12,
+          blocks=(2, 1, 1), seed=7):
+    import peregrine_b200 as pg
+    from oracle.oracle import Oracle
+
+    cfg = cases.reacting_config(simulator, integrator, primary, recon, "koren", chemistry)
+    mesh = cases.reacting_mesh(cells, blocks)
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    consts = mb.mixture.constants()
+    prims = cases.reacting_prims(mb.metrics, mb.mixture.spnames, consts["MW"], cells, seed=seed, width=2.0, dT=600.0,
+                                 radicals=2e-3)
+    mb.set_prims(prims)
+    orc = Oracle(consts, mb.ns, simulator, mb.mesh_blocks, mb.metrics, integrator, primary=primary, recon=recon,
+                 limiter="koren" if recon == "muscl" else None, eos="tpg",
+                 trans="kinetic-theory" if simulator == "navier-stokes" else "constant",
+                 chemistry="finite-rate" if chemistry else None)
+    orc.set_prims(prims)
+    return mb, orc
+
+
+def test_the_fold_matches_the_oracle_on_the_golden_states():
+    import ctypes
+    import peregrine_b200 as pg
+    from oracle.oracle import Oracle
+
+    g = np.load(os.path.join(GOLD, "rates_h2o2_gri30.npz"))
+    mb, _ = build("euler", cells=8, blocks=(1, 1, 1))
+    n, ns = g["Y"].shape
+    omega = np.zeros((n, ns))
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rho, Y, T = (np.ascontiguousarray(g[k], dtype=np.float64) for k in ("rho", "Y", "T"))
+    pg.native.call("pgb_production", mb.case, n, f(rho), f(Y), f(T), omega.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    want = g["omega"]
+    for q in range(n):
+        assert np.abs(omega[q] - want[q]).max() < 1e-12 * np.abs(want[q]).max(), q
+
+
+@pytest.mark.parametrize("simulator", ["euler", "navier-stokes"])
+def test_reacting_rhs_matches_oracle(simulator):
+    mb, orc = build(simulator)
+    dq = mb.regs[-1]
+    mb.rhs(Q="Q", dQ=dq)
+    want = [np.zeros_like(r) for r in orc.regs[0]]
+    orc.rhs(orc.regs[0], want)
+    for b, w in zip(mb.blocks, want):
+        err = rowmax(b.__getattribute__(dq).get()[b.mesh.interior], w[b.mesh.interior])
+        assert err[:5].max() < 1e-12 and err[5:].max() < 1e-11, err
+
+
+def test_tpg_kinetic_rhs_without_chemistry_matches_oracle():
+    mb, orc = build("navier-stokes", chemistry=False)
+    dq = mb.regs[-1]
+    mb.rhs(Q="Q", dQ=dq)
+    want = [np.zeros_like(r) for r in orc.regs[0]]
+    orc.rhs(orc.regs[0], want)
+    for b, w in zip(mb.blocks, want):
+        assert rowmax(getattr(b, dq).get()[b.mesh.interior], w[b.mesh.interior]).max() < 1e-12
+
+
+@pytest.mark.parametrize("integrator", ["tvd-rk3", "rk4"])
+def test_reacting_steps_match_oracle(integrator):
+    mb, orc = build("navier-stokes", integrator)
+    dt = 2e-8
+    for _ in range(3):
+        mb.step(dt)
+        orc.step(dt)
+    for b, w in zip(mb.blocks, orc.regs[0]):
+        assert rowmax(b.Q.get()[b.mesh.interior], w[b.mesh.interior]).max() < 1e-9
+
+
+def test_reacting_steps_conserve_mass_and_energy():
+    mb, _ = build("euler")
+
+    def totals():
+        s = 0.0
+        for b, m in zip(mb.blocks, mb.metrics):
+            vol = 1.0 / m["detJinv"][b.mesh.interior]
+            s = s + (b.Q.get()[b.mesh.interior] * vol[..., None]).sum(axis=(0, 1, 2))
+        return s
+
+    before = totals()
+    mb.step(2e-8, 5)
+    after = totals()
+    assert abs(after[0] - before[0]) <= 1e-13 * abs(before[0])
+    assert abs(after[4] - before[4]) <= 1e-12 * abs(before[4])
