@@ -966,7 +966,7 @@ int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m) {
     if (r.kind < PGB_RXN_ELEMENTARY || r.kind > PGB_RXN_TROE) return fail(PGB_ERR_ARG, "no such reaction kind");
     if ((r.kind != PGB_RXN_ELEMENTARY) && (r.tb < 0 || r.tb >= m->ntb))
       return fail(PGB_ERR_ARG, "a third-body reaction names no set");
-    if (r.kind == PGB_RXN_TROE && r.nfcent > 0 && (r.troe < 0 || r.troe >= m->ntroe))
+    if (r.kind == PGB_RXN_TROE && r.nfcent > 0 && (r.troe < 0 || r.troe >= m->ntroe || m->nlfc < 1))
       return fail(PGB_ERR_ARG, "a Troe reaction names no fit");
     if (r.nfwd < 0 || r.nfwd > PGB_MAXSIDE || r.nreact < 0 || r.nreact > PGB_MAXSIDE || r.nprod < 0 ||
         r.nprod > PGB_MAXSIDE || r.nnet < 0 || r.nnet > PGB_MAXNET)
