@@ -157,7 +157,9 @@ const double *table(const pgb_case *c, const char *name) {
 int build_species(pgb_case *c) {
   const int ns = c->phys.ns;
   static const char *names[T_NTAB] = {"Rsp", "cp0", "h298R", "MWinv", "hpoly0", "h298", "mu0", "kappa0", "MWqinv", "lewis"};
-  static const bool need[T_NTAB] = {true, true, true, true, false, false, false, false, false, false};
+  // cp0 is the calorically perfect gas's; the thermally perfect one reads its fits
+  const bool cpg = c->phys.eos == PGB_EOS_CPG;
+  const bool need[T_NTAB] = {true, cpg, true, true, false, false, false, false, false, false};
   const double *tab[T_NTAB];
   for (int q = 0; q < T_NTAB; q++) {
     tab[q] = table(c, names[q]);

@@ -147,17 +147,24 @@ class Solver:
         return (self.ns == 1 and cfg["adv-flux"]["primary"] == "kepaec" and cfg["adv-flux"]["recon"] == "constant"
                 and cfg["mixture"]["eos"] == "cpg")
 
-    def _fill(self, records):
+    def species_tables(self):
+        """The named species tables the case takes (pgb_case_set_table), from
+        the mixture's constants."""
         consts = self.mixture.constants()
-        tables = dict(Rsp=consts["Rsp"], cp0=consts["cp0"], h298R=consts["h298R"], MWinv=consts["MWinv"],
+        tables = dict(Rsp=consts["Rsp"], h298R=consts["h298R"], MWinv=consts["MWinv"],
                       hpoly0=np.asarray(consts["hpoly"])[:, 0], h298=consts["h298"])
-        for key in ("mu0", "kappa0", "MWqinv", "wilkepair", "lewis"):
+        for key in ("cp0", "mu0", "kappa0", "MWqinv", "wilkepair", "lewis"):
             if key in consts:
                 tables[key] = consts[key]
         if self.mixture.eos == "tpg":
             tables.update(cppolyR=consts["cppolyR"], hpoly=consts["hpoly"])
         if self.mixture.trans == "kinetic-theory":
             tables.update(mupoly=consts["mupoly"], kappapoly=consts["kappapoly"])
+        return tables
+
+    def _fill(self, records):
+        consts = self.mixture.constants()
+        tables = self.species_tables()
         for name, values in tables.items():
             v = np.ascontiguousarray(values, dtype=np.float64).ravel()
             native.call("pgb_case_set_table", self.case, name.encode(), _fptr(v), v.size)

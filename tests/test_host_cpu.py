@@ -127,3 +127,27 @@ def test_two_ranks_report_the_slowest_time_and_the_whole_job():
     ms, value = out[0]
     assert ms == 11.0
     assert value == pytest.approx(1000 * 4 * 10 * 2 / 0.011)
+
+
+def test_reacting_tables_and_mechanism_structs_build_on_the_host():
+    import types
+
+    from peregrine_b200 import cases, native
+    from peregrine_b200.mixture import Mixture
+    from peregrine_b200.solver import Solver
+
+    cfg = cases.reacting_config()
+    mix = Mixture(cfg["mixture"])
+    tables = Solver.species_tables(types.SimpleNamespace(mixture=mix))
+    assert "cp0" not in tables and tables["cppolyR"].shape == (9, 7) and tables["mupoly"].shape[0] == 9
+    consts = mix.constants()
+    mech, keep = native.mechanism(consts)
+    assert mech.nr == 28 and mech.ntb == 5 and mech.ntroe == 1 and mech.ng == 8
+    kinds = [mech.rxn[k].kind for k in range(mech.nr)]
+    assert kinds.count(native.RXN_TROE if hasattr(native, "RXN_TROE") else 3) == 1
+    # every species index on the device's sides lies within the mixture
+    for k in range(mech.nr):
+        r = mech.rxn[k]
+        for j in range(r.nnet):
+            assert 0 <= r.netsp[j] < 9
+        assert 0 < r.nnet <= native.MAXNET and r.nreact <= native.MAXSIDE and r.nprod <= native.MAXSIDE
