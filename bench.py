@@ -19,6 +19,15 @@ oracle on a bounded sample.  With N > 1 (torchrun), every rank runs its own
 replica of the workload (the cross-GPU halo exchange is not built); the
 time is the max over ranks.  The reference arm times the reference CPU
 restatement (oracle/, OpenMP on every host core) on the same workload.
+
+A reacting leg (key "reacting") reports the reacting configuration beside
+the headline: a single periodic block of 96^3 cells, 1 cm a side, of
+stoichiometric H2/air at 1 atm and 1000 K with seeded Gaussian hot spots
+(up to 400 K, 8 cells wide) and a seeded divergence-free velocity (u_rms
+10 m/s); the 9-species H2/O2/N2 subset of GRI-Mech 3.0 (28 reactions,
+thermally perfect, kinetic-theory transport, coupled finite-rate chemistry),
+MUSCL with the koren limiter and HLLC, Navier-Stokes, TVD-RK3, on the
+per-block device path; with the CPU oracle on one stage of it beside it.
 """
 
 import argparse
@@ -193,6 +202,53 @@ def cpu_baseline(mesh_blocks, metrics, prims, constants, budget_s=15.0):
     return ncells * stages / wall, stages, wall
 
 
+REACT_CELLS = 96
+REACT_STAGES = 3
+# TVD-RK3 register traffic per cell and stage (reads + writes): stage 0 reads
+# Q and writes Q1 (2), stages 1 and 2 read Q1 and Q and write one (3); 8/3
+# registers of 13 doubles, 277 bytes
+REACT_BYTES = 8 * 13 * 8 / 3
+
+
+def reacting_leg(steps, cpu=True):
+    """Cell-stage/s of the reacting configuration on the per-block path."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases
+
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True, launch="per-block")
+    mesh = cases.reacting_mesh(REACT_CELLS, (1, 1, 1))
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    consts = mb.mixture.constants()
+    prims = cases.reacting_prims(mb.metrics, mb.mixture.spnames, consts["MW"], REACT_CELLS, seed=SEED)
+    mb.set_prims(prims)
+    dt = 2e-8
+    mb.step(dt, 3)
+    mb.backend.sync()
+    ms = time_graph(mb, dt, steps)
+    ncells = mb.ncells
+    value = ncells * REACT_STAGES * steps / (ms / 1e3)
+    out = {"value": value, "unit": "cell-stage/s", "steps": steps, "ms_per_step": ms / steps,
+           "launches_per_step": mb.launches_per_step(), "dt": dt,
+           "workload": "h2-air-96^3-9sp-28rxn-tpg-kinetic-coupled-chem-muscl-koren-hllc-ns-tvd-rk3",
+           "path": "per-block kernels, one launch per block and pass",
+           "algorithmic_bytes_per_cell_stage": REACT_BYTES,
+           "hbm_gbs_of_algorithmic_bytes": value * REACT_BYTES / 1e9}
+    if cpu:
+        from oracle.oracle import Oracle
+
+        orc = Oracle(consts, mb.ns, "navier-stokes", mb.mesh_blocks, mb.metrics, "tvd-rk3", primary="hllc",
+                     recon="muscl", limiter="koren", eos="tpg", trans="kinetic-theory", chemistry="finite-rate")
+        orc.set_prims(prims)
+        dQ = [np.zeros_like(r) for r in orc.regs[0]]
+        t0 = time.perf_counter()
+        orc.rhs(orc.regs[0], dQ)
+        wall = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": ncells / wall, "unit": "cell-stage/s", "cores": os.cpu_count(),
+                               "kind": "port", "sample": f"one stage (RHS) of the 96^3 reacting field, {wall:.1f} s"}
+    del mb
+    return out
+
+
 def reference_arm(args):
     """The reference CPU restatement's throughput on the same workload; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -244,11 +300,16 @@ def main():
     ap.add_argument("--shape", default=None, help="force the fused kernel's THREADSxMINBLOCKSxWIDTH (no tuning)")
     ap.add_argument("--ksplit", type=int, default=3, help="k runs per block with --shape")
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
+    ap.add_argument("--no-reacting", action="store_true", help="skip the reacting leg")
+    ap.add_argument("--reacting-only", action="store_true", help="the reacting leg alone (profiling)")
     args = ap.parse_args()
     set_cells(args.cells)
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.reacting_only:
+        print(json.dumps({"reacting": reacting_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -339,6 +400,10 @@ def main():
         cpu = {"value": v, "unit": "cell-stage/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"{stages} RK stages (RHS) of the full workload, {cwall:.1f} s, OpenMP"}
 
+    reacting = None
+    if rank == 0 and not args.no_reacting and not args.no_extra:
+        reacting = reacting_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-stage/s", "n_gpus": world, "steps": args.steps,
@@ -357,6 +422,7 @@ def main():
                          "halo_ms_per_stage": float(np.mean(halo)) if halo else None,
                          "algorithmic_bytes_per_cell_stage": 170},
             "cpu_baseline": cpu,
+            "reacting": reacting,
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
