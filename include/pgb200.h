@@ -267,6 +267,38 @@ int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tables, int nx,
                           const double *met, double *dQ, void *stream);
 long long pgb_rhs_block_noalloc_max_cells(int ns);
 
+/* ---- serving pool ----
+ * No counterpart in the reference, which runs one case per solver.  A pool
+ * holds independent cases, each one block periodic onto itself, in one
+ * device arena; cases are admitted while others run, and every running case
+ * advances in the same launches (one launch per pass over all running
+ * blocks) at one shared dt.  A block reads only its own cells, so each case's
+ * result is the same as it would be alone.  The pool copies its physics,
+ * tables, mechanism and RK stages from a finalized prototype case. */
+typedef struct pgb_pool pgb_pool;
+/* an arena of max_cells cells (halos included) and max_blocks slots (<= 65535) */
+int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, pgb_pool **out);
+int pgb_pool_destroy(pgb_pool *p);
+/* a slot for an ni x nj x nk block; PGB_ERR_NOMEM when no slot or arena
+ * range is free (queue the case and admit it once another is released) */
+int pgb_pool_admit(pgb_pool *p, int ni, int nj, int nk, int *slot);
+/* the slot's metrics and primitives, laid out as pgb_metric_set's and pgb_set_prims' */
+int pgb_pool_metric_set(pgb_pool *p, int slot, int which, const double *host, long count);
+int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count);
+/* the slot runs from the next step on, for nsteps RK steps */
+int pgb_pool_start(pgb_pool *p, int slot, int nsteps);
+/* nsteps RK steps of every running case; returns when they are done */
+int pgb_pool_step(pgb_pool *p, double dt, int nsteps);
+/* the slots whose steps are done (up to cap; n is how many there are) */
+int pgb_pool_done(const pgb_pool *p, int *slots, int cap, int *n);
+/* a slot's register over its interior, laid out as pgb_array_get's */
+int pgb_pool_get(pgb_pool *p, int slot, int reg, double *host, long count);
+int pgb_pool_release(pgb_pool *p, int slot);
+/* the largest free arena range (cells) and the running and done counts */
+int pgb_pool_info(const pgb_pool *p, long long *largest_free, int *running, int *done);
+/* the last pgb_pool_step's device time (CUDA events on the pool's stream) and launches */
+int pgb_pool_last(const pgb_pool *p, float *ms, int *launches);
+
 #ifdef __cplusplus
 }
 #endif

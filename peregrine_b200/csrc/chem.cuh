@@ -211,7 +211,7 @@ template <int NS>
 __global__ void k_source(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                          const double *__restrict__ stall, double *__restrict__ dQall) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)B.nx * B.ny * B.nz) return;
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;

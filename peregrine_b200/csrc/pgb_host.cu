@@ -1478,3 +1478,437 @@ int pgb_block_uniform(const pgb_case *c, int blk, int *uniform) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The serving pool: independent cases, each one periodic block, admitted into
+// one device arena while others run, advanced together by packed launches
+// (each pass one launch over every running block) at one shared dt, and read
+// out when their step count is done.  A block's cells never read another
+// block's, so a case's result does not depend on what else is in the pool.
+// ---------------------------------------------------------------------------
+
+struct PoolSlot {
+  int state = 0;  // 0 free, 1 admitted (filling), 2 running, 3 done
+  int nx = 0, ny = 0, nz = 0;
+  long long cv = 0, vol = 0;
+  int steps_left = 0;
+  int active = -1;  // its row in the running table
+};
+
+struct pgb_pool {
+  unsigned long long uid = 0;
+  unsigned version = 1;
+  pgb_physics phys{};
+  Species sp{};
+  std::unique_ptr<Mech> mech;
+  std::vector<pgb_stage> stages;
+  int ne = 5;
+  long long cap_cells = 0;
+  int cap_blocks = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double *d_reg[MAXREGS] = {};
+  double *d_met = nullptr, *d_state = nullptr, *d_tr = nullptr, *d_hsp = nullptr, *d_grads = nullptr;
+  double *d_F[3] = {};
+  double *d_dt = nullptr, *d_host = nullptr;  // dt, and the staging of one block's interior
+  long long host_cap = 0;
+  BlockDev *d_blks = nullptr;  // every slot's descriptor, by slot
+  BlockDev *d_run = nullptr;   // the running table, by row
+  HaloEntry *d_halo = nullptr;
+  long long halo_cap = 0, nhalo = 0, nhalo_l0 = 0;
+  std::vector<PoolSlot> slots;
+  std::map<long long, long long> free_;  // arena ranges: start -> cells
+  std::vector<BlockDev> run;             // running blocks, host copy
+  bool dirty = true;
+  float last_ms = 0.0f;
+  int last_launches = 0;
+};
+
+namespace {
+
+int pool_current(pgb_pool *p) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  Uploaded &u = g_plain_up[p->phys.ns - 1];
+  // a pool's tables share the units' constant memory with the cases: keyed
+  // by the pool's own unique id
+  if (u.uid != p->uid || u.version != p->version || u.device != dev) {
+    static MathTables mt;
+    static bool filled = false;
+    if (!filled) math_tables_fill(mt), filled = true;
+    RET(kPlain[p->phys.ns - 1].upload(&p->sp, p->mech.get(), p->mech ? &mt : nullptr, p->stream));
+    u.uid = p->uid, u.version = p->version, u.device = dev;
+  }
+  return PGB_OK;
+}
+
+// the slot's block as the kernels see it: halo NG deep, cells from cv
+BlockDev slot_dev(const PoolSlot &s) {
+  BlockDev D{};
+  D.nx = s.nx, D.ny = s.ny, D.nz = s.nz;
+  D.X = s.nx + 2 * NG, D.Y = s.ny + 2 * NG, D.Z = s.nz + 2 * NG;
+  D.vol = s.vol;
+  D.cv = s.cv;
+  return D;
+}
+
+// the running table and its halo: each block periodic onto itself, the face
+// halos NG deep, every block's first layer before any second layer
+int pool_rebuild(pgb_pool *p) {
+  p->run.clear();
+  std::vector<HaloEntry> l0, l1;
+  for (size_t q = 0; q < p->slots.size(); q++) {
+    PoolSlot &s = p->slots[q];
+    s.active = -1;
+    if (s.state != 2) continue;
+    s.active = (int)p->run.size();
+    const BlockDev D = slot_dev(s);
+    p->run.push_back(D);
+    const int n[3] = {s.nx, s.ny, s.nz};
+    for (int a = 0; a < 3; a++)
+      for (int layer = 0; layer < NG; layer++)
+        for (int side = 0; side < 2; side++) {
+          // the halo plane at distance layer + 1 beyond the interior on this side
+          const int h = side == 0 ? NG - 1 - layer : NG + n[a] + layer;
+          const int src = side == 0 ? h + n[a] : h - n[a];
+          const int e1 = (a + 1) % 3, e2 = (a + 2) % 3;
+          for (int u = NG; u < NG + n[e2]; u++)
+            for (int v = NG; v < NG + n[e1]; v++) {
+              int di[3], si[3];
+              di[a] = h, si[a] = src;
+              di[e1] = si[e1] = v;
+              di[e2] = si[e2] = u;
+              HaloEntry e{};
+              e.dcv = e.scv = D.cv;
+              e.dvol = e.svol = D.vol;
+              e.didx = cell_index(D, di[0], di[1], di[2]);
+              e.sidx = cell_index(D, si[0], si[1], si[2]);
+              (layer == 0 ? l0 : l1).push_back(e);
+            }
+        }
+  }
+  p->nhalo_l0 = (long long)l0.size();
+  p->nhalo = (long long)(l0.size() + l1.size());
+  l0.insert(l0.end(), l1.begin(), l1.end());
+  if (p->nhalo > p->halo_cap) {
+    if (p->d_halo) CK(cudaFree(p->d_halo));
+    p->d_halo = nullptr;
+    const long long cap = std::max<long long>(p->nhalo, 2 * p->halo_cap);
+    CK(cudaMalloc(&p->d_halo, sizeof(HaloEntry) * cap));
+    p->halo_cap = cap;
+  }
+  if (p->nhalo)
+    CK(cudaMemcpyAsync(p->d_halo, l0.data(), sizeof(HaloEntry) * p->nhalo, cudaMemcpyHostToDevice, p->stream));
+  if (!p->run.empty())
+    CK(cudaMemcpyAsync(p->d_run, p->run.data(), sizeof(BlockDev) * p->run.size(), cudaMemcpyHostToDevice, p->stream));
+  // the host vectors are read by the copies above: wait before they change
+  CK(cudaStreamSynchronize(p->stream));
+  p->dirty = false;
+  return PGB_OK;
+}
+
+PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks, int n) {
+  PlainCase pc{};
+  pc.d_blks = d_blks;
+  pc.h_blks = h_blks;
+  pc.nblocks = n;
+  pc.state = p->d_state, pc.tr = p->d_tr, pc.hsp = p->d_hsp, pc.grads = p->d_grads;
+  for (int a = 0; a < 3; a++) pc.F[a] = p->d_F[a];
+  pc.met = p->d_met;
+  pc.halo = p->d_halo;
+  pc.nhalo = p->nhalo, pc.nhalo_l0 = p->nhalo_l0;
+  pc.visc = p->phys.simulator == PGB_NAVIER_STOKES;
+  pc.primary = p->phys.primary, pc.recon = p->phys.recon, pc.limiter = p->phys.limiter;
+  pc.chem = p->phys.chemistry == PGB_CHEM_COUPLED;
+  pc.packed = 1;
+  pc.stream = p->stream;
+  return pc;
+}
+
+void count_cb(void *ctx, int) { ++*(int *)ctx; }
+
+int pool_slot(pgb_pool *p, int slot, int want) {
+  if (!p) return fail(PGB_ERR_ARG, "null pool");
+  if (slot < 0 || slot >= (int)p->slots.size() || p->slots[slot].state == 0) return fail(PGB_ERR_ARG, "no such slot");
+  if (want >= 0 && p->slots[slot].state != want) return fail(PGB_ERR_STATE, "the slot is not in that state");
+  return PGB_OK;
+}
+
+int pool_stage_host(pgb_pool *p, long long n) {
+  if (n > p->host_cap) {
+    if (p->d_host) CK(cudaFree(p->d_host));
+    p->d_host = nullptr;
+    CK(cudaMalloc(&p->d_host, sizeof(double) * n));
+    p->host_cap = n;
+  }
+  return PGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, pgb_pool **out) {
+  if (!proto || !out) return fail(PGB_ERR_ARG, "null argument");
+  if (!proto->finalized) return fail(PGB_ERR_STATE, "finalize the prototype case first");
+  if (max_cells < 64 || max_blocks < 1 || max_blocks > 65535)
+    return fail(PGB_ERR_ARG, "a pool holds at least 64 cells and 1 to 65535 blocks");
+  auto p = std::make_unique<pgb_pool>();
+  p->uid = ++g_next_uid;
+  p->phys = proto->phys;
+  p->sp = proto->sp;
+  if (proto->mech) p->mech = std::make_unique<Mech>(*proto->mech);
+  p->stages = proto->stages;
+  p->ne = proto->ne;
+  p->cap_cells = max_cells;
+  p->cap_blocks = max_blocks;
+  p->slots.resize(max_blocks);
+  p->free_[0] = max_cells;
+  const int ns = p->phys.ns, ne = p->ne;
+  const size_t n = (size_t)max_cells;
+  CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&p->ev0));
+  CK(cudaEventCreate(&p->ev1));
+  for (int r = 0; r < p->phys.nregs; r++) CK(cudaMalloc(&p->d_reg[r], sizeof(double) * ne * n));
+  CK(cudaMalloc(&p->d_met, sizeof(double) * M_NCOMP * n));
+  CK(cudaMalloc(&p->d_state, sizeof(double) * 8 * n));
+  CK(cudaMalloc(&p->d_tr, sizeof(double) * (2 + ns) * n));
+  CK(cudaMalloc(&p->d_hsp, sizeof(double) * ns * n));
+  CK(cudaMalloc(&p->d_grads, sizeof(double) * 3 * (ne - 1) * n));
+  for (int a = 0; a < 3; a++) CK(cudaMalloc(&p->d_F[a], sizeof(double) * ne * n));
+  CK(cudaMalloc(&p->d_dt, sizeof(double)));
+  CK(cudaMalloc(&p->d_blks, sizeof(BlockDev) * max_blocks));
+  CK(cudaMalloc(&p->d_run, sizeof(BlockDev) * max_blocks));
+  *out = p.release();
+  return PGB_OK;
+}
+
+int pgb_pool_destroy(pgb_pool *p) {
+  if (!p) return PGB_OK;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  for (auto &r : p->d_reg)
+    if (r) cudaFree(r);
+  void *ptrs[] = {p->d_met, p->d_state, p->d_tr, p->d_hsp, p->d_grads, p->d_F[0], p->d_F[1], p->d_F[2],
+                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  if (p->ev0) cudaEventDestroy(p->ev0);
+  if (p->ev1) cudaEventDestroy(p->ev1);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return PGB_OK;
+}
+
+// a slot for an ni x nj x nk periodic block; PGB_ERR_NOMEM when the arena or
+// the slot table has no room (the caller queues the case and tries later)
+int pgb_pool_admit(pgb_pool *p, int ni, int nj, int nk, int *slot) {
+  if (!p || !slot) return fail(PGB_ERR_ARG, "null argument");
+  if (ni < 2 || nj < 2 || nk < 2 || ni > 30000 || nj > 30000 || nk > 30000)
+    return fail(PGB_ERR_ARG, "a block has 2 to 30000 cells per axis");
+  const long long vol = (long long)(ni + 2 * NG) * (nj + 2 * NG) * (nk + 2 * NG);
+  int id = -1;
+  for (int q = 0; q < (int)p->slots.size(); q++)
+    if (p->slots[q].state == 0) {
+      id = q;
+      break;
+    }
+  if (id < 0) return fail(PGB_ERR_NOMEM, "every slot of the pool is taken");
+  // first fit over the arena's free ranges
+  auto it = p->free_.begin();
+  for (; it != p->free_.end(); ++it)
+    if (it->second >= vol) break;
+  if (it == p->free_.end()) return fail(PGB_ERR_NOMEM, "the pool's arena has no free range that large");
+  const long long cv = it->first, left = it->second - vol;
+  p->free_.erase(it);
+  if (left > 0) p->free_[cv + vol] = left;
+  PoolSlot &s = p->slots[id];
+  s = PoolSlot{};
+  s.state = 1;
+  s.nx = ni, s.ny = nj, s.nz = nk;
+  s.cv = cv, s.vol = vol;
+  const BlockDev D = slot_dev(s);
+  // a new occupant starts from zeros: its halo's first Newton from the cold
+  // guess, whatever the range held before
+  for (int r = 0; r < p->phys.nregs; r++)
+    CK(cudaMemsetAsync(p->d_reg[r] + (size_t)p->ne * cv, 0, sizeof(double) * p->ne * vol, p->stream));
+  CK(cudaMemsetAsync(p->d_state + (size_t)8 * cv, 0, sizeof(double) * 8 * vol, p->stream));
+  CK(cudaMemcpyAsync(p->d_blks + id, &D, sizeof(BlockDev), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  *slot = id;
+  return PGB_OK;
+}
+
+// a slot's metric array, laid out as pgb_metric_set's
+int pgb_pool_metric_set(pgb_pool *p, int slot, int which, const double *host, long count) {
+  RET(pool_slot(p, slot, 1));
+  if (!host || which < 0 || which >= PGB_NMETRICS) return fail(PGB_ERR_ARG, "no such metric");
+  const BlockDev D = slot_dev(p->slots[slot]);
+  static const int comps[PGB_NMETRICS] = {3, 1, 9, 3, 3, 3, 3, 3, 3};
+  static const int first[PGB_NMETRICS] = {M_XCC, M_DETJINV, M_JINV, M_S, M_S + 3, M_S + 6, M_XF, M_XF + 3, M_XF + 6};
+  const int face = which >= PGB_ARR_IS ? (which - PGB_ARR_IS) % 3 : -1;
+  const int X = D.X + (face == 0), Y = D.Y + (face == 1), Z = D.Z + (face == 2);
+  const int nc = comps[which];
+  if (count != (long)X * Y * Z * nc) return fail(PGB_ERR_ARG, "metric array of the wrong size");
+  std::vector<double> dev((size_t)nc * D.vol);
+  for (int q = 0; q < nc; q++)
+    for (int k = 0; k < D.Z; k++)
+      for (int j = 0; j < D.Y; j++)
+        for (int i = 0; i < D.X; i++)
+          dev[(size_t)q * D.vol + cell_index(D, i, j, k)] = host[(((size_t)q * Z + k) * Y + j) * X + i];
+  CK(cudaMemcpyAsync(p->d_met + (size_t)M_NCOMP * D.cv + (size_t)first[which] * D.vol, dev.data(),
+                     sizeof(double) * dev.size(), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return PGB_OK;
+}
+
+// a slot's Q and state from interior primitives (F order, as pgb_set_prims)
+int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count) {
+  RET(pool_slot(p, slot, 1));
+  const PoolSlot &s = p->slots[slot];
+  if (!host || count != (long)s.nx * s.ny * s.nz * p->ne) return fail(PGB_ERR_ARG, "primitives of the wrong size");
+  RET(pool_current(p));
+  RET(pool_stage_host(p, count));
+  CK(cudaMemcpyAsync(p->d_host, host, sizeof(double) * count, cudaMemcpyHostToDevice, p->stream));
+  // the unit reads the launch size from the host table at the slot's index
+  std::vector<BlockDev> hb((size_t)slot + 1);
+  hb[slot] = slot_dev(s);
+  const PlainCase pc = pool_plain(p, p->d_blks, hb.data(), slot + 1);
+  RET(kPlain[p->phys.ns - 1].fromprims(&pc, slot, p->d_host, p->d_reg[0]));
+  CK(cudaStreamSynchronize(p->stream));
+  return PGB_OK;
+}
+
+// the slot joins the running cases at the next step, for nsteps steps
+int pgb_pool_start(pgb_pool *p, int slot, int nsteps) {
+  RET(pool_slot(p, slot, 1));
+  if (nsteps < 1) return fail(PGB_ERR_ARG, "at least one step");
+  p->slots[slot].state = 2;
+  p->slots[slot].steps_left = nsteps;
+  p->dirty = true;
+  return PGB_OK;
+}
+
+// nsteps RK steps of every running case at dt; a case whose count runs out
+// is done and leaves the running set after that step
+int pgb_pool_step(pgb_pool *p, double dt, int nsteps) {
+  if (!p) return fail(PGB_ERR_ARG, "null pool");
+  if (nsteps < 1) return fail(PGB_ERR_ARG, "at least one step");
+  RET(pool_current(p));
+  k_setscalar<<<1, 1, 0, p->stream>>>(p->d_dt, dt);
+  int launches = 0;
+  CK(cudaEventRecord(p->ev0, p->stream));
+  for (int it = 0; it < nsteps; it++) {
+    if (p->dirty) RET(pool_rebuild(p));
+    const int nrun = (int)p->run.size();
+    if (nrun == 0) break;
+    PlainCase pc = pool_plain(p, p->d_run, p->run.data(), nrun);
+    pc.mark = count_cb;
+    pc.ctx = &launches;
+    long long most = 0;
+    for (const BlockDev &D : p->run) most = std::max<long long>(most, (long long)D.nx * D.ny * D.nz);
+    const dim3 g((unsigned)grid_for(most, 256), (unsigned)nrun, 1);
+    for (const pgb_stage &st : p->stages) {
+      RET(kPlain[p->phys.ns - 1].rhs(&pc, p->d_reg[st.q], p->d_reg[st.dq]));
+      for (int m = 0; m < st.ncombine; m++) {
+        const pgb_combine &cb = st.combine[m];
+        CombineDev cd{};
+        cd.out = p->d_reg[cb.out];
+        cd.own = cb.own;
+        cd.wout = cb.wout;
+        cd.nterms = cb.nterms;
+        cd.step = cb.step;
+        for (int n = 0; n < cb.nterms; n++) {
+          cd.X[n] = p->d_reg[cb.reg[n] < 0 ? st.dq : cb.reg[n]];
+          cd.w[n] = cb.w[n];
+        }
+        k_combine<<<g, 256, 0, p->stream>>>(p->d_run, 0, p->ne, cd, p->d_dt);
+        launches++;
+      }
+    }
+    CK(cudaGetLastError());
+    for (auto &s : p->slots)
+      if (s.state == 2 && --s.steps_left == 0) s.state = 3, p->dirty = true;
+  }
+  CK(cudaEventRecord(p->ev1, p->stream));
+  CK(cudaEventSynchronize(p->ev1));
+  CK(cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1));
+  p->last_launches = launches;
+  return PGB_OK;
+}
+
+// the done slots, up to cap of them; n the count there are
+int pgb_pool_done(const pgb_pool *p, int *slots, int cap, int *n) {
+  if (!p || !n || (cap > 0 && !slots)) return fail(PGB_ERR_ARG, "null argument");
+  int k = 0;
+  for (int q = 0; q < (int)p->slots.size(); q++)
+    if (p->slots[q].state == 3) {
+      if (k < cap) slots[k] = q;
+      k++;
+    }
+  *n = k;
+  return PGB_OK;
+}
+
+// a slot's register reg over its interior, F order (as pgb_array_get)
+int pgb_pool_get(pgb_pool *p, int slot, int reg, double *host, long count) {
+  RET(pool_slot(p, slot, -1));
+  const PoolSlot &s = p->slots[slot];
+  if (reg < 0 || reg >= p->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  if (!host || count != (long)s.nx * s.ny * s.nz * p->ne) return fail(PGB_ERR_ARG, "host array of the wrong size");
+  RET(pool_stage_host(p, count));
+  k_pack<<<grid_for((long long)s.nx * s.ny * s.nz, 256), 256, 0, p->stream>>>(p->d_blks, slot, p->ne, p->d_reg[reg],
+                                                                               p->d_host);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, p->d_host, sizeof(double) * count, cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return PGB_OK;
+}
+
+// the slot and its arena range are free again
+int pgb_pool_release(pgb_pool *p, int slot) {
+  RET(pool_slot(p, slot, -1));
+  PoolSlot &s = p->slots[slot];
+  if (s.state == 2) p->dirty = true;
+  // give the range back, merged with free neighbours
+  long long cv = s.cv, vol = s.vol;
+  auto nx = p->free_.lower_bound(cv);
+  if (nx != p->free_.end() && nx->first == cv + vol) {
+    vol += nx->second;
+    p->free_.erase(nx);
+  }
+  auto pv = p->free_.lower_bound(cv);
+  if (pv != p->free_.begin()) {
+    --pv;
+    if (pv->first + pv->second == cv) {
+      cv = pv->first;
+      vol += pv->second;
+      p->free_.erase(pv);
+    }
+  }
+  p->free_[cv] = vol;
+  s = PoolSlot{};
+  return PGB_OK;
+}
+
+// the largest free range of cells (halo included), and the running and done counts
+int pgb_pool_info(const pgb_pool *p, long long *largest_free, int *running, int *done) {
+  if (!p) return fail(PGB_ERR_ARG, "null pool");
+  long long big = 0;
+  for (auto &f : p->free_) big = std::max(big, f.second);
+  int r = 0, d = 0;
+  for (auto &s : p->slots) r += s.state == 2, d += s.state == 3;
+  if (largest_free) *largest_free = big;
+  if (running) *running = r;
+  if (done) *done = d;
+  return PGB_OK;
+}
+
+// the last pgb_pool_step's device time and its launches
+int pgb_pool_last(const pgb_pool *p, float *ms, int *launches) {
+  if (!p) return fail(PGB_ERR_ARG, "null pool");
+  if (ms) *ms = p->last_ms;
+  if (launches) *launches = p->last_launches;
+  return PGB_OK;
+}
+
+}  // extern "C"

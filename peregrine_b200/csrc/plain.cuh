@@ -3,7 +3,9 @@
 // reference's rhs graph (peregrine/simulator/advec/simulator.py:57-87,
 // peregrine/simulator/advecdiff/simulator.py:110-124).  It is the baseline
 // the fused path is measured against and the path for physics the fused
-// kernel does not take.
+// kernel does not take.  Every kernel's block is blks[b + blockIdx.y]: a
+// launch of one block has gridDim.y 1, a packed launch covers many blocks
+// at once, one grid row each (the serving pool's).
 #pragma once
 #include "layout.cuh"
 #include "physics.cuh"
@@ -34,7 +36,7 @@ __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi,
 template <int NS>
 __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                         double *__restrict__ stall) {
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
@@ -58,7 +60,7 @@ template <int NS>
 __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                             const double *__restrict__ stall, double *__restrict__ trall,
                             double *__restrict__ hall) {
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
@@ -83,7 +85,7 @@ __global__ void k_grads(const BlockDev *__restrict__ blks, int b, const double *
                         const double *__restrict__ stall, const double *__restrict__ met,
                         double *__restrict__ gall, int grow = 0) {
   constexpr int NE = 4 + NS, NGRAD = NE - 1;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int gx = B.nx + 2 * grow, gy = B.ny + 2 * grow, gz = B.nz + 2 * grow;
   const long long n = (long long)gx * gy * gz;
@@ -140,7 +142,7 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
                           const double *__restrict__ stall, const double *__restrict__ met,
                           double *__restrict__ Fall) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   int i, j, k;
   if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
   const long long R = cell_index(B, i, j, k);
@@ -178,7 +180,7 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
                           const double *__restrict__ stall, const double *__restrict__ met,
                           double *__restrict__ Fall, const int lim) {
   constexpr int NE = 4 + NS, NY = NS > 1 ? NS - 1 : 1;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   int i, j, k;
   if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
   const long long R = cell_index(B, i, j, k);
@@ -237,7 +239,7 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
                            const double *__restrict__ hall, const double *__restrict__ gall,
                            const double *__restrict__ met, double *__restrict__ Fall) {
   constexpr int NE = 4 + NS, NGRAD = NE - 1;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   int i, j, k;
   if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
   const long long R = cell_index(B, i, j, k);
@@ -333,7 +335,7 @@ __global__ void k_applyflux(const BlockDev *__restrict__ blks, int b, const doub
                             const double *__restrict__ Fj, const double *__restrict__ Fk,
                             const double *__restrict__ met, double *__restrict__ dQall, int append = 0) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)B.nx * B.ny * B.nz) return;
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
@@ -360,7 +362,7 @@ struct CombineDev {
 };
 
 static __global__ void k_combine(const BlockDev *__restrict__ blks, int b, int ne, CombineDev cd, const double *__restrict__ dt) {
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)B.nx * B.ny * B.nz) return;
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
@@ -389,7 +391,7 @@ template <int NS>
 __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const double *__restrict__ prims,
                             double *__restrict__ Qall, double *__restrict__ stall) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = (long long)B.nx * B.ny * B.nz;
   if (t >= n) return;
@@ -413,7 +415,7 @@ __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const doub
 // interior cells between a packed host-order buffer [comp][k][j][i] and a register
 static __global__ void k_unpack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ src,
                          double *__restrict__ Rall) {
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long n = (long long)B.nx * B.ny * B.nz;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -424,7 +426,7 @@ static __global__ void k_unpack(const BlockDev *__restrict__ blks, int b, int ne
 
 static __global__ void k_pack(const BlockDev *__restrict__ blks, int b, int ne, const double *__restrict__ Rall,
                        double *__restrict__ dst) {
-  const BlockDev &B = blks[b];
+  const BlockDev &B = blks[b + blockIdx.y];
   const long long n = (long long)B.nx * B.ny * B.nz;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= n) return;

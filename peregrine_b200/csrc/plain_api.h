@@ -21,6 +21,7 @@ struct PlainCase {
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
   int visc, primary, recon, limiter, chem;
+  int packed;  // 1: each pass is one launch over every block, a grid row per block
   cudaStream_t stream;
   void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block
   void *ctx;

@@ -37,20 +37,73 @@ void mark(const PlainCase *pc, int kind) {
   if (pc->mark) pc->mark(pc->ctx, kind);
 }
 
-template <int A, int FN>
-void launch_riemann(const PlainCase *pc, int b, const double *Q, long long nf) {
+// a pass over every block: one launch per block, or packed, one launch whose
+// rows are the blocks, each row as long as the largest block needs
+template <class F>
+void for_blocks(const PlainCase *pc, F size, void (*launch)(const PlainCase *, int, dim3, const void *),
+                const void *ctx, int kind) {
+  if (pc->packed) {
+    long long most = 0;
+    for (int b = 0; b < pc->nblocks; b++) most = std::max(most, size(pc->h_blks[b]));
+    if (pc->nblocks > 0) launch(pc, 0, dim3(grid_of(most), (unsigned)pc->nblocks, 1), ctx);
+    mark(pc, kind);
+  } else {
+    for (int b = 0; b < pc->nblocks; b++) {
+      launch(pc, b, dim3(grid_of(size(pc->h_blks[b])), 1, 1), ctx);
+      mark(pc, kind);
+    }
+  }
+}
+
+struct RhsArgs {
+  const double *Q;
+  double *dQ;
+};
+
+long long vol_of(const BlockDev &D) { return D.vol; }
+long long inner_of(const BlockDev &D) { return (long long)D.nx * D.ny * D.nz; }
+long long fx_of(const BlockDev &D) { return (long long)(D.nx + 1) * D.ny * D.nz; }
+long long fy_of(const BlockDev &D) { return (long long)D.nx * (D.ny + 1) * D.nz; }
+long long fz_of(const BlockDev &D) { return (long long)D.nx * D.ny * (D.nz + 1); }
+
+template <int A>
+void adv_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
   const int lim = pc->recon == PGB_RECON_MUSCL ? pc->limiter : 0;
-  k_riemann<NS, A, FN><<<grid_of(nf), TH, 0, pc->stream>>>(pc->d_blks, b, Q, pc->state, pc->met, pc->F[A], lim);
+  cudaStream_t s = pc->stream;
+  switch (pc->primary) {
+    case PGB_FLUX_HLLC: k_riemann<NS, A, FN_HLLC><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim); break;
+    case PGB_FLUX_RUSANOV: k_riemann<NS, A, FN_RUSANOV><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim); break;
+    case PGB_FLUX_AUSMUP: k_riemann<NS, A, FN_AUSMUP><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim); break;
+    default: k_advflux<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A]);
+  }
 }
 
 template <int A>
-void launch_advflux(const PlainCase *pc, int b, const double *Q, long long nf) {
-  switch (pc->primary) {
-    case PGB_FLUX_HLLC: launch_riemann<A, FN_HLLC>(pc, b, Q, nf); break;
-    case PGB_FLUX_RUSANOV: launch_riemann<A, FN_RUSANOV>(pc, b, Q, nf); break;
-    case PGB_FLUX_AUSMUP: launch_riemann<A, FN_AUSMUP>(pc, b, Q, nf); break;
-    default: k_advflux<NS, A><<<grid_of(nf), TH, 0, pc->stream>>>(pc->d_blks, b, Q, pc->state, pc->met, pc->F[A]);
-  }
+void diff_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_diffflux<NS, A><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A]);
+}
+
+void fromQ_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_fromQ<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state);
+}
+void transport_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_transport<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp);
+}
+void grads_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_grads<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->grads);
+}
+void source_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, a.dQ);
+}
+void apply_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_applyflux<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, a.dQ, pc->chem);
 }
 
 }  // namespace
@@ -83,53 +136,72 @@ extern "C" int PGB_ENTRY(pgb_plain_upload_)(const Species *sp, const Mech *mech,
 
 // one right-hand side of every block: Q's halo, the state everywhere (the
 // transport and gradients on the viscous path, the gradients' first halo
-// layer), the chemistry source, the face fluxes per axis and the divergence
+// layer), the chemistry source, the face fluxes per axis and the divergence.
+// Per block the passes run block by block (the reference's order); packed,
+// each pass is one launch over every block.
 extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, double *dQ) {
   cudaStream_t s = pc->stream;
-  double *Qm = const_cast<double *>(Q);
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(Qm, pc->halo, pc->nhalo, NE);
+  const RhsArgs a{Q, dQ};
+  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(Q), pc->halo, pc->nhalo, NE);
   mark(pc, 0);
-  for (int b = 0; b < pc->nblocks; b++) {
-    const BlockDev &D = pc->h_blks[b];
-    const long long inner = (long long)D.nx * D.ny * D.nz;
-    k_fromQ<NS><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state);
-    mark(pc, 2);
+  if (pc->packed) {
+    for_blocks(pc, vol_of, fromQ_launch, &a, 2);
     if (pc->visc) {
-      k_transport<NS><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, pc->tr, pc->hsp);
+      for_blocks(pc, vol_of, transport_launch, &a, 2);
+      for_blocks(pc, inner_of, grads_launch, &a, 2);
+    }
+  } else {
+    for (int b = 0; b < pc->nblocks; b++) {
+      const BlockDev &D = pc->h_blks[b];
+      fromQ_launch(pc, b, dim3(grid_of(D.vol)), &a);
       mark(pc, 2);
-      k_grads<NS><<<grid_of(inner), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, pc->met, pc->grads);
-      mark(pc, 2);
+      if (pc->visc) {
+        transport_launch(pc, b, dim3(grid_of(D.vol)), &a);
+        mark(pc, 2);
+        grads_launch(pc, b, dim3(grid_of(inner_of(D))), &a);
+        mark(pc, 2);
+      }
     }
   }
   if (pc->visc) {
     k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1));
     mark(pc, 0);
   }
-  for (int b = 0; b < pc->nblocks; b++) {
-    const BlockDev &D = pc->h_blks[b];
-    const long long inner = (long long)D.nx * D.ny * D.nz;
-    const long long fx = (long long)(D.nx + 1) * D.ny * D.nz, fy = (long long)D.nx * (D.ny + 1) * D.nz,
-                    fz = (long long)D.nx * D.ny * (D.nz + 1);
-    if (pc->chem) {
-      k_source<NS><<<grid_of(inner), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, dQ);
-      mark(pc, 2);
-    }
-    launch_advflux<0>(pc, b, Q, fx);
-    mark(pc, 2);
-    launch_advflux<1>(pc, b, Q, fy);
-    mark(pc, 2);
-    launch_advflux<2>(pc, b, Q, fz);
-    mark(pc, 2);
+  if (pc->packed) {
+    if (pc->chem) for_blocks(pc, inner_of, source_launch, &a, 2);
+    for_blocks(pc, fx_of, adv_launch<0>, &a, 2);
+    for_blocks(pc, fy_of, adv_launch<1>, &a, 2);
+    for_blocks(pc, fz_of, adv_launch<2>, &a, 2);
     if (pc->visc) {
-      k_diffflux<NS, 0><<<grid_of(fx), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[0]);
+      for_blocks(pc, fx_of, diff_launch<0>, &a, 2);
+      for_blocks(pc, fy_of, diff_launch<1>, &a, 2);
+      for_blocks(pc, fz_of, diff_launch<2>, &a, 2);
+    }
+    for_blocks(pc, inner_of, apply_launch, &a, 2);
+  } else {
+    for (int b = 0; b < pc->nblocks; b++) {
+      const BlockDev &D = pc->h_blks[b];
+      if (pc->chem) {
+        source_launch(pc, b, dim3(grid_of(inner_of(D))), &a);
+        mark(pc, 2);
+      }
+      adv_launch<0>(pc, b, dim3(grid_of(fx_of(D))), &a);
       mark(pc, 2);
-      k_diffflux<NS, 1><<<grid_of(fy), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[1]);
+      adv_launch<1>(pc, b, dim3(grid_of(fy_of(D))), &a);
       mark(pc, 2);
-      k_diffflux<NS, 2><<<grid_of(fz), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[2]);
+      adv_launch<2>(pc, b, dim3(grid_of(fz_of(D))), &a);
+      mark(pc, 2);
+      if (pc->visc) {
+        diff_launch<0>(pc, b, dim3(grid_of(fx_of(D))), &a);
+        mark(pc, 2);
+        diff_launch<1>(pc, b, dim3(grid_of(fy_of(D))), &a);
+        mark(pc, 2);
+        diff_launch<2>(pc, b, dim3(grid_of(fz_of(D))), &a);
+        mark(pc, 2);
+      }
+      apply_launch(pc, b, dim3(grid_of(inner_of(D))), &a);
       mark(pc, 2);
     }
-    k_applyflux<NS><<<grid_of(inner), TH, 0, s>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, dQ, pc->chem);
-    mark(pc, 2);
   }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "per-block launch");

@@ -174,6 +174,18 @@ SIGNATURES = {
     "pgb_case_create": ([ctypes.POINTER(Physics), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "pgb_case_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "pgb_case_set_table": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_pool_create": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "pgb_pool_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "pgb_pool_admit": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_pool_metric_set": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_pool_set_prims": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_pool_start": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "pgb_pool_step": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int], ctypes.c_int),
+    "pgb_pool_done": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_pool_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_pool_release": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "pgb_pool_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_pool_last": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_case_set_mechanism": ([ctypes.c_void_p, ctypes.POINTER(Mechanism)], ctypes.c_int),
     "pgb_production": ([ctypes.c_void_p, ctypes.c_long] + [ctypes.POINTER(ctypes.c_double)] * 4, ctypes.c_int),
     "pgb_case_add_block": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),

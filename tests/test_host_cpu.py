@@ -151,3 +151,76 @@ def test_reacting_tables_and_mechanism_structs_build_on_the_host():
         for j in range(r.nnet):
             assert 0 <= r.netsp[j] < 9
         assert 0 < r.nnet <= native.MAXNET and r.nreact <= native.MAXSIDE and r.nprod <= native.MAXSIDE
+
+
+class _FakePool:
+    """A pool of fixed cell capacity that finishes a case after its steps."""
+
+    def __init__(self, cap):
+        self.cap, self.used, self.slots, self.next = cap, 0, {}, 0
+        self.admitted = []
+
+    def admit(self, req):
+        need = int(np.prod([c + 4 for c in req.cells]))
+        if self.used + need > self.cap:
+            return None
+        s = self.next
+        self.next += 1
+        self.used += need
+        self.slots[s] = [req, req.steps, need]
+        self.admitted.append(req.rid)
+        return s
+
+    def step(self, dt, n=1):
+        for v in self.slots.values():
+            v[1] -= 1
+        return 0.5, 14
+
+    def done(self):
+        return [s for s, v in self.slots.items() if v[1] <= 0]
+
+    def take(self, slot, cells):
+        req, _, need = self.slots.pop(slot)
+        self.used -= need
+        return np.full(cells, float(req.rid))
+
+
+def test_server_admits_in_order_as_room_frees_and_times_each_request():
+    from peregrine_b200 import serving
+
+    spn, MW = ["H2", "O2", "N2"], [2.016, 31.998, 28.014]
+    reqs = serving.requests(12, 0.0, spn, MW, seed=4, steps=3, nmin=8, nmax=16)
+    t = [0.0]
+
+    def clock():
+        t[0] += 1e-3
+        return t[0]
+
+    pool = _FakePool(cap=3 * 20 * 6 * 6)
+    out = serving.Server(pool, 1e-8).run(reqs, 3, clock=clock, sleep=lambda s: None)
+    # first come, first admitted; every request finished with its own result
+    assert pool.admitted == sorted(pool.admitted)
+    assert all(r.finished is not None and r.finished >= r.admitted >= r.arrival for r in out)
+    assert all(np.all(r.result == r.rid) for r in out)
+    st = serving.latency_stats(out)
+    assert st["n"] == 12 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_serving_requests_follow_the_workload():
+    from peregrine_b200 import serving
+
+    spn, MW = ["H2", "H", "O2", "N2"], [2.016, 1.008, 31.998, 28.014]
+    reqs = serving.requests(400, 50.0, spn, MW, seed=1)
+    arr = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(arr) >= 0) and abs(arr[-1] / 400 - 1 / 50.0) < 0.3 / 50.0
+    zero = [r for r in reqs if r.kind == "0d"]
+    one = [r for r in reqs if r.kind == "1d"]
+    assert 150 < len(zero) < 250 and all(r.cells == (2, 2, 2) for r in zero)
+    assert all(64 <= r.cells[0] <= 2048 for r in one)
+    for r in zero:
+        p, T = r.prims[0, 0, 0, 0], r.prims[0, 0, 0, 4]
+        assert 900 <= T <= 1400 and 1 * 101325 <= p <= 40 * 101325
+        Y = np.append(r.prims[0, 0, 0, 5:], 1 - r.prims[0, 0, 0, 5:].sum())
+        X = Y / np.array(MW)
+        phi = X[0] / X[2] / 2.0
+        assert 0.5 - 1e-9 <= phi <= 2.0 + 1e-9
