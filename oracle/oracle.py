@@ -325,6 +325,11 @@ class Oracle:
             assert q.shape == Q.shape
             self.lib.oracle_fromprims(ctypes.byref(self.case), _ptr(q), _ptr(Q), ctypes.c_long(Q.size // self.ne),
                                       _ptr(self.Tg[n]))
+        # a halo cell's first Newton starts from the stored T of the cell it
+        # copies, as the device's set_prims leaves it
+        m = self.map
+        for r in m:
+            self.Tg[r["dblk"]][r["di"], r["dj"], r["dk"]] = self.Tg[r["sblk"]][r["si"], r["sj"], r["sk"]]
 
     def production(self, rho, Y, T):
         """omega[n, ns] of independent states, rho[n], Y[n, ns] every species, T[n]."""

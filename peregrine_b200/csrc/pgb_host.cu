@@ -1222,6 +1222,9 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
   std::vector<BlockDev> hb;
   const PlainCase pc = plain_case(c, hb);
   RET(kPlain[c->phys.ns - 1].fromprims(&pc, blk, c->d_prims, c->d_reg[c->phys_of[reg]]));
+  // a halo cell's first Newton starts from the stored T of the cell it copies
+  if (c->nhalo) k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_state, c->d_halo, c->nhalo, 8);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
 }
@@ -1607,6 +1610,24 @@ int pool_rebuild(pgb_pool *p) {
   return PGB_OK;
 }
 
+// one periodic block's face halos (NG deep) from its own interior, comps
+// components: the copy the running table's halo makes, for a block not yet
+// running
+__global__ void k_selfhalo(const BlockDev *__restrict__ blks, int b, double *__restrict__ base, int comps) {
+  const BlockDev &B = blks[b];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= B.vol) return;
+  const int i = (int)(t % B.X), j = (int)((t / B.X) % B.Y), k = (int)(t / ((long long)B.X * B.Y));
+  const int oi = i < NG || i >= NG + B.nx, oj = j < NG || j >= NG + B.ny, ok = k < NG || k >= NG + B.nz;
+  if (oi + oj + ok != 1) return;
+  const int si = oi ? (i < NG ? i + B.nx : i - B.nx) : i;
+  const int sj = oj ? (j < NG ? j + B.ny : j - B.ny) : j;
+  const int sk = ok ? (k < NG ? k + B.nz : k - B.nz) : k;
+  double *d = base + comps * B.cv;
+  const long long dc = cell_index(B, i, j, k), sc = cell_index(B, si, sj, sk);
+  for (int c = 0; c < comps; c++) d[c * B.vol + dc] = d[c * B.vol + sc];
+}
+
 PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks, int n) {
   PlainCase pc{};
   pc.d_blks = d_blks;
@@ -1774,6 +1795,9 @@ int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count) {
   hb[slot] = slot_dev(s);
   const PlainCase pc = pool_plain(p, p->d_blks, hb.data(), slot + 1);
   RET(kPlain[p->phys.ns - 1].fromprims(&pc, slot, p->d_host, p->d_reg[0]));
+  // a halo cell's first Newton starts from the stored T of the cell it copies
+  k_selfhalo<<<grid_for(hb[slot].vol, 256), 256, 0, p->stream>>>(p->d_blks, slot, p->d_state, 8);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(p->stream));
   return PGB_OK;
 }
