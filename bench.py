@@ -28,6 +28,13 @@ stoichiometric H2/air at 1 atm and 1000 K with seeded Gaussian hot spots
 thermally perfect, kinetic-theory transport, coupled finite-rate chemistry),
 MUSCL with the koren limiter and HLLC, Navier-Stokes, TVD-RK3, on the
 per-block device path; with the CPU oracle on one stage of it beside it.
+
+A serving leg (key "serving") plays a seeded Poisson stream of 400 H2/air
+requests at 500 per second: closed constant-volume reactors (phi, T0 and p
+drawn uniformly) and periodic 1-D domains of 64 to 2048 cells (log-uniform),
+100 RK3 steps each at one shared dt, admitted into one device pool while
+others run (peregrine_b200/serving.py); it reports throughput and the p50
+and p99 time from a request's arrival to its result on the host.
 """
 
 import argparse
@@ -249,6 +256,49 @@ def reacting_leg(steps, cpu=True):
     return out
 
 
+def serving_leg(n=400, rate=500.0, steps=100):
+    """The serving stream: Poisson arrivals of H2/air closed reactors and
+    periodic 1-D domains, admitted into one pool while others run."""
+    import ctypes
+
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases, native, serving
+
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True)
+    proto = pg.get_solver(cfg, cases.reacting_mesh(4), pg.get_backend("cuda", cfg))
+    consts = proto.mixture.constants()
+    reqs = serving.requests(n, rate, proto.mixture.spnames, consts["MW"], seed=SEED, steps=steps)
+    # the client side: each case arrives with its mesh's metrics made
+    for r in reqs:
+        serving.box_metrics(r.cells, r.lengths)
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    native.call("pgb_mem_info", ctypes.byref(free), ctypes.byref(total))
+    ns, ne = proto.ns, proto.ne
+    per_cell = 8 * (proto.nregs * ne + 31 + 8 + (2 + ns) + ns + 3 * (ne - 1) + 3 * ne)
+    cap = int(min(free.value * 0.5 / per_cell, 20_000_000))
+    pool = serving.Pool(proto, cap, 4096)
+    dt = 2e-8
+    # warm the kernels on one case
+    warm = serving.requests(1, 0.0, proto.mixture.spnames, consts["MW"], seed=SEED + 1, steps=3)
+    serving.Server(pool, dt).run(warm, 3)
+    srv = serving.Server(pool, dt)
+    t0 = time.perf_counter()
+    srv.run(reqs, 3)
+    wall = time.perf_counter() - t0
+    pool.close()
+    st = serving.latency_stats(reqs)
+    zero = [r for r in reqs if r.kind == "0d"]
+    one = [r for r in reqs if r.kind == "1d"]
+    return {"requests": n, "arrival_rate_per_s": rate, "steps_per_request": steps, "dt": dt,
+            "cell_stages_per_s": srv.cell_stages / wall, "requests_per_s": n / wall, "wall_s": wall,
+            "device_ms": srv.device_ms, "pool_steps": srv.steps, "launches": srv.launches,
+            "latency_ms": st, "latency_0d_ms": serving.latency_stats(zero) if zero else None,
+            "latency_1d_ms": serving.latency_stats(one) if one else None,
+            "arena_cells": cap, "per_cell_bytes": per_cell,
+            "workload": "h2-air-serving: closed reactors (phi U[0.5,2], T0 U[900,1400] K, p U[1,40] atm) and "
+                        "periodic 1-D domains of 64-2048 cells, Poisson arrivals, one pool, continuous batching"}
+
+
 def reference_arm(args):
     """The reference CPU restatement's throughput on the same workload; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -302,11 +352,16 @@ def main():
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
     ap.add_argument("--no-reacting", action="store_true", help="skip the reacting leg")
     ap.add_argument("--reacting-only", action="store_true", help="the reacting leg alone (profiling)")
+    ap.add_argument("--serving-only", action="store_true", help="the serving leg alone")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     args = ap.parse_args()
     set_cells(args.cells)
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.serving_only:
+        print(json.dumps({"serving": serving_leg()}), flush=True)
         return
     if args.reacting_only:
         print(json.dumps({"reacting": reacting_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
@@ -403,6 +458,9 @@ def main():
     reacting = None
     if rank == 0 and not args.no_reacting and not args.no_extra:
         reacting = reacting_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
+    served = None
+    if rank == 0 and not args.no_serving and not args.no_extra:
+        served = serving_leg()
 
     if rank == 0:
         line = {
@@ -423,6 +481,7 @@ def main():
                          "algorithmic_bytes_per_cell_stage": 170},
             "cpu_baseline": cpu,
             "reacting": reacting,
+            "serving": served,
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),

@@ -1770,14 +1770,22 @@ int pgb_pool_metric_set(pgb_pool *p, int slot, int which, const double *host, lo
   const int X = D.X + (face == 0), Y = D.Y + (face == 1), Z = D.Z + (face == 2);
   const int nc = comps[which];
   if (count != (long)X * Y * Z * nc) return fail(PGB_ERR_ARG, "metric array of the wrong size");
-  std::vector<double> dev((size_t)nc * D.vol);
-  for (int q = 0; q < nc; q++)
-    for (int k = 0; k < D.Z; k++)
-      for (int j = 0; j < D.Y; j++)
-        for (int i = 0; i < D.X; i++)
-          dev[(size_t)q * D.vol + cell_index(D, i, j, k)] = host[(((size_t)q * Z + k) * Y + j) * X + i];
-  CK(cudaMemcpyAsync(p->d_met + (size_t)M_NCOMP * D.cv + (size_t)first[which] * D.vol, dev.data(),
-                     sizeof(double) * dev.size(), cudaMemcpyHostToDevice, p->stream));
+  // the host array is F order over its own extents, as the device's: a cell
+  // array copies straight; a face array's rows (i faces), planes (j) or
+  // volumes (k) are one cell longer, and that last cell, past the halo, is
+  // never read: a pitched copy drops it
+  double *dst = p->d_met + (size_t)M_NCOMP * D.cv + (size_t)first[which] * D.vol;
+  const size_t w = sizeof(double);
+  if (face < 0)
+    CK(cudaMemcpyAsync(dst, host, w * nc * D.vol, cudaMemcpyHostToDevice, p->stream));
+  else if (face == 0)
+    CK(cudaMemcpy2DAsync(dst, w * D.X, host, w * X, w * D.X, (size_t)D.Y * D.Z * nc, cudaMemcpyHostToDevice, p->stream));
+  else if (face == 1)
+    CK(cudaMemcpy2DAsync(dst, w * D.X * D.Y, host, w * D.X * Y, w * D.X * D.Y, (size_t)D.Z * nc,
+                         cudaMemcpyHostToDevice, p->stream));
+  else
+    CK(cudaMemcpy2DAsync(dst, w * D.vol, host, w * (size_t)D.X * D.Y * Z, w * D.vol, (size_t)nc,
+                         cudaMemcpyHostToDevice, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   return PGB_OK;
 }
