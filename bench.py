@@ -30,7 +30,7 @@ MUSCL with the koren limiter and HLLC, Navier-Stokes, TVD-RK3, on the
 per-block device path; with the CPU oracle on one stage of it beside it.
 
 A serving leg (key "serving") plays a seeded Poisson stream of 400 H2/air
-requests at 500 per second: closed constant-volume reactors (phi, T0 and p
+requests at 200 per second: closed constant-volume reactors (phi, T0 and p
 drawn uniformly) and periodic 1-D domains of 64 to 2048 cells (log-uniform),
 100 RK3 steps each at one shared dt, admitted into one device pool while
 others run (peregrine_b200/serving.py); it reports throughput and the p50
@@ -256,7 +256,7 @@ def reacting_leg(steps, cpu=True):
     return out
 
 
-def serving_leg(n=400, rate=500.0, steps=100):
+def serving_leg(n=400, rate=200.0, steps=100):
     """The serving stream: Poisson arrivals of H2/air closed reactors and
     periodic 1-D domains, admitted into one pool while others run."""
     import ctypes
@@ -292,6 +292,7 @@ def serving_leg(n=400, rate=500.0, steps=100):
     return {"requests": n, "arrival_rate_per_s": rate, "steps_per_request": steps, "dt": dt,
             "cell_stages_per_s": srv.cell_stages / wall, "requests_per_s": n / wall, "wall_s": wall,
             "device_ms": srv.device_ms, "pool_steps": srv.steps, "launches": srv.launches,
+            "mean_running": srv.running_sum / max(srv.steps, 1), "admit_s": srv.admit_s,
             "latency_ms": st, "latency_0d_ms": serving.latency_stats(zero) if zero else None,
             "latency_1d_ms": serving.latency_stats(one) if one else None,
             "arena_cells": cap, "per_cell_bytes": per_cell,

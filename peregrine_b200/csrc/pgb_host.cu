@@ -1657,6 +1657,8 @@ int pool_slot(pgb_pool *p, int slot, int want) {
 
 int pool_stage_host(pgb_pool *p, long long n) {
   if (n > p->host_cap) {
+    // queued work may still read the old staging buffer
+    CK(cudaStreamSynchronize(p->stream));
     if (p->d_host) CK(cudaFree(p->d_host));
     p->d_host = nullptr;
     CK(cudaMalloc(&p->d_host, sizeof(double) * n));
@@ -1753,8 +1755,8 @@ int pgb_pool_admit(pgb_pool *p, int ni, int nj, int nk, int *slot) {
   for (int r = 0; r < p->phys.nregs; r++)
     CK(cudaMemsetAsync(p->d_reg[r] + (size_t)p->ne * cv, 0, sizeof(double) * p->ne * vol, p->stream));
   CK(cudaMemsetAsync(p->d_state + (size_t)8 * cv, 0, sizeof(double) * 8 * vol, p->stream));
+  // from pageable memory: the call returns once D is staged, so the stack copy may go
   CK(cudaMemcpyAsync(p->d_blks + id, &D, sizeof(BlockDev), cudaMemcpyHostToDevice, p->stream));
-  CK(cudaStreamSynchronize(p->stream));
   *slot = id;
   return PGB_OK;
 }
@@ -1786,7 +1788,8 @@ int pgb_pool_metric_set(pgb_pool *p, int slot, int which, const double *host, lo
   else
     CK(cudaMemcpy2DAsync(dst, w * D.vol, host, w * (size_t)D.X * D.Y * Z, w * D.vol, (size_t)nc,
                          cudaMemcpyHostToDevice, p->stream));
-  CK(cudaStreamSynchronize(p->stream));
+  // pageable source: each copy has taken the host data when it returns, and
+  // the launches that read it follow on the same stream
   return PGB_OK;
 }
 
@@ -1806,7 +1809,6 @@ int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count) {
   // a halo cell's first Newton starts from the stored T of the cell it copies
   k_selfhalo<<<grid_for(hb[slot].vol, 256), 256, 0, p->stream>>>(p->d_blks, slot, p->d_state, 8);
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(p->stream));
   return PGB_OK;
 }
 

@@ -133,6 +133,8 @@ class Server:
         self.launches = 0
         self.steps = 0
         self.cell_stages = 0
+        self.running_sum = 0
+        self.admit_s = 0.0
 
     def run(self, requests, stages_per_step, clock=time.perf_counter, sleep=time.sleep):
         """Serve every request; arrival times are seconds from the start.
@@ -147,7 +149,9 @@ class Server:
             now = clock() - t0
             # admit every arrival so far, in order, while the arena has room
             while q < len(pending) and pending[q].arrival <= now:
+                ta = clock()
                 slot = self.pool.admit(pending[q])
+                self.admit_s += clock() - ta
                 if slot is None:
                     break
                 pending[q].admitted = clock() - t0
@@ -161,6 +165,7 @@ class Server:
             self.device_ms += ms
             self.launches += launches
             self.steps += 1
+            self.running_sum += len(running)
             self.cell_stages += stages_per_step * sum(int(np.prod(r.cells)) for r in running.values())
             for slot in self.pool.done():
                 req = running.pop(slot)
