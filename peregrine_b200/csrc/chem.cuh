@@ -209,10 +209,10 @@ __device__ __forceinline__ void cellrates(QF Q, const double T, double *omega) {
 // it (peregrine/simulator/chemint/kernels/source.mako:3-10, cell.mako:14-19)
 template <int NS>
 __global__ void k_source(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                         const double *__restrict__ stall, double *__restrict__ dQall) {
+                         const double *__restrict__ stall, double *__restrict__ dQall,
+                         const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  PGB_WHERE(B, t);
   if (t >= (long long)B.nx * B.ny * B.nz) return;
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
   const long long c = cell_index(B, i, j, k), v = B.vol;

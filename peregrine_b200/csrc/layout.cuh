@@ -44,6 +44,17 @@ __host__ __device__ __forceinline__ long long cell_index(const BlockDev &b, int 
   return (long long)fi + (long long)b.X * ((long long)fj + (long long)b.Y * fk);
 }
 
+// Where a per-block kernel's thread works: its block and its index t in the
+// pass's range over that block.  With a tile table (a packed launch over many
+// blocks), CTA x does tile ctab[x].y of block row ctab[x].x, so a launch has
+// exactly the CTAs its blocks need; without one, the block is b plus the grid
+// row and the tile the CTA's x.  The kernel names its block index b, its
+// descriptor table blks and its tile table ctab.
+#define PGB_WHERE(B, t)                                                                              \
+  const int2 where_ = ctab ? ctab[blockIdx.x] : make_int2(b + (int)blockIdx.y, (int)blockIdx.x); \
+  const BlockDev &B = blks[where_.x];                                                                \
+  const long long t = (long long)where_.y * blockDim.x + threadIdx.x
+
 // one cell of a halo filled from another cell: each side's block start in
 // cells (cv), its cell index inside the block and its component stride (vol)
 struct HaloEntry {

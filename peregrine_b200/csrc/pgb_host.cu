@@ -1519,6 +1519,8 @@ struct pgb_pool {
   BlockDev *d_run = nullptr;   // the running table, by row
   HaloEntry *d_halo = nullptr;
   long long halo_cap = 0, nhalo = 0, nhalo_l0 = 0;
+  int2 *d_ctab = nullptr;  // the running blocks' tile tables, one per range, end to end
+  long long ctab_cap = 0, ctab_off[5] = {}, nctab[5] = {};
   std::vector<PoolSlot> slots;
   std::map<long long, long long> free_;  // arena ranges: start -> cells
   std::vector<BlockDev> run;             // running blocks, host copy
@@ -1604,6 +1606,26 @@ int pool_rebuild(pgb_pool *p) {
     CK(cudaMemcpyAsync(p->d_halo, l0.data(), sizeof(HaloEntry) * p->nhalo, cudaMemcpyHostToDevice, p->stream));
   if (!p->run.empty())
     CK(cudaMemcpyAsync(p->d_run, p->run.data(), sizeof(BlockDev) * p->run.size(), cudaMemcpyHostToDevice, p->stream));
+  // each range's tiles: as many 256-thread CTAs as each block needs, no more
+  std::vector<int2> tiles;
+  for (int r = 0; r < 5; r++) {
+    p->ctab_off[r] = (long long)tiles.size();
+    for (int row = 0; row < (int)p->run.size(); row++) {
+      const long long n = (range_size(p->run[row], r) + 255) / 256;
+      for (long long t = 0; t < n; t++) tiles.push_back(make_int2(row, (int)t));
+    }
+    p->nctab[r] = (long long)tiles.size() - p->ctab_off[r];
+  }
+  if ((long long)tiles.size() > p->ctab_cap) {
+    CK(cudaStreamSynchronize(p->stream));
+    if (p->d_ctab) CK(cudaFree(p->d_ctab));
+    p->d_ctab = nullptr;
+    const long long cap = std::max<long long>((long long)tiles.size(), 2 * p->ctab_cap);
+    CK(cudaMalloc(&p->d_ctab, sizeof(int2) * cap));
+    p->ctab_cap = cap;
+  }
+  if (!tiles.empty())
+    CK(cudaMemcpyAsync(p->d_ctab, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, p->stream));
   // the host vectors are read by the copies above: wait before they change
   CK(cudaStreamSynchronize(p->stream));
   p->dirty = false;
@@ -1644,6 +1666,14 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.packed = 1;
   pc.stream = p->stream;
   return pc;
+}
+
+// the running table's packing: its tile tables
+void pool_tiles(const pgb_pool *p, PlainCase &pc) {
+  for (int r = 0; r < 5; r++) {
+    pc.ctab[r] = p->d_ctab ? p->d_ctab + p->ctab_off[r] : nullptr;
+    pc.nctab[r] = p->nctab[r];
+  }
 }
 
 void count_cb(void *ctx, int) { ++*(int *)ctx; }
@@ -1712,7 +1742,7 @@ int pgb_pool_destroy(pgb_pool *p) {
   for (auto &r : p->d_reg)
     if (r) cudaFree(r);
   void *ptrs[] = {p->d_met, p->d_state, p->d_tr, p->d_hsp, p->d_grads, p->d_F[0], p->d_F[1], p->d_F[2],
-                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo};
+                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo, p->d_ctab};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->ev0) cudaEventDestroy(p->ev0);
@@ -1836,11 +1866,11 @@ int pgb_pool_step(pgb_pool *p, double dt, int nsteps) {
     const int nrun = (int)p->run.size();
     if (nrun == 0) break;
     PlainCase pc = pool_plain(p, p->d_run, p->run.data(), nrun);
+    pool_tiles(p, pc);
     pc.mark = count_cb;
     pc.ctx = &launches;
-    long long most = 0;
-    for (const BlockDev &D : p->run) most = std::max<long long>(most, (long long)D.nx * D.ny * D.nz);
-    const dim3 g((unsigned)grid_for(most, 256), (unsigned)nrun, 1);
+    const dim3 g((unsigned)p->nctab[R_INNER], 1, 1);
+    const int2 *inner_tiles = pc.ctab[R_INNER];
     for (const pgb_stage &st : p->stages) {
       RET(kPlain[p->phys.ns - 1].rhs(&pc, p->d_reg[st.q], p->d_reg[st.dq]));
       for (int m = 0; m < st.ncombine; m++) {
@@ -1855,7 +1885,7 @@ int pgb_pool_step(pgb_pool *p, double dt, int nsteps) {
           cd.X[n] = p->d_reg[cb.reg[n] < 0 ? st.dq : cb.reg[n]];
           cd.w[n] = cb.w[n];
         }
-        k_combine<<<g, 256, 0, p->stream>>>(p->d_run, 0, p->ne, cd, p->d_dt);
+        k_combine<<<g, 256, 0, p->stream>>>(p->d_run, 0, p->ne, cd, p->d_dt, inner_tiles);
         launches++;
       }
     }

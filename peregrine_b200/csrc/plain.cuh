@@ -35,9 +35,8 @@ __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi,
 // (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19)
 template <int NS>
 __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                        double *__restrict__ stall) {
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                        double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr) {
+  PGB_WHERE(B, t);
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
   double *st = stall + 8 * B.cv + t;
@@ -59,9 +58,8 @@ __device__ __forceinline__ State load_state(const double *st, long long v) {
 template <int NS>
 __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                             const double *__restrict__ stall, double *__restrict__ trall,
-                            double *__restrict__ hall) {
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                            double *__restrict__ hall, const int2 *__restrict__ ctab = nullptr) {
+  PGB_WHERE(B, t);
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
   const State s = load_state(stall + 8 * B.cv + t, B.vol);
@@ -83,10 +81,10 @@ __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const doub
 template <int NS>
 __global__ void k_grads(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                         const double *__restrict__ stall, const double *__restrict__ met,
-                        double *__restrict__ gall, int grow = 0) {
+                        double *__restrict__ gall, int grow = 0,
+                        const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS, NGRAD = NE - 1;
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  PGB_WHERE(B, t);
   const int gx = B.nx + 2 * grow, gy = B.ny + 2 * grow, gz = B.nz + 2 * grow;
   const long long n = (long long)gx * gy * gz;
   if (t >= n) return;
@@ -140,11 +138,11 @@ __device__ __forceinline__ bool face_at(const BlockDev &B, long long t, int &i, 
 template <int NS, int A>
 __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                           const double *__restrict__ stall, const double *__restrict__ met,
-                          double *__restrict__ Fall) {
+                          double *__restrict__ Fall, const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b + blockIdx.y];
+  PGB_WHERE(B, t);
   int i, j, k;
-  if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+  if (!face_at<A>(B, t, i, j, k)) return;
   const long long R = cell_index(B, i, j, k);
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
@@ -178,11 +176,12 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
 template <int NS, int A, int FN>
 __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                           const double *__restrict__ stall, const double *__restrict__ met,
-                          double *__restrict__ Fall, const int lim) {
+                          double *__restrict__ Fall, const int lim,
+                          const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS, NY = NS > 1 ? NS - 1 : 1;
-  const BlockDev &B = blks[b + blockIdx.y];
+  PGB_WHERE(B, t);
   int i, j, k;
-  if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+  if (!face_at<A>(B, t, i, j, k)) return;
   const long long R = cell_index(B, i, j, k);
   const long long d = A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y;
   const long long L = R - d;
@@ -237,11 +236,12 @@ template <int NS, int A>
 __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                            const double *__restrict__ stall, const double *__restrict__ trall,
                            const double *__restrict__ hall, const double *__restrict__ gall,
-                           const double *__restrict__ met, double *__restrict__ Fall) {
+                           const double *__restrict__ met, double *__restrict__ Fall,
+                           const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS, NGRAD = NE - 1;
-  const BlockDev &B = blks[b + blockIdx.y];
+  PGB_WHERE(B, t);
   int i, j, k;
-  if (!face_at<A>(B, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+  if (!face_at<A>(B, t, i, j, k)) return;
   const long long R = cell_index(B, i, j, k);
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
@@ -333,10 +333,10 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
 template <int NS>
 __global__ void k_applyflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Fi,
                             const double *__restrict__ Fj, const double *__restrict__ Fk,
-                            const double *__restrict__ met, double *__restrict__ dQall, int append = 0) {
+                            const double *__restrict__ met, double *__restrict__ dQall, int append = 0,
+                            const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  PGB_WHERE(B, t);
   if (t >= (long long)B.nx * B.ny * B.nz) return;
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
   const long long c = cell_index(B, i, j, k), v = B.vol;
@@ -361,9 +361,9 @@ struct CombineDev {
   int own, nterms, step;
 };
 
-static __global__ void k_combine(const BlockDev *__restrict__ blks, int b, int ne, CombineDev cd, const double *__restrict__ dt) {
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+static __global__ void k_combine(const BlockDev *__restrict__ blks, int b, int ne, CombineDev cd, const double *__restrict__ dt,
+                                 const int2 *__restrict__ ctab = nullptr) {
+  PGB_WHERE(B, t);
   if (t >= (long long)B.nx * B.ny * B.nz) return;
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
   const long long c = cell_index(B, i, j, k) + ne * B.cv;

@@ -11,6 +11,18 @@
 
 namespace pgb {
 
+// the ranges a pass runs over
+enum { R_VOL = 0, R_INNER = 1, R_FX = 2, R_FY = 3, R_FZ = 4 };
+inline long long range_size(const BlockDev &D, int r) {
+  switch (r) {
+    case R_VOL: return D.vol;
+    case R_INNER: return (long long)D.nx * D.ny * D.nz;
+    case R_FX: return (long long)(D.nx + 1) * D.ny * D.nz;
+    case R_FY: return (long long)D.nx * (D.ny + 1) * D.nz;
+    default: return (long long)D.nx * D.ny * (D.nz + 1);
+  }
+}
+
 // what a right-hand side on the per-block path reads of a case
 struct PlainCase {
   const BlockDev *d_blks;  // device descriptors
@@ -21,7 +33,12 @@ struct PlainCase {
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
   int visc, primary, recon, limiter, chem;
-  int packed;  // 1: each pass is one launch over every block, a grid row per block
+  int packed;  // 1: each pass is one launch over every block
+  // with packing, each range's tile table (cells with halo, interior cells,
+  // i, j and k faces): CTA x works tile ctab[r][x].y of block ctab[r][x].x;
+  // without a table a packed launch gives each block a grid row
+  const int2 *ctab[5];
+  long long nctab[5];
   cudaStream_t stream;
   void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block
   void *ctx;

@@ -37,19 +37,24 @@ void mark(const PlainCase *pc, int kind) {
   if (pc->mark) pc->mark(pc->ctx, kind);
 }
 
-// a pass over every block: one launch per block, or packed, one launch whose
-// rows are the blocks, each row as long as the largest block needs
-template <class F>
-void for_blocks(const PlainCase *pc, F size, void (*launch)(const PlainCase *, int, dim3, const void *),
-                const void *ctx, int kind) {
+// a pass over every block: one launch per block, or packed, one launch over
+// them all, by the range's tile table when there is one, else a grid row per
+// block as long as the largest block needs
+typedef void (*Launch)(const PlainCase *, int, dim3, const int2 *, const void *);
+
+void for_blocks(const PlainCase *pc, int range, Launch launch, const void *ctx, int kind) {
   if (pc->packed) {
-    long long most = 0;
-    for (int b = 0; b < pc->nblocks; b++) most = std::max(most, size(pc->h_blks[b]));
-    if (pc->nblocks > 0) launch(pc, 0, dim3(grid_of(most), (unsigned)pc->nblocks, 1), ctx);
+    if (pc->ctab[range]) {
+      if (pc->nctab[range] > 0) launch(pc, 0, dim3((unsigned)pc->nctab[range], 1, 1), pc->ctab[range], ctx);
+    } else {
+      long long most = 0;
+      for (int b = 0; b < pc->nblocks; b++) most = std::max(most, range_size(pc->h_blks[b], range));
+      if (pc->nblocks > 0) launch(pc, 0, dim3(grid_of(most), (unsigned)pc->nblocks, 1), nullptr, ctx);
+    }
     mark(pc, kind);
   } else {
     for (int b = 0; b < pc->nblocks; b++) {
-      launch(pc, b, dim3(grid_of(size(pc->h_blks[b])), 1, 1), ctx);
+      launch(pc, b, dim3(grid_of(range_size(pc->h_blks[b], range)), 1, 1), nullptr, ctx);
       mark(pc, kind);
     }
   }
@@ -60,50 +65,44 @@ struct RhsArgs {
   double *dQ;
 };
 
-long long vol_of(const BlockDev &D) { return D.vol; }
-long long inner_of(const BlockDev &D) { return (long long)D.nx * D.ny * D.nz; }
-long long fx_of(const BlockDev &D) { return (long long)(D.nx + 1) * D.ny * D.nz; }
-long long fy_of(const BlockDev &D) { return (long long)D.nx * (D.ny + 1) * D.nz; }
-long long fz_of(const BlockDev &D) { return (long long)D.nx * D.ny * (D.nz + 1); }
-
 template <int A>
-void adv_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void adv_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
   const int lim = pc->recon == PGB_RECON_MUSCL ? pc->limiter : 0;
   cudaStream_t s = pc->stream;
   switch (pc->primary) {
-    case PGB_FLUX_HLLC: k_riemann<NS, A, FN_HLLC><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim); break;
-    case PGB_FLUX_RUSANOV: k_riemann<NS, A, FN_RUSANOV><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim); break;
-    case PGB_FLUX_AUSMUP: k_riemann<NS, A, FN_AUSMUP><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim); break;
-    default: k_advflux<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A]);
+    case PGB_FLUX_HLLC: k_riemann<NS, A, FN_HLLC><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
+    case PGB_FLUX_RUSANOV: k_riemann<NS, A, FN_RUSANOV><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
+    case PGB_FLUX_AUSMUP: k_riemann<NS, A, FN_AUSMUP><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
+    default: k_advflux<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
   }
 }
 
 template <int A>
-void diff_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void diff_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_diffflux<NS, A><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A]);
+  k_diffflux<NS, A><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A], ct);
 }
 
-void fromQ_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_fromQ<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state);
+  k_fromQ<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct);
 }
-void transport_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void transport_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_transport<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp);
+  k_transport<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, ct);
 }
-void grads_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void grads_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_grads<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->grads);
+  k_grads<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->grads, 0, ct);
 }
-void source_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void source_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, a.dQ);
+  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, a.dQ, ct);
 }
-void apply_launch(const PlainCase *pc, int b, dim3 g, const void *ctx) {
+void apply_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_applyflux<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, a.dQ, pc->chem);
+  k_applyflux<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, a.dQ, pc->chem, ct);
 }
 
 }  // namespace
@@ -145,20 +144,20 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
   k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(Q), pc->halo, pc->nhalo, NE);
   mark(pc, 0);
   if (pc->packed) {
-    for_blocks(pc, vol_of, fromQ_launch, &a, 2);
+    for_blocks(pc, R_VOL, fromQ_launch, &a, 2);
     if (pc->visc) {
-      for_blocks(pc, vol_of, transport_launch, &a, 2);
-      for_blocks(pc, inner_of, grads_launch, &a, 2);
+      for_blocks(pc, R_VOL, transport_launch, &a, 2);
+      for_blocks(pc, R_INNER, grads_launch, &a, 2);
     }
   } else {
     for (int b = 0; b < pc->nblocks; b++) {
       const BlockDev &D = pc->h_blks[b];
-      fromQ_launch(pc, b, dim3(grid_of(D.vol)), &a);
+      fromQ_launch(pc, b, dim3(grid_of(D.vol)), nullptr, &a);
       mark(pc, 2);
       if (pc->visc) {
-        transport_launch(pc, b, dim3(grid_of(D.vol)), &a);
+        transport_launch(pc, b, dim3(grid_of(D.vol)), nullptr, &a);
         mark(pc, 2);
-        grads_launch(pc, b, dim3(grid_of(inner_of(D))), &a);
+        grads_launch(pc, b, dim3(grid_of(range_size(D, R_INNER))), nullptr, &a);
         mark(pc, 2);
       }
     }
@@ -168,38 +167,39 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
     mark(pc, 0);
   }
   if (pc->packed) {
-    if (pc->chem) for_blocks(pc, inner_of, source_launch, &a, 2);
-    for_blocks(pc, fx_of, adv_launch<0>, &a, 2);
-    for_blocks(pc, fy_of, adv_launch<1>, &a, 2);
-    for_blocks(pc, fz_of, adv_launch<2>, &a, 2);
+    if (pc->chem) for_blocks(pc, R_INNER, source_launch, &a, 2);
+    for_blocks(pc, R_FX, adv_launch<0>, &a, 2);
+    for_blocks(pc, R_FY, adv_launch<1>, &a, 2);
+    for_blocks(pc, R_FZ, adv_launch<2>, &a, 2);
     if (pc->visc) {
-      for_blocks(pc, fx_of, diff_launch<0>, &a, 2);
-      for_blocks(pc, fy_of, diff_launch<1>, &a, 2);
-      for_blocks(pc, fz_of, diff_launch<2>, &a, 2);
+      for_blocks(pc, R_FX, diff_launch<0>, &a, 2);
+      for_blocks(pc, R_FY, diff_launch<1>, &a, 2);
+      for_blocks(pc, R_FZ, diff_launch<2>, &a, 2);
     }
-    for_blocks(pc, inner_of, apply_launch, &a, 2);
+    for_blocks(pc, R_INNER, apply_launch, &a, 2);
   } else {
     for (int b = 0; b < pc->nblocks; b++) {
       const BlockDev &D = pc->h_blks[b];
+      auto g = [&](int r) { return dim3(grid_of(range_size(D, r))); };
       if (pc->chem) {
-        source_launch(pc, b, dim3(grid_of(inner_of(D))), &a);
+        source_launch(pc, b, g(R_INNER), nullptr, &a);
         mark(pc, 2);
       }
-      adv_launch<0>(pc, b, dim3(grid_of(fx_of(D))), &a);
+      adv_launch<0>(pc, b, g(R_FX), nullptr, &a);
       mark(pc, 2);
-      adv_launch<1>(pc, b, dim3(grid_of(fy_of(D))), &a);
+      adv_launch<1>(pc, b, g(R_FY), nullptr, &a);
       mark(pc, 2);
-      adv_launch<2>(pc, b, dim3(grid_of(fz_of(D))), &a);
+      adv_launch<2>(pc, b, g(R_FZ), nullptr, &a);
       mark(pc, 2);
       if (pc->visc) {
-        diff_launch<0>(pc, b, dim3(grid_of(fx_of(D))), &a);
+        diff_launch<0>(pc, b, g(R_FX), nullptr, &a);
         mark(pc, 2);
-        diff_launch<1>(pc, b, dim3(grid_of(fy_of(D))), &a);
+        diff_launch<1>(pc, b, g(R_FY), nullptr, &a);
         mark(pc, 2);
-        diff_launch<2>(pc, b, dim3(grid_of(fz_of(D))), &a);
+        diff_launch<2>(pc, b, g(R_FZ), nullptr, &a);
         mark(pc, 2);
       }
-      apply_launch(pc, b, dim3(grid_of(inner_of(D))), &a);
+      apply_launch(pc, b, g(R_INNER), nullptr, &a);
       mark(pc, 2);
     }
   }
