@@ -29,8 +29,8 @@ thermally perfect, kinetic-theory transport, coupled finite-rate chemistry),
 MUSCL with the koren limiter and HLLC, Navier-Stokes, TVD-RK3, on the
 per-block device path; with the CPU oracle on one stage of it beside it.
 
-A serving leg (key "serving") plays a seeded Poisson stream of 400 H2/air
-requests at 200 per second: closed constant-volume reactors (phi, T0 and p
+A serving leg (key "serving") plays a seeded Poisson stream of 300 H2/air
+requests at 60 per second: closed constant-volume reactors (phi, T0 and p
 drawn uniformly) and periodic 1-D domains of 64 to 2048 cells (log-uniform),
 100 RK3 steps each at one shared dt, admitted into one device pool while
 others run (peregrine_b200/serving.py); it reports throughput and the p50
@@ -256,7 +256,7 @@ def reacting_leg(steps, cpu=True):
     return out
 
 
-def serving_leg(n=400, rate=200.0, steps=100):
+def serving_leg(n=300, rate=60.0, steps=100):
     """The serving stream: Poisson arrivals of H2/air closed reactors and
     periodic 1-D domains, admitted into one pool while others run."""
     import ctypes
