@@ -41,8 +41,8 @@ enum {
 };
 
 /* physics selectors: the config's names (peregrine/config.py:12-98) */
-enum { PGB_EULER = 0, PGB_NAVIER_STOKES = 1 };
-enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1 };
+enum { PGB_EULER = 0, PGB_NAVIER_STOKES = 1, PGB_EULER_DF = 2 };
+enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1, PGB_EOS_REALGAS = 2, PGB_EOS_REALGAS_DF = 3 };
 enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2, PGB_FLUX_AUSMUP = 3 };
 enum { PGB_RECON_CONSTANT = 0, PGB_RECON_MUSCL = 1 };
 enum { PGB_TRANS_NONE = 0, PGB_TRANS_CONSTANT = 1, PGB_TRANS_KINETIC = 2 };
@@ -157,7 +157,11 @@ int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long
 /* the thermally perfect gas reads "cppolyR" (cp in ln T times R_sp) and
  * "hpoly" (h / R T), kinetic-theory transport "mupoly" and "kappapoly", each
  * [ns][terms] with 1 to 8 terms (peregrine/simulator/mixture/eos/tpg/model.py,
- * peregrine/simulator/mixture/transport/kinetic.py) */
+ * peregrine/simulator/mixture/transport/kinetic.py); the real gas those of
+ * the thermally perfect gas and the cubic's: "cubicu", "cubicw",
+ * "cubicsigma", "cubiceps" (one value each), "cubicsqrtac", "cubicb",
+ * "cubicda", "cubicmTc", "cubiconepm", "vshift", "cubicsqrtacMW", "cubicbMW",
+ * "cubicdaMW", "vshiftMW" (ns each; peregrine/simulator/mixture/eos/realgas/model.py:43-98) */
 /* the case's finite-rate mechanism, copied; before finalize */
 int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m);
 /* net production rates omega[n][ns], kg / m^3 / s, of n states rho[n],

@@ -35,7 +35,13 @@ class OCase(ctypes.Structure):
                 ("eos", ctypes.c_int), ("ncp", ctypes.c_int), ("cppolyR", ctypes.POINTER(ctypes.c_double)),
                 ("nh", ctypes.c_int), ("hpoly", ctypes.POINTER(ctypes.c_double)), ("trans", ctypes.c_int),
                 ("nmu", ctypes.c_int), ("nkappa", ctypes.c_int), ("mupoly", ctypes.POINTER(ctypes.c_double)),
-                ("kappapoly", ctypes.POINTER(ctypes.c_double)), ("mech", ctypes.c_void_p)]
+                ("kappapoly", ctypes.POINTER(ctypes.c_double)), ("mech", ctypes.c_void_p),
+                ("realgas", ctypes.c_int), ("df", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in ("cu", "cw", "csigma", "ceps")] + \
+               [(n, ctypes.POINTER(ctypes.c_double)) for n in
+                ("csqrtac", "cb", "cda", "cmTc", "conepm", "vshift", "csqrtacMW", "cbMW", "cdaMW", "vshiftMW")]
+
+NSTATE = 24  # the oracle's per-cell record: EosState, Z, the double flux's plane
 
 
 MAXSIDE = 8
@@ -69,7 +75,7 @@ class OBlock(ctypes.Structure):
                 ("xcc", ctypes.POINTER(ctypes.c_double)), ("detJinv", ctypes.POINTER(ctypes.c_double)),
                 ("Jinv", ctypes.POINTER(ctypes.c_double)),
                 ("S", ctypes.POINTER(ctypes.c_double) * 3), ("xf", ctypes.POINTER(ctypes.c_double) * 3),
-                ("Tg", ctypes.POINTER(ctypes.c_double))]
+                ("Tg", ctypes.POINTER(ctypes.c_double)), ("pst", ctypes.POINTER(ctypes.c_double))]
 
 
 def _side(sp, val):
@@ -141,7 +147,8 @@ def _lib():
     lib.oracle_kepaec_faces.restype = ctypes.c_int
     lib.oracle_advective_faces.restype = ctypes.c_int
     for name in ("oracle_production", "oracle_gibbs", "oracle_tlog", "oracle_texp", "oracle_mathtables",
-                 "oracle_species_cph", "oracle_fromQ"):
+                 "oracle_species_cph", "oracle_fromQ", "oracle_prestep", "oracle_realgas_frompT",
+                 "oracle_realgas_fromQ", "oracle_freeze"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 
@@ -276,7 +283,18 @@ class Oracle:
         hp = np.ascontiguousarray(np.asarray(constants["hpoly"])[:, 0], dtype=np.float64)
         self._tables["hpoly0"] = hp
         c.hpoly0 = _ptr(hp)
-        if eos == "tpg":
+        if eos in ("real-gas", "real-gas-df"):
+            c.realgas, c.df = 1, int(eos == "real-gas-df")
+            for name in ("cu", "cw", "csigma", "ceps"):
+                setattr(c, name, float(constants["cubic" + name[1:]]))
+            keys = dict(csqrtac="cubicsqrtac", cb="cubicb", cda="cubicda", cmTc="cubicmTc", conepm="cubiconepm",
+                        vshift="vshift", csqrtacMW="cubicsqrtacMW", cbMW="cubicbMW", cdaMW="cubicdaMW",
+                        vshiftMW="vshiftMW")
+            for field, key in keys.items():
+                arr = np.ascontiguousarray(constants[key], dtype=np.float64).ravel()
+                self._tables[field] = arr
+                setattr(c, field, _ptr(arr))
+        if eos != "cpg":
             c.eos = 1
             cpr = np.ascontiguousarray(constants["cppolyR"], dtype=np.float64)
             hpoly = np.ascontiguousarray(constants["hpoly"], dtype=np.float64)
@@ -299,6 +317,11 @@ class Oracle:
         self.regs = [[np.zeros(self._shape(b)) for b in blocks] for _ in range(self.nregs)]
         # each cell's last temperature, the iterative eos's starting guess
         self.Tg = [np.zeros(self._shape(b)[:3]) for b in blocks]
+        # the double flux's kept records (state and frozen plane), and whether
+        # the planes are yet to be frozen for the state set
+        self.df = eos == "real-gas-df"
+        self.pst = [np.zeros(self._shape(b)[:3] + (NSTATE,)) for b in blocks] if self.df else None
+        self.df_fresh = True
 
     def _shape(self, blk):
         return tuple(n + 2 * blk.ng for n in blk.cells) + (self.ne,)
@@ -316,6 +339,8 @@ class Oracle:
                 o.S[a] = _ptr(m[f"{d}S"])
                 o.xf[a] = _ptr(m[f"{d}xc"])
             o.Tg = _ptr(self.Tg[n])
+            if self.pst is not None:
+                o.pst = _ptr(self.pst[n])
             keep.append(o)
         return obs
 
@@ -325,6 +350,7 @@ class Oracle:
             assert q.shape == Q.shape
             self.lib.oracle_fromprims(ctypes.byref(self.case), _ptr(q), _ptr(Q), ctypes.c_long(Q.size // self.ne),
                                       _ptr(self.Tg[n]))
+        self.df_fresh = True
         # a halo cell's first Newton starts from the stored T of the cell it
         # copies, as the device's set_prims leaves it
         m = self.map
@@ -364,13 +390,16 @@ class Oracle:
         m = np.ascontiguousarray(self.map)
         ptrs = (ctypes.POINTER(ctypes.c_double) * len(dQ))(*[_ptr(d) for d in dQ])
         fl, fptr = None, None
+        if self.df and self.df_fresh:
+            self.prestep(Q)
         if faces:
             fl = []
+            nf = self.ne + (1 if self.df else 0)
             for blk in self.blocks:
                 for a in range(3):
                     shape = [n + 2 * blk.ng for n in blk.cells]
                     shape[a] += 1
-                    fl.append(np.zeros(tuple(shape) + (self.ne,)))
+                    fl.append(np.zeros(tuple(shape) + (nf,)))
             fptr = (ctypes.POINTER(ctypes.c_double) * len(fl))(*[_ptr(f) for f in fl])
         self.case.skip_adv = int(diffusive_only)
         rc = self.lib.oracle_rhs(ctypes.byref(self.case), obs, len(self.blocks),
@@ -397,9 +426,38 @@ class Oracle:
         self.lib.oracle_kepaec_faces(ctypes.byref(self.case), ctypes.c_long(QL.shape[0]), _ptr(QL), _ptr(QR), _ptr(S), _ptr(F))
         return F
 
+    def prestep(self, Q):
+        """The double flux's step start on register Q (its freeze)."""
+        obs = self._oblocks(Q)
+        m = np.ascontiguousarray(self.map)
+        self.lib.oracle_prestep(ctypes.byref(self.case), obs, len(self.blocks), m.ctypes.data_as(ctypes.c_void_p),
+                                ctypes.c_long(m.size), int(self.df_fresh))
+        self.df_fresh = False
+
+    def realgas_frompT(self, p, T, Y):
+        """Records [n, NSTATE] of the real gas at (p, T, Y carried) points."""
+        p, T, Y = (np.ascontiguousarray(x, dtype=np.float64) for x in (p, T, Y))
+        out = np.zeros((len(p), NSTATE))
+        self.lib.oracle_realgas_frompT(ctypes.byref(self.case), ctypes.c_long(len(p)), _ptr(p), _ptr(T), _ptr(Y),
+                                       _ptr(out))
+        return out
+
+    def realgas_fromQ(self, Q, Tguess):
+        Q, Tg = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, Tguess))
+        out = np.zeros((len(Tg), NSTATE))
+        self.lib.oracle_realgas_fromQ(ctypes.byref(self.case), ctypes.c_long(len(Tg)), _ptr(Q), _ptr(Tg), _ptr(out))
+        return out
+
+    def freeze(self, Q, rec):
+        """Freeze at independent cells: Q's energy and rec's planes in place."""
+        assert Q.flags["C_CONTIGUOUS"] and rec.flags["C_CONTIGUOUS"]
+        self.lib.oracle_freeze(ctypes.byref(self.case), ctypes.c_long(len(Q)), _ptr(Q), _ptr(rec))
+
     def step(self, dt):
         names = list(range(self.nregs))
         stages, dQ = stage_combines(self.integrator, names)
+        if self.df:
+            self.prestep(self.regs[stages[0][0]])
         for Q, combines in stages:
             self.rhs(self.regs[Q], self.regs[dQ])
             for out, own, reads, step in combines:

@@ -46,6 +46,9 @@ struct OCase {
   int nmu, nkappa;        // kinetic theory: terms of the fits below
   const double *mupoly, *kappapoly;  // [ns][nmu] sqrt(mu) / T^(1/4), [ns][nkappa] kappa / sqrt(T), in ln T
   const struct OMech *mech;  // finite-rate chemistry, coupled; null for none
+  int realgas, df;           // the cubic real gas; its double flux (euler-df)
+  double cu, cw, csigma, ceps;
+  const double *csqrtac, *cb, *cda, *cmTc, *conepm, *vshift, *csqrtacMW, *cbMW, *cdaMW, *vshiftMW;  // [ns]
 };
 
 // one reaction, the columns of FiniteRateModel.rxnconsts
@@ -84,6 +87,7 @@ struct OBlock {
   const double *xcc, *detJinv, *Jinv;       // cells: [..][3], [..], [..][3][3]
   const double *S[3], *xf[3];               // faces of axis a: [..][3]
   double *Tg;                               // [..]: each cell's last T, an iterative eos's starting guess
+  double *pst;                              // [..][NSTATE]: the double flux's kept state and frozen planes
 };
 
 // one halo cell of one block filled from a cell of another (the place kernel,
@@ -117,7 +121,9 @@ Dims face_dims(const OBlock &b, int a) {
 struct State {
   double p, T, rhoinv, rho, e, cp, gamma, c;
 };
-enum { NSTATE = 8 };
+// the per-cell state record: EosState, then the real gas's Z and the double
+// flux's plane theta, eps, kappa, zeta[ns - 1]
+enum { NSTATE = 24, S_Z = 8, S_THETA = 9, S_EPS = 10, S_KAPPA = 11, S_ZETA = 12 };
 
 // mixmom, simulator/mixture/eos/kernels/mixing.mako:3-30: cpg's moments are
 // R <- Rsp, cp <- cp0, h298 <- h298R (simulator/mixture/eos/cpg/__init__.py),
@@ -217,7 +223,15 @@ State fromQ(const OCase &c, const double *Q, double Tguess = 0.0) {
 
 // frompT: cpg (simulator/mixture/eos/cpg/kernels/eos.mako:17-27), tpg
 // (simulator/mixture/eos/tpg/kernels/eos.mako:22-32)
+// the real gas's frompT and species enthalpies, further down
+template <class YF> State rfrompT(const OCase &c, double p, double T, YF Y, double &Zout);
+template <class YF> void rhspecies(const OCase &c, double *h, YF Y, double p, double T, double Z);
+
 State frompT(const OCase &c, double p, double T, const double *Y) {
+  if (c.realgas) {
+    double Z;
+    return rfrompT(c, p, T, [&](int n) { return Y[n]; }, Z);
+  }
   Mom mom = mixmom(c, [&](int n) { return Y[n]; });
   State s;
   s.p = p;
@@ -260,7 +274,7 @@ double fromprims(const OCase &c, const double *q, double *Q) {
 // series/parallel conductivity (simulator/mixture/transport/kernels/mixing.mako:3-10),
 // Lewis diffusivities (simulator/mixture/diffusion/kernels/lewis.mako:3-8) and
 // the species enthalpies (simulator/mixture/eos/kernels/species.mako:9-36)
-void transport(const OCase &c, const double *Q, const State &st, double *tr, double *hsp) {
+void transport(const OCase &c, const double *Q, const State &st, double *tr, double *hsp, double Z = 0.0) {
   const int ns = c.ns;
   const double rho = Q[0], rhoinv = 1.0 / rho;
   double Ylast = 1.0;
@@ -315,6 +329,10 @@ void transport(const OCase &c, const double *Q, const State &st, double *tr, dou
   tr[1] = kappa;
   const double kor = kappa * rhoinv / st.cp;
   for (int n = 0; n < ns; n++) tr[2 + n] = kor / c.lewis[n];
+  if (c.realgas) {
+    rhspecies(c, hsp, [&](int n) { return Q[5 + n] * rhoinv; }, st.p, T, Z);
+    return;
+  }
   const double u = std::log(T), Tinv = 1.0 / T;
   for (int n = 0; n < ns; n++) {
     double hRT = 0.0;
@@ -534,6 +552,426 @@ void cellrates(const OCase &c, const double *Q, double T, double *omega) {
   RateState s;
   ratestate(c, s, Q[0], Y, T);
   production(c, s, omega);
+}
+
+// ---- the cubic real gas (simulator/mixture/eos/realgas/kernels/eos.mako,
+// realgas/kernels/newton.mako) and its double flux
+// (simulator/mixture/eos/realgasdf/kernels/eos.mako, simulator/eulerdf/kernels/) ----
+struct Cubic {
+  double MWmix, bm, cm, S1, S2, am, dam, Astar, Bstar, Cstar, invRuT, Z, z1, z2, invslope, dZdT, v, I, logratio, q, qd;
+};
+struct RMom {
+  double R, h298, b, c, da;
+  Mom ideal;  // cp's coefficients and h298, for ideal_cph
+};
+
+template <class YF> RMom rmixmom(const OCase &c, YF Y) {
+  RMom m{};
+  m.ideal = mixmom(c, Y);
+  m.R = m.ideal.R, m.h298 = m.ideal.h298;
+  double Ylast = 1.0;
+  for (int n = 0; n < c.ns - 1; n++) {
+    const double Yn = Y(n);
+    Ylast -= Yn;
+    m.b += Yn * c.cbMW[n];
+    m.c += Yn * c.vshiftMW[n];
+    m.da += Yn * c.cdaMW[n];
+  }
+  const int L = c.ns - 1;
+  m.b += Ylast * c.cbMW[L];
+  m.c += Ylast * c.vshiftMW[L];
+  m.da += Ylast * c.cdaMW[L];
+  return m;
+}
+
+void cubicmix(const OCase &c, Cubic &q, const RMom &m) {
+  q.MWmix = c.Ru / m.R;
+  q.bm = m.b * q.MWmix;
+  q.cm = m.c * q.MWmix;
+  q.S2 = m.da * q.MWmix;
+}
+
+// sqrt(a_n), whole or per unit of Y_n / MW_n, Soave's modulus opened (eos.mako:5-8)
+double sqrtaMW(const OCase &c, int n, double sqrtT) {
+  return c.csqrtacMW[n] * std::fabs(std::fma(-sqrtT, c.cmTc[n], c.conepm[n]));
+}
+double sqrta(const OCase &c, int n, double sqrtT) {
+  return c.csqrtac[n] * std::fabs(std::fma(-sqrtT, c.cmTc[n], c.conepm[n]));
+}
+
+template <class YF> void attraction(const OCase &c, Cubic &q, YF Y, double T) {
+  const double sqrtT = std::sqrt(T);
+  double s1 = 0.0, Ylast = 1.0;
+  for (int n = 0; n < c.ns - 1; n++) {
+    const double Yn = Y(n);
+    Ylast -= Yn;
+    s1 = std::fma(Yn, sqrtaMW(c, n, sqrtT), s1);
+  }
+  s1 = std::fma(Ylast, sqrtaMW(c, c.ns - 1, sqrtT), s1);
+  q.S1 = s1 * q.MWmix;
+  q.am = q.S1 * q.S1;
+  q.dam = -q.S1 * q.S2 / sqrtT;
+}
+
+void dimless(const OCase &c, Cubic &q, double p, double T) {
+  q.invRuT = 1.0 / (c.Ru * T);
+  const double pRT = p * q.invRuT;
+  q.Astar = q.am * pRT * q.invRuT;
+  q.Bstar = q.bm * pRT;
+  q.Cstar = q.cm * pRT;
+  const double B = q.Bstar, B2 = B * B;
+  q.z1 = q.Astar + c.cw * B2 - c.cu * B - c.cu * B2;
+  q.z2 = -(1.0 + B - c.cu * B);
+}
+
+void rootslope(Cubic &q) { q.invslope = 1.0 / (3.0 * q.Z * q.Z + 2.0 * q.Z * q.z2 + q.z1); }
+
+void zsolve(const OCase &c, Cubic &q, double p, double T) {
+  dimless(c, q, p, T);
+  const double B = q.Bstar, B2 = B * B, z1 = q.z1, z2 = q.z2;
+  const double z0 = -(q.Astar * B + c.cw * B2 * (1.0 + B));
+  const double Q = (z2 * z2 - 3.0 * z1) * (1.0 / 9.0);
+  const double R = (2.0 * z2 * z2 * z2 - 9.0 * z2 * z1 + 27.0 * z0) * (1.0 / 54.0);
+  const double M = R * R - Q * Q * Q;
+  const double z2o3 = z2 * (1.0 / 3.0);
+  if (M > 0.0) {
+    const double S = -std::copysign(std::cbrt(std::fabs(R) + std::sqrt(M)), R);
+    q.Z = S + Q / S - z2o3;
+  } else {
+    const double sqQ = std::sqrt(Q), twopio3 = 2.0943951023931954923;
+    const double theta3 = std::acos(R / (Q * sqQ)) * (1.0 / 3.0);
+    const double roots[3] = {-2.0 * sqQ * std::cos(theta3) - z2o3, -2.0 * sqQ * std::cos(theta3 + twopio3) - z2o3,
+                             -2.0 * sqQ * std::cos(theta3 - twopio3) - z2o3};
+    double Z = std::fmax(roots[0], std::fmax(roots[1], roots[2]));
+    int above = 0;
+    for (int k = 0; k < 3; k++) above += roots[k] > B;
+    if (above > 1) {
+      const double AoBse = q.Astar / (B * (c.csigma - c.ceps));
+      double gmin = 0.0;
+      bool found = false;
+      for (int k = 0; k < 3; k++) {
+        const double z = roots[k];
+        if (z <= B) continue;
+        const double g = z - 1.0 - std::log(z - B) + AoBse * std::log((z + c.ceps * B) / (z + c.csigma * B));
+        if (!found || g < gmin) gmin = g, Z = z, found = true;
+      }
+    }
+    q.Z = Z;
+  }
+  rootslope(q);
+}
+
+double dZ(const OCase &c, const Cubic &q, double dA, double dB) {
+  const double B = q.Bstar, Z = q.Z, Z2 = Z * Z;
+  const double dz0 = -(B * dA + (q.Astar + (2.0 * B + 3.0 * B * B) * c.cw) * dB);
+  const double dz1 = dA + (2.0 * B * (c.cw - c.cu) - c.cu) * dB;
+  const double dz2 = -(1.0 - c.cu) * dB;
+  return -(dz2 * Z2 + dz1 * Z + dz0) * q.invslope;
+}
+
+void departures(const OCase &c, double &hdep, double &cpdep, Cubic &q, double T) {
+  const double Tinv = c.Ru * q.invRuT;
+  const double dlnamdT = q.dam / q.am;
+  q.dZdT = dZ(c, q, -2.0 * q.Astar * Tinv * (1.0 - 0.5 * T * dlnamdT), -q.Bstar * Tinv);
+  const double x = q.Z / q.Bstar, xm1 = x - 1.0;
+  const double D = x * x + c.cu * x + c.cw;
+  q.logratio = std::log((x + c.ceps) / (x + c.csigma));
+  const double invBmRu = 1.0 / (q.bm * c.Ru);
+  const double hres = invBmRu / (c.csigma - c.ceps) * (q.am * Tinv - q.dam) * q.logratio;
+  q.qd = q.dam * invBmRu;
+  q.q = q.am * invBmRu * Tinv;
+  const double num = D - q.qd * xm1;
+  cpdep = hres * 0.5 * T * dlnamdT + num * num / (D * D - q.q * (2.0 * x + c.cu) * xm1 * xm1) - 1.0;
+  hdep = hres + (q.Z - 1.0) - q.Cstar;
+}
+
+void gamma_c(const OCase &c, double &gamma, double &cs, const Cubic &q, double p, double T, double rho, double cp,
+             double invZt) {
+  const double invp = 1.0 / p, Tinv = c.Ru * q.invRuT;
+  const double dZtdT = q.dZdT + q.Cstar * Tinv;
+  const double dZdp = dZ(c, q, q.Astar * invp, q.Bstar * invp);
+  const double dZtdp = dZdp - q.Cstar * invp;
+  const double drhodp = rho * invp * (1.0 - p * dZtdp * invZt);
+  const double r = -Tinv * (1.0 + T * dZtdT * invZt);
+  const double csq = 1.0 / (drhodp - (T / cp) * r * r);
+  gamma = drhodp * csq;
+  cs = std::sqrt(std::fabs(csq));
+}
+
+// frompT (eos.mako:139-155); Z out
+template <class YF> State rfrompT(const OCase &c, double p, double T, YF Y, double &Zout) {
+  const RMom m = rmixmom(c, Y);
+  Cubic q{};
+  cubicmix(c, q, m);
+  attraction(c, q, Y, T);
+  double cpi, hi;
+  ideal_cph(c, m.ideal, T, cpi, hi);
+  zsolve(c, q, p, T);
+  double hdep, cpdep;
+  departures(c, hdep, cpdep, q, T);
+  State s;
+  s.p = p;
+  s.T = T;
+  Zout = q.Z;
+  s.cp = cpi + m.R * cpdep;
+  const double Zt = q.Z - q.Cstar, invZt = 1.0 / Zt, porho = Zt * m.R * T;
+  s.rho = p * q.invRuT * q.MWmix * invZt;
+  s.rhoinv = 1.0 / s.rho;
+  s.e = hi + m.R * T * hdep - porho;
+  gamma_c(c, s.gamma, s.c, q, p, T, s.rho, s.cp, invZt);
+  return s;
+}
+
+void atvolume(const OCase &c, Cubic &q, double rho) {
+  q.v = q.MWmix / rho + q.cm;
+  q.I = std::log((q.v + c.csigma * q.bm) / (q.v + c.ceps * q.bm)) / ((c.csigma - c.ceps) * q.bm);
+}
+
+// fromrhoE (eos.mako:162-190, realgas/kernels/newton.mako:3-14)
+template <class YF> State rfromrhoE(const OCase &c, YF Y, double rho, double e, double Tguess, double &Zout) {
+  const RMom m = rmixmom(c, Y);
+  Cubic q{};
+  cubicmix(c, q, m);
+  atvolume(c, q, rho);
+  const double invMWmix = 1.0 / q.MWmix;
+  double T = (Tguess < 1.0) ? 300.0 : Tguess;
+  double cpi = 0.0, hi = 0.0;
+  const double tol = 1e5 * DBL_EPSILON;
+  for (int k = 0; k < 12; k++) {
+    attraction(c, q, Y, T);
+    ideal_cph(c, m.ideal, T, cpi, hi);
+    const double app = 0.5 * (q.S2 * q.S2 - q.dam) / T;
+    const double f = hi - m.R * T - (q.am - T * q.dam) * q.I * invMWmix - e;
+    const double cv = cpi - m.R + T * app * q.I * invMWmix;
+    const double dT = f / cv;
+    T -= dT;
+    if (k >= 2 && std::fabs(dT) <= tol * T) break;
+  }
+  attraction(c, q, Y, T);
+  ideal_cph(c, m.ideal, T, cpi, hi);
+  const double vs = q.v + c.csigma * q.bm, ve = q.v + c.ceps * q.bm;
+  const double p = c.Ru * T / (q.v - q.bm) - q.am / (vs * ve);
+  dimless(c, q, p, T);
+  q.Z = p * q.invRuT * q.v;
+  rootslope(q);
+  double hdep, cpdep;
+  departures(c, hdep, cpdep, q, T);
+  State s;
+  s.rho = rho;
+  s.rhoinv = 1.0 / rho;
+  s.e = e;
+  s.p = p;
+  s.T = T;
+  Zout = q.Z;
+  s.cp = cpi + m.R * cpdep;
+  const double invZt = 1.0 / (q.Z - q.Cstar);
+  gamma_c(c, s.gamma, s.c, q, p, T, rho, s.cp, invZt);
+  return s;
+}
+
+// fromrhop (realgasdf/kernels/eos.mako:6-30, realgasdf/kernels/newton.mako:3-13)
+template <class YF> State rfromrhop(const OCase &c, YF Y, double rho, double p, double Tguess, double &Zout) {
+  const RMom m = rmixmom(c, Y);
+  Cubic q{};
+  cubicmix(c, q, m);
+  atvolume(c, q, rho);
+  const double vs = q.v + c.csigma * q.bm, ve = q.v + c.ceps * q.bm;
+  const double invvmb = 1.0 / (q.v - q.bm), invD = 1.0 / (vs * ve);
+  double T = (Tguess < 1.0) ? 300.0 : Tguess;
+  const double tol = 1e5 * DBL_EPSILON;
+  for (int k = 0; k < 12; k++) {
+    attraction(c, q, Y, T);
+    const double f = c.Ru * T * invvmb - q.am * invD - p;
+    const double dpdT = c.Ru * invvmb - q.dam * invD;
+    const double dT = f / dpdT;
+    T -= dT;
+    if (k >= 2 && std::fabs(dT) <= tol * T) break;
+  }
+  attraction(c, q, Y, T);
+  double cpi, hi;
+  ideal_cph(c, m.ideal, T, cpi, hi);
+  dimless(c, q, p, T);
+  q.Z = p * q.invRuT * q.v;
+  rootslope(q);
+  double hdep, cpdep;
+  departures(c, hdep, cpdep, q, T);
+  State s;
+  s.rho = rho;
+  s.rhoinv = 1.0 / rho;
+  s.p = p;
+  s.T = T;
+  Zout = q.Z;
+  s.cp = cpi + m.R * cpdep;
+  s.e = hi + m.R * T * hdep - p / rho;
+  const double invZt = 1.0 / (q.Z - q.Cstar);
+  gamma_c(c, s.gamma, s.c, q, p, T, rho, s.cp, invZt);
+  return s;
+}
+
+// hspecies at a stored state: hpartialpoint and hpartial (eos.mako:192-224, 257-273)
+template <class YF> void rhspecies(const OCase &c, double *h, YF Y, double p, double T, double Z) {
+  const RMom m = rmixmom(c, Y);
+  Cubic q{};
+  cubicmix(c, q, m);
+  attraction(c, q, Y, T);
+  dimless(c, q, p, T);
+  q.Z = Z;
+  rootslope(q);
+  double hdep, cpdep;
+  departures(c, hdep, cpdep, q, T);
+  const double lnT = std::log(T), Tinv = c.Ru * q.invRuT, sqrtT = std::sqrt(T);
+  const double B = q.Bstar, ZT = q.dZdT, BT = -B * Tinv;
+  const double invZsB = 1.0 / (Z + c.csigma * B), invZeB = 1.0 / (Z + c.ceps * B);
+  const double Iz = -q.logratio / (c.csigma - c.ceps);
+  const double IzT = ((ZT + c.csigma * BT) * invZsB - (ZT + c.ceps * BT) * invZeB) / (c.csigma - c.ceps);
+  const double dlnZmB = (ZT - BT) / (Z - B);
+  const double invS1 = 1.0 / q.S1, invBm = 1.0 / q.bm;
+  const double invamsqrtT = invS1 * invS1 / sqrtT;
+  for (int n = 0; n < c.ns; n++) {
+    double hRT = 0.0;
+    for (int t = c.nh - 1; t >= 0; t--) hRT = hRT * lnT + c.hpoly[n * c.nh + t];
+    hRT += c.h298[n] * Tinv;
+    const double qT = (q.qd - q.q) * Tinv;
+    const double sqrtan = sqrta(c, n, sqrtT);
+    const double r = 2.0 * sqrtan * invS1;
+    const double rT = (sqrtan * q.S2 - c.cda[n] * q.S1) * invamsqrtT;
+    const double bb = c.cb[n] * invBm;
+    const double qbar = q.q * (r - bb), qbarT = qT * (r - bb) + q.q * rT;
+    const double dlnphidT = bb * q.dZdT - dlnZmB - qbarT * Iz - qbar * IzT;
+    h[n] = (hRT * T * c.Ru - c.Ru * T * T * dlnphidT - c.vshift[n] * p) * c.MWinv[n];
+  }
+}
+
+// drho (eos.mako:226-255)
+template <class YF>
+void rdrho(const OCase &c, double &rho_p, double &rho_T, double *rho_Y, YF Y, double p, double T, double rho) {
+  const RMom m = rmixmom(c, Y);
+  Cubic q{};
+  cubicmix(c, q, m);
+  attraction(c, q, Y, T);
+  zsolve(c, q, p, T);
+  double hdep, cpdep;
+  departures(c, hdep, cpdep, q, T);
+  const double invp = 1.0 / p, Tinv = c.Ru * q.invRuT, sqrtT = std::sqrt(T);
+  const double Zt = q.Z - q.Cstar, dZtdT = q.dZdT + q.Cstar * Tinv, invZt = 1.0 / Zt;
+  const double dZdp = dZ(c, q, q.Astar * invp, q.Bstar * invp);
+  rho_p = rho * invp * (1.0 - (p * dZdp - q.Cstar) * invZt);
+  rho_T = -rho * Tinv * (1.0 + T * dZtdT * invZt);
+  const double twoS1 = 2.0 * q.S1;
+  const double invRuT = Tinv / c.Ru, pRT = p * invRuT;
+  const int L = c.ns - 1;
+  const double MWinv_last = c.MWinv[L], sqrta_last = sqrtaMW(c, L, sqrtT);
+  const double b_last = c.cbMW[L], c_last = c.vshiftMW[L];
+  for (int n = 0; n < c.ns - 1; n++) {
+    const double dlnMWmix = -q.MWmix * (c.MWinv[n] - MWinv_last);
+    const double dam = twoS1 * (q.S1 * dlnMWmix + q.MWmix * (sqrtaMW(c, n, sqrtT) - sqrta_last));
+    const double dbm = q.bm * dlnMWmix + q.MWmix * (c.cbMW[n] - b_last);
+    const double dcm = q.cm * dlnMWmix + q.MWmix * (c.vshiftMW[n] - c_last);
+    const double dZdY = dZ(c, q, dam * pRT * invRuT, dbm * pRT);
+    rho_Y[n] = rho * (dlnMWmix - (dZdY - dcm * pRT) * invZt);
+  }
+}
+
+// planeslopes (realgasdf/kernels/eos.mako:32-48)
+template <class YF>
+void planeslopes(const OCase &c, double &theta, double &epsY, YF Y, double rho, double rhoinv, double T, double e) {
+  const RMom m = rmixmom(c, Y);
+  Cubic q{};
+  cubicmix(c, q, m);
+  atvolume(c, q, rho);
+  attraction(c, q, Y, T);
+  const double vs = q.v + c.csigma * q.bm, ve = q.v + c.ceps * q.bm;
+  const double invvmb = 1.0 / (q.v - q.bm), invD = 1.0 / (vs * ve), invMWmix = 1.0 / q.MWmix;
+  double cpi, hi;
+  ideal_cph(c, m.ideal, T, cpi, hi);
+  const double app = 0.5 * (q.S2 * q.S2 - q.dam) / T;
+  const double cv = cpi - m.R + T * app * q.I * invMWmix;
+  const double p = c.Ru * T * invvmb - q.am * invD;
+  const double dpdT = c.Ru * invvmb - q.dam * invD;
+  const double dpdrho = q.MWmix * rhoinv * rhoinv * (c.Ru * T * invvmb * invvmb - q.am * (vs + ve) * invD * invD);
+  theta = rho * cv / dpdT;
+  epsY = e - (T * dpdT - p) * rhoinv - theta * dpdrho;
+}
+
+// freeze of one cell: the energy reset to the eos's and the tangent plane
+// (simulator/eulerdf/kernels/freeze.mako:3-32); st is the cell's record
+void freeze(const OCase &c, double *Q, double *st) {
+  const double rho = Q[0], rhoinv = 1.0 / rho;
+  const double p = st[0], T = st[1], e = st[4];
+  const double rhoe = rho * e;
+  Q[4] = rhoe + 0.5 * ((Q[1]) * (Q[1]) + (Q[2]) * (Q[2]) + (Q[3]) * (Q[3])) * rhoinv;
+  auto Y = [&](int n) { return Q[5 + n] * rhoinv; };
+  double theta, epsY;
+  planeslopes(c, theta, epsY, Y, rho, rhoinv, T, e);
+  double rho_p, rho_T, rho_Y[16];
+  rdrho(c, rho_p, rho_T, rho_Y, Y, p, T, rho);
+  double h[16];
+  rhspecies(c, h, Y, p, T, st[S_Z]);
+  const double cpoverrhoT = st[5] / rho_T;
+  double zetaY = 0.0;
+  for (int n = 0; n < c.ns - 1; n++) {
+    st[S_ZETA + n] = h[n] - h[c.ns - 1] - cpoverrhoT * rho_Y[n];
+    zetaY += st[S_ZETA + n] * Y(n);
+  }
+  st[S_THETA] = theta;
+  st[S_EPS] = epsY - zetaY;
+  st[S_KAPPA] = rhoe - epsY * rho - theta * p;
+}
+
+// the state of one cell from Q: the real gas's fromrhoE, or with plane its
+// fromplane, p off the cell's frozen plane (simulator/eulerdf/kernels/fromplane.mako:3-17)
+void rstate(const OCase &c, const double *Q, double *st, double Tguess, bool plane) {
+  const double rho = Q[0], rhoinv = 1.0 / rho;
+  auto Y = [&](int n) { return Q[5 + n] * rhoinv; };
+  double Z = 0.0;
+  State s;
+  if (plane) {
+    double composition = 0.0;
+    for (int n = 0; n < c.ns - 1; n++) composition += st[S_ZETA + n] * Q[5 + n];
+    const double p = (Q[4] - 0.5 * ((Q[1]) * (Q[1]) + (Q[2]) * (Q[2]) + (Q[3]) * (Q[3])) * rhoinv - st[S_EPS] * Q[0] -
+                      composition - st[S_KAPPA]) / st[S_THETA];
+    s = rfromrhop(c, Y, rho, p, Tguess, Z);
+  } else {
+    s = rfromrhoE(c, Y, rho, efromQ(Q, rhoinv), Tguess, Z);
+  }
+  std::memcpy(st, &s, sizeof(State));
+  st[S_Z] = Z;
+}
+
+// the double flux's kepaec with its two energy rows (eulerdf/kernels/flux/function/kepaec.mako:1-21)
+void kepaec_df(const OCase &c, const double *QL, const double *QR, const double *sL, const double *sR,
+               const double *S, double *F) {
+  const int ns = c.ns, ne = 4 + ns;
+  const double uL = QL[1] / QL[0], vL = QL[2] / QL[0], wL = QL[3] / QL[0];
+  const double uR = QR[1] / QR[0], vR = QR[2] / QR[0], wR = QR[3] / QR[0];
+  const double pL = sL[0], pR = sR[0], rL = sL[3], rR = sR[3];
+  const double uf = 0.5 * (uR + uL), vf = 0.5 * (vR + vL), wf = 0.5 * (wR + wL);
+  const double U = (S[0]) * (uf) + (S[1]) * (vf) + (S[2]) * (wf);
+  const double pf = 0.5 * (pR + pL), rho = 0.5 * (rR + rL);
+  const double C = rho * U;
+  F[0] = C;
+  F[1] = C * uf + pf * S[0];
+  F[2] = C * vf + pf * S[1];
+  F[3] = C * wf + pf * S[2];
+  const double Kj = C * 0.5 * ((uR) * (uL) + (vR) * (vL) + (wR) * (wL));
+  const double Pj = 0.5 * (pL * ((uR) * (S[0]) + (vR) * (S[1]) + (wR) * (S[2])) +
+                           pR * ((uL) * (S[0]) + (vL) * (S[1]) + (wL) * (S[2])));
+  double YL[16], YR[16];
+  for (int n = 0; n < ns - 1; n++) {
+    YL[n] = QL[5 + n] / QL[0], YR[n] = QR[5 + n] / QR[0];
+    F[5 + n] = 0.5 * (YR[n] + YL[n]) * C;
+  }
+  const double rhoinvL = 1.0 / rL, rhoinvR = 1.0 / rR;
+  double cL[2] = {0.0, 0.0}, cR[2] = {0.0, 0.0};
+  for (int n = 0; n < ns - 1; n++) {
+    cL[0] += sL[S_ZETA + n] * YL[n], cL[1] += sR[S_ZETA + n] * YL[n];
+    cR[0] += sL[S_ZETA + n] * YR[n], cR[1] += sR[S_ZETA + n] * YR[n];
+  }
+  for (int q = 0; q < 2; q++) {
+    const double *pl = q == 0 ? sL : sR;
+    const double tL = (pl[S_THETA] * pL + pl[S_KAPPA]) * rhoinvL, tR = (pl[S_THETA] * pR + pl[S_KAPPA]) * rhoinvR;
+    F[q == 0 ? 4 : ne] = (pl[S_EPS] + 0.5 * (cL[q] + cR[q]) + 2.0 * tL * tR / (tL + tR)) * C + Kj + Pj;
+  }
 }
 
 // a face's side: the cell's state plus its velocity as Q[1..3] / Q[0]
@@ -872,14 +1310,25 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
                           (k < B.ng || k >= d.Z - B.ng);
           if (out > 1) continue;
           const long at = d.at(i, j, k);
-          State st = fromQ(c, B.Q + at * ne, B.Tg ? B.Tg[at] : 0.0);
+          State st;
+          if (c.realgas) {
+            // the real gas's record: the state, Z and, with the double flux,
+            // the cell's frozen plane kept across stages
+            double *rec = &s.state[at * NSTATE];
+            if (c.df) std::memcpy(rec, B.pst + at * NSTATE, sizeof(double) * NSTATE);
+            rstate(c, B.Q + at * ne, rec, B.Tg ? B.Tg[at] : 0.0, c.df != 0);
+            std::memcpy(&st, rec, sizeof(State));
+            if (c.df) std::memcpy(B.pst + at * NSTATE, rec, sizeof(double) * NSTATE);
+          } else {
+            st = fromQ(c, B.Q + at * ne, B.Tg ? B.Tg[at] : 0.0);
+            std::memcpy(&s.state[at * NSTATE], &st, sizeof(State));
+          }
           if (B.Tg) B.Tg[at] = st.T;
-          std::memcpy(&s.state[at * NSTATE], &st, sizeof(State));
           if (visc) {
             // the shallow range: interior plus one halo layer
             const int deep = (i < B.ng - 1 || i > d.X - B.ng) + (j < B.ng - 1 || j > d.Y - B.ng) +
                              (k < B.ng - 1 || k > d.Z - B.ng);
-            if (!deep) transport(c, B.Q + at * ne, st, &s.tr[at * (2 + ns)], &s.hsp[at * ns]);
+            if (!deep) transport(c, B.Q + at * ne, st, &s.tr[at * (2 + ns)], &s.hsp[at * ns], s.state[at * NSTATE + S_Z]);
           }
         }
     if (visc) {
@@ -928,9 +1377,11 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
     const Dims d = cells(B);
     Scratch &s = scr[b];
     const int g = B.ng;
+    // the double flux writes its energy row twice: one row more per face
+    const int nf = ne + (c.df ? 1 : 0);
     for (int a = 0; a < 3; a++) {
       const Dims f = face_dims(B, a);
-      s.F[a].assign((long)f.X * f.Y * f.Z * ne, 0.0);
+      s.F[a].assign((long)f.X * f.Y * f.Z * nf, 0.0);
       const int hi[3] = {B.nx + (a == 0), B.ny + (a == 1), B.nz + (a == 2)};
       // the interior faces of axis a: a face is indexed like the cell to its right
       // (peregrine/launch/policy.py:78-86)
@@ -948,9 +1399,11 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
             const State &sR = *reinterpret_cast<const State *>(&s.state[R * NSTATE]);
             const State &sLL = *reinterpret_cast<const State *>(&s.state[LL * NSTATE]);
             const State &sRR = *reinterpret_cast<const State *>(&s.state[RR * NSTATE]);
-            double *F = &s.F[a][at * ne];
+            double *F = &s.F[a][at * nf];
             const double *S = B.S[a] + at * 3;
-            if (!c.skip_adv)
+            if (c.df)
+              kepaec_df(c, QL, QR, &s.state[L * NSTATE], &s.state[R * NSTATE], S, F);
+            else if (!c.skip_adv)
               advective(c, B.Q + LL * ne, QL, QR, B.Q + RR * ne, sLL, sL, sR, sRR, S, F);
             if (visc)
               alphadamping(c, S, B.xf[a] + at * 3, B.xcc + L * 3, B.xcc + R * 3, QL, QR, sL, sR,
@@ -965,12 +1418,20 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
     for (int i = g; i < g + B.nx; i++)
       for (int j = g; j < g + B.ny; j++)
         for (int k = g; k < g + B.nz; k++) {
-          const double *iFl = &s.F[0][fi.at(i, j, k) * ne], *iFh = &s.F[0][fi.at(i + 1, j, k) * ne];
-          const double *jFl = &s.F[1][fj.at(i, j, k) * ne], *jFh = &s.F[1][fj.at(i, j + 1, k) * ne];
-          const double *kFl = &s.F[2][fk.at(i, j, k) * ne], *kFh = &s.F[2][fk.at(i, j, k + 1) * ne];
+          const double *iFl = &s.F[0][fi.at(i, j, k) * nf], *iFh = &s.F[0][fi.at(i + 1, j, k) * nf];
+          const double *jFl = &s.F[1][fj.at(i, j, k) * nf], *jFh = &s.F[1][fj.at(i, j + 1, k) * nf];
+          const double *kFl = &s.F[2][fk.at(i, j, k) * nf], *kFh = &s.F[2][fk.at(i, j, k + 1) * nf];
           const long at = d.at(i, j, k);
           const double detJinv = B.detJinv[at];
-          if (c.mech) {
+          if (c.df) {
+            // the cell's own energy row: F[ne] on its low faces, where it is the
+            // right cell, F[4] on its high faces (simulator/eulerdf/kernels/applyflux.mako:2-14)
+            for (int l = 0; l < ne; l++) {
+              if (l == 4) continue;
+              dQ[b][at * ne + l] = (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
+            }
+            dQ[b][at * ne + 4] = (iFl[ne] + jFl[ne] + kFl[ne] - iFh[4] - jFh[4] - kFh[4]) * detJinv;
+          } else if (c.mech) {
             // coupled chemistry begins dQ with the carried species' production
             // rates, the fluxes add to it (simulator/chemint/kernels/source.mako:3-10,
             // cell.mako:14-19, applyflux.mako with append)
@@ -986,6 +1447,67 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
           }
         }
   }
+  return 0;
+}
+
+// The double flux's step start on register Q: each interior cell's state
+// (the real gas's fromrhoE when first, else off its frozen plane), its plane
+// frozen anew with the energy reset to the eos's, then Q, the kept records
+// and the starting guesses copied into every halo layer, so a halo's plane is
+// its image's (simulator/eulerdf/simulator.py:58-66, freeze.mako:3-32)
+int oracle_prestep(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *map, long nmap, int first) {
+  const OCase &c = *cp;
+  const int ne = 4 + c.ns;
+  for (int b = 0; b < nblocks; b++) {
+    OBlock &B = blocks[b];
+    const Dims d = cells(B);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int i = B.ng; i < d.X - B.ng; i++)
+      for (int j = B.ng; j < d.Y - B.ng; j++)
+        for (int k = B.ng; k < d.Z - B.ng; k++) {
+          const long at = d.at(i, j, k);
+          double *rec = B.pst + at * NSTATE;
+          rstate(c, B.Q + at * ne, rec, B.Tg[at], !first);
+          B.Tg[at] = rec[1];
+          freeze(c, B.Q + at * ne, rec);
+        }
+  }
+  for (long m = 0; m < nmap; m++) {
+    const OHaloEntry &h = map[m];
+    OBlock &D = blocks[h.dblk];
+    OBlock &S = blocks[h.sblk];
+    const long dt = cells(D).at(h.di, h.dj, h.dk), st = cells(S).at(h.si, h.sj, h.sk);
+    std::memcpy(D.Q + dt * ne, S.Q + st * ne, sizeof(double) * ne);
+    std::memcpy(D.pst + dt * NSTATE, S.pst + st * NSTATE, sizeof(double) * NSTATE);
+    D.Tg[dt] = S.Tg[st];
+  }
+  return 0;
+}
+
+// the real gas's state at n (p, T, Y of the carried species) points by
+// frompT, records [n][NSTATE] (Z at S_Z)
+int oracle_realgas_frompT(const OCase *cp, long n, const double *p, const double *T, const double *Y, double *rec) {
+  const int ns = cp->ns;
+  for (long q = 0; q < n; q++) {
+    double Z;
+    const State s = rfrompT(*cp, p[q], T[q], [&](int k) { return Y[q * (ns - 1) + k]; }, Z);
+    std::memcpy(rec + q * NSTATE, &s, sizeof(State));
+    rec[q * NSTATE + S_Z] = Z;
+  }
+  return 0;
+}
+
+// the real gas's state at n (Q, T guess) by fromrhoE, records [n][NSTATE]
+int oracle_realgas_fromQ(const OCase *cp, long n, const double *Q, const double *Tg, double *rec) {
+  const int ne = 4 + cp->ns;
+  for (long q = 0; q < n; q++) rstate(*cp, Q + q * ne, rec + q * NSTATE, Tg[q], false);
+  return 0;
+}
+
+// freeze at n cells (Q rows, records from the eos): Q's energy and the planes in place
+int oracle_freeze(const OCase *cp, long n, double *Q, double *rec) {
+  const int ne = 4 + cp->ns;
+  for (long q = 0; q < n; q++) freeze(*cp, Q + q * ne, rec + q * NSTATE);
   return 0;
 }
 
@@ -1084,7 +1606,7 @@ int oracle_fromQ(const OCase *cp, long n, const double *Q, const double *Tguess,
   const int ne = 4 + cp->ns;
   for (long q = 0; q < n; q++) {
     const State st = fromQ(*cp, Q + q * ne, Tguess[q]);
-    std::memcpy(state + q * NSTATE, &st, sizeof st);
+    std::memcpy(state + q * 8, &st, sizeof st);
   }
   return 0;
 }

@@ -84,9 +84,9 @@ _DEFAULTS = {
     "halo-exchange": {"kind": "device"},
 }
 
-SIMULATORS = ("euler", "navier-stokes")
+SIMULATORS = ("euler", "navier-stokes", "euler-df")
 INTEGRATORS = ("rk1", "rk2", "tvd-rk3", "rk34", "rk4")
-EOSES = ("cpg", "tpg")
+EOSES = ("cpg", "tpg", "real-gas", "real-gas-df")
 TRANS = (None, "constant", "kinetic-theory")
 PRIMARIES = ("kepaec", "hllc", "rusanov", "ausmup")
 RECONS = ("constant", "muscl")
@@ -144,6 +144,9 @@ class Config(dict):
             raise ConfigError("adv-flux.recon", "kepaec takes the constant reconstruction only")
         if sim["simulator"] == "navier-stokes" and self["mixture"]["trans"] is None:
             raise ConfigError("mixture.trans", "a viscous case names a transport model")
+        # the double flux freezes the real gas's tangent plane (peregrine/simulator/eulerdf/simulator.py:15-20)
+        if (sim["simulator"] == "euler-df") != (self["mixture"]["eos"] == "real-gas-df"):
+            raise ConfigError("mixture.eos", "euler-df takes real-gas-df, and that eos euler-df")
         if self["diff-flux"]["formula"] != "alpha-damping":
             raise ConfigError("diff-flux.formula", "only 'alpha-damping' is built")
         if self["mixture"]["chemistry"] not in (None, "finite-rate"):

@@ -217,7 +217,7 @@ __global__ void k_source(const BlockDev *__restrict__ blks, int b, const double 
   const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
   const long long c = cell_index(B, i, j, k), v = B.vol;
   const double *Q = Qall + NE * B.cv + c;
-  const double T = stall[8 * B.cv + 1 * v + c];
+  const double T = stall[SW * B.cv + 1 * v + c];
   double omega[NS];
   cellrates<NS>([&](int l) { return Q[l * v]; }, T, omega);
   double *dQ = dQall + NE * B.cv + c;

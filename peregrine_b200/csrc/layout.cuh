@@ -44,6 +44,14 @@ __host__ __device__ __forceinline__ long long cell_index(const BlockDev &b, int 
   return (long long)fi + (long long)b.X * ((long long)fj + (long long)b.Y * fk);
 }
 
+// The per-cell state of the per-block path, fields of one cell SW apart in
+// vol-strided planes: the EosState (p, T, rhoinv, rho, e, cp, gamma, c), the
+// real gas's root Z, and the double flux's tangent plane of rho e
+// (theta, eps, kappa, zeta[ns - 1]) (peregrine/simulator/mixture/eos/base.py:85-86,
+// realgas/model.py:31-34, realgasdf/model.py:8-10)
+constexpr int SW = 24;
+enum { ST_Z = 8, ST_THETA = 9, ST_EPS = 10, ST_KAPPA = 11, ST_ZETA = 12 };
+
 // Where a per-block kernel's thread works: its block and its index t in the
 // pass's range over that block.  With a tile table (a packed launch over many
 // blocks), CTA x does tile ctab[x].y of block row ctab[x].x, so a launch has

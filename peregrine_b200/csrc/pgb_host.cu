@@ -35,7 +35,8 @@ PGB_PLAIN_DECL(11)
 PGB_PLAIN_DECL(12)
 
 namespace {
-#define PGB_OPS(N) {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N}
+#define PGB_OPS(N) \
+  {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N, pgb_plain_prestep_##N}
 // the per-block path of each species count, 1 to MAXNS
 const PlainOps kPlain[MAXNS] = {PGB_OPS(1), PGB_OPS(2), PGB_OPS(3), PGB_OPS(4),  PGB_OPS(5),  PGB_OPS(6),
                                 PGB_OPS(7), PGB_OPS(8), PGB_OPS(9), PGB_OPS(10), PGB_OPS(11), PGB_OPS(12)};
@@ -138,6 +139,7 @@ struct pgb_case {
   std::unique_ptr<Mech> mech;
   unsigned long long uid = 0;  // unique over the process, never reused
   unsigned version = 0;        // bumped when the species or mechanism tables change
+  bool df_fresh = true;        // the double flux has no frozen planes for the state yet
 };
 
 namespace {
@@ -180,10 +182,36 @@ int build_species(pgb_case *c) {
     fit_fill(dst, terms, it->second.data(), ns, (int)(n / ns));
     return PGB_OK;
   };
-  if (c->phys.eos == PGB_EOS_TPG) {
+  if (c->phys.eos != PGB_EOS_CPG) {
     c->sp.tpg = 1;
     RET(fit("cppolyR", c->sp.cppolyR, c->sp.ncp));
     RET(fit("hpoly", c->sp.hpoly, c->sp.nh));
+  }
+  if (c->phys.eos == PGB_EOS_REALGAS || c->phys.eos == PGB_EOS_REALGAS_DF) {
+    c->sp.realgas = 1;
+    c->sp.df = c->phys.eos == PGB_EOS_REALGAS_DF;
+    struct {
+      const char *name;
+      double *dst;
+    } one[] = {{"cubicu", &c->sp.cu}, {"cubicw", &c->sp.cw}, {"cubicsigma", &c->sp.csigma}, {"cubiceps", &c->sp.ceps}};
+    for (auto &t : one) {
+      const double *v = table(c, t.name);
+      if (!v) return fail(PGB_ERR_ARG, std::string("real-gas table ") + t.name + " not set");
+      *t.dst = v[0];
+    }
+    struct {
+      const char *name;
+      double *dst;
+    } per[] = {{"cubicsqrtac", c->sp.csqrtac}, {"cubicb", c->sp.cb}, {"cubicda", c->sp.cda},
+               {"cubicmTc", c->sp.cmTc}, {"cubiconepm", c->sp.conepm}, {"vshift", c->sp.vshift},
+               {"cubicsqrtacMW", c->sp.csqrtacMW}, {"cubicbMW", c->sp.cbMW}, {"cubicdaMW", c->sp.cdaMW},
+               {"vshiftMW", c->sp.vshiftMW}};
+    for (auto &t : per) {
+      auto it = c->tables.find(t.name);
+      if (it == c->tables.end() || (long)it->second.size() < ns)
+        return fail(PGB_ERR_ARG, std::string("real-gas table ") + t.name + " not set or short");
+      for (int n = 0; n < ns; n++) t.dst[n] = it->second[n];
+    }
   }
   if (c->phys.trans == PGB_TRANS_KINETIC) {
     c->sp.kinetic = 1;
@@ -719,8 +747,8 @@ int step_fused(pgb_case *c, int &count) {
 int ensure_state(pgb_case *c) {
   if (c->d_state) return PGB_OK;
   const size_t n = (size_t)c->cells;
-  CK(cudaMalloc(&c->d_state, sizeof(double) * 8 * n));
-  CK(cudaMemsetAsync(c->d_state, 0, sizeof(double) * 8 * n, c->stream));
+  CK(cudaMalloc(&c->d_state, sizeof(double) * SW * n));
+  CK(cudaMemsetAsync(c->d_state, 0, sizeof(double) * SW * n, c->stream));
   return PGB_OK;
 }
 
@@ -732,11 +760,13 @@ int ensure_scratch(pgb_case *c) {
   CK(cudaMalloc(&c->d_tr, sizeof(double) * (2 + ns) * n));
   CK(cudaMalloc(&c->d_hsp, sizeof(double) * ns * n));
   CK(cudaMalloc(&c->d_grads, sizeof(double) * 3 * ngrad * n));
-  for (int a = 0; a < 3; a++) CK(cudaMalloc(&c->d_F[a], sizeof(double) * ne * n));
+  // the double flux writes its energy row twice: one row more per face
+  const int nf = ne + (c->phys.simulator == PGB_EULER_DF);
+  for (int a = 0; a < 3; a++) CK(cudaMalloc(&c->d_F[a], sizeof(double) * nf * n));
   CK(cudaMemsetAsync(c->d_tr, 0, sizeof(double) * (2 + ns) * n, c->stream));
   CK(cudaMemsetAsync(c->d_hsp, 0, sizeof(double) * ns * n, c->stream));
   CK(cudaMemsetAsync(c->d_grads, 0, sizeof(double) * 3 * ngrad * n, c->stream));
-  for (int a = 0; a < 3; a++) CK(cudaMemsetAsync(c->d_F[a], 0, sizeof(double) * ne * n, c->stream));
+  for (int a = 0; a < 3; a++) CK(cudaMemsetAsync(c->d_F[a], 0, sizeof(double) * nf * n, c->stream));
   return PGB_OK;
 }
 
@@ -765,8 +795,23 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.visc = c->phys.simulator == PGB_NAVIER_STOKES;
   pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
   pc.chem = c->phys.chemistry == PGB_CHEM_COUPLED;
+  pc.df = c->phys.simulator == PGB_EULER_DF;
   pc.stream = c->stream;
   return pc;
+}
+
+// the double flux's step start (freeze) on register qphys
+int prestep_plain(pgb_case *c, int qphys, int &count) {
+  if (c->phys.simulator != PGB_EULER_DF) return PGB_OK;
+  RET(ensure_scratch(c));
+  std::vector<BlockDev> hb;
+  PlainCase pc = plain_case(c, hb);
+  MarkCtx mc{c, &count};
+  pc.mark = mark_cb;
+  pc.ctx = &mc;
+  RET(kPlain[c->phys.ns - 1].prestep(&pc, c->d_reg[qphys], c->df_fresh ? 1 : 0));
+  c->df_fresh = false;
+  return PGB_OK;
 }
 
 int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
@@ -782,6 +827,7 @@ int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
 int step_plain(pgb_case *c, int &count) {
   const int TH = 256;
   const auto &map = c->phys_of;
+  if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count));
   for (const pgb_stage &st : c->stages) {
     RET(rhs_plain(c, map[st.q], map[st.dq], count));
     for (int m = 0; m < st.ncombine; m++) {
@@ -869,8 +915,14 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
   if (!phys || !out) return fail(PGB_ERR_ARG, "null argument");
   if (phys->ns < 1 || phys->ns > MAXNS) return fail(PGB_ERR_ARG, "ns out of range");
   if (phys->nregs < 2 || phys->nregs > MAXREGS) return fail(PGB_ERR_ARG, "nregs out of range");
-  if (phys->eos != PGB_EOS_CPG && phys->eos != PGB_EOS_TPG)
-    return fail(PGB_ERR_UNSUPPORTED, "this build has the calorically and thermally perfect gases");
+  if (phys->eos < PGB_EOS_CPG || phys->eos > PGB_EOS_REALGAS_DF)
+    return fail(PGB_ERR_UNSUPPORTED, "no such eos");
+  if (phys->simulator < PGB_EULER || phys->simulator > PGB_EULER_DF) return fail(PGB_ERR_ARG, "no such simulator");
+  if ((phys->simulator == PGB_EULER_DF) != (phys->eos == PGB_EOS_REALGAS_DF))
+    return fail(PGB_ERR_ARG, "euler-df freezes the real gas's tangent plane: it takes real-gas-df, and that eos it");
+  if (phys->simulator == PGB_EULER_DF &&
+      (phys->primary != PGB_FLUX_KEPAEC || phys->recon != PGB_RECON_CONSTANT || phys->chemistry != PGB_CHEM_NONE))
+    return fail(PGB_ERR_UNSUPPORTED, "the double flux takes kepaec on the cells as they are, without chemistry");
   if (phys->primary < PGB_FLUX_KEPAEC || phys->primary > PGB_FLUX_AUSMUP)
     return fail(PGB_ERR_ARG, "no such flux function");
   if (phys->recon != PGB_RECON_CONSTANT && phys->recon != PGB_RECON_MUSCL)
@@ -881,12 +933,12 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
     return fail(PGB_ERR_UNSUPPORTED, "kepaec is a two-point flux of the cells as they are; it takes no muscl sides");
   if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT && phys->trans != PGB_TRANS_KINETIC)
     return fail(PGB_ERR_UNSUPPORTED, "the viscous path takes constant or kinetic-theory transport");
-  if (phys->trans == PGB_TRANS_KINETIC && phys->eos != PGB_EOS_TPG)
-    return fail(PGB_ERR_ARG, "kinetic-theory transport needs the thermally perfect gas");
+  if (phys->trans == PGB_TRANS_KINETIC && phys->eos == PGB_EOS_CPG)
+    return fail(PGB_ERR_ARG, "kinetic-theory transport needs the thermally perfect caloric");
   if (phys->chemistry != PGB_CHEM_NONE && phys->chemistry != PGB_CHEM_COUPLED)
     return fail(PGB_ERR_UNSUPPORTED, "the chemistry takes none or coupled");
   if (phys->chemistry == PGB_CHEM_COUPLED && phys->eos != PGB_EOS_TPG)
-    return fail(PGB_ERR_ARG, "finite-rate chemistry needs the thermally perfect gas");
+    return fail(PGB_ERR_UNSUPPORTED, "finite-rate chemistry takes the thermally perfect gas in this build");
   auto c = std::make_unique<pgb_case>();
   c->uid = ++g_next_uid;
   c->phys = *phys;
@@ -1223,7 +1275,8 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
   const PlainCase pc = plain_case(c, hb);
   RET(kPlain[c->phys.ns - 1].fromprims(&pc, blk, c->d_prims, c->d_reg[c->phys_of[reg]]));
   // a halo cell's first Newton starts from the stored T of the cell it copies
-  if (c->nhalo) k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_state, c->d_halo, c->nhalo, 8);
+  if (c->nhalo) k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_state, c->d_halo, c->nhalo, SW);
+  c->df_fresh = true;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
@@ -1235,6 +1288,8 @@ int pgb_rhs(pgb_case *c, int q, int dq) {
   if (q < 0 || q >= c->phys.nregs || dq < 0 || dq >= c->phys.nregs || q == dq)
     return fail(PGB_ERR_ARG, "bad registers");
   int count = 0;
+  // the double flux's planes, frozen once after the state was set
+  if (c->df_fresh) RET(prestep_plain(c, c->phys_of[q], count));
   RET(rhs_plain(c, c->phys_of[q], c->phys_of[dq], count));
   return PGB_OK;
 }
@@ -1704,6 +1759,7 @@ extern "C" {
 int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, pgb_pool **out) {
   if (!proto || !out) return fail(PGB_ERR_ARG, "null argument");
   if (!proto->finalized) return fail(PGB_ERR_STATE, "finalize the prototype case first");
+  if (proto->phys.simulator == PGB_EULER_DF) return fail(PGB_ERR_UNSUPPORTED, "the pool does not take the double flux");
   if (max_cells < 64 || max_blocks < 1 || max_blocks > 65535)
     return fail(PGB_ERR_ARG, "a pool holds at least 64 cells and 1 to 65535 blocks");
   auto p = std::make_unique<pgb_pool>();
@@ -1724,7 +1780,7 @@ int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, 
   CK(cudaEventCreate(&p->ev1));
   for (int r = 0; r < p->phys.nregs; r++) CK(cudaMalloc(&p->d_reg[r], sizeof(double) * ne * n));
   CK(cudaMalloc(&p->d_met, sizeof(double) * M_NCOMP * n));
-  CK(cudaMalloc(&p->d_state, sizeof(double) * 8 * n));
+  CK(cudaMalloc(&p->d_state, sizeof(double) * SW * n));
   CK(cudaMalloc(&p->d_tr, sizeof(double) * (2 + ns) * n));
   CK(cudaMalloc(&p->d_hsp, sizeof(double) * ns * n));
   CK(cudaMalloc(&p->d_grads, sizeof(double) * 3 * (ne - 1) * n));
@@ -1784,7 +1840,7 @@ int pgb_pool_admit(pgb_pool *p, int ni, int nj, int nk, int *slot) {
   // guess, whatever the range held before
   for (int r = 0; r < p->phys.nregs; r++)
     CK(cudaMemsetAsync(p->d_reg[r] + (size_t)p->ne * cv, 0, sizeof(double) * p->ne * vol, p->stream));
-  CK(cudaMemsetAsync(p->d_state + (size_t)8 * cv, 0, sizeof(double) * 8 * vol, p->stream));
+  CK(cudaMemsetAsync(p->d_state + (size_t)SW * cv, 0, sizeof(double) * SW * vol, p->stream));
   // from pageable memory: the call returns once D is staged, so the stack copy may go
   CK(cudaMemcpyAsync(p->d_blks + id, &D, sizeof(BlockDev), cudaMemcpyHostToDevice, p->stream));
   *slot = id;
@@ -1837,7 +1893,7 @@ int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count) {
   const PlainCase pc = pool_plain(p, p->d_blks, hb.data(), slot + 1);
   RET(kPlain[p->phys.ns - 1].fromprims(&pc, slot, p->d_host, p->d_reg[0]));
   // a halo cell's first Newton starts from the stored T of the cell it copies
-  k_selfhalo<<<grid_for(hb[slot].vol, 256), 256, 0, p->stream>>>(p->d_blks, slot, p->d_state, 8);
+  k_selfhalo<<<grid_for(hb[slot].vol, 256), 256, 0, p->stream>>>(p->d_blks, slot, p->d_state, SW);
   CK(cudaGetLastError());
   return PGB_OK;
 }

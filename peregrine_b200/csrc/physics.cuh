@@ -36,6 +36,15 @@ struct Species {
   int tpg, kinetic;
   int ncp, nh, nmu, nkappa;
   double cppolyR[MAXNS * MAXT], hpoly[MAXNS * MAXT], mupoly[MAXNS * MAXT], kappapoly[MAXNS * MAXT];
+  // the cubic real gas (a thermally perfect gas underneath, tpg set too) and
+  // its double flux: the form's u, w and roots sigma, eps; per species
+  // sqrt(a_c), b, -(da/dT) sqrt(T / a), m / sqrt(Tc), 1 + m, each of the first
+  // three and the translation also per unit of 1 / MW
+  // (peregrine/simulator/mixture/eos/realgas/model.py:43-98)
+  int realgas, df;
+  double cu, cw, csigma, ceps;
+  double csqrtac[MAXNS], cb[MAXNS], cda[MAXNS], cmTc[MAXNS], conepm[MAXNS], vshift[MAXNS];
+  double csqrtacMW[MAXNS], cbMW[MAXNS], cdaMW[MAXNS], vshiftMW[MAXNS];
 };
 
 static __constant__ Species kSp;
@@ -65,6 +74,7 @@ inline void species_fill(Species &s, int ns, double alpha, bool constant_transpo
   s.mu1 = s.kappa1 = 0.0;
   s.tpg = s.kinetic = 0;
   s.ncp = s.nh = s.nmu = s.nkappa = 0;
+  s.realgas = s.df = 0;
   if (ns == 1 && constant_transport) {
     volatile double Y = 1.0;
     const double denom = 0.0 + Y * s.MWinv[0];
@@ -206,10 +216,16 @@ __device__ __forceinline__ State fromQ(QF Q, const double Tguess = 0.0) {
   return s;
 }
 
-// frompT: the calorically perfect (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:17-27)
-// or the thermally perfect (peregrine/simulator/mixture/eos/tpg/kernels/eos.mako:22-32)
+// the real gas's frompT, in realgas.cuh
+template <int NS, class YF>
+__device__ __forceinline__ State frompT_rg_state(const double p, const double T, YF Y);
+
+// frompT: the calorically perfect (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:17-27),
+// the thermally perfect (peregrine/simulator/mixture/eos/tpg/kernels/eos.mako:22-32)
+// or the real gas (realgas.cuh)
 template <int NS, class YF>
 __device__ __forceinline__ State frompT(const double p, const double T, YF Y) {
+  if (kSp.realgas) return frompT_rg_state<NS>(p, T, Y);
   State s;
   s.p = p;
   s.T = T;
@@ -262,8 +278,11 @@ __device__ __forceinline__ State fromprims(const double *q, double *Q) {
 //  peregrine/simulator/mixture/transport/kernels/mixing.mako:3-10,
 //  peregrine/simulator/mixture/diffusion/kernels/lewis.mako:3-8,
 //  peregrine/simulator/mixture/eos/kernels/species.mako:9-36)
+template <int NS, class YF>
+__device__ __forceinline__ void hspecies_rg_of(double *h, YF Y, const double p, const double T, const double Z);
+
 template <int NS, class QF>
-__device__ __forceinline__ void transport(QF Q, const State &st, double *tr, double *hsp) {
+__device__ __forceinline__ void transport(QF Q, const State &st, double *tr, double *hsp, const double Z = 0.0) {
   const double rho = Q(0), rhoinv = 1.0 / rho;
   double Ylast = 1.0;
 #pragma unroll
@@ -323,7 +342,12 @@ __device__ __forceinline__ void transport(QF Q, const State &st, double *tr, dou
   const double kor = kappa * rhoinv / st.cp;
 #pragma unroll
   for (int n = 0; n < NS; n++) tr[2 + n] = kor / kSp.lewis[n];
-  // hspecies (peregrine/simulator/mixture/eos/kernels/species.mako:9-15, 31-36)
+  // hspecies: the real gas's partial enthalpies at the stored state, or the
+  // ideal ones (peregrine/simulator/mixture/eos/kernels/species.mako:9-15, 31-36)
+  if (kSp.realgas) {
+    hspecies_rg_of<NS>(hsp, [&](int n) { return Q(5 + n) * rhoinv; }, st.p, T, Z);
+    return;
+  }
   const double u = lnT, Tinv = 1.0 / T;
 #pragma unroll
   for (int n = 0; n < NS; n++) {
@@ -601,3 +625,5 @@ __device__ __forceinline__ void viscous1(const FaceGeom &g, const double mu, con
 }
 
 }  // namespace pgb
+
+#include "realgas.cuh"

@@ -30,20 +30,86 @@ __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi,
   fk = (int)(r / B.Y);
 }
 
-// fromQ over the whole block, halo included: state[8] per cell, the cell's
+// fromQ over the whole block, halo included: the state per cell, the cell's
 // last T the starting guess of an iterative eos
-// (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19)
+// (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19); for the real
+// gas its fromrhoE and root Z; with plane set, the double flux's fromplane:
+// p off the cell's frozen plane, then the state at rho and p
+// (peregrine/simulator/eulerdf/kernels/fromplane.mako:3-17)
 template <int NS>
 __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                        double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr) {
+                        double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr, const int plane = 0) {
   PGB_WHERE(B, t);
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
-  double *st = stall + 8 * B.cv + t;
+  double *st = stall + SW * B.cv + t;
   const long long v = B.vol;
-  const State s = fromQ<NS>([&](int c) { return Q[c * B.vol]; }, st[1 * v]);
+  auto Qf = [&](int c) { return Q[c * v]; };
+  State s;
+  if (kSp.realgas) {
+    const double rho = Qf(0), rhoinv = 1.0 / rho;
+    auto Y = [&](int n) { return Qf(5 + n) * rhoinv; };
+    const RGMom mom = mixmom_rg<NS>(Y);
+    RGState o;
+    if (plane) {
+      // pplane (peregrine/simulator/mixture/eos/realgasdf/kernels/eos.mako:50-56)
+      double composition = 0.0;
+#pragma unroll
+      for (int n = 0; n < NS - 1; n++) composition += st[(ST_ZETA + n) * v] * Qf(5 + n);
+      const double q1 = Qf(1), q2 = Qf(2), q3 = Qf(3);
+      const double p = (Qf(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv - st[ST_EPS * v] * Qf(0) - composition -
+                        st[ST_KAPPA * v]) / st[ST_THETA * v];
+      o = fromrhop_rg<NS>(mom, Y, rho, p, st[1 * v]);
+    } else {
+      const double q1 = Qf(1), q2 = Qf(2), q3 = Qf(3);
+      const double e = (Qf(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv) * rhoinv;
+      o = fromrhoE_rg<NS>(mom, Y, rho, e, st[1 * v]);
+    }
+    s = o.s;
+    st[ST_Z * v] = o.Z;
+  } else {
+    s = fromQ<NS>(Qf, st[1 * v]);
+  }
   st[0 * v] = s.p, st[1 * v] = s.T, st[2 * v] = s.rhoinv, st[3 * v] = s.rho;
   st[4 * v] = s.e, st[5 * v] = s.cp, st[6 * v] = s.gamma, st[7 * v] = s.c;
+}
+
+// the double flux's freeze, on the interior: the energy reset to the eos's,
+// and the tangent plane of rho e at the cell's state, rho e = theta p + eps rho
+// + sum zeta_n rho Y_n + kappa (peregrine/simulator/eulerdf/kernels/freeze.mako:3-32)
+template <int NS>
+__global__ void k_freeze(const BlockDev *__restrict__ blks, int b, double *__restrict__ Qall,
+                         double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr) {
+  PGB_WHERE(B, t);
+  if (t >= (long long)B.nx * B.ny * B.nz) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k), v = B.vol;
+  double *Q = Qall + (4 + NS) * B.cv + c;
+  double *st = stall + SW * B.cv + c;
+  const double rho = Q[0], rhoinv = 1.0 / rho;
+  const double p = st[0], T = st[1 * v], e = st[4 * v];
+  const double rhoe = rho * e;
+  Q[4 * v] = rhoe + 0.5 * (Q[1 * v] * Q[1 * v] + Q[2 * v] * Q[2 * v] + Q[3 * v] * Q[3 * v]) * rhoinv;
+  auto Y = [&](int n) { return Q[(5 + n) * v] * rhoinv; };
+  const RGMom mom = mixmom_rg<NS>(Y);
+  double theta, epsY;
+  planeslopes<NS>(theta, epsY, mom, Y, rho, rhoinv, T, e);
+  double rho_p, rho_T, rho_Y[NS > 1 ? NS - 1 : 1];
+  drho_rg<NS>(rho_p, rho_T, rho_Y, mom, Y, p, T, rho);
+  double h[NS];
+  hspecies_rg<NS>(h, mom, Y, p, T, st[ST_Z * v]);
+  const double cpoverrhoT = st[5 * v] / rho_T;
+  double zetaY = 0.0;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    const double zeta = h[n] - h[NS - 1] - cpoverrhoT * rho_Y[n];
+    st[(ST_ZETA + n) * v] = zeta;
+    zetaY += zeta * Y(n);
+  }
+  st[ST_THETA * v] = theta;
+  st[ST_EPS * v] = epsY - zetaY;
+  st[ST_KAPPA * v] = rhoe - epsY * rho - theta * p;
+  (void)rho_p;
 }
 
 __device__ __forceinline__ State load_state(const double *st, long long v) {
@@ -62,9 +128,9 @@ __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const doub
   PGB_WHERE(B, t);
   if (t >= B.vol) return;
   const double *Q = Qall + (4 + NS) * B.cv + t;
-  const State s = load_state(stall + 8 * B.cv + t, B.vol);
+  const State s = load_state(stall + SW * B.cv + t, B.vol);
   double tr[2 + NS], h[NS];
-  transport<NS>([&](int c) { return Q[c * B.vol]; }, s, tr, h);
+  transport<NS>([&](int c) { return Q[c * B.vol]; }, s, tr, h, stall[SW * B.cv + ST_Z * B.vol + t]);
   double *trp = trall + (2 + NS) * B.cv + t;
   double *hp = hall + NS * B.cv + t;
 #pragma unroll
@@ -93,7 +159,7 @@ __global__ void k_grads(const BlockDev *__restrict__ blks, int b, const double *
   const long long c = cell_index(B, i, j, k);
   const long long sI = 1, sJ = B.X, sK = (long long)B.X * B.Y;
   const double *Q = Qall + NE * B.cv + c;
-  const double *T = stall + 8 * B.cv + 1 * B.vol + c;
+  const double *T = stall + SW * B.cv + 1 * B.vol + c;
   const double *J = met + M_NCOMP * B.cv + M_JINV * B.vol + c;
   double *g = gall + 3 * NGRAD * B.cv + c;
   const long long v = B.vol;
@@ -147,7 +213,7 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
   const double *Q = Qall + NE * B.cv;
-  const double *st = stall + 8 * B.cv;
+  const double *st = stall + SW * B.cv;
   const double *S = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
   auto side = [&](long long c) {
     const State s = load_state(st + c, v);
@@ -169,6 +235,68 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
   for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
 }
 
+// the double flux's kepaec: the plain two-point flux with the energy row
+// written twice, in the left cell's frozen plane at F[4] and in the right
+// cell's at F[ne] (peregrine/simulator/eulerdf/kernels/flux/function/kepaec.mako:1-21,
+// the plain flux function/kepaec.mako:2-20); NE + 1 rows per face
+template <int NS, int A>
+__global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                             const double *__restrict__ stall, const double *__restrict__ met,
+                             double *__restrict__ Fall, const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS, NF = NE + 1;
+  PGB_WHERE(B, t);
+  int i, j, k;
+  if (!face_at<A>(B, t, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
+  const long long v = B.vol;
+  const double *Q = Qall + NE * B.cv;
+  const double *st = stall + SW * B.cv;
+  const double *Sp = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
+  const double S0 = Sp[0], S1 = Sp[v], S2 = Sp[2 * v];
+  const double uL = Q[1 * v + L] / Q[L], vL = Q[2 * v + L] / Q[L], wL = Q[3 * v + L] / Q[L];
+  const double uR = Q[1 * v + R] / Q[R], vR = Q[2 * v + R] / Q[R], wR = Q[3 * v + R] / Q[R];
+  const double pL = st[L], pR = st[R], rhoL = st[3 * v + L], rhoR = st[3 * v + R];
+  const double uf = 0.5 * (uR + uL), vf = 0.5 * (vR + vL), wf = 0.5 * (wR + wL);
+  const double U = S0 * uf + S1 * vf + S2 * wf;
+  const double pf = 0.5 * (pR + pL);
+  const double rho = 0.5 * (rhoR + rhoL);
+  const double C = rho * U;
+  double F[NF];
+  F[0] = C;
+  F[1] = C * uf + pf * S0;
+  F[2] = C * vf + pf * S1;
+  F[3] = C * wf + pf * S2;
+  const double Kj = C * 0.5 * (uR * uL + vR * vL + wR * wL);
+  const double Pj = 0.5 * (pL * (uR * S0 + vR * S1 + wR * S2) + pR * (uL * S0 + vL * S1 + wL * S2));
+  double YL[NS > 1 ? NS - 1 : 1], YR[NS > 1 ? NS - 1 : 1];
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    YL[n] = Q[(5 + n) * v + L] / Q[L], YR[n] = Q[(5 + n) * v + R] / Q[R];
+    F[5 + n] = 0.5 * (YR[n] + YL[n]) * C;
+  }
+  const double rhoinvL = 1.0 / rhoL, rhoinvR = 1.0 / rhoR;
+  // ecomp: each side's composition energy in each plane
+  double cL[2] = {0.0, 0.0}, cR[2] = {0.0, 0.0};
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    const double zL = st[(ST_ZETA + n) * v + L], zR = st[(ST_ZETA + n) * v + R];
+    cL[0] += zL * YL[n], cL[1] += zR * YL[n];
+    cR[0] += zL * YR[n], cR[1] += zR * YR[n];
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const long long P = q == 0 ? L : R;
+    const double theta = st[ST_THETA * v + P], eps = st[ST_EPS * v + P], kappa = st[ST_KAPPA * v + P];
+    // ethermal: the thermal part theta p + kappa over the density, at each side's pressure
+    const double tL = (theta * pL + kappa) * rhoinvL, tR = (theta * pR + kappa) * rhoinvR;
+    F[q == 0 ? 4 : NE] = (eps + 0.5 * (cL[q] + cR[q]) + 2.0 * tL * tR / (tL + tR)) * C + Kj + Pj;
+  }
+  double *Fo = Fall + NF * B.cv + R;
+#pragma unroll
+  for (int l = 0; l < NF; l++) Fo[l * v] = F[l];
+}
+
 // the advective face flux of a Riemann solver FN on the cells as they are
 // (lim 0; recon/constant.mako:3-18) or on MUSCL's sides under limiter lim
 // (recon/muscl.mako:15-51), both sides from the four cells LL, L, R, RR
@@ -187,7 +315,7 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
   const long long L = R - d;
   const long long v = B.vol;
   const double *Q = Qall + NE * B.cv;
-  const double *st = stall + 8 * B.cv;
+  const double *st = stall + SW * B.cv;
   const double *Sp = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
   const double S[3] = {Sp[0], Sp[v], Sp[2 * v]};
   RSide sl, sr;
@@ -246,7 +374,7 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
   const double *Q = Qall + NE * B.cv;
-  const double *st = stall + 8 * B.cv;
+  const double *st = stall + SW * B.cv;
   const double *tr = trall + (2 + NS) * B.cv;
   const double *hs = hall + NS * B.cv;
   const double *gr = gall + 3 * NGRAD * B.cv;
@@ -352,6 +480,31 @@ __global__ void k_applyflux(const BlockDev *__restrict__ blks, int b, const doub
   }
 }
 
+// the double flux's divergence: the energy row takes F[ne] on the cell's low
+// faces, where it is the right cell, and F[4] on its high faces
+// (peregrine/simulator/eulerdf/kernels/applyflux.mako:2-14)
+template <int NS>
+__global__ void k_applyflux_df(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Fi,
+                               const double *__restrict__ Fj, const double *__restrict__ Fk,
+                               const double *__restrict__ met, double *__restrict__ dQall,
+                               const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS, NF = NE + 1;
+  PGB_WHERE(B, t);
+  if (t >= (long long)B.nx * B.ny * B.nz) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k), v = B.vol;
+  const long long sJ = B.X, sK = (long long)B.X * B.Y;
+  const double detJinv = met[M_NCOMP * B.cv + M_DETJINV * v + c];
+  const double *fi = Fi + NF * B.cv + c, *fj = Fj + NF * B.cv + c, *fk = Fk + NF * B.cv + c;
+  double *dQ = dQall + NE * B.cv + c;
+#pragma unroll
+  for (int l = 0; l < NE; l++) {
+    if (l == 4) continue;
+    dQ[l * v] = (fi[l * v] + fj[l * v] + fk[l * v] - fi[l * v + 1] - fj[l * v + sJ] - fk[l * v + sK]) * detJinv;
+  }
+  dQ[4 * v] = (fi[NE * v] + fj[NE * v] + fk[NE * v] - fi[4 * v + 1] - fj[4 * v + sJ] - fk[4 * v + sK]) * detJinv;
+}
+
 // one combine (peregrine/integrators/kernels/combine.mako:1-13) on a block's interior
 struct CombineDev {
   double *out;
@@ -400,15 +553,31 @@ __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const doub
   double q[NE], Q[NE];
 #pragma unroll
   for (int l = 0; l < NE; l++) q[l] = prims[l * n + t];
-  const State th = fromprims<NS>(q, Q);
+  State th;
+  double Z = 0.0;
+  if (kSp.realgas) {
+    const RGState o = frompT_rg<NS>(q[0], q[4], [&](int n) { return q[5 + n]; });
+    th = o.s;
+    Z = o.Z;
+    Q[0] = th.rho;
+    Q[1] = th.rho * q[1];
+    Q[2] = th.rho * q[2];
+    Q[3] = th.rho * q[3];
+    Q[4] = th.rho * (th.e + 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]));
+#pragma unroll
+    for (int n = 0; n < NS - 1; n++) Q[5 + n] = th.rho * q[5 + n];
+  } else {
+    th = fromprims<NS>(q, Q);
+  }
   double *Qo = Qall + NE * B.cv + c;
 #pragma unroll
   for (int l = 0; l < NE; l++) Qo[l * B.vol] = Q[l];
   if (stall) {
-    double *st = stall + 8 * B.cv + c;
+    double *st = stall + SW * B.cv + c;
     const long long v = B.vol;
     st[0 * v] = th.p, st[1 * v] = th.T, st[2 * v] = th.rhoinv, st[3 * v] = th.rho;
     st[4 * v] = th.e, st[5 * v] = th.cp, st[6 * v] = th.gamma, st[7 * v] = th.c;
+    st[ST_Z * v] = Z;
   }
 }
 

@@ -33,6 +33,7 @@ struct PlainCase {
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
   int visc, primary, recon, limiter, chem;
+  int df;      // the double flux: fromplane in the stages, two energy rows per face (F holds NE + 1 rows)
   int packed;  // 1: each pass is one launch over every block
   // with packing, each range's tile table (cells with halo, interior cells,
   // i, j and k faces): CTA x works tile ctab[r][x].y of block ctab[r][x].x;
@@ -49,6 +50,7 @@ struct PlainOps {
   int (*rhs)(const PlainCase *, const double *Q, double *dQ);
   int (*fromprims)(const PlainCase *, int blk, const double *prims, double *Q);
   int (*production)(long long n, const double *rho, const double *Y, const double *T, double *omega, cudaStream_t);
+  int (*prestep)(const PlainCase *, double *Q, int first);
 };
 
 }  // namespace pgb
@@ -62,4 +64,5 @@ struct PlainOps {
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_fromprims_##N(const pgb::PlainCase *, int,      \
                                                                                const double *, double *);        \
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_production_##N(                                 \
-      long long, const double *, const double *, const double *, double *, cudaStream_t);
+      long long, const double *, const double *, const double *, double *, cudaStream_t);                        \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_prestep_##N(const pgb::PlainCase *, double *, int);

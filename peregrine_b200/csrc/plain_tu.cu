@@ -70,6 +70,10 @@ void adv_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *
   const RhsArgs &a = *(const RhsArgs *)ctx;
   const int lim = pc->recon == PGB_RECON_MUSCL ? pc->limiter : 0;
   cudaStream_t s = pc->stream;
+  if (pc->df) {
+    k_advflux_df<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
+    return;
+  }
   switch (pc->primary) {
     case PGB_FLUX_HLLC: k_riemann<NS, A, FN_HLLC><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
     case PGB_FLUX_RUSANOV: k_riemann<NS, A, FN_RUSANOV><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
@@ -86,7 +90,7 @@ void diff_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void 
 
 void fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_fromQ<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct);
+  k_fromQ<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, pc->df);
 }
 void transport_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
@@ -102,7 +106,10 @@ void source_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const voi
 }
 void apply_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_applyflux<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, a.dQ, pc->chem, ct);
+  if (pc->df)
+    k_applyflux_df<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, a.dQ, ct);
+  else
+    k_applyflux<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, a.dQ, pc->chem, ct);
 }
 
 }  // namespace
@@ -221,4 +228,26 @@ extern "C" int PGB_ENTRY(pgb_plain_production_)(long long n, const double *rho, 
   if (n > 0) k_production<NS><<<grid_of(n), TH, 0, s>>>(n, rho, Y, T, omega);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "production");
+}
+
+// the double flux's step start: the state of Q (the eos's fromrhoE on the
+// first step, the frozen planes' after), the planes frozen anew on the
+// interior with the energy reset to the eos's, then Q and the state (planes
+// included) copied into the halos, so a halo's plane is its image's
+// (peregrine/simulator/eulerdf/simulator.py:58-66)
+extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int first) {
+  cudaStream_t s = pc->stream;
+  for (int b = 0; b < pc->nblocks; b++) {
+    const BlockDev &D = pc->h_blks[b];
+    k_fromQ<NS><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, nullptr, first ? 0 : 1);
+    mark(pc, 2);
+    k_freeze<NS><<<grid_of(range_size(D, R_INNER)), TH, 0, s>>>(pc->d_blks, b, Q, pc->state);
+    mark(pc, 2);
+  }
+  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(Q, pc->halo, pc->nhalo, NE);
+  mark(pc, 0);
+  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(pc->state, pc->halo, pc->nhalo, SW);
+  mark(pc, 0);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PGB_OK : cuda_fail(e, "double-flux freeze");
 }

@@ -3,7 +3,10 @@ them, to an .npz that peregrine_b200 loads.
 
     python -m peregrine_b200.data.export_mixture REFERENCE OUT.npz MECHANISM \\
         [--keep H2,H,O,...] [--eos tpg] [--trans kinetic-theory] \\
-        [--chemistry finite-rate] [--trange 300 3500]
+        [--chemistry finite-rate] [--trange 300 3500] [--cubic srk|pr]
+
+MECHANISM is a mechanism file, or species of the reference's library
+separated by commas.
 
 The thermally perfect fits (cp, h and s in ln T), the kinetic-theory fits of
 mu and kappa, the reaction columns and the third-body sets are all worked out
@@ -32,6 +35,18 @@ import numpy as np
 
 # reaction kinds, shared with include/pgb200.h
 KINDS = {"elementary": 0, "three-body": 1, "lindemann": 2, "troe": 3}
+
+# The reference ships the Soave-Redlich-Kwong cubic
+# (peregrine/simulator/mixture/eos/realgas/model.py:26-29); its kernels are
+# generic in the form's u and w and the species' a, b and m.  Peng-Robinson is
+# these constants (Peng and Robinson, 1976): v^2 + 2 b v - b^2 in the
+# attraction's denominator, Omega_a 0.45724, Omega_b 0.07780 and
+# m = 0.37464 + 1.54226 w - 0.26992 w^2.  Set on the reference's model class
+# here, on the export's side; the reference is not edited.
+CUBICS = {
+    "srk": None,
+    "pr": dict(u=2.0, w=-1.0, omega_a=0.45724, omega_b=0.07780, m=(0.37464, 1.54226, -0.26992)),
+}
 
 
 def _stub(name, **attrs):
@@ -120,13 +135,19 @@ def subset(mechanism, keep, where):
     return path
 
 
-def reference_mixture(reference, species, eos="tpg", trans=None, chemistry=None, trange=(300.0, 3500.0)):
+def reference_mixture(reference, species, eos="tpg", trans=None, chemistry=None, trange=(300.0, 3500.0),
+                      cubic="srk"):
     """The reference's Mixture for a config, from a checkout at reference."""
     install_stubs()
     if reference not in sys.path:
         sys.path.insert(0, reference)
     import peregrine as pg
     from peregrine.simulator.mixture import get_mixture
+    from peregrine.simulator.mixture.eos.realgas.model import RealGasModel
+
+    if not hasattr(RealGasModel, "_shipped_cubic"):
+        RealGasModel._shipped_cubic = dict(RealGasModel.cubic)
+    RealGasModel.cubic = CUBICS[cubic] or RealGasModel._shipped_cubic
 
     cfg = pg.Config()
     m = cfg["mixture"]
@@ -140,6 +161,10 @@ def tables(mix):
     out = {k: np.asarray(v, dtype=np.float64) for k, v in mix.constants().items()}
     out["spnames"] = np.array(mix.spnames)
     out["eos"] = np.array(mix.eos.name)
+    if hasattr(mix.eos, "cubic"):
+        c = mix.eos.cubic
+        out["cubic_omega_a"], out["cubic_omega_b"] = np.array(c["omega_a"]), np.array(c["omega_b"])
+        out["cubic_m"] = np.array(c["m"])
     out["trans"] = np.array(mix.trans.name if mix.trans is not None else "")
     out["ns"] = np.array(mix.ns)
     if mix.chemistry is not None:
@@ -169,14 +194,18 @@ def main(argv=None):
     ap.add_argument("--trans", default=None)
     ap.add_argument("--chemistry", default=None)
     ap.add_argument("--trange", nargs=2, type=float, default=(300.0, 3500.0))
+    ap.add_argument("--cubic", default="srk", choices=sorted(CUBICS))
     a = ap.parse_args(argv)
     mech = a.mechanism
-    if not os.path.isfile(mech):
+    if "," in mech:
+        # species from the reference's library by name
+        mech = mech.split(",")
+    elif not os.path.isfile(mech):
         mech = os.path.join(a.reference, "peregrine", "simulator", "mixture", "database", "mechanisms", mech)
     with tempfile.TemporaryDirectory() as tmp:
-        if a.keep:
+        if a.keep and isinstance(mech, str):
             mech = subset(mech, a.keep.split(","), tmp)
-        mix = reference_mixture(a.reference, mech, a.eos, a.trans, a.chemistry, a.trange)
+        mix = reference_mixture(a.reference, mech, a.eos, a.trans, a.chemistry, a.trange, a.cubic)
         np.savez(a.out, **tables(mix))
     print(a.out, mix)
 

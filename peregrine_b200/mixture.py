@@ -84,7 +84,9 @@ class Mixture:
         self.eos, self.trans = cfgsect["eos"], cfgsect["trans"]
         self.chemistry = cfgsect.get("chemistry")
         made = str(tables["eos"])
-        if self.eos != made:
+        # the double flux's real gas is the real gas's, same tables
+        same = {"real-gas-df": "real-gas"}
+        if same.get(self.eos, self.eos) != same.get(made, made):
             raise ValueError(f"mixture.eos {self.eos!r}: the tables were made for {made!r}")
         if self.trans is not None and self.trans != str(tables["trans"]):
             raise ValueError(f"mixture.trans {self.trans!r}: the tables were made for {str(tables['trans'])!r}")

@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libpgb200.so")
 
 OK, ERR_ARG, ERR_STATE, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
-EULER, NAVIER_STOKES = 0, 1
-EOS_CPG, EOS_TPG = 0, 1
+EULER, NAVIER_STOKES, EULER_DF = 0, 1, 2
+EOS_CPG, EOS_TPG, EOS_REALGAS, EOS_REALGAS_DF = 0, 1, 2, 3
 FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV, FLUX_AUSMUP = 0, 1, 2, 3
 RECON_CONSTANT, RECON_MUSCL = 0, 1
 LIMITERS = {"koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}

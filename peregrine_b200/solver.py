@@ -112,8 +112,10 @@ class Solver:
         self.graph = bool(cfg["backend-b200"]["graph"])
         adv = cfg["adv-flux"]
         phys = native.Physics()
-        phys.simulator = native.NAVIER_STOKES if sim["simulator"] == "navier-stokes" else native.EULER
-        phys.eos = native.EOS_TPG if cfg["mixture"]["eos"] == "tpg" else native.EOS_CPG
+        phys.simulator = {"euler": native.EULER, "navier-stokes": native.NAVIER_STOKES,
+                          "euler-df": native.EULER_DF}[sim["simulator"]]
+        phys.eos = {"cpg": native.EOS_CPG, "tpg": native.EOS_TPG, "real-gas": native.EOS_REALGAS,
+                    "real-gas-df": native.EOS_REALGAS_DF}[cfg["mixture"]["eos"]]
         phys.primary = {"kepaec": native.FLUX_KEPAEC, "hllc": native.FLUX_HLLC, "rusanov": native.FLUX_RUSANOV,
                         "ausmup": native.FLUX_AUSMUP}[adv["primary"]]
         phys.recon = native.RECON_CONSTANT if adv["recon"] == "constant" else native.RECON_MUSCL
@@ -156,8 +158,12 @@ class Solver:
         for key in ("cp0", "mu0", "kappa0", "MWqinv", "wilkepair", "lewis"):
             if key in consts:
                 tables[key] = consts[key]
-        if self.mixture.eos == "tpg":
+        if self.mixture.eos != "cpg":
             tables.update(cppolyR=consts["cppolyR"], hpoly=consts["hpoly"])
+        if self.mixture.eos in ("real-gas", "real-gas-df"):
+            for key in ("cubicu", "cubicw", "cubicsigma", "cubiceps", "cubicsqrtac", "cubicb", "cubicda", "cubicmTc",
+                        "cubiconepm", "vshift", "cubicsqrtacMW", "cubicbMW", "cubicdaMW", "vshiftMW"):
+                tables[key] = np.atleast_1d(consts[key])
         if self.mixture.trans == "kinetic-theory":
             tables.update(mupoly=consts["mupoly"], kappapoly=consts["kappapoly"])
         return tables

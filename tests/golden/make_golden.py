@@ -30,6 +30,11 @@ What it records, each from the reference's own code:
                      Gibbs functions, and the species' cp and h by the
                      reference's own polynomial evaluation.
 
+  realgas_<cubic>.npz tests/eos/support.py's textbook density of the cubic
+                     (numpy's roots and the least Gibbs energy phase) for O2/H2
+                     at random (p, T, Y), the reference's Soave-Redlich-Kwong
+                     and, with its constants set on the numpy twin, Peng-Robinson.
+
 The mixtures' constant tables themselves are written by
 peregrine_b200/data/export_mixture.py from the same reference code.
 """
@@ -218,6 +223,22 @@ def rates_of(reference, mech, keep, n, rng):
                 Ts=Ts, cpR=cpR, hR=hR)
 
 
+def realgas_densities(reference, cubic, n, rng):
+    from peregrine_b200.data.export_mixture import CUBICS, reference_mixture
+    from tests.eos import support
+
+    mix = reference_mixture(reference, ["O2", "H2"], "real-gas", trange=(100.0, 1000.0), cubic=cubic)
+    support.cubic = CUBICS[cubic] or mix.eos.cubic
+    sp = [dict(MW=s["MW"], Tcrit=s["Tcrit"], pcrit=s["pcrit"], acentric=s["acentric"]) for s in mix.species.values()]
+    p = rng.uniform(1e6, 8e7, n)
+    T = rng.uniform(100.0, 600.0, n)
+    Y0 = rng.uniform(0.0, 1.0, n)
+    # dense and liquid-like oxygen at the mixing layer's cold side
+    p[:8], T[:8], Y0[:8] = 6e6, np.linspace(100.0, 160.0, 8), 1.0
+    rho = np.array([support.textbookdensity(sp, p[k], T[k], np.array([Y0[k], 1.0 - Y0[k]])) for k in range(n)])
+    return dict(p=p, T=T, Y=Y0[:, None], rho=rho)
+
+
 def metrics(GridBlock, rng):
     ng = 2
     shape = (7 + 2 * ng, 6 + 2 * ng, 5 + 2 * ng)
@@ -299,6 +320,9 @@ def main():
              **rates_of(REF, "GRI30.yaml", h2o2, 96, np.random.default_rng(20261206)))
     np.savez(os.path.join(HERE, "rates_ch4_o2_ffcmy.npz"),
              **rates_of(REF, "CH4_O2_FFCMY.yaml", None, 96, np.random.default_rng(20261207)))
+    for cubic in ("srk", "pr"):
+        np.savez(os.path.join(HERE, f"realgas_{cubic}.npz"),
+                 **realgas_densities(REF, cubic, 128, np.random.default_rng(20261208)))
     with open(os.path.join(HERE, "gases.json"), "w") as f:
         json.dump(dict(air=air, binary=BINARY), f, indent=1)
     print("wrote", sorted(p for p in os.listdir(HERE) if not p.endswith(".py")))
