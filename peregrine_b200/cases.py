@@ -212,3 +212,53 @@ def reacting_prims(metrics, spnames, MW, cells, length=0.01, seed=0, spots=4, dT
     for q, u in zip(out, vel):
         q[..., 1:4] = u * (urms / rms)
     return out
+
+
+# the transcritical mixing layer: O2 (dense, 120 K) and H2 (300 K) at 60 bar,
+# the real gas with the double flux
+def mixing_layer_config(cubic="pr", simulator="euler-df", integrator="tvd-rk3", launch="per-block"):
+    cfg = Config()
+    cfg["simulation"]["simulator"] = simulator
+    cfg["mixture"]["species"] = f"o2_h2_{cubic}"
+    cfg["mixture"]["eos"] = "real-gas-df" if simulator == "euler-df" else "real-gas"
+    cfg["mixture"]["trans"] = "constant" if simulator == "navier-stokes" else None
+    cfg["time-integration"]["integrator"] = integrator
+    cfg["adv-flux"]["primary"] = "kepaec"
+    cfg["backend-b200"]["launch"] = launch
+    return cfg.validate()
+
+
+def mixing_layer_mesh(nx=256, ny=128, nz=4, blocks=8, dx=2e-5, seed=0, low=None, high=None):
+    """A periodic box of nx x ny x nz cells of dx, cut along i into blocks of
+    seeded uneven widths (low..high cells)."""
+    rng = np.random.default_rng(seed)
+    if blocks == 1:
+        cuts = [nx]
+    else:
+        lo = low if low is not None else int(0.75 * nx / blocks)
+        hi = high if high is not None else int(1.25 * nx / blocks)
+        cuts = uneven_cuts(nx, blocks, lo, hi, rng)
+    return CubeMesher(mbdims=[blocks, 1, 1], cells=[cuts, [ny], [nz]], lengths=[nx * dx, ny * dx, nz * dx],
+                      periodic=[True] * 3)
+
+
+def mixing_layer_prims(metrics, ny, dx=2e-5, seed=0, p=6e6, Tcold=120.0, Thot=300.0, dU=50.0, noise=0.01,
+                       width=4.0):
+    """Primitives (p, u, v, w, T, Y_O2): a band of cold O2 between two tanh
+    interfaces (width cells thick) in a periodic H2 stream, the streams at
+    +-dU/2, with seeded noise of noise * dU on u and v."""
+    rng = np.random.default_rng(seed)
+    Ly = ny * dx
+    out = []
+    for m in metrics:
+        y = m["xcc"][..., 1]
+        d = width * dx
+        f = 0.5 * (np.tanh((y - 0.25 * Ly) / d) - np.tanh((y - 0.75 * Ly) / d))
+        q = np.zeros(y.shape + (6,))
+        q[..., 0] = p
+        q[..., 1] = -0.5 * dU + dU * f + noise * dU * rng.standard_normal(y.shape)
+        q[..., 2] = noise * dU * rng.standard_normal(y.shape)
+        q[..., 4] = Thot + (Tcold - Thot) * f
+        q[..., 5] = np.clip(f, 0.0, 1.0)
+        out.append(q)
+    return out

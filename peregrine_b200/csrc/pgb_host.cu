@@ -933,6 +933,8 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
     return fail(PGB_ERR_UNSUPPORTED, "kepaec is a two-point flux of the cells as they are; it takes no muscl sides");
   if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT && phys->trans != PGB_TRANS_KINETIC)
     return fail(PGB_ERR_UNSUPPORTED, "the viscous path takes constant or kinetic-theory transport");
+  if (phys->simulator == PGB_NAVIER_STOKES && (phys->eos == PGB_EOS_REALGAS || phys->eos == PGB_EOS_REALGAS_DF))
+    return fail(PGB_ERR_UNSUPPORTED, "the real gas runs inviscid in this build (euler, euler-df)");
   if (phys->trans == PGB_TRANS_KINETIC && phys->eos == PGB_EOS_CPG)
     return fail(PGB_ERR_ARG, "kinetic-theory transport needs the thermally perfect caloric");
   if (phys->chemistry != PGB_CHEM_NONE && phys->chemistry != PGB_CHEM_COUPLED)
