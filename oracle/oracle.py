@@ -427,7 +427,8 @@ class Oracle:
         return F
 
     def prestep(self, Q):
-        """The double flux's step start on register Q (its freeze)."""
+        """The double flux's freeze on register Q: off the eos once after the
+        state was set, off the frozen planes at every step's start."""
         obs = self._oblocks(Q)
         m = np.ascontiguousarray(self.map)
         self.lib.oracle_prestep(ctypes.byref(self.case), obs, len(self.blocks), m.ctypes.data_as(ctypes.c_void_p),
@@ -457,6 +458,8 @@ class Oracle:
         names = list(range(self.nregs))
         stages, dQ = stage_combines(self.integrator, names)
         if self.df:
+            if self.df_fresh:
+                self.prestep(self.regs[stages[0][0]])
             self.prestep(self.regs[stages[0][0]])
         for Q, combines in stages:
             self.rhs(self.regs[Q], self.regs[dQ])

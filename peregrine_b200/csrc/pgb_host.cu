@@ -800,8 +800,11 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   return pc;
 }
 
-// the double flux's step start (freeze) on register qphys
-int prestep_plain(pgb_case *c, int qphys, int &count) {
+// the double flux's freeze on register qphys: at every step's start off the
+// frozen planes (first 0), or once after the state was set, off the eos
+// (first 1; the reference's initialize graph,
+// peregrine/simulator/eulerdf/simulator.py:63-66)
+int prestep_plain(pgb_case *c, int qphys, int &count, int first) {
   if (c->phys.simulator != PGB_EULER_DF) return PGB_OK;
   RET(ensure_scratch(c));
   std::vector<BlockDev> hb;
@@ -809,9 +812,16 @@ int prestep_plain(pgb_case *c, int qphys, int &count) {
   MarkCtx mc{c, &count};
   pc.mark = mark_cb;
   pc.ctx = &mc;
-  RET(kPlain[c->phys.ns - 1].prestep(&pc, c->d_reg[qphys], c->df_fresh ? 1 : 0));
-  c->df_fresh = false;
+  RET(kPlain[c->phys.ns - 1].prestep(&pc, c->d_reg[qphys], first));
+  if (first) c->df_fresh = false;
   return PGB_OK;
+}
+
+// the double flux's planes for a state just set
+int df_settle(pgb_case *c, int qphys) {
+  if (c->phys.simulator != PGB_EULER_DF || !c->df_fresh) return PGB_OK;
+  int count = 0;
+  return prestep_plain(c, qphys, count, 1);
 }
 
 int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
@@ -827,7 +837,7 @@ int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
 int step_plain(pgb_case *c, int &count) {
   const int TH = 256;
   const auto &map = c->phys_of;
-  if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count));
+  if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count, 0));
   for (const pgb_stage &st : c->stages) {
     RET(rhs_plain(c, map[st.q], map[st.dq], count));
     for (int m = 0; m < st.ncombine; m++) {
@@ -1291,7 +1301,7 @@ int pgb_rhs(pgb_case *c, int q, int dq) {
     return fail(PGB_ERR_ARG, "bad registers");
   int count = 0;
   // the double flux's planes, frozen once after the state was set
-  if (c->df_fresh) RET(prestep_plain(c, c->phys_of[q], count));
+  RET(df_settle(c, c->phys_of[q]));
   RET(rhs_plain(c, c->phys_of[q], c->phys_of[dq], count));
   return PGB_OK;
 }
@@ -1305,6 +1315,7 @@ int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph) {
     return fail(PGB_ERR_UNSUPPORTED, "the batched path takes the single-species cpg kepaec case; use the per-block path");
   RET(prepare(c, fused));
   if (!fused) RET(ensure_scratch(c));
+  if (!fused && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
   k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev0, c->stream));
@@ -1358,6 +1369,7 @@ int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int 
   if (fused && !fused_capable(c)) return fail(PGB_ERR_UNSUPPORTED, "the batched path does not take this case");
   RET(prepare(c, fused));
   if (!fused) RET(ensure_scratch(c));
+  if (!fused && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
   k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
   CK(cudaGetLastError());
   c->timing = true;
