@@ -29,6 +29,12 @@ thermally perfect, kinetic-theory transport, coupled finite-rate chemistry),
 MUSCL with the koren limiter and HLLC, Navier-Stokes, TVD-RK3, on the
 per-block device path; with the CPU oracle on one stage of it beside it.
 
+A real-gas leg (key "realgas") times the transcritical mixing layer: 256 x
+128 x 4 cells of 20 um in 8 blocks of seeded uneven widths along i, O2 at
+120 K in a band between two tanh interfaces in an H2 stream at 300 K, 60
+bar, the streams 50 m/s apart with seeded 1 % noise; Peng-Robinson with the
+double flux, kepaec, Euler, TVD-RK3, per-block path.
+
 A serving leg (key "serving") plays a seeded Poisson stream of 300 H2/air
 requests at 60 per second: closed constant-volume reactors (phi, T0 and p
 drawn uniformly) and periodic 1-D domains of 64 to 2048 cells (log-uniform),
@@ -256,6 +262,47 @@ def reacting_leg(steps, cpu=True):
     return out
 
 
+def realgas_leg(steps, cpu=True):
+    """Cell-stage/s of the transcritical mixing layer on the per-block path."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases
+
+    cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3")
+    mesh = cases.mixing_layer_mesh(256, 128, 4, 8, seed=SEED)
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    prims = cases.mixing_layer_prims(mb.metrics, 128, seed=SEED)
+    mb.set_prims(prims)
+    dt = 2e-9
+    mb.step(dt, 3)
+    mb.backend.sync()
+    ms = time_graph(mb, dt, steps)
+    ncells = mb.ncells
+    value = ncells * 3 * steps / (ms / 1e3)
+    # RK3 registers (8/3 of 6 doubles) and the frozen plane's 4 doubles read
+    nbytes = 8 * 6 * 8 / 3 + 8 * 4
+    out = {"value": value, "unit": "cell-stage/s", "steps": steps, "ms_per_step": ms / steps,
+           "launches_per_step": mb.launches_per_step(), "dt": dt,
+           "workload": "mixing-layer-256x128x4-8-uneven-blocks-o2-h2-60bar-peng-robinson-double-flux-kepaec-euler-rk3",
+           "path": "per-block kernels, one launch per block and pass",
+           "blocks": [b.cells[0] for b in mb.mesh_blocks],
+           "algorithmic_bytes_per_cell_stage": nbytes, "hbm_gbs_of_algorithmic_bytes": value * nbytes / 1e9}
+    if cpu:
+        from oracle.oracle import Oracle
+
+        orc = Oracle(mb.mixture.constants(), mb.ns, "euler", mb.mesh_blocks, mb.metrics, "tvd-rk3",
+                     eos="real-gas-df", trans="constant")
+        orc.set_prims(prims)
+        dQ = [np.zeros_like(r) for r in orc.regs[0]]
+        orc.rhs(orc.regs[0], dQ)  # the planes' settle
+        t0 = time.perf_counter()
+        orc.rhs(orc.regs[0], dQ)
+        wall = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": ncells / wall, "unit": "cell-stage/s", "cores": os.cpu_count(),
+                               "kind": "port", "sample": f"one stage (RHS) of the mixing layer, {wall:.2f} s"}
+    del mb
+    return out
+
+
 def serving_leg(n=300, rate=60.0, steps=100):
     """The serving stream: Poisson arrivals of H2/air closed reactors and
     periodic 1-D domains, admitted into one pool while others run."""
@@ -354,12 +401,17 @@ def main():
     ap.add_argument("--no-reacting", action="store_true", help="skip the reacting leg")
     ap.add_argument("--reacting-only", action="store_true", help="the reacting leg alone (profiling)")
     ap.add_argument("--serving-only", action="store_true", help="the serving leg alone")
+    ap.add_argument("--realgas-only", action="store_true", help="the real-gas leg alone")
+    ap.add_argument("--no-realgas", action="store_true", help="skip the real-gas leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     args = ap.parse_args()
     set_cells(args.cells)
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.realgas_only:
+        print(json.dumps({"realgas": realgas_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
         return
     if args.serving_only:
         print(json.dumps({"serving": serving_leg()}), flush=True)
@@ -462,6 +514,9 @@ def main():
     served = None
     if rank == 0 and not args.no_serving and not args.no_extra:
         served = serving_leg()
+    realgas = None
+    if rank == 0 and not args.no_realgas and not args.no_extra:
+        realgas = realgas_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
 
     if rank == 0:
         line = {
@@ -483,6 +538,7 @@ def main():
             "cpu_baseline": cpu,
             "reacting": reacting,
             "serving": served,
+            "realgas": realgas,
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
