@@ -796,6 +796,7 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
   pc.chem = c->phys.chemistry == PGB_CHEM_COUPLED;
   pc.df = c->phys.simulator == PGB_EULER_DF;
+  pc.realgas = c->phys.eos == PGB_EOS_REALGAS || c->phys.eos == PGB_EOS_REALGAS_DF;
   pc.stream = c->stream;
   return pc;
 }
@@ -1732,6 +1733,7 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.visc = p->phys.simulator == PGB_NAVIER_STOKES;
   pc.primary = p->phys.primary, pc.recon = p->phys.recon, pc.limiter = p->phys.limiter;
   pc.chem = p->phys.chemistry == PGB_CHEM_COUPLED;
+  pc.realgas = p->phys.eos == PGB_EOS_REALGAS || p->phys.eos == PGB_EOS_REALGAS_DF;
   pc.packed = 1;
   pc.stream = p->stream;
   return pc;

@@ -220,12 +220,15 @@ __device__ __forceinline__ State fromQ(QF Q, const double Tguess = 0.0) {
 template <int NS, class YF>
 __device__ __forceinline__ State frompT_rg_state(const double p, const double T, YF Y);
 
+// RG: the case's gas is the cubic real gas.  A compile-time switch, so the
+// ideal gases' kernels carry none of its registers.
+
 // frompT: the calorically perfect (peregrine/simulator/mixture/eos/cpg/kernels/eos.mako:17-27),
 // the thermally perfect (peregrine/simulator/mixture/eos/tpg/kernels/eos.mako:22-32)
 // or the real gas (realgas.cuh)
-template <int NS, class YF>
+template <int NS, class YF, bool RG = false>
 __device__ __forceinline__ State frompT(const double p, const double T, YF Y) {
-  if (kSp.realgas) return frompT_rg_state<NS>(p, T, Y);
+  if (RG) return frompT_rg_state<NS>(p, T, Y);
   State s;
   s.p = p;
   s.T = T;
@@ -281,7 +284,7 @@ __device__ __forceinline__ State fromprims(const double *q, double *Q) {
 template <int NS, class YF>
 __device__ __forceinline__ void hspecies_rg_of(double *h, YF Y, const double p, const double T, const double Z);
 
-template <int NS, class QF>
+template <int NS, class QF, bool RG = false>
 __device__ __forceinline__ void transport(QF Q, const State &st, double *tr, double *hsp, const double Z = 0.0) {
   const double rho = Q(0), rhoinv = 1.0 / rho;
   double Ylast = 1.0;
@@ -344,7 +347,7 @@ __device__ __forceinline__ void transport(QF Q, const State &st, double *tr, dou
   for (int n = 0; n < NS; n++) tr[2 + n] = kor / kSp.lewis[n];
   // hspecies: the real gas's partial enthalpies at the stored state, or the
   // ideal ones (peregrine/simulator/mixture/eos/kernels/species.mako:9-15, 31-36)
-  if (kSp.realgas) {
+  if (RG) {
     hspecies_rg_of<NS>(hsp, [&](int n) { return Q(5 + n) * rhoinv; }, st.p, T, Z);
     return;
   }
@@ -397,9 +400,10 @@ struct RSide {
 };
 
 // frompT onto a side (the eos's frompT)
-template <int NS>
+template <int NS, bool RG = false>
 __device__ __forceinline__ void side_frompT(const double p, const double T, const double *Y, RSide &s) {
-  const State th = frompT<NS>(p, T, [&](int n) { return Y[n]; });
+  auto Yf = [&](int n) { return Y[n]; };
+  const State th = frompT<NS, decltype(Yf), RG>(p, T, Yf);
   s.p = th.p;
   s.rho = th.rho;
   s.e = th.e;

@@ -36,7 +36,7 @@ __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi,
 // gas its fromrhoE and root Z; with plane set, the double flux's fromplane:
 // p off the cell's frozen plane, then the state at rho and p
 // (peregrine/simulator/eulerdf/kernels/fromplane.mako:3-17)
-template <int NS>
+template <int NS, bool RG = false>
 __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                         double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr, const int plane = 0) {
   PGB_WHERE(B, t);
@@ -46,7 +46,7 @@ __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *
   const long long v = B.vol;
   auto Qf = [&](int c) { return Q[c * v]; };
   State s;
-  if (kSp.realgas) {
+  if (RG) {
     const double rho = Qf(0), rhoinv = 1.0 / rho;
     auto Y = [&](int n) { return Qf(5 + n) * rhoinv; };
     const RGMom mom = mixmom_rg<NS>(Y);
@@ -121,7 +121,7 @@ __device__ __forceinline__ State load_state(const double *st, long long v) {
 
 // transport over the whole block: trstate[2 + ns] and hsp[ns] per cell
 // (peregrine/simulator/navstokes/kernels/transport.mako:5-35)
-template <int NS>
+template <int NS, bool RG = false>
 __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                             const double *__restrict__ stall, double *__restrict__ trall,
                             double *__restrict__ hall, const int2 *__restrict__ ctab = nullptr) {
@@ -130,7 +130,8 @@ __global__ void k_transport(const BlockDev *__restrict__ blks, int b, const doub
   const double *Q = Qall + (4 + NS) * B.cv + t;
   const State s = load_state(stall + SW * B.cv + t, B.vol);
   double tr[2 + NS], h[NS];
-  transport<NS>([&](int c) { return Q[c * B.vol]; }, s, tr, h, stall[SW * B.cv + ST_Z * B.vol + t]);
+  auto Qf = [&](int c) { return Q[c * B.vol]; };
+  transport<NS, decltype(Qf), RG>(Qf, s, tr, h, stall[SW * B.cv + ST_Z * B.vol + t]);
   double *trp = trall + (2 + NS) * B.cv + t;
   double *hp = hall + NS * B.cv + t;
 #pragma unroll
@@ -301,7 +302,7 @@ __global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const dou
 // (lim 0; recon/constant.mako:3-18) or on MUSCL's sides under limiter lim
 // (recon/muscl.mako:15-51), both sides from the four cells LL, L, R, RR
 // along the axis (peregrine/simulator/euler/kernels/flux/single.mako:4-9)
-template <int NS, int A, int FN>
+template <int NS, int A, int FN, bool RG = false>
 __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                           const double *__restrict__ stall, const double *__restrict__ met,
                           double *__restrict__ Fall, const int lim,
@@ -347,8 +348,8 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
     const double TR = muscl_right(lim, st[v + L], st[v + R], st[v + RR]);
 #pragma unroll
     for (int n = 0; n < NS - 1; n++) YL[n] = lft(5 + n), YR[n] = rgt(5 + n);
-    side_frompT<NS>(pL, TL, YL, sl);
-    side_frompT<NS>(pR, TR, YR, sr);
+    side_frompT<NS, RG>(pL, TL, YL, sl);
+    side_frompT<NS, RG>(pR, TR, YR, sr);
     sl.u = lft(1), sl.v = lft(2), sl.w = lft(3);
     sr.u = rgt(1), sr.v = rgt(2), sr.w = rgt(3);
   }
@@ -540,7 +541,7 @@ static __global__ void k_combine(const BlockDev *__restrict__ blks, int b, int n
 
 // Q and the state from primitives on the interior (the reference's fromprims);
 // the stored T is the next fromQ's starting guess
-template <int NS>
+template <int NS, bool RG = false>
 __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const double *__restrict__ prims,
                             double *__restrict__ Qall, double *__restrict__ stall) {
   constexpr int NE = 4 + NS;
@@ -555,7 +556,7 @@ __global__ void k_fromprims(const BlockDev *__restrict__ blks, int b, const doub
   for (int l = 0; l < NE; l++) q[l] = prims[l * n + t];
   State th;
   double Z = 0.0;
-  if (kSp.realgas) {
+  if (RG) {
     const RGState o = frompT_rg<NS>(q[0], q[4], [&](int n) { return q[5 + n]; });
     th = o.s;
     Z = o.Z;

@@ -33,6 +33,7 @@ struct PlainCase {
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
   int visc, primary, recon, limiter, chem;
+  int realgas;  // the cubic real gas: the kernels built for it
   int df;      // the double flux: fromplane in the stages, two energy rows per face (F holds NE + 1 rows)
   int packed;  // 1: each pass is one launch over every block
   // with packing, each range's tile table (cells with halo, interior cells,

@@ -65,6 +65,16 @@ struct RhsArgs {
   double *dQ;
 };
 
+template <int A, bool RG>
+void riemann_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const RhsArgs &a, int lim) {
+  cudaStream_t s = pc->stream;
+  switch (pc->primary) {
+    case PGB_FLUX_HLLC: k_riemann<NS, A, FN_HLLC, RG><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
+    case PGB_FLUX_RUSANOV: k_riemann<NS, A, FN_RUSANOV, RG><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
+    default: k_riemann<NS, A, FN_AUSMUP, RG><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
+  }
+}
+
 template <int A>
 void adv_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
@@ -74,11 +84,12 @@ void adv_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *
     k_advflux_df<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
     return;
   }
-  switch (pc->primary) {
-    case PGB_FLUX_HLLC: k_riemann<NS, A, FN_HLLC><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
-    case PGB_FLUX_RUSANOV: k_riemann<NS, A, FN_RUSANOV><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
-    case PGB_FLUX_AUSMUP: k_riemann<NS, A, FN_AUSMUP><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct); break;
-    default: k_advflux<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
+  if (pc->primary == PGB_FLUX_KEPAEC) {
+    k_advflux<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
+  } else if (pc->realgas) {
+    riemann_launch<A, true>(pc, b, g, ct, a, lim);
+  } else {
+    riemann_launch<A, false>(pc, b, g, ct, a, lim);
   }
 }
 
@@ -90,11 +101,17 @@ void diff_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void 
 
 void fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_fromQ<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, pc->df);
+  if (pc->realgas)
+    k_fromQ<NS, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, pc->df);
+  else
+    k_fromQ<NS, false><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, 0);
 }
 void transport_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_transport<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, ct);
+  if (pc->realgas)
+    k_transport<NS, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, ct);
+  else
+    k_transport<NS, false><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, ct);
 }
 void grads_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
@@ -217,7 +234,10 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
 // Q and the state of one block's interior from its primitives
 extern "C" int PGB_ENTRY(pgb_plain_fromprims_)(const PlainCase *pc, int blk, const double *prims, double *Q) {
   const BlockDev &D = pc->h_blks[blk];
-  k_fromprims<NS><<<grid_of((long long)D.nx * D.ny * D.nz), TH, 0, pc->stream>>>(pc->d_blks, blk, prims, Q, pc->state);
+  if (pc->realgas)
+    k_fromprims<NS, true><<<grid_of((long long)D.nx * D.ny * D.nz), TH, 0, pc->stream>>>(pc->d_blks, blk, prims, Q, pc->state);
+  else
+    k_fromprims<NS, false><<<grid_of((long long)D.nx * D.ny * D.nz), TH, 0, pc->stream>>>(pc->d_blks, blk, prims, Q, pc->state);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "fromprims");
 }
@@ -239,7 +259,7 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
   cudaStream_t s = pc->stream;
   for (int b = 0; b < pc->nblocks; b++) {
     const BlockDev &D = pc->h_blks[b];
-    k_fromQ<NS><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, nullptr, first ? 0 : 1);
+    k_fromQ<NS, true><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, nullptr, first ? 0 : 1);
     mark(pc, 2);
     k_freeze<NS><<<grid_of(range_size(D, R_INNER)), TH, 0, s>>>(pc->d_blks, b, Q, pc->state);
     mark(pc, 2);
