@@ -130,13 +130,58 @@ typedef struct {
   int step;
 } pgb_combine;
 
-/* One stage: the register its right-hand side reads, the combines after it */
+/* One stage: the register its right-hand side reads, the combines after it,
+ * and the stage's time as a fraction of dt past the step's start, the clock
+ * its boundary values read (peregrine/integrators/rungekutta.py:28-39) */
 typedef struct {
   int q;
   int dq;         /* the logical register holding dQ on the per-block path */
   int ncombine;   /* 1 or 2 */
   pgb_combine combine[2];
+  double tfrac;
 } pgb_stage;
+
+/* Boundary kinds: the reference's bcvals kinds
+ * (peregrine/simulator/euler/bcs.py, peregrine/simulator/navstokes/bcs.py).
+ * The values an entry gives, in order (each a program, below):
+ *   SLIP_ADIA_WALL, NOSLIP_ADIA_WALL, SUP_OUT_FN: none
+ *   SLIP_ISOT_WALL, NOSLIP_ISOT_WALL: T      MOV_ADIA_WALL: u v w
+ *   MOV_ISOT_WALL: u v w T                    SUB_OUT_FP: p
+ *   SUB_IN_FVT: u v w T, Y[ns - 1]            SUP_IN_FA: p u v w T, Y[ns - 1]
+ *   SUB_IN_FTPTT: pt Tt, Y[ns - 1]            SUB_IN_FMT: mflux T, Y[ns - 1]
+ * The no-slip and moving walls are the Navier-Stokes simulator's. */
+enum {
+  PGB_BC_SLIP_ADIA_WALL = 1,   /* slp-adia-wall */
+  PGB_BC_SLIP_ISOT_WALL = 2,   /* slp-isot-wall */
+  PGB_BC_NOSLIP_ADIA_WALL = 3, /* no-slp-adia-wall */
+  PGB_BC_MOV_ADIA_WALL = 4,    /* mov-adia-wall */
+  PGB_BC_NOSLIP_ISOT_WALL = 5, /* no-slp-isot-wall */
+  PGB_BC_MOV_ISOT_WALL = 6,    /* mov-isot-wall */
+  PGB_BC_SUB_IN_FVT = 7,       /* sub-in-fvt */
+  PGB_BC_SUP_IN_FA = 8,        /* sup-in-fa */
+  PGB_BC_SUB_IN_FTPTT = 9,     /* sub-in-ftptt */
+  PGB_BC_SUB_IN_FMT = 10,      /* sub-in-fmt */
+  PGB_BC_SUB_OUT_FP = 11,      /* sub-out-fp */
+  PGB_BC_SUP_OUT_FN = 12,      /* sup-out-fn */
+  PGB_BC_NKINDS = 13
+};
+
+/* A boundary value is a program for a small stack machine, evaluated at each
+ * boundary face's centre (x, y, z) and the stage's time t: the reference's
+ * expressions of x, y, z and t (peregrine/simulator/bcs.py:101-143) in
+ * postfix.  CONST pushes its argument; X Y Z T push the coordinate or time;
+ * the binary operations pop b then a and push a op b; the functions pop
+ * their arguments the same way.  A program leaves one value and never holds
+ * more than PGB_BC_STACK. */
+enum {
+  PGB_OP_CONST = 0, PGB_OP_X, PGB_OP_Y, PGB_OP_Z, PGB_OP_T,
+  PGB_OP_ADD, PGB_OP_SUB, PGB_OP_MUL, PGB_OP_DIV, PGB_OP_NEG, PGB_OP_POW,
+  PGB_OP_SIN, PGB_OP_COS, PGB_OP_TAN, PGB_OP_EXP, PGB_OP_LOG, PGB_OP_SQRT, PGB_OP_TANH,
+  PGB_OP_ABS, PGB_OP_MIN, PGB_OP_MAX,
+  PGB_NOPS
+};
+#define PGB_BC_STACK 16
+#define PGB_BC_MAXOPS 4096
 
 /* library */
 const char *pgb_last_error(void);
@@ -173,6 +218,21 @@ int pgb_case_add_block(pgb_case *c, int ni, int nj, int nk, int *blk);
  * face nbrface of nbr, orientation "123" (the lattice meshers' only one,
  * peregrine/mesher/base.py:117-133); nbr -1 is a boundary */
 int pgb_case_connect(pgb_case *c, int blk, int nface, int nbr, int nbrface);
+/* A boundary entry (one entry of the reference's bcvals,
+ * peregrine/simulator/bcs.py:10-98): its kind (PGB_BC_*) and its values, value
+ * v the program ops[starts[v] .. starts[v + 1]) with args the CONST operands
+ * (one per op, read for CONST alone).  nvalues is what the kind reads for the
+ * case's species.  Before finalize; *id numbers the entry. */
+int pgb_case_add_bc(pgb_case *c, int kind, const int *ops, const double *args, const int *starts, int nvalues,
+                    int *id);
+/* A boundary face (connected with nbr -1) takes entry bc: the reference's
+ * interface named in bcvals (peregrine/multiblock/solver.py:157-173).  A
+ * boundary face given no entry keeps its halo as set.  Before finalize. */
+int pgb_case_set_face_bc(pgb_case *c, int blk, int nface, int bc);
+/* the case's clock, the t boundary values read at a step's start
+ * (peregrine/multiblock/solver.py:35, 355-364); a step moves it on by dt */
+int pgb_set_time(pgb_case *c, double t);
+int pgb_get_time(pgb_case *c, double *t);
 /* the integrator's stages, in order */
 int pgb_case_set_stages(pgb_case *c, const pgb_stage *stages, int nstages);
 /* allocate the device arrays, build halo tables and work lists */
@@ -191,6 +251,11 @@ int pgb_metric_set(pgb_case *c, int blk, int which, const double *host, long cou
  * outermost), interior only.  Logical register reg. */
 int pgb_array_set(pgb_case *c, int blk, int reg, const double *host, long count);
 int pgb_array_get(pgb_case *c, int blk, int reg, double *host, long count);
+/* The same register with its halo: full extents (nx+4, ny+4, nz+4), F order,
+ * count = ne x full cells.  The halo holds what the last right-hand side
+ * left there (exchanged, or set by a boundary); its edges and corners are
+ * never read (the reference's full host view, peregrine/backend/allocation.py) */
+int pgb_array_get_full(pgb_case *c, int blk, int reg, double *host, long count);
 
 /* Every block's interior cells of register reg at once: the blocks' F-order
  * interior arrays end to end, in block order (count = ne x total cells). */

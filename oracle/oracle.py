@@ -15,6 +15,7 @@ reference's solver drives its kernels:
   one right-hand side, then each stage's combine kernels in order.
 """
 
+import ast
 import ctypes
 import os
 
@@ -24,6 +25,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
 _halo_dtype = np.dtype([(n, np.int32) for n in ("dblk", "di", "dj", "dk", "sblk", "si", "sj", "sk", "layer")])
+
+
+class OBc(ctypes.Structure):
+    _fields_ = [("blk", ctypes.c_int), ("nface", ctypes.c_int), ("kind", ctypes.c_int), ("nval", ctypes.c_int),
+                ("vals", ctypes.POINTER(ctypes.c_double))]
 
 
 class OCase(ctypes.Structure):
@@ -39,7 +45,56 @@ class OCase(ctypes.Structure):
                 ("realgas", ctypes.c_int), ("df", ctypes.c_int)] + \
                [(n, ctypes.c_double) for n in ("cu", "cw", "csigma", "ceps")] + \
                [(n, ctypes.POINTER(ctypes.c_double)) for n in
-                ("csqrtac", "cb", "cda", "cmTc", "conepm", "vshift", "csqrtacMW", "cbMW", "cdaMW", "vshiftMW")]
+                ("csqrtac", "cb", "cda", "cmTc", "conepm", "vshift", "csqrtacMW", "cbMW", "cdaMW", "vshiftMW")] + \
+               [("nbc", ctypes.c_int), ("bc", ctypes.POINTER(OBc))]
+
+# the boundary kinds (peregrine/simulator/euler/bcs.py, navstokes/bcs.py): the
+# oracle's number for each and the variables an entry gives, in order; the
+# inflows' carried species follow them
+BC_KINDS = {"slp-adia-wall": (1, ()), "slp-isot-wall": (2, ("T",)), "no-slp-adia-wall": (3, ()),
+            "mov-adia-wall": (4, ("u", "v", "w")), "no-slp-isot-wall": (5, ("T",)),
+            "mov-isot-wall": (6, ("u", "v", "w", "T")), "sub-in-fvt": (7, ("u", "v", "w", "T")),
+            "sup-in-fa": (8, ("p", "u", "v", "w", "T")), "sub-in-ftptt": (9, ("pt", "Tt")),
+            "sub-in-fmt": (10, ("mflux", "T")), "sub-out-fp": (11, ("p",)), "sup-out-fn": (12, ())}
+BC_INLETS = ("sub-in-fvt", "sup-in-fa", "sub-in-ftptt", "sub-in-fmt")
+
+_NP_FUNCS = dict(sin=np.sin, cos=np.cos, tan=np.tan, exp=np.exp, log=np.log, sqrt=np.sqrt, tanh=np.tanh,
+                 abs=np.abs, min=np.minimum, max=np.maximum, pow=np.power)
+
+
+def bc_value(value, x, y, z, t):
+    """A bcvals value at face centres x, y, z and time t: a number, or an
+    expression of x, y, z and t (peregrine/simulator/bcs.py:101-143) evaluated
+    here by numpy, on its own, as the reference's compiled C++ would."""
+    if not isinstance(value, str):
+        return np.full(x.shape, float(value))
+    names = dict(x=x, y=y, z=z, t=t)
+
+    def ev(node):
+        if isinstance(node, ast.Constant):
+            return float(node.value)
+        if isinstance(node, ast.Name):
+            return names[node.id]
+        if isinstance(node, ast.UnaryOp):
+            return -ev(node.operand) if isinstance(node.op, ast.USub) else ev(node.operand)
+        if isinstance(node, ast.BinOp):
+            a, b = ev(node.left), ev(node.right)
+            if isinstance(node.op, ast.Pow):
+                return np.power(a, b)
+            return {ast.Add: np.add, ast.Sub: np.subtract, ast.Mult: np.multiply, ast.Div: np.divide}[type(node.op)](a, b)
+        if isinstance(node, ast.Call):
+            return _NP_FUNCS[node.func.id](*[ev(a) for a in node.args])
+        raise ValueError(f"{value!r}: {type(node).__name__}")
+
+    return np.broadcast_to(np.asarray(ev(ast.parse(value, mode="eval").body), dtype=np.float64), x.shape)
+
+
+def stage_fractions(integrator):
+    """Each stage's time as a fraction of dt past the step's start
+    (peregrine/integrators/rungekutta.py:28-39: stage n's right-hand side runs
+    at the n-th stage table row's fraction)."""
+    return {"rk1": (0.0,), "rk2": (0.0, 1.0), "tvd-rk3": (0.0, 1.0, 0.5), "rk34": (0.0, 0.5, 1.0, 0.5),
+            "rk4": (0.0, 0.5, 0.5, 1.0)}[integrator]
 
 NSTATE = 24  # the oracle's per-cell record: EosState, Z, the double flux's plane
 
@@ -148,7 +203,7 @@ def _lib():
     lib.oracle_advective_faces.restype = ctypes.c_int
     for name in ("oracle_production", "oracle_gibbs", "oracle_tlog", "oracle_texp", "oracle_mathtables",
                  "oracle_species_cph", "oracle_fromQ", "oracle_prestep", "oracle_realgas_frompT",
-                 "oracle_realgas_fromQ", "oracle_freeze"):
+                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 
@@ -256,10 +311,15 @@ class Oracle:
     LIMITERS = {None: 0, "koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
 
     def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0, primary="kepaec",
-                 recon="constant", limiter=None, eos="cpg", trans="constant", chemistry=None):
+                 recon="constant", limiter=None, eos="cpg", trans="constant", chemistry=None, bcvals=None,
+                 species=None):
         """constants: the mixture's tables; blocks/metrics may be empty for face-only use.
         eos "cpg" or "tpg", trans "constant" or "kinetic-theory", chemistry
-        None or "finite-rate" (coupled: the source begins dQ)."""
+        None or "finite-rate" (coupled: the source begins dQ).  bcvals: the
+        config's boundary entries, by the name each boundary face carries
+        (face.bcname); species: the mixture's species names, for the
+        inflows' mass fractions.  A boundary face without a name keeps its
+        halo as set."""
         self.lib = _lib()
         self.ns, self.ne = ns, 4 + ns
         self.blocks = blocks
@@ -322,6 +382,40 @@ class Oracle:
         self.df = eos == "real-gas-df"
         self.pst = [np.zeros(self._shape(b)[:3] + (NSTATE,)) for b in blocks] if self.df else None
         self.df_fresh = True
+        self.tme = 0.0
+        self.bcvals = dict(bcvals or {})
+        self.species = list(species or [])
+        self.bcfaces = []
+        for blk in blocks:
+            for face in blk.intfaces:
+                if face.nbr is None and face.bcname is not None:
+                    if face.bcname not in self.bcvals:
+                        raise ValueError(f"block {blk.nblki} face {face.nface}: {face.bcname!r} is not in bcvals")
+                    self.bcfaces.append((blk, face))
+
+    def _bcs(self, t):
+        """The boundary faces with their values at the face centres and time t."""
+        rows = (OBc * max(1, len(self.bcfaces)))()
+        keep = []
+        for m, (blk, face) in enumerate(self.bcfaces):
+            given = self.bcvals[face.bcname]
+            kind, variables = BC_KINDS[given["kind"]]
+            names = list(variables)
+            if given["kind"] in BC_INLETS:
+                names += self.species[:self.ns - 1]
+            a, g, n = face.axis, blk.ng, blk.cells
+            xc = self.metrics[blk.nblki]["ijk"[a] + "xc"]
+            at = [slice(g, g + n[d]) for d in range(3)]
+            at[a] = g if face.is_low else g + n[a]
+            plane = xc[tuple(at)]
+            x, y, z = plane[..., 0], plane[..., 1], plane[..., 2]
+            cols = [bc_value(given.get(v, 0.0) if v not in variables else given[v], x, y, z, t) for v in names]
+            vals = np.ascontiguousarray(np.stack(cols, -1) if cols else np.zeros(x.shape + (1,)), dtype=np.float64)
+            keep.append(vals)
+            r = rows[m]
+            r.blk, r.nface, r.kind, r.nval = blk.nblki, face.nface, kind, max(1, len(names))
+            r.vals = _ptr(vals)
+        return rows, keep
 
     def _shape(self, blk):
         return tuple(n + 2 * blk.ng for n in blk.cells) + (self.ne,)
@@ -384,9 +478,12 @@ class Oracle:
         self.lib.oracle_fromQ(ctypes.byref(self.case), ctypes.c_long(len(Tg)), _ptr(Q), _ptr(Tg), _ptr(out))
         return out
 
-    def rhs(self, Q, dQ, faces=False, diffusive_only=False):
-        """dQ of every block from Q; with faces, each block's [iF, jF, kF] too."""
+    def rhs(self, Q, dQ, faces=False, diffusive_only=False, t=None):
+        """dQ of every block from Q; with faces, each block's [iF, jF, kF] too.
+        t: the time the boundary values read (the oracle's clock if None)."""
         obs = self._oblocks(Q)
+        bcs, keep = self._bcs(self.tme if t is None else t)
+        self.case.nbc, self.case.bc = len(self.bcfaces), bcs
         m = np.ascontiguousarray(self.map)
         ptrs = (ctypes.POINTER(ctypes.c_double) * len(dQ))(*[_ptr(d) for d in dQ])
         fl, fptr = None, None
@@ -409,6 +506,15 @@ class Oracle:
             raise RuntimeError(f"oracle_rhs: {rc}")
         if faces:
             return [fl[3 * b:3 * b + 3] for b in range(len(self.blocks))]
+
+    def bc_grads(self, grads, t=None):
+        """The boundaries' gradient hook alone on grads[b] ([X][Y][Z][ngrad][3]
+        per block), in place."""
+        bcs, keep = self._bcs(self.tme if t is None else t)
+        self.case.nbc, self.case.bc = len(self.bcfaces), bcs
+        obs = self._oblocks(self.regs[0])
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(grads))(*[_ptr(g) for g in grads])
+        self.lib.oracle_bc_grads(ctypes.byref(self.case), obs, ptrs)
 
     def advective_faces(self, QLL, QL, QR, QRR, S):
         """The advective flux on independent faces from their four cells' Q."""
@@ -457,12 +563,14 @@ class Oracle:
     def step(self, dt):
         names = list(range(self.nregs))
         stages, dQ = stage_combines(self.integrator, names)
+        start = self.tme
+        fracs = stage_fractions(self.integrator)
         if self.df:
             if self.df_fresh:
                 self.prestep(self.regs[stages[0][0]])
             self.prestep(self.regs[stages[0][0]])
-        for Q, combines in stages:
-            self.rhs(self.regs[Q], self.regs[dQ])
+        for n, (Q, combines) in enumerate(stages):
+            self.rhs(self.regs[Q], self.regs[dQ], t=start + fracs[n] * dt)
             for out, own, reads, step in combines:
                 for b, blk in enumerate(self.blocks):
                     X = (ctypes.POINTER(ctypes.c_double) * len(reads))(*[_ptr(self.regs[r][b]) for r, _ in reads])
@@ -470,6 +578,7 @@ class Oracle:
                     self.lib.oracle_combine(*blk.cells, blk.ng, self.ne, _ptr(self.regs[out][b]),
                                             int(own is not None), ctypes.c_double(own or 0.0),
                                             len(reads), X, w, int(step), ctypes.c_double(dt))
+        self.tme = start + dt
 
 
 def tlog(x):

@@ -25,6 +25,17 @@ extern "C" {
 enum { O_EULER = 0, O_NAVSTOKES = 1 };
 enum { O_KEPAEC = 0, O_HLLC = 1, O_RUSANOV = 2, O_AUSMUP = 3 };
 
+// one boundary face: block, face (1..6, i-low .. k-high), kind (1..12 in the
+// order slp-adia-wall, slp-isot-wall, no-slp-adia-wall, mov-adia-wall,
+// no-slp-isot-wall, mov-isot-wall, sub-in-fvt, sup-in-fa, sub-in-ftptt,
+// sub-in-fmt, sub-out-fp, sup-out-fn) and the entry's values at the face's
+// cells, vals[p][q][nval] with p the lower in-plane axis's interior index
+// (the caller evaluates the values at the face centres and the stage's time)
+struct OBc {
+  int blk, nface, kind, nval;
+  const double *vals;
+};
+
 struct OCase {
   int simulator;   // O_EULER / O_NAVSTOKES
   int primary;     // flux function
@@ -49,6 +60,8 @@ struct OCase {
   int realgas, df;           // the cubic real gas; its double flux (euler-df)
   double cu, cw, csigma, ceps;
   const double *csqrtac, *cb, *cda, *cmTc, *conepm, *vshift, *csqrtacMW, *cbMW, *cdaMW, *vshiftMW;  // [ns]
+  int nbc;                   // boundary faces; a boundary face not listed keeps its halo as set
+  const OBc *bc;
 };
 
 // one reaction, the columns of FiniteRateModel.rxnconsts
@@ -1258,6 +1271,317 @@ struct Scratch {
   std::vector<double> state, tr, hsp, grads, F[3];
 };
 
+// ---- boundaries: each kind's preadvflux on the halo cells behind its faces,
+// the inflows' and outflows' postgrads, the walls' postflux
+// (simulator/euler/kernels/bcs/*.mako, simulator/navstokes/kernels/bcs/*.mako,
+// on the carried offsets of launch/policy.py:143-232: "interior" the first
+// cell in whatever the layer, "mirror" layer l's image l deep, clamped to the
+// block's depth, "mirror1" one deeper, "intface" the boundary face) ----
+enum { B_SLIP_ADIA = 1, B_SLIP_ISOT, B_NOSLIP_ADIA, B_MOV_ADIA, B_NOSLIP_ISOT, B_MOV_ISOT, B_SUB_IN_FVT, B_SUP_IN_FA,
+       B_SUB_IN_FTPTT, B_SUB_IN_FMT, B_SUB_OUT_FP, B_SUP_OUT_FN };
+
+bool bc_wall(int kind) { return kind >= B_SLIP_ADIA && kind <= B_MOV_ISOT; }
+
+// a boundary face's cells: the full index along its axis a of the cell d
+// deep, of halo layer l and of the face; the in-plane axes a1 < a2
+struct BFace {
+  int a, a1, a2, g;
+  bool low;
+  int n[3];
+  BFace(const OBlock &B, int nface) {
+    a = (nface - 1) / 2;
+    low = nface % 2 == 1;
+    a1 = a == 0 ? 1 : 0;
+    a2 = a == 2 ? 1 : 2;
+    g = B.ng;
+    n[0] = B.nx, n[1] = B.ny, n[2] = B.nz;
+  }
+  int deep(int d) const {
+    d = std::min(d, n[a] - 1);
+    return low ? g + d : g + n[a] - 1 - d;
+  }
+  int halo(int l) const { return low ? g - 1 - l : g + n[a] + l; }
+  int face() const { return low ? g : g + n[a]; }
+  long at(const Dims &d, int p, int q, int along) const {
+    int c[3];
+    c[a] = along, c[a1] = g + p, c[a2] = g + q;
+    return d.at(c[0], c[1], c[2]);
+  }
+};
+
+// fromprims into a cell's Q and record (simulator/euler/kernels/solution.mako:14-23)
+void bc_fromprims(const OCase &c, double p, double T, const double *u, const double *Y, double *Q, double *rec) {
+  double Z = 0.0;
+  State th;
+  if (c.realgas)
+    th = rfrompT(c, p, T, [&](int n) { return Y[n]; }, Z);
+  else
+    th = frompT(c, p, T, Y);
+  Q[0] = th.rho;
+  Q[1] = th.rho * u[0];
+  Q[2] = th.rho * u[1];
+  Q[3] = th.rho * u[2];
+  Q[4] = th.rho * (th.e + 0.5 * ((u[0]) * (u[0]) + (u[1]) * (u[1]) + (u[2]) * (u[2])));
+  for (int n = 0; n < c.ns - 1; n++) Q[5 + n] = th.rho * Y[n];
+  std::memcpy(rec, &th, sizeof(State));
+  rec[S_Z] = Z;
+}
+
+// a face's unit normal scaled by sign (outward[0] for the outward one)
+void unit_normal(const double *S, double sign, double *nrm) {
+  const double Sinv = sign / std::sqrt((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2]));
+  for (int d = 0; d < 3; d++) nrm[d] = S[d] * Sinv;
+}
+
+// the outflows' velocity (sub-out-fp.mako:17-30, sup-out-fn.mako:22-35)
+void outflow_velocity(const double *Qi, double rhoinv, const double *Qm, const double *Qm1, const double *nrm,
+                      double *u) {
+  const double u0[3] = {Qi[1] * rhoinv, Qi[2] * rhoinv, Qi[3] * rhoinv};
+  const double un = u0[0] * nrm[0] + u0[1] * nrm[1] + u0[2] * nrm[2];
+  if (un > 0.0) {
+    const double rhoinv1 = 1.0 / Qm1[0];
+    for (int d = 0; d < 3; d++) u[d] = 2.0 * u0[d] - Qm1[1 + d] * rhoinv1;
+  } else {
+    const double rhoinvm = 1.0 / Qm[0];
+    const double um[3] = {Qm[1] * rhoinvm, Qm[2] * rhoinvm, Qm[3] * rhoinvm};
+    const double umn = 2.0 * (um[0] * nrm[0] + um[1] * nrm[1] + um[2] * nrm[2]);
+    for (int d = 0; d < 3; d++) u[d] = um[d] - umn * nrm[d];
+  }
+}
+
+// preadvflux of one boundary face: Q and the record of every halo cell behind it
+void bc_halo(const OCase &c, OBlock &B, std::vector<double> &state, const OBc &bc) {
+  const int ne = 4 + c.ns, ns = c.ns;
+  const BFace w(B, bc.nface);
+  const Dims d = cells(B), fd = face_dims(B, w.a);
+  const double outward = w.low ? -1.0 : 1.0;
+  for (int l = 0; l < B.ng; l++)
+    for (int p = 0; p < w.n[w.a1]; p++)
+      for (int q = 0; q < w.n[w.a2]; q++) {
+        const double *v = bc.vals + ((long)p * w.n[w.a2] + q) * bc.nval;
+        const long ci = w.at(d, p, q, w.deep(0)), cm = w.at(d, p, q, w.deep(l)), cm1 = w.at(d, p, q, w.deep(l + 1));
+        const long ch = w.at(d, p, q, w.halo(l));
+        const double *S = B.S[w.a] + w.at(fd, p, q, w.face()) * 3;
+        const double *Qi = B.Q + ci * ne, *Qm = B.Q + cm * ne, *Qm1 = B.Q + cm1 * ne;
+        const double *si = &state[ci * NSTATE], *sm = &state[cm * NSTATE], *sm1 = &state[cm1 * NSTATE];
+        double *Qh = B.Q + ch * ne, *sh = &state[ch * NSTATE];
+        double Y[16], u[3];
+        switch (bc.kind) {
+          case B_SLIP_ADIA: {  // slp-adia-wall.mako:4-22
+            double nrm[3];
+            unit_normal(S, 1.0, nrm);
+            const double mn = 2.0 * (Qm[1] * nrm[0] + Qm[2] * nrm[1] + Qm[3] * nrm[2]);
+            Qh[0] = Qm[0];
+            for (int e = 0; e < 3; e++) Qh[1 + e] = Qm[1 + e] - mn * nrm[e];
+            Qh[4] = Qm[4];
+            for (int n = 0; n < ns - 1; n++) Qh[5 + n] = Qm[5 + n];
+            std::memcpy(sh, sm, sizeof(double) * NSTATE);
+            break;
+          }
+          case B_NOSLIP_ADIA:
+          case B_MOV_ADIA: {  // navstokes/kernels/bcs/wall.mako:7-25, stuckhalo
+            const bool mov = bc.kind == B_MOV_ADIA;
+            const double rho = Qm[0], rhoinv = 1.0 / rho;
+            double ke = 0.0, kehalo = 0.0;
+            for (int e = 0; e < 3; e++) {
+              const double ue = Qm[1 + e] * rhoinv, uh = 2.0 * (mov ? v[e] : 0.0) - ue;
+              Qh[1 + e] = rho * uh;
+              ke += ue * ue;
+              kehalo += uh * uh;
+            }
+            Qh[0] = rho;
+            Qh[4] = Qm[4] + 0.5 * rho * (kehalo - ke);
+            for (int n = 0; n < ns - 1; n++) Qh[5 + n] = Qm[5 + n];
+            std::memcpy(sh, sm, sizeof(double) * NSTATE);
+            break;
+          }
+          case B_SLIP_ISOT: {  // slp-isot-wall.mako:5-20
+            double nrm[3];
+            unit_normal(S, 1.0, nrm);
+            const double rhoinv = 1.0 / Qm[0];
+            const double ui = Qm[1] * rhoinv, vi = Qm[2] * rhoinv, wi = Qm[3] * rhoinv;
+            const double un = 2.0 * (ui * nrm[0] + vi * nrm[1] + wi * nrm[2]);
+            u[0] = ui - un * nrm[0], u[1] = vi - un * nrm[1], u[2] = wi - un * nrm[2];
+            for (int n = 0; n < ns - 1; n++) Y[n] = Qm[5 + n] * rhoinv;
+            bc_fromprims(c, sm[0], v[0], u, Y, Qh, sh);
+            break;
+          }
+          case B_NOSLIP_ISOT:
+          case B_MOV_ISOT: {  // wall.mako:27-38, stuckhaloisot
+            const bool mov = bc.kind == B_MOV_ISOT;
+            const double rhoinv = 1.0 / Qm[0];
+            for (int e = 0; e < 3; e++) u[e] = 2.0 * (mov ? v[e] : 0.0) - Qm[1 + e] * rhoinv;
+            for (int n = 0; n < ns - 1; n++) Y[n] = Qm[5 + n] * rhoinv;
+            bc_fromprims(c, sm[0], mov ? v[3] : v[0], u, Y, Qh, sh);
+            break;
+          }
+          case B_SUB_IN_FVT: {  // sub-in-fvt.mako:4-14
+            const double pp = 2.0 * si[0] - sm1[0];
+            for (int e = 0; e < 3; e++) u[e] = v[e];
+            for (int n = 0; n < ns - 1; n++) Y[n] = v[4 + n];
+            bc_fromprims(c, pp, v[3], u, Y, Qh, sh);
+            break;
+          }
+          case B_SUP_IN_FA: {  // sup-in-fa.mako:4-13
+            for (int e = 0; e < 3; e++) u[e] = v[1 + e];
+            for (int n = 0; n < ns - 1; n++) Y[n] = v[5 + n];
+            bc_fromprims(c, v[0], v[4], u, Y, Qh, sh);
+            break;
+          }
+          case B_SUB_IN_FMT: {  // sub-in-fmt.mako:4-30
+            double nrm[3];
+            unit_normal(S, -outward, nrm);
+            const double pp = 2.0 * si[0] - sm1[0], T = v[1];
+            for (int n = 0; n < ns - 1; n++) Y[n] = v[2 + n];
+            double Z = 0.0;
+            State th;
+            if (c.realgas)
+              th = rfrompT(c, pp, T, [&](int n) { return Y[n]; }, Z);
+            else
+              th = frompT(c, pp, T, Y);
+            const double rhoinv = 1.0 / Qi[0];
+            const double scale = 4.0 * v[0] / (Qi[0] + th.rho);
+            for (int e = 0; e < 3; e++) u[e] = nrm[e] * scale - Qi[1 + e] * rhoinv;
+            Qh[0] = th.rho;
+            for (int e = 0; e < 3; e++) Qh[1 + e] = th.rho * u[e];
+            Qh[4] = th.rho * (th.e + 0.5 * ((u[0]) * (u[0]) + (u[1]) * (u[1]) + (u[2]) * (u[2])));
+            for (int n = 0; n < ns - 1; n++) Qh[5 + n] = th.rho * Y[n];
+            std::memcpy(sh, &th, sizeof(State));
+            sh[S_Z] = Z;
+            break;
+          }
+          case B_SUB_IN_FTPTT: {  // sub-in-ftptt.mako:4-45
+            double nrm[3];
+            unit_normal(S, -outward, nrm);
+            State sti;
+            std::memcpy(&sti, si, sizeof(State));
+            const double gamma = sti.gamma, cs = sti.c, gm1 = gamma - 1.0;
+            const double rhoinv = 1.0 / Qi[0];
+            const double u0[3] = {Qi[1] * rhoinv, Qi[2] * rhoinv, Qi[3] * rhoinv};
+            for (int n = 0; n < ns - 1; n++) Y[n] = v[2 + n];
+            const double Ttotal = v[1];
+            const State total = frompT(c, sti.p, Ttotal, Y);
+            const State cell = frompT(c, sti.p, sti.T, Y);
+            const double Ht = cs * cs / gm1 + (total.e + total.p / total.rho) - (cell.e + cell.p / cell.rho);
+            const double Un = u0[0] * nrm[0] + u0[1] * nrm[1] + u0[2] * nrm[2];
+            const double Jm = -Un + 2.0 * cs / gm1;
+            const double aq = 1.0 + 2.0 / gm1;
+            const double bq = -2.0 * Jm;
+            const double cq = gm1 * (0.5 * Jm * Jm - Ht);
+            const double t1 = -bq / (2.0 * aq);
+            const double t2 = std::sqrt(std::fmax(bq * bq - 4.0 * aq * cq, 0.0)) / (2.0 * aq);
+            const double cb = std::fmax(t1 + t2, t1 - t2);
+            const double Vb = 2.0 * cb / gm1 - Jm;
+            const double Mb = Vb / cb;
+            const double isentropic = 1.0 + 0.5 * gm1 * Mb * Mb;
+            const double pp = v[0] * std::pow(isentropic, -gamma / gm1), T = Ttotal / isentropic;
+            for (int e = 0; e < 3; e++) u[e] = Vb * nrm[e];
+            bc_fromprims(c, pp, T, u, Y, Qh, sh);
+            break;
+          }
+          case B_SUB_OUT_FP: {  // sub-out-fp.mako:4-41
+            double nrm[3];
+            unit_normal(S, outward, nrm);
+            const double rhoinv = 1.0 / Qi[0];
+            outflow_velocity(Qi, rhoinv, Qm, Qm1, nrm, u);
+            for (int n = 0; n < ns - 1; n++) Y[n] = Qi[5 + n] * rhoinv;
+            bc_fromprims(c, v[0], si[1], u, Y, Qh, sh);
+            break;
+          }
+          case B_SUP_OUT_FN: {  // sup-out-fn.mako:4-48
+            double nrm[3];
+            unit_normal(S, outward, nrm);
+            const double rhoinv = 1.0 / Qi[0], rhoinv1 = 1.0 / Qm1[0];
+            const double least = 0.01, p0 = si[0], T0 = si[1];
+            const double pp = std::fmin(std::fmax(least * p0, 2.0 * p0 - sm1[0]), p0);
+            const double T = std::fmax(least * T0, 2.0 * T0 - sm1[1]);
+            outflow_velocity(Qi, rhoinv, Qm, Qm1, nrm, u);
+            for (int n = 0; n < ns - 1; n++)
+              Y[n] = std::fmax(0.0, std::fmin(1.0, 2.0 * Qi[5 + n] * rhoinv - Qm1[5 + n] * rhoinv1));
+            bc_fromprims(c, pp, T, u, Y, Qh, sh);
+            break;
+          }
+          default: break;
+        }
+        if (B.Tg) B.Tg[ch] = sh[1];
+      }
+}
+
+// postgrads of an inflow or outflow: the halo's gradients its image's
+// (navstokes/kernels/bcs/gradients.mako:2-6)
+void bc_grads(const OBlock &B, double *grads, int ngrad, const OBc &bc) {
+  const BFace w(B, bc.nface);
+  const Dims d = cells(B);
+  for (int l = 0; l < B.ng; l++)
+    for (int p = 0; p < w.n[w.a1]; p++)
+      for (int q = 0; q < w.n[w.a2]; q++) {
+        const long cm = w.at(d, p, q, w.deep(l)), ch = w.at(d, p, q, w.halo(l));
+        std::memcpy(&grads[ch * ngrad * 3], &grads[cm * ngrad * 3], sizeof(double) * ngrad * 3);
+      }
+}
+
+// postflux of a wall: the face flux from the first cell in, over the flux
+// function's (euler/kernels/bcs/wall.mako:2-16; with viscosity
+// navstokes/kernels/bcs/wall.mako:40-99)
+void bc_wallflux(const OCase &c, const OBlock &B, const std::vector<double> &state, const std::vector<double> &tr,
+                 std::vector<double> &F, int nf, const OBc &bc) {
+  const int ne = 4 + c.ns, ns = c.ns;
+  const bool visc = c.simulator == O_NAVSTOKES;
+  const BFace w(B, bc.nface);
+  const Dims d = cells(B), fd = face_dims(B, w.a);
+  const double outward = w.low ? -1.0 : 1.0;
+  const bool mov = bc.kind == B_MOV_ADIA || bc.kind == B_MOV_ISOT;
+  const bool isot = bc.kind == B_SLIP_ISOT || bc.kind == B_NOSLIP_ISOT || bc.kind == B_MOV_ISOT;
+  const double stuck = (bc.kind == B_SLIP_ADIA || bc.kind == B_SLIP_ISOT) ? 0.0 : 1.0;
+  for (int p = 0; p < w.n[w.a1]; p++)
+    for (int q = 0; q < w.n[w.a2]; q++) {
+      const double *v = bc.vals + ((long)p * w.n[w.a2] + q) * bc.nval;
+      const long fi = w.at(fd, p, q, w.face()), ci = w.at(d, p, q, w.deep(0));
+      const double *S = B.S[w.a] + fi * 3, *xf = B.xf[w.a] + fi * 3, *xcc = B.xcc + ci * 3;
+      const double *Q = B.Q + ci * ne;
+      State st;
+      std::memcpy(&st, &state[ci * NSTATE], sizeof(State));
+      double *Fo = &F[fi * nf];
+      // wallpressure and wallflux
+      const double area = std::sqrt((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2]));
+      const double un = outward * ((Q[1]) * (S[0]) + (Q[2]) * (S[1]) + (Q[3]) * (S[2])) / (Q[0] * area);
+      const double pw = std::fmax(st.p + Q[0] * st.c * un, 0.0);
+      Fo[0] = 0.0;
+      for (int e = 0; e < 3; e++) Fo[1 + e] = pw * S[e];
+      for (int l = 4; l < nf; l++) Fo[l] = 0.0;
+      if (!visc) continue;
+      const double wall[3] = {mov ? v[0] : 0.0, mov ? v[1] : 0.0, mov ? v[2] : 0.0};
+      double mu, kappa, dT;
+      if (isot) {
+        // wallcoeffs at the wall's temperature and the first cell's pressure and composition
+        const double Tw = bc.kind == B_MOV_ISOT ? v[3] : v[0];
+        const double rhoinv = 1.0 / Q[0];
+        double Y[16], trw[2 + 16], hw[16];
+        for (int n = 0; n < ns - 1; n++) Y[n] = Q[5 + n] * rhoinv;
+        const State at = frompT(c, st.p, Tw, Y);
+        transport(c, Q, at, trw, hw);
+        mu = trw[0], kappa = trw[1], dT = Tw - st.T;
+      } else {
+        mu = tr[ci * (2 + ns)], kappa = tr[ci * (2 + ns) + 1], dT = 0.0;
+      }
+      const double Sabs = area, Sinv = 1.0 / Sabs;
+      const double n[3] = {S[0] * Sinv, S[1] * Sinv, S[2] * Sinv};
+      const double dn = std::fabs(((xcc[0] - xf[0])) * (n[0]) + ((xcc[1] - xf[1])) * (n[1]) + ((xcc[2] - xf[2])) * (n[2]));
+      const double rhoinv = 1.0 / Q[0];
+      double dun[3];
+      for (int e = 0; e < 3; e++) dun[e] = outward * (wall[e] - Q[1 + e] * rhoinv) / dn;
+      const double div = (dun[0]) * (n[0]) + (dun[1]) * (n[1]) + (dun[2]) * (n[2]);
+      for (int e = 0; e < 3; e++) dun[e] = div * n[e] + stuck * (dun[e] - div * n[e]);
+      double work = 0.0;
+      for (int e = 0; e < 3; e++) {
+        const double tS = -mu * Sabs * (dun[e] + div * n[e] / 3.0);
+        Fo[1 + e] += tS;
+        work += wall[e] * tS;
+      }
+      Fo[4] += work - kappa * outward * (dT) / dn * Sabs;
+    }
+}
+
 void halo_fill(std::vector<OBlock> &blks, const OHaloEntry *map, long nmap, int maxlayer, int comps,
                double *(*arr)(OBlock &, std::vector<Scratch> &, int), std::vector<Scratch> &scr) {
   for (long m = 0; m < nmap; m++) {
@@ -1324,13 +1648,32 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
             std::memcpy(&s.state[at * NSTATE], &st, sizeof(State));
           }
           if (B.Tg) B.Tg[at] = st.T;
-          if (visc) {
-            // the shallow range: interior plus one halo layer
+        }
+  }
+  // the boundaries' halo cells, after the state they read and before the
+  // transport reads theirs (simulator/advec/simulator.py:57-75)
+  for (int m = 0; m < c.nbc; m++) bc_halo(c, blks[c.bc[m].blk], scr[c.bc[m].blk].state, c.bc[m]);
+  for (int b = 0; b < nblocks; b++) {
+    OBlock &B = blks[b];
+    const Dims d = cells(B);
+    Scratch &s = scr[b];
+    if (visc) {
+      // the shallow range: interior plus one halo layer
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int i = 0; i < d.X; i++)
+        for (int j = 0; j < d.Y; j++)
+          for (int k = 0; k < d.Z; k++) {
+            const int out = (i < B.ng || i >= d.X - B.ng) + (j < B.ng || j >= d.Y - B.ng) +
+                            (k < B.ng || k >= d.Z - B.ng);
             const int deep = (i < B.ng - 1 || i > d.X - B.ng) + (j < B.ng - 1 || j > d.Y - B.ng) +
                              (k < B.ng - 1 || k > d.Z - B.ng);
-            if (!deep) transport(c, B.Q + at * ne, st, &s.tr[at * (2 + ns)], &s.hsp[at * ns], s.state[at * NSTATE + S_Z]);
+            if (out > 1 || deep) continue;
+            const long at = d.at(i, j, k);
+            State st;
+            std::memcpy(&st, &s.state[at * NSTATE], sizeof(State));
+            transport(c, B.Q + at * ne, st, &s.tr[at * (2 + ns)], &s.hsp[at * ns], s.state[at * NSTATE + S_Z]);
           }
-        }
+    }
     if (visc) {
       // dqdxyz (simulator/navstokes/kernels/dqdxyz.mako:16-41) on the interior
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1371,14 +1714,17 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
     // grads: one halo plane (simulator/advecdiff/simulator.py:11-14, 116-117)
     halo_fill(blks, map, nmap, 1, ngrad * 3,
               [](OBlock &, std::vector<Scratch> &s, int b) { return s[b].grads.data(); }, scr);
+    // the inflows' and outflows' halo gradients (simulator/advecdiff/simulator.py:113-114)
+    for (int m = 0; m < c.nbc; m++)
+      if (!bc_wall(c.bc[m].kind)) bc_grads(blks[c.bc[m].blk], scr[c.bc[m].blk].grads.data(), ngrad, c.bc[m]);
   }
+  const int nf = ne + (c.df ? 1 : 0);
   for (int b = 0; b < nblocks; b++) {
     OBlock &B = blks[b];
     const Dims d = cells(B);
     Scratch &s = scr[b];
     const int g = B.ng;
     // the double flux writes its energy row twice: one row more per face
-    const int nf = ne + (c.df ? 1 : 0);
     for (int a = 0; a < 3; a++) {
       const Dims f = face_dims(B, a);
       s.F[a].assign((long)f.X * f.Y * f.Z * nf, 0.0);
@@ -1411,6 +1757,20 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
                            &s.grads[L * ngrad * 3], &s.grads[R * ngrad * 3], F);
           }
     }
+  }
+  // the walls write the flux through their faces over the flux function's
+  // (simulator/advec/simulator.py:80-84)
+  for (int m = 0; m < c.nbc; m++) {
+    const OBc &bc = c.bc[m];
+    if (!bc_wall(bc.kind)) continue;
+    const int a = (bc.nface - 1) / 2;
+    bc_wallflux(c, blks[bc.blk], scr[bc.blk].state, scr[bc.blk].tr, scr[bc.blk].F[a], nf, bc);
+  }
+  for (int b = 0; b < nblocks; b++) {
+    OBlock &B = blks[b];
+    const Dims d = cells(B);
+    Scratch &s = scr[b];
+    const int g = B.ng;
     if (faces)
       for (int a = 0; a < 3; a++) std::memcpy(faces[3 * b + a], s.F[a].data(), sizeof(double) * s.F[a].size());
     const Dims fi = face_dims(B, 0), fj = face_dims(B, 1), fk = face_dims(B, 2);
@@ -1447,6 +1807,15 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
           }
         }
   }
+  return 0;
+}
+
+// The boundaries' gradient hook alone on given gradient arrays, grads[b]
+// [..][ngrad][3] over block b's full extents (the reference's postgrads)
+int oracle_bc_grads(const OCase *cp, const OBlock *blocks, double **grads) {
+  const OCase &c = *cp;
+  for (int m = 0; m < c.nbc; m++)
+    if (!bc_wall(c.bc[m].kind)) bc_grads(blocks[c.bc[m].blk], grads[c.bc[m].blk], 3 + c.ns, c.bc[m]);
   return 0;
 }
 

@@ -262,3 +262,73 @@ def mixing_layer_prims(metrics, ny, dx=2e-5, seed=0, p=6e6, Tcold=120.0, Thot=30
         q[..., 5] = np.clip(f, 0.0, 1.0)
         out.append(q)
     return out
+
+
+# the boundary test box: one jostled block whose every face carries the same
+# boundary entry at seeded values (the reference's own boundary tests run
+# such a box, tests/bcs/bcblock.py), the velocity random cell by cell so an
+# exit sees flow both ways, p, T and Y smooth so an extrapolated halo stays
+# physical
+def bc_box_config(kind, ns=1, simulator="euler", primary="kepaec", recon="constant", limiter=None, eos="cpg",
+                  integrator="rk4", seed=0, entry=None, launch="per-block", tables=None):
+    """tables: a mixture's stored tables (the real gases) instead of ns of the MIXED species."""
+    rng = np.random.default_rng(seed)
+    cfg = Config()
+    cfg["simulation"]["simulator"] = simulator
+    if tables is not None:
+        cfg["mixture"]["species"] = tables
+    elif ns == 1:
+        cfg["mixture"]["species"] = {"Air": {"MW": MW_AIR, "cp0": CP_AIR, "mu0": 1.8e-5, "kappa0": 0.026}}
+    else:
+        cfg["mixture"]["species"] = {k: MIXED[k] for k in list(MIXED)[:ns]}
+    cfg["mixture"]["eos"] = eos
+    cfg["mixture"]["trans"] = "constant" if simulator == "navier-stokes" else None
+    cfg["time-integration"]["integrator"] = integrator
+    cfg["adv-flux"]["primary"] = primary
+    cfg["adv-flux"]["recon"] = recon
+    cfg["adv-flux"]["limiter"] = limiter if recon == "muscl" else None
+    cfg["backend-b200"]["launch"] = launch
+
+    def rounded(v):
+        return float(f"{v:.6g}")
+
+    values = {"kind": kind, "p": rounded(rng.uniform(0.9, 1.1) * P0), "u": rounded(rng.uniform(1, 300)),
+              "v": rounded(rng.uniform(1, 300)), "w": rounded(rng.uniform(1, 300)),
+              "T": rounded(rng.uniform(270.0, 330.0)), "mflux": rounded(rng.uniform(1, 300))}
+    values["pt"], values["Tt"] = rounded(1.3 * values["p"]), rounded(1.1 * values["T"])
+    if tables is not None:
+        from peregrine_b200.mixture import Mixture
+
+        names = Mixture(cfg["mixture"]).spnames
+        ns = len(names)
+    else:
+        names = list(cfg["mixture"]["species"])
+    if ns > 1:
+        Y = rng.uniform(0.2, 1.0, ns)
+        values.update(zip(names[:-1], map(rounded, Y[:-1] / Y.sum())))
+    values.update(entry or {})
+    cfg["bcvals"]["outer"] = values
+    return cfg.validate()
+
+
+def bc_box_mesh(cells=(7, 5, 3), jostle=0.1, bcnames=None, defaultbc="outer", periodic=(False, False, False),
+                lengths=(1.0, 1.0, 1.0)):
+    return CubeMesher(cells=[[c] for c in cells], lengths=list(lengths), periodic=list(periodic),
+                      bcnames=bcnames, defaultbc=defaultbc, jostle=jostle)
+
+
+def bc_box_prims(metrics, ns, seed=0, speed=200.0):
+    rng = np.random.default_rng(seed + 1)
+    ph = rng.uniform(0.0, 2 * np.pi, 6)
+    out = []
+    for m in metrics:
+        x, y, z = (m["xcc"][..., d] for d in range(3))
+        smooth = np.cos(2.0 * x + ph[0]) * np.cos(1.5 * y + ph[1]) * np.cos(z + ph[2])
+        q = np.zeros(x.shape + (4 + ns,))
+        q[..., 0] = P0 * (1.0 + 0.3 * smooth)
+        q[..., 1:4] = rng.uniform(-speed, speed, x.shape + (3,))
+        q[..., 4] = 1000.0 * (1.0 + 0.3 * np.cos(x + ph[3]) * np.cos(2.0 * z + ph[4]))
+        for n in range(ns - 1):
+            q[..., 5 + n] = 0.9 / (ns - 1) * (0.5 + 0.4 * np.cos((n + 1) * x + y + ph[5]) ** 2)
+        out.append(q)
+    return out

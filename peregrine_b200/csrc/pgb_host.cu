@@ -67,11 +67,14 @@ int fail(int code, const std::string &msg) {
   } while (0)
 
 static __global__ void k_setscalar(double *p, double v) { *p = v; }
+// the clock at a step's end: start + dt (peregrine/multiblock/solver.py:355-364)
+static __global__ void k_clock(double *clock, const double *dt) { *clock = *clock + *dt; }
 
 struct HostBlock {
   int nx, ny, nz;
   int nbr[6] = {-1, -1, -1, -1, -1, -1};
   int nbrface[6] = {0, 0, 0, 0, 0, 0};
+  int bc[6] = {-1, -1, -1, -1, -1, -1};  // a boundary face's entry, -1 for none
   int tw = 0, th = 0, kchunk = 0;
   bool metrics_set[PGB_NMETRICS] = {};
   BlockDev dev{};
@@ -140,12 +143,30 @@ struct pgb_case {
   unsigned long long uid = 0;  // unique over the process, never reused
   unsigned version = 0;        // bumped when the species or mechanism tables change
   bool df_fresh = true;        // the double flux has no frozen planes for the state yet
+  // boundaries: the entries and their programs as given, then on the device
+  // the entries, programs and the three passes' face tables (each with its
+  // sentinel), and the clock the boundary values read
+  std::vector<BcEntry> bc_entries;
+  std::vector<BcOp> bc_ops;
+  BcEntry *d_bcent = nullptr;
+  BcOp *d_bcops = nullptr;
+  BcFace *d_bcface[3] = {};  // halo, gradient and wall passes
+  int nbcface[3] = {0, 0, 0};
+  long long bcthreads[3] = {0, 0, 0};
+  double *d_clock = nullptr;
 };
 
 namespace {
 
 bool fused_capable(const pgb_case *c) {
   const pgb_physics &p = c->phys;
+  // the batched kernel's halo is the periodic or block-to-block fill alone,
+  // and its tiles and stencil take blocks of two cells or more per axis
+  for (const HostBlock &B : c->blocks) {
+    if (B.nx < 2 || B.ny < 2 || B.nz < 2) return false;
+    for (int f = 0; f < 6; f++)
+      if (B.bc[f] >= 0) return false;
+  }
   return p.eos == PGB_EOS_CPG && p.primary == PGB_FLUX_KEPAEC && p.recon == PGB_RECON_CONSTANT && p.ns == 1 &&
          (p.simulator == PGB_EULER || p.trans == PGB_TRANS_CONSTANT);
 }
@@ -255,24 +276,29 @@ int set_current(pgb_case *c) {
 }
 
 // where a cell outside a block lies: step across faces one axis at a time
-// (orientation "123", a conforming lattice); false at a boundary
+// (orientation "123", a conforming lattice), across as many blocks as a
+// block thinner than the halo needs; false at a boundary
 bool locate(const pgb_case *c, int b, int ijk[3], int &sb) {
   sb = b;
   for (int a = 0; a < 3; a++) {
-    const HostBlock &B = c->blocks[sb];
-    const int n[3] = {B.nx, B.ny, B.nz};
-    if (ijk[a] < 0) {
-      const int nb = B.nbr[2 * a];
-      if (nb < 0) return false;
-      const HostBlock &N = c->blocks[nb];
-      const int m[3] = {N.nx, N.ny, N.nz};
-      ijk[a] += m[a];
-      sb = nb;
-    } else if (ijk[a] >= n[a]) {
-      const int nb = B.nbr[2 * a + 1];
-      if (nb < 0) return false;
-      ijk[a] -= n[a];
-      sb = nb;
+    for (int hop = 0; hop <= NG; hop++) {
+      const HostBlock &B = c->blocks[sb];
+      const int n[3] = {B.nx, B.ny, B.nz};
+      if (ijk[a] < 0) {
+        const int nb = B.nbr[2 * a];
+        if (nb < 0) return false;
+        const HostBlock &N = c->blocks[nb];
+        const int m[3] = {N.nx, N.ny, N.nz};
+        ijk[a] += m[a];
+        sb = nb;
+      } else if (ijk[a] >= n[a]) {
+        const int nb = B.nbr[2 * a + 1];
+        if (nb < 0) return false;
+        ijk[a] -= n[a];
+        sb = nb;
+      } else {
+        break;
+      }
     }
   }
   const HostBlock &S = c->blocks[sb];
@@ -797,6 +823,12 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.chem = c->phys.chemistry == PGB_CHEM_COUPLED;
   pc.df = c->phys.simulator == PGB_EULER_DF;
   pc.realgas = c->phys.eos == PGB_EOS_REALGAS || c->phys.eos == PGB_EOS_REALGAS_DF;
+  pc.bchalo = c->d_bcface[0], pc.bcgrad = c->d_bcface[1], pc.bcwall = c->d_bcface[2];
+  pc.nbchalo = c->nbcface[0], pc.nbcgrad = c->nbcface[1], pc.nbcwall = c->nbcface[2];
+  pc.bchalo_n = c->bcthreads[0], pc.bcgrad_n = c->bcthreads[1], pc.bcwall_n = c->bcthreads[2];
+  pc.bcent = c->d_bcent, pc.bcops = c->d_bcops;
+  pc.clock = c->d_clock, pc.dt = c->d_dt;
+  pc.tfrac = 0.0;
   pc.stream = c->stream;
   return pc;
 }
@@ -825,13 +857,14 @@ int df_settle(pgb_case *c, int qphys) {
   return prestep_plain(c, qphys, count, 1);
 }
 
-int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count) {
+int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count, double tfrac = 0.0) {
   RET(ensure_scratch(c));
   std::vector<BlockDev> hb;
   PlainCase pc = plain_case(c, hb);
   MarkCtx mc{c, &count};
   pc.mark = mark_cb;
   pc.ctx = &mc;
+  pc.tfrac = tfrac;
   return kPlain[c->phys.ns - 1].rhs(&pc, c->d_reg[qphys], c->d_reg[dqphys]);
 }
 
@@ -840,7 +873,7 @@ int step_plain(pgb_case *c, int &count) {
   const auto &map = c->phys_of;
   if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count, 0));
   for (const pgb_stage &st : c->stages) {
-    RET(rhs_plain(c, map[st.q], map[st.dq], count));
+    RET(rhs_plain(c, map[st.q], map[st.dq], count, st.tfrac));
     for (int m = 0; m < st.ncombine; m++) {
       const pgb_combine &cb = st.combine[m];
       CombineDev cd{};
@@ -861,7 +894,59 @@ int step_plain(pgb_case *c, int &count) {
       }
     }
   }
+  // the boundaries' clock moves on by dt; a case without boundaries reads none
+  if (c->nbcface[0]) {
+    k_clock<<<1, 1, 0, c->stream>>>(c->d_clock, c->d_dt);
+    mark(c, K_COMBINE, count);
+  }
   CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+// the boundary passes' face tables: every boundary face given an entry in the
+// halo pass, the inflows' and outflows' faces again in the gradient pass when
+// the case is viscous, the walls' in the wall pass; each table's threads end
+// to end, closed by a sentinel holding the pass's thread count
+int build_bcs(pgb_case *c) {
+  std::vector<BcFace> t[3];
+  long long n[3] = {0, 0, 0};
+  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const HostBlock &B = c->blocks[b];
+    const int ext[3] = {B.nx, B.ny, B.nz};
+    for (int f = 0; f < 6; f++) {
+      const int e = B.bc[f];
+      if (e < 0) continue;
+      const int a = f / 2;
+      const long long plane = (long long)ext[a == 0 ? 1 : 0] * ext[a == 2 ? 1 : 2];
+      const bool wall = bc_is_wall(c->bc_entries[e].kind);
+      t[0].push_back(BcFace{b, f, e, 0, n[0]});
+      n[0] += NG * plane;
+      if (visc && !wall) {
+        t[1].push_back(BcFace{b, f, e, 0, n[1]});
+        n[1] += NG * plane;
+      }
+      if (wall) {
+        t[2].push_back(BcFace{b, f, e, 0, n[2]});
+        n[2] += plane;
+      }
+    }
+  }
+  for (int p = 0; p < 3; p++) {
+    c->nbcface[p] = (int)t[p].size();
+    c->bcthreads[p] = n[p];
+    if (t[p].empty()) continue;
+    t[p].push_back(BcFace{0, 0, 0, 0, n[p]});
+    CK(cudaMalloc(&c->d_bcface[p], sizeof(BcFace) * t[p].size()));
+    CK(cudaMemcpy(c->d_bcface[p], t[p].data(), sizeof(BcFace) * t[p].size(), cudaMemcpyHostToDevice));
+  }
+  if (!c->bc_entries.empty()) {
+    CK(cudaMalloc(&c->d_bcent, sizeof(BcEntry) * c->bc_entries.size()));
+    CK(cudaMemcpy(c->d_bcent, c->bc_entries.data(), sizeof(BcEntry) * c->bc_entries.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_bcops, sizeof(BcOp) * std::max<size_t>(1, c->bc_ops.size())));
+    if (!c->bc_ops.empty())
+      CK(cudaMemcpy(c->d_bcops, c->bc_ops.data(), sizeof(BcOp) * c->bc_ops.size(), cudaMemcpyHostToDevice));
+  }
   return PGB_OK;
 }
 
@@ -971,7 +1056,8 @@ int pgb_case_destroy(pgb_case *c) {
   for (auto &r : c->d_reg)
     if (r) cudaFree(r);
   void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
-                  c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage};
+                  c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
+                  c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock};
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1097,7 +1183,7 @@ int pgb_production(pgb_case *c, long n, const double *rho, const double *Y, cons
 int pgb_case_add_block(pgb_case *c, int ni, int nj, int nk, int *blk) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
   if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
-  if (ni < 2 || nj < 2 || nk < 2) return fail(PGB_ERR_ARG, "a block has at least two cells per axis");
+  if (ni < 1 || nj < 1 || nk < 1) return fail(PGB_ERR_ARG, "a block has at least one cell per axis");
   if (ni > 30000 || nj > 30000 || nk > 30000) return fail(PGB_ERR_ARG, "block too large");
   HostBlock B;
   B.nx = ni, B.ny = nj, B.nz = nk;
@@ -1122,7 +1208,80 @@ int pgb_case_connect(pgb_case *c, int blk, int nface, int nbr, int nbrface) {
       if (d != a && n[d] != m[d]) return fail(PGB_ERR_ARG, "the two faces do not match cell for cell");
   }
   c->blocks[blk].nbr[nface - 1] = nbr;
+  if (nbr >= 0) c->blocks[blk].bc[nface - 1] = -1;
   c->blocks[blk].nbrface[nface - 1] = nbrface;
+  return PGB_OK;
+}
+
+int pgb_case_add_bc(pgb_case *c, int kind, const int *ops, const double *args, const int *starts, int nvalues,
+                    int *id) {
+  if (!c || !id || !starts || (nvalues && (!ops || !args))) return fail(PGB_ERR_ARG, "null argument");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (kind < 1 || kind >= PGB_BC_NKINDS) return fail(PGB_ERR_ARG, "no such boundary kind");
+  const bool ns_only = kind >= PGB_BC_NOSLIP_ADIA_WALL && kind <= PGB_BC_MOV_ISOT_WALL;
+  if (ns_only && c->phys.simulator != PGB_NAVIER_STOKES)
+    return fail(PGB_ERR_ARG, "the no-slip and moving walls are the navier-stokes simulator's kinds");
+  const int want = bc_head_values(kind) + (bc_is_inlet(kind) ? c->phys.ns - 1 : 0);
+  if (nvalues != want) return fail(PGB_ERR_ARG, "the entry gives another number of values than its kind reads");
+  if (starts[0] < 0) return fail(PGB_ERR_ARG, "a negative program start");
+  const int total = starts[nvalues] - starts[0];
+  if (total < 0 || (long long)c->bc_ops.size() + total > PGB_BC_MAXOPS)
+    return fail(PGB_ERR_ARG, "the boundary programs are longer than the build takes");
+  BcEntry E{};
+  E.kind = kind;
+  E.nval = nvalues;
+  const int base = (int)c->bc_ops.size();
+  for (int v = 0; v < nvalues; v++) {
+    if (starts[v + 1] < starts[v]) return fail(PGB_ERR_ARG, "program starts out of order");
+    // each program is checked on a model of the device's stack
+    int depth = 0;
+    for (int k = starts[v]; k < starts[v + 1]; k++) {
+      const int op = ops[k];
+      if (op < 0 || op >= PGB_NOPS) return fail(PGB_ERR_ARG, "no such program operation");
+      if (op <= PGB_OP_T) {
+        if (++depth > PGB_BC_STACK) return fail(PGB_ERR_ARG, "a boundary program deeper than its stack");
+        continue;
+      }
+      const bool binary = op == PGB_OP_ADD || op == PGB_OP_SUB || op == PGB_OP_MUL || op == PGB_OP_DIV ||
+                          op == PGB_OP_POW || op == PGB_OP_MIN || op == PGB_OP_MAX;
+      if (depth < (binary ? 2 : 1)) return fail(PGB_ERR_ARG, "a boundary program takes more than it has");
+      if (binary) depth--;
+    }
+    if (depth != 1) return fail(PGB_ERR_ARG, "a boundary program must leave one value");
+  }
+  for (int v = 0; v <= nvalues; v++) E.start[v] = base + starts[v] - starts[0];
+  for (int k = starts[0]; k < starts[nvalues]; k++) c->bc_ops.push_back(BcOp{ops[k], 0, args[k]});
+  *id = (int)c->bc_entries.size();
+  c->bc_entries.push_back(E);
+  return PGB_OK;
+}
+
+int pgb_case_set_face_bc(pgb_case *c, int blk, int nface, int bc) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size() || nface < 1 || nface > 6)
+    return fail(PGB_ERR_ARG, "no such block face");
+  if (bc < 0 || bc >= (int)c->bc_entries.size()) return fail(PGB_ERR_ARG, "no such boundary entry");
+  if (c->blocks[blk].nbr[nface - 1] >= 0) return fail(PGB_ERR_ARG, "the face joins a neighbour; it is no boundary");
+  if (c->phys.simulator == PGB_EULER_DF)
+    return fail(PGB_ERR_UNSUPPORTED, "the double flux's boundaries are not built in this build");
+  c->blocks[blk].bc[nface - 1] = bc;
+  return PGB_OK;
+}
+
+int pgb_set_time(pgb_case *c, double t) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_clock, t);
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int pgb_get_time(pgb_case *c, double *t) {
+  if (!c || !t) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  CK(cudaMemcpyAsync(t, c->d_clock, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
 }
 
@@ -1170,6 +1329,9 @@ int pgb_case_finalize(pgb_case *c) {
   CK(cudaMalloc(&c->d_met, sizeof(double) * M_NCOMP * n));
   CK(cudaMemsetAsync(c->d_met, 0, sizeof(double) * M_NCOMP * n, c->stream));
   CK(cudaMalloc(&c->d_dt, sizeof(double)));
+  CK(cudaMalloc(&c->d_clock, sizeof(double)));
+  CK(cudaMemsetAsync(c->d_clock, 0, sizeof(double), c->stream));
+  RET(build_bcs(c));
   CK(cudaMalloc(&c->d_counter, sizeof(unsigned int) * 16));
   CK(cudaMalloc(&c->d_blks, sizeof(BlockDev) * c->blocks.size()));
   std::vector<BlockDev> devs;
@@ -1273,6 +1435,21 @@ int pgb_array_get(pgb_case *c, int blk, int reg, double *host, long count) {
                                                                                  c->d_reg[c->phys_of[reg]], c->d_prims);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(host, c->d_prims, sizeof(double) * count, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_array_get_full(pgb_case *c, int blk, int reg, double *host, long count) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
+  if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  if (!host) return fail(PGB_ERR_ARG, "null host array");
+  const BlockDev &D = c->blocks[blk].dev;
+  if (count != (long)D.vol * c->ne) return fail(PGB_ERR_ARG, "host array of the wrong size");
+  // a block's register is its components' full arrays end to end: F order already
+  CK(cudaMemcpyAsync(host, c->d_reg[c->phys_of[reg]] + (size_t)c->ne * D.cv, sizeof(double) * count,
+                     cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
 }

@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "bc_types.h"
 #include "chem_types.h"
 #include "layout.cuh"
 #include "physics.cuh"
@@ -41,6 +42,17 @@ struct PlainCase {
   // without a table a packed launch gives each block a grid row
   const int2 *ctab[5];
   long long nctab[5];
+  // boundaries: the face tables of the halo, gradient and wall passes (each
+  // ending in its sentinel) and their face counts, the entries, their value
+  // programs, the clock and dt in device memory and the stage's time as a
+  // fraction of dt
+  const BcFace *bchalo, *bcgrad, *bcwall;
+  int nbchalo, nbcgrad, nbcwall;
+  long long bchalo_n, bcgrad_n, bcwall_n;
+  const BcEntry *bcent;
+  const BcOp *bcops;
+  const double *clock, *dt;
+  double tfrac;
   cudaStream_t stream;
   void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block
   void *ctx;

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <string>
 
+#include "bc.cuh"
 #include "chem.cuh"
 #include "pgb200.h"
 #include "plain.cuh"
@@ -157,11 +158,44 @@ extern "C" int PGB_ENTRY(pgb_plain_upload_)(const Species *sp, const Mech *mech,
   return PGB_OK;
 }
 
-// one right-hand side of every block: Q's halo, the state everywhere (the
-// transport and gradients on the viscous path, the gradients' first halo
-// layer), the chemistry source, the face fluxes per axis and the divergence.
-// Per block the passes run block by block (the reference's order); packed,
-// each pass is one launch over every block.
+// the boundary passes: the halo cells behind every boundary face (after the
+// state, before the transport reads them), the inflows' and outflows' halo
+// gradients (after the gradients' exchange) and the walls' face fluxes (after
+// the flux functions, before the divergence), one launch each over every
+// block's boundary faces
+static void bc_halo_launch(const PlainCase *pc, const double *Q) {
+  if (!pc->nbchalo) return;
+  if (pc->realgas)
+    k_bc_halo<NS, true><<<grid_of(pc->bchalo_n), TH, 0, pc->stream>>>(
+        pc->d_blks, pc->bchalo, pc->nbchalo, pc->bcent, pc->bcops, const_cast<double *>(Q), pc->state, pc->met,
+        pc->clock, pc->dt, pc->tfrac);
+  else
+    k_bc_halo<NS, false><<<grid_of(pc->bchalo_n), TH, 0, pc->stream>>>(
+        pc->d_blks, pc->bchalo, pc->nbchalo, pc->bcent, pc->bcops, const_cast<double *>(Q), pc->state, pc->met,
+        pc->clock, pc->dt, pc->tfrac);
+  mark(pc, 0);
+}
+static void bc_grads_launch(const PlainCase *pc) {
+  if (!pc->nbcgrad) return;
+  k_bc_grads<NS><<<grid_of(pc->bcgrad_n), TH, 0, pc->stream>>>(pc->d_blks, pc->bcgrad, pc->nbcgrad, pc->grads);
+  mark(pc, 0);
+}
+static void bc_wall_launch(const PlainCase *pc, const double *Q) {
+  if (!pc->nbcwall) return;
+  k_bc_wall<NS><<<grid_of(pc->bcwall_n), TH, 0, pc->stream>>>(
+      pc->d_blks, pc->bcwall, pc->nbcwall, pc->bcent, pc->bcops, Q, pc->state, pc->tr, pc->met, pc->F[0], pc->F[1],
+      pc->F[2], NE + (pc->df ? 1 : 0), pc->visc, pc->clock, pc->dt, pc->tfrac);
+  mark(pc, 2);
+}
+
+// one right-hand side of every block: Q's halo, the state everywhere, the
+// boundaries' halo cells, the transport and gradients on the viscous path
+// (the gradients' first halo layer exchanged or set by the boundaries), the
+// chemistry source, the face fluxes per axis, the walls' fluxes and the
+// divergence (peregrine/simulator/advec/simulator.py:57-84,
+// peregrine/simulator/advecdiff/simulator.py:110-124).  Per block the passes
+// run block by block (the reference's order); packed, each pass is one launch
+// over every block.
 extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, double *dQ) {
   cudaStream_t s = pc->stream;
   const RhsArgs a{Q, dQ};
@@ -169,16 +203,20 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
   mark(pc, 0);
   if (pc->packed) {
     for_blocks(pc, R_VOL, fromQ_launch, &a, 2);
+    bc_halo_launch(pc, Q);
     if (pc->visc) {
       for_blocks(pc, R_VOL, transport_launch, &a, 2);
       for_blocks(pc, R_INNER, grads_launch, &a, 2);
     }
   } else {
     for (int b = 0; b < pc->nblocks; b++) {
-      const BlockDev &D = pc->h_blks[b];
-      fromQ_launch(pc, b, dim3(grid_of(D.vol)), nullptr, &a);
+      fromQ_launch(pc, b, dim3(grid_of(pc->h_blks[b].vol)), nullptr, &a);
       mark(pc, 2);
-      if (pc->visc) {
+    }
+    bc_halo_launch(pc, Q);
+    if (pc->visc) {
+      for (int b = 0; b < pc->nblocks; b++) {
+        const BlockDev &D = pc->h_blks[b];
         transport_launch(pc, b, dim3(grid_of(D.vol)), nullptr, &a);
         mark(pc, 2);
         grads_launch(pc, b, dim3(grid_of(range_size(D, R_INNER))), nullptr, &a);
@@ -189,6 +227,7 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
   if (pc->visc) {
     k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1));
     mark(pc, 0);
+    bc_grads_launch(pc);
   }
   if (pc->packed) {
     if (pc->chem) for_blocks(pc, R_INNER, source_launch, &a, 2);
@@ -200,6 +239,7 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
       for_blocks(pc, R_FY, diff_launch<1>, &a, 2);
       for_blocks(pc, R_FZ, diff_launch<2>, &a, 2);
     }
+    bc_wall_launch(pc, Q);
     for_blocks(pc, R_INNER, apply_launch, &a, 2);
   } else {
     for (int b = 0; b < pc->nblocks; b++) {
@@ -223,8 +263,18 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
         diff_launch<2>(pc, b, g(R_FZ), nullptr, &a);
         mark(pc, 2);
       }
-      apply_launch(pc, b, g(R_INNER), nullptr, &a);
-      mark(pc, 2);
+      // without walls a block's divergence follows its own fluxes
+      if (!pc->nbcwall) {
+        apply_launch(pc, b, g(R_INNER), nullptr, &a);
+        mark(pc, 2);
+      }
+    }
+    if (pc->nbcwall) {
+      bc_wall_launch(pc, Q);
+      for (int b = 0; b < pc->nblocks; b++) {
+        apply_launch(pc, b, dim3(grid_of(range_size(pc->h_blks[b], R_INNER))), nullptr, &a);
+        mark(pc, 2);
+      }
     }
   }
   const cudaError_t e = cudaGetLastError();

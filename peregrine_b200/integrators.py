@@ -59,12 +59,22 @@ def stages(name):
     return out, dQ, nregs
 
 
+def stage_fractions(name):
+    """The time each stage's right-hand side reads, as a fraction of dt past
+    the step's start: the stage table's first column (stage 0 at the start;
+    the reference moves its clock to stage n's time before stage n's
+    right-hand side, peregrine/integrators/rungekutta.py:28-39)."""
+    return [row[0] for row in (RK4 if name == "rk4" else TABLES[name])]
+
+
 def stage_records(name):
     rows, dQ, nregs = stages(name)
     recs = (native.Stage * len(rows))()
+    fracs = stage_fractions(name)
     for s, (q, combines) in enumerate(rows):
         rec = recs[s]
         rec.q, rec.dq, rec.ncombine = q, dQ, len(combines)
+        rec.tfrac = fracs[s]
         for m, cb in enumerate(combines):
             c = rec.combine[m]
             c.out = cb["out"]

@@ -21,6 +21,14 @@ FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV, FLUX_AUSMUP = 0, 1, 2, 3
 RECON_CONSTANT, RECON_MUSCL = 0, 1
 LIMITERS = {"koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
 CHEM_NONE, CHEM_COUPLED = 0, 1
+# boundary kinds, by the reference's bcvals names
+BC_KINDS = {"slp-adia-wall": 1, "slp-isot-wall": 2, "no-slp-adia-wall": 3, "mov-adia-wall": 4,
+            "no-slp-isot-wall": 5, "mov-isot-wall": 6, "sub-in-fvt": 7, "sup-in-fa": 8, "sub-in-ftptt": 9,
+            "sub-in-fmt": 10, "sub-out-fp": 11, "sup-out-fn": 12}
+# the boundary value programs' operations
+OPS = {name: n for n, name in enumerate(("const", "x", "y", "z", "t", "add", "sub", "mul", "div", "neg", "pow", "sin",
+                                         "cos", "tan", "exp", "log", "sqrt", "tanh", "abs", "min", "max"))}
+BC_STACK = 16
 
 
 def mechanism(consts):
@@ -160,7 +168,7 @@ class Combine(ctypes.Structure):
 
 class Stage(ctypes.Structure):
     _fields_ = [("q", ctypes.c_int), ("dq", ctypes.c_int), ("ncombine", ctypes.c_int),
-                ("combine", Combine * 2)]
+                ("combine", Combine * 2), ("tfrac", ctypes.c_double)]
 
 
 # every symbol include/pgb200.h declares, with its argument types
@@ -190,6 +198,11 @@ SIGNATURES = {
     "pgb_production": ([ctypes.c_void_p, ctypes.c_long] + [ctypes.POINTER(ctypes.c_double)] * 4, ctypes.c_int),
     "pgb_case_add_block": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_case_connect": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "pgb_case_add_bc": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_case_set_face_bc": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "pgb_set_time": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
+    "pgb_get_time": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "pgb_case_set_stages": ([ctypes.c_void_p, ctypes.POINTER(Stage), ctypes.c_int], ctypes.c_int),
     "pgb_case_finalize": ([ctypes.c_void_p], ctypes.c_int),
     "pgb_case_halo": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
@@ -197,6 +210,7 @@ SIGNATURES = {
     "pgb_metric_set": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_array_set": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_array_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_array_get_full": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_set_prims": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_rhs": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_step": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),

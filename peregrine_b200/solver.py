@@ -13,6 +13,7 @@ import ctypes
 
 import numpy as np
 
+from peregrine_b200 import bcs as bcmod
 from peregrine_b200 import native
 from peregrine_b200.config import ConfigError
 from peregrine_b200.grid import metrics as make_metrics
@@ -66,13 +67,12 @@ class Array:
         return tuple(n + 2 * NG for n in b.cells) + (self.solver.ne,)
 
     def get(self):
-        """The full-shaped host array; halo cells are NaN (the device keeps them)."""
-        b = self.solver.blocks[self.blk]
-        inner = np.empty(b.cells + (self.solver.ne,), order="F")
-        native.call("pgb_array_get", self.solver.case, self.blk, self.reg, _fptr(inner), inner.size)
-        out = np.full(self.shape, np.nan)
-        out[b.interior] = inner
-        return out
+        """The full-shaped host array, halo included: what the last right-hand
+        side left there (exchanged, or set by a boundary); the halo's edges and
+        corners are never read."""
+        full = np.empty(self.shape, order="F")
+        native.call("pgb_array_get_full", self.solver.case, self.blk, self.reg, _fptr(full), full.size)
+        return np.ascontiguousarray(full)
 
     def set(self, values):
         b = self.solver.blocks[self.blk]
@@ -101,6 +101,8 @@ class Solver:
         self.nrt, self.tme = 0, 0.0
         self.mixture = Mixture(cfg["mixture"])
         self.ns = self.mixture.ns
+        # every bcvals entry, checked whether or not a face names it
+        self.bcs = bcmod.entries(cfg["bcvals"], sim["simulator"], self.mixture.spnames)
         self.ne = 4 + self.ns
         self.integrator = cfg["time-integration"]["integrator"]
         records, nregs = stage_records(self.integrator)
@@ -144,9 +146,13 @@ class Solver:
         if state is None:
             self._uniform_ics()
 
+    @property
+    def has_bcs(self):
+        return any(face.nbr is None for blk in self.mesh_blocks for face in blk.intfaces)
+
     def fused_capable(self):
         cfg = self.cfg
-        return (self.ns == 1 and cfg["adv-flux"]["primary"] == "kepaec" and cfg["adv-flux"]["recon"] == "constant"
+        return (not self.has_bcs and min(min(b.cells) for b in self.mesh_blocks) >= 2 and self.ns == 1 and cfg["adv-flux"]["primary"] == "kepaec" and cfg["adv-flux"]["recon"] == "constant"
                 and cfg["mixture"]["eos"] == "cpg")
 
     def species_tables(self):
@@ -182,6 +188,7 @@ class Solver:
             for face in blk.intfaces:
                 nbr = -1 if face.nbr is None else face.nbr
                 native.call("pgb_case_connect", self.case, blk.nblki, face.nface, nbr, face.nbrface or 0)
+        self._fill_bcs()
         if self.cfg["chem-integration"]["kind"] == "coupled":
             mech, keep = native.mechanism(consts)
             native.call("pgb_case_set_mechanism", self.case, ctypes.byref(mech))
@@ -196,6 +203,23 @@ class Solver:
                 a = np.asfortranarray(a.reshape(a.shape[:3] + (-1,)))
                 native.call("pgb_metric_set", self.case, blk.nblki, native.METRIC_IDS[name], _fptr(a), a.size)
         self.blocks = [SolverBlock(self, b) for b in self.mesh_blocks]
+
+    def _fill_bcs(self):
+        """The bcvals entries and the boundary faces that name them."""
+        bcmod.check_faces(self.mesh_blocks, self.cfg["bcvals"])
+        ids = {}
+        for name, entry in self.bcs.items():
+            kind, ops, args, starts = entry.program()
+            o = (ctypes.c_int * max(1, len(ops)))(*ops)
+            a = (ctypes.c_double * max(1, len(args)))(*args)
+            st = (ctypes.c_int * len(starts))(*starts)
+            out = ctypes.c_int()
+            native.call("pgb_case_add_bc", self.case, kind, o, a, st, len(entry.values), ctypes.byref(out))
+            ids[name] = out.value
+        for blk in self.mesh_blocks:
+            for face in blk.intfaces:
+                if face.nbr is None:
+                    native.call("pgb_case_set_face_bc", self.case, blk.nblki, face.nface, ids[face.bcname])
 
     def __del__(self):
         case = getattr(self, "case", None)
@@ -237,9 +261,14 @@ class Solver:
 
     def rhs(self, *, Q="Q", dQ=None):
         dQ = dQ or self.regs[-1]
+        if self.has_bcs:
+            native.call("pgb_set_time", self.case, float(self.tme))
         native.call("pgb_rhs", self.case, self.regnum[Q], self.regnum[dQ])
 
     def step(self, dt, nsteps=1):
+        # the boundaries read the clock from the step's start on
+        if self.has_bcs:
+            native.call("pgb_set_time", self.case, float(self.tme))
         native.call("pgb_step", self.case, float(dt), int(nsteps), self.path, int(self.graph))
         self.nrt += nsteps
         self.tme += dt * nsteps
