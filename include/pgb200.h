@@ -277,6 +277,20 @@ int pgb_rhs(pgb_case *c, int q, int dq);
  * graph and replays it.  Returns when queued on the case's stream. */
 int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph);
 
+/* nsteps steps under the cfl controller (peregrine/integrators/controllers.py:21-30,
+ * peregrine/multiblock/solver.py:366-370): each step's size is
+ * min(cfl / the combined CFL number per unit step of its start, dtmax), worked
+ * out on the device, so the steps queue (and a graph replays them) without a
+ * host round trip; the clock moves on by each step's size (pgb_get_time,
+ * pgb_last_dt read them back).  Returns when queued. */
+int pgb_step_cfl(pgb_case *c, double cfl, double dtmax, int nsteps, int path, int graph);
+/* the largest acoustic, convective and combined CFL number per unit step over
+ * every block's interior of logical register reg, out[3] (the reference's
+ * cflmax, peregrine/simulator/euler/kernels/cflmax.mako, solver.py:292-296) */
+int pgb_cflmax(pgb_case *c, int reg, double *out);
+/* the step size of the last step queued */
+int pgb_last_dt(pgb_case *c, double *dt);
+
 /* nsteps steps without a graph, a CUDA event between every launch; waits for
  * them and returns each launch's device time (ms) and kind (0 halo fill,
  * 1 fused stage, 2 per-block kernel, 3 combine) in launch order, up to cap

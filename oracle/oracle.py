@@ -203,7 +203,7 @@ def _lib():
     lib.oracle_advective_faces.restype = ctypes.c_int
     for name in ("oracle_production", "oracle_gibbs", "oracle_tlog", "oracle_texp", "oracle_mathtables",
                  "oracle_species_cph", "oracle_fromQ", "oracle_prestep", "oracle_realgas_frompT",
-                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads"):
+                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads", "oracle_cflmax"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 
@@ -506,6 +506,14 @@ class Oracle:
             raise RuntimeError(f"oracle_rhs: {rc}")
         if faces:
             return [fl[3 * b:3 * b + 3] for b in range(len(self.blocks))]
+
+    def cflmax(self, Q=None):
+        """(acoustic, convective, combined): the largest CFL number per unit
+        step of each over every block's interior of register Q (regs[0])."""
+        obs = self._oblocks(self.regs[0] if Q is None else Q)
+        out = np.zeros(3)
+        self.lib.oracle_cflmax(ctypes.byref(self.case), obs, len(self.blocks), _ptr(out))
+        return dict(zip(("acoustic", "convective", "combined"), out))
 
     def bc_grads(self, grads, t=None):
         """The boundaries' gradient hook alone on grads[b] ([X][Y][Z][ngrad][3]

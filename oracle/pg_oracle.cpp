@@ -1810,6 +1810,62 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
   return 0;
 }
 
+// cflmax over every block's interior (simulator/euler/kernels/cflmax.mako:2-33
+// with the cell lengths of multiblock/block/grid.py:164-176): the largest
+// acoustic, convective and combined CFL number per unit step, out[3]; the
+// state from Q as the stage's fromQ makes it (the cell's Tg as the guess)
+int oracle_cflmax(const OCase *cp, const OBlock *blocks, int nblocks, double *out) {
+  const OCase &c = *cp;
+  const int ne = 4 + c.ns;
+  double m[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < nblocks; b++) {
+    const OBlock &B = blocks[b];
+    const Dims d = cells(B);
+    const int n[3] = {B.nx, B.ny, B.nz};
+    const int g = B.ng;
+    for (int i = g; i < g + B.nx; i++)
+      for (int j = g; j < g + B.ny; j++)
+        for (int k = g; k < g + B.nz; k++) {
+          const long at = d.at(i, j, k);
+          const double *Q = B.Q + at * ne;
+          State st;
+          if (c.realgas) {
+            double rec[NSTATE] = {};
+            if (c.df) std::memcpy(rec, B.pst + at * NSTATE, sizeof(double) * NSTATE);
+            rstate(c, Q, rec, B.Tg ? B.Tg[at] : 0.0, c.df != 0);
+            std::memcpy(&st, rec, sizeof(State));
+          } else {
+            st = fromQ(c, Q, B.Tg ? B.Tg[at] : 0.0);
+          }
+          const double rhoinv = 1.0 / Q[0];
+          const double u = Q[1] * rhoinv, v = Q[2] * rhoinv, w = Q[3] * rhoinv;
+          double dl[3], un[3];
+          for (int a = 0; a < 3; a++) {
+            const Dims f = face_dims(B, a);
+            const long lo = f.at(i, j, k), hi = f.at(i + (a == 0), j + (a == 1), k + (a == 2));
+            const double *L = B.S[a] + lo * 3, *H = B.S[a] + hi * 3;
+            const double *xl = B.xf[a] + lo * 3, *xh = B.xf[a] + hi * 3;
+            const double s0 = xh[0] - xl[0], s1 = xh[1] - xl[1], s2 = xh[2] - xl[2];
+            // an axis one cell thick is not marched in: infinitely long
+            dl[a] = n[a] == 1 ? INFINITY : std::sqrt(s0 * s0 + s1 * s1 + s2 * s2);
+            const double S0inv = 1.0 / std::sqrt((L[0]) * (L[0]) + (L[1]) * (L[1]) + (L[2]) * (L[2]));
+            const double S1inv = 1.0 / std::sqrt((H[0]) * (H[0]) + (H[1]) * (H[1]) + (H[2]) * (H[2]));
+            const double nx = 0.5 * (L[0] * S0inv + H[0] * S1inv);
+            const double ny = 0.5 * (L[1] * S0inv + H[1] * S1inv);
+            const double nz = 0.5 * (L[2] * S0inv + H[2] * S1inv);
+            un[a] = std::fabs(nx * u + ny * v + nz * w);
+          }
+          const double acoustic = st.c * std::sqrt(1.0 / (dl[0] * dl[0]) + 1.0 / (dl[1] * dl[1]) + 1.0 / (dl[2] * dl[2]));
+          const double convective = un[0] / dl[0] + un[1] / dl[1] + un[2] / dl[2];
+          m[0] = std::fmax(m[0], acoustic);
+          m[1] = std::fmax(m[1], convective);
+          m[2] = std::fmax(m[2], acoustic + convective);
+        }
+  }
+  for (int q = 0; q < 3; q++) out[q] = m[q];
+  return 0;
+}
+
 // The boundaries' gradient hook alone on given gradient arrays, grads[b]
 // [..][ngrad][3] over block b's full extents (the reference's postgrads)
 int oracle_bc_grads(const OCase *cp, const OBlock *blocks, double **grads) {

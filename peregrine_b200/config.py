@@ -156,6 +156,12 @@ class Config(dict):
             raise ConfigError("chem-integration.kind", "null or coupled")
         if kind is not None and self["mixture"]["chemistry"] is None:
             raise ConfigError("chem-integration.kind", "set without mixture.chemistry")
+        if sim["controller"] not in ("fixed", "cfl"):
+            raise ConfigError("simulation.controller", f"{sim['controller']!r} is not one of ('fixed', 'cfl')")
+        for key in ("cfl", "dt-max"):
+            sim[key] = float(sim[key])
+            if not sim[key] > 0.0:
+                raise ConfigError(f"simulation.{key}", "a positive number")
         launch = self["backend-b200"]["launch"]
         if launch not in ("batched", "per-block"):
             raise ConfigError("backend-b200.launch", "batched or per-block")

@@ -35,8 +35,9 @@ PGB_PLAIN_DECL(11)
 PGB_PLAIN_DECL(12)
 
 namespace {
-#define PGB_OPS(N) \
-  {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N, pgb_plain_prestep_##N}
+#define PGB_OPS(N)                                                                                          \
+  {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N, pgb_plain_prestep_##N, \
+   pgb_plain_cflmax_##N}
 // the per-block path of each species count, 1 to MAXNS
 const PlainOps kPlain[MAXNS] = {PGB_OPS(1), PGB_OPS(2), PGB_OPS(3), PGB_OPS(4),  PGB_OPS(5),  PGB_OPS(6),
                                 PGB_OPS(7), PGB_OPS(8), PGB_OPS(9), PGB_OPS(10), PGB_OPS(11), PGB_OPS(12)};
@@ -69,6 +70,11 @@ int fail(int code, const std::string &msg) {
 static __global__ void k_setscalar(double *p, double v) { *p = v; }
 // the clock at a step's end: start + dt (peregrine/multiblock/solver.py:355-364)
 static __global__ void k_clock(double *clock, const double *dt) { *clock = *clock + *dt; }
+// the cfl controller's step: min(cfl / the combined CFL number per unit step,
+// dt-max), ctrl = {cfl, dt-max} (peregrine/integrators/controllers.py:21-30)
+static __global__ void k_cfldt(double *dt, const double *cfl, const double *ctrl) {
+  *dt = fmin(ctrl[0] / cfl[2], ctrl[1]);
+}
 
 struct HostBlock {
   int nx, ny, nz;
@@ -154,6 +160,11 @@ struct pgb_case {
   int nbcface[3] = {0, 0, 0};
   long long bcthreads[3] = {0, 0, 0};
   double *d_clock = nullptr;
+  // the cfl controller: its reduction's three maxima, its {cfl, dt-max}, whether
+  // the steps run under it, and the mode each path's graph was captured in
+  double *d_cfl = nullptr, *d_ctrl = nullptr;
+  bool ctrl_cfl = false;
+  bool graph_cfl[2] = {false, false};
 };
 
 namespace {
@@ -759,10 +770,32 @@ int fused_attrs(pgb_case *c) {
 }
 
 // one step of the fused path at the current phase
+PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb);
+struct MarkCtx;
+void mark_cb(void *ctx, int kind);
+
+// the CFL reduction of physical register qphys into d_cfl
+int cfl_pass(pgb_case *c, int qphys, int &count);
+
+// under the cfl controller a step opens with the reduction of its start
+// register and the step size it gives (peregrine/multiblock/solver.py:366-370)
+int cfl_prologue(pgb_case *c, int qphys, int &count) {
+  if (!c->ctrl_cfl) return PGB_OK;
+  RET(cfl_pass(c, qphys, count));
+  k_cfldt<<<1, 1, 0, c->stream>>>(c->d_dt, c->d_cfl, c->d_ctrl);
+  mark(c, K_COMBINE, count);
+  return PGB_OK;
+}
+
 int step_fused(pgb_case *c, int &count) {
   const auto &plan = c->plans[c->phase];
+  RET(cfl_prologue(c, plan[0].qin, count));
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int) * plan.size(), c->stream));
   for (int s = 0; s < (int)plan.size(); s++) RET(launch_fused(c, plan[s], s, count));
+  if (c->ctrl_cfl) {
+    k_clock<<<1, 1, 0, c->stream>>>(c->d_clock, c->d_dt);
+    mark(c, K_COMBINE, count);
+  }
   c->phase = (c->phase + 1) % c->period;
   c->phys_of = c->maps[c->phase];
   return PGB_OK;
@@ -868,9 +901,20 @@ int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count, double tfrac = 0.0
   return kPlain[c->phys.ns - 1].rhs(&pc, c->d_reg[qphys], c->d_reg[dqphys]);
 }
 
+int cfl_pass(pgb_case *c, int qphys, int &count) {
+  CK(cudaMemsetAsync(c->d_cfl, 0, sizeof(double) * 3, c->stream));
+  std::vector<BlockDev> hb;
+  PlainCase pc = plain_case(c, hb);
+  MarkCtx mc{c, &count};
+  pc.mark = mark_cb;
+  pc.ctx = &mc;
+  return kPlain[c->phys.ns - 1].cflmax(&pc, c->d_reg[qphys], c->d_cfl);
+}
+
 int step_plain(pgb_case *c, int &count) {
   const int TH = 256;
   const auto &map = c->phys_of;
+  if (!c->stages.empty()) RET(cfl_prologue(c, map[c->stages[0].q], count));
   if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count, 0));
   for (const pgb_stage &st : c->stages) {
     RET(rhs_plain(c, map[st.q], map[st.dq], count, st.tfrac));
@@ -894,8 +938,8 @@ int step_plain(pgb_case *c, int &count) {
       }
     }
   }
-  // the boundaries' clock moves on by dt; a case without boundaries reads none
-  if (c->nbcface[0]) {
+  // the clock moves on by dt where boundaries read it or the step size is the device's
+  if (c->nbcface[0] || c->ctrl_cfl) {
     k_clock<<<1, 1, 0, c->stream>>>(c->d_clock, c->d_dt);
     mark(c, K_COMBINE, count);
   }
@@ -953,8 +997,11 @@ int build_bcs(pgb_case *c) {
 int prepare(pgb_case *c, bool fused) {
   if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
   RET(set_current(c));
-  if (!c->uniform_done) {
-    RET(detect_uniform(c, fused));
+  // the uniform forms are the batched path's alone: the per-block path reads
+  // the metric arrays, so a per-block call leaves the detection to the first
+  // batched step
+  if (fused && !c->uniform_done) {
+    RET(detect_uniform(c, true));
     bool all = true;
     for (auto &B : c->blocks) all = all && B.dev.uniform;
     if (all != c->use_v2) c->tiles_dirty = true;
@@ -1057,7 +1104,8 @@ int pgb_case_destroy(pgb_case *c) {
     if (r) cudaFree(r);
   void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
-                  c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock};
+                  c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
+                  c->d_cfl, c->d_ctrl};
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1331,6 +1379,9 @@ int pgb_case_finalize(pgb_case *c) {
   CK(cudaMalloc(&c->d_dt, sizeof(double)));
   CK(cudaMalloc(&c->d_clock, sizeof(double)));
   CK(cudaMemsetAsync(c->d_clock, 0, sizeof(double), c->stream));
+  CK(cudaMalloc(&c->d_cfl, sizeof(double) * 3));
+  CK(cudaMemsetAsync(c->d_cfl, 0, sizeof(double) * 3, c->stream));
+  CK(cudaMalloc(&c->d_ctrl, sizeof(double) * 2));
   RET(build_bcs(c));
   CK(cudaMalloc(&c->d_counter, sizeof(unsigned int) * 16));
   CK(cudaMalloc(&c->d_blks, sizeof(BlockDev) * c->blocks.size()));
@@ -1484,30 +1535,23 @@ int pgb_rhs(pgb_case *c, int q, int dq) {
   return PGB_OK;
 }
 
-int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph) {
-  if (!c) return fail(PGB_ERR_ARG, "null case");
-  if (nsteps < 0) return fail(PGB_ERR_ARG, "negative step count");
-  if (path != PGB_PATH_BATCHED && path != PGB_PATH_PER_BLOCK) return fail(PGB_ERR_ARG, "no such path");
+// nsteps steps at the step size in d_dt (or the cfl controller's, with
+// ctrl_cfl): whole graph units while they fit, single steps after
+static int step_loop(pgb_case *c, int nsteps, int path, int graph) {
   const bool fused = path == PGB_PATH_BATCHED;
-  if (fused && !fused_capable(c))
-    return fail(PGB_ERR_UNSUPPORTED, "the batched path takes the single-species cpg kepaec case; use the per-block path");
-  RET(prepare(c, fused));
-  if (!fused) RET(ensure_scratch(c));
-  if (!fused && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
-  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
-  CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev0, c->stream));
   int done = 0;
   while (done < nsteps) {
     const int unit = fused ? c->period : 1;
     if (graph && c->phase == 0 && nsteps - done >= unit) {
       cudaGraphExec_t &ge = c->graph[path];
-      if (ge && c->graph_map[path] != c->phys_of) {
+      if (ge && (c->graph_map[path] != c->phys_of || c->graph_cfl[path] != c->ctrl_cfl)) {
         cudaGraphExecDestroy(ge);
         ge = nullptr;
       }
       if (!ge) {
         c->graph_map[path] = c->phys_of;
+        c->graph_cfl[path] = c->ctrl_cfl;
         cudaGraph_t g;
         int count = 0;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1537,6 +1581,58 @@ int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph) {
     done += 1;
   }
   CK(cudaEventRecord(c->ev1, c->stream));
+  return PGB_OK;
+}
+
+static int step_begin(pgb_case *c, int nsteps, int path) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (nsteps < 0) return fail(PGB_ERR_ARG, "negative step count");
+  if (path != PGB_PATH_BATCHED && path != PGB_PATH_PER_BLOCK) return fail(PGB_ERR_ARG, "no such path");
+  const bool fused = path == PGB_PATH_BATCHED;
+  if (fused && !fused_capable(c))
+    return fail(PGB_ERR_UNSUPPORTED, "the batched path takes the single-species cpg kepaec case; use the per-block path");
+  RET(prepare(c, fused));
+  if (!fused) RET(ensure_scratch(c));
+  if (!fused && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
+  return PGB_OK;
+}
+
+int pgb_step(pgb_case *c, double dt, int nsteps, int path, int graph) {
+  RET(step_begin(c, nsteps, path));
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
+  CK(cudaGetLastError());
+  c->ctrl_cfl = false;
+  return step_loop(c, nsteps, path, graph);
+}
+
+int pgb_step_cfl(pgb_case *c, double cfl, double dtmax, int nsteps, int path, int graph) {
+  if (!(cfl > 0.0) || !(dtmax > 0.0)) return fail(PGB_ERR_ARG, "cfl and dt-max are positive");
+  RET(step_begin(c, nsteps, path));
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_ctrl, cfl);
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_ctrl + 1, dtmax);
+  CK(cudaGetLastError());
+  c->ctrl_cfl = true;
+  const int rc = step_loop(c, nsteps, path, graph);
+  c->ctrl_cfl = false;
+  return rc;
+}
+
+int pgb_cflmax(pgb_case *c, int reg, double *out) {
+  if (!c || !out) return fail(PGB_ERR_ARG, "null argument");
+  RET(prepare(c, false));
+  if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  int count = 0;
+  RET(cfl_pass(c, c->phys_of[reg], count));
+  CK(cudaMemcpyAsync(out, c->d_cfl, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_last_dt(pgb_case *c, double *dt) {
+  if (!c || !dt) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  CK(cudaMemcpyAsync(dt, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
 }
 

@@ -64,6 +64,7 @@ struct PlainOps {
   int (*fromprims)(const PlainCase *, int blk, const double *prims, double *Q);
   int (*production)(long long n, const double *rho, const double *Y, const double *T, double *omega, cudaStream_t);
   int (*prestep)(const PlainCase *, double *Q, int first);
+  int (*cflmax)(const PlainCase *, const double *Q, double *out);
 };
 
 }  // namespace pgb
@@ -78,4 +79,6 @@ struct PlainOps {
                                                                                const double *, double *);        \
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_production_##N(                                 \
       long long, const double *, const double *, const double *, double *, cudaStream_t);                        \
-  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_prestep_##N(const pgb::PlainCase *, double *, int);
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_prestep_##N(const pgb::PlainCase *, double *, int); \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_cflmax_##N(const pgb::PlainCase *, const double *,  \
+                                                                            double *);

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "bc.cuh"
+#include "cfl.cuh"
 #include "chem.cuh"
 #include "pgb200.h"
 #include "plain.cuh"
@@ -279,6 +280,24 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
   }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "per-block launch");
+}
+
+// the CFL reduction of register Q over every block's interior into out[0..2],
+// which the caller zeroed: one launch, a grid row per block
+extern "C" int PGB_ENTRY(pgb_plain_cflmax_)(const PlainCase *pc, const double *Q, double *out) {
+  long long most = 0;
+  for (int b = 0; b < pc->nblocks; b++) {
+    const BlockDev &D = pc->h_blks[b];
+    most = std::max(most, (long long)D.nx * D.ny * D.nz);
+  }
+  const dim3 g(grid_of(most), (unsigned)pc->nblocks, 1);
+  if (pc->realgas)
+    k_cflmax<NS, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, 0, Q, pc->state, pc->met, out, pc->df);
+  else
+    k_cflmax<NS, false><<<g, TH, 0, pc->stream>>>(pc->d_blks, 0, Q, pc->state, pc->met, out, 0);
+  mark(pc, 2);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PGB_OK : cuda_fail(e, "cflmax");
 }
 
 // Q and the state of one block's interior from its primitives

@@ -86,3 +86,36 @@ def stage_records(name):
                 c.w[n] = w
             c.step = int(cb["step"])
     return recs, nregs
+
+
+class Fixed:
+    """The fixed step: the config's dt (peregrine/integrators/controllers.py:12-17)."""
+
+    name = "fixed"
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+
+    def stepsize(self, solver):
+        return self.cfg["simulation"]["dt"]
+
+
+class CFL(Fixed):
+    """The CFL target over the combined CFL number per unit step, under
+    dt-max (peregrine/integrators/controllers.py:20-30; the reference's
+    plugins' output times, which shorten a step, are not built here)."""
+
+    name = "cfl"
+
+    def stepsize(self, solver):
+        sim = self.cfg["simulation"]
+        return min(sim["cfl"] / solver.cflmax()["combined"], sim["dt-max"])
+
+
+class Integrator:
+    """The integrator's name and its step-size controller, as the reference's
+    solver carries them (``solver.integ.controller``)."""
+
+    def __init__(self, cfg):
+        self.name = cfg["time-integration"]["integrator"]
+        self.controller = {"fixed": Fixed, "cfl": CFL}[cfg["simulation"]["controller"]](cfg)

@@ -214,6 +214,9 @@ SIGNATURES = {
     "pgb_set_prims": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_rhs": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_step": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "pgb_step_cfl": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "pgb_cflmax": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "pgb_last_dt": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "pgb_case_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "pgb_last_step_ms": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "pgb_launches_per_step": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),

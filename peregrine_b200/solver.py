@@ -17,7 +17,7 @@ from peregrine_b200 import bcs as bcmod
 from peregrine_b200 import native
 from peregrine_b200.config import ConfigError
 from peregrine_b200.grid import metrics as make_metrics
-from peregrine_b200.integrators import stage_records
+from peregrine_b200.integrators import Integrator, stage_records
 from peregrine_b200.mixture import Mixture
 
 NG = 2
@@ -105,6 +105,7 @@ class Solver:
         self.bcs = bcmod.entries(cfg["bcvals"], sim["simulator"], self.mixture.spnames)
         self.ne = 4 + self.ns
         self.integrator = cfg["time-integration"]["integrator"]
+        self.integ = Integrator(cfg)
         records, nregs = stage_records(self.integrator)
         self.nregs = nregs
         self.regs = tuple(["Q"] + [f"Q{n}" for n in range(1, nregs)])
@@ -274,9 +275,37 @@ class Solver:
         self.tme += dt * nsteps
 
     def run(self):
-        dt = self.cfg["simulation"]["dt"]
-        self.step(dt, self.cfg["simulation"]["niter"])
+        """niter steps under the config's controller (peregrine/multiblock/solver.py:366-370).
+        Under the cfl controller each step's size is worked out on the device
+        from the step's own start, so the steps queue without a host round
+        trip; the clock is read back at the end."""
+        sim = self.cfg["simulation"]
+        n = sim["niter"]
+        if sim["controller"] == "cfl":
+            self.step_cfl(sim["cfl"], sim["dt-max"], n)
+        else:
+            self.step(sim["dt"], n)
         self.backend.sync()
+
+    def step_cfl(self, cfl, dtmax, nsteps=1):
+        native.call("pgb_set_time", self.case, float(self.tme))
+        native.call("pgb_step_cfl", self.case, float(cfl), float(dtmax), int(nsteps), self.path, int(self.graph))
+        self.nrt += nsteps
+        t = ctypes.c_double()
+        native.call("pgb_get_time", self.case, ctypes.byref(t))
+        self.tme = t.value
+
+    def cflmax(self):
+        """The largest acoustic, convective and combined CFL number per unit
+        step over every block's interior of Q (peregrine/multiblock/solver.py:292-296)."""
+        out = (ctypes.c_double * 3)()
+        native.call("pgb_cflmax", self.case, 0, out)
+        return dict(zip(("acoustic", "convective", "combined"), list(out)))
+
+    def last_dt(self):
+        dt = ctypes.c_double()
+        native.call("pgb_last_dt", self.case, ctypes.byref(dt))
+        return dt.value
 
     def last_step_ms(self):
         ms = ctypes.c_float()
