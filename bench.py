@@ -303,6 +303,59 @@ def realgas_leg(steps, cpu=True):
     return out
 
 
+def boundary_leg(steps, cpu=True):
+    """Cell-stage/s of the bounded channel on the per-block path, under the
+    device-side cfl controller, and the boundary passes' share of a step."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases
+
+    cfg = cases.channel_config()
+    mb = pg.get_solver(cfg, cases.channel_mesh(), pg.get_backend("cuda", cfg))
+    sim = cfg["simulation"]
+    mb.step_cfl(sim["cfl"], sim["dt-max"], 3)
+    mb.backend.sync()
+    mb.step_cfl(sim["cfl"], sim["dt-max"], steps)
+    ms = mb.last_step_ms()
+    dt = mb.last_dt()
+    # the same steps at the controller's last size: what the controller's
+    # reduction and step-size kernel cost per step
+    mb.step(dt, steps)
+    ms_fixed = mb.last_step_ms()
+    rows = fused_kernel_times(mb, dt, 2)
+    total = sum(m for m, _ in rows)
+    boundary = sum(m for m, k in rows if k == 4)
+    ncells = mb.ncells
+    value = ncells * 3 * steps / (ms / 1e3)
+    out = {"value": value, "unit": "cell-stage/s", "steps": steps, "ms_per_step": ms / steps,
+           "ms_per_step_fixed_dt": ms_fixed / steps, "controller_overhead": ms / ms_fixed - 1.0,
+           "last_dt": dt, "launches_per_step": mb.launches_per_step(),
+           "boundary_share_of_step": boundary / total if total else None,
+           "boundary_ms_per_step": boundary / 2,
+           "workload": "channel-192x96x96-8-blocks-2sp-ns-muscl-koren-hllc-rk3-cfl-0.8: velocity inflow "
+                       "(expressions of y, z, t), pressure exit, isothermal no-slip floor, moving lid, periodic across",
+           "path": "per-block kernels, boundary passes one launch each over every boundary face"}
+    if cpu:
+        from oracle.oracle import Oracle
+
+        orc = Oracle(mb.mixture.constants(), mb.ns, "navier-stokes", mb.mesh_blocks, mb.metrics, "tvd-rk3",
+                     primary="hllc", recon="muscl", limiter="koren", bcvals=cfg["bcvals"], species=mb.mixture.spnames)
+        ic = cfg["ics"]
+        prims = []
+        for b in mb.mesh_blocks:
+            q = np.empty(tuple(n + 4 for n in b.cells) + (mb.ne,))
+            q[...] = [ic["p"], ic["u"], ic["v"], ic["w"], ic["T"], ic["Y"]["A"]]
+            prims.append(q)
+        orc.set_prims(prims)
+        dQ = [np.zeros_like(r) for r in orc.regs[0]]
+        t0 = time.perf_counter()
+        orc.rhs(orc.regs[0], dQ)
+        wall = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": ncells / wall, "unit": "cell-stage/s", "cores": os.cpu_count(),
+                               "kind": "port", "sample": f"one stage (RHS) of the channel, {wall:.2f} s"}
+    del mb
+    return out
+
+
 def serving_leg(n=300, rate=60.0, steps=100):
     """The serving stream: Poisson arrivals of H2/air closed reactors and
     periodic 1-D domains, admitted into one pool while others run."""
@@ -404,6 +457,8 @@ def main():
     ap.add_argument("--realgas-only", action="store_true", help="the real-gas leg alone")
     ap.add_argument("--no-realgas", action="store_true", help="skip the real-gas leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--boundary-only", action="store_true", help="the bounded channel leg alone")
+    ap.add_argument("--no-boundary", action="store_true", help="skip the bounded channel leg")
     args = ap.parse_args()
     set_cells(args.cells)
     args.warmup = max(3, args.warmup)
@@ -412,6 +467,9 @@ def main():
         return
     if args.realgas_only:
         print(json.dumps({"realgas": realgas_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
+        return
+    if args.boundary_only:
+        print(json.dumps({"boundary": boundary_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
         return
     if args.serving_only:
         print(json.dumps({"serving": serving_leg()}), flush=True)
@@ -483,6 +541,20 @@ def main():
 
     from peregrine_b200 import native
 
+    # the cfl controller on the headline: the same steps with the device's
+    # reduction and step-size kernel ahead of each (dt-max the fixed dt, so
+    # the steps are the same size)
+    cfl_cost = None
+    if not args.no_extra:
+        cfl_steps = max(3, min(args.steps // 4, 50))
+        mb.step_cfl(1e6, dt, 2)
+        mb.step_cfl(1e6, dt, cfl_steps)
+        ms_c = mb.last_step_ms()
+        mb.step(dt, cfl_steps)
+        ms_f = mb.last_step_ms()
+        cfl_cost = {"ms_per_step": ms_c / cfl_steps, "ms_per_step_fixed": ms_f / cfl_steps,
+                    "overhead": ms_c / ms_f - 1.0, "cflmax": mb.cflmax()}
+
     per_block, e2e = None, None
     if not args.no_extra:
         # the plain per-block path
@@ -517,6 +589,9 @@ def main():
     realgas = None
     if rank == 0 and not args.no_realgas and not args.no_extra:
         realgas = realgas_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
+    boundary = None
+    if rank == 0 and not args.no_boundary and not args.no_extra:
+        boundary = boundary_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
 
     if rank == 0:
         line = {
@@ -539,6 +614,8 @@ def main():
             "reacting": reacting,
             "serving": served,
             "realgas": realgas,
+            "boundary": boundary,
+            "cfl": cfl_cost,
             "e2e": e2e,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),

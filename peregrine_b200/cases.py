@@ -332,3 +332,41 @@ def bc_box_prims(metrics, ns, seed=0, speed=200.0):
             q[..., 5 + n] = 0.9 / (ns - 1) * (0.5 + 0.4 * np.cos((n + 1) * x + y + ph[5]) ** 2)
         out.append(q)
     return out
+
+
+# the bounded channel: a box of air and a second gas between a still
+# isothermal wall and a moving lid, periodic across, a velocity inflow whose
+# profile and temperature move with position and time, and a pressure exit;
+# Navier-Stokes with MUSCL-koren and HLLC, TVD-RK3 under the cfl controller
+CHANNEL_CELLS = (192, 96, 96)
+CHANNEL_BLOCKS = (2, 2, 2)
+CHANNEL_LENGTHS = (0.04, 0.02, 0.02)
+
+
+def channel_config(launch="per-block", cfl=0.8):
+    cfg = Config()
+    cfg["simulation"]["simulator"] = "navier-stokes"
+    cfg["simulation"]["controller"] = "cfl"
+    cfg["simulation"]["cfl"] = cfl
+    cfg["simulation"]["dt-max"] = 1e-5
+    cfg["mixture"]["species"] = {k: MIXED[k] for k in ("A", "B")}
+    cfg["mixture"]["trans"] = "constant"
+    cfg["time-integration"]["integrator"] = "tvd-rk3"
+    cfg["adv-flux"]["primary"] = "hllc"
+    cfg["adv-flux"]["recon"] = "muscl"
+    cfg["adv-flux"]["limiter"] = "koren"
+    cfg["backend-b200"]["launch"] = launch
+    cfg["ics"].update(p=P0, u=30.0, T=T0, Y={"A": 0.5})
+    h = CHANNEL_LENGTHS[1]
+    cfg["bcvals"]["inflow"] = {"kind": "sub-in-fvt", "u": f"60.0 * (y / {h}) * (1.0 - y / {h}) * 4.0 + 5.0 * sin(2000.0 * t)",
+                               "v": 0.0, "w": "2.0 * sin(300.0 * z)", "T": "300.0 + 20.0 * cos(300.0 * z)", "A": 0.6}
+    cfg["bcvals"]["exit"] = {"kind": "sub-out-fp", "p": P0}
+    cfg["bcvals"]["floor"] = {"kind": "no-slp-isot-wall", "T": 320.0}
+    cfg["bcvals"]["lid"] = {"kind": "mov-adia-wall", "u": 20.0, "v": 0.0, "w": 0.0}
+    return cfg.validate()
+
+
+def channel_mesh(cells=CHANNEL_CELLS, blocks=CHANNEL_BLOCKS):
+    cuts = [[n // b + (1 if m < n - (n // b) * b else 0) for m in range(b)] for n, b in zip(cells, blocks)]
+    return CubeMesher(mbdims=list(blocks), cells=cuts, lengths=list(CHANNEL_LENGTHS), periodic=[False, False, True],
+                      bcnames={1: "inflow", 2: "exit", 3: "floor", 4: "lid"})

@@ -23,46 +23,51 @@ __device__ inline void cfl_atomic_max(double *slot, const double v) {
 // convective, combined), which the caller zeroed.  A NaN cell is passed
 // over, as fmax passes it.
 template <int NS, bool RG>
-__global__ void k_cflmax(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                         const double *__restrict__ stall, const double *__restrict__ met, double *out,
-                         const int plane = 0) {
+__device__ inline void cfl_cell(const BlockDev &B, const long long t, const double *__restrict__ Qall,
+                                const double *__restrict__ stall, const double *__restrict__ met, const int plane,
+                                double *m) {
   constexpr int NE = 4 + NS;
-  const BlockDev &B = blks[b + blockIdx.y];
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double m[3] = {0.0, 0.0, 0.0};
-  if (t < (long long)B.nx * B.ny * B.nz) {
-    const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
-    const long long c = cell_index(B, i, j, k), v = B.vol;
-    const double *Q = Qall + NE * B.cv + c;
-    auto Qf = [&](int l) { return Q[l * v]; };
-    const double *st = stall ? stall + SW * B.cv + c : nullptr;
-    const double Tg = st ? st[1 * v] : 0.0;
-    double cs;
-    if (RG) {
-      const double rho = Qf(0), rhoinv = 1.0 / rho;
-      auto Y = [&](int n) { return Qf(5 + n) * rhoinv; };
-      const RGMom mom = mixmom_rg<NS>(Y);
-      const double q1 = Qf(1), q2 = Qf(2), q3 = Qf(3);
-      if (plane && st) {
-        double composition = 0.0;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k), v = B.vol;
+  const double *Q = Qall + NE * B.cv + c;
+  auto Qf = [&](int l) { return Q[l * v]; };
+  const double *st = stall ? stall + SW * B.cv + c : nullptr;
+  const double Tg = st ? st[1 * v] : 0.0;
+  double cs;
+  if (RG) {
+    const double rho = Qf(0), rhoinv = 1.0 / rho;
+    auto Y = [&](int n) { return Qf(5 + n) * rhoinv; };
+    const RGMom mom = mixmom_rg<NS>(Y);
+    const double q1 = Qf(1), q2 = Qf(2), q3 = Qf(3);
+    if (plane && st) {
+      double composition = 0.0;
 #pragma unroll
-        for (int n = 0; n < NS - 1; n++) composition += st[(ST_ZETA + n) * v] * Qf(5 + n);
-        const double p = (Qf(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv - st[ST_EPS * v] * Qf(0) -
-                          composition - st[ST_KAPPA * v]) / st[ST_THETA * v];
-        cs = fromrhop_rg<NS>(mom, Y, rho, p, Tg).s.c;
-      } else {
-        const double e = (Qf(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv) * rhoinv;
-        cs = fromrhoE_rg<NS>(mom, Y, rho, e, Tg).s.c;
-      }
+      for (int n = 0; n < NS - 1; n++) composition += st[(ST_ZETA + n) * v] * Qf(5 + n);
+      const double p = (Qf(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv - st[ST_EPS * v] * Qf(0) -
+                        composition - st[ST_KAPPA * v]) / st[ST_THETA * v];
+      cs = fromrhop_rg<NS>(mom, Y, rho, p, Tg).s.c;
     } else {
-      cs = fromQ<NS>(Qf, Tg).c;
+      const double e = (Qf(4) - 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) * rhoinv) * rhoinv;
+      cs = fromrhoE_rg<NS>(mom, Y, rho, e, Tg).s.c;
     }
+  } else {
+    cs = fromQ<NS>(Qf, Tg).c;
+  }
+  const int n[3] = {B.nx, B.ny, B.nz};
+  const double rhoinv = 1.0 / Qf(0);
+  const double vel[3] = {Qf(1) * rhoinv, Qf(2) * rhoinv, Qf(3) * rhoinv};
+  double d[3], un[3];
+  if (B.uniform) {
+    // a uniform block's faces are its axes and its cells one length per
+    // axis: the unit normals' mean is the axis, the length the spacing
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      d[a] = n[a] == 1 ? (double)INFINITY : fabs(B.ex[a]);
+      un[a] = fabs(vel[a]);
+    }
+  } else {
     const double *mb = met + M_NCOMP * B.cv;
     const long long step[3] = {1, B.X, (long long)B.X * B.Y};
-    const int n[3] = {B.nx, B.ny, B.nz};
-    const double rhoinv = 1.0 / Qf(0);
-    const double u = Qf(1) * rhoinv, vv = Qf(2) * rhoinv, w = Qf(3) * rhoinv;
-    double d[3], un[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const double *S = mb + (M_S + 3 * a) * v + c;
@@ -80,14 +85,32 @@ __global__ void k_cflmax(const BlockDev *__restrict__ blks, int b, const double 
       const double nx = 0.5 * (L0 * S0inv + H0 * S1inv);
       const double ny = 0.5 * (L1 * S0inv + H1 * S1inv);
       const double nz = 0.5 * (L2 * S0inv + H2 * S1inv);
-      un[a] = fabs(nx * u + ny * vv + nz * w);
+      un[a] = fabs(nx * vel[0] + ny * vel[1] + nz * vel[2]);
     }
-    const double acoustic = cs * sqrt(1.0 / (d[0] * d[0]) + 1.0 / (d[1] * d[1]) + 1.0 / (d[2] * d[2]));
-    const double convective = un[0] / d[0] + un[1] / d[1] + un[2] / d[2];
-    m[0] = fmax(0.0, acoustic);
-    m[1] = fmax(0.0, convective);
-    m[2] = fmax(0.0, acoustic + convective);
   }
+  const double acoustic = cs * sqrt(1.0 / (d[0] * d[0]) + 1.0 / (d[1] * d[1]) + 1.0 / (d[2] * d[2]));
+  const double convective = un[0] / d[0] + un[1] / d[1] + un[2] / d[2];
+  m[0] = fmax(m[0], acoustic);
+  m[1] = fmax(m[1], convective);
+  m[2] = fmax(m[2], acoustic + convective);
+}
+
+// one grid row per block, its CTAs striding over the block's interior cells
+// (a few hundred CTAs in all, so the atomics stay few); the sound speed of
+// the state fromQ makes of Q (the cell's stored T as the iterative eos's
+// starting guess when there is a state; with plane, the double flux's p off
+// the cell's frozen plane); each CTA's maxima folded into out[0..2]
+// (acoustic, convective, combined), which the caller zeroed.  A NaN cell is
+// passed over, as fmax passes it.
+template <int NS, bool RG>
+__global__ void __launch_bounds__(256, RG ? 2 : 3) k_cflmax(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                         const double *__restrict__ stall, const double *__restrict__ met, double *out,
+                         const int plane = 0) {
+  const BlockDev &B = blks[b + blockIdx.y];
+  const long long n = (long long)B.nx * B.ny * B.nz;
+  double m[3] = {0.0, 0.0, 0.0};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    cfl_cell<NS, RG>(B, t, Qall, stall, met, plane, m);
   // the warp's maxima, then the CTA's, then one atomic per slot
   __shared__ double red[3][32];
 #pragma unroll

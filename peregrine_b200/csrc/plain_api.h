@@ -54,7 +54,7 @@ struct PlainCase {
   const double *clock, *dt;
   double tfrac;
   cudaStream_t stream;
-  void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block
+  void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block, 4 boundary, 5 CFL
   void *ctx;
 };
 

@@ -174,19 +174,19 @@ static void bc_halo_launch(const PlainCase *pc, const double *Q) {
     k_bc_halo<NS, false><<<grid_of(pc->bchalo_n), TH, 0, pc->stream>>>(
         pc->d_blks, pc->bchalo, pc->nbchalo, pc->bcent, pc->bcops, const_cast<double *>(Q), pc->state, pc->met,
         pc->clock, pc->dt, pc->tfrac);
-  mark(pc, 0);
+  mark(pc, 4);
 }
 static void bc_grads_launch(const PlainCase *pc) {
   if (!pc->nbcgrad) return;
   k_bc_grads<NS><<<grid_of(pc->bcgrad_n), TH, 0, pc->stream>>>(pc->d_blks, pc->bcgrad, pc->nbcgrad, pc->grads);
-  mark(pc, 0);
+  mark(pc, 4);
 }
 static void bc_wall_launch(const PlainCase *pc, const double *Q) {
   if (!pc->nbcwall) return;
   k_bc_wall<NS><<<grid_of(pc->bcwall_n), TH, 0, pc->stream>>>(
       pc->d_blks, pc->bcwall, pc->nbcwall, pc->bcent, pc->bcops, Q, pc->state, pc->tr, pc->met, pc->F[0], pc->F[1],
       pc->F[2], NE + (pc->df ? 1 : 0), pc->visc, pc->clock, pc->dt, pc->tfrac);
-  mark(pc, 2);
+  mark(pc, 4);
 }
 
 // one right-hand side of every block: Q's halo, the state everywhere, the
@@ -290,12 +290,14 @@ extern "C" int PGB_ENTRY(pgb_plain_cflmax_)(const PlainCase *pc, const double *Q
     const BlockDev &D = pc->h_blks[b];
     most = std::max(most, (long long)D.nx * D.ny * D.nz);
   }
-  const dim3 g(grid_of(most), (unsigned)pc->nblocks, 1);
+  // about eight CTAs per SM in all, each striding over its block's cells
+  const long long want = std::max<long long>(1, (8 * 148 + pc->nblocks - 1) / pc->nblocks);
+  const dim3 g((unsigned)std::min<long long>(grid_of(most), want), (unsigned)pc->nblocks, 1);
   if (pc->realgas)
     k_cflmax<NS, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, 0, Q, pc->state, pc->met, out, pc->df);
   else
     k_cflmax<NS, false><<<g, TH, 0, pc->stream>>>(pc->d_blks, 0, Q, pc->state, pc->met, out, 0);
-  mark(pc, 2);
+  mark(pc, 5);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "cflmax");
 }

@@ -50,6 +50,24 @@ def test_cflmax_matches_the_oracle_on_a_jostled_multiblock_case(launch):
     close(mb.cflmax(), orc.cflmax(), 1e-12)
 
 
+def test_cflmax_on_uniform_blocks_matches_the_oracle():
+    # the batched path's first step finds the blocks uniform; the reduction
+    # then takes the uniform form (the axes as normals, the spacing as lengths)
+    import peregrine_b200 as pg
+    from oracle.oracle import Oracle
+
+    cfg = cases.tgv_config("navier-stokes", "rk4", "batched")
+    mesh = cases.tgv_mesh(16, (2, 1, 2), seed=3)
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    prims = cases.tgv_prims(mb.mesh_blocks, mb.metrics, seed=3, noise=1e-3, mach=0.3)
+    mb.set_prims(prims)
+    mb.step(0.0, 1)
+    assert all(mb.uniform(n) for n in range(len(mb.blocks)))
+    orc = Oracle(mb.mixture.constants(), 1, "navier-stokes", mb.mesh_blocks, mb.metrics, "rk4")
+    orc.set_prims(prims)
+    close(mb.cflmax(), orc.cflmax(), 1e-12)
+
+
 @pytest.mark.parametrize("kind,ns,eos", [("sub-in-fvt", 3, "cpg"), ("slp-adia-wall", 1, "cpg"),
                                          ("sup-out-fn", 2, "real-gas")])
 def test_cflmax_matches_the_oracle_on_a_boundary_box(kind, ns, eos):
