@@ -46,9 +46,10 @@ enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1, PGB_EOS_REALGAS = 2, PGB_EOS_REALGAS_DF
 enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2, PGB_FLUX_AUSMUP = 3 };
 enum { PGB_RECON_CONSTANT = 0, PGB_RECON_MUSCL = 1 };
 enum { PGB_TRANS_NONE = 0, PGB_TRANS_CONSTANT = 1, PGB_TRANS_KINETIC = 2 };
-/* chemistry: none, or finite-rate coupled into the right-hand side
- * (peregrine/simulator/chemint/coupled.py) */
-enum { PGB_CHEM_NONE = 0, PGB_CHEM_COUPLED = 1 };
+/* chemistry: none, finite-rate coupled into the right-hand side
+ * (peregrine/simulator/chemint/coupled.py), or sub-stepped over the step with
+ * stiff-cell compaction (peregrine/simulator/chemint/substepped.py) */
+enum { PGB_CHEM_NONE = 0, PGB_CHEM_COUPLED = 1, PGB_CHEM_SUBSTEPPED = 2 };
 /* the launch paths */
 enum { PGB_PATH_BATCHED = 0, PGB_PATH_PER_BLOCK = 1 };
 
@@ -209,6 +210,17 @@ int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long
  * "cubicdaMW", "vshiftMW" (ns each; peregrine/simulator/mixture/eos/realgas/model.py:43-98) */
 /* the case's finite-rate mechanism, copied; before finalize */
 int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m);
+/* the sub-stepped chemistry's options (the reference's chem-integration
+ * section, peregrine/simulator/chemint/substepped.py:14-33): max-substeps
+ * cap >= 1, bulk-substeps 1 <= bulk <= cap (bulk < cap compacts the stiff
+ * cells into a second pass), stiff-bins 1..16, equilibrium-tolerance
+ * 0 <= eqtol < 1 (0: no exit).  Defaults 200, 1, 8, 1e-7.  Before finalize. */
+int pgb_case_set_substeps(pgb_case *c, int cap, int bulk, int bins, double eqtol);
+/* each interior cell's substep count at the last right-hand side (host F
+ * order, count = the block's interior cells), and the stiff list's header:
+ * head[0] the cells listed, head[1 + b] bin b's, n = bins + 1 */
+int pgb_substeps_get(pgb_case *c, int blk, int *host, long count);
+int pgb_stiff_head(pgb_case *c, unsigned int *head, int n);
 /* net production rates omega[n][ns], kg / m^3 / s, of n states rho[n],
  * Y[n][ns] (every species) and T[n], host arrays, by the device fold */
 int pgb_production(pgb_case *c, long n, const double *rho, const double *Y, const double *T, double *omega);
@@ -290,6 +302,10 @@ int pgb_step_cfl(pgb_case *c, double cfl, double dtmax, int nsteps, int path, in
 int pgb_cflmax(pgb_case *c, int reg, double *out);
 /* the step size of the last step queued */
 int pgb_last_dt(pgb_case *c, double *dt);
+/* the step scalar a right-hand side outside a step reads, the step the
+ * sub-stepped chemistry integrates over (the reference's solver.dt,
+ * peregrine/multiblock/solver.py:34); 0 until a step or this sets it */
+int pgb_set_dt(pgb_case *c, double dt);
 
 /* nsteps steps without a graph, a CUDA event between every launch; waits for
  * them and returns each launch's device time (ms) and kind (0 halo fill,

@@ -46,7 +46,10 @@ class OCase(ctypes.Structure):
                [(n, ctypes.c_double) for n in ("cu", "cw", "csigma", "ceps")] + \
                [(n, ctypes.POINTER(ctypes.c_double)) for n in
                 ("csqrtac", "cb", "cda", "cmTc", "conepm", "vshift", "csqrtacMW", "cbMW", "cdaMW", "vshiftMW")] + \
-               [("nbc", ctypes.c_int), ("bc", ctypes.POINTER(OBc))]
+               [("nbc", ctypes.c_int), ("bc", ctypes.POINTER(OBc)), ("substepped", ctypes.c_int), ("cap", ctypes.c_int),
+                ("eqtol", ctypes.c_double), ("dt", ctypes.c_double), ("ncppoly", ctypes.c_int),
+                ("cppoly", ctypes.POINTER(ctypes.c_double)), ("MW", ctypes.POINTER(ctypes.c_double)),
+                ("cfloor", ctypes.c_double)]
 
 # the boundary kinds (peregrine/simulator/euler/bcs.py, navstokes/bcs.py): the
 # oracle's number for each and the variables an entry gives, in order; the
@@ -130,7 +133,8 @@ class OBlock(ctypes.Structure):
                 ("xcc", ctypes.POINTER(ctypes.c_double)), ("detJinv", ctypes.POINTER(ctypes.c_double)),
                 ("Jinv", ctypes.POINTER(ctypes.c_double)),
                 ("S", ctypes.POINTER(ctypes.c_double) * 3), ("xf", ctypes.POINTER(ctypes.c_double) * 3),
-                ("Tg", ctypes.POINTER(ctypes.c_double)), ("pst", ctypes.POINTER(ctypes.c_double))]
+                ("Tg", ctypes.POINTER(ctypes.c_double)), ("pst", ctypes.POINTER(ctypes.c_double)),
+                ("subs", ctypes.POINTER(ctypes.c_int))]
 
 
 def _side(sp, val):
@@ -312,7 +316,7 @@ class Oracle:
 
     def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0, primary="kepaec",
                  recon="constant", limiter=None, eos="cpg", trans="constant", chemistry=None, bcvals=None,
-                 species=None):
+                 species=None, chemint="coupled", max_substeps=200, eqtol=1e-7):
         """constants: the mixture's tables; blocks/metrics may be empty for face-only use.
         eos "cpg" or "tpg", trans "constant" or "kinetic-theory", chemistry
         None or "finite-rate" (coupled: the source begins dQ).  bcvals: the
@@ -371,6 +375,17 @@ class Oracle:
         if chemistry == "finite-rate":
             self._mech = build_mech(constants)
             c.mech = ctypes.cast(ctypes.pointer(self._mech["mech"]), ctypes.c_void_p)
+        # the sub-stepped integration (chemint "sub-stepped"): the one-pass form
+        # with max_substeps and the exit's tolerance eqtol, over the step dt
+        self.substepped = chemistry == "finite-rate" and chemint == "sub-stepped"
+        self.dt = 0.0
+        if self.substepped:
+            c.substepped, c.cap, c.eqtol = 1, int(max_substeps), float(eqtol)
+            cpp = np.ascontiguousarray(constants["cppoly"], dtype=np.float64)
+            mw = np.ascontiguousarray(constants["MW"], dtype=np.float64)
+            self._tables["cppoly"], self._tables["MW"] = cpp, mw
+            c.ncppoly, c.cppoly, c.MW = cpp.shape[1], _ptr(cpp), _ptr(mw)
+            c.cfloor = float(np.exp(float(constants["logcfloor"])))
         self.case = c
         self.map = halo_map(blocks)
         self.nregs = NREGS[integrator]
@@ -383,6 +398,7 @@ class Oracle:
         self.pst = [np.zeros(self._shape(b)[:3] + (NSTATE,)) for b in blocks] if self.df else None
         self.df_fresh = True
         self.tme = 0.0
+        self.subs = [np.zeros(self._shape(b)[:3], dtype=np.int32) for b in blocks] if self.substepped else None
         self.bcvals = dict(bcvals or {})
         self.species = list(species or [])
         self.bcfaces = []
@@ -435,6 +451,8 @@ class Oracle:
             o.Tg = _ptr(self.Tg[n])
             if self.pst is not None:
                 o.pst = _ptr(self.pst[n])
+            if self.subs is not None:
+                o.subs = self.subs[n].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
             keep.append(o)
         return obs
 
@@ -484,6 +502,7 @@ class Oracle:
         obs = self._oblocks(Q)
         bcs, keep = self._bcs(self.tme if t is None else t)
         self.case.nbc, self.case.bc = len(self.bcfaces), bcs
+        self.case.dt = self.dt
         m = np.ascontiguousarray(self.map)
         ptrs = (ctypes.POINTER(ctypes.c_double) * len(dQ))(*[_ptr(d) for d in dQ])
         fl, fptr = None, None
@@ -573,6 +592,7 @@ class Oracle:
         stages, dQ = stage_combines(self.integrator, names)
         start = self.tme
         fracs = stage_fractions(self.integrator)
+        self.dt = dt
         if self.df:
             if self.df_fresh:
                 self.prestep(self.regs[stages[0][0]])

@@ -62,6 +62,15 @@ struct OCase {
   const double *csqrtac, *cb, *cda, *cmTc, *conepm, *vshift, *csqrtacMW, *cbMW, *cdaMW, *vshiftMW;  // [ns]
   int nbc;                   // boundary faces; a boundary face not listed keeps its halo as set
   const OBc *bc;
+  // the chemistry's integration: 0 the coupled source, 1 sub-stepped over dt
+  // (simulator/chemint/substepped.py) with its cap, the tolerance of its
+  // equilibrium exit, cp / R_sp in ln T [ns][ncppoly], the molar masses and
+  // the exit's concentration floor
+  int substepped, cap;
+  double eqtol, dt;
+  int ncppoly;
+  const double *cppoly, *MW;
+  double cfloor;
 };
 
 // one reaction, the columns of FiniteRateModel.rxnconsts
@@ -101,6 +110,7 @@ struct OBlock {
   const double *S[3], *xf[3];               // faces of axis a: [..][3]
   double *Tg;                               // [..]: each cell's last T, an iterative eos's starting guess
   double *pst;                              // [..][NSTATE]: the double flux's kept state and frozen planes
+  int *subs;                                // [..]: the sub-stepped chemistry's count per cell, or null
 };
 
 // one halo cell of one block filled from a cell of another (the place kernel,
@@ -487,7 +497,8 @@ double troeblend(const OMech &m, const ORxn &r, const RateState &s, double logpr
 
 // one reaction's net rate of progress: the product form (finiterate.mako:66-125)
 // or the log form (finiterate.mako:7-46 and the double fold, :201-214)
-double rate_of_progress(const OMech &m, const ORxn &r, const RateState &s) {
+// one reaction's one-way rates (fwd, rev; rev 0 for an irreversible one)
+void oneway(const OMech &m, const ORxn &r, const RateState &s, double &fwd, double &rev) {
   double lk = r.logA;
   if (r.b != 0.0) lk += r.b * s.logT;
   if (r.EaR != 0.0) lk -= r.EaR * s.Tinv;
@@ -510,10 +521,10 @@ double rate_of_progress(const OMech &m, const ORxn &r, const RateState &s) {
     double K = texp(std::fmin(xk, m.expclamp));
     if (thirdbody && !falloff) K *= s.ctb[r.tb];
     if (falloff) K *= pfac;
-    double fwd = K;
+    fwd = K;
     for (int j = 0; j < r.nreact; j++)
       for (int q = 0; q < (int)r.reactnu[j]; q++) fwd *= s.cG[r.reactsp[j]];
-    double rev = 0.0;
+    rev = 0.0;
     if (r.reversible) {
       rev = K;
       const int nu = (int)std::fabs(r.nusum);
@@ -521,31 +532,43 @@ double rate_of_progress(const OMech &m, const ORxn &r, const RateState &s) {
       for (int j = 0; j < r.nprod; j++)
         for (int q = 0; q < (int)r.prodnu[j]; q++) rev *= s.cG[r.prodsp[j]];
     }
-    return fwd - rev;
+    return;
   }
   if (thirdbody && !falloff) lk += s.logtb[r.tb];
   if (falloff) lk += std::fmin(logpr, 0.0) - std::log1p(texp(-std::fabs(logpr)));
   if (r.kind == O_TROE) lk += troeblend(m, r, s, logpr);
   double lrp = lk;
   for (int j = 0; j < r.nfwd; j++) lrp += r.fwdorder[j] * s.logc[r.fwdsp[j]];
-  const double fwd = texp(std::fmin(lrp, m.expclamp));
-  if (!r.reversible) return fwd;
+  fwd = texp(std::fmin(lrp, m.expclamp));
+  rev = 0.0;
+  if (!r.reversible) return;
   double diff = r.nusum != 0.0 ? r.nusum * s.logprefRuT : 0.0;
   for (int j = 0; j < r.nnet; j++) diff -= r.netnu[j] * (s.gRT[r.netsp[j]] + s.logc[r.netsp[j]]);
-  const double rev = texp(std::fmin(lrp - diff, m.expclamp));
-  return fwd - rev;
+  rev = texp(std::fmin(lrp - diff, m.expclamp));
+}
+
+// the fold (finiterate.mako:186-236): the net production rates omega and,
+// given D, the destruction rates, kg / m^3 / s; one pass over the reactions
+void fold(const OCase &c, const RateState &s, double *omega, double *D) {
+  const OMech &m = *c.mech;
+  for (int n = 0; n < c.ns; n++) omega[n] = 0.0;
+  if (D)
+    for (int n = 0; n < c.ns; n++) D[n] = 0.0;
+  for (int k = 0; k < m.nr; k++) {
+    const ORxn &r = m.rxn[k];
+    double fwd, rev;
+    oneway(m, r, s, fwd, rev);
+    const double rp = r.reversible ? fwd - rev : fwd;
+    for (int j = 0; j < r.nnet; j++) {
+      const double nuMW = r.netnuMW[j];
+      omega[r.netsp[j]] += nuMW * rp;
+      if (D) D[r.netsp[j]] += (nuMW < 0.0 ? -nuMW : 0.0) * fwd + (nuMW > 0.0 ? nuMW : 0.0) * rev;
+    }
+  }
 }
 
 // production: the net mass production rates, kg / m^3 / s (finiterate.mako:186-231)
-void production(const OCase &c, const RateState &s, double *omega) {
-  const OMech &m = *c.mech;
-  for (int n = 0; n < c.ns; n++) omega[n] = 0.0;
-  for (int k = 0; k < m.nr; k++) {
-    const ORxn &r = m.rxn[k];
-    const double rp = rate_of_progress(m, r, s);
-    for (int j = 0; j < r.nnet; j++) omega[r.netsp[j]] += r.netnuMW[j] * rp;
-  }
-}
+void production(const OCase &c, const RateState &s, double *omega) { fold(c, s, omega, nullptr); }
 
 // cellrates: the clipped mass fractions (simulator/euler/kernels/solution.mako:25-38),
 // the rate state at the cell's T and the production rates
@@ -565,6 +588,118 @@ void cellrates(const OCase &c, const double *Q, double T, double *omega) {
   RateState s;
   ratestate(c, s, Q[0], Y, T);
   production(c, s, omega);
+}
+
+// ---- the sub-stepped chemistry (simulator/chemint/kernels/substep.mako,
+// bulk.mako, stiff.mako): the one-pass form, every cell with the cap, which
+// the compacted passes give to the bit ----
+
+// cp / R and the internal energy per mass of species n (simulator/mixture/eos/kernels/species.mako:3-27)
+double cpRof(const OCase &c, int n, double u) {
+  double cpR = 0.0;
+  for (int m = c.ncppoly - 1; m >= 0; m--) cpR = cpR * u + c.cppoly[n * c.ncppoly + m];
+  return cpR;
+}
+double eof(const OCase &c, int n, double T, double u, double Tinv) {
+  double hRT = 0.0;
+  for (int m = c.nh - 1; m >= 0; m--) hRT = hRT * u + c.hpoly[n * c.nh + m];
+  hRT += c.h298[n] * Tinv;
+  return (hRT - 1.0) * T * c.Rsp[n];
+}
+
+// integrate (substep.mako:4-87) from Y, T over the step; src the mean rate,
+// the substeps taken returned
+int integrate(const OCase &c, double rho, double rhoinv, double step, double *Y, double &T, double *src,
+              double &remaining, int limit, bool exit) {
+  const int ns = c.ns;
+  const double eps = 2.220446049250313e-16, tiny = 2.2250738585072014e-308, stepinv = 1.0 / step;
+  const double stepfrac = 1e-12;
+  auto Yof = [&](int n) { return Y[n]; };
+  double rate[16], D[16];
+  int sub = 0;
+  bool early = false;
+  for (; sub < limit && remaining > stepfrac; sub++) {
+    RateState s;
+    ratestate(c, s, rho, Yof, T);
+    fold(c, s, rate, exit && c.eqtol > 0.0 && sub == 0 ? D : nullptr);
+    double abest = 0.0, bbest = 0.0;
+    for (int n = 0; n < ns; n++) {
+      const double sign = std::copysign(1.0, rate[n]);
+      const double headroom = 0.5 * ((1.0 - sign) * Y[n] + (1.0 + sign) * (1.0 - Y[n]));
+      const double a = rho * std::fmax(headroom, eps), b = std::fmax(std::fabs(rate[n]), tiny);
+      if (n == 0 || a * bbest < abest * b) {
+        abest = a;
+        bbest = b;
+      }
+    }
+    const double share = std::fmin(remaining, abest / bbest * stepinv);
+    double cv = 0.0, dTdt = 0.0;
+    for (int n = 0; n < ns; n++) {
+      const double cpR = cpRof(c, n, s.logT);
+      const double e = eof(c, n, T, s.logT, s.Tinv);
+      cv += (cpR - 1.0) * c.Rsp[n] * Y[n];
+      dTdt -= e * rate[n];
+    }
+    const double cvrhoinv = 1.0 / (cv * rho);
+    dTdt *= cvrhoinv;
+    if (exit && c.eqtol > 0.0) {
+      const double tleft = remaining * step, tleftinv = 1.0 / tleft;
+      bool settled = sub == 0 && tleft > 0.0 && std::fabs(dTdt) * tleft < 0.1;
+      for (int n = 0; n < ns && settled; n++) settled = std::fabs(rate[n] * rhoinv) * tleft < c.eqtol;
+      if (settled) {
+        double dT = 0.0;
+        for (int n = 0; n < ns; n++) {
+          const double rhoden = rho * std::fmax(Y[n], c.cfloor * c.MW[n] * rhoinv);
+          const double move = std::fmax((rate[n] * rhoinv) * tleft * rhoden / (rhoden + D[n] * tleft), -Y[n]);
+          const double r = move * rho * tleftinv;
+          const double e = eof(c, n, T, s.logT, s.Tinv);
+          dT -= e * r;
+          Y[n] += move;
+          src[n] += r * remaining;
+        }
+        T += dT * cvrhoinv * tleft;
+        remaining = 0.0;
+        early = true;
+        break;
+      }
+    }
+    const double tsub = share * step;
+    for (int n = 0; n < ns; n++) {
+      Y[n] += (rate[n] * rhoinv) * tsub;
+      src[n] += rate[n] * share;
+    }
+    T += dTdt * tsub;
+    remaining -= share;
+    if (share <= stepfrac) {
+      remaining = 0.0;
+      early = true;
+      break;
+    }
+  }
+  return early ? sub + 1 : sub;
+}
+
+// a cell's sub-stepped source over the step: the clipped mass fractions
+// and the cell's T (substep.mako:89-95), the cap, the exit where the
+// tolerance is set; the mean rates into omega, the count returned
+int substepped(const OCase &c, const double *Q, double T, double *omega) {
+  const int ns = c.ns;
+  const double rho = Q[0], rhoinv = 1.0 / Q[0];
+  double Ylast = 1.0, Ysum = 0.0;
+  for (int n = 0; n < ns - 1; n++) {
+    const double Yn = std::fmax(std::fmin(Q[5 + n] * rhoinv, 1.0), 0.0);
+    Ylast -= Yn;
+    Ysum += Yn;
+  }
+  const double Yscale = 1.0 / std::fmax(Ysum, 1.0);
+  Ylast = std::fmax(Ylast, 0.0);
+  double Y[16];
+  for (int n = 0; n < ns; n++) {
+    Y[n] = n < ns - 1 ? std::fmax(std::fmin(Q[5 + n] * rhoinv, 1.0), 0.0) * Yscale : Ylast;
+    omega[n] = 0.0;
+  }
+  double remaining = 1.0;
+  return integrate(c, rho, rhoinv, c.dt, Y, T, omega, remaining, c.cap, true);
 }
 
 // ---- the cubic real gas (simulator/mixture/eos/realgas/kernels/eos.mako,
@@ -1796,7 +1931,12 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
             // rates, the fluxes add to it (simulator/chemint/kernels/source.mako:3-10,
             // cell.mako:14-19, applyflux.mako with append)
             double omega[16], src[32];
-            cellrates(c, B.Q + at * ne, s.state[at * NSTATE + 1], omega);
+            if (c.substepped) {
+              const int taken = substepped(c, B.Q + at * ne, s.state[at * NSTATE + 1], omega);
+              if (B.subs) B.subs[at] = taken;
+            } else {
+              cellrates(c, B.Q + at * ne, s.state[at * NSTATE + 1], omega);
+            }
             for (int l = 0; l < 5; l++) src[l] = 0.0;
             for (int n = 0; n < ns - 1; n++) src[5 + n] = omega[n];
             for (int l = 0; l < ne; l++)

@@ -151,11 +151,25 @@ class Config(dict):
             raise ConfigError("diff-flux.formula", "only 'alpha-damping' is built")
         if self["mixture"]["chemistry"] not in (None, "finite-rate"):
             raise ConfigError("mixture.chemistry", "null or finite-rate")
-        kind = self["chem-integration"]["kind"]
-        if kind not in (None, "coupled"):
-            raise ConfigError("chem-integration.kind", "null or coupled")
+        chem = self["chem-integration"]
+        kind = chem["kind"]
+        if kind not in (None, "coupled", "sub-stepped"):
+            raise ConfigError("chem-integration.kind", "null, coupled or sub-stepped")
         if kind is not None and self["mixture"]["chemistry"] is None:
-            raise ConfigError("chem-integration.kind", "set without mixture.chemistry")
+            raise ConfigError("chem-integration.kind", f"{kind} needs mixture.chemistry")
+        if kind == "sub-stepped":
+            # peregrine/simulator/chemint/substepped.py:21-33
+            cap, bulk, bins, tol = (chem[k] for k in ("max-substeps", "bulk-substeps", "stiff-bins",
+                                                       "equilibrium-tolerance"))
+            if not isinstance(cap, int) or isinstance(cap, bool) or cap < 1:
+                raise ConfigError("chem-integration.max-substeps", f"{cap!r} is not a count of one or more")
+            if not isinstance(bulk, int) or isinstance(bulk, bool) or not 1 <= bulk <= cap:
+                raise ConfigError("chem-integration.bulk-substeps", f"{bulk!r} is not a count from one to max-substeps")
+            if not isinstance(bins, int) or isinstance(bins, bool) or not 1 <= bins <= 16:
+                raise ConfigError("chem-integration.stiff-bins", f"{bins!r} is not a count from one to sixteen")
+            if not isinstance(tol, (int, float)) or isinstance(tol, bool) or not 0.0 <= tol < 1.0:
+                raise ConfigError("chem-integration.equilibrium-tolerance",
+                                  f"{tol!r} is not a mass fraction below one, zero for no exit")
         if sim["controller"] not in ("fixed", "cfl"):
             raise ConfigError("simulation.controller", f"{sim['controller']!r} is not one of ('fixed', 'cfl')")
         for key in ("cfl", "dt-max"):

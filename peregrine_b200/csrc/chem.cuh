@@ -119,11 +119,11 @@ __device__ __forceinline__ double troeblend(const Rxn &r, const double logT, con
   return lfc * B2 / (B2 + A * A) * 2.302585092994046;
 }
 
-// one reaction's net rate of progress: the product form (finiterate.mako:66-125)
-// or the log form with the double fold's difference of one-way rates
-// (finiterate.mako:7-46, 201-214)
+// one reaction's one-way rates of progress, fwd and rev (0 for an
+// irreversible one): the product form (finiterate.mako:66-125) or the log form
+// with the double fold's one-way rates (finiterate.mako:7-46, 201-214)
 template <int NS>
-__device__ __forceinline__ double progress(const Rxn &r, const RateState<NS> &s) {
+__device__ __forceinline__ void oneway(const Rxn &r, const RateState<NS> &s, double &fwd, double &rev) {
   const Mech &m = kMech;
   double lk = r.logA;
   if (r.b != 0.0) lk += r.b * s.logT;
@@ -147,12 +147,12 @@ __device__ __forceinline__ double progress(const Rxn &r, const RateState<NS> &s)
     double K = texp(fmin(xk, m.expclamp));
     if (thirdbody && !falloff) K *= s.ctb[r.tb];
     if (falloff) K *= pfac;
-    double fwd = K;
+    fwd = K;
     for (int j = 0; j < r.nreact; j++) {
       const double cg = s.cG[r.reactsp[j]];
       for (int q = 0; q < (int)r.reactnu[j]; q++) fwd *= cg;
     }
-    double rev = 0.0;
+    rev = 0.0;
     if (r.reversible) {
       rev = K;
       const double f = r.nusum > 0.0 ? s.prefRuTinv : s.prefRuT;
@@ -162,19 +162,50 @@ __device__ __forceinline__ double progress(const Rxn &r, const RateState<NS> &s)
         for (int q = 0; q < (int)r.prodnu[j]; q++) rev *= cg;
       }
     }
-    return fwd - rev;
+    return;
   }
   if (thirdbody && !falloff) lk += s.logtb[r.tb];
   if (falloff) lk += fmin(logpr, 0.0) - log1p(texp(-fabs(logpr)));
   if (r.kind == 3) lk += troeblend(r, s.logT, logpr);
   double lrp = lk;
   for (int j = 0; j < r.nfwd; j++) lrp += r.fwdorder[j] * s.logc[r.fwdsp[j]];
-  const double fwd = texp(fmin(lrp, m.expclamp));
-  if (!r.reversible) return fwd;
+  fwd = texp(fmin(lrp, m.expclamp));
+  rev = 0.0;
+  if (!r.reversible) return;
   double diff = r.nusum != 0.0 ? r.nusum * s.logprefRuT : 0.0;
   for (int j = 0; j < r.nnet; j++) diff -= r.netnu[j] * (s.gRT[r.netsp[j]] + s.logc[r.netsp[j]]);
-  const double rev = texp(fmin(lrp - diff, m.expclamp));
-  return fwd - rev;
+  rev = texp(fmin(lrp - diff, m.expclamp));
+}
+
+// one reaction's net rate of progress; an irreversible one's is its forward rate
+template <int NS>
+__device__ __forceinline__ double progress(const Rxn &r, const RateState<NS> &s) {
+  double fwd, rev;
+  oneway<NS>(r, s, fwd, rev);
+  return r.reversible ? fwd - rev : fwd;
+}
+
+// the fold: the net production rates omega and, with D, the destruction
+// rates, kg / m^3 / s, in one pass over the reactions (finiterate.mako:186-236)
+template <int NS, bool WITHD>
+__device__ __forceinline__ void fold(const RateState<NS> &s, double *omega, double *D) {
+#pragma unroll
+  for (int n = 0; n < NS; n++) omega[n] = 0.0;
+  if (WITHD)
+#pragma unroll
+    for (int n = 0; n < NS; n++) D[n] = 0.0;
+  for (int k = 0; k < kMech.nr; k++) {
+    const Rxn &r = kMech.rxn[k];
+    double fwd, rev;
+    oneway<NS>(r, s, fwd, rev);
+    const double rp = r.reversible ? fwd - rev : fwd;
+    for (int j = 0; j < r.nnet; j++) {
+      const double nuMW = r.netnuMW[j];
+      omega[r.netsp[j]] += nuMW * rp;
+      // a species a side destroys: the forward rate where it is a reactant, the reverse where a product
+      if (WITHD) D[r.netsp[j]] += (nuMW < 0.0 ? -nuMW : 0.0) * fwd + (nuMW > 0.0 ? nuMW : 0.0) * rev;
+    }
+  }
 }
 
 // cellrates: the clipped mass fractions (peregrine/simulator/euler/kernels/solution.mako:25-38),
@@ -195,13 +226,7 @@ __device__ __forceinline__ void cellrates(QF Q, const double T, double *omega) {
   auto Y = [&](int n) { return n < NS - 1 ? fmax(fmin(Q(5 + n) * rhoinv, 1.0), 0.0) * Yscale : Ylast; };
   RateState<NS> s;
   ratestate<NS>(s, rho, Y, T);
-#pragma unroll
-  for (int n = 0; n < NS; n++) omega[n] = 0.0;
-  for (int k = 0; k < kMech.nr; k++) {
-    const Rxn &r = kMech.rxn[k];
-    const double rp = progress<NS>(r, s);
-    for (int j = 0; j < r.nnet; j++) omega[r.netsp[j]] += r.netnuMW[j] * rp;
-  }
+  fold<NS, false>(s, omega, nullptr);
 }
 
 // the coupled source: dQ begins with zeros in the mass, momentum and energy
@@ -237,13 +262,7 @@ __global__ void k_production(long long n, const double *__restrict__ rho, const 
   RateState<NS> s;
   ratestate<NS>(s, rho[q], [&](int k) { return Y[q * NS + k]; }, T[q]);
   double w[NS];
-#pragma unroll
-  for (int k = 0; k < NS; k++) w[k] = 0.0;
-  for (int k = 0; k < kMech.nr; k++) {
-    const Rxn &r = kMech.rxn[k];
-    const double rp = progress<NS>(r, s);
-    for (int j = 0; j < r.nnet; j++) w[r.netsp[j]] += r.netnuMW[j] * rp;
-  }
+  fold<NS, false>(s, w, nullptr);
 #pragma unroll
   for (int k = 0; k < NS; k++) omega[q * NS + k] = w[k];
 }

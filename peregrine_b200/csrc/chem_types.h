@@ -25,6 +25,7 @@ struct Mech {
   int nr, ntb, nlfc, ngp;  // reactions, third-body sets, Troe fit terms, Gibbs fit terms
   int logform, product;  // whether any reaction takes the log form / the product form
   double logprefRu, prefRu, Rupref, logcfloor, troeuc, troeuhinv;
+  double cfloor;    // exp(logcfloor): the concentration floor of the equilibrium exit's relaxation
   double expclamp;  // ln(DBL_MAX) - ln(2 maxgain): the largest ln rate whose production rates stay finite
   double lfcfloor;  // log10 of the smallest normal double, a Troe centre without terms
   double tbdefeff[MAXTB];
@@ -34,6 +35,22 @@ struct Mech {
   double lfcpoly[MAXTROE][MAXLFC];
   double gpoly[MAXNS][MAXT + 1];  // g / Ru T in ln T less h298 / T, one more term than cp
   Rxn rxn[MAXRXN];
+};
+
+// the sub-stepped chemistry's options (peregrine/simulator/chemint/substepped.py:14-19, 47-52)
+struct SubstepOpts {
+  int cap, bulk, bins;
+  double eqtol, stepfrac;
+  double limitinv, binscale;  // the bulk pass's 1 / limit and bins / ln(cap / limit)
+};
+
+// the stiff list: head[0] every listed cell, head[1 + b] bin b's count,
+// head[bins + 1] the stiff pass's work counter; bin b's codes from cell
+// b * capacity
+struct StiffList {
+  unsigned int *head;
+  int2 *cells;  // (block, cell index in the block's full layout)
+  long long capacity;
 };
 
 // the table log's and exp's tables

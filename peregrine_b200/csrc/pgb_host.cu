@@ -165,6 +165,12 @@ struct pgb_case {
   double *d_cfl = nullptr, *d_ctrl = nullptr;
   bool ctrl_cfl = false;
   bool graph_cfl[2] = {false, false};
+  // the sub-stepped chemistry: its options, each cell's last count, the stiff list
+  SubstepOpts subopt{200, 1, 8, 1e-7, 1e-12, 1.0, 0.0};
+  int *d_subs = nullptr;
+  unsigned int *d_stiffhead = nullptr;
+  int2 *d_stiffcells = nullptr;
+  long long interior_cells = 0;
 };
 
 namespace {
@@ -250,8 +256,15 @@ int build_species(pgb_case *c) {
     RET(fit("mupoly", c->sp.mupoly, c->sp.nmu));
     RET(fit("kappapoly", c->sp.kappapoly, c->sp.nkappa));
   }
-  if (c->phys.chemistry == PGB_CHEM_COUPLED && !c->mech)
+  if (c->phys.chemistry != PGB_CHEM_NONE && !c->mech)
     return fail(PGB_ERR_STATE, "finite-rate chemistry needs pgb_case_set_mechanism before finalize");
+  if (c->phys.chemistry == PGB_CHEM_SUBSTEPPED) {
+    // the integrator's cv and the exit's concentration floor read cp / R and the molar masses
+    RET(fit("cppoly", c->sp.cppoly, c->sp.ncppoly));
+    const double *mw = table(c, "MW");
+    if (!mw || (long)c->tables["MW"].size() < ns) return fail(PGB_ERR_ARG, "the sub-stepped chemistry reads MW");
+    for (int n = 0; n < ns; n++) c->sp.MW[n] = mw[n];
+  }
   c->version++;
   return PGB_OK;
 }
@@ -826,6 +839,14 @@ int ensure_scratch(pgb_case *c) {
   CK(cudaMemsetAsync(c->d_hsp, 0, sizeof(double) * ns * n, c->stream));
   CK(cudaMemsetAsync(c->d_grads, 0, sizeof(double) * 3 * ngrad * n, c->stream));
   for (int a = 0; a < 3; a++) CK(cudaMemsetAsync(c->d_F[a], 0, sizeof(double) * nf * n, c->stream));
+  if (c->phys.chemistry == PGB_CHEM_SUBSTEPPED) {
+    // a bin's segment holds every interior cell, so it never fills
+    CK(cudaMalloc(&c->d_subs, sizeof(int) * n));
+    CK(cudaMemsetAsync(c->d_subs, 0, sizeof(int) * n, c->stream));
+    CK(cudaMalloc(&c->d_stiffhead, sizeof(unsigned int) * (16 + 2)));
+    CK(cudaMemsetAsync(c->d_stiffhead, 0, sizeof(unsigned int) * (16 + 2), c->stream));
+    CK(cudaMalloc(&c->d_stiffcells, sizeof(int2) * (size_t)c->subopt.bins * (size_t)c->interior_cells));
+  }
   return PGB_OK;
 }
 
@@ -853,7 +874,10 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.nhalo = c->nhalo, pc.nhalo_l0 = c->nhalo_l0;
   pc.visc = c->phys.simulator == PGB_NAVIER_STOKES;
   pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
-  pc.chem = c->phys.chemistry == PGB_CHEM_COUPLED;
+  pc.chem = c->phys.chemistry;
+  pc.subopt = c->subopt;
+  pc.subs = c->d_subs;
+  pc.stiff = StiffList{c->d_stiffhead, c->d_stiffcells, c->interior_cells};
   pc.df = c->phys.simulator == PGB_EULER_DF;
   pc.realgas = c->phys.eos == PGB_EOS_REALGAS || c->phys.eos == PGB_EOS_REALGAS_DF;
   pc.bchalo = c->d_bcface[0], pc.bcgrad = c->d_bcface[1], pc.bcwall = c->d_bcface[2];
@@ -1080,9 +1104,9 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
     return fail(PGB_ERR_UNSUPPORTED, "the real gas runs inviscid in this build (euler, euler-df)");
   if (phys->trans == PGB_TRANS_KINETIC && phys->eos == PGB_EOS_CPG)
     return fail(PGB_ERR_ARG, "kinetic-theory transport needs the thermally perfect caloric");
-  if (phys->chemistry != PGB_CHEM_NONE && phys->chemistry != PGB_CHEM_COUPLED)
-    return fail(PGB_ERR_UNSUPPORTED, "the chemistry takes none or coupled");
-  if (phys->chemistry == PGB_CHEM_COUPLED && phys->eos != PGB_EOS_TPG)
+  if (phys->chemistry < PGB_CHEM_NONE || phys->chemistry > PGB_CHEM_SUBSTEPPED)
+    return fail(PGB_ERR_UNSUPPORTED, "the chemistry takes none, coupled or sub-stepped");
+  if (phys->chemistry != PGB_CHEM_NONE && phys->eos != PGB_EOS_TPG)
     return fail(PGB_ERR_UNSUPPORTED, "finite-rate chemistry takes the thermally perfect gas in this build");
   auto c = std::make_unique<pgb_case>();
   c->uid = ++g_next_uid;
@@ -1105,7 +1129,7 @@ int pgb_case_destroy(pgb_case *c) {
   void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
-                  c->d_cfl, c->d_ctrl};
+                  c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells};
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1127,7 +1151,7 @@ int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long
 int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m) {
   if (!c || !m) return fail(PGB_ERR_ARG, "null argument");
   if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
-  if (c->phys.chemistry != PGB_CHEM_COUPLED) return fail(PGB_ERR_STATE, "the case has no chemistry");
+  if (c->phys.chemistry == PGB_CHEM_NONE) return fail(PGB_ERR_STATE, "the case has no chemistry");
   const int ns = c->phys.ns;
   if (m->nr < 0 || m->nr > MAXRXN) return fail(PGB_ERR_UNSUPPORTED, "at most 64 reactions in this build");
   if (m->nr && !m->rxn) return fail(PGB_ERR_ARG, "null reactions");
@@ -1140,6 +1164,7 @@ int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m) {
   std::memset(M.get(), 0, sizeof(Mech));
   M->nr = m->nr, M->ntb = m->ntb, M->nlfc = m->nlfc, M->ngp = m->ng;
   M->logprefRu = m->logprefRu, M->prefRu = m->prefRu, M->Rupref = m->Rupref, M->logcfloor = m->logcfloor;
+  M->cfloor = std::exp(m->logcfloor);
   M->troeuc = m->troeuc, M->troeuhinv = m->troeuhinv;
   // the fold's clamp and the floor of a Troe centre with no terms, as the
   // reference works them out on the host (finiterate.mako:128-133, 50-52)
@@ -1261,6 +1286,48 @@ int pgb_case_connect(pgb_case *c, int blk, int nface, int nbr, int nbrface) {
   return PGB_OK;
 }
 
+int pgb_case_set_substeps(pgb_case *c, int cap, int bulk, int bins, double eqtol) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (c->phys.chemistry != PGB_CHEM_SUBSTEPPED) return fail(PGB_ERR_STATE, "the case's chemistry is not sub-stepped");
+  if (cap < 1) return fail(PGB_ERR_ARG, "max-substeps is a count of one or more");
+  if (bulk < 1 || bulk > cap) return fail(PGB_ERR_ARG, "bulk-substeps is a count from one to max-substeps");
+  if (bins < 1 || bins > 16) return fail(PGB_ERR_ARG, "stiff-bins is a count from one to sixteen");
+  if (!(eqtol >= 0.0 && eqtol < 1.0)) return fail(PGB_ERR_ARG, "equilibrium-tolerance is a mass fraction below one");
+  SubstepOpts &o = c->subopt;
+  o.cap = cap, o.bulk = bulk, o.bins = bins, o.eqtol = eqtol, o.stepfrac = 1e-12;
+  // the bulk pass's limit and the bins' spacing in ln(count / limit) (substepped.py:47-52)
+  o.limitinv = 1.0 / bulk;
+  o.binscale = bulk < cap ? bins / std::log((double)cap / bulk) : 0.0;
+  return PGB_OK;
+}
+
+int pgb_substeps_get(pgb_case *c, int blk, int *host, long count) {
+  if (!c || !host) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
+  if (!c->d_subs) return fail(PGB_ERR_STATE, "no sub-stepped right-hand side has run");
+  const BlockDev &D = c->blocks[blk].dev;
+  if (count != (long)D.nx * D.ny * D.nz) return fail(PGB_ERR_ARG, "host array of the wrong size");
+  std::vector<int> full((size_t)D.vol);
+  CK(cudaMemcpyAsync(full.data(), c->d_subs + D.cv, sizeof(int) * D.vol, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  long q = 0;
+  for (int k = 0; k < D.nz; k++)
+    for (int j = 0; j < D.ny; j++)
+      for (int i = 0; i < D.nx; i++) host[q++] = full[cell_index(D, i + NG, j + NG, k + NG)];
+  return PGB_OK;
+}
+
+int pgb_stiff_head(pgb_case *c, unsigned int *head, int n) {
+  if (!c || !head) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->d_stiffhead) return fail(PGB_ERR_STATE, "no sub-stepped right-hand side has run");
+  if (n < 1 || n > c->subopt.bins + 1) return fail(PGB_ERR_ARG, "the header holds bins + 1 counts");
+  CK(cudaMemcpyAsync(head, c->d_stiffhead, sizeof(unsigned int) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
 int pgb_case_add_bc(pgb_case *c, int kind, const int *ops, const double *args, const int *starts, int nvalues,
                     int *id) {
   if (!c || !id || !starts || (nvalues && (!ops || !args))) return fail(PGB_ERR_ARG, "null argument");
@@ -1369,6 +1436,8 @@ int pgb_case_finalize(pgb_case *c) {
     cv += D.vol;
   }
   c->cells = cv;
+  c->interior_cells = 0;
+  for (auto &B : c->blocks) c->interior_cells += (long long)B.nx * B.ny * B.nz;
   const size_t n = (size_t)cv;
   for (int r = 0; r < c->phys.nregs; r++) {
     CK(cudaMalloc(&c->d_reg[r], sizeof(double) * c->ne * n));
@@ -1377,6 +1446,9 @@ int pgb_case_finalize(pgb_case *c) {
   CK(cudaMalloc(&c->d_met, sizeof(double) * M_NCOMP * n));
   CK(cudaMemsetAsync(c->d_met, 0, sizeof(double) * M_NCOMP * n, c->stream));
   CK(cudaMalloc(&c->d_dt, sizeof(double)));
+  // the step scalar is nothing until a step sets it (a right-hand side
+  // before any step integrates the chemistry over no time)
+  CK(cudaMemsetAsync(c->d_dt, 0, sizeof(double), c->stream));
   CK(cudaMalloc(&c->d_clock, sizeof(double)));
   CK(cudaMemsetAsync(c->d_clock, 0, sizeof(double), c->stream));
   CK(cudaMalloc(&c->d_cfl, sizeof(double) * 3));
@@ -1625,6 +1697,14 @@ int pgb_cflmax(pgb_case *c, int reg, double *out) {
   RET(cfl_pass(c, c->phys_of[reg], count));
   CK(cudaMemcpyAsync(out, c->d_cfl, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_set_dt(pgb_case *c, double dt) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
+  CK(cudaGetLastError());
   return PGB_OK;
 }
 
@@ -2049,6 +2129,8 @@ int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, 
   if (!proto || !out) return fail(PGB_ERR_ARG, "null argument");
   if (!proto->finalized) return fail(PGB_ERR_STATE, "finalize the prototype case first");
   if (proto->phys.simulator == PGB_EULER_DF) return fail(PGB_ERR_UNSUPPORTED, "the pool does not take the double flux");
+  if (proto->phys.chemistry == PGB_CHEM_SUBSTEPPED)
+    return fail(PGB_ERR_UNSUPPORTED, "the pool takes the coupled chemistry, not the sub-stepped");
   if (max_cells < 64 || max_blocks < 1 || max_blocks > 65535)
     return fail(PGB_ERR_ARG, "a pool holds at least 64 cells and 1 to 65535 blocks");
   auto p = std::make_unique<pgb_pool>();

@@ -36,6 +36,10 @@ struct Species {
   int tpg, kinetic;
   int ncp, nh, nmu, nkappa;
   double cppolyR[MAXNS * MAXT], hpoly[MAXNS * MAXT], mupoly[MAXNS * MAXT], kappapoly[MAXNS * MAXT];
+  // the sub-stepped chemistry's species heat capacities, cp / R_sp in ln T
+  // (peregrine/simulator/mixture/eos/base.py:33-47), and molar masses
+  int ncppoly;
+  double cppoly[MAXNS * MAXT], MW[MAXNS];
   // the cubic real gas (a thermally perfect gas underneath, tpg set too) and
   // its double flux: the form's u, w and roots sigma, eps; per species
   // sqrt(a_c), b, -(da/dT) sqrt(T / a), m / sqrt(Tc), 1 + m, each of the first

@@ -33,7 +33,13 @@ struct PlainCase {
   const double *met;
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
-  int visc, primary, recon, limiter, chem;
+  int visc, primary, recon, limiter;
+  int chem;  // 0 none, 1 coupled source, 2 sub-stepped (PGB_CHEM_*)
+  // the sub-stepped chemistry: its options, each cell's last substep count
+  // (every block's full layout, end to end) and the stiff list
+  SubstepOpts subopt;
+  int *subs;
+  StiffList stiff;
   int realgas;  // the cubic real gas: the kernels built for it
   int df;      // the double flux: fromplane in the stages, two energy rows per face (F holds NE + 1 rows)
   int packed;  // 1: each pass is one launch over every block

@@ -12,6 +12,7 @@
 #include "cfl.cuh"
 #include "chem.cuh"
 #include "pgb200.h"
+#include "substep.cuh"
 #include "plain.cuh"
 #include "plain_api.h"
 
@@ -29,6 +30,11 @@ constexpr int NE = 4 + NS;
 constexpr int TH = 256;
 
 unsigned grid_of(long long n) { return (unsigned)std::max<long long>(1, (n + TH - 1) / TH); }
+
+// the sub-stepped chemistry's stiff pass: its persistent grid, every SM
+// filled with its CTAs (set when the unit's tables are uploaded, outside any
+// stream capture)
+int g_stiff_ctas = 148;
 
 int cuda_fail(cudaError_t e, const char *what) {
   return pgb_internal_fail(e == cudaErrorMemoryAllocation ? PGB_ERR_NOMEM : PGB_ERR_CUDA,
@@ -123,6 +129,11 @@ void source_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const voi
   const RhsArgs &a = *(const RhsArgs *)ctx;
   k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, a.dQ, ct);
 }
+void bulk_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_substep_bulk<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, a.dQ, pc->subs, pc->dt, pc->subopt,
+                                               pc->stiff, ct);
+}
 void apply_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
   if (pc->df)
@@ -155,6 +166,10 @@ extern "C" int PGB_ENTRY(pgb_plain_upload_)(const Species *sp, const Mech *mech,
   if (mt) {
     e = cudaMemcpyToSymbolAsync(gMath, mt, sizeof(MathTables), 0, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "math tables");
+    int per_sm = 0, sms = 148, dev = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_substep_stiff<NS>, 128, 0) != cudaSuccess) per_sm = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g_stiff_ctas = sms * std::max(1, per_sm);
   }
   return PGB_OK;
 }
@@ -187,6 +202,20 @@ static void bc_wall_launch(const PlainCase *pc, const double *Q) {
       pc->d_blks, pc->bcwall, pc->nbcwall, pc->bcent, pc->bcops, Q, pc->state, pc->tr, pc->met, pc->F[0], pc->F[1],
       pc->F[2], NE + (pc->df ? 1 : 0), pc->visc, pc->clock, pc->dt, pc->tfrac);
   mark(pc, 4);
+}
+
+// the sub-stepped chemistry's passes: the list's header cleared, the bulk
+// pass over every block (it lists the cells short of the step's end), and,
+// compacted, the stiff pass over the list, one persistent launch
+static void substep_passes(const PlainCase *pc, const RhsArgs &a) {
+  const SubstepOpts &o = pc->subopt;
+  cudaMemsetAsync(pc->stiff.head, 0, sizeof(unsigned int) * (o.bins + 2), pc->stream);
+  for_blocks(pc, R_INNER, bulk_launch, &a, 2);
+  if (o.bulk < o.cap) {
+    k_substep_stiff<NS><<<g_stiff_ctas, 128, 0, pc->stream>>>(pc->d_blks, a.Q, pc->state, a.dQ, pc->subs, pc->dt,
+                                                               o, pc->stiff);
+    mark(pc, 2);
+  }
 }
 
 // one right-hand side of every block: Q's halo, the state everywhere, the
@@ -230,8 +259,9 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
     mark(pc, 0);
     bc_grads_launch(pc);
   }
+  if (pc->chem == PGB_CHEM_SUBSTEPPED) substep_passes(pc, a);
   if (pc->packed) {
-    if (pc->chem) for_blocks(pc, R_INNER, source_launch, &a, 2);
+    if (pc->chem == PGB_CHEM_COUPLED) for_blocks(pc, R_INNER, source_launch, &a, 2);
     for_blocks(pc, R_FX, adv_launch<0>, &a, 2);
     for_blocks(pc, R_FY, adv_launch<1>, &a, 2);
     for_blocks(pc, R_FZ, adv_launch<2>, &a, 2);
@@ -246,7 +276,7 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
     for (int b = 0; b < pc->nblocks; b++) {
       const BlockDev &D = pc->h_blks[b];
       auto g = [&](int r) { return dim3(grid_of(range_size(D, r))); };
-      if (pc->chem) {
+      if (pc->chem == PGB_CHEM_COUPLED) {
         source_launch(pc, b, g(R_INNER), nullptr, &a);
         mark(pc, 2);
       }

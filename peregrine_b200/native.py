@@ -20,7 +20,7 @@ EOS_CPG, EOS_TPG, EOS_REALGAS, EOS_REALGAS_DF = 0, 1, 2, 3
 FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV, FLUX_AUSMUP = 0, 1, 2, 3
 RECON_CONSTANT, RECON_MUSCL = 0, 1
 LIMITERS = {"koren": 1, "minmod": 2, "mc": 3, "superbee": 4, "vanleer": 5}
-CHEM_NONE, CHEM_COUPLED = 0, 1
+CHEM_NONE, CHEM_COUPLED, CHEM_SUBSTEPPED = 0, 1, 2
 # boundary kinds, by the reference's bcvals names
 BC_KINDS = {"slp-adia-wall": 1, "slp-isot-wall": 2, "no-slp-adia-wall": 3, "mov-adia-wall": 4,
             "no-slp-isot-wall": 5, "mov-isot-wall": 6, "sub-in-fvt": 7, "sup-in-fa": 8, "sub-in-ftptt": 9,
@@ -195,6 +195,9 @@ SIGNATURES = {
     "pgb_pool_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_pool_last": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_case_set_mechanism": ([ctypes.c_void_p, ctypes.POINTER(Mechanism)], ctypes.c_int),
+    "pgb_case_set_substeps": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double], ctypes.c_int),
+    "pgb_substeps_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_long], ctypes.c_int),
+    "pgb_stiff_head": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint), ctypes.c_int], ctypes.c_int),
     "pgb_production": ([ctypes.c_void_p, ctypes.c_long] + [ctypes.POINTER(ctypes.c_double)] * 4, ctypes.c_int),
     "pgb_case_add_block": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_case_connect": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -216,6 +219,7 @@ SIGNATURES = {
     "pgb_step": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_step_cfl": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_cflmax": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "pgb_set_dt": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
     "pgb_last_dt": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "pgb_case_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "pgb_last_step_ms": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),

@@ -130,7 +130,8 @@ class Solver:
         phys.nregs = nregs
         phys.alpha = float(cfg["diff-flux"]["values"].get("alpha", 1.0))
         kind = cfg["chem-integration"]["kind"]
-        phys.chemistry = native.CHEM_COUPLED if kind == "coupled" else native.CHEM_NONE
+        phys.chemistry = {None: native.CHEM_NONE, "coupled": native.CHEM_COUPLED,
+                          "sub-stepped": native.CHEM_SUBSTEPPED}[kind]
         handle = ctypes.c_void_p()
         native.call("pgb_case_create", ctypes.byref(phys), ctypes.byref(handle))
         self.case = handle
@@ -173,6 +174,8 @@ class Solver:
                 tables[key] = np.atleast_1d(consts[key])
         if self.mixture.trans == "kinetic-theory":
             tables.update(mupoly=consts["mupoly"], kappapoly=consts["kappapoly"])
+        if self.cfg["chem-integration"]["kind"] == "sub-stepped":
+            tables.update(cppoly=consts["cppoly"], MW=consts["MW"])
         return tables
 
     def _fill(self, records):
@@ -190,9 +193,13 @@ class Solver:
                 nbr = -1 if face.nbr is None else face.nbr
                 native.call("pgb_case_connect", self.case, blk.nblki, face.nface, nbr, face.nbrface or 0)
         self._fill_bcs()
-        if self.cfg["chem-integration"]["kind"] == "coupled":
+        chem = self.cfg["chem-integration"]
+        if chem["kind"] is not None:
             mech, keep = native.mechanism(consts)
             native.call("pgb_case_set_mechanism", self.case, ctypes.byref(mech))
+        if chem["kind"] == "sub-stepped":
+            native.call("pgb_case_set_substeps", self.case, chem["max-substeps"], chem["bulk-substeps"],
+                        chem["stiff-bins"], float(chem["equilibrium-tolerance"]))
         native.call("pgb_case_set_stages", self.case, records, len(records))
         native.call("pgb_case_finalize", self.case)
         self.metrics = []
@@ -301,6 +308,26 @@ class Solver:
         out = (ctypes.c_double * 3)()
         native.call("pgb_cflmax", self.case, 0, out)
         return dict(zip(("acoustic", "convective", "combined"), list(out)))
+
+    def substeps(self, blk=0):
+        """Each interior cell's substep count at the last right-hand side (the
+        reference's ``substeps`` array)."""
+        b = self.mesh_blocks[blk]
+        out = np.zeros(b.cells, dtype=np.int32, order="F")
+        native.call("pgb_substeps_get", self.case, blk, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), out.size)
+        return out
+
+    def stiff_head(self):
+        """The stiff list's header: the cells listed, then each bin's count."""
+        n = self.cfg["chem-integration"]["stiff-bins"] + 1
+        out = (ctypes.c_uint * n)()
+        native.call("pgb_stiff_head", self.case, out, n)
+        return list(out)
+
+    def set_dt(self, dt):
+        """The step scalar the sub-stepped chemistry integrates over (the
+        reference's ``solver.dt``), for a right-hand side outside a step."""
+        native.call("pgb_set_dt", self.case, float(dt))
 
     def last_dt(self):
         dt = ctypes.c_double()

@@ -138,7 +138,7 @@ def test_reacting_tables_and_mechanism_structs_build_on_the_host():
 
     cfg = cases.reacting_config()
     mix = Mixture(cfg["mixture"])
-    tables = Solver.species_tables(types.SimpleNamespace(mixture=mix))
+    tables = Solver.species_tables(types.SimpleNamespace(mixture=mix, cfg=cfg))
     assert "cp0" not in tables and tables["cppolyR"].shape == (9, 7) and tables["mupoly"].shape[0] == 9
     consts = mix.constants()
     mech, keep = native.mechanism(consts)
