@@ -262,6 +262,53 @@ def reacting_leg(steps, cpu=True):
     return out
 
 
+def substep_leg(steps, dt=1e-7, dT=1500.0):
+    """The reacting field with burnt-hot spots (up to 2500 K) and the
+    sub-stepped chemistry (the reference's defaults: a 200-substep cap, one
+    bulk substep, 8 bins, the 1e-7 exit) at five times the coupled leg's step:
+    cell-stage/s, the bulk and stiff passes' shares of a step and the share of
+    cells the stiff pass takes."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases
+
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True, launch="per-block")
+    cfg["chem-integration"]["kind"] = "sub-stepped"
+    cfg.validate()
+    mesh = cases.reacting_mesh(REACT_CELLS, (1, 1, 1))
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    consts = mb.mixture.constants()
+    prims = cases.reacting_prims(mb.metrics, mb.mixture.spnames, consts["MW"], REACT_CELLS, seed=SEED, dT=dT)
+    mb.set_prims(prims)
+    mb.step(dt, 3)
+    mb.backend.sync()
+    ms = time_graph(mb, dt, steps)
+    rows = fused_kernel_times(mb, dt, 1)
+    total = sum(m for m, _ in rows)
+    bulk = sum(m for m, k in rows if k == 6)
+    stiff = sum(m for m, k in rows if k == 7)
+    per_stage_stiff = [m for m, k in rows if k == 7]
+    # the listing of a step's first stage (the later stages start from states
+    # the first stage's mean rates carried near the hot cells' equilibrium)
+    mb.rhs()
+    head = mb.stiff_head()
+    subs = mb.substeps()
+    ncells = mb.ncells
+    value = ncells * REACT_STAGES * steps / (ms / 1e3)
+    out = {"value": value, "unit": "cell-stage/s", "steps": steps, "ms_per_step": ms / steps, "dt": dt,
+           "launches_per_step": mb.launches_per_step(),
+           "bulk_share_of_step": bulk / total if total else None,
+           "stiff_share_of_step": stiff / total if total else None,
+           "stiff_ms_per_stage": per_stage_stiff,
+           "first_stage_listed_fraction": head[0] / ncells, "first_stage_bin_counts": head[1:],
+           "first_stage_mean_substeps": float(subs.mean()), "first_stage_max_substeps": int(subs.max()),
+           "first_stage_listed_mean_substeps": float(subs[subs > 1].mean()) if (subs > 1).any() else None,
+           "workload": f"h2-air-96^3-9sp-28rxn hot spots of {dT:g} K over 1000 K, sub-stepped chemistry (cap 200, "
+                       "bulk 1, 8 bins, exit 1e-7), muscl-koren-hllc-ns-tvd-rk3",
+           "path": "per-block kernels; chemistry: bulk pass over every cell, one persistent stiff pass over the list"}
+    del mb
+    return out
+
+
 def realgas_leg(steps, cpu=True):
     """Cell-stage/s of the transcritical mixing layer on the per-block path."""
     import peregrine_b200 as pg
@@ -458,6 +505,8 @@ def main():
     ap.add_argument("--no-realgas", action="store_true", help="skip the real-gas leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--boundary-only", action="store_true", help="the bounded channel leg alone")
+    ap.add_argument("--substep-only", action="store_true", help="the sub-stepped chemistry leg alone")
+    ap.add_argument("--no-substep", action="store_true", help="skip the sub-stepped chemistry leg")
     ap.add_argument("--no-boundary", action="store_true", help="skip the bounded channel leg")
     args = ap.parse_args()
     set_cells(args.cells)
@@ -467,6 +516,9 @@ def main():
         return
     if args.realgas_only:
         print(json.dumps({"realgas": realgas_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
+        return
+    if args.substep_only:
+        print(json.dumps({"substepped": substep_leg(max(1, min(args.steps, 10)))}), flush=True)
         return
     if args.boundary_only:
         print(json.dumps({"boundary": boundary_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
@@ -589,6 +641,9 @@ def main():
     realgas = None
     if rank == 0 and not args.no_realgas and not args.no_extra:
         realgas = realgas_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
+    substepped = None
+    if rank == 0 and not args.no_substep and not args.no_extra:
+        substepped = substep_leg(max(2, min(args.steps // 60, 10)))
     boundary = None
     if rank == 0 and not args.no_boundary and not args.no_extra:
         boundary = boundary_leg(max(2, min(args.steps // 30, 20)), cpu=not args.no_cpu)
@@ -615,6 +670,7 @@ def main():
             "serving": served,
             "realgas": realgas,
             "boundary": boundary,
+            "substepped": substepped,
             "cfl": cfl_cost,
             "e2e": e2e,
             "gpu_launches": launches * args.steps,

@@ -310,8 +310,8 @@ int pgb_set_dt(pgb_case *c, double dt);
 /* nsteps steps without a graph, a CUDA event between every launch; waits for
  * them and returns each launch's device time (ms) and kind (0 halo fill,
  * 1 fused stage, 2 per-block kernel, 3 combine or clock, 4 boundary pass,
- * 5 CFL reduction) in launch order, up to cap launches; n is the number of
- * launches. */
+ * 5 CFL reduction, 6 sub-stepped chemistry's bulk pass, 7 its stiff pass) in
+ * launch order, up to cap launches; n is the number of launches. */
 int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int *kind, int cap, int *n);
 
 /* the stream the case queues on (a cudaStream_t) */

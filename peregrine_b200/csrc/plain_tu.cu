@@ -210,11 +210,11 @@ static void bc_wall_launch(const PlainCase *pc, const double *Q) {
 static void substep_passes(const PlainCase *pc, const RhsArgs &a) {
   const SubstepOpts &o = pc->subopt;
   cudaMemsetAsync(pc->stiff.head, 0, sizeof(unsigned int) * (o.bins + 2), pc->stream);
-  for_blocks(pc, R_INNER, bulk_launch, &a, 2);
+  for_blocks(pc, R_INNER, bulk_launch, &a, 6);
   if (o.bulk < o.cap) {
     k_substep_stiff<NS><<<g_stiff_ctas, 128, 0, pc->stream>>>(pc->d_blks, a.Q, pc->state, a.dQ, pc->subs, pc->dt,
                                                                o, pc->stiff);
-    mark(pc, 2);
+    mark(pc, 7);
   }
 }
 
