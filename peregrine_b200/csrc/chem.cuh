@@ -16,6 +16,9 @@
 namespace pgb {
 
 static __constant__ Mech kMech;
+// the same tables in global memory, for the passes whose lanes read
+// different reactions at once (constant memory serialises differing addresses)
+static __device__ Mech gMech;
 
 // the table log's and exp's tables, read per lane at differing bins: global
 // memory through the read-only cache rather than constant memory, which
@@ -205,6 +208,37 @@ __device__ __forceinline__ void fold(const RateState<NS> &s, double *omega, doub
       // a species a side destroys: the forward rate where it is a reactant, the reverse where a product
       if (WITHD) D[r.netsp[j]] += (nuMW < 0.0 ? -nuMW : 0.0) * fwd + (nuMW > 0.0 ? nuMW : 0.0) * rev;
     }
+  }
+}
+
+// the fold with the reactions across a warp's lanes, each lane its own
+// reactions' terms per species, a butterfly sum after: every lane ends with
+// the same omega (the terms' order differs from the one-lane fold's)
+template <int NS>
+__device__ __forceinline__ void fold_warp(const RateState<NS> &s, double *omega, const int lane) {
+  double part[NS];
+#pragma unroll
+  for (int n = 0; n < NS; n++) part[n] = 0.0;
+  const int nr = kMech.nr;
+  for (int k = lane; k < nr; k += 32) {
+    const Rxn &r = gMech.rxn[k];
+    double fwd, rev;
+    oneway<NS>(r, s, fwd, rev);
+    const double rp = r.reversible ? fwd - rev : fwd;
+    for (int j = 0; j < r.nnet; j++) {
+      const double add = r.netnuMW[j] * rp;
+      const int sp = r.netsp[j];
+#pragma unroll
+      for (int n = 0; n < NS; n++)
+        if (sp == n) part[n] += add;
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    double x = part[n];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    omega[n] = x;
   }
 }
 

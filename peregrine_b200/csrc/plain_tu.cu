@@ -162,6 +162,8 @@ extern "C" int PGB_ENTRY(pgb_plain_upload_)(const Species *sp, const Mech *mech,
   if (mech) {
     e = cudaMemcpyToSymbolAsync(kMech, mech, sizeof(Mech), 0, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "mechanism constants");
+    e = cudaMemcpyToSymbolAsync(gMech, mech, sizeof(Mech), 0, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "mechanism tables");
   }
   if (mt) {
     e = cudaMemcpyToSymbolAsync(gMath, mt, sizeof(MathTables), 0, cudaMemcpyHostToDevice, s);

@@ -40,11 +40,13 @@ __device__ __forceinline__ double especies(const int n, const double T, const do
 
 // integrate (substep.mako:4-87): up to limit substeps from Y, T over what
 // remains of the step; src gathers the mean rate; EXIT judges the
-// equilibrium exit at the first substep.  Returns the substeps taken.
-template <int NS, bool EXIT>
+// equilibrium exit at the first substep.  With WARP a whole warp integrates
+// the one cell, its lanes over the reactions (every lane holds the cell's
+// state alike).  Returns the substeps taken.
+template <int NS, bool EXIT, bool WARP = false>
 __device__ int substep_integrate(const double rho, const double rhoinv, const double step, double *Y, double &T,
                                  double *src, double &remaining, const int limit, const double eqtol,
-                                 const double stepfrac) {
+                                 const double stepfrac, const int lane = 0) {
   const double eps = 2.220446049250313e-16, tiny = 2.2250738585072014e-308, stepinv = 1.0 / step;
   auto Yof = [&](int n) { return Y[n]; };
   double rate[NS];
@@ -55,7 +57,9 @@ __device__ int substep_integrate(const double rho, const double rhoinv, const do
     ratestate<NS>(s, rho, Yof, T);
     // the first substep's fold carries the destruction rates the exit relaxes by
     double D[NS];
-    if (EXIT && eqtol > 0.0 && sub == 0)
+    if (WARP)
+      fold_warp<NS>(s, rate, lane);
+    else if (EXIT && eqtol > 0.0 && sub == 0)
       fold<NS, true>(s, rate, D);
     else
       fold<NS, false>(s, rate, nullptr);
@@ -200,7 +204,10 @@ __global__ void k_substep_bulk(const BlockDev *__restrict__ blks, int b, const d
 }
 
 // the stiff pass (stiff.mako:3-18): the listed cells from the start with the
-// cap and no exit, the warps taking the list 32 at a time, top bin first
+// cap and no exit, the list read top bin first.  A long list goes a cell to
+// a lane, the warps taking it 32 cells at a time; a list no longer than two
+// cells a warp goes a cell to a warp, its lanes over the reactions, so a few
+// cells that take the cap are not one lane's serial substeps
 template <int NS>
 __global__ void k_substep_stiff(const BlockDev *__restrict__ blks, const double *__restrict__ Qall,
                                 const double *__restrict__ stall, double *__restrict__ dQall, int *__restrict__ subs,
@@ -208,21 +215,26 @@ __global__ void k_substep_stiff(const BlockDev *__restrict__ blks, const double 
   constexpr int NE = 4 + NS;
   const int lane = threadIdx.x & 31;
   const unsigned int total = list.head[0];
+  const unsigned int nwarps = gridDim.x * (blockDim.x >> 5);
+  const bool per_warp = total <= 2u * nwarps;
+  // position p in the list read top bin first
+  auto at = [&](unsigned int p) {
+    int bin = o.bins - 1;
+    for (; bin > 0; bin--) {
+      const unsigned int n = list.head[1 + bin];
+      if (p < n) break;
+      p -= n;
+    }
+    return list.cells[(long long)bin * list.capacity + p];
+  };
   for (;;) {
     unsigned int base = 0;
-    if (lane == 0) base = atomicAdd(&list.head[o.bins + 1], 32u);
+    if (lane == 0) base = atomicAdd(&list.head[o.bins + 1], per_warp ? 1u : 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) return;  // the warp's lanes alike
-    unsigned int p = base + lane;
+    const unsigned int p = per_warp ? base : base + lane;
     if (p < total) {
-      // position p in the list read top bin first
-      int bin = o.bins - 1;
-      for (; bin > 0; bin--) {
-        const unsigned int n = list.head[1 + bin];
-        if (p < n) break;
-        p -= n;
-      }
-      const int2 code = list.cells[(long long)bin * list.capacity + p];
+      const int2 code = at(p);
       const BlockDev &B = blks[code.x];
       const long long c = code.y, v = B.vol;
       const double *Q = Qall + NE * B.cv + c;
@@ -230,10 +242,16 @@ __global__ void k_substep_stiff(const BlockDev *__restrict__ blks, const double 
       const double rho = Qf(0), rhoinv = 1.0 / rho, step = *dt;
       double Y[NS], src[NS], T = stall[SW * B.cv + 1 * v + c], remaining = 1.0;
       substep_start<NS>(Qf, rhoinv, Y, src);
-      const int taken =
-          substep_integrate<NS, false>(rho, rhoinv, step, Y, T, src, remaining, o.cap, o.eqtol, o.stepfrac);
-      subs[B.cv + c] = taken;
-      substep_source<NS>(dQall + NE * B.cv + c, v, src);
+      int taken;
+      if (per_warp)
+        taken = substep_integrate<NS, false, true>(rho, rhoinv, step, Y, T, src, remaining, o.cap, o.eqtol,
+                                                   o.stepfrac, lane);
+      else
+        taken = substep_integrate<NS, false>(rho, rhoinv, step, Y, T, src, remaining, o.cap, o.eqtol, o.stepfrac);
+      if (!per_warp || lane == 0) {
+        subs[B.cv + c] = taken;
+        substep_source<NS>(dQall + NE * B.cv + c, v, src);
+      }
     }
     __syncwarp();
   }
