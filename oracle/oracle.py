@@ -49,7 +49,9 @@ class OCase(ctypes.Structure):
                [("nbc", ctypes.c_int), ("bc", ctypes.POINTER(OBc)), ("substepped", ctypes.c_int), ("cap", ctypes.c_int),
                 ("eqtol", ctypes.c_double), ("dt", ctypes.c_double), ("ncppoly", ctypes.c_int),
                 ("cppoly", ctypes.POINTER(ctypes.c_double)), ("MW", ctypes.POINTER(ctypes.c_double)),
-                ("cfloor", ctypes.c_double)]
+                ("cfloor", ctypes.c_double), ("binary", ctypes.c_int), ("bwidth", ctypes.c_int),
+                ("nfit", ctypes.c_int), ("bpartial", ctypes.c_int), ("pairfit", ctypes.POINTER(ctypes.c_double)),
+                ("selffit", ctypes.POINTER(ctypes.c_double)), ("bath", ctypes.POINTER(ctypes.c_int))]
 
 # the boundary kinds (peregrine/simulator/euler/bcs.py, navstokes/bcs.py): the
 # oracle's number for each and the variables an entry gives, in order; the
@@ -207,7 +209,7 @@ def _lib():
     lib.oracle_advective_faces.restype = ctypes.c_int
     for name in ("oracle_production", "oracle_gibbs", "oracle_tlog", "oracle_texp", "oracle_mathtables",
                  "oracle_species_cph", "oracle_fromQ", "oracle_prestep", "oracle_realgas_frompT",
-                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads", "oracle_cflmax"):
+                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads", "oracle_cflmax", "oracle_transport"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 
@@ -365,6 +367,20 @@ class Oracle:
             self._tables["cppolyR"], self._tables["hpoly"] = cpr, hpoly
             c.ncp, c.cppolyR = cpr.shape[1], _ptr(cpr)
             c.nh, c.hpoly = hpoly.shape[1], _ptr(hpoly)
+        if "pairfit" in constants and trans is not None:
+            # binary diffusion, the mixture's pair fits (a table set made for it)
+            ns_ = ns
+            self_ = np.ascontiguousarray(constants["selffit"], dtype=np.float64)
+            pair = np.ascontiguousarray(constants["pairfit"], dtype=np.float64)
+            bath = np.ascontiguousarray(np.asarray(constants["bath"]).astype(np.int32))
+            mw = np.ascontiguousarray(constants["MW"], dtype=np.float64)
+            self._tables.update(selffit=self_, pairfit=pair, MWb=mw)
+            self._bath = bath
+            c.binary, c.nfit = 1, self_.shape[1]
+            c.bpartial = int(len(bath) < ns_)
+            c.bwidth = len(bath) if c.bpartial else ns_ - 1
+            c.pairfit, c.selffit, c.MW = _ptr(pair), _ptr(self_), _ptr(mw)
+            c.bath = bath.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         if trans == "kinetic-theory":
             c.trans = 1
             mu = np.ascontiguousarray(constants["mupoly"], dtype=np.float64)
@@ -533,6 +549,13 @@ class Oracle:
         out = np.zeros(3)
         self.lib.oracle_cflmax(ctypes.byref(self.case), obs, len(self.blocks), _ptr(out))
         return dict(zip(("acoustic", "convective", "combined"), out))
+
+    def transport(self, Q, state):
+        """(mu, kappa, D[ns]) rows of Q rows at their states (8-wide EosState rows)."""
+        Q, st = (np.ascontiguousarray(x, dtype=np.float64) for x in (Q, state))
+        out = np.zeros((len(Q), 2 + self.ns))
+        self.lib.oracle_transport(ctypes.byref(self.case), ctypes.c_long(len(Q)), _ptr(Q), _ptr(st), _ptr(out))
+        return out
 
     def bc_grads(self, grads, t=None):
         """The boundaries' gradient hook alone on grads[b] ([X][Y][Z][ngrad][3]

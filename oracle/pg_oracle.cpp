@@ -71,6 +71,11 @@ struct OCase {
   int ncppoly;
   const double *cppoly, *MW;
   double cfloor;
+  // binary diffusion (simulator/mixture/diffusion/binary.py): the pair fits
+  // [ns][width][nfit], the self fits [ns][nfit], and a partial bath's species
+  int binary, bwidth, nfit, bpartial;
+  const double *pairfit, *selffit;
+  const int *bath;
 };
 
 // one reaction, the columns of FiniteRateModel.rxnconsts
@@ -350,8 +355,51 @@ void transport(const OCase &c, const double *Q, const State &st, double *tr, dou
   const double kappa = 0.5 * (series + 1.0 / parallel);
   tr[0] = mu;
   tr[1] = kappa;
-  const double kor = kappa * rhoinv / st.cp;
-  for (int n = 0; n < ns; n++) tr[2 + n] = kor / c.lewis[n];
+  if (c.binary) {
+    // the mixture average of the pair fits (simulator/mixture/diffusion/kernels/binary.mako:13-62)
+    const double invT32 = 1.0 / (T * std::sqrt(T));
+    const double tiny = 64 * 2.220446049250313e-16;
+    for (int n = 0; n < ns; n++) {
+      double sum1 = 0.0, sum2 = 0.0, rest = 0.0, bathx = 0.0;
+      for (int k = 0; k < c.bwidth; k++) {
+        int m;
+        double Xm;
+        if (c.bpartial) {
+          m = c.bath[k];
+          Xm = m != n ? std::fmax(X(m), 0.0) : 0.0;
+        } else {
+          m = k + (k >= n);
+          Xm = std::fmax(X(m), 0.0);
+        }
+        double Dinv = 0.0;
+        for (int t = c.nfit - 1; t >= 0; t--) Dinv = Dinv * lnT + c.pairfit[(n * c.bwidth + k) * c.nfit + t];
+        Dinv *= invT32 * 1.0;
+        sum1 += Xm * Dinv;
+        sum2 += Xm * c.MW[m] * Dinv;
+        rest += Xm * c.MW[m];
+        bathx += Xm;
+      }
+      double Dinvself = 0.0;
+      for (int t = c.nfit - 1; t >= 0; t--) Dinvself = Dinvself * lnT + c.selffit[n * c.nfit + t];
+      Dinvself *= invT32 * 1.0;
+      const double Xn = std::fmax(X(n), 0.0);
+      bool alone;
+      double num, den;
+      if (c.bpartial) {
+        alone = 1.0 - Xn <= tiny || bathx <= tiny;
+        num = alone ? 1.0 : rest * bathx;
+        den = alone ? st.p * Dinvself : st.p * ((1.0 - Xn) * rest * sum1 + Xn * bathx * sum2);
+      } else {
+        alone = 1.0 - Xn <= tiny;
+        num = alone ? 1.0 : rest;
+        den = alone ? st.p * Dinvself : st.p * (rest * sum1 + Xn * sum2);
+      }
+      tr[2 + n] = (alone || (rest > 0.0 && den > 0.0)) ? num / den : 0.0;
+    }
+  } else {
+    const double kor = kappa * rhoinv / st.cp;
+    for (int n = 0; n < ns; n++) tr[2 + n] = kor / c.lewis[n];
+  }
   if (c.realgas) {
     rhspecies(c, hsp, [&](int n) { return Q[5 + n] * rhoinv; }, st.p, T, Z);
     return;
@@ -1946,6 +1994,20 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
               dQ[b][at * ne + l] = (iFl[l] + jFl[l] + kFl[l] - iFh[l] - jFh[l] - kFh[l]) * detJinv;
           }
         }
+  }
+  return 0;
+}
+
+// the transport state (mu, kappa, D[ns]) of n cells: Q rows and their
+// states (EosState rows, 8 wide); tr [n][2 + ns]
+int oracle_transport(const OCase *cp, long n, const double *Q, const double *st, double *tr) {
+  const OCase &c = *cp;
+  const int ne = 4 + c.ns;
+  std::vector<double> h(c.ns);
+  for (long q = 0; q < n; q++) {
+    State s;
+    std::memcpy(&s, st + q * 8, sizeof(State));
+    transport(c, Q + q * ne, s, tr + q * (2 + c.ns), h.data());
   }
   return 0;
 }

@@ -147,6 +147,8 @@ class Config(dict):
         # the double flux freezes the real gas's tangent plane (peregrine/simulator/eulerdf/simulator.py:15-20)
         if (sim["simulator"] == "euler-df") != (self["mixture"]["eos"] == "real-gas-df"):
             raise ConfigError("mixture.eos", "euler-df takes real-gas-df, and that eos euler-df")
+        if self["mixture"]["diffusion"] not in ("lewis", "binary"):
+            raise ConfigError("mixture.diffusion", f"{self['mixture']['diffusion']!r} is not one of ('lewis', 'binary')")
         if self["diff-flux"]["formula"] != "alpha-damping":
             raise ConfigError("diff-flux.formula", "only 'alpha-damping' is built")
         if self["mixture"]["chemistry"] not in (None, "finite-rate"):

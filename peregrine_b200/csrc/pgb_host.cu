@@ -256,6 +256,42 @@ int build_species(pgb_case *c) {
     RET(fit("mupoly", c->sp.mupoly, c->sp.nmu));
     RET(fit("kappapoly", c->sp.kappapoly, c->sp.nkappa));
   }
+  // binary diffusion, when its pair fits are given: "selffit" [ns][terms],
+  // "pairfit" [ns][width][terms], "bath" the species a partial bath sums over
+  // (peregrine/simulator/mixture/diffusion/binary.py:18-37)
+  c->sp.binary = 0;
+  if (table(c, "pairfit") || table(c, "selffit")) {
+    if (!table(c, "pairfit") || !table(c, "selffit")) return fail(PGB_ERR_ARG, "binary diffusion takes pairfit and selffit");
+    const std::vector<double> &self = c->tables["selffit"], &pair = c->tables["pairfit"];
+    if (self.size() % ns || self.size() / ns < 1 || self.size() / ns > MAXT)
+      return fail(PGB_ERR_ARG, "selffit: species times 1 to 8 terms");
+    const int terms = (int)(self.size() / ns);
+    int width = ns - 1;
+    c->sp.bpartial = 0;
+    if (table(c, "bath")) {
+      const std::vector<double> &bath = c->tables["bath"];
+      if (bath.empty() || (int)bath.size() > ns) return fail(PGB_ERR_ARG, "bath: 1 to ns species");
+      for (size_t k = 0; k < bath.size(); k++) {
+        const int m = (int)bath[k];
+        if (m < 0 || m >= ns || (double)m != bath[k]) return fail(PGB_ERR_ARG, "bath: species indices");
+        c->sp.bath[k] = m;
+      }
+      if ((int)bath.size() < ns) c->sp.bpartial = 1, width = (int)bath.size();
+    }
+    if ((long)pair.size() != (long)ns * width * terms)
+      return fail(PGB_ERR_ARG, "pairfit: species times partners times the selffit's terms");
+    c->sp.bwidth = width, c->sp.npair = terms, c->sp.nself = terms;
+    for (int n = 0; n < ns; n++)
+      for (int t = 0; t < MAXT; t++) {
+        c->sp.selffit[n * MAXT + t] = t < terms ? self[n * terms + t] : 0.0;
+        for (int k = 0; k < MAXNS; k++)
+          c->sp.pairfit[(n * MAXNS + k) * MAXT + t] = (k < width && t < terms) ? pair[(n * width + k) * terms + t] : 0.0;
+      }
+    const double *mw = table(c, "MW");
+    if (!mw || (long)c->tables["MW"].size() < ns) return fail(PGB_ERR_ARG, "binary diffusion reads MW");
+    for (int n = 0; n < ns; n++) c->sp.MW[n] = mw[n];
+    c->sp.binary = 1;
+  }
   if (c->phys.chemistry != PGB_CHEM_NONE && !c->mech)
     return fail(PGB_ERR_STATE, "finite-rate chemistry needs pgb_case_set_mechanism before finalize");
   if (c->phys.chemistry == PGB_CHEM_SUBSTEPPED) {

@@ -40,6 +40,13 @@ struct Species {
   // (peregrine/simulator/mixture/eos/base.py:33-47), and molar masses
   int ncppoly;
   double cppoly[MAXNS * MAXT], MW[MAXNS];
+  // binary diffusion (peregrine/simulator/mixture/diffusion/binary.py): the
+  // pair fits of T^(3/2) / D at unit pressure, a row per species of its
+  // partners' in walk order ([species][partner][term]), each species' own
+  // pair, and the bath (a partial bath lists its species; width partners)
+  int binary, bpartial, bwidth, npair, nself;
+  int bath[MAXNS];
+  double pairfit[MAXNS * MAXNS * MAXT], selffit[MAXNS * MAXT];
   // the cubic real gas (a thermally perfect gas underneath, tpg set too) and
   // its double flux: the form's u, w and roots sigma, eps; per species
   // sqrt(a_c), b, -(da/dT) sqrt(T / a), m / sqrt(Tc), 1 + m, each of the first
@@ -288,6 +295,68 @@ __device__ __forceinline__ State fromprims(const double *q, double *Q) {
 template <int NS, class YF>
 __device__ __forceinline__ void hspecies_rg_of(double *h, YF Y, const double p, const double T, const double Z);
 
+// the mixture-averaged diffusion coefficients from the pair fits
+// (peregrine/simulator/mixture/diffusion/kernels/binary.mako:13-62): per
+// species the sums over its partners of X_m / D_nm and X_m MW_m / D_nm, one
+// quotient; a species alone (X_n within 64 eps of one) takes its
+// self-diffusion coefficient, a composition of nothing D = 0
+template <int NS>
+__device__ __forceinline__ void binary_diffusion(double *D, const double p, const double T, const double lnT,
+                                                 const double *X) {
+  const double invT32 = 1.0 / (T * sqrt(T));
+  const double tiny = 64 * 2.220446049250313e-16;
+  const int width = kSp.bwidth;
+#pragma unroll
+  for (int n = 0; n < NS; n++) {
+    double sum1 = 0.0, sum2 = 0.0, rest = 0.0, bathx = 0.0;
+    auto partner = [&](const int k, const int m, const double Xm) {
+      double Dinv = 0.0;
+#pragma unroll
+      for (int t = MAXT - 1; t >= 0; t--)
+        if (t < kSp.npair) Dinv = Dinv * lnT + kSp.pairfit[(n * MAXNS + k) * MAXT + t];
+      Dinv *= invT32 * 1.0;
+      sum1 += Xm * Dinv;
+      sum2 += Xm * kSp.MW[m] * Dinv;
+      rest += Xm * kSp.MW[m];
+      bathx += Xm;
+    };
+    if (kSp.bpartial) {
+      for (int k = 0; k < width; k++) {
+        const int m = kSp.bath[k];
+        double Xm = 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; q++)
+          if (q == m && m != n) Xm = fmax(X[q], 0.0);
+        partner(k, m, Xm);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NS - 1; k++) {
+        const int m = k + (k >= n);
+        partner(k, m, fmax(X[m], 0.0));
+      }
+    }
+    double Dinvself = 0.0;
+#pragma unroll
+    for (int t = MAXT - 1; t >= 0; t--)
+      if (t < kSp.nself) Dinvself = Dinvself * lnT + kSp.selffit[n * MAXT + t];
+    Dinvself *= invT32 * 1.0;
+    const double Xn = fmax(X[n], 0.0);
+    bool alone;
+    double num, den;
+    if (kSp.bpartial) {
+      alone = 1.0 - Xn <= tiny || bathx <= tiny;
+      num = alone ? 1.0 : rest * bathx;
+      den = alone ? p * Dinvself : p * ((1.0 - Xn) * rest * sum1 + Xn * bathx * sum2);
+    } else {
+      alone = 1.0 - Xn <= tiny;
+      num = alone ? 1.0 : rest;
+      den = alone ? p * Dinvself : p * (rest * sum1 + Xn * sum2);
+    }
+    D[n] = (alone || (rest > 0.0 && den > 0.0)) ? num / den : 0.0;
+  }
+}
+
 template <int NS, class QF, bool RG = false>
 __device__ __forceinline__ void transport(QF Q, const State &st, double *tr, double *hsp, const double Z = 0.0) {
   const double rho = Q(0), rhoinv = 1.0 / rho;
@@ -346,9 +415,13 @@ __device__ __forceinline__ void transport(QF Q, const State &st, double *tr, dou
   const double kappa = 0.5 * (series + 1.0 / parallel);
   tr[0] = mu;
   tr[1] = kappa;
-  const double kor = kappa * rhoinv / st.cp;
+  if (kSp.binary) {
+    binary_diffusion<NS>(tr + 2, st.p, T, lnT, X);
+  } else {
+    const double kor = kappa * rhoinv / st.cp;
 #pragma unroll
-  for (int n = 0; n < NS; n++) tr[2 + n] = kor / kSp.lewis[n];
+    for (int n = 0; n < NS; n++) tr[2 + n] = kor / kSp.lewis[n];
+  }
   // hspecies: the real gas's partial enthalpies at the stored state, or the
   // ideal ones (peregrine/simulator/mixture/eos/kernels/species.mako:9-15, 31-36)
   if (RG) {

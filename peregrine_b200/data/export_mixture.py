@@ -3,7 +3,8 @@ them, to an .npz that peregrine_b200 loads.
 
     python -m peregrine_b200.data.export_mixture REFERENCE OUT.npz MECHANISM \\
         [--keep H2,H,O,...] [--eos tpg] [--trans kinetic-theory] \\
-        [--chemistry finite-rate] [--trange 300 3500] [--cubic srk|pr]
+        [--chemistry finite-rate] [--trange 300 3500] [--cubic srk|pr] \\
+        [--diffusion lewis|binary]
 
 MECHANISM is a mechanism file, or species of the reference's library
 separated by commas.
@@ -136,7 +137,7 @@ def subset(mechanism, keep, where):
 
 
 def reference_mixture(reference, species, eos="tpg", trans=None, chemistry=None, trange=(300.0, 3500.0),
-                      cubic="srk"):
+                      cubic="srk", diffusion="lewis"):
     """The reference's Mixture for a config, from a checkout at reference."""
     install_stubs()
     if reference not in sys.path:
@@ -153,6 +154,7 @@ def reference_mixture(reference, species, eos="tpg", trans=None, chemistry=None,
     m = cfg["mixture"]
     m["species"], m["eos"], m["trans"], m["chemistry"] = species, eos, trans, chemistry
     m["T-range"] = tuple(trange)
+    m["diffusion"] = diffusion
     return get_mixture(cfg)
 
 
@@ -167,6 +169,7 @@ def tables(mix):
         out["cubic_m"] = np.array(c["m"])
     out["trans"] = np.array(mix.trans.name if mix.trans is not None else "")
     out["ns"] = np.array(mix.ns)
+    out["diffusion"] = np.array(mix.diffusion.name if getattr(mix, "diffusion", None) is not None else "lewis")
     if mix.chemistry is not None:
         cols = mix.chemistry.rxnconsts(mix.species)
         terms = mix.chemistry.terms(mix.species)
@@ -195,6 +198,7 @@ def main(argv=None):
     ap.add_argument("--chemistry", default=None)
     ap.add_argument("--trange", nargs=2, type=float, default=(300.0, 3500.0))
     ap.add_argument("--cubic", default="srk", choices=sorted(CUBICS))
+    ap.add_argument("--diffusion", default="lewis", choices=("lewis", "binary"))
     a = ap.parse_args(argv)
     mech = a.mechanism
     if "," in mech:
@@ -205,7 +209,7 @@ def main(argv=None):
     with tempfile.TemporaryDirectory() as tmp:
         if a.keep and isinstance(mech, str):
             mech = subset(mech, a.keep.split(","), tmp)
-        mix = reference_mixture(a.reference, mech, a.eos, a.trans, a.chemistry, a.trange, a.cubic)
+        mix = reference_mixture(a.reference, mech, a.eos, a.trans, a.chemistry, a.trange, a.cubic, a.diffusion)
         np.savez(a.out, **tables(mix))
     print(a.out, mix)
 

@@ -64,6 +64,10 @@ class Mixture:
         self.ns = len(self.spnames)
         self.eos = cfgsect["eos"]
         self.trans = cfgsect["trans"]
+        self.diffusion = cfgsect.get("diffusion", "lewis") or "lewis"
+        if self.diffusion != "lewis":
+            raise ValueError(f"mixture.diffusion {self.diffusion!r}: binary diffusion reads the pair fits a table "
+                             "set carries (its species' collision parameters)")
         if self.eos != "cpg":
             raise ValueError(f"mixture.eos {self.eos!r}: this gas model is not built yet")
         for name, sp in self.species.items():
@@ -92,6 +96,12 @@ class Mixture:
             raise ValueError(f"mixture.trans {self.trans!r}: the tables were made for {str(tables['trans'])!r}")
         if self.chemistry is not None and "rxn_nr" not in tables:
             raise ValueError("mixture.chemistry: the tables carry no reactions")
+        # species diffusion: Lewis numbers, or binary diffusion's pair fits
+        # (peregrine/simulator/mixture/diffusion/{lewis,binary}.py)
+        self.diffusion = cfgsect.get("diffusion", "lewis") or "lewis"
+        made = str(tables["diffusion"]) if "diffusion" in tables else "lewis"
+        if self.trans is not None and self.diffusion != made:
+            raise ValueError(f"mixture.diffusion {self.diffusion!r}: the tables were made for {made!r}")
 
     def collect(self, key, default=None):
         values = [sp.get(key, default) for sp in self.species.values()]

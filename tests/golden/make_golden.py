@@ -30,6 +30,11 @@ What it records, each from the reference's own code:
                      Gibbs functions, and the species' cp and h by the
                      reference's own polynomial evaluation.
 
+  binary_h2o2.npz    peregrine/simulator/mixture/diffusion/binary.py's pair
+                     coefficients T^(3/2) / D at unit pressure for the
+                     9-species H2/O2/N2 gas, at its fit's sample temperatures,
+                     unfitted (the model's fit step replaced by the identity);
+
   realgas_<cubic>.npz tests/eos/support.py's textbook density of the cubic
                      (numpy's roots and the least Gibbs energy phase) for O2/H2
                      at random (p, T, Y), the reference's Soave-Redlich-Kwong
@@ -223,6 +228,24 @@ def rates_of(reference, mech, keep, n, rng):
                 Ts=Ts, cpR=cpR, hR=hR)
 
 
+def binary_pairs(reference):
+    from peregrine_b200.data.export_mixture import reference_mixture, subset
+    from peregrine.simulator.mixture.diffusion.binary import BinaryModel
+    from peregrine.simulator.mixture.transport.kinetic import KineticTheoryModel
+    import tempfile
+
+    path = os.path.join(reference, "peregrine", "simulator", "mixture", "database", "mechanisms", "GRI30.yaml")
+    keep = ["H2", "H", "O", "O2", "OH", "H2O", "HO2", "H2O2", "N2"]
+    with tempfile.TemporaryDirectory() as tmp:
+        mix = reference_mixture(reference, subset(path, keep, tmp), "tpg", "kinetic-theory", None, diffusion="binary")
+    model = BinaryModel(mix.cfgsect)
+    Ts = KineticTheoryModel(mix.cfgsect).ljparams(mix.species)["Ts"]
+    # the model's own pair coefficients before its refit
+    model.fit = lambda x, y, tol, deg: (np.asarray(y), None)
+    raw = np.array(model.dijinv(mix.species))
+    return dict(Ts=np.asarray(Ts), diffinv=raw, tol=np.array(mix.cfgsect["refit-tol"]))
+
+
 def realgas_densities(reference, cubic, n, rng):
     from peregrine_b200.data.export_mixture import CUBICS, reference_mixture
     from tests.eos import support
@@ -320,6 +343,7 @@ def main():
              **rates_of(REF, "GRI30.yaml", h2o2, 96, np.random.default_rng(20261206)))
     np.savez(os.path.join(HERE, "rates_ch4_o2_ffcmy.npz"),
              **rates_of(REF, "CH4_O2_FFCMY.yaml", None, 96, np.random.default_rng(20261207)))
+    np.savez(os.path.join(HERE, "binary_h2o2.npz"), **binary_pairs(REF))
     for cubic in ("srk", "pr"):
         np.savez(os.path.join(HERE, f"realgas_{cubic}.npz"),
                  **realgas_densities(REF, cubic, 128, np.random.default_rng(20261208)))
