@@ -202,6 +202,7 @@ def cpu_baseline(mesh_blocks, metrics, prims, constants, budget_s=15.0):
 
     orc = Oracle(constants, 1, "navier-stokes", mesh_blocks, metrics, "rk4")
     orc.set_prims(prims)
+    orc.threads = os.cpu_count() or 1
     dQ = [np.zeros_like(r) for r in orc.regs[0]]
     ncells = sum(b.ncells for b in mesh_blocks)
     stages = 0
@@ -252,6 +253,7 @@ def reacting_leg(steps, cpu=True):
         orc = Oracle(consts, mb.ns, "navier-stokes", mb.mesh_blocks, mb.metrics, "tvd-rk3", primary="hllc",
                      recon="muscl", limiter="koren", eos="tpg", trans="kinetic-theory", chemistry="finite-rate")
         orc.set_prims(prims)
+        orc.threads = os.cpu_count() or 1
         dQ = [np.zeros_like(r) for r in orc.regs[0]]
         t0 = time.perf_counter()
         orc.rhs(orc.regs[0], dQ)
@@ -339,6 +341,7 @@ def realgas_leg(steps, cpu=True):
         orc = Oracle(mb.mixture.constants(), mb.ns, "euler", mb.mesh_blocks, mb.metrics, "tvd-rk3",
                      eos="real-gas-df", trans="constant")
         orc.set_prims(prims)
+        orc.threads = os.cpu_count() or 1
         dQ = [np.zeros_like(r) for r in orc.regs[0]]
         orc.rhs(orc.regs[0], dQ)  # the planes' settle
         t0 = time.perf_counter()
@@ -393,6 +396,7 @@ def boundary_leg(steps, cpu=True):
             q[...] = [ic["p"], ic["u"], ic["v"], ic["w"], ic["T"], ic["Y"]["A"]]
             prims.append(q)
         orc.set_prims(prims)
+        orc.threads = os.cpu_count() or 1
         dQ = [np.zeros_like(r) for r in orc.regs[0]]
         t0 = time.perf_counter()
         orc.rhs(orc.regs[0], dQ)
@@ -465,6 +469,7 @@ def reference_arm(args):
     mix = Mixture(cfg["mixture"])
     orc = Oracle(mix.constants(), 1, "navier-stokes", blocks, mets, "rk4")
     orc.set_prims(prims)
+    orc.threads = os.cpu_count() or 1
     dQ = [np.zeros_like(r) for r in orc.regs[0]]
     ncells = sum(b.ncells for b in blocks)
     for _ in range(args.warmup):

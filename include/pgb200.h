@@ -41,7 +41,9 @@ enum {
 };
 
 /* physics selectors: the config's names (peregrine/config.py:12-98) */
-enum { PGB_EULER = 0, PGB_NAVIER_STOKES = 1, PGB_EULER_DF = 2 };
+/* the double flux's simulators freeze the real gas's tangent plane each step
+ * (peregrine/simulator/eulerdf/simulator.py, navstokesdf/simulator.py) */
+enum { PGB_EULER = 0, PGB_NAVIER_STOKES = 1, PGB_EULER_DF = 2, PGB_NAVIER_STOKES_DF = 3 };
 enum { PGB_EOS_CPG = 0, PGB_EOS_TPG = 1, PGB_EOS_REALGAS = 2, PGB_EOS_REALGAS_DF = 3 };
 enum { PGB_FLUX_KEPAEC = 0, PGB_FLUX_HLLC = 1, PGB_FLUX_RUSANOV = 2, PGB_FLUX_AUSMUP = 3 };
 enum { PGB_RECON_CONSTANT = 0, PGB_RECON_MUSCL = 1 };
@@ -68,7 +70,7 @@ enum {
 typedef struct pgb_case pgb_case;
 
 typedef struct {
-  int simulator;  /* PGB_EULER / PGB_NAVIER_STOKES */
+  int simulator;  /* PGB_EULER, PGB_NAVIER_STOKES, PGB_EULER_DF, PGB_NAVIER_STOKES_DF */
   int eos;        /* PGB_EOS_* */
   int primary;    /* PGB_FLUX_* */
   int recon;      /* PGB_RECON_* */
@@ -268,6 +270,15 @@ int pgb_array_get(pgb_case *c, int blk, int reg, double *host, long count);
  * left there (exchanged, or set by a boundary); its edges and corners are
  * never read (the reference's full host view, peregrine/backend/allocation.py) */
 int pgb_array_get_full(pgb_case *c, int blk, int reg, double *host, long count);
+
+/* One field of a block's eos state, full extents (nx+4, ny+4, nz+4), F order,
+ * count = full cells: the state the last right-hand side or pgb_set_prims
+ * formed.  Fields: 0 p, 1 T, 2 1/rho, 3 rho, 4 e, 5 cp, 6 gamma, 7 c, 8 the
+ * real gas's Z, 9.. the double flux's plane (theta, eps, kappa, zeta per
+ * carried species).  PGB_ERR_STATE after a batched step, which keeps no
+ * state array (the reference's block state, read by its export,
+ * peregrine/simulator/euler/simulator.py:66-90) */
+int pgb_eos_get(pgb_case *c, int blk, int field, double *host, long count);
 
 /* Every block's interior cells of register reg at once: the blocks' F-order
  * interior arrays end to end, in block order (count = ne x total cells). */

@@ -198,6 +198,10 @@ def build_mech(consts):
     return keep
 
 
+# the case size from which the oracle's loops share the host's cores
+SMALL = 1 << 16
+
+
 def _lib():
     if not os.path.exists(LIB):
         raise RuntimeError(f"{LIB} is not built; run oracle/build.sh")
@@ -333,7 +337,7 @@ class Oracle:
         self.integrator = integrator
         self._tables = {}
         c = OCase()
-        c.simulator = 1 if simulator == "navier-stokes" else 0
+        c.simulator = 1 if simulator in ("navier-stokes", "navier-stokes-df") else 0
         c.primary = self.PRIMARY[primary]
         c.recon = 1 if recon == "muscl" else 0
         c.limiter = self.LIMITERS[limiter]
@@ -403,6 +407,9 @@ class Oracle:
             c.ncppoly, c.cppoly, c.MW = cpp.shape[1], _ptr(cpp), _ptr(mw)
             c.cfloor = float(np.exp(float(constants["logcfloor"])))
         self.case = c
+        # one thread below SMALL cells in all (a test's case), every core above
+        cells = sum(int(np.prod([n + 2 * b.ng for n in b.cells])) for b in blocks)
+        self.threads = 1 if cells < SMALL else (os.cpu_count() or 1)
         self.map = halo_map(blocks)
         self.nregs = NREGS[integrator]
         self.regs = [[np.zeros(self._shape(b)) for b in blocks] for _ in range(self.nregs)]
@@ -453,6 +460,7 @@ class Oracle:
         return tuple(n + 2 * blk.ng for n in blk.cells) + (self.ne,)
 
     def _oblocks(self, Q):
+        self.lib.oracle_set_threads(self.threads)
         obs = (OBlock * len(self.blocks))()
         keep = []
         for n, (blk, m) in enumerate(zip(self.blocks, self.metrics)):

@@ -19,6 +19,7 @@
 #include <vector>
 #include <algorithm>
 #include <cfloat>
+#include <omp.h>
 
 extern "C" {
 
@@ -1343,10 +1344,51 @@ void ausmup(const OCase &c, const Side &L, const Side &R, const double *YL, cons
   for (int n = 0; n < c.ns - 1; n++) F[5 + n] = mdot * Y[n];
 }
 
+// the double flux's Rusanov and AUSM+-up (simulator/eulerdf/kernels/flux/function/rusanov.mako:1-14,
+// ausmup.mako:1-15): over the plain flux the energy row again in each cell's
+// frozen plane, F[4] in the left's (recL) and F[ne] in the right's (recR),
+// from each side's energy in that plane (eside,
+// simulator/mixture/eos/realgasdf/kernels/eos.mako:73-83)
+void riemann_df(const OCase &c, const Side &L, const Side &R, const double *YL, const double *YR, const double *S,
+                const double *recL, const double *recR, double *F) {
+  const int ns = c.ns, ne = 4 + ns;
+  auto eside = [&](const Side &x, const double *Y, double *E) {
+    for (int q = 0; q < 2; q++) {
+      const double *pl = q == 0 ? recL : recR;
+      double comp = 0.0;
+      for (int n = 0; n < ns - 1; n++) comp += pl[S_ZETA + n] * Y[n];
+      E[q] = pl[S_THETA] * x.s.p + x.s.rho * (pl[S_EPS] + comp + 0.5 * ((x.u) * (x.u) + (x.v) * (x.v) + (x.w) * (x.w))) +
+             pl[S_KAPPA];
+    }
+  };
+  if (c.primary == O_RUSANOV) {
+    const double area = std::sqrt(((S[0]) * (S[0]) + (S[1]) * (S[1]) + (S[2]) * (S[2])));
+    const double unL = ((L.u) * (S[0]) + (L.v) * (S[1]) + (L.w) * (S[2])) / area;
+    const double unR = ((R.u) * (S[0]) + (R.v) * (S[1]) + (R.w) * (S[2])) / area;
+    const double lam = std::fmax(std::fabs(unL) + L.s.c, std::fabs(unR) + R.s.c) * area;
+    const double UL = unL * area, UR = unR * area;
+    double EpL[2], EpR[2];
+    eside(L, YL, EpL);
+    eside(R, YR, EpR);
+    for (int q = 0; q < 2; q++)
+      F[q == 0 ? 4 : ne] = 0.5 * (UR * (EpR[q] + R.s.p) + UL * (EpL[q] + L.s.p) - lam * (EpR[q] - EpL[q]));
+  } else {
+    const double mdot = F[0];
+    const bool left = mdot > 0.0;
+    const Side &U = left ? L : R;
+    const double rhoinvU = 1.0 / U.s.rho;
+    double Ep[2];
+    eside(U, left ? YL : YR, Ep);
+    for (int q = 0; q < 2; q++) F[q == 0 ? 4 : ne] = mdot * (Ep[q] + U.s.p) * rhoinvU;
+  }
+}
+
 // the advective flux of one face from its four cells (LL and RR read by MUSCL only):
-// the reconstruction, then the flux function (simulator/euler/kernels/flux/single.mako:4-9)
+// the reconstruction, then the flux function (simulator/euler/kernels/flux/single.mako:4-9);
+// with the double flux's records of the two cells (recL, recR), its form
 void advective(const OCase &c, const double *QLL, const double *QL, const double *QR, const double *QRR,
-               const State &sLL, const State &sL, const State &sR, const State &sRR, const double *S, double *F) {
+               const State &sLL, const State &sL, const State &sR, const State &sRR, const double *S, double *F,
+               const double *recL = nullptr, const double *recR = nullptr) {
   double YL[16], YR[16];
   if (c.primary == O_KEPAEC) {
     kepaec(c, side(QL, sL), side(QR, sR), QL, QR, S, F);
@@ -1362,6 +1404,7 @@ void advective(const OCase &c, const double *QLL, const double *QL, const double
   if (c.primary == O_HLLC) hllc(c, L, R, YL, YR, S, F);
   else if (c.primary == O_RUSANOV) rusanov(c, L, R, YL, YR, S, F);
   else ausmup(c, L, R, YL, YR, S, F);
+  if (recL) riemann_df(c, L, R, YL, YR, S, recL, recR, F);
 }
 
 // alpha damping (simulator/navstokes/kernels/flux/alpha-damping.mako:3-92)
@@ -1447,6 +1490,9 @@ void alphadamping(const OCase &c, const double *S, const double *xf, const doubl
   const double hns = 0.5 * (hspR[ns - 1] + hspL[ns - 1]);
   f4 += (-rho * Dk * gradYns + Yns * corr) * hns;
   F[4] += f4;
+  // the double flux's second energy row takes the same diffusive energy flux
+  // (simulator/navstokesdf/kernels/flux/alpha-damping.mako:1-9)
+  if (c.df) F[4 + ns] += f4;
 }
 
 // the per-block scratch one right-hand side fills, as the reference's arrays
@@ -1930,8 +1976,11 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
             const State &sRR = *reinterpret_cast<const State *>(&s.state[RR * NSTATE]);
             double *F = &s.F[a][at * nf];
             const double *S = B.S[a] + at * 3;
-            if (c.df)
+            if (c.df && c.primary == O_KEPAEC)
               kepaec_df(c, QL, QR, &s.state[L * NSTATE], &s.state[R * NSTATE], S, F);
+            else if (c.df)
+              advective(c, B.Q + LL * ne, QL, QR, B.Q + RR * ne, sLL, sL, sR, sRR, S, F, &s.state[L * NSTATE],
+                        &s.state[R * NSTATE]);
             else if (!c.skip_adv)
               advective(c, B.Q + LL * ne, QL, QR, B.Q + RR * ne, sLL, sL, sR, sRR, S, F);
             if (visc)
@@ -2271,3 +2320,11 @@ int oracle_combine(int nx, int ny, int nz, int ng, int ne, double *out, int own,
 }
 
 }  // extern "C"
+
+// the threads the oracle's loops share: one for the small cases a test
+// runs (a fork per loop costs more than the loop), the host's cores for
+// the large ones
+extern "C" int oracle_set_threads(int n) {
+  omp_set_num_threads(n < 1 ? 1 : n);
+  return 0;
+}

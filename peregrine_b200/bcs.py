@@ -117,10 +117,9 @@ class Entry:
         if kind not in KINDS:
             raise ConfigError(f"bcvals.{name}.kind", f"{kind!r} is not a boundary kind; the kinds are {sorted(KINDS)}")
         variables, simulators = KINDS[kind]
-        # the double flux's simulator takes the inviscid kinds
-        # (peregrine/simulator/eulerdf/simulator.py:10)
-        if simulator == "euler-df":
-            simulator = "euler"
+        # the double flux's simulators take their plain twins' kinds
+        # (peregrine/simulator/eulerdf/simulator.py:10, navstokesdf/bcs.py)
+        simulator = {"euler-df": "euler", "navier-stokes-df": "navier-stokes"}.get(simulator, simulator)
         if simulator not in simulators:
             raise ConfigError(f"bcvals.{name}.kind", f"{kind} is not a boundary of the {simulator} simulator")
         self.kind = kind

@@ -216,14 +216,15 @@ def reacting_prims(metrics, spnames, MW, cells, length=0.01, seed=0, spots=4, dT
 
 # the transcritical mixing layer: O2 (dense, 120 K) and H2 (300 K) at 60 bar,
 # the real gas with the double flux
-def mixing_layer_config(cubic="pr", simulator="euler-df", integrator="tvd-rk3", launch="per-block"):
+def mixing_layer_config(cubic="pr", simulator="euler-df", integrator="tvd-rk3", launch="per-block", primary="kepaec",
+                        recon="constant", limiter=None):
     cfg = Config()
     cfg["simulation"]["simulator"] = simulator
     cfg["mixture"]["species"] = f"o2_h2_{cubic}"
-    cfg["mixture"]["eos"] = "real-gas-df" if simulator == "euler-df" else "real-gas"
-    cfg["mixture"]["trans"] = "constant" if simulator == "navier-stokes" else None
+    cfg["mixture"]["eos"] = "real-gas-df" if simulator.endswith("-df") else "real-gas"
+    cfg["mixture"]["trans"] = "kinetic-theory" if simulator.startswith("navier-stokes") else None
     cfg["time-integration"]["integrator"] = integrator
-    cfg["adv-flux"]["primary"] = "kepaec"
+    cfg["adv-flux"].update(primary=primary, recon=recon, limiter=limiter)
     cfg["backend-b200"]["launch"] = launch
     return cfg.validate()
 

@@ -84,7 +84,9 @@ _DEFAULTS = {
     "halo-exchange": {"kind": "device"},
 }
 
-SIMULATORS = ("euler", "navier-stokes", "euler-df")
+SIMULATORS = ("euler", "navier-stokes", "euler-df", "navier-stokes-df")
+VISCOUS = ("navier-stokes", "navier-stokes-df")
+DOUBLE_FLUX = ("euler-df", "navier-stokes-df")
 INTEGRATORS = ("rk1", "rk2", "tvd-rk3", "rk34", "rk4")
 EOSES = ("cpg", "tpg", "real-gas", "real-gas-df")
 TRANS = (None, "constant", "kinetic-theory")
@@ -142,11 +144,15 @@ class Config(dict):
             raise ConfigError("adv-flux.limiter", "muscl names a limiter")
         if adv["primary"] == "kepaec" and adv["recon"] != "constant":
             raise ConfigError("adv-flux.recon", "kepaec takes the constant reconstruction only")
-        if sim["simulator"] == "navier-stokes" and self["mixture"]["trans"] is None:
+        if sim["simulator"] in VISCOUS and self["mixture"]["trans"] is None:
             raise ConfigError("mixture.trans", "a viscous case names a transport model")
-        # the double flux freezes the real gas's tangent plane (peregrine/simulator/eulerdf/simulator.py:15-20)
-        if (sim["simulator"] == "euler-df") != (self["mixture"]["eos"] == "real-gas-df"):
-            raise ConfigError("mixture.eos", "euler-df takes real-gas-df, and that eos euler-df")
+        # the double flux freezes the real gas's tangent plane (peregrine/simulator/eulerdf/simulator.py:15-20),
+        # with the flux functions it has a form of (peregrine/simulator/eulerdf/kernels/flux/function/)
+        if (sim["simulator"] in DOUBLE_FLUX) != (self["mixture"]["eos"] == "real-gas-df"):
+            raise ConfigError("mixture.eos", f"{sim['simulator']}: euler-df and navier-stokes-df take real-gas-df, "
+                                             "and that eos one of them")
+        if sim["simulator"] in DOUBLE_FLUX and adv["primary"] == "hllc":
+            raise ConfigError("adv-flux.primary", "the double flux has kepaec, rusanov and ausmup")
         if self["mixture"]["diffusion"] not in ("lewis", "binary"):
             raise ConfigError("mixture.diffusion", f"{self['mixture']['diffusion']!r} is not one of ('lewis', 'binary')")
         if self["diff-flux"]["formula"] != "alpha-damping":

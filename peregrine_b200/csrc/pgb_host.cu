@@ -149,6 +149,7 @@ struct pgb_case {
   unsigned long long uid = 0;  // unique over the process, never reused
   unsigned version = 0;        // bumped when the species or mechanism tables change
   bool df_fresh = true;        // the double flux has no frozen planes for the state yet
+  bool state_stale = false;    // a batched step since the state array was last written
   // boundaries: the entries and their programs as given, then on the device
   // the entries, programs and the three passes' face tables (each with its
   // sentinel), and the clock the boundary values read
@@ -174,6 +175,11 @@ struct pgb_case {
 };
 
 namespace {
+
+// the simulators' two traits: viscous (navier-stokes, navier-stokes-df) and
+// the double flux (euler-df, navier-stokes-df)
+inline bool sim_visc(int s) { return s == PGB_NAVIER_STOKES || s == PGB_NAVIER_STOKES_DF; }
+inline bool sim_df(int s) { return s == PGB_EULER_DF || s == PGB_NAVIER_STOKES_DF; }
 
 bool fused_capable(const pgb_case *c) {
   const pgb_physics &p = c->phys;
@@ -838,6 +844,7 @@ int cfl_prologue(pgb_case *c, int qphys, int &count) {
 
 int step_fused(pgb_case *c, int &count) {
   const auto &plan = c->plans[c->phase];
+  c->state_stale = true;
   RET(cfl_prologue(c, plan[0].qin, count));
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int) * plan.size(), c->stream));
   for (int s = 0; s < (int)plan.size(); s++) RET(launch_fused(c, plan[s], s, count));
@@ -869,7 +876,7 @@ int ensure_scratch(pgb_case *c) {
   CK(cudaMalloc(&c->d_hsp, sizeof(double) * ns * n));
   CK(cudaMalloc(&c->d_grads, sizeof(double) * 3 * ngrad * n));
   // the double flux writes its energy row twice: one row more per face
-  const int nf = ne + (c->phys.simulator == PGB_EULER_DF);
+  const int nf = ne + sim_df(c->phys.simulator);
   for (int a = 0; a < 3; a++) CK(cudaMalloc(&c->d_F[a], sizeof(double) * nf * n));
   CK(cudaMemsetAsync(c->d_tr, 0, sizeof(double) * (2 + ns) * n, c->stream));
   CK(cudaMemsetAsync(c->d_hsp, 0, sizeof(double) * ns * n, c->stream));
@@ -908,13 +915,13 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.met = c->d_met;
   pc.halo = c->d_halo;
   pc.nhalo = c->nhalo, pc.nhalo_l0 = c->nhalo_l0;
-  pc.visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  pc.visc = sim_visc(c->phys.simulator);
   pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
   pc.chem = c->phys.chemistry;
   pc.subopt = c->subopt;
   pc.subs = c->d_subs;
   pc.stiff = StiffList{c->d_stiffhead, c->d_stiffcells, c->interior_cells};
-  pc.df = c->phys.simulator == PGB_EULER_DF;
+  pc.df = sim_df(c->phys.simulator);
   pc.realgas = c->phys.eos == PGB_EOS_REALGAS || c->phys.eos == PGB_EOS_REALGAS_DF;
   pc.bchalo = c->d_bcface[0], pc.bcgrad = c->d_bcface[1], pc.bcwall = c->d_bcface[2];
   pc.nbchalo = c->nbcface[0], pc.nbcgrad = c->nbcface[1], pc.nbcwall = c->nbcface[2];
@@ -931,7 +938,7 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
 // (first 1; the reference's initialize graph,
 // peregrine/simulator/eulerdf/simulator.py:63-66)
 int prestep_plain(pgb_case *c, int qphys, int &count, int first) {
-  if (c->phys.simulator != PGB_EULER_DF) return PGB_OK;
+  if (!sim_df(c->phys.simulator)) return PGB_OK;
   RET(ensure_scratch(c));
   std::vector<BlockDev> hb;
   PlainCase pc = plain_case(c, hb);
@@ -945,7 +952,7 @@ int prestep_plain(pgb_case *c, int qphys, int &count, int first) {
 
 // the double flux's planes for a state just set
 int df_settle(pgb_case *c, int qphys) {
-  if (c->phys.simulator != PGB_EULER_DF || !c->df_fresh) return PGB_OK;
+  if (!sim_df(c->phys.simulator) || !c->df_fresh) return PGB_OK;
   int count = 0;
   return prestep_plain(c, qphys, count, 1);
 }
@@ -958,6 +965,7 @@ int rhs_plain(pgb_case *c, int qphys, int dqphys, int &count, double tfrac = 0.0
   pc.mark = mark_cb;
   pc.ctx = &mc;
   pc.tfrac = tfrac;
+  c->state_stale = false;
   return kPlain[c->phys.ns - 1].rhs(&pc, c->d_reg[qphys], c->d_reg[dqphys]);
 }
 
@@ -1014,7 +1022,7 @@ int step_plain(pgb_case *c, int &count) {
 int build_bcs(pgb_case *c) {
   std::vector<BcFace> t[3];
   long long n[3] = {0, 0, 0};
-  const bool visc = c->phys.simulator == PGB_NAVIER_STOKES;
+  const bool visc = sim_visc(c->phys.simulator);
   for (int b = 0; b < (int)c->blocks.size(); b++) {
     const HostBlock &B = c->blocks[b];
     const int ext[3] = {B.nx, B.ny, B.nz};
@@ -1120,24 +1128,23 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
   if (phys->nregs < 2 || phys->nregs > MAXREGS) return fail(PGB_ERR_ARG, "nregs out of range");
   if (phys->eos < PGB_EOS_CPG || phys->eos > PGB_EOS_REALGAS_DF)
     return fail(PGB_ERR_UNSUPPORTED, "no such eos");
-  if (phys->simulator < PGB_EULER || phys->simulator > PGB_EULER_DF) return fail(PGB_ERR_ARG, "no such simulator");
-  if ((phys->simulator == PGB_EULER_DF) != (phys->eos == PGB_EOS_REALGAS_DF))
-    return fail(PGB_ERR_ARG, "euler-df freezes the real gas's tangent plane: it takes real-gas-df, and that eos it");
-  if (phys->simulator == PGB_EULER_DF &&
-      (phys->primary != PGB_FLUX_KEPAEC || phys->recon != PGB_RECON_CONSTANT || phys->chemistry != PGB_CHEM_NONE))
-    return fail(PGB_ERR_UNSUPPORTED, "the double flux takes kepaec on the cells as they are, without chemistry");
+  if (phys->simulator < PGB_EULER || phys->simulator > PGB_NAVIER_STOKES_DF) return fail(PGB_ERR_ARG, "no such simulator");
+  if (sim_df(phys->simulator) != (phys->eos == PGB_EOS_REALGAS_DF))
+    return fail(PGB_ERR_ARG, "the double flux freezes the real gas's tangent plane: euler-df and navier-stokes-df take "
+                             "real-gas-df, and that eos one of them");
   if (phys->primary < PGB_FLUX_KEPAEC || phys->primary > PGB_FLUX_AUSMUP)
     return fail(PGB_ERR_ARG, "no such flux function");
+  // the double flux's flux functions (peregrine/simulator/eulerdf/kernels/flux/function/)
+  if (sim_df(phys->simulator) && (phys->primary == PGB_FLUX_HLLC || phys->chemistry != PGB_CHEM_NONE))
+    return fail(PGB_ERR_UNSUPPORTED, "the double flux takes kepaec, rusanov or ausmup, without chemistry");
   if (phys->recon != PGB_RECON_CONSTANT && phys->recon != PGB_RECON_MUSCL)
     return fail(PGB_ERR_ARG, "no such reconstruction");
   if (phys->recon == PGB_RECON_MUSCL && (phys->limiter < 1 || phys->limiter > 5))
     return fail(PGB_ERR_ARG, "muscl needs a limiter: koren, minmod, mc, superbee or vanleer");
   if (phys->primary == PGB_FLUX_KEPAEC && phys->recon != PGB_RECON_CONSTANT)
     return fail(PGB_ERR_UNSUPPORTED, "kepaec is a two-point flux of the cells as they are; it takes no muscl sides");
-  if (phys->simulator == PGB_NAVIER_STOKES && phys->trans != PGB_TRANS_CONSTANT && phys->trans != PGB_TRANS_KINETIC)
+  if (sim_visc(phys->simulator) && phys->trans != PGB_TRANS_CONSTANT && phys->trans != PGB_TRANS_KINETIC)
     return fail(PGB_ERR_UNSUPPORTED, "the viscous path takes constant or kinetic-theory transport");
-  if (phys->simulator == PGB_NAVIER_STOKES && (phys->eos == PGB_EOS_REALGAS || phys->eos == PGB_EOS_REALGAS_DF))
-    return fail(PGB_ERR_UNSUPPORTED, "the real gas runs inviscid in this build (euler, euler-df)");
   if (phys->trans == PGB_TRANS_KINETIC && phys->eos == PGB_EOS_CPG)
     return fail(PGB_ERR_ARG, "kinetic-theory transport needs the thermally perfect caloric");
   if (phys->chemistry < PGB_CHEM_NONE || phys->chemistry > PGB_CHEM_SUBSTEPPED)
@@ -1370,7 +1377,7 @@ int pgb_case_add_bc(pgb_case *c, int kind, const int *ops, const double *args, c
   if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
   if (kind < 1 || kind >= PGB_BC_NKINDS) return fail(PGB_ERR_ARG, "no such boundary kind");
   const bool ns_only = kind >= PGB_BC_NOSLIP_ADIA_WALL && kind <= PGB_BC_MOV_ISOT_WALL;
-  if (ns_only && c->phys.simulator != PGB_NAVIER_STOKES)
+  if (ns_only && !sim_visc(c->phys.simulator))
     return fail(PGB_ERR_ARG, "the no-slip and moving walls are the navier-stokes simulator's kinds");
   const int want = bc_head_values(kind) + (bc_is_inlet(kind) ? c->phys.ns - 1 : 0);
   if (nvalues != want) return fail(PGB_ERR_ARG, "the entry gives another number of values than its kind reads");
@@ -1414,7 +1421,7 @@ int pgb_case_set_face_bc(pgb_case *c, int blk, int nface, int bc) {
     return fail(PGB_ERR_ARG, "no such block face");
   if (bc < 0 || bc >= (int)c->bc_entries.size()) return fail(PGB_ERR_ARG, "no such boundary entry");
   if (c->blocks[blk].nbr[nface - 1] >= 0) return fail(PGB_ERR_ARG, "the face joins a neighbour; it is no boundary");
-  if (c->phys.simulator == PGB_EULER_DF)
+  if (sim_df(c->phys.simulator))
     return fail(PGB_ERR_UNSUPPORTED, "the double flux's boundaries are not built in this build");
   c->blocks[blk].bc[nface - 1] = bc;
   return PGB_OK;
@@ -1613,6 +1620,27 @@ int pgb_array_get_full(pgb_case *c, int blk, int reg, double *host, long count) 
   return PGB_OK;
 }
 
+// one field of a block's eos state over its full extents, F order: the
+// state the last right-hand side (or set_prims) formed, each cell's
+// (p, T, rhoinv, rho, e, cp, gamma, c), the real gas's Z, the double flux's
+// plane (theta, eps, kappa, zeta...) (the reference's state array,
+// peregrine/simulator/euler/simulator.py:66-90 reads p and T from it)
+int pgb_eos_get(pgb_case *c, int blk, int field, double *host, long count) {
+  if (!c || !host) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such block");
+  if (field < 0 || field >= SW) return fail(PGB_ERR_ARG, "no such state field");
+  const BlockDev &D = c->blocks[blk].dev;
+  if (count != (long)D.vol) return fail(PGB_ERR_ARG, "host array of the wrong size");
+  if (!c->d_state) return fail(PGB_ERR_STATE, "no state yet: set the primitives first");
+  if (c->state_stale) return fail(PGB_ERR_STATE, "the batched path forms the state in registers and keeps none");
+  RET(set_current(c));
+  CK(cudaMemcpyAsync(host, c->d_state + (size_t)SW * D.cv + (size_t)field * D.vol, sizeof(double) * count,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
 int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count) {
   RET(check_reg(c, blk, reg, count, c->ne));
   if (!host) return fail(PGB_ERR_ARG, "null host array");
@@ -1623,6 +1651,7 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
   std::vector<BlockDev> hb;
   const PlainCase pc = plain_case(c, hb);
   RET(kPlain[c->phys.ns - 1].fromprims(&pc, blk, c->d_prims, c->d_reg[c->phys_of[reg]]));
+  c->state_stale = false;
   // a halo cell's first Newton starts from the stored T of the cell it copies
   if (c->nhalo) k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_state, c->d_halo, c->nhalo, SW);
   c->df_fresh = true;
@@ -2119,7 +2148,7 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.met = p->d_met;
   pc.halo = p->d_halo;
   pc.nhalo = p->nhalo, pc.nhalo_l0 = p->nhalo_l0;
-  pc.visc = p->phys.simulator == PGB_NAVIER_STOKES;
+  pc.visc = sim_visc(p->phys.simulator);
   pc.primary = p->phys.primary, pc.recon = p->phys.recon, pc.limiter = p->phys.limiter;
   pc.chem = p->phys.chemistry == PGB_CHEM_COUPLED;
   pc.realgas = p->phys.eos == PGB_EOS_REALGAS || p->phys.eos == PGB_EOS_REALGAS_DF;
@@ -2164,7 +2193,7 @@ extern "C" {
 int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, pgb_pool **out) {
   if (!proto || !out) return fail(PGB_ERR_ARG, "null argument");
   if (!proto->finalized) return fail(PGB_ERR_STATE, "finalize the prototype case first");
-  if (proto->phys.simulator == PGB_EULER_DF) return fail(PGB_ERR_UNSUPPORTED, "the pool does not take the double flux");
+  if (sim_df(proto->phys.simulator)) return fail(PGB_ERR_UNSUPPORTED, "the pool does not take the double flux");
   if (proto->phys.chemistry == PGB_CHEM_SUBSTEPPED)
     return fail(PGB_ERR_UNSUPPORTED, "the pool takes the coupled chemistry, not the sub-stepped");
   if (max_cells < 64 || max_blocks < 1 || max_blocks > 65535)

@@ -301,8 +301,13 @@ __global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const dou
 // the advective face flux of a Riemann solver FN on the cells as they are
 // (lim 0; recon/constant.mako:3-18) or on MUSCL's sides under limiter lim
 // (recon/muscl.mako:15-51), both sides from the four cells LL, L, R, RR
-// along the axis (peregrine/simulator/euler/kernels/flux/single.mako:4-9)
-template <int NS, int A, int FN, bool RG = false>
+// along the axis (peregrine/simulator/euler/kernels/flux/single.mako:4-9).
+// DF: the double flux's form (Rusanov or AUSM+-up), the energy row written
+// again in each of the two cells' frozen planes, F[4] in the left's and
+// F[ne] in the right's, from each side's energy in that plane
+// (peregrine/simulator/eulerdf/kernels/flux/function/{rusanov,ausmup}.mako,
+// eside at peregrine/simulator/mixture/eos/realgasdf/kernels/eos.mako:73-83)
+template <int NS, int A, int FN, bool RG = false, bool DF = false>
 __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                           const double *__restrict__ stall, const double *__restrict__ met,
                           double *__restrict__ Fall, const int lim,
@@ -353,15 +358,58 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
     sl.u = lft(1), sl.v = lft(2), sl.w = lft(3);
     sr.u = rgt(1), sr.v = rgt(2), sr.w = rgt(3);
   }
-  double F[NE];
+  constexpr int NF = NE + (DF ? 1 : 0);
+  double F[NF];
   riemann<FN, NS>(sl, sr, YL, YR, S, F);
-  double *Fo = Fall + NE * B.cv + R;
+  if (DF) {
+    // eside: a side's total energy in plane q, theta p + rho (eps + the
+    // composition's zeta . Y + |u|^2 / 2) + kappa
+    auto eside = [&](const RSide &x, const double *Y, double *E) {
 #pragma unroll
-  for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
+      for (int q = 0; q < 2; q++) {
+        const long long P = q == 0 ? L : R;
+        double comp = 0.0;
+#pragma unroll
+        for (int n = 0; n < NS - 1; n++) comp += st[(ST_ZETA + n) * v + P] * Y[n];
+        E[q] = st[ST_THETA * v + P] * x.p +
+               x.rho * (st[ST_EPS * v + P] + comp + 0.5 * (x.u * x.u + x.v * x.v + x.w * x.w)) +
+               st[ST_KAPPA * v + P];
+      }
+    };
+    if (FN == FN_RUSANOV) {
+      // the plain Rusanov's UL, UR and lam, formed as it forms them
+      const double area = sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+      const double unL = (sl.u * S[0] + sl.v * S[1] + sl.w * S[2]) / area;
+      const double unR = (sr.u * S[0] + sr.v * S[1] + sr.w * S[2]) / area;
+      const double lam = fmax(fabs(unL) + sl.c, fabs(unR) + sr.c) * area;
+      const double UL = unL * area, UR = unR * area;
+      double EpL[2], EpR[2];
+      eside(sl, YL, EpL);
+      eside(sr, YR, EpR);
+#pragma unroll
+      for (int q = 0; q < 2; q++)
+        F[q == 0 ? 4 : NE] = 0.5 * (UR * (EpR[q] + sr.p) + UL * (EpL[q] + sl.p) - lam * (EpR[q] - EpL[q]));
+    } else {
+      // AUSM+-up: the mass flux F[0] from the upwind side U
+      const double mdot = F[0];
+      const bool left = mdot > 0.0;
+      const RSide &U = left ? sl : sr;
+      const double rhoinvU = 1.0 / U.rho;
+      double Ep[2];
+      eside(U, left ? YL : YR, Ep);
+#pragma unroll
+      for (int q = 0; q < 2; q++) F[q == 0 ? 4 : NE] = mdot * (Ep[q] + U.p) * rhoinvU;
+    }
+  }
+  double *Fo = Fall + NF * B.cv + R;
+#pragma unroll
+  for (int l = 0; l < NF; l++) Fo[l * v] = F[l];
 }
 
-// the diffusive face flux added to F (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:3-99)
-template <int NS, int A>
+// the diffusive face flux added to F (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:3-99);
+// DF: the double flux's faces carry the energy row twice, and the diffusive
+// energy flux adds to both (peregrine/simulator/navstokesdf/kernels/flux/alpha-damping.mako:1-9)
+template <int NS, int A, bool DF = false>
 __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                            const double *__restrict__ stall, const double *__restrict__ trall,
                            const double *__restrict__ hall, const double *__restrict__ gall,
@@ -396,7 +444,7 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
   const double uL = Q[1 * v + L] * rhoinvL, vL = Q[2 * v + L] * rhoinvL, wL = Q[3 * v + L] * rhoinvL;
   const double uR = Q[1 * v + R] * rhoinvR, vR = Q[2 * v + R] * rhoinvR, wR = Q[3 * v + R] * rhoinvR;
   double F[NE];
-  double *Fo = Fall + NE * B.cv + R;
+  double *Fo = Fall + (NE + (DF ? 1 : 0)) * B.cv + R;
 #pragma unroll
   for (int l = 0; l < NE; l++) F[l] = Fo[l * v];
   double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
@@ -456,6 +504,7 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
   F[4] += f4;
 #pragma unroll
   for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
+  if (DF) Fo[NE * v] += f4;
 }
 
 // dQ = (low faces - high faces) detJinv (peregrine/simulator/advec/kernels/applyflux.mako:2-11)

@@ -83,13 +83,26 @@ void riemann_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const Rh
   }
 }
 
+// the double flux's Riemann forms (Rusanov, AUSM+-up; the case refuses HLLC)
+template <int A>
+void riemann_df_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const RhsArgs &a, int lim) {
+  cudaStream_t s = pc->stream;
+  if (pc->primary == PGB_FLUX_RUSANOV)
+    k_riemann<NS, A, FN_RUSANOV, true, true><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct);
+  else
+    k_riemann<NS, A, FN_AUSMUP, true, true><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], lim, ct);
+}
+
 template <int A>
 void adv_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
   const int lim = pc->recon == PGB_RECON_MUSCL ? pc->limiter : 0;
   cudaStream_t s = pc->stream;
   if (pc->df) {
-    k_advflux_df<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
+    if (pc->primary == PGB_FLUX_KEPAEC)
+      k_advflux_df<NS, A><<<g, TH, 0, s>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->F[A], ct);
+    else
+      riemann_df_launch<A>(pc, b, g, ct, a, lim);
     return;
   }
   if (pc->primary == PGB_FLUX_KEPAEC) {
@@ -104,7 +117,10 @@ void adv_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *
 template <int A>
 void diff_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_diffflux<NS, A><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A], ct);
+  if (pc->df)
+    k_diffflux<NS, A, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A], ct);
+  else
+    k_diffflux<NS, A><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A], ct);
 }
 
 void fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libpgb200.so")
 
 OK, ERR_ARG, ERR_STATE, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
-EULER, NAVIER_STOKES, EULER_DF = 0, 1, 2
+EULER, NAVIER_STOKES, EULER_DF, NAVIER_STOKES_DF = 0, 1, 2, 3
 EOS_CPG, EOS_TPG, EOS_REALGAS, EOS_REALGAS_DF = 0, 1, 2, 3
 FLUX_KEPAEC, FLUX_HLLC, FLUX_RUSANOV, FLUX_AUSMUP = 0, 1, 2, 3
 RECON_CONSTANT, RECON_MUSCL = 0, 1
@@ -214,6 +214,7 @@ SIGNATURES = {
     "pgb_array_set": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_array_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_array_get_full": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
+    "pgb_eos_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_set_prims": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_rhs": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_step": ([ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),

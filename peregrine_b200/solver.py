@@ -18,6 +18,7 @@ from peregrine_b200 import native
 from peregrine_b200.config import ConfigError
 from peregrine_b200.grid import metrics as make_metrics
 from peregrine_b200.integrators import Integrator, stage_records
+from peregrine_b200.iovars import Simulator
 from peregrine_b200.mixture import Mixture
 
 NG = 2
@@ -104,6 +105,7 @@ class Solver:
         # every bcvals entry, checked whether or not a face names it
         self.bcs = bcmod.entries(cfg["bcvals"], sim["simulator"], self.mixture.spnames)
         self.ne = 4 + self.ns
+        self.sim = Simulator(self)
         self.integrator = cfg["time-integration"]["integrator"]
         self.integ = Integrator(cfg)
         records, nregs = stage_records(self.integrator)
@@ -116,7 +118,8 @@ class Solver:
         adv = cfg["adv-flux"]
         phys = native.Physics()
         phys.simulator = {"euler": native.EULER, "navier-stokes": native.NAVIER_STOKES,
-                          "euler-df": native.EULER_DF}[sim["simulator"]]
+                          "euler-df": native.EULER_DF,
+                          "navier-stokes-df": native.NAVIER_STOKES_DF}[sim["simulator"]]
         phys.eos = {"cpg": native.EOS_CPG, "tpg": native.EOS_TPG, "real-gas": native.EOS_REALGAS,
                     "real-gas-df": native.EOS_REALGAS_DF}[cfg["mixture"]["eos"]]
         phys.primary = {"kepaec": native.FLUX_KEPAEC, "hllc": native.FLUX_HLLC, "rusanov": native.FLUX_RUSANOV,

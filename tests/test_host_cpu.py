@@ -56,6 +56,32 @@ def test_config_refuses_unknown_keys_and_bad_choices():
     assert cfg["simulation"]["dt"] == 1e-7
 
 
+def double_flux(simulator="navier-stokes-df", eos="real-gas-df", primary="rusanov", **more):
+    given = {"simulation": {"simulator": simulator},
+             "mixture": {"species": "o2_h2_pr", "eos": eos, "trans": "kinetic-theory"},
+             "adv-flux": {"primary": primary, **more}}
+    return Config.from_dict(given)
+
+
+def test_the_double_flux_takes_its_eos_and_its_flux_functions():
+    # peregrine/simulator/eulerdf/simulator.py:15-20 and eulerdf/kernels/flux/function/
+    assert double_flux()["simulation"]["simulator"] == "navier-stokes-df"
+    assert double_flux(primary="ausmup", recon="muscl", limiter="koren")
+    for bad in (dict(eos="real-gas"), dict(simulator="navier-stokes"), dict(primary="hllc")):
+        with pytest.raises(ConfigError):
+            double_flux(**bad)
+    # the library refuses the same before it touches a device
+    phys = native.Physics()
+    phys.simulator, phys.eos, phys.ns, phys.nregs = native.NAVIER_STOKES_DF, native.EOS_REALGAS_DF, 2, 3
+    phys.primary, phys.trans = native.FLUX_HLLC, native.TRANS_KINETIC
+    handle = ctypes.c_void_p()
+    with pytest.raises(native.PgbUnsupported):
+        native.call("pgb_case_create", ctypes.byref(phys), ctypes.byref(handle))
+    phys.primary, phys.eos = native.FLUX_RUSANOV, native.EOS_REALGAS
+    with pytest.raises(native.PgbArgumentError):
+        native.call("pgb_case_create", ctypes.byref(phys), ctypes.byref(handle))
+
+
 def test_uneven_cuts_are_seeded_and_bounded():
     for seed in range(5):
         cuts = uneven_cuts(128, 3, 30, 56, np.random.default_rng(seed))
