@@ -196,7 +196,22 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
     const int sJ = B.X, sK = B.X * B.Y;
     const double *Q = a.R[a.qin] + 5 * B.cv;
     const bool col = tid < N1;
-    const int ii = tid % W1, jj = tid / W1;
+    // the columns in warp order: the tile's first, then the ring's high edges
+    // (the i-faces of its last column and the j-faces of its top row are the
+    // tile's), then the rest of the ring, which has no face the tile needs,
+    // so whole warps of it skip the face pass
+    int ii = 0, jj = 0;
+    {
+      int q = tid;
+      if (q < tw * th) ii = q % tw + 1, jj = q / tw + 1;
+      else if ((q -= tw * th) < th) ii = tw + 1, jj = q + 1;
+      else if ((q -= th) < tw) ii = q + 1, jj = th + 1;
+      else if ((q -= tw) < th) ii = 0, jj = q + 1;
+      else if ((q -= th) < tw) ii = q + 1, jj = 0;
+      else if ((q -= tw) < 4) ii = (q & 1) ? tw + 1 : 0, jj = (q & 2) ? th + 1 : 0;
+    }
+    const bool needi = col && jj >= 1 && jj <= th && ii >= 1;
+    const bool needj = col && ii >= 1 && ii <= tw && jj >= 1;
     const int c1 = ii + LW1 * jj;
     const int c2 = (ii + 1) + LW2 * (jj + 1);
     const bool tile = col && ii >= 1 && ii <= tw && jj >= 1 && jj <= th;
@@ -343,9 +358,10 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
       if (k + 2 < k1) fetch_pre(k + 2);
       cp_commit();
       // 1. this column's low i and j faces at plane k, both in one straight
-      //    run so their arithmetic interleaves; a column with no such face
-      //    (the ring) computes one from its neighbour anyway and drops it
-      if (col) {
+      //    run so their arithmetic interleaves; a ring column on the tile's
+      //    high edges computes both and keeps the one the tile needs, the
+      //    rest of the ring (whole warps of it) none
+      if (needi || needj) {
         const int li = ii >= 1 ? 1 : 0, lj = jj >= 1 ? LW1 : 0;
         const int li2 = ii >= 1 ? 1 : 0, lj2 = jj >= 1 ? LW2 : 0;
         double Fa[5], Fb[5], gli[12], glj[12], gr[12];
@@ -357,11 +373,11 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
         const CellP me = getP(s0, c2);
         face_u<0, VISC>(B, getP(s0, c2 - li2), me, gli, gr, Fa);
         face_u<1, VISC>(B, getP(s0, c2 - lj2), me, glj, gr, Fb);
-        if (jj >= 1 && jj <= th && ii >= 1) {
+        if (needi) {
 #pragma unroll
           for (int l = 0; l < 5; l++) Fi[l * LN1 + c1] = Fa[l];
         }
-        if (ii >= 1 && ii <= tw && jj >= 1) {
+        if (needj) {
 #pragma unroll
           for (int l = 0; l < 5; l++) Fj[l * LN1 + c1] = Fb[l];
         }

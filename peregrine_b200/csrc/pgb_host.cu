@@ -14,6 +14,7 @@
 
 #include "fused.cuh"
 #include "fused2.cuh"
+#include "fused3.cuh"
 #include "layout.cuh"
 #include "physics.cuh"
 #include "plain.cuh"
@@ -452,8 +453,15 @@ struct V2Inst {
   V2Inst{NT, MB, TW, TH, (const void *)k_fused2<true, NT, MB, TW, TH>,                             \
          (const void *)k_fused2<false, NT, MB, TW, TH>, fused2_smem<NT, TW, TH>(true),             \
          fused2_smem<NT, TW, TH>(false)}
-const V2Inst kV2[] = {PGB_V2(256, 1, 24, 7), PGB_V2(256, 1, 30, 6), PGB_V2(128, 2, 14, 6)};
+// the warp-specialised form: sixteen warps of 128 registers
+#define PGB_V3(NT, MB, TW, TH)                                                                    \
+  V2Inst{NT, MB, TW, TH, (const void *)k_fused3<true, NT, MB, TW, TH>,                             \
+         (const void *)k_fused3<false, NT, MB, TW, TH>, fused3_smem<NT, TW, TH>(true),             \
+         fused3_smem<NT, TW, TH>(false)}
+const V2Inst kV2[] = {PGB_V2(256, 1, 24, 7), PGB_V2(256, 1, 30, 6), PGB_V2(128, 2, 14, 6), PGB_V3(512, 1, 14, 8),
+                      PGB_V3(512, 1, 16, 7)};
 #undef PGB_V2
+#undef PGB_V3
 constexpr int kNV2 = sizeof(kV2) / sizeof(kV2[0]);
 
 // the uniform kernel's default tile: i and j cut evenly in pieces the layout holds

@@ -118,6 +118,33 @@ def test_batched_euler_and_ns_on_both_kernels(simulator):
             assert rowmax_err(b.Q.get()[b.mesh.interior], w[b.mesh.interior]) < STATE_TOL
 
 
+@pytest.mark.parametrize("shape", range(6))
+@pytest.mark.parametrize("simulator,integrator", [("navier-stokes", "rk4"), ("euler", "tvd-rk3"),
+                                                  ("navier-stokes", "tvd-rk3")])
+def test_every_uniform_kernel_shape_matches_the_oracle(shape, simulator, integrator):
+    # each launch shape the library has, on ragged tiles (blocks of uneven
+    # widths) and several k runs a block, two steps against the oracle
+    from peregrine_b200 import autotune
+
+    shapes = autotune.shapes()
+    if shape >= len(shapes):
+        pytest.skip("the library has fewer shapes")
+    threads, minb, width, _ = shapes[shape]
+    mb, orc = build(simulator, integrator, cells=24, blocks=(2, 1, 2), low=9, high=15)
+    mb.step(1e-6)
+    orc.step(1e-6)
+    assert all(mb.uniform(n) for n in range(len(mb.blocks)))
+    native.call("pgb_set_fused_shape", mb.case, threads, minb, width)
+    for n, (tw, th, kc) in enumerate(autotune._tiles(mb, threads, 3)):
+        mb.set_tile(n, tw, th, kc)
+    dt = 2e-5
+    mb.step(dt, 2)
+    orc.step(dt)
+    orc.step(dt)
+    for b, w in zip(mb.blocks, orc.regs[0]):
+        assert rowmax_err(b.Q.get()[b.mesh.interior], w[b.mesh.interior]) < STATE_TOL
+
+
 def test_unsupported_physics_is_refused():
     import peregrine_b200 as pg
 
