@@ -523,6 +523,10 @@ class Oracle:
     def rhs(self, Q, dQ, faces=False, diffusive_only=False, t=None):
         """dQ of every block from Q; with faces, each block's [iF, jF, kF] too.
         t: the time the boundary values read (the oracle's clock if None)."""
+        # the double flux's first freeze before this pass's boundary rows are
+        # set: the freeze sets (and lets go of) its own
+        if self.df and self.df_fresh:
+            self.prestep(Q)
         obs = self._oblocks(Q)
         bcs, keep = self._bcs(self.tme if t is None else t)
         self.case.nbc, self.case.bc = len(self.bcfaces), bcs
@@ -530,8 +534,6 @@ class Oracle:
         m = np.ascontiguousarray(self.map)
         ptrs = (ctypes.POINTER(ctypes.c_double) * len(dQ))(*[_ptr(d) for d in dQ])
         fl, fptr = None, None
-        if self.df and self.df_fresh:
-            self.prestep(Q)
         if faces:
             fl = []
             nf = self.ne + (1 if self.df else 0)
@@ -595,6 +597,9 @@ class Oracle:
         state was set, off the frozen planes at every step's start."""
         obs = self._oblocks(Q)
         m = np.ascontiguousarray(self.map)
+        # the boundaries' halo cells at the step's start, frozen with the rest
+        bcs, keep = self._bcs(self.tme)
+        self.case.nbc, self.case.bc = len(self.bcfaces), bcs
         self.lib.oracle_prestep(ctypes.byref(self.case), obs, len(self.blocks), m.ctypes.data_as(ctypes.c_void_p),
                                 ctypes.c_long(m.size), int(self.df_fresh))
         self.df_fresh = False

@@ -1808,6 +1808,9 @@ void bc_wallflux(const OCase &c, const OBlock &B, const std::vector<double> &sta
         work += wall[e] * tS;
       }
       Fo[4] += work - kappa * outward * (dT) / dn * Sabs;
+      // the double flux's second energy row: nothing is advected through a
+      // wall, so it is the first's (simulator/navstokesdf/kernels/bcs/*-wall.mako)
+      if (nf > ne) Fo[ne] = Fo[4];
     }
 }
 
@@ -2156,6 +2159,24 @@ int oracle_prestep(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntr
     std::memcpy(D.Q + dt * ne, S.Q + st * ne, sizeof(double) * ne);
     std::memcpy(D.pst + dt * NSTATE, S.pst + st * NSTATE, sizeof(double) * NSTATE);
     D.Tg[dt] = S.Tg[st];
+  }
+  // the boundaries' halo cells from the state just formed, then frozen like
+  // every other cell (simulator/eulerdf/simulator.py:58-66 freezes "all")
+  for (int m = 0; m < c.nbc; m++) {
+    const OBc &bc = c.bc[m];
+    OBlock &B = blocks[bc.blk];
+    const Dims d = cells(B);
+    const long N = (long)d.X * d.Y * d.Z;
+    std::vector<double> state(B.pst, B.pst + N * NSTATE);
+    bc_halo(c, B, state, bc);
+    std::memcpy(B.pst, state.data(), sizeof(double) * N * NSTATE);
+    const BFace w(B, bc.nface);
+    for (int l = 0; l < B.ng; l++)
+      for (int p = 0; p < w.n[w.a1]; p++)
+        for (int q = 0; q < w.n[w.a2]; q++) {
+          const long ch = w.at(d, p, q, w.halo(l));
+          freeze(c, B.Q + ch * ne, B.pst + ch * NSTATE);
+        }
   }
   return 0;
 }

@@ -283,7 +283,9 @@ def bc_box_config(kind, ns=1, simulator="euler", primary="kepaec", recon="consta
     else:
         cfg["mixture"]["species"] = {k: MIXED[k] for k in list(MIXED)[:ns]}
     cfg["mixture"]["eos"] = eos
-    cfg["mixture"]["trans"] = "constant" if simulator == "navier-stokes" else None
+    # the real gases' stored tables carry the kinetic-theory fits
+    viscous = simulator.startswith("navier-stokes")
+    cfg["mixture"]["trans"] = ("kinetic-theory" if tables is not None else "constant") if viscous else None
     cfg["time-integration"]["integrator"] = integrator
     cfg["adv-flux"]["primary"] = primary
     cfg["adv-flux"]["recon"] = recon

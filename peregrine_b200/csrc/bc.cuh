@@ -385,12 +385,34 @@ __global__ void k_bc_halo(const BlockDev *__restrict__ blks, const BcFace *__res
   if (copy) {
     const double *sm = sb + cm;
 #pragma unroll
-    for (int q = 0; q <= ST_Z; q++) so[q * v] = sm[q * v];
+    // the whole record, the double flux's plane with it (the reference's
+    // statehalo.copy, every field of the state array)
+#pragma unroll
+    for (int q = 0; q < ST_ZETA + NS - 1; q++) so[q * v] = sm[q * v];
   } else {
     so[0 * v] = th.p, so[1 * v] = th.T, so[2 * v] = th.rhoinv, so[3 * v] = th.rho;
     so[4 * v] = th.e, so[5 * v] = th.cp, so[6 * v] = th.gamma, so[7 * v] = th.c;
     so[ST_Z * v] = Z;
   }
+}
+
+// the double flux's freeze of the boundaries' halo cells, once the halo pass
+// has set them at a step's start: a halo cell carries the plane of its own
+// state, as the reference's freeze over every cell gives it
+// (peregrine/simulator/eulerdf/simulator.py:58-66)
+template <int NS>
+__global__ void k_bc_freeze(const BlockDev *__restrict__ blks, const BcFace *__restrict__ faces, int nfaces,
+                            double *__restrict__ Qall, double *__restrict__ stall) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= faces[nfaces].start) return;
+  const int f = bc_face_of(faces, nfaces, t);
+  const BcFace F = faces[f];
+  const BlockDev &B = blks[F.blk];
+  const long long plane = bc_plane(B, F.face), local = t - F.start;
+  const int layer = (int)(local / plane);
+  const BcAt w = bc_at(B, F.face, local % plane);
+  const long long ch = w.halo(B, layer);
+  freeze_cell<NS>(Qall + (4 + NS) * B.cv + ch, stall + SW * B.cv + ch, B.vol);
 }
 
 // postgrads of the inflows and outflows: each halo cell's gradients its
@@ -502,6 +524,9 @@ __global__ void k_bc_wall(const BlockDev *__restrict__ blks, const BcFace *__res
     }
     Fo[4] += work - kappa * outward * dT / dn * Sabs;
   }
+  // the double flux's second energy row: nothing is advected through a wall,
+  // so it is the first's (peregrine/simulator/navstokesdf/kernels/bcs/*-wall.mako)
+  if (nf > NE) Fo[NE] = Fo[4];
   double *Fa = (w.a == 0 ? Fi : w.a == 1 ? Fj : Fk) + (long long)nf * B.cv + fc;
   for (int l = 0; l < nf; l++) Fa[l * v] = Fo[l];
 }

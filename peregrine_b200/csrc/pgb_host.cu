@@ -1429,8 +1429,6 @@ int pgb_case_set_face_bc(pgb_case *c, int blk, int nface, int bc) {
     return fail(PGB_ERR_ARG, "no such block face");
   if (bc < 0 || bc >= (int)c->bc_entries.size()) return fail(PGB_ERR_ARG, "no such boundary entry");
   if (c->blocks[blk].nbr[nface - 1] >= 0) return fail(PGB_ERR_ARG, "the face joins a neighbour; it is no boundary");
-  if (sim_df(c->phys.simulator))
-    return fail(PGB_ERR_UNSUPPORTED, "the double flux's boundaries are not built in this build");
   c->blocks[blk].bc[nface - 1] = bc;
   return PGB_OK;
 }

@@ -74,18 +74,12 @@ __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *
   st[4 * v] = s.e, st[5 * v] = s.cp, st[6 * v] = s.gamma, st[7 * v] = s.c;
 }
 
-// the double flux's freeze, on the interior: the energy reset to the eos's,
-// and the tangent plane of rho e at the cell's state, rho e = theta p + eps rho
-// + sum zeta_n rho Y_n + kappa (peregrine/simulator/eulerdf/kernels/freeze.mako:3-32)
+// the double flux's freeze of one cell (Q and its state record, component
+// stride v): the energy reset to the eos's, and the tangent plane of rho e
+// at the cell's state, rho e = theta p + eps rho + sum zeta_n rho Y_n + kappa
+// (peregrine/simulator/eulerdf/kernels/freeze.mako:3-32)
 template <int NS>
-__global__ void k_freeze(const BlockDev *__restrict__ blks, int b, double *__restrict__ Qall,
-                         double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr) {
-  PGB_WHERE(B, t);
-  if (t >= (long long)B.nx * B.ny * B.nz) return;
-  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
-  const long long c = cell_index(B, i, j, k), v = B.vol;
-  double *Q = Qall + (4 + NS) * B.cv + c;
-  double *st = stall + SW * B.cv + c;
+__device__ __forceinline__ void freeze_cell(double *Q, double *st, const long long v) {
   const double rho = Q[0], rhoinv = 1.0 / rho;
   const double p = st[0], T = st[1 * v], e = st[4 * v];
   const double rhoe = rho * e;
@@ -110,6 +104,17 @@ __global__ void k_freeze(const BlockDev *__restrict__ blks, int b, double *__res
   st[ST_EPS * v] = epsY - zetaY;
   st[ST_KAPPA * v] = rhoe - epsY * rho - theta * p;
   (void)rho_p;
+}
+
+// the freeze on the interior
+template <int NS>
+__global__ void k_freeze(const BlockDev *__restrict__ blks, int b, double *__restrict__ Qall,
+                         double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr) {
+  PGB_WHERE(B, t);
+  if (t >= (long long)B.nx * B.ny * B.nz) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k);
+  freeze_cell<NS>(Qall + (4 + NS) * B.cv + c, stall + SW * B.cv + c, B.vol);
 }
 
 __device__ __forceinline__ State load_state(const double *st, long long v) {

@@ -387,6 +387,12 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
   mark(pc, 0);
   k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(pc->state, pc->halo, pc->nhalo, SW);
   mark(pc, 0);
+  // the boundaries' halo cells from the state just formed, then their planes
+  if (pc->nbchalo) {
+    bc_halo_launch(pc, Q);
+    k_bc_freeze<NS><<<grid_of(pc->bchalo_n), TH, 0, s>>>(pc->d_blks, pc->bchalo, pc->nbchalo, Q, pc->state);
+    mark(pc, 4);
+  }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "double-flux freeze");
 }

@@ -6,7 +6,10 @@ cells, keeps its pressure to 1e-9 under the double flux's Rusanov and
 AUSM+-up, on the cells as they are and on MUSCL's Koren sides, where the
 plain fluxes scatter it; mass and species are kept to 1e-12.  Under
 navier-stokes-df a diffusing layer at rest keeps the plain simulator's
-temperature within 0.1 K and its pressure within 1e-4 of P0.
+temperature within 0.1 K and its pressure within 1e-4 of P0.  Behind
+isothermal no-slip walls the double flux heats a box at rest as the plain
+simulator does (dQ's energy row to 1e-12), both sides alike, and a hot box
+against cold walls stays finite and cools.
 
 The reference walls its line's one-cell-thick cross-section with slip walls;
 a flow along the line alone sees the same halo cells through a periodic
@@ -125,3 +128,43 @@ def test_a_diffusing_layer_keeps_its_temperature():
     assert np.abs(T - Tplain).max() < 0.1
     assert np.abs(p - pplain).max() / P0 < 1e-4
     assert abs(drift) < 1e-4
+
+
+def heated(simulator, Tbox=300.0, Twall=400.0, steps=0):
+    """A closed box of CH4/O2 at rest behind isothermal no-slip walls
+    (tests/doubleflux/test_doubleflux.py:268-288): dQ's energy row on the
+    first and last layer along each axis after steps."""
+    t = load_tables("ch4_o2_srk")
+    mesh = CubeMesher(cells=[[5], [4], [3]], lengths=[2.5e-4, 2e-4, 1.5e-4], defaultbc="walls")
+    blocks = mesh.make_blocks(2)
+    mets = [make_metrics(b.nodes, 2) for b in blocks]
+    df = simulator.endswith("-df")
+    orc = Oracle(t, 2, simulator, blocks, mets, "tvd-rk3", eos="real-gas-df" if df else "real-gas",
+                 trans="kinetic-theory", bcvals={"walls": {"kind": "no-slp-isot-wall", "T": Twall}},
+                 species=[str(n) for n in t["spnames"]])
+    q = np.zeros((9, 8, 7, 6))
+    q[..., 0], q[..., 4], q[..., 5] = P0, Tbox, 0.5
+    orc.set_prims([q])
+    inner = blocks[0].interior
+    dt = 0.3 * 5e-5 / sound(orc, np.ascontiguousarray(orc.regs[0][0][inner].reshape(-1, 6))).max()
+    for _ in range(steps):
+        orc.step(dt)
+    dQ = [np.zeros_like(orc.regs[0][0])]
+    orc.rhs(orc.regs[0], dQ)
+    e = dQ[0][inner][..., 4]
+    return [(np.take(e, 0, axis=a), np.take(e, -1, axis=a)) for a in range(3)]
+
+
+def test_a_wall_heats_both_sides_of_the_box_alike():
+    plain, df = heated("navier-stokes"), heated("navier-stokes-df")
+    for (low, high), (lowdf, highdf) in zip(plain, df):
+        assert np.allclose(lowdf, low, rtol=1e-12)
+        assert np.allclose(highdf, high, rtol=1e-12)
+        assert np.allclose(lowdf.mean(), highdf.mean(), rtol=1e-12)
+
+
+def test_a_hot_box_against_cold_walls_stays_finite():
+    # a mirrored halo at 2 Twall - Tbox would have no real-gas state; the halo holds the wall's own
+    for low, high in heated("navier-stokes-df", Tbox=1400.0, Twall=300.0, steps=30):
+        assert np.isfinite(low).all() and np.isfinite(high).all()
+        assert (low < 0.0).all() and (high < 0.0).all()
