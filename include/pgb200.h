@@ -243,6 +243,18 @@ int pgb_case_add_bc(pgb_case *c, int kind, const int *ops, const double *args, c
  * interface named in bcvals (peregrine/multiblock/solver.py:157-173).  A
  * boundary face given no entry keeps its halo as set.  Before finalize. */
 int pgb_case_set_face_bc(pgb_case *c, int blk, int nface, int bc);
+/* A face joined to a neighbour by any of the 24 orientations: orient holds
+ * the reference's three digits, for each axis of blk the neighbour's axis it
+ * runs along, 1-3 forward and 4-6 backward (the neighbour's face follows from
+ * the digit of the face's own axis); rot, when not null, the 3 x 3 rotation
+ * (row major) a rotationally periodic face turns the vectors arriving in its
+ * halo by (peregrine/multiblock/interface/base.py:6-160,
+ * peregrine/multiblock/collections/exchange/kernels/place.mako:3-36) */
+int pgb_case_connect_oriented(pgb_case *c, int blk, int nface, int nbr, const char *orient, const double *rot);
+/* register reg's halo filled from the blocks across every interface, the
+ * vectors of a rotationally periodic face turned (the reference's exchange
+ * of a bank, peregrine/multiblock/collections/exchange/collection.py) */
+int pgb_exchange(pgb_case *c, int reg);
 /* the case's clock, the t boundary values read at a step's start
  * (peregrine/multiblock/solver.py:35, 355-364); a step moves it on by dt */
 int pgb_set_time(pgb_case *c, double t);

@@ -24,7 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
-_halo_dtype = np.dtype([(n, np.int32) for n in ("dblk", "di", "dj", "dk", "sblk", "si", "sj", "sk", "layer")])
+_halo_dtype = np.dtype([(n, np.int32) for n in ("dblk", "di", "dj", "dk", "sblk", "si", "sj", "sk", "layer", "rot")])
 
 
 class OBc(ctypes.Structure):
@@ -51,7 +51,8 @@ class OCase(ctypes.Structure):
                 ("cppoly", ctypes.POINTER(ctypes.c_double)), ("MW", ctypes.POINTER(ctypes.c_double)),
                 ("cfloor", ctypes.c_double), ("binary", ctypes.c_int), ("bwidth", ctypes.c_int),
                 ("nfit", ctypes.c_int), ("bpartial", ctypes.c_int), ("pairfit", ctypes.POINTER(ctypes.c_double)),
-                ("selffit", ctypes.POINTER(ctypes.c_double)), ("bath", ctypes.POINTER(ctypes.c_int))]
+                ("selffit", ctypes.POINTER(ctypes.c_double)), ("bath", ctypes.POINTER(ctypes.c_int)),
+                ("rots", ctypes.POINTER(ctypes.c_double))]
 
 # the boundary kinds (peregrine/simulator/euler/bcs.py, navstokes/bcs.py): the
 # oracle's number for each and the variables an entry gives, in order; the
@@ -213,7 +214,8 @@ def _lib():
     lib.oracle_advective_faces.restype = ctypes.c_int
     for name in ("oracle_production", "oracle_gibbs", "oracle_tlog", "oracle_texp", "oracle_mathtables",
                  "oracle_species_cph", "oracle_fromQ", "oracle_prestep", "oracle_realgas_frompT",
-                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads", "oracle_cflmax", "oracle_transport"):
+                 "oracle_realgas_fromQ", "oracle_freeze", "oracle_bc_grads", "oracle_cflmax", "oracle_transport",
+                 "oracle_exchange"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 
@@ -223,11 +225,14 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def halo_map(blocks):
+def halo_map(blocks, rots=None):
     """Every face-halo cell of every block and the neighbour cell it copies.
 
-    Identity orientation ("123"), which is what the lattice meshers make: a low
-    face's halo layer l is the neighbour's l-th cell in from its high face.
+    A face's halo layer l is the neighbour's l-th cell in from the face it
+    meets, the neighbour's cells laid out along this block's axes by the
+    face's orientation digits (peregrine/multiblock/interface/base.py:96-160).
+    rots, a list, gathers the rotational periodics' rotations: an entry's rot
+    is 1 + its index there, 0 for none.
     """
     rows = []
     for blk in blocks:
@@ -238,26 +243,34 @@ def halo_map(blocks):
                 continue
             a = face.axis
             nbr = blocks[face.nbr]
-            m = nbr.cells
+            # the neighbour's own cell indices, halo included (as wide on every
+            # side), laid out along this block's axes
+            idx = np.stack(np.meshgrid(*[np.arange(c + 2 * g) for c in nbr.cells], indexing="ij"), axis=-1)
+            view = face.inframe(idx)
+            assert all(view.shape[d] == n[d] + 2 * g for d in range(3) if d != a), "the faces do not match"
+            rot = 0
+            if getattr(face, "rotperiodic", False) and rots is not None:
+                rots.append(np.asarray(face.rot, np.float64))
+                rot = len(rots)
             other = [d for d in range(3) if d != a]
             grid = np.meshgrid(*[np.arange(g, g + n[d]) for d in other], indexing="ij")
             for layer in range(g):
                 dst = [None] * 3
-                src = [None] * 3
                 for d, gd in zip(other, grid):
                     dst[d] = gd.ravel()
-                    src[d] = gd.ravel()
                 cnt = dst[other[0]].size
+                sel = [slice(g, g + n[d]) for d in range(3)]
                 if face.is_low:
                     dst[a] = np.full(cnt, g - 1 - layer)
-                    src[a] = np.full(cnt, g + m[a] - 1 - layer)
+                    sel[a] = view.shape[a] - g - 1 - layer
                 else:
                     dst[a] = np.full(cnt, g + n[a] + layer)
-                    src[a] = np.full(cnt, g + layer)
+                    sel[a] = g + layer
+                src = view[tuple(sel)].reshape(-1, 3)
                 r = np.zeros(cnt, _halo_dtype)
-                r["dblk"], r["sblk"], r["layer"] = blk.nblki, face.nbr, layer
+                r["dblk"], r["sblk"], r["layer"], r["rot"] = blk.nblki, face.nbr, layer, rot
                 r["di"], r["dj"], r["dk"] = dst
-                r["si"], r["sj"], r["sk"] = src
+                r["si"], r["sj"], r["sk"] = src[:, 0], src[:, 1], src[:, 2]
                 rows.append(r)
     return np.concatenate(rows) if rows else np.zeros(0, _halo_dtype)
 
@@ -410,7 +423,11 @@ class Oracle:
         # one thread below SMALL cells in all (a test's case), every core above
         cells = sum(int(np.prod([n + 2 * b.ng for n in b.cells])) for b in blocks)
         self.threads = 1 if cells < SMALL else (os.cpu_count() or 1)
-        self.map = halo_map(blocks)
+        self._rots = []
+        self.map = halo_map(blocks, self._rots)
+        if self._rots:
+            self._tables["rots"] = np.ascontiguousarray(np.stack(self._rots), dtype=np.float64)
+            c.rots = _ptr(self._tables["rots"])
         self.nregs = NREGS[integrator]
         self.regs = [[np.zeros(self._shape(b)) for b in blocks] for _ in range(self.nregs)]
         # each cell's last temperature, the iterative eos's starting guess
@@ -591,6 +608,15 @@ class Oracle:
         F = np.zeros_like(QL)
         self.lib.oracle_kepaec_faces(ctypes.byref(self.case), ctypes.c_long(QL.shape[0]), _ptr(QL), _ptr(QR), _ptr(S), _ptr(F))
         return F
+
+    def exchange(self, Q=None):
+        """Register Q's halo filled across every interface, a rotational
+        periodic's vectors turned (the reference's exchange of a bank)."""
+        Q = self.regs[0] if Q is None else Q
+        obs = self._oblocks(Q)
+        m = np.ascontiguousarray(self.map)
+        self.lib.oracle_exchange(ctypes.byref(self.case), obs, len(self.blocks), m.ctypes.data_as(ctypes.c_void_p),
+                                 ctypes.c_long(m.size))
 
     def prestep(self, Q):
         """The double flux's freeze on register Q: off the eos once after the

@@ -77,6 +77,9 @@ struct OCase {
   int binary, bwidth, nfit, bpartial;
   const double *pairfit, *selffit;
   const int *bath;
+  // the rotational periodics' rotations, 3 x 3 each, a halo entry's rot
+  // (1 + its index, 0 for none) naming one
+  const double *rots;
 };
 
 // one reaction, the columns of FiniteRateModel.rxnconsts
@@ -125,7 +128,7 @@ struct OBlock {
 // out): dst block, dst i j k, src block, src i j k, and the halo layer
 // (0 = next to the interface), all full-array indices.
 struct OHaloEntry {
-  int32_t dblk, di, dj, dk, sblk, si, sj, sk, layer;
+  int32_t dblk, di, dj, dk, sblk, si, sj, sk, layer, rot;
 };
 
 }  // extern "C"
@@ -1814,8 +1817,31 @@ void bc_wallflux(const OCase &c, const OBlock &B, const std::vector<double> &sta
     }
 }
 
-void halo_fill(std::vector<OBlock> &blks, const OHaloEntry *map, long nmap, int maxlayer, int comps,
-               double *(*arr)(OBlock &, std::vector<Scratch> &, int), std::vector<Scratch> &scr) {
+// a three-vector at stride st turned by R (place.mako:4-9)
+void rotate3(double *x, int st, const double *R) {
+  const double a = x[0], b = x[st], c = x[2 * st];
+  x[0] = R[0] * a + R[1] * b + R[2] * c;
+  x[st] = R[3] * a + R[4] * b + R[5] * c;
+  x[2 * st] = R[6] * a + R[7] * b + R[8] * c;
+}
+
+// the turn a rotational periodic gives what lands in its halo: the vector at
+// component vec (Q's momentum at 1), or with vec -2 the gradients' tensor,
+// each row's directions and then the velocity rows down every direction
+// (simulator place.mako:11-36)
+void rotate_cell(const OCase &c, const OHaloEntry &h, double *dp, int comps, int vec) {
+  if (!h.rot || !c.rots || vec == -1) return;
+  const double *R = c.rots + 9 * (h.rot - 1);
+  if (vec >= 0) {
+    rotate3(dp + vec, 1, R);
+    return;
+  }
+  for (int r = 0; r < comps / 3; r++) rotate3(dp + 3 * r, 1, R);
+  for (int m = 0; m < 3; m++) rotate3(dp + m, 3, R);
+}
+
+void halo_fill(const OCase &c, std::vector<OBlock> &blks, const OHaloEntry *map, long nmap, int maxlayer, int comps,
+               int vec, double *(*arr)(OBlock &, std::vector<Scratch> &, int), std::vector<Scratch> &scr) {
   for (long m = 0; m < nmap; m++) {
     const OHaloEntry &h = map[m];
     if (h.layer >= maxlayer) continue;
@@ -1824,6 +1850,7 @@ void halo_fill(std::vector<OBlock> &blks, const OHaloEntry *map, long nmap, int 
     double *dp = arr(d, scr, h.dblk) + cells(d).at(h.di, h.dj, h.dk) * comps;
     const double *sp = arr(s, scr, h.sblk) + cells(s).at(h.si, h.sj, h.sk) * comps;
     std::memcpy(dp, sp, sizeof(double) * comps);
+    rotate_cell(c, h, dp, comps, vec);
   }
 }
 
@@ -1846,7 +1873,7 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
   std::vector<OBlock> blks(blocks, blocks + nblocks);
   std::vector<Scratch> scr(nblocks);
   // Q's halo: every layer (simulator/advec/simulator.py:57-63)
-  halo_fill(blks, map, nmap, 1 << 30, ne, [](OBlock &b, std::vector<Scratch> &, int) { return b.Q; }, scr);
+  halo_fill(c, blks, map, nmap, 1 << 30, ne, 1, [](OBlock &b, std::vector<Scratch> &, int) { return b.Q; }, scr);
   for (int b = 0; b < nblocks; b++) {
     OBlock &B = blks[b];
     const Dims d = cells(B);
@@ -1944,7 +1971,7 @@ int oracle_rhs(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *m
   }
   if (visc) {
     // grads: one halo plane (simulator/advecdiff/simulator.py:11-14, 116-117)
-    halo_fill(blks, map, nmap, 1, ngrad * 3,
+    halo_fill(c, blks, map, nmap, 1, ngrad * 3, -2,
               [](OBlock &, std::vector<Scratch> &s, int b) { return s[b].grads.data(); }, scr);
     // the inflows' and outflows' halo gradients (simulator/advecdiff/simulator.py:113-114)
     for (int m = 0; m < c.nbc; m++)
@@ -2157,6 +2184,7 @@ int oracle_prestep(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntr
     OBlock &S = blocks[h.sblk];
     const long dt = cells(D).at(h.di, h.dj, h.dk), st = cells(S).at(h.si, h.sj, h.sk);
     std::memcpy(D.Q + dt * ne, S.Q + st * ne, sizeof(double) * ne);
+    rotate_cell(c, h, D.Q + dt * ne, ne, 1);
     std::memcpy(D.pst + dt * NSTATE, S.pst + st * NSTATE, sizeof(double) * NSTATE);
     D.Tg[dt] = S.Tg[st];
   }
@@ -2347,5 +2375,15 @@ int oracle_combine(int nx, int ny, int nz, int ng, int ne, double *out, int own,
 // the large ones
 extern "C" int oracle_set_threads(int n) {
   omp_set_num_threads(n < 1 ? 1 : n);
+  return 0;
+}
+
+// register Q's halo of every block filled across the interfaces, a
+// rotational periodic's vectors turned (the reference's exchange of a bank)
+extern "C" int oracle_exchange(const OCase *cp, OBlock *blocks, int nblocks, const OHaloEntry *map, long nmap) {
+  std::vector<OBlock> blks(blocks, blocks + nblocks);
+  std::vector<Scratch> scr(nblocks);
+  halo_fill(*cp, blks, map, nmap, 1 << 30, 4 + cp->ns, 1, [](OBlock &b, std::vector<Scratch> &, int) { return b.Q; },
+            scr);
   return 0;
 }

@@ -64,11 +64,19 @@ enum { ST_Z = 8, ST_THETA = 9, ST_EPS = 10, ST_KAPPA = 11, ST_ZETA = 12 };
   const long long t = (long long)where_.y * blockDim.x + threadIdx.x
 
 // one cell of a halo filled from another cell: each side's block start in
-// cells (cv), its cell index inside the block and its component stride (vol)
+// cells (cv), its cell index inside the block and its component stride
+// (vol); rot, when not 0, the rotation (rot - 1 in the case's table) a
+// rotationally periodic interface turns the cell's vectors by
 struct HaloEntry {
   long long dcv, scv;
   int didx, sidx, dvol, svol;
+  int rot;
 };
+
+// what k_halo turns with an entry's rotation: nothing, the vector at a
+// component (Q's momentum at 1), or the gradients' tensor (each row's three
+// directions, and the velocity rows u, v, w down every direction)
+enum { HALO_SCALARS = -1, HALO_TENSOR = -2 };
 
 // a fused work item: a column of tw x th cells of one block over k0 .. k1 - 1
 struct TileDev {

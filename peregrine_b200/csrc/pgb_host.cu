@@ -81,6 +81,10 @@ struct HostBlock {
   int nx, ny, nz;
   int nbr[6] = {-1, -1, -1, -1, -1, -1};
   int nbrface[6] = {0, 0, 0, 0, 0, 0};
+  // per face, the reference's orientation digits: for each of this block's
+  // axes the neighbour's axis it runs along, 1-3 forward, 4-6 backward
+  int orient[6][3] = {{1, 2, 3}, {1, 2, 3}, {1, 2, 3}, {1, 2, 3}, {1, 2, 3}, {1, 2, 3}};
+  int rot[6] = {0, 0, 0, 0, 0, 0};  // a rotationally periodic face's rotation, 1 + its index
   int bc[6] = {-1, -1, -1, -1, -1, -1};  // a boundary face's entry, -1 for none
   int tw = 0, th = 0, kchunk = 0;
   bool metrics_set[PGB_NMETRICS] = {};
@@ -113,6 +117,10 @@ struct pgb_case {
   double *d_dt = nullptr;
   HaloEntry *d_halo = nullptr;
   long long nhalo = 0, nhalo_l0 = 0;  // all entries; face layer 0 only (first)
+  // the rotationally periodic faces' rotations, then the products a halo
+  // cell reached across two of them needs, 3 x 3 each
+  std::vector<double> rots;
+  double *d_rots = nullptr;
   // per-block path scratch
   double *d_state = nullptr, *d_tr = nullptr, *d_hsp = nullptr, *d_grads = nullptr, *d_F[3] = {};
   double *d_prims = nullptr;
@@ -342,37 +350,59 @@ int set_current(pgb_case *c) {
   return PGB_OK;
 }
 
-// where a cell outside a block lies: step across faces one axis at a time
-// (orientation "123", a conforming lattice), across as many blocks as a
-// block thinner than the halo needs; false at a boundary
-bool locate(const pgb_case *c, int b, int ijk[3], int &sb) {
+// where a cell outside a block lies: step across the face of the first axis
+// it lies outside of, into the neighbour's own axes by the face's
+// orientation (the reference's digits, peregrine/multiblock/interface/base.py:96-160),
+// as many times as a block thinner than the halo or an edge cell needs;
+// false at a boundary.  rot: the rotation the cell's vectors take on the way
+// (1 + its index in the case's table, 0 for none), the faces' own composed.
+bool locate(pgb_case *c, int b, int ijk[3], int &sb, int &rot) {
   sb = b;
-  for (int a = 0; a < 3; a++) {
-    for (int hop = 0; hop <= NG; hop++) {
-      const HostBlock &B = c->blocks[sb];
-      const int n[3] = {B.nx, B.ny, B.nz};
-      if (ijk[a] < 0) {
-        const int nb = B.nbr[2 * a];
-        if (nb < 0) return false;
-        const HostBlock &N = c->blocks[nb];
-        const int m[3] = {N.nx, N.ny, N.nz};
-        ijk[a] += m[a];
-        sb = nb;
-      } else if (ijk[a] >= n[a]) {
-        const int nb = B.nbr[2 * a + 1];
-        if (nb < 0) return false;
-        ijk[a] -= n[a];
-        sb = nb;
+  rot = 0;
+  for (int hop = 0; hop < 4 * (NG + 1); hop++) {
+    const HostBlock &B = c->blocks[sb];
+    const int n[3] = {B.nx, B.ny, B.nz};
+    int a = -1;
+    for (int d = 0; d < 3 && a < 0; d++)
+      if (ijk[d] < 0 || ijk[d] >= n[d]) a = d;
+    if (a < 0) return true;
+    const bool low = ijk[a] < 0;
+    const int f = 2 * a + (low ? 0 : 1);
+    const int nb = B.nbr[f];
+    if (nb < 0) return false;
+    const HostBlock &N = c->blocks[nb];
+    const int m[3] = {N.nx, N.ny, N.nz};
+    int out[3];
+    for (int d = 0; d < 3; d++) {
+      const int t = (B.orient[f][d] - 1) % 3;
+      const bool flip = B.orient[f][d] > 3;
+      if (d == a) {
+        // the depth past the face; the neighbour meets a low face with its
+        // high one unless the axis runs backward
+        const int depth = low ? -1 - ijk[a] : ijk[a] - n[a];
+        const bool theirlow = low == flip;
+        out[t] = theirlow ? depth : m[t] - 1 - depth;
       } else {
-        break;
+        out[t] = flip ? m[t] - 1 - ijk[d] : ijk[d];
       }
     }
+    if (B.rot[f]) {
+      if (!rot) {
+        rot = B.rot[f];
+      } else {
+        // a cell across two rotating faces: the product, the nearer face's on the left
+        const double *R1 = &c->rots[9 * (rot - 1)], *R2 = &c->rots[9 * (B.rot[f] - 1)];
+        double P[9];
+        for (int r = 0; r < 3; r++)
+          for (int q = 0; q < 3; q++) P[3 * r + q] = R1[3 * r] * R2[q] + R1[3 * r + 1] * R2[3 + q] + R1[3 * r + 2] * R2[6 + q];
+        c->rots.insert(c->rots.end(), P, P + 9);
+        rot = (int)(c->rots.size() / 9);
+      }
+    }
+    ijk[0] = out[0], ijk[1] = out[1], ijk[2] = out[2];
+    sb = nb;
   }
-  const HostBlock &S = c->blocks[sb];
-  const int n[3] = {S.nx, S.ny, S.nz};
-  for (int a = 0; a < 3; a++)
-    if (ijk[a] < 0 || ijk[a] >= n[a]) return false;
-  return true;
+  return false;
 }
 
 // every halo cell a stage reads: the face halos two deep (layer 0 of every
@@ -382,14 +412,15 @@ void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0) {
   out.clear();
   auto add = [&](int b, int i, int j, int k) {
     int ijk[3] = {i, j, k};
-    int sb;
-    if (!locate(c, b, ijk, sb)) return;
+    int sb, rot;
+    if (!locate(c, b, ijk, sb, rot)) return;
     const BlockDev &D = c->blocks[b].dev, &S = c->blocks[sb].dev;
     HaloEntry h;
     h.dcv = D.cv, h.scv = S.cv;
     h.didx = (int)cell_index(D, i + NG, j + NG, k + NG);
     h.sidx = (int)cell_index(S, ijk[0] + NG, ijk[1] + NG, ijk[2] + NG);
     h.dvol = (int)D.vol, h.svol = (int)S.vol;
+    h.rot = rot;
     out.push_back(h);
   };
   for (int layer = 0; layer < NG; layer++) {
@@ -783,7 +814,7 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
   for (int q = 0; q < 2; q++) a.prep[q] = q < a.npre ? c->d_reg[a.pre[q]] : nullptr;
   a.dt = c->d_dt;
   // the stencil register's halo first
-  k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne);
+  k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne, 1, c->d_rots);
   mark(c, K_HALO, count);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -923,6 +954,7 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.met = c->d_met;
   pc.halo = c->d_halo;
   pc.nhalo = c->nhalo, pc.nhalo_l0 = c->nhalo_l0;
+  pc.rots = c->d_rots;
   pc.visc = sim_visc(c->phys.simulator);
   pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
   pc.chem = c->phys.chemistry;
@@ -1180,7 +1212,7 @@ int pgb_case_destroy(pgb_case *c) {
   void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
-                  c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells};
+                  c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots};
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1334,6 +1366,56 @@ int pgb_case_connect(pgb_case *c, int blk, int nface, int nbr, int nbrface) {
   c->blocks[blk].nbr[nface - 1] = nbr;
   if (nbr >= 0) c->blocks[blk].bc[nface - 1] = -1;
   c->blocks[blk].nbrface[nface - 1] = nbrface;
+  return PGB_OK;
+}
+
+int pgb_case_connect_oriented(pgb_case *c, int blk, int nface, int nbr, const char *orient, const double *rot) {
+  if (!c || !orient) return fail(PGB_ERR_ARG, "null argument");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  if (blk < 0 || blk >= (int)c->blocks.size() || nface < 1 || nface > 6)
+    return fail(PGB_ERR_ARG, "no such block face");
+  if (nbr < 0 || nbr >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "no such neighbour");
+  int code[3], seen = 0;
+  for (int d = 0; d < 3; d++) {
+    if (orient[d] < '1' || orient[d] > '6') return fail(PGB_ERR_ARG, "an orientation is three digits 1-6");
+    code[d] = orient[d] - '0';
+    seen |= 1 << ((code[d] - 1) % 3);
+  }
+  if (seen != 7 || orient[3] != '\0') return fail(PGB_ERR_ARG, "the orientation does not name three distinct axes");
+  const int a = (nface - 1) / 2;
+  HostBlock &B = c->blocks[blk];
+  const HostBlock &N = c->blocks[nbr];
+  const int n[3] = {B.nx, B.ny, B.nz}, m[3] = {N.nx, N.ny, N.nz};
+  for (int d = 0; d < 3; d++)
+    if (d != a && n[d] != m[(code[d] - 1) % 3]) return fail(PGB_ERR_ARG, "the two faces do not match cell for cell");
+  for (int d = 0; d < 3; d++) B.orient[nface - 1][d] = code[d];
+  const int t = (code[a] - 1) % 3;
+  const bool flip = code[a] > 3, low = nface % 2 == 1;
+  B.nbr[nface - 1] = nbr;
+  B.nbrface[nface - 1] = 2 * t + (low == flip ? 1 : 2);
+  B.bc[nface - 1] = -1;
+  B.rot[nface - 1] = 0;
+  if (rot) {
+    bool identity = true;
+    for (int q = 0; q < 9; q++) identity = identity && std::fabs(rot[q] - (q % 4 == 0 ? 1.0 : 0.0)) <= 1e-14;
+    if (!identity) {
+      c->rots.insert(c->rots.end(), rot, rot + 9);
+      B.rot[nface - 1] = (int)(c->rots.size() / 9);
+    }
+  }
+  return PGB_OK;
+}
+
+int pgb_exchange(pgb_case *c, int reg) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
+  RET(set_current(c));
+  if (c->nhalo)
+    k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[c->phys_of[reg]], c->d_halo, c->nhalo, c->ne, 1,
+                                                           c->d_rots);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
   return PGB_OK;
 }
 
@@ -1514,6 +1596,10 @@ int pgb_case_finalize(pgb_case *c) {
   c->nhalo = (long long)halo.size();
   CK(cudaMalloc(&c->d_halo, sizeof(HaloEntry) * std::max<size_t>(1, halo.size())));
   CK(cudaMemcpy(c->d_halo, halo.data(), sizeof(HaloEntry) * halo.size(), cudaMemcpyHostToDevice));
+  if (!c->rots.empty()) {
+    CK(cudaMalloc(&c->d_rots, sizeof(double) * c->rots.size()));
+    CK(cudaMemcpy(c->d_rots, c->rots.data(), sizeof(double) * c->rots.size(), cudaMemcpyHostToDevice));
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->finalized = true;
   RET(build_plans(c));

@@ -12,14 +12,36 @@
 
 namespace pgb {
 
-// the halo fill over every block at once: comps components per entry
-// (the reference's place kernel, peregrine/multiblock/collections/exchange/kernels/place.mako:11-20)
-static __global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps) {
+// a vector of three components at stride st turned by R
+__device__ __forceinline__ void rotate3(double *x, const long long st, const double *R) {
+  const double a = x[0], b = x[st], c = x[2 * st];
+  x[0] = R[0] * a + R[1] * b + R[2] * c;
+  x[st] = R[3] * a + R[4] * b + R[5] * c;
+  x[2 * st] = R[6] * a + R[7] * b + R[8] * c;
+}
+
+// the halo fill over every block at once: comps components per entry, the
+// vectors an entry's rotation turns given by vec (a component, or
+// HALO_TENSOR for the gradients), rots the case's rotations, 3 x 3 each
+// (the reference's place kernel, peregrine/multiblock/collections/exchange/kernels/place.mako:3-36)
+static __global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps,
+                              int vec = HALO_SCALARS, const double *__restrict__ rots = nullptr) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const HaloEntry h = tab[e];
     double *d = base + comps * h.dcv + h.didx;
     const double *s = base + comps * h.scv + h.sidx;
     for (int c = 0; c < comps; c++) d[(long long)c * h.dvol] = s[(long long)c * h.svol];
+    if (h.rot && rots && vec != HALO_SCALARS) {
+      const double *R = rots + 9 * (h.rot - 1);
+      const long long st = h.dvol;
+      if (vec >= 0) {
+        rotate3(d + vec * st, st, R);
+      } else {
+        // each row's directions, then the velocity rows down every direction
+        for (int r = 0; r < comps / 3; r++) rotate3(d + 3 * r * st, st, R);
+        for (int m = 0; m < 3; m++) rotate3(d + m * st, 3 * st, R);
+      }
+    }
   }
 }
 

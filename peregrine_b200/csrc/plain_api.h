@@ -33,6 +33,7 @@ struct PlainCase {
   const double *met;
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
+  const double *rots;         // the rotationally periodic interfaces' rotations, 3 x 3 each
   int visc, primary, recon, limiter;
   int chem;  // 0 none, 1 coupled source, 2 sub-stepped (PGB_CHEM_*)
   // the sub-stepped chemistry: its options, each cell's last substep count

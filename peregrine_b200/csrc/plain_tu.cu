@@ -247,7 +247,7 @@ static void substep_passes(const PlainCase *pc, const RhsArgs &a) {
 extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, double *dQ) {
   cudaStream_t s = pc->stream;
   const RhsArgs a{Q, dQ};
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(Q), pc->halo, pc->nhalo, NE);
+  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(Q), pc->halo, pc->nhalo, NE, 1, pc->rots);
   mark(pc, 0);
   if (pc->packed) {
     for_blocks(pc, R_VOL, fromQ_launch, &a, 2);
@@ -273,7 +273,8 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
     }
   }
   if (pc->visc) {
-    k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1));
+    k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1), HALO_TENSOR,
+                                                pc->rots);
     mark(pc, 0);
     bc_grads_launch(pc);
   }
@@ -383,7 +384,7 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
     k_freeze<NS><<<grid_of(range_size(D, R_INNER)), TH, 0, s>>>(pc->d_blks, b, Q, pc->state);
     mark(pc, 2);
   }
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(Q, pc->halo, pc->nhalo, NE);
+  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(Q, pc->halo, pc->nhalo, NE, 1, pc->rots);
   mark(pc, 0);
   k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(pc->state, pc->halo, pc->nhalo, SW);
   mark(pc, 0);

@@ -9,9 +9,37 @@ of one box length (cube.py:34-42).  Beyond the reference it takes uneven cuts:
 ``cells`` gives each axis's per-block cell counts, so a 128-cell axis can be
 cut 41 + 30 + 57.  ``blkdims`` (nodes per block, every block alike) is the
 reference's form and still accepted.
+
+An interface's orientation is the reference's three digits: for each axis
+of the block, the neighbour's axis it runs along, 1-3 forward and 4-6
+backward (peregrine/multiblock/interface/base.py:96-160).  ``reorient``
+lays a block out along other axes, its neighbours' digits following, as
+the reference's partitioner does; ``AnnulusMesher`` sweeps blocks about an
+axis, its ends joined as rotational periodics (peregrine/mesher/annulus.py).
 """
 
 import numpy as np
+
+
+def signedaxis(code):
+    """An orientation digit's axis and whether it runs backward."""
+    n = int(code)
+    return (n - 1) % 3, n > 3
+
+
+def orientcode(axis, flip):
+    return str(axis + 1 + (3 if flip else 0))
+
+
+def rotabout(axis, deg):
+    """The rotation by deg degrees about axis (Rodrigues' formula)."""
+    u = np.asarray(axis, np.float64)
+    u = u / np.linalg.norm(u)
+    th = np.radians(deg)
+    ct, st = np.cos(th), np.sin(th)
+    x, y, z = u
+    cross = np.array([[0.0, -z, y], [z, 0.0, -x], [-y, x, 0.0]])
+    return ct * np.eye(3) + st * cross + (1.0 - ct) * np.outer(u, u)
 
 
 class Interface:
@@ -23,8 +51,28 @@ class Interface:
         self.nbrface = None      # the neighbour's face across
         self.orient = "123"
         self.xlate = np.zeros(3)  # periodic translation of what lands in this halo
+        self.rot = None           # a rotational periodic's turn of what lands in this halo
         self.periodic = False
         self.bcname = None
+
+    @property
+    def rotperiodic(self):
+        return self.rot is not None and not np.allclose(self.rot, np.eye(3))
+
+    def set_nbrface(self):
+        """The neighbour's face, from the digit of this face's own axis: a low
+        face meets the neighbour's high one unless the axis runs backward."""
+        axis, flip = signedaxis(self.orient[self.axis])
+        self.nbrface = 2 * axis + (1 if self.is_low == flip else 2)
+
+    def inframe(self, a):
+        """An array of the neighbour's cells or nodes (its three index axes
+        first) laid out along this block's axes."""
+        out = np.moveaxis(a, [signedaxis(c)[0] for c in self.orient], [0, 1, 2])
+        for m, c in enumerate(self.orient):
+            if signedaxis(c)[1]:
+                out = np.flip(out, axis=m)
+        return out
 
 
 class Block:
@@ -176,14 +224,131 @@ def fill_node_halos(blocks):
                     near[a], far[a] = edge, edge + step * (layer + 1)
                     blk.nodes[tuple(dst)] = 2.0 * blk.nodes[tuple(near)] - blk.nodes[tuple(far)]
                     continue
-                nbr = blocks[face.nbr]
+                # the neighbour's nodes (its halo as wide on every side) along
+                # this block's axes, then its plane one in from the shared
+                # plane, deeper by layer (past a thin neighbour, into its halo)
+                nbr = face.inframe(blocks[face.nbr].nodes)
                 src = list(inplane)
-                # the neighbour's plane one in from the shared plane, then deeper by layer
-                if face.is_low:
-                    src[a] = g + nbr.extents[a] - 2 - layer
-                else:
-                    src[a] = g + 1 + layer
-                blk.nodes[tuple(dst)] = nbr.nodes[tuple(src)] + face.xlate
+                src[a] = nbr.shape[a] - g - 2 - layer if face.is_low else g + 1 + layer
+                x = nbr[tuple(src)]
+                if face.rot is not None:
+                    x = x @ np.asarray(face.rot).T
+                blk.nodes[tuple(dst)] = x + face.xlate
+
+
+def reorient(blocks, n, S):
+    """Block n laid out along other axes: its old axis m becomes axis
+    axes[m] of the new layout, running backward where flips[m] (S the
+    reference's digits; tests/communication/test_orientation.py:39-46), its
+    faces and its neighbours' orientation digits following."""
+    axes = [signedaxis(c)[0] for c in S]
+    flips = [signedaxis(c)[1] for c in S]
+    blk = blocks[n]
+    # the digits of every face across into block n: its axis t is now axes[t]
+    for other in blocks:
+        for face in other.intfaces:
+            if face.nbr == n:
+                codes = [signedaxis(c) for c in face.orient]
+                face.orient = "".join(orientcode(axes[t], f != flips[t]) for t, f in codes)
+    # block n's own faces move with its axes, and their digits with them
+    old = list(blk.intfaces)
+    new = [None] * 6
+    for face in old:
+        m = face.axis
+        low = face.is_low != flips[m]
+        nface = 2 * axes[m] + (1 if low else 2)
+        if face.nbr is not None:
+            codes = [None] * 3
+            for d, c in enumerate(face.orient):
+                t, f = signedaxis(c)
+                codes[axes[d]] = orientcode(t, f != flips[d])
+            face.orient = "".join(codes)
+        face.nface, face.axis, face.is_low = nface, (nface - 1) // 2, nface % 2 == 1
+        new[nface - 1] = face
+    blk.intfaces = new
+    out = blk.nodes
+    for m, f in enumerate(flips):
+        if f:
+            out = np.flip(out, axis=m)
+    blk.nodes = np.ascontiguousarray(np.moveaxis(out, (0, 1, 2), axes))
+    ext = [None] * 3
+    for m in range(3):
+        ext[axes[m]] = blk.extents[m]
+    blk.ni, blk.nj, blk.nk = ext
+    for other in blocks:
+        for face in other.intfaces:
+            if face.nbr is not None:
+                face.set_nbrface()
+
+
+class AnnulusMesher:
+    """Blocks swept about the axis p1 -> p2 (peregrine/mesher/annulus.py):
+    i along the axis, j out from it from the radius of p3 by thickness, k
+    round it through sweep degrees; periodic joins the sweep's ends, as a
+    rotational periodic whose low face takes its halo turned back by the
+    sweep and whose high face turned on by it (annulus.py:82-94)."""
+
+    name = "annulus"
+
+    def __init__(self, mbdims=(1, 1, 1), blkdims=(5, 5, 5), p1=(0, 0, 0), p2=(1, 0, 0), p3=(0, 1, 0), sweep=45.0,
+                 thickness=0.1, periodic=False, bcnames=None, defaultbc=None):
+        self.mbdims = [int(n) for n in mbdims]
+        self.blkdims = [int(n) for n in blkdims]
+        self.p1, self.p2, self.p3 = (np.asarray(p, np.float64) for p in (p1, p2, p3))
+        self.sweep, self.thickness, self.periodic = float(sweep), float(thickness), bool(periodic)
+        self.bcnames = dict(bcnames or {})
+        self.defaultbc = defaultbc
+        length = np.linalg.norm(self.p2 - self.p1)
+        rin = np.linalg.norm(self.p3 - self.p1)
+        if length == 0.0 or rin == 0.0:
+            raise ValueError("p1 -> p2 is the axis and p3 off it")
+        self.axis = (self.p2 - self.p1) / length
+        self.radial = (self.p3 - self.p1) / rin
+        if abs(np.dot(self.axis, self.radial)) > 1e-7:
+            raise ValueError("the line (p1, p3) is not orthogonal to (p1, p2)")
+        if not 0.0 < self.sweep <= 360.0:
+            raise ValueError("the sweep is more than 0 and at most 360 degrees")
+        self.edges = [np.linspace(0.0, length, self.mbdims[0] + 1),
+                      np.linspace(rin, rin + self.thickness, self.mbdims[1] + 1),
+                      np.linspace(0.0, self.sweep, self.mbdims[2] + 1)]
+
+    def _turn(self, p, theta):
+        n = self.axis
+        ct, st = np.cos(theta)[:, None], np.sin(theta)[:, None]
+        return ct * p + st * np.cross(n, p) + (1.0 - ct) * np.dot(n, p) * n
+
+    def make_blocks(self, ng):
+        mbi, mbj, mbk = self.mbdims
+        blocks = []
+        for k in range(mbk):
+            for j in range(mbj):
+                for i in range(mbi):
+                    nblki = k * mbj * mbi + j * mbi + i
+                    blk = Block(nblki, *self.blkdims, ng)
+                    x, r, theta = (np.linspace(e[m], e[m + 1], nn)
+                                   for e, m, nn in zip(self.edges, (i, j, k), self.blkdims))
+                    radial = self._turn(self.radial, np.radians(theta))
+                    pts = (self.p1 + x[:, None, None, None] * self.axis +
+                           r[None, :, None, None] * radial[None, None, :, :])
+                    blk.nodes[blk.interior] = pts
+                    for axis, (nb, index) in enumerate(zip(self.mbdims, (i, j, k))):
+                        stride = int(np.prod(self.mbdims[:axis]))
+                        for nface, end, step in ((2 * axis + 1, 0, -1), (2 * axis + 2, nb - 1, 1)):
+                            face = blk.get_intface(nface)
+                            if index != end:
+                                face.nbr = nblki + step * stride
+                            elif axis == 2 and self.periodic:
+                                face.nbr = nblki - step * stride * (nb - 1)
+                                face.periodic = True
+                                if self.sweep != 360.0:
+                                    face.rot = rotabout(self.axis, -self.sweep if face.is_low else self.sweep)
+                            else:
+                                face.bcname = self.bcnames.get(nface, self.defaultbc)
+                                continue
+                            face.set_nbrface()
+                    blocks.append(blk)
+        fill_node_halos(blocks)
+        return blocks
 
 
 def uneven_cuts(total, pieces, low, high, rng):

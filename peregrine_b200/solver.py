@@ -196,7 +196,13 @@ class Solver:
         for blk in self.mesh_blocks:
             for face in blk.intfaces:
                 nbr = -1 if face.nbr is None else face.nbr
-                native.call("pgb_case_connect", self.case, blk.nblki, face.nface, nbr, face.nbrface or 0)
+                rot = getattr(face, "rot", None)
+                if face.nbr is not None and (face.orient != "123" or rot is not None):
+                    r = None if rot is None else _fptr(np.ascontiguousarray(rot, dtype=np.float64).ravel())
+                    native.call("pgb_case_connect_oriented", self.case, blk.nblki, face.nface, nbr,
+                                face.orient.encode(), r)
+                else:
+                    native.call("pgb_case_connect", self.case, blk.nblki, face.nface, nbr, face.nbrface or 0)
         self._fill_bcs()
         chem = self.cfg["chem-integration"]
         if chem["kind"] is not None:
@@ -271,6 +277,11 @@ class Solver:
                 raise ValueError(f"block {b.nblki}: primitives of shape {q.shape}")
             inner = np.asfortranarray(inner)
             native.call("pgb_set_prims", self.case, b.nblki, 0, _fptr(inner), inner.size)
+
+    def exchange(self, Q="Q"):
+        """Register Q's halo filled across every interface, a rotationally
+        periodic face's vectors turned (the reference's exchange of a bank)."""
+        native.call("pgb_exchange", self.case, self.regnum[Q])
 
     def rhs(self, *, Q="Q", dQ=None):
         dQ = dQ or self.regs[-1]
