@@ -307,6 +307,9 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
 /* The right-hand side dQ of logical register q into logical register dq, on
  * the per-block path (halo exchange included).  Returns when queued. */
 int pgb_rhs(pgb_case *c, int q, int dq);
+/* stage n's combines on the registers as they are, dt the last set or
+ * stepped (the reference's Solver.advance, peregrine/multiblock/solver.py:276-280) */
+int pgb_advance(pgb_case *c, int n);
 
 /* nsteps steps of dt on the chosen path; graph 1 captures one step into a CUDA
  * graph and replays it.  Returns when queued on the case's stream. */

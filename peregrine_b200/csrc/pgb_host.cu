@@ -1019,14 +1019,12 @@ int cfl_pass(pgb_case *c, int qphys, int &count) {
   return kPlain[c->phys.ns - 1].cflmax(&pc, c->d_reg[qphys], c->d_cfl);
 }
 
-int step_plain(pgb_case *c, int &count) {
+// a stage's combines on the registers as they are (the reference's advance
+// graph, peregrine/integrators/rungekutta.py:21-26)
+void combine_stage(pgb_case *c, const pgb_stage &st, int &count) {
   const int TH = 256;
   const auto &map = c->phys_of;
-  if (!c->stages.empty()) RET(cfl_prologue(c, map[c->stages[0].q], count));
-  if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count, 0));
-  for (const pgb_stage &st : c->stages) {
-    RET(rhs_plain(c, map[st.q], map[st.dq], count, st.tfrac));
-    for (int m = 0; m < st.ncombine; m++) {
+  for (int m = 0; m < st.ncombine; m++) {
       const pgb_combine &cb = st.combine[m];
       CombineDev cd{};
       cd.out = c->d_reg[map[cb.out]];
@@ -1044,7 +1042,16 @@ int step_plain(pgb_case *c, int &count) {
         k_combine<<<grid_for((long long)D.nx * D.ny * D.nz, TH), TH, 0, c->stream>>>(c->d_blks, b, c->ne, cd, c->d_dt);
         mark(c, K_COMBINE, count);
       }
-    }
+  }
+}
+
+int step_plain(pgb_case *c, int &count) {
+  const auto &map = c->phys_of;
+  if (!c->stages.empty()) RET(cfl_prologue(c, map[c->stages[0].q], count));
+  if (!c->stages.empty()) RET(prestep_plain(c, map[c->stages[0].q], count, 0));
+  for (const pgb_stage &st : c->stages) {
+    RET(rhs_plain(c, map[st.q], map[st.dq], count, st.tfrac));
+    combine_stage(c, st, count);
   }
   // the clock moves on by dt where boundaries read it or the step size is the device's
   if (c->nbcface[0] || c->ctrl_cfl) {
@@ -1749,6 +1756,16 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
   c->df_fresh = true;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_advance(pgb_case *c, int n) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  RET(prepare(c, false));
+  if (n < 0 || n >= (int)c->stages.size()) return fail(PGB_ERR_ARG, "no such stage");
+  int count = 0;
+  combine_stage(c, c->stages[n], count);
+  CK(cudaGetLastError());
   return PGB_OK;
 }
 

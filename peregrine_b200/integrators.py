@@ -112,6 +112,20 @@ class CFL(Fixed):
         return min(sim["cfl"] / solver.cflmax()["combined"], sim["dt-max"])
 
 
+class StageRegisters(tuple):
+    """A stage's registers by name: the one its right-hand side reads, dQ,
+    and the one its last combine writes (peregrine/integrators/base.py:4-10)."""
+
+    __slots__ = ()
+
+    def __new__(cls, Q, dQ, Qout):
+        return super().__new__(cls, (Q, dQ, Qout))
+
+    Q = property(lambda self: self[0])
+    dQ = property(lambda self: self[1])
+    Qout = property(lambda self: self[2])
+
+
 class Integrator:
     """The integrator's name and its step-size controller, as the reference's
     solver carries them (``solver.integ.controller``)."""
@@ -119,3 +133,10 @@ class Integrator:
     def __init__(self, cfg):
         self.name = cfg["time-integration"]["integrator"]
         self.controller = {"fixed": Fixed, "cfl": CFL}[cfg["simulation"]["controller"]](cfg)
+
+    def stageregs(self, registers):
+        """Each stage's registers named from ``registers``, the solver's
+        ``regs`` (peregrine/integrators/rungekutta.py:9-14)."""
+        rows, dQ, _ = stages(self.name)
+        return [StageRegisters(registers[q], registers[dQ], registers[combines[-1]["out"]])
+                for q, combines in rows]

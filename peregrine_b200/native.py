@@ -217,6 +217,7 @@ SIGNATURES = {
     "pgb_case_connect_oriented": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                    ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "pgb_exchange": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "pgb_advance": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "pgb_eos_get": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_set_prims": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_rhs": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),

@@ -278,6 +278,29 @@ class Solver:
             inner = np.asfortranarray(inner)
             native.call("pgb_set_prims", self.case, b.nblki, 0, _fptr(inner), inner.size)
 
+    def advance(self, n):
+        """Stage n's combines on the registers as they are, after its
+        right-hand side (peregrine/multiblock/solver.py:276-280); the step
+        size is ``dt``'s."""
+        native.call("pgb_advance", self.case, int(n))
+
+    def prerhs(self, Q="Q", dQ=None):
+        """Register Q readied for reading: its halo, state and boundary halo
+        cells formed (peregrine/multiblock/solver.py:246-250).  The library
+        forms them in a right-hand side, into dQ (the last register unless
+        named), as the reference's prerhs begins dQ."""
+        self.rhs(Q=Q, dQ=dQ)
+
+    def postrhs(self, Q=None):
+        """Register Q (the solution unless named) readied after it was written
+        (peregrine/multiblock/solver.py:282-285)."""
+        self.prerhs(Q or "Q")
+
+    @property
+    def dt(self):
+        """The step scalar, read and set as the reference's ``mb.dt``."""
+        return _DeviceScalar(self.last_dt, self.set_dt)
+
     def exchange(self, Q="Q"):
         """Register Q's halo filled across every interface, a rotationally
         periodic face's vectors turned (the reference's exchange of a bank)."""
@@ -381,6 +404,13 @@ class Solver:
     @property
     def ncells(self):
         return sum(b.ncells for b in self.mesh_blocks)
+
+
+class _DeviceScalar:
+    """A device scalar's get and set (the reference's Scalar)."""
+
+    def __init__(self, get, set_):
+        self.get, self.set = get, set_
 
 
 def get_solver(cfg, mesh, backend, state=None, cls=Solver):

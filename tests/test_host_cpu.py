@@ -250,3 +250,18 @@ def test_serving_requests_follow_the_workload():
         X = Y / np.array(MW)
         phi = X[0] / X[2] / 2.0
         assert 0.5 - 1e-9 <= phi <= 2.0 + 1e-9
+
+
+def test_the_stage_registers_are_the_references():
+    # peregrine/integrators/rungekutta.py:9-14: each stage reads start then
+    # stage, and writes stage, the last writing start
+    from peregrine_b200.integrators import Integrator
+
+    cfg = Config()
+    cfg["simulation"]["simulator"] = "euler"
+    for name, regs in (("tvd-rk3", ("Q", "Q1", "Q2")), ("rk2", ("Q", "Q1", "Q2")), ("rk4", ("Q", "Q1", "Q2", "Q3"))):
+        cfg["time-integration"]["integrator"] = name
+        st = Integrator(cfg.validate()).stageregs(regs)
+        assert st[0].Q == "Q" and all(s.Q == "Q1" for s in st[1:])
+        assert all(s.dQ == regs[-1] for s in st)
+        assert st[-1].Qout == "Q" and all(s.Qout == "Q1" for s in st[:-1])

@@ -185,3 +185,20 @@ def test_the_tgv_after_100_steps_matches_the_oracle():
     end = (got * vol[..., None]).sum(axis=(0, 1, 2))
     assert abs(end[0] - start[0]) <= 5e-12 * abs(start[0])
     assert abs(end[4] - start[4]) <= 5e-12 * abs(start[4])
+
+
+@pytest.mark.parametrize("integrator", ["tvd-rk3", "rk4"])
+def test_the_stages_by_hand_are_a_step(integrator):
+    # the reference's hand-rolled step (tests/integrators/test_postrhs.py:73-80):
+    # each stage's right-hand side, then its advance
+    mb, _ = build("navier-stokes", integrator, cells=12, blocks=(2, 1, 1), launch="per-block")
+    ref, _ = build("navier-stokes", integrator, cells=12, blocks=(2, 1, 1), launch="per-block")
+    dt = 2e-5
+    ref.step(dt)
+    mb.dt.set(dt)
+    for n, stage in enumerate(mb.integ.stageregs(mb.regs)):
+        mb.rhs(Q=stage.Q, dQ=stage.dQ)
+        mb.advance(n)
+    for a, b in zip(mb.blocks, ref.blocks):
+        assert np.array_equal(a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior])
+    assert mb.dt.get() == dt
