@@ -152,8 +152,11 @@ __device__ __forceinline__ void cp_wait() {
 
 // Shared memory of the uniform kernel, laid out for tiles of at most TW x TH
 // cells (the layout's extents are compile-time, so every neighbour and field
-// offset is an immediate; a tile may be smaller): P[2][P_N][LN2] two planes of
-// cell values, G[12][LN1] one plane of gradients, Fi[5][LN1], Fj[5][LN1]
+// offset is an immediate; a tile may be smaller): P[2][LN2][P_N] two planes of
+// cell values, a cell's six contiguous (48 bytes: three 16-byte loads, no two
+// lanes of a quarter warp on one bank), G[LN1][GS] one plane of gradients,
+// a cell's twelve contiguous in a record of GS (14 doubles, for the same
+// reason), Fi[5][LN1], Fj[5][LN1]
 // low-face fluxes, raw[3][5][NT + LNR] the Q copies of three planes in
 // flight, pre[3][2][5][LNT] the combines' registers of three planes.
 template <int NT, int TW, int TH>
@@ -161,10 +164,11 @@ struct F2L {
   static constexpr int LW1 = TW + 2, LH1 = TH + 2, LN1 = LW1 * LH1;
   static constexpr int LW2 = TW + 4, LN2 = LW2 * (TH + 4), LNR = 2 * (TW + TH), LNT = TW * TH;
   static constexpr int RAW = 5 * (NT + LNR), PRE = 2 * 5 * LNT;
+  static constexpr int GS = 14;  // a gradient record: twelve values and two of padding
   static_assert(LN1 <= NT, "the tile and its ring fit the CTA");
   static_assert(LNR <= NT, "the outer ring fits the CTA");
   __host__ __device__ static constexpr size_t doubles(bool visc) {
-    return (size_t)2 * P_N * LN2 + (visc ? 12 * LN1 : 0) + 10 * LN1 + 3 * RAW + 3 * PRE;
+    return (size_t)2 * P_N * LN2 + (visc ? GS * LN1 : 0) + 10 * LN1 + 3 * RAW + 3 * PRE;
   }
 };
 
@@ -177,7 +181,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
   const int tid = threadIdx.x;
   double *P = smem;
   double *G = P + 2 * P_N * LN2;
-  double *Fi = G + (VISC ? 12 * LN1 : 0);
+  double *Fi = G + (VISC ? L::GS * LN1 : 0);
   double *Fj = Fi + 5 * LN1;
   double *raw = Fj + 5 * LN1;  // [3][5][NT] own cells then [5][LNR] ring cells, per slot
   double *pre = raw + 3 * L::RAW;  // [3][2][5][LNT]
@@ -232,16 +236,15 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
     auto slot = [](int p) { return p & 1; };
     auto ring3 = [](int p) { return (p + 6) % 3; };
     auto getP = [&](int s, int r) {
-      const double *Ps = P + s * P_N * LN2 + r;
+      const double2 *Ps = reinterpret_cast<const double2 *>(P + s * P_N * LN2 + P_N * r);
+      const double2 a = Ps[0], b = Ps[1], d = Ps[2];
       CellP c;
-      c.rho = Ps[P_RHO * LN2], c.u = Ps[P_U * LN2], c.v = Ps[P_V * LN2];
-      c.w = Ps[P_W * LN2], c.T = Ps[P_T * LN2], c.e = Ps[P_E * LN2];
+      c.rho = a.x, c.u = a.y, c.v = b.x, c.w = b.y, c.T = d.x, c.e = d.y;
       return c;
     };
     auto putP = [&](int s, int r, const CellP &c) {
-      double *Ps = P + s * P_N * LN2 + r;
-      Ps[P_RHO * LN2] = c.rho, Ps[P_U * LN2] = c.u, Ps[P_V * LN2] = c.v;
-      Ps[P_W * LN2] = c.w, Ps[P_T * LN2] = c.T, Ps[P_E * LN2] = c.e;
+      double2 *Ps = reinterpret_cast<double2 *>(P + s * P_N * LN2 + P_N * r);
+      Ps[0] = make_double2(c.rho, c.u), Ps[1] = make_double2(c.v, c.w), Ps[2] = make_double2(c.T, c.e);
     };
     // plane p's Q copies for this thread's cells, into raw slot p mod 3
     auto fetch = [&](int p) {
@@ -292,7 +295,8 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
     };
     auto putG = [&](const double *g) {
 #pragma unroll
-      for (int q = 0; q < 12; q++) G[q * LN1 + c1] = g[q];
+      for (int q = 0; q < 12; q += 2)
+        reinterpret_cast<double2 *>(G + L::GS * c1)[q / 2] = make_double2(g[q], g[q + 1]);
     };
     auto grad_col = [&](int s, const CellP &below, const CellP &above, double *g) {
       grad_u(B, getP(s, c2 - 1), getP(s, c2 + 1), getP(s, c2 - LW2), getP(s, c2 + LW2), below, above, g);
@@ -366,9 +370,15 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
         const int li2 = ii >= 1 ? 1 : 0, lj2 = jj >= 1 ? LW2 : 0;
         double Fa[5], Fb[5], gli[12], glj[12], gr[12];
         if (VISC) {
+          const double2 *Gi = reinterpret_cast<const double2 *>(G + L::GS * (c1 - li));
+          const double2 *Gj = reinterpret_cast<const double2 *>(G + L::GS * (c1 - lj));
+          const double2 *Gr = reinterpret_cast<const double2 *>(G + L::GS * c1);
 #pragma unroll
-          for (int q = 0; q < 12; q++)
-            gli[q] = G[q * LN1 + c1 - li], glj[q] = G[q * LN1 + c1 - lj], gr[q] = G[q * LN1 + c1];
+          for (int q = 0; q < 6; q++) {
+            const double2 x = Gi[q], y = Gj[q], z = Gr[q];
+            gli[2 * q] = x.x, gli[2 * q + 1] = x.y, glj[2 * q] = y.x, glj[2 * q + 1] = y.y;
+            gr[2 * q] = z.x, gr[2 * q + 1] = z.y;
+          }
         }
         const CellP me = getP(s0, c2);
         face_u<0, VISC>(B, getP(s0, c2 - li2), me, gli, gr, Fa);
@@ -395,8 +405,17 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
       if (VISC && gcol) grad_col(s1, pk, p2, gup);
       if (tile) {
         double Fkh[5], gk[12];
+        if (VISC) {
+          const double2 *Gc = reinterpret_cast<const double2 *>(G + L::GS * c1);
 #pragma unroll
-        for (int q = 0; q < 12; q++) gk[q] = VISC ? G[q * LN1 + c1] : 0.0;
+          for (int q = 0; q < 6; q++) {
+            const double2 x = Gc[q];
+            gk[2 * q] = x.x, gk[2 * q + 1] = x.y;
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 12; q++) gk[q] = 0.0;
+        }
         face_u<2, VISC>(B, pk, pk1, gk, gup, Fkh);
         const double dJ = B.detJinv;
         double dQ[5];
