@@ -317,6 +317,22 @@ def substep_leg(steps, dt=1e-7, dT=1500.0):
     return out
 
 
+def packed_leg(mb, dt, steps, ncells, stages):
+    """The same steps on the packed path: the per-block kernels, each pass one
+    launch over every block."""
+    from peregrine_b200 import native
+
+    path = mb.path
+    mb.path = native.PATH_PACKED
+    mb.step(dt, 2)
+    mb.backend.sync()
+    ms = time_graph(mb, dt, steps)
+    out = {"value": ncells * stages * steps / (ms / 1e3), "ms_per_step": ms / steps,
+           "launches_per_step": mb.launches_per_step()}
+    mb.path = path
+    return out
+
+
 def realgas_leg(steps, cpu=True):
     """Cell-stage/s of the transcritical mixing layer on the per-block path."""
     import peregrine_b200 as pg
@@ -341,6 +357,7 @@ def realgas_leg(steps, cpu=True):
            "path": "per-block kernels, one launch per block and pass",
            "blocks": [b.cells[0] for b in mb.mesh_blocks],
            "algorithmic_bytes_per_cell_stage": nbytes, "hbm_gbs_of_algorithmic_bytes": value * nbytes / 1e9}
+    out["packed"] = packed_leg(mb, dt, steps, ncells, 3)
     if cpu:
         from oracle.oracle import Oracle
 
@@ -390,6 +407,7 @@ def boundary_leg(steps, cpu=True):
            "workload": "channel-192x96x96-8-blocks-2sp-ns-muscl-koren-hllc-rk3-cfl-0.8: velocity inflow "
                        "(expressions of y, z, t), pressure exit, isothermal no-slip floor, moving lid, periodic across",
            "path": "per-block kernels, boundary passes one launch each over every boundary face"}
+    out["packed"] = packed_leg(mb, dt, steps, ncells, 3)
     if cpu:
         from oracle.oracle import Oracle
 

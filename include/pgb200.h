@@ -53,7 +53,10 @@ enum { PGB_TRANS_NONE = 0, PGB_TRANS_CONSTANT = 1, PGB_TRANS_KINETIC = 2 };
  * stiff-cell compaction (peregrine/simulator/chemint/substepped.py) */
 enum { PGB_CHEM_NONE = 0, PGB_CHEM_COUPLED = 1, PGB_CHEM_SUBSTEPPED = 2 };
 /* the launch paths */
-enum { PGB_PATH_BATCHED = 0, PGB_PATH_PER_BLOCK = 1 };
+/* the launch paths: the batched fused kernel; the per-block kernels one
+ * launch per block and pass (the reference's order); the same kernels
+ * packed, each pass one launch over every block */
+enum { PGB_PATH_BATCHED = 0, PGB_PATH_PER_BLOCK = 1, PGB_PATH_PACKED = 2 };
 
 /* the per-cell and per-face arrays of a block the caller sets (metrics) or
  * reads and writes (registers, prims): the reference's array names

@@ -185,6 +185,6 @@ class Config(dict):
             if not sim[key] > 0.0:
                 raise ConfigError(f"simulation.{key}", "a positive number")
         launch = self["backend-b200"]["launch"]
-        if launch not in ("batched", "per-block"):
-            raise ConfigError("backend-b200.launch", "batched or per-block")
+        if launch not in ("batched", "per-block", "packed"):
+            raise ConfigError("backend-b200.launch", "batched, per-block or packed")
         return self

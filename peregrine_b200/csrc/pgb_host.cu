@@ -141,11 +141,12 @@ struct pgb_case {
   std::vector<std::vector<FusedStagePlan>> plans;  // [phase][stage]
   std::vector<std::vector<int>> maps;              // mapping at the start of each phase
   // graphs
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  std::vector<int> graph_map[2];  // the mapping a graph was captured under
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  std::vector<int> graph_map[3];  // the mapping a graph was captured under
+  bool packed = false;            // the per-block kernels, each pass one launch over every block
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.0f;
-  int launches[2] = {0, 0};
+  int launches[3] = {0, 0, 0};
   // per-launch timing (pgb_step_timed): an event after every launch
   bool timing = false;
   std::vector<cudaEvent_t> tev;
@@ -174,7 +175,7 @@ struct pgb_case {
   // the steps run under it, and the mode each path's graph was captured in
   double *d_cfl = nullptr, *d_ctrl = nullptr;
   bool ctrl_cfl = false;
-  bool graph_cfl[2] = {false, false};
+  bool graph_cfl[3] = {false, false, false};
   // the sub-stepped chemistry: its options, each cell's last count, the stiff list
   SubstepOpts subopt{200, 1, 8, 1e-7, 1e-12, 1.0, 0.0};
   int *d_subs = nullptr;
@@ -956,6 +957,7 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.nhalo = c->nhalo, pc.nhalo_l0 = c->nhalo_l0;
   pc.rots = c->d_rots;
   pc.visc = sim_visc(c->phys.simulator);
+  pc.packed = c->packed ? 1 : 0;
   pc.primary = c->phys.primary, pc.recon = c->phys.recon, pc.limiter = c->phys.limiter;
   pc.chem = c->phys.chemistry;
   pc.subopt = c->subopt;
@@ -1036,6 +1038,15 @@ void combine_stage(pgb_case *c, const pgb_stage &st, int &count) {
         const int r = cb.reg[n] < 0 ? st.dq : cb.reg[n];
         cd.X[n] = c->d_reg[map[r]];
         cd.w[n] = cb.w[n];
+      }
+      if (c->packed) {
+        // one launch over every block, a grid row each
+        long long most = 0;
+        for (const HostBlock &B : c->blocks) most = std::max(most, (long long)B.nx * B.ny * B.nz);
+        k_combine<<<dim3(grid_for(most, TH), (unsigned)c->blocks.size(), 1), TH, 0, c->stream>>>(c->d_blks, 0, c->ne,
+                                                                                                 cd, c->d_dt);
+        mark(c, K_COMBINE, count);
+        continue;
       }
       for (int b = 0; b < (int)c->blocks.size(); b++) {
         const BlockDev &D = c->blocks[b].dev;
@@ -1785,6 +1796,12 @@ int pgb_rhs(pgb_case *c, int q, int dq) {
 // ctrl_cfl): whole graph units while they fit, single steps after
 static int step_loop(pgb_case *c, int nsteps, int path, int graph) {
   const bool fused = path == PGB_PATH_BATCHED;
+  // the per-block kernels packed: each pass one launch over every block
+  struct Packed {
+    pgb_case *c;
+    ~Packed() { c->packed = false; }
+  } unpack{c};
+  c->packed = path == PGB_PATH_PACKED;
   CK(cudaEventRecord(c->ev0, c->stream));
   int done = 0;
   while (done < nsteps) {
@@ -1833,7 +1850,7 @@ static int step_loop(pgb_case *c, int nsteps, int path, int graph) {
 static int step_begin(pgb_case *c, int nsteps, int path) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
   if (nsteps < 0) return fail(PGB_ERR_ARG, "negative step count");
-  if (path != PGB_PATH_BATCHED && path != PGB_PATH_PER_BLOCK) return fail(PGB_ERR_ARG, "no such path");
+  if (path < PGB_PATH_BATCHED || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "no such path");
   const bool fused = path == PGB_PATH_BATCHED;
   if (fused && !fused_capable(c))
     return fail(PGB_ERR_UNSUPPORTED, "the batched path takes the single-species cpg kepaec case; use the per-block path");
@@ -1892,7 +1909,7 @@ int pgb_last_dt(pgb_case *c, double *dt) {
 
 int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int *kind, int cap, int *n) {
   if (!c || !n || (cap > 0 && (!ms || !kind))) return fail(PGB_ERR_ARG, "null argument");
-  if (path != PGB_PATH_BATCHED && path != PGB_PATH_PER_BLOCK) return fail(PGB_ERR_ARG, "no such path");
+  if (path < PGB_PATH_BATCHED || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "no such path");
   const bool fused = path == PGB_PATH_BATCHED;
   if (fused && !fused_capable(c)) return fail(PGB_ERR_UNSUPPORTED, "the batched path does not take this case");
   RET(prepare(c, fused));
@@ -1903,6 +1920,7 @@ int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int 
   c->timing = true;
   c->tnext = 0;
   c->tkind.clear();
+  c->packed = path == PGB_PATH_PACKED;
   CK(cudaEventRecord(c->ev0, c->stream));
   int rc = PGB_OK;
   for (int s = 0; s < nsteps && rc == PGB_OK; s++) {
@@ -1911,6 +1929,7 @@ int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int 
     c->launches[path] = count;
   }
   c->timing = false;
+  c->packed = false;
   if (rc != PGB_OK) return rc;
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
@@ -2004,7 +2023,7 @@ int pgb_last_step_ms(const pgb_case *c, float *ms) {
 }
 
 int pgb_launches_per_step(const pgb_case *c, int path, int *count) {
-  if (!c || !count || path < 0 || path > 1) return fail(PGB_ERR_ARG, "bad argument");
+  if (!c || !count || path < 0 || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "bad argument");
   *count = c->launches[path];
   return PGB_OK;
 }

@@ -89,7 +89,7 @@ def mechanism(consts):
         setattr(m, name, float(consts[name]))
     return m, (rxns, tbs, lfc, gpoly)
 TRANS_NONE, TRANS_CONSTANT, TRANS_KINETIC = 0, 1, 2
-PATH_BATCHED, PATH_PER_BLOCK = 0, 1
+PATH_BATCHED, PATH_PER_BLOCK, PATH_PACKED = 0, 1, 2
 ARR_XCC, ARR_DETJINV, ARR_JINV, ARR_IS, ARR_JS, ARR_KS, ARR_IXC, ARR_JXC, ARR_KXC = range(9)
 METRIC_IDS = {"xcc": ARR_XCC, "detJinv": ARR_DETJINV, "Jinv": ARR_JINV, "iS": ARR_IS, "jS": ARR_JS,
               "kS": ARR_KS, "ixc": ARR_IXC, "jxc": ARR_JXC, "kxc": ARR_KXC}

@@ -113,7 +113,8 @@ class Solver:
         self.regs = tuple(["Q"] + [f"Q{n}" for n in range(1, nregs)])
         self.regnum = {name: n for n, name in enumerate(self.regs)}
         launch = cfg["backend-b200"]["launch"]
-        self.path = native.PATH_BATCHED if launch == "batched" else native.PATH_PER_BLOCK
+        self.path = {"batched": native.PATH_BATCHED, "per-block": native.PATH_PER_BLOCK,
+                     "packed": native.PATH_PACKED}[launch]
         self.graph = bool(cfg["backend-b200"]["graph"])
         adv = cfg["adv-flux"]
         phys = native.Physics()

@@ -302,3 +302,16 @@ def test_conduction_is_linear_on_the_device():
     want = T1 + (T2 - T1) * (np.arange(N) + 0.5) / N
     assert np.allclose(st[:, 1], want, rtol=0.0, atol=1e-12 * (T2 - T1))
     assert np.allclose(Q[:, 1:4] / Q[:, :1], 0.0, atol=1e-11)
+
+
+def test_the_packed_path_steps_as_the_per_block_path():
+    # the channel's boundaries on the packed path: the same bits
+    from peregrine_b200 import native
+
+    mb, _ = channel()
+    ref, _ = channel()
+    mb.path = native.PATH_PACKED
+    mb.step(2e-7, 3)
+    ref.step(2e-7, 3)
+    for a, b in zip(mb.blocks, ref.blocks):
+        assert np.array_equal(a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior])

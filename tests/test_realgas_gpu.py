@@ -132,3 +132,18 @@ def test_double_flux_keeps_mass_and_species():
     after = totals()
     for row in (0, 5):
         assert abs(after[row] - before[row]) <= 1e-13 * abs(before[row]), row
+
+
+@pytest.mark.parametrize("simulator", ["euler-df", "navier-stokes"])
+def test_the_packed_path_steps_as_the_per_block_path(simulator):
+    # the same kernels, each pass one launch over every block: the same bits
+    from peregrine_b200 import native
+
+    mb, _ = build("pr", simulator)
+    ref, _ = build("pr", simulator)
+    mb.path = native.PATH_PACKED
+    mb.step(2e-9, 3)
+    ref.step(2e-9, 3)
+    assert mb.launches_per_step() < ref.launches_per_step()
+    for a, b in zip(mb.blocks, ref.blocks):
+        assert np.array_equal(a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior])
