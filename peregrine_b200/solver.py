@@ -147,8 +147,9 @@ class Solver:
             raise
         if self.path == native.PATH_BATCHED and not self.fused_capable():
             # the batched kernel takes the single-species kepaec case; any other
-            # physics runs the per-block kernels, still on the device
-            self.path = native.PATH_PER_BLOCK
+            # physics runs the per-block kernels, still on the device, packed
+            # (each pass one launch over every block, the same bits)
+            self.path = native.PATH_PACKED
         if state is None:
             self._uniform_ics()
 

@@ -236,11 +236,13 @@ def test_a_graph_replays_the_moving_boundary_values():
 
 
 def test_a_boundary_case_asked_for_the_batched_path_runs_per_block():
+    # the per-block kernels, packed: each pass one launch over every block
     import peregrine_b200 as pg
+    from peregrine_b200 import native
 
     cfg = cases.bc_box_config("slp-adia-wall", launch="batched")
     mb = pg.get_solver(cfg, cases.bc_box_mesh(), pg.get_backend("cuda", cfg))
-    assert mb.path == 1
+    assert mb.path == native.PATH_PACKED
 
 
 # -- the viscous walls' known answers on the device (tests/bcs/test_viscwalls.py)
