@@ -432,7 +432,9 @@ void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0) {
         const int a = f / 2;
         const bool low = f % 2 == 0;
         const int x = low ? -1 - layer : n[a] + layer;
-        const int a1 = (a + 1) % 3, a2 = (a + 2) % 3;
+        // the lower tangential axis fastest, so neighbouring entries (threads)
+        // touch neighbouring cells: i on the j- and k-faces, j on the i-faces
+        const int a1 = a == 0 ? 1 : 0, a2 = a == 2 ? 1 : 2;
         for (int q2 = 0; q2 < n[a2]; q2++)
           for (int q1 = 0; q1 < n[a1]; q1++) {
             int ijk[3];
