@@ -122,3 +122,38 @@ def test_the_mixture_average_is_the_kernels_sums(gas):
             rest = sum(X[q, m] * MW[m] for m in others)
             want[q, n] = rest / (p[q] * (rest * sum1 + X[q, n] * sum2))
     assert np.abs(D / want - 1.0).max() < 1e-12
+
+
+@pytest.mark.parametrize("trace, counts", [(1e-44, 1e-9)])
+def test_traces_of_either_sign_read_as_the_pure_cell(gas, trace, counts):
+    # tests/transport/test_diffusion.py:31-57: traces of both signs beside a
+    # pure species, the negative ones absent and the positive ones under the
+    # kernel's tolerance of 64 epsilon too, leave the pure cell; a trace over
+    # the tolerance is what the dominant species diffuses in
+    t, orc = gas
+    ns = int(t["ns"])
+    names = [str(n) for n in t["spnames"]]
+    lone, up = ns - 1, names.index("OH")
+    T, p = np.array([700.0, 1900.0]), np.array([2e5, 1.5e6])
+
+    def D_of(Y):
+        Q, st = states(orc, t, np.tile(Y, (2, 1)), T, p)
+        return orc.transport(Q, st)[:, 2:]
+
+    Y = np.zeros(ns)
+    Y[lone] = 1.0
+    Y[names.index("O2")], Y[up], Y[names.index("H2O")] = -3 * trace, 5 * trace, -0.8 * trace
+    others = np.arange(ns) != lone
+    for sign in (1.0, -1.0):
+        Y[up] = sign * 5 * trace
+        D = D_of(Y)
+        assert np.all(np.isfinite(D))
+        for q in range(2):
+            assert np.abs(D[q, lone] / pair_D(t, lone, lone, T[q], p[q]) - 1.0) < 1e-12
+            want = np.array([pair_D(t, n, lone, T[q], p[q]) for n in np.flatnonzero(others)])
+            assert np.abs(D[q, others] / want - 1.0).max() < 1e-12
+    # a trace that counts sets the direction: the dominant species' pair with it
+    Y[up] = counts
+    D = D_of(Y)
+    for q in range(2):
+        assert np.abs(D[q, lone] / pair_D(t, lone, up, T[q], p[q]) - 1.0) < 1e-8
