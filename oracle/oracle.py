@@ -52,7 +52,8 @@ class OCase(ctypes.Structure):
                 ("cfloor", ctypes.c_double), ("binary", ctypes.c_int), ("bwidth", ctypes.c_int),
                 ("nfit", ctypes.c_int), ("bpartial", ctypes.c_int), ("pairfit", ctypes.POINTER(ctypes.c_double)),
                 ("selffit", ctypes.POINTER(ctypes.c_double)), ("bath", ctypes.POINTER(ctypes.c_int)),
-                ("rots", ctypes.POINTER(ctypes.c_double))]
+                ("rots", ctypes.POINTER(ctypes.c_double)), ("herning", ctypes.c_int),
+                ("sqrtMW", ctypes.POINTER(ctypes.c_double))]
 
 # the boundary kinds (peregrine/simulator/euler/bcs.py, navstokes/bcs.py): the
 # oracle's number for each and the variables an entry gives, in order; the
@@ -335,7 +336,7 @@ class Oracle:
 
     def __init__(self, constants, ns, simulator, blocks, metrics, integrator="rk4", alpha=1.0, primary="kepaec",
                  recon="constant", limiter=None, eos="cpg", trans="constant", chemistry=None, bcvals=None,
-                 species=None, chemint="coupled", max_substeps=200, eqtol=1e-7):
+                 species=None, chemint="coupled", max_substeps=200, eqtol=1e-7, mixrule="wilke"):
         """constants: the mixture's tables; blocks/metrics may be empty for face-only use.
         eos "cpg" or "tpg", trans "constant" or "kinetic-theory", chemistry
         None or "finite-rate" (coupled: the source begins dQ).  bcvals: the
@@ -398,6 +399,11 @@ class Oracle:
             c.bwidth = len(bath) if c.bpartial else ns_ - 1
             c.pairfit, c.selffit, c.MW = _ptr(pair), _ptr(self_), _ptr(mw)
             c.bath = bath.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        if mixrule == "herning":
+            # Herning's viscosity mixing rule (peregrine/simulator/mixture/mixrule/herning.py)
+            sq = np.ascontiguousarray(np.sqrt(1.0 / np.asarray(constants["MWinv"], dtype=np.float64)))
+            self._tables["sqrtMW"] = sq
+            c.herning, c.sqrtMW = 1, _ptr(sq)
         if trans == "kinetic-theory":
             c.trans = 1
             mu = np.ascontiguousarray(constants["mupoly"], dtype=np.float64)

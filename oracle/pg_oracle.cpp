@@ -80,6 +80,9 @@ struct OCase {
   // the rotational periodics' rotations, 3 x 3 each, a halo entry's rot
   // (1 + its index, 0 for none) naming one
   const double *rots;
+  // Herning's viscosity mixing rule (simulator/mixture/mixrule/herning.py), sqrt(MW) per species
+  int herning;
+  const double *sqrtMW;
 };
 
 // one reaction, the columns of FiniteRateModel.rxnconsts
@@ -333,14 +336,25 @@ void transport(const OCase &c, const double *Q, const State &st, double *tr, dou
   }
   for (int n = 0; n < ns; n++) sinv[n] = 1.0 / (sqrtmu[n] * c.MWqinv[n]);
   double mu = 0.0;
-  for (int n = 0; n < ns; n++) {
-    const double sn = sqrtmu[n] * c.MWqinv[n];
-    double phi = 0.0;
-    for (int m = 0; m < ns; m++) {
-      const double r = 1.0 + sn * sinv[m];
-      phi += r * r * c.wilkepair[n * ns + m] * X(m);
+  if (c.herning) {
+    // simulator/mixture/mixrule/kernels/herning.mako:3-12
+    double num = 0.0, den = 0.0;
+    for (int n = 0; n < ns; n++) {
+      const double w = X(n) * c.sqrtMW[n];
+      num += w * sqrtmu[n] * sqrtmu[n];
+      den += w;
     }
-    mu += sqrtmu[n] * sqrtmu[n] * X(n) / phi;
+    mu = num / den;
+  } else {
+    for (int n = 0; n < ns; n++) {
+      const double sn = sqrtmu[n] * c.MWqinv[n];
+      double phi = 0.0;
+      for (int m = 0; m < ns; m++) {
+        const double r = 1.0 + sn * sinv[m];
+        phi += r * r * c.wilkepair[n * ns + m] * X(m);
+      }
+      mu += sqrtmu[n] * sqrtmu[n] * X(n) / phi;
+    }
   }
   for (int n = 0; n < ns; n++) {
     if (c.trans == 1) {

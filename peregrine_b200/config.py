@@ -153,6 +153,8 @@ class Config(dict):
                                              "and that eos one of them")
         if sim["simulator"] in DOUBLE_FLUX and adv["primary"] == "hllc":
             raise ConfigError("adv-flux.primary", "the double flux has kepaec, rusanov and ausmup")
+        if self["mixture"]["mixing-rule"] not in ("wilke", "herning"):
+            raise ConfigError("mixture.mixing-rule", f"{self['mixture']['mixing-rule']!r} is not one of ('wilke', 'herning')")
         if self["mixture"]["diffusion"] not in ("lewis", "binary"):
             raise ConfigError("mixture.diffusion", f"{self['mixture']['diffusion']!r} is not one of ('lewis', 'binary')")
         if self["diff-flux"]["formula"] != "alpha-damping":

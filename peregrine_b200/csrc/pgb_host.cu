@@ -272,6 +272,13 @@ int build_species(pgb_case *c) {
     RET(fit("mupoly", c->sp.mupoly, c->sp.nmu));
     RET(fit("kappapoly", c->sp.kappapoly, c->sp.nkappa));
   }
+  // Herning's mixing rule, when its sqrt(MW) are given
+  c->sp.herning = 0;
+  if (const double *sq = table(c, "sqrtMW")) {
+    if ((long)c->tables["sqrtMW"].size() < ns) return fail(PGB_ERR_ARG, "sqrtMW short");
+    for (int n = 0; n < ns; n++) c->sp.sqrtMW[n] = sq[n];
+    c->sp.herning = 1;
+  }
   // binary diffusion, when its pair fits are given: "selffit" [ns][terms],
   // "pairfit" [ns][width][terms], "bath" the species a partial bath sums over
   // (peregrine/simulator/mixture/diffusion/binary.py:18-37)

@@ -46,6 +46,10 @@ struct Species {
   // pair, and the bath (a partial bath lists its species; width partners)
   int binary, bpartial, bwidth, npair, nself;
   int bath[MAXNS];
+  // Herning's viscosity mixing rule in place of Wilke's
+  // (peregrine/simulator/mixture/mixrule/herning.py): sqrt(MW) per species
+  int herning;
+  double sqrtMW[MAXNS];
   double pairfit[MAXNS * MAXNS * MAXT], selffit[MAXNS * MAXT];
   // the cubic real gas (a thermally perfect gas underneath, tpg set too) and
   // its double flux: the form's u, w and roots sigma, eps; per species
@@ -395,16 +399,28 @@ __device__ __forceinline__ void transport(QF Q, const State &st, double *tr, dou
 #pragma unroll
   for (int n = 0; n < NS; n++) sinv[n] = 1.0 / (sqrtmu[n] * kSp.MWqinv[n]);
   double mu = 0.0;
+  if (kSp.herning) {
+    // peregrine/simulator/mixture/mixrule/kernels/herning.mako:3-12
+    double num = 0.0, den = 0.0;
 #pragma unroll
-  for (int n = 0; n < NS; n++) {
-    const double sn = sqrtmu[n] * kSp.MWqinv[n];
-    double phi = 0.0;
-#pragma unroll
-    for (int m = 0; m < NS; m++) {
-      const double r = 1.0 + sn * sinv[m];
-      phi += r * r * kSp.wilkepair[n * MAXNS + m] * X[m];
+    for (int n = 0; n < NS; n++) {
+      const double w = X[n] * kSp.sqrtMW[n];
+      num += w * sqrtmu[n] * sqrtmu[n];
+      den += w;
     }
-    mu += sqrtmu[n] * sqrtmu[n] * X[n] / phi;
+    mu = num / den;
+  } else {
+#pragma unroll
+    for (int n = 0; n < NS; n++) {
+      const double sn = sqrtmu[n] * kSp.MWqinv[n];
+      double phi = 0.0;
+#pragma unroll
+      for (int m = 0; m < NS; m++) {
+        const double r = 1.0 + sn * sinv[m];
+        phi += r * r * kSp.wilkepair[n * MAXNS + m] * X[m];
+      }
+      mu += sqrtmu[n] * sqrtmu[n] * X[n] / phi;
+    }
   }
   double series = 0.0, parallel = 0.0;
 #pragma unroll

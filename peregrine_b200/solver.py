@@ -181,6 +181,8 @@ class Solver:
             tables.update(mupoly=consts["mupoly"], kappapoly=consts["kappapoly"])
         if self.cfg["chem-integration"]["kind"] == "sub-stepped":
             tables.update(cppoly=consts["cppoly"], MW=consts["MW"])
+        if self.mixture.trans is not None and self.cfg["mixture"]["mixing-rule"] == "herning":
+            tables["sqrtMW"] = np.sqrt(1.0 / np.asarray(consts["MWinv"], dtype=np.float64))
         if self.mixture.trans is not None and getattr(self.mixture, "diffusion", "lewis") == "binary":
             tables.update(pairfit=consts["pairfit"], selffit=consts["selffit"], bath=consts["bath"], MW=consts["MW"])
         return tables

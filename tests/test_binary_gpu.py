@@ -124,3 +124,25 @@ def test_traces_beside_a_pure_species_match_the_oracle(sign):
     mb.rhs(Q="Q", dQ=dq)
     err = summand_err(mb, orc, dq)
     assert np.all(np.isfinite(err)) and err.max() < 5e-10, err
+
+
+def test_herning_viscosity_matches_the_oracle():
+    # Herning's mixing rule in place of Wilke's (peregrine/simulator/mixture/mixrule/herning.py)
+    import peregrine_b200 as pg
+    from oracle.oracle import Oracle
+
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", False)
+    cfg["mixture"]["mixing-rule"] = "herning"
+    cfg.validate()
+    mesh = cases.reacting_mesh(12, (2, 1, 1))
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    consts = mb.mixture.constants()
+    prims = cases.reacting_prims(mb.metrics, mb.mixture.spnames, consts["MW"], 12, seed=5, width=2.0, dT=600.0,
+                                 radicals=2e-3)
+    mb.set_prims(prims)
+    orc = Oracle(consts, mb.ns, "navier-stokes", mb.mesh_blocks, mb.metrics, "tvd-rk3", primary="hllc",
+                 recon="muscl", limiter="koren", eos="tpg", trans="kinetic-theory", mixrule="herning")
+    orc.set_prims(prims)
+    dq = mb.regs[-1]
+    mb.rhs(Q="Q", dQ=dq)
+    assert summand_err(mb, orc, dq).max() < 5e-10
