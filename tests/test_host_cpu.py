@@ -146,7 +146,8 @@ def _rank(rank, world, port, out):
 def test_two_ranks_report_the_slowest_time_and_the_whole_job():
     import torch.multiprocessing as mp
 
-    mgr = mp.Manager()
+    # the manager's server process spawned, as the ranks are: no fork of a threaded process
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_rank, args=(2, _free_port(), out), nprocs=2, join=True)
     assert out[0] == out[1]
