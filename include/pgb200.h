@@ -310,6 +310,14 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
 /* The right-hand side dQ of logical register q into logical register dq, on
  * the per-block path (halo exchange included).  Returns when queued. */
 int pgb_rhs(pgb_case *c, int q, int dq);
+/* The same right-hand side on a chosen path (the reference's Solver.rhs,
+ * peregrine/multiblock/solver.py:270-273): PGB_PATH_PER_BLOCK as pgb_rhs,
+ * PGB_PATH_PACKED the same kernels one launch a pass, PGB_PATH_BATCHED the
+ * fused stage kernel itself with one combine dQ = 1 x dt x dQ at dt = 1 (the
+ * halo fill of q, then one launch; PGB_ERR_UNSUPPORTED for a case the fused
+ * kernel does not take).  The batched form keeps no eos state array.
+ * Returns when queued. */
+int pgb_rhs_path(pgb_case *c, int q, int dq, int path);
 /* stage n's combines on the registers as they are, dt the last set or
  * stepped (the reference's Solver.advance, peregrine/multiblock/solver.py:276-280) */
 int pgb_advance(pgb_case *c, int n);
@@ -373,25 +381,28 @@ int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);
  * its backend.  For callers that may not call cudaMalloc or any allocating
  * library routine (torch's allocator included): code living in another
  * framework's memory pool or a fixed arena, or a host application that owns
- * all device memory.  The caller passes device arrays, all F order with the
- * case layout's halo of two cells (full extents nx+4, ny+4, nz+4, i fastest,
- * components outermost):
+ * all device memory.  The caller passes Q, met and dQ as device arrays, all
+ * F order with the case layout's halo of two cells (full extents nx+4, ny+4,
+ * nz+4, i fastest, components outermost):
  *   Q    ne = 4 + ns components, its halo filled by the caller (two layers on
  *        every face, the first layer of every edge);
  *   met  31 components: xcc (3), detJinv (1), Jinv (9, row-major), iS, jS,
  *        kS (3 each), ixc, jxc, kxc (3 each); a face of axis a is stored at
  *        the index of the cell on its high side;
  *   dQ   ne components; the interior is written, the halo left alone.
- * tables: Rsp, cp0, h298R, MWinv, hpoly0, h298, mu0, kappa0, MWqinv, lewis
- * (ns each), then wilkepair (ns x ns, row-major).  The work goes on stream (a
- * cudaStream_t; NULL for the default stream) and is queued when the call
- * returns.  The scratch is one static device array of 16 MiB that every GPU
- * loading the library holds until exit; a block larger than
- * pgb_rhs_block_noalloc_max_cells(ns) cells (halo included; 53,773 for one
+ * tables, a HOST array read during the call: Rsp, cp0, h298R, MWinv, hpoly0,
+ * h298, mu0, kappa0, MWqinv, lewis (ns each), then wilkepair (ns x ns,
+ * row-major).  The simulator is euler or navier-stokes, the gas calorically
+ * perfect with one to three species, the flux kepaec.  The work goes on
+ * stream (a cudaStream_t; NULL for the default stream) and is queued when the
+ * call returns.  The scratch is one static device array of 16 MiB that every
+ * GPU loading the library holds until exit; a block larger than
+ * pgb_rhs_block_noalloc_max_cells(ns) cells (halo included; 52,428 for one
  * species, room for 32^3 interior cells) is refused with PGB_ERR_ARG.  The
  * first call on a device looks up the array's device address, so make it
- * before any stream capture.  Every call uses the same array: calls that
- * overlap on the GPU race, so keep them ordered on one stream. */
+ * before any stream capture.  Every call uses the same array and the same
+ * species constants: calls that overlap on the GPU race on both, so keep
+ * them ordered on one stream. */
 int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tables, int nx, int ny, int nz, const double *Q,
                           const double *met, double *dQ, void *stream);
 long long pgb_rhs_block_noalloc_max_cells(int ns);

@@ -115,6 +115,7 @@ struct pgb_case {
   double *d_reg[MAXREGS] = {};
   double *d_met = nullptr;
   double *d_dt = nullptr;
+  double *d_one = nullptr;  // 1.0: the step size of a right-hand side on the fused path
   HaloEntry *d_halo = nullptr;
   long long nhalo = 0, nhalo_l0 = 0;  // all entries; face layer 0 only (first)
   // the rotationally periodic faces' rotations, then the products a halo
@@ -330,30 +331,59 @@ int build_species(pgb_case *c) {
 
 // which case's tables each species count's unit holds, so a case's repeated
 // launches upload nothing
+// The owner is the case (or pool) whose launches were queued last against
+// the tables: its stream is where launches that read them may still be
+// waiting.
 struct Uploaded {
   unsigned long long uid = 0;
   unsigned version = 0;
   int device = -1;
-  bool same(const pgb_case *c, int dev) const { return uid == c->uid && version == c->version && device == dev; }
-  void set(const pgb_case *c, int dev) { uid = c->uid, version = c->version, device = dev; }
+  cudaStream_t stream = nullptr;
+  bool same(unsigned long long id, unsigned ver, int dev) const { return uid == id && version == ver && device == dev; }
 };
 Uploaded g_host_up, g_plain_up[MAXNS];
 unsigned long long g_next_uid = 0;
 
+// A new owner's upload must not land while the previous owner's queued
+// launches can still read the tables: the new owner's stream waits for an
+// event marking everything the previous owner's stream holds now.  The
+// previous owner, taking the tables back later, waits the same way.
+int take_tables(Uploaded &u, unsigned long long id, unsigned ver, int dev, cudaStream_t to) {
+  if (u.stream && u.device == dev && u.stream != to) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t r = cudaEventRecord(e, u.stream);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(to, e, 0);
+    cudaEventDestroy(e);  // released once it completes
+    if (r != cudaSuccess) return fail(PGB_ERR_CUDA, std::string("table handover: ") + cudaGetErrorString(r));
+  }
+  u.uid = id, u.version = ver, u.device = dev, u.stream = to;
+  return PGB_OK;
+}
+
+// a stream about to be destroyed (its work done) owns nothing any more
+void forget_stream(cudaStream_t s) {
+  if (g_host_up.stream == s) g_host_up.stream = nullptr;
+  for (Uploaded &u : g_plain_up)
+    if (u.stream == s) u.stream = nullptr;
+}
+
 int set_current(pgb_case *c) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  if (!g_host_up.same(c, dev)) {
+  if (!g_host_up.same(c->uid, c->version, dev)) {
+    RET(take_tables(g_host_up, c->uid, c->version, dev, c->stream));
     CK(cudaMemcpyToSymbolAsync(kSp, &c->sp, sizeof(Species), 0, cudaMemcpyHostToDevice, c->stream));
-    g_host_up.set(c, dev);
+  } else if (g_host_up.stream != c->stream) {
+    g_host_up.stream = c->stream;
   }
   Uploaded &u = g_plain_up[c->phys.ns - 1];
-  if (!u.same(c, dev)) {
+  if (!u.same(c->uid, c->version, dev)) {
     static MathTables mt;
     static bool filled = false;
     if (!filled) math_tables_fill(mt), filled = true;
+    RET(take_tables(u, c->uid, c->version, dev, c->stream));
     RET(kPlain[c->phys.ns - 1].upload(&c->sp, c->mech.get(), c->mech ? &mt : nullptr, c->stream));
-    u.set(c, dev);
   }
   return PGB_OK;
 }
@@ -766,8 +796,9 @@ const void *v2_kernel(const pgb_case *c) {
   return c->phys.simulator == PGB_NAVIER_STOKES ? kV2[c->v2].fvisc : kV2[c->v2].feuler;
 }
 
-// one stage of the fused path
-int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &count) {
+// one stage of the fused path; dtp, when given, the step size the combines read
+// in place of the case's
+int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &count, const double *dtp = nullptr) {
   FusedArgs a{};
   a.blks = c->d_blks;
   a.tiles = c->d_tiles;
@@ -822,7 +853,7 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
     a.write[m] = cb.write;
   }
   for (int q = 0; q < 2; q++) a.prep[q] = q < a.npre ? c->d_reg[a.pre[q]] : nullptr;
-  a.dt = c->d_dt;
+  a.dt = dtp ? dtp : c->d_dt;
   // the stencil register's halo first
   k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne, 1, c->d_rots);
   mark(c, K_HALO, count);
@@ -904,6 +935,26 @@ int step_fused(pgb_case *c, int &count) {
   c->phase = (c->phase + 1) % c->period;
   c->phys_of = c->maps[c->phase];
   return PGB_OK;
+}
+
+// The right-hand side alone on the fused path: the stage kernel with one
+// combine, out = 1 x dt x dQ at dt = 1 (no register term, the fixed form's
+// other weights zero), so it writes exactly the dQ it forms.  The halo fill
+// of q comes first, as in a stage.
+int rhs_fused(pgb_case *c, int qphys, int dqphys, int &count) {
+  FusedStagePlan p{};
+  p.qin = qphys;
+  p.ncomb = 1;
+  FusedCombine &f = p.comb[0];
+  f.step = 1;
+  f.nterms = 1;
+  f.src[0] = -1;
+  f.w[0] = 1.0;
+  f.out = dqphys;
+  f.write = 1;
+  c->state_stale = true;
+  CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), c->stream));
+  return launch_fused(c, p, 0, count, c->d_one);
 }
 
 // the per-cell state, kept between right-hand sides: an iterative eos starts
@@ -1236,7 +1287,7 @@ int pgb_case_destroy(pgb_case *c) {
     if (g) cudaGraphExecDestroy(g);
   for (auto &r : c->d_reg)
     if (r) cudaFree(r);
-  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
+  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_one, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
                   c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots};
@@ -1245,7 +1296,7 @@ int pgb_case_destroy(pgb_case *c) {
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream) forget_stream(c->stream), cudaStreamDestroy(c->stream);
   delete c;
   return PGB_OK;
 }
@@ -1609,6 +1660,9 @@ int pgb_case_finalize(pgb_case *c) {
   CK(cudaMemsetAsync(c->d_dt, 0, sizeof(double), c->stream));
   CK(cudaMalloc(&c->d_clock, sizeof(double)));
   CK(cudaMemsetAsync(c->d_clock, 0, sizeof(double), c->stream));
+  CK(cudaMalloc(&c->d_one, sizeof(double)));
+  k_setscalar<<<1, 1, 0, c->stream>>>(c->d_one, 1.0);
+  CK(cudaGetLastError());
   CK(cudaMalloc(&c->d_cfl, sizeof(double) * 3));
   CK(cudaMemsetAsync(c->d_cfl, 0, sizeof(double) * 3, c->stream));
   CK(cudaMalloc(&c->d_ctrl, sizeof(double) * 2));
@@ -1798,6 +1852,27 @@ int pgb_rhs(pgb_case *c, int q, int dq) {
   // the double flux's planes, frozen once after the state was set
   RET(df_settle(c, c->phys_of[q]));
   RET(rhs_plain(c, c->phys_of[q], c->phys_of[dq], count));
+  return PGB_OK;
+}
+
+int pgb_rhs_path(pgb_case *c, int q, int dq, int path) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (path < PGB_PATH_BATCHED || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "no such path");
+  if (path != PGB_PATH_BATCHED) {
+    struct Packed {
+      pgb_case *c;
+      ~Packed() { c->packed = false; }
+    } unpack{c};
+    c->packed = path == PGB_PATH_PACKED;
+    return pgb_rhs(c, q, dq);
+  }
+  if (!fused_capable(c)) return fail(PGB_ERR_UNSUPPORTED, "the batched path does not take this case");
+  if (q < 0 || q >= c->phys.nregs || dq < 0 || dq >= c->phys.nregs || q == dq)
+    return fail(PGB_ERR_ARG, "bad registers");
+  RET(prepare(c, true));
+  int count = 0;
+  RET(rhs_fused(c, c->phys_of[q], c->phys_of[dq], count));
+  CK(cudaGetLastError());
   return PGB_OK;
 }
 
@@ -2161,13 +2236,13 @@ int pool_current(pgb_pool *p) {
   CK(cudaGetDevice(&dev));
   Uploaded &u = g_plain_up[p->phys.ns - 1];
   // a pool's tables share the units' constant memory with the cases: keyed
-  // by the pool's own unique id
-  if (u.uid != p->uid || u.version != p->version || u.device != dev) {
+  // by the pool's own unique id, handed over as a case's are
+  if (!u.same(p->uid, p->version, dev)) {
     static MathTables mt;
     static bool filled = false;
     if (!filled) math_tables_fill(mt), filled = true;
+    RET(take_tables(u, p->uid, p->version, dev, p->stream));
     RET(kPlain[p->phys.ns - 1].upload(&p->sp, p->mech.get(), p->mech ? &mt : nullptr, p->stream));
-    u.uid = p->uid, u.version = p->version, u.device = dev;
   }
   return PGB_OK;
 }
@@ -2376,7 +2451,7 @@ int pgb_pool_destroy(pgb_pool *p) {
     if (q) cudaFree(q);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
-  if (p->stream) cudaStreamDestroy(p->stream);
+  if (p->stream) forget_stream(p->stream), cudaStreamDestroy(p->stream);
   delete p;
   return PGB_OK;
 }

@@ -3,9 +3,8 @@
 //
 // Who needs it: a caller that may not call cudaMalloc, or any routine that
 // allocates device memory (torch's caching allocator included): code running
-// inside another framework's memory pool or a fixed arena, a solver embedded
-// in a host application that owns all device memory, or code whose
-// allocations would break an ongoing CUDA graph capture.  The case API
+// inside another framework's memory pool or a fixed arena, or a solver
+// embedded in a host application that owns all device memory.  The case API
 // (pgb_case_finalize) allocates its registers, metrics and scratch; this call
 // takes the caller's input and output arrays and keeps its scratch in a
 // static device array instead.
@@ -19,9 +18,10 @@
 // file-scope array below, of fixed size; every GPU that loads the library
 // holds it until the process exits.  Every scratch value is written before
 // it is read within one call, so nothing needs clearing; the array keeps the
-// last call's contents.  All calls share the one array, so calls whose work
-// overlaps on the GPU (two streams, two host threads) race and give wrong
-// results: keep them ordered on one stream.
+// last call's contents.  All calls share the one array, and the species
+// constants each call copies into this file's constant memory, so calls whose
+// work overlaps on the GPU (two streams, two host threads) race on both and
+// give wrong results: keep them ordered on one stream.
 #include <mutex>
 #include <string>
 
@@ -32,10 +32,16 @@ using namespace pgb;
 
 namespace {
 
-// 2^21 doubles, 16 MiB: a block of up to (2^21 - 32) / (31 + 8 ns) cells
-// halo included, 53,773 for one species (32^3 cells with their halo of two)
+// 2^21 doubles, 16 MiB: a block of up to (2^21 - 32) / (32 + 8 ns) cells
+// halo included, 52,428 for one species (32^3 cells with their halo of two).
+// Per cell: the state's 8 fields and the real gas's Z plane the transport
+// kernel reads beside them (kept so no two of its arrays overlap), the
+// transport properties (2 + ns), the species enthalpies (ns), the gradients
+// (3 (ne - 1)) and the three axes' face fluxes (3 ne).
 constexpr long long kScratchDoubles = 1ll << 21;
 constexpr long long kHeadDoubles = 32;  // the block descriptor, 256 bytes
+constexpr long long kStatePlanes = ST_Z + 1;
+constexpr long long per_cell(int ns) { return kStatePlanes + (2 + ns) + ns + 3 * (3 + ns) + 3 * (4 + ns); }
 
 static __device__ __align__(256) double g_scratch[kScratchDoubles];
 
@@ -55,7 +61,7 @@ int fail(int code, const std::string &msg) { return pgb_internal_fail(code, msg.
 
 extern "C" long long pgb_rhs_block_noalloc_max_cells(int ns) {
   if (ns < 1 || ns > MAXNS) return 0;
-  return (kScratchDoubles - kHeadDoubles) / (31 + 8 * ns);
+  return (kScratchDoubles - kHeadDoubles) / per_cell(ns);
 }
 
 extern "C" int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tables, int nx, int ny, int nz,
@@ -63,6 +69,8 @@ extern "C" int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tabl
   if (!phys || !tables || !Q || !met || !dQ) return fail(PGB_ERR_ARG, "null argument");
   const int ns = phys->ns;
   if (ns < 1 || ns > 3) return fail(PGB_ERR_UNSUPPORTED, "one to three species");
+  if (phys->simulator != PGB_EULER && phys->simulator != PGB_NAVIER_STOKES)
+    return fail(PGB_ERR_UNSUPPORTED, "the euler or navier-stokes simulator");
   if (phys->eos != PGB_EOS_CPG || phys->primary != PGB_FLUX_KEPAEC || phys->recon != PGB_RECON_CONSTANT)
     return fail(PGB_ERR_UNSUPPORTED, "the calorically perfect gas with kepaec on the cells as they are");
   const bool visc = phys->simulator == PGB_NAVIER_STOKES;
@@ -71,7 +79,7 @@ extern "C" int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tabl
   if (nx < 2 || ny < 2 || nz < 2) return fail(PGB_ERR_ARG, "a block has at least two cells per axis");
   const long long X = nx + 2 * NG, Y = ny + 2 * NG, Z = nz + 2 * NG, V = X * Y * Z;
   const int ne = 4 + ns;
-  const long long need = kHeadDoubles + V * (8 + (2 + ns) + ns + 3 * (ne - 1) + 3 * ne);
+  const long long need = kHeadDoubles + V * per_cell(ns);
   if (need > kScratchDoubles)
     return fail(PGB_ERR_ARG, "block too large for the no-allocation scratch: at most " +
                                  std::to_string(pgb_rhs_block_noalloc_max_cells(ns)) +
@@ -112,7 +120,7 @@ extern "C" int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tabl
   if (e != cudaSuccess) return fail(PGB_ERR_CUDA, std::string("block descriptor: ") + cudaGetErrorString(e));
   const BlockDev *blks = (const BlockDev *)base;
   double *state = base + kHeadDoubles;
-  double *tr = state + 8 * V;
+  double *tr = state + kStatePlanes * V;
   double *hsp = tr + (2 + ns) * V;
   double *grads = hsp + ns * V;
   double *F[3];

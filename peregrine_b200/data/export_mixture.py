@@ -4,7 +4,7 @@ them, to an .npz that peregrine_b200 loads.
     python -m peregrine_b200.data.export_mixture REFERENCE OUT.npz MECHANISM \\
         [--keep H2,H,O,...] [--eos tpg] [--trans kinetic-theory] \\
         [--chemistry finite-rate] [--trange 300 3500] [--cubic srk|pr] \\
-        [--diffusion lewis|binary]
+        [--diffusion lewis|binary] [--oneway]
 
 MECHANISM is a mechanism file, or species of the reference's library
 separated by commas.
@@ -113,13 +113,16 @@ def _species_of(equation):
     return out
 
 
-def subset(mechanism, keep, where):
-    """A Cantera-format mechanism cut to the species in keep, written under where."""
+def subset(mechanism, keep, where, oneway=False):
+    """A Cantera-format mechanism cut to the species in keep (every species
+    when keep is None), written under where; with oneway every reaction
+    irreversible, "<=>" written "=>" (the parser's irreversible arrow,
+    peregrine/simulator/mixture/parser/base.py:90-95)."""
     import yaml
 
     with open(mechanism) as f:
         src = yaml.safe_load(f)
-    keep = list(keep)
+    keep = list(keep) if keep is not None else [s["name"] for s in src["species"]]
     phase = dict(src["phases"][0], species=keep)
     reactions = []
     for r in src["reactions"]:
@@ -127,6 +130,8 @@ def subset(mechanism, keep, where):
             r = dict(r)
             if "efficiencies" in r:
                 r["efficiencies"] = {k: v for k, v in r["efficiencies"].items() if k in keep}
+            if oneway:
+                r["equation"] = r["equation"].replace("<=>", "=>")
             reactions.append(r)
     out = dict(units=src["units"], phases=[phase], species=[s for s in src["species"] if s["name"] in keep],
                reactions=reactions)
@@ -199,6 +204,7 @@ def main(argv=None):
     ap.add_argument("--trange", nargs=2, type=float, default=(300.0, 3500.0))
     ap.add_argument("--cubic", default="srk", choices=sorted(CUBICS))
     ap.add_argument("--diffusion", default="lewis", choices=("lewis", "binary"))
+    ap.add_argument("--oneway", action="store_true", help="every reaction irreversible")
     a = ap.parse_args(argv)
     mech = a.mechanism
     if "," in mech:
@@ -207,8 +213,8 @@ def main(argv=None):
     elif not os.path.isfile(mech):
         mech = os.path.join(a.reference, "peregrine", "simulator", "mixture", "database", "mechanisms", mech)
     with tempfile.TemporaryDirectory() as tmp:
-        if a.keep and isinstance(mech, str):
-            mech = subset(mech, a.keep.split(","), tmp)
+        if (a.keep or a.oneway) and isinstance(mech, str):
+            mech = subset(mech, a.keep.split(",") if a.keep else None, tmp, oneway=a.oneway)
         mix = reference_mixture(a.reference, mech, a.eos, a.trans, a.chemistry, a.trange, a.cubic, a.diffusion)
         np.savez(a.out, **tables(mix))
     print(a.out, mix)

@@ -291,9 +291,12 @@ class Solver:
     def prerhs(self, Q="Q", dQ=None):
         """Register Q readied for reading: its halo, state and boundary halo
         cells formed (peregrine/multiblock/solver.py:246-250).  The library
-        forms them in a right-hand side, into dQ (the last register unless
-        named), as the reference's prerhs begins dQ."""
-        self.rhs(Q=Q, dQ=dQ)
+        forms them in a right-hand side of the per-block kernels, which keep
+        the state array, into dQ (the last register unless named), as the
+        reference's prerhs begins dQ."""
+        if self.has_bcs:
+            native.call("pgb_set_time", self.case, float(self.tme))
+        native.call("pgb_rhs", self.case, self.regnum[Q], self.regnum[dQ or self.regs[-1]])
 
     def postrhs(self, Q=None):
         """Register Q (the solution unless named) readied after it was written
@@ -311,10 +314,13 @@ class Solver:
         native.call("pgb_exchange", self.case, self.regnum[Q])
 
     def rhs(self, *, Q="Q", dQ=None):
+        """dQ of register Q on the case's path: on the batched path the fused
+        stage kernel itself, writing the dQ it forms (at unit step and no
+        register term), on the others the per-block kernels."""
         dQ = dQ or self.regs[-1]
         if self.has_bcs:
             native.call("pgb_set_time", self.case, float(self.tme))
-        native.call("pgb_rhs", self.case, self.regnum[Q], self.regnum[dQ])
+        native.call("pgb_rhs_path", self.case, self.regnum[Q], self.regnum[dQ], self.path)
 
     def step(self, dt, nsteps=1):
         # the boundaries read the clock from the step's start on

@@ -1,6 +1,9 @@
 """Generates the golden fixtures of tests/golden from the reference itself.
 
-    python tests/golden/make_golden.py [path to the reference checkout]
+    python tests/golden/make_golden.py REFERENCE [FIXTURE ...]
+
+REFERENCE is the path of a checkout of the reference; with FIXTURE names
+(the file names below without their extension) only those are rewritten.
 
 Run here, where the reference's Python can be imported; the fixtures it
 writes (*.npz, *.json) are committed, and nothing at test time reads the
@@ -28,7 +31,11 @@ What it records, each from the reference's own code:
                      form) on random states of the 9-species H2/O2/N2 subset of
                      GRI-Mech 3.0 and of CH4_O2_FFCMY, with the reference's
                      Gibbs functions, and the species' cp and h by the
-                     reference's own polynomial evaluation.
+                     reference's own polynomial evaluation;
+  rates_h2o2_gri30_oneway.npz  the same for the H2/O2/N2 subset with every
+                     reaction irreversible (the reference's one-way twin,
+                     tests/mixture/rates.py:195-202, as a mechanism file), where
+                     no reverse rate cancels a forward one;
 
   binary_h2o2.npz    peregrine/simulator/mixture/diffusion/binary.py's pair
                      coefficients T^(3/2) / D at unit pressure for the
@@ -52,7 +59,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = None
 
 
 def stub(name, **attrs):
@@ -195,15 +202,15 @@ def mathfns():
                 xexp=xe, texp=rates.texp(xe))
 
 
-def rates_of(reference, mech, keep, n, rng):
+def rates_of(reference, mech, keep, n, rng, oneway=False):
     from peregrine_b200.data.export_mixture import reference_mixture, subset
     from tests.mixture import rates
     import tempfile
 
     path = os.path.join(reference, "peregrine", "simulator", "mixture", "database", "mechanisms", mech)
     with tempfile.TemporaryDirectory() as tmp:
-        if keep:
-            path = subset(path, keep, tmp)
+        if keep or oneway:
+            path = subset(path, keep, tmp, oneway=oneway)
         mix = reference_mixture(reference, path, "tpg", "kinetic-theory", "finite-rate")
     ns = mix.ns
     rho, T, Y, omega, gRT = [], [], [], [], []
@@ -316,6 +323,11 @@ def rk_tables(integrators):
 
 
 def main():
+    global REF
+    if len(sys.argv) < 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: make_golden.py REFERENCE [FIXTURE ...]  (REFERENCE: a checkout of the reference)")
+    REF = sys.argv[1]
+    only = set(sys.argv[2:])
     install_stubs()
     sys.path.insert(0, REF)
     import peregrine as pg
@@ -324,6 +336,18 @@ def main():
     from peregrine.simulator.mixture import get_mixture
     from tests.simulator import oracle as orc
 
+    h2o2 = ["H2", "H", "O", "O2", "OH", "H2O", "HO2", "H2O2", "N2"]
+    if only:
+        air_tgv()  # puts this package on the path, as the full run does
+        # fixtures that draw from their own seeds, one at a time
+        single = {"rates_h2o2_gri30_oneway": lambda: rates_of(REF, "GRI30.yaml", h2o2, 96,
+                                                              np.random.default_rng(20261209), oneway=True)}
+        for name in only:
+            if name not in single:
+                sys.exit(f"{name}: not a fixture written alone ({sorted(single)})")
+            np.savez(os.path.join(HERE, name + ".npz"), **single[name]())
+            print("wrote", name)
+        return
     rng = np.random.default_rng(20261203)
     air = air_tgv()
     np.savez(os.path.join(HERE, "faces_kepaec.npz"),
@@ -338,11 +362,12 @@ def main():
     binary = {k: dict(MW=v["MW"], cp0=v["cp0"]) for k, v in BINARY.items()}
     np.savez(os.path.join(HERE, "faces_riemann.npz"), **faces4(orc, binary, 256, np.random.default_rng(20261204)))
     np.savez(os.path.join(HERE, "mathfns.npz"), **mathfns())
-    h2o2 = ["H2", "H", "O", "O2", "OH", "H2O", "HO2", "H2O2", "N2"]
     np.savez(os.path.join(HERE, "rates_h2o2_gri30.npz"),
              **rates_of(REF, "GRI30.yaml", h2o2, 96, np.random.default_rng(20261206)))
     np.savez(os.path.join(HERE, "rates_ch4_o2_ffcmy.npz"),
              **rates_of(REF, "CH4_O2_FFCMY.yaml", None, 96, np.random.default_rng(20261207)))
+    np.savez(os.path.join(HERE, "rates_h2o2_gri30_oneway.npz"),
+             **rates_of(REF, "GRI30.yaml", h2o2, 96, np.random.default_rng(20261209), oneway=True))
     np.savez(os.path.join(HERE, "binary_h2o2.npz"), **binary_pairs(REF))
     for cubic in ("srk", "pr"):
         np.savez(os.path.join(HERE, f"realgas_{cubic}.npz"),

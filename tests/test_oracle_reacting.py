@@ -7,7 +7,8 @@ tests/mixture/rates.py), its production rates in the kernels' form
 (tests/mixture/rates.py:169-185), its Gibbs functions
 (peregrine/simulator/mixture/eos/base.py:62-67) and the species' cp and h by
 its own polynomial evaluation, for the 9-species H2/O2/N2 subset of GRI-Mech
-3.0 and for CH4_O2_FFCMY.  The mixtures' tables come from
+3.0, the same subset with every reaction irreversible (the reference's
+one-way twin), and CH4_O2_FFCMY.  The mixtures' tables come from
 peregrine_b200/data, written by the reference's mixture code.  Bars are the
 reference's: 3e-14 of the largest rate for the rates against the numpy twin
 (tests/chemint/test_rates.py:34-35), bit for bit for the tables.
@@ -87,7 +88,7 @@ def test_species_cp_and_h_match_the_references_fits(mech):
         assert np.all(np.abs(h - g["hR"][:, n] * Rsp) <= 16 * np.finfo(float).eps * hmag)
 
 
-@pytest.mark.parametrize("mech", MECHS)
+@pytest.mark.parametrize("mech", MECHS + ["h2o2_gri30_oneway"])
 def test_production_rates_match_the_references_numpy_twin(mech):
     g = gold(f"rates_{mech}.npz")
     _, o = reacting(mech)
@@ -95,9 +96,11 @@ def test_production_rates_match_the_references_numpy_twin(mech):
     want = g["omega"]
     for q in range(len(want)):
         scale = np.abs(want[q]).max()
-        assert np.abs(got[q] - want[q]).max() < 3e-14 * scale, q
+        # (a state whose present species react with nothing has every rate
+        # exactly zero on both sides)
+        assert np.abs(got[q] - want[q]).max() <= 3e-14 * scale, q
     # mass is conserved: the rates sum to nothing
-    assert np.all(np.abs(got.sum(axis=1)) < 1e-12 * np.abs(want).max(axis=1))
+    assert np.all(np.abs(got.sum(axis=1)) <= 1e-12 * np.abs(want).max(axis=1))
 
 
 def test_tpg_converges_from_cold_starts():
@@ -144,3 +147,19 @@ def prims_to_Q(o, q):
     Tg = np.zeros(len(q))
     o.lib.oracle_fromprims(orc.ctypes.byref(o.case), orc._ptr(q), orc._ptr(Q), orc.ctypes.c_long(len(q)), orc._ptr(Tg))
     return Q
+
+
+def test_the_oneway_mechanism_is_the_mechanism_without_its_reverse_rates():
+    # the one-way twin's columns are the mechanism's, every reaction
+    # irreversible; its rates are the forward halves of the mechanism's
+    a, b = load_tables("h2o2_gri30"), load_tables("h2o2_gri30_oneway")
+    assert not b["rxn_reversible"].any() and a["rxn_reversible"].all()
+    for k in ("rxn_logA", "rxn_b", "rxn_EaR", "rxn_netnuMW", "rxn_netsp", "gpoly"):
+        assert np.array_equal(a[k], b[k]), k
+    g = gold("rates_h2o2_gri30_oneway.npz")
+    _, o = reacting("h2o2_gri30_oneway")
+    got = o.production(g["rho"], g["Y"], g["T"])
+    _, two = reacting("h2o2_gri30")
+    both = two.production(g["rho"], g["Y"], g["T"])
+    # no reverse rate cancels a forward one: the one-way rates differ
+    assert np.abs(got - both).max() > 1e-3 * np.abs(got).max()

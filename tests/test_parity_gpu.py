@@ -8,6 +8,7 @@ steps 1e-9, conservation to rounding.
 
 import numpy as np
 import pytest
+from totals import totals
 
 from peregrine_b200 import cases
 from peregrine_b200 import native
@@ -44,10 +45,16 @@ def interiors(mb, arrays):
     return [a[b.interior] for a, b in zip(arrays, mb.mesh_blocks)]
 
 
+@pytest.mark.parametrize("launch", ["batched", "per-block", "packed"])
 @pytest.mark.parametrize("jostle", [False, True])
 @pytest.mark.parametrize("simulator", ["euler", "navier-stokes"])
-def test_rhs_matches_oracle(simulator, jostle):
-    mb, orc = build(simulator, cells=16, blocks=(2, 2, 1), jostle=jostle)
+def test_rhs_matches_oracle(simulator, jostle, launch):
+    # on the batched path the right-hand side is the fused stage kernel's own
+    # (the uniform-metric kernel on the even grid, the metric-array kernel on
+    # the jostled one), written at unit step with no register term
+    mb, orc = build(simulator, cells=16, blocks=(2, 2, 1), jostle=jostle, launch=launch)
+    assert mb.path == {"batched": native.PATH_BATCHED, "per-block": native.PATH_PER_BLOCK,
+                       "packed": native.PATH_PACKED}[launch]
     dq = mb.regs[-1]
     mb.rhs(Q="Q", dQ=dq)
     got = [getattr(b, dq).get() for b in mb.blocks]
@@ -55,6 +62,8 @@ def test_rhs_matches_oracle(simulator, jostle):
     orc.rhs(orc.regs[0], want)
     for g, w in zip(interiors(mb, got), interiors(mb, want)):
         assert rowmax_err(g, w) < RHS_TOL
+    if launch == "batched":
+        assert all(mb.uniform(n) != jostle for n in range(len(mb.blocks)))
 
 
 @pytest.mark.parametrize("jostle", [False, True])
@@ -86,18 +95,11 @@ def test_batched_equals_per_block():
 def test_mass_is_conserved():
     mb, _ = build("navier-stokes", "rk4", cells=16, blocks=(2, 2, 2), low=6, high=10)
 
-    def totals():
-        s = 0.0
-        for b, m in zip(mb.blocks, mb.metrics):
-            vol = 1.0 / m["detJinv"][b.mesh.interior]
-            s = s + (b.Q.get()[b.mesh.interior] * vol[..., None]).sum(axis=(0, 1, 2))
-        return s
-
-    before = totals()
+    before = totals(mb)
     mb.step(1e-5, 10)
-    after = totals()
-    assert abs(after[0] - before[0]) <= 1e-13 * abs(before[0])
-    assert abs(after[4] - before[4]) <= 1e-13 * abs(before[4])
+    after = totals(mb)
+    assert abs(after[0] - before[0]) <= 1e-14 * abs(before[0])
+    assert abs(after[4] - before[4]) <= 1e-14 * abs(before[4])
 
 
 @pytest.mark.parametrize("jostle", [False, True])
@@ -171,20 +173,20 @@ def test_the_tgv_after_100_steps_matches_the_oracle():
     orc.set_prims(prims)
     _, g = cases.tgv_gas()
     dt = 0.3 * (2 * np.pi / 32) / (g["U0"] + np.sqrt(g["gamma"] * g["R"] * cases.T0))
-    vol = 1.0 / mb.metrics[0]["detJinv"][mb.mesh_blocks[0].interior]
-    start = (mb.blocks[0].Q.get()[mb.mesh_blocks[0].interior] * vol[..., None]).sum(axis=(0, 1, 2))
+    start = totals(mb)
     mb.step(dt, 100)
     for _ in range(100):
         orc.step(dt)
     got = mb.blocks[0].Q.get()[mb.mesh_blocks[0].interior]
     want = orc.regs[0][0][mb.mesh_blocks[0].interior]
     assert rowmax_err(got, want) < STATE_TOL
-    # each cell's update rounds once per stage, so the totals drift like a
-    # random walk over 32768 cells x 400 stages: sqrt(1.3e7) x 1.1e-16 = 4e-13
-    # of the total; the bar is ten times that
-    end = (got * vol[..., None]).sum(axis=(0, 1, 2))
-    assert abs(end[0] - start[0]) <= 5e-12 * abs(start[0])
-    assert abs(end[4] - start[4]) <= 5e-12 * abs(start[4])
+    # the face fluxes cancel pair by pair, so the exact totals move only by
+    # each cell's rounding of its update, of random sign: over 32768 cells x
+    # 400 stages about 1e-16 / sqrt(32768 / 400) of the total; the bar is far
+    # above that and far below any flux a face gave one side and not the other
+    end = totals(mb)
+    assert abs(end[0] - start[0]) <= 1e-14 * abs(start[0])
+    assert abs(end[4] - start[4]) <= 1e-14 * abs(start[4])
 
 
 @pytest.mark.parametrize("integrator", ["tvd-rk3", "rk4"])
