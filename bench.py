@@ -27,7 +27,8 @@ stoichiometric H2/air at 1 atm and 1000 K with seeded Gaussian hot spots
 10 m/s); the 9-species H2/O2/N2 subset of GRI-Mech 3.0 (28 reactions,
 thermally perfect, kinetic-theory transport, coupled finite-rate chemistry),
 MUSCL with the koren limiter and HLLC, Navier-Stokes, TVD-RK3, on the
-per-block device path; with the CPU oracle on one stage of it beside it.
+batched path (the fused passes), with the per-block and packed paths and
+the CPU oracle on one stage of it beside it.
 
 A real-gas leg (key "realgas") times the transcritical mixing layer: 256 x
 128 x 4 cells of 20 um in 8 blocks of seeded uneven widths along i, O2 at
@@ -225,28 +226,51 @@ REACT_BYTES = 8 * 13 * 8 / 3
 
 
 def reacting_leg(steps, cpu=True):
-    """Cell-stage/s of the reacting configuration on the per-block path."""
+    """Cell-stage/s of the reacting configuration: the batched path (the fused
+    passes), with the per-block and packed paths beside it."""
     import peregrine_b200 as pg
-    from peregrine_b200 import cases
+    from peregrine_b200 import cases, native
 
-    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True, launch="per-block")
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True, launch="batched")
     mesh = cases.reacting_mesh(REACT_CELLS, (1, 1, 1))
     mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
     consts = mb.mixture.constants()
     prims = cases.reacting_prims(mb.metrics, mb.mixture.spnames, consts["MW"], REACT_CELLS, seed=SEED)
-    mb.set_prims(prims)
-    dt = 2e-8
-    mb.step(dt, 3)
-    mb.backend.sync()
-    ms = time_graph(mb, dt, steps)
     ncells = mb.ncells
-    value = ncells * REACT_STAGES * steps / (ms / 1e3)
-    out = {"value": value, "unit": "cell-stage/s", "steps": steps, "ms_per_step": ms / steps,
-           "launches_per_step": mb.launches_per_step(), "dt": dt,
+    dt = 2e-8
+    legs = {}
+    for path, name in ((native.PATH_PER_BLOCK, "per_block"), (native.PATH_PACKED, "packed"),
+                       (native.PATH_BATCHED, "batched")):
+        mb.set_prims(prims)
+        mb.path = path
+        mb.step(dt, 3)
+        mb.backend.sync()
+        ms = time_graph(mb, dt, steps)
+        legs[name] = {"value": ncells * REACT_STAGES * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                      "launches_per_step": mb.launches_per_step()}
+    # the batched path's launches by kind, timed by events between launches
+    kinds = {0: "halo fill", 1: "divergence and combines", 2: "face, gradient and source passes",
+             8: "cell pass (fromQ and transport)"}
+    rows = fused_kernel_times(mb, dt, 2)
+    share = {}
+    for k, label in kinds.items():
+        t = [m for m, kk in rows if kk == k]
+        if t:
+            share[label] = {"launches_per_step": len(t) // 2, "ms_per_step": float(np.sum(t)) / 2}
+    b = legs["batched"]
+    peak, peak_kind = peaks()
+    achieved = b["value"] * REACT_BYTES / 1e9
+    out = {"value": b["value"], "unit": "cell-stage/s", "steps": steps, "ms_per_step": b["ms_per_step"],
+           "launches_per_step": b["launches_per_step"], "dt": dt,
            "workload": "h2-air-96^3-9sp-28rxn-tpg-kinetic-coupled-chem-muscl-koren-hllc-ns-tvd-rk3",
-           "path": "per-block kernels, one launch per block and pass",
-           "algorithmic_bytes_per_cell_stage": REACT_BYTES,
-           "hbm_gbs_of_algorithmic_bytes": value * REACT_BYTES / 1e9}
+           "path": "batched: the fused passes (cell pass, source, gradients, a face pass per axis with the "
+                   "advective and diffusive flux in one thread, divergence and combines in one pass)",
+           "per_block": legs["per_block"], "packed": legs["packed"],
+           "speedup_vs_per_block": legs["per_block"]["ms_per_step"] / b["ms_per_step"],
+           "batched_launch_kinds": share,
+           "roofline": {"bound": "fp64 (see profiles); hbm fraction of the algorithmic bytes", "achieved": achieved,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                        "algorithmic_bytes_per_cell_stage": REACT_BYTES}}
     if cpu:
         from oracle.oracle import Oracle
 

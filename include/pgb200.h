@@ -346,8 +346,9 @@ int pgb_set_dt(pgb_case *c, double dt);
 
 /* nsteps steps without a graph, a CUDA event between every launch; waits for
  * them and returns each launch's device time (ms) and kind (0 halo fill,
- * 1 fused stage, 2 per-block kernel, 3 combine or clock, 4 boundary pass,
- * 5 CFL reduction, 6 sub-stepped chemistry's bulk pass, 7 its stiff pass) in
+ * 1 fused stage or the fused passes' tile kernel, 2 per-block kernel, 3
+ * combine or clock, 4 boundary pass, 5 CFL reduction, 6 sub-stepped
+ * chemistry's bulk pass, 7 its stiff pass, 8 the fused passes' cell pass) in
  * launch order, up to cap launches; n is the number of launches. */
 int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int *kind, int cap, int *n);
 
@@ -372,6 +373,17 @@ int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk);
  * ints each (threads, minblocks, width, height) */
 int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks, int width);
 int pgb_fused_shapes(int *shapes, int cap, int *n);
+
+/* The batched path's form for the case: 1 the fused stage kernel (the
+ * calorically perfect single-species gas with kepaec on the cells as they
+ * are), 2 the fused passes (any other ideal gas, flux function and
+ * reconstruction, inviscid or viscous, with or without the coupled
+ * chemistry: a cell pass and one tile kernel of every face, the divergence
+ * and the combines a stage), 0 neither (boundaries, the real gas, the double
+ * flux, the sub-stepped chemistry run the per-block kernels, packed).  No
+ * counterpart in the reference, whose every case runs its per-kernel launches
+ * (peregrine/simulator/advecdiff/simulator.py:110-124). */
+int pgb_case_batched_form(const pgb_case *c, int *form);
 
 /* whether blk runs in the uniform-metric form (1) or reads its metric arrays (0) */
 int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);
@@ -406,6 +418,11 @@ int pgb_block_uniform(const pgb_case *c, int blk, int *uniform);
 int pgb_rhs_block_noalloc(const pgb_physics *phys, const double *tables, int nx, int ny, int nz, const double *Q,
                           const double *met, double *dQ, void *stream);
 long long pgb_rhs_block_noalloc_max_cells(int ns);
+
+/* The device's FP64 fused multiply-add rate, TFLOP/s (two flops a DFMA),
+ * measured by independent FMA chains filling every SM: the denominator of the
+ * FP64 roofline.  No counterpart in the reference. */
+int pgb_fp64_fma_rate(double *tflops);
 
 /* ---- serving pool ----
  * No counterpart in the reference, which runs one case per solver.  A pool

@@ -2,8 +2,9 @@
 
     python -m peregrine_b200.build [--force]
 
-nvcc cross-compiles without a GPU.  The host unit, the no-allocation unit
-and one per-block unit per species count (plain_tu.cu with PGB_NS = 1..12)
+nvcc cross-compiles without a GPU.  The host unit, the no-allocation unit,
+the FP64 rate unit and one per-block unit per species count (plain_tu.cu
+with PGB_NS = 1..12)
 compile in parallel into objects under _build/, then link into one shared
 library.  The library is built in-tree so it travels with the source to
 wherever it runs.
@@ -19,7 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 MAXNS = 12
-SOURCES = [os.path.join(CSRC, f) for f in ("pgb_host.cu", "pgb_noalloc.cu", "plain_tu.cu")]
+SOURCES = [os.path.join(CSRC, f) for f in ("pgb_host.cu", "pgb_noalloc.cu", "plain_tu.cu", "fp64_peak.cu")]
 HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cuh", ".h"))] + \
           [os.path.join(ROOT, "include", "pgb200.h")]
 TARGET = os.path.join(HERE, "libpgb200.so")
@@ -31,7 +32,8 @@ FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{os
 def units():
     """(source, object, extra flags) of every translation unit."""
     out = [(os.path.join(CSRC, "pgb_host.cu"), os.path.join(OBJ, "pgb_host.o"), []),
-           (os.path.join(CSRC, "pgb_noalloc.cu"), os.path.join(OBJ, "pgb_noalloc.o"), [])]
+           (os.path.join(CSRC, "pgb_noalloc.cu"), os.path.join(OBJ, "pgb_noalloc.o"), []),
+           (os.path.join(CSRC, "fp64_peak.cu"), os.path.join(OBJ, "fp64_peak.o"), [])]
     for n in range(1, MAXNS + 1):
         out.append((os.path.join(CSRC, "plain_tu.cu"), os.path.join(OBJ, f"plain_ns{n}.o"), [f"-DPGB_NS={n}"]))
     return out

@@ -38,7 +38,7 @@ PGB_PLAIN_DECL(12)
 namespace {
 #define PGB_OPS(N)                                                                                          \
   {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N, pgb_plain_prestep_##N, \
-   pgb_plain_cflmax_##N}
+   pgb_plain_cflmax_##N, pgb_plain_fused_##N}
 // the per-block path of each species count, 1 to MAXNS
 const PlainOps kPlain[MAXNS] = {PGB_OPS(1), PGB_OPS(2), PGB_OPS(3), PGB_OPS(4),  PGB_OPS(5),  PGB_OPS(6),
                                 PGB_OPS(7), PGB_OPS(8), PGB_OPS(9), PGB_OPS(10), PGB_OPS(11), PGB_OPS(12)};
@@ -91,9 +91,12 @@ struct HostBlock {
   BlockDev dev{};
 };
 
-// a stage's launch plan on the fused path, physical registers resolved
+// a stage's launch plan on the fused path, physical registers resolved: the
+// register the stage reads, the buffer dQ's logical register names at the
+// stage's start (the fused passes' source lands there), the combines
 struct FusedStagePlan {
   int qin;
+  int dqbuf;
   int ncomb;
   FusedCombine comb[2];
 };
@@ -134,6 +137,8 @@ struct pgb_case {
   bool tiles_dirty = true;
   bool uniform_done = false;
   bool use_v2 = false;  // every block uniform: the uniform-metric fused kernel
+  int form = 0;         // the batched path's form: 1 the fused stage kernel, 2 the fused passes
+
   int v2_ctas = 1;      // its resident CTAs per SM
   int v2 = 0;           // its instance: threads per CTA, launch bound, tile layout
   // register mapping: logical -> physical
@@ -192,18 +197,30 @@ namespace {
 inline bool sim_visc(int s) { return s == PGB_NAVIER_STOKES || s == PGB_NAVIER_STOKES_DF; }
 inline bool sim_df(int s) { return s == PGB_EULER_DF || s == PGB_NAVIER_STOKES_DF; }
 
-bool fused_capable(const pgb_case *c) {
+// The batched path's form for a case: 1, the fused stage kernel (the
+// calorically perfect single-species gas, kepaec on the cells as they are,
+// inviscid or with constant transport); 2, the fused passes (any other ideal
+// gas, flux function and reconstruction, inviscid or viscous, with or without
+// the coupled chemistry source); 0, neither (boundaries, the real gas, the
+// double flux, the sub-stepped chemistry: the per-block kernels, packed).
+int batched_form(const pgb_case *c) {
   const pgb_physics &p = c->phys;
-  // the batched kernel's halo is the periodic or block-to-block fill alone,
-  // and its tiles and stencil take blocks of two cells or more per axis
+  // the batched kernels' halo is the periodic or block-to-block fill alone,
+  // and their tiles and stencil take blocks of two cells or more per axis
   for (const HostBlock &B : c->blocks) {
-    if (B.nx < 2 || B.ny < 2 || B.nz < 2) return false;
+    if (B.nx < 2 || B.ny < 2 || B.nz < 2) return 0;
     for (int f = 0; f < 6; f++)
-      if (B.bc[f] >= 0) return false;
+      if (B.bc[f] >= 0) return 0;
   }
-  return p.eos == PGB_EOS_CPG && p.primary == PGB_FLUX_KEPAEC && p.recon == PGB_RECON_CONSTANT && p.ns == 1 &&
-         (p.simulator == PGB_EULER || p.trans == PGB_TRANS_CONSTANT);
+  if (p.simulator != PGB_EULER && p.simulator != PGB_NAVIER_STOKES) return 0;
+  if (p.eos != PGB_EOS_CPG && p.eos != PGB_EOS_TPG) return 0;
+  if (p.chemistry == PGB_CHEM_SUBSTEPPED) return 0;
+  if (p.eos == PGB_EOS_CPG && p.primary == PGB_FLUX_KEPAEC && p.recon == PGB_RECON_CONSTANT && p.ns == 1 &&
+      (p.simulator == PGB_EULER || p.trans == PGB_TRANS_CONSTANT))
+    return 1;
+  return 2;
 }
+bool fused_capable(const pgb_case *c) { return batched_form(c) > 0; }
 
 const double *table(const pgb_case *c, const char *name) {
   auto it = c->tables.find(name);
@@ -697,6 +714,7 @@ int plan_step(pgb_case *c, std::vector<int> &map, std::vector<FusedStagePlan> &p
     const pgb_stage &st = c->stages[s];
     FusedStagePlan p{};
     p.qin = map[st.q];
+    p.dqbuf = map[dq];
     p.ncomb = st.ncombine;
     int written0 = -1;
     for (int m = 0; m < st.ncombine; m++) {
@@ -906,7 +924,10 @@ int fused_attrs(pgb_case *c) {
 
 // one step of the fused path at the current phase
 PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb);
-struct MarkCtx;
+struct MarkCtx {
+  pgb_case *c;
+  int *count;
+};
 void mark_cb(void *ctx, int kind);
 
 // the CFL reduction of physical register qphys into d_cfl
@@ -922,12 +943,42 @@ int cfl_prologue(pgb_case *c, int qphys, int &count) {
   return PGB_OK;
 }
 
+// one stage of the fused passes (react.cuh): the plan's combines on physical
+// registers; with dq set (a right-hand side alone) no combine, dQ stored there
+int launch_react(pgb_case *c, const FusedStagePlan &p, int &count, int dq = -1) {
+  RStage r{};
+  r.Q = c->d_reg[p.qin];
+  r.dQ = c->d_reg[dq >= 0 ? dq : p.dqbuf];
+  r.write_dq = dq >= 0;
+  r.ncomb = dq >= 0 ? 0 : p.ncomb;
+  for (int m = 0; m < r.ncomb; m++) {
+    const FusedCombine &f = p.comb[m];
+    RCombine &rc = r.comb[m];
+    rc.out = c->d_reg[f.out];
+    rc.nterms = f.nterms, rc.step = f.step, rc.write = f.write;
+    for (int n = 0; n < f.nterms; n++) {
+      rc.src[n] = f.src[n] < 0 ? f.src[n] : 0;
+      rc.X[n] = f.src[n] >= 0 ? c->d_reg[f.src[n]] : nullptr;
+      rc.w[n] = f.w[n];
+    }
+  }
+  std::vector<BlockDev> hb;
+  PlainCase pc = plain_case(c, hb);
+  MarkCtx mc{c, &count};
+  pc.mark = mark_cb;
+  pc.ctx = &mc;
+  pc.packed = 1;
+  c->state_stale = false;
+  return kPlain[c->phys.ns - 1].fused(&pc, &r);
+}
+
 int step_fused(pgb_case *c, int &count) {
   const auto &plan = c->plans[c->phase];
-  c->state_stale = true;
+  if (c->form != 2) c->state_stale = true;
   RET(cfl_prologue(c, plan[0].qin, count));
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int) * plan.size(), c->stream));
-  for (int s = 0; s < (int)plan.size(); s++) RET(launch_fused(c, plan[s], s, count));
+  for (int s = 0; s < (int)plan.size(); s++)
+    RET(c->form == 2 ? launch_react(c, plan[s], count) : launch_fused(c, plan[s], s, count));
   if (c->ctrl_cfl) {
     k_clock<<<1, 1, 0, c->stream>>>(c->d_clock, c->d_dt);
     mark(c, K_COMBINE, count);
@@ -942,6 +993,11 @@ int step_fused(pgb_case *c, int &count) {
 // other weights zero), so it writes exactly the dQ it forms.  The halo fill
 // of q comes first, as in a stage.
 int rhs_fused(pgb_case *c, int qphys, int dqphys, int &count) {
+  if (c->form == 2) {
+    FusedStagePlan p{};
+    p.qin = qphys;
+    return launch_react(c, p, count, dqphys);
+  }
   FusedStagePlan p{};
   p.qin = qphys;
   p.ncomb = 1;
@@ -992,11 +1048,6 @@ int ensure_scratch(pgb_case *c) {
   }
   return PGB_OK;
 }
-
-struct MarkCtx {
-  pgb_case *c;
-  int *count;
-};
 
 void mark_cb(void *ctx, int kind) {
   MarkCtx *m = (MarkCtx *)ctx;
@@ -1183,6 +1234,14 @@ int build_bcs(pgb_case *c) {
 int prepare(pgb_case *c, bool fused) {
   if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
   RET(set_current(c));
+  if (fused) {
+    const int form = batched_form(c);
+    if (form != c->form) c->tiles_dirty = true;
+    c->form = form;
+  }
+  // the fused passes read the per-block path's state, transport, gradient
+  // and face arrays and keep the metric arrays' form
+  if (fused && c->form == 2) return ensure_scratch(c);
   // the uniform forms are the batched path's alone: the per-block path reads
   // the metric arrays, so a per-block call leaves the detection to the first
   // batched step
@@ -2171,6 +2230,12 @@ int pgb_fused_shapes(int *shapes, int cap, int *n) {
     shapes[4 * q] = kV2[q].nt, shapes[4 * q + 1] = kV2[q].minb;
     shapes[4 * q + 2] = kV2[q].tw, shapes[4 * q + 3] = kV2[q].th;
   }
+  return PGB_OK;
+}
+
+int pgb_case_batched_form(const pgb_case *c, int *form) {
+  if (!c || !form) return fail(PGB_ERR_ARG, "null argument");
+  *form = batched_form(c);
   return PGB_OK;
 }
 

@@ -229,20 +229,15 @@ __device__ __forceinline__ bool face_at(const BlockDev &B, long long t, int &i, 
 // the advective face flux, kepaec on the cells as they are
 // (peregrine/simulator/euler/kernels/flux/single.mako:4-9 with
 //  recon/constant.mako:3-18 and function/kepaec.mako:2-20)
+// one face of axis A of a block (Q, st, met the block's own arrays), R the
+// index of the cell on its high side, into F[NE]
 template <int NS, int A>
-__global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                          const double *__restrict__ stall, const double *__restrict__ met,
-                          double *__restrict__ Fall, const int2 *__restrict__ ctab = nullptr) {
-  constexpr int NE = 4 + NS;
-  PGB_WHERE(B, t);
-  int i, j, k;
-  if (!face_at<A>(B, t, i, j, k)) return;
-  const long long R = cell_index(B, i, j, k);
+__device__ __forceinline__ void advflux_face(const BlockDev &B, const double *__restrict__ Q,
+                                             const double *__restrict__ st, const double *__restrict__ met,
+                                             const long long R, double *F) {
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
-  const double *Q = Qall + NE * B.cv;
-  const double *st = stall + SW * B.cv;
-  const double *S = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
+  const double *S = met + (M_S + 3 * A) * v + R;
   auto side = [&](long long c) {
     const State s = load_state(st + c, v);
     KSide x;
@@ -254,13 +249,26 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
     return x;
   };
   const KSide sl = side(L), sr = side(R);
-  double F[NE], C;
+  double C;
   kepaec(sl, sr, S[0], S[v], S[2 * v], F, C);
 #pragma unroll
   for (int n = 0; n < NS - 1; n++) F[5 + n] = 0.5 * (Q[(5 + n) * v + R] / Q[R] + Q[(5 + n) * v + L] / Q[L]) * C;
+}
+
+template <int NS, int A>
+__global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                          const double *__restrict__ stall, const double *__restrict__ met,
+                          double *__restrict__ Fall, const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS;
+  PGB_WHERE(B, t);
+  int i, j, k;
+  if (!face_at<A>(B, t, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  double F[NE];
+  advflux_face<NS, A>(B, Qall + NE * B.cv, stall + SW * B.cv, met + M_NCOMP * B.cv, R, F);
   double *Fo = Fall + NE * B.cv + R;
 #pragma unroll
-  for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
+  for (int l = 0; l < NE; l++) Fo[l * B.vol] = F[l];
 }
 
 // the double flux's kepaec: the plain two-point flux with the energy row
@@ -335,21 +343,14 @@ __global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const dou
 // (peregrine/simulator/eulerdf/kernels/flux/function/{rusanov,ausmup}.mako,
 // eside at peregrine/simulator/mixture/eos/realgasdf/kernels/eos.mako:73-83)
 template <int NS, int A, int FN, bool RG = false, bool DF = false>
-__global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                          const double *__restrict__ stall, const double *__restrict__ met,
-                          double *__restrict__ Fall, const int lim,
-                          const int2 *__restrict__ ctab = nullptr) {
+__device__ __forceinline__ void riemann_face(const BlockDev &B, const double *__restrict__ Q,
+                                             const double *__restrict__ st, const double *__restrict__ met,
+                                             const int lim, const long long R, double *F) {
   constexpr int NE = 4 + NS, NY = NS > 1 ? NS - 1 : 1;
-  PGB_WHERE(B, t);
-  int i, j, k;
-  if (!face_at<A>(B, t, i, j, k)) return;
-  const long long R = cell_index(B, i, j, k);
   const long long d = A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y;
   const long long L = R - d;
   const long long v = B.vol;
-  const double *Q = Qall + NE * B.cv;
-  const double *st = stall + SW * B.cv;
-  const double *Sp = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
+  const double *Sp = met + (M_S + 3 * A) * v + R;
   const double S[3] = {Sp[0], Sp[v], Sp[2 * v]};
   RSide sl, sr;
   double YL[NY], YR[NY];
@@ -385,8 +386,6 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
     sl.u = lft(1), sl.v = lft(2), sl.w = lft(3);
     sr.u = rgt(1), sr.v = rgt(2), sr.w = rgt(3);
   }
-  constexpr int NF = NE + (DF ? 1 : 0);
-  double F[NF];
   riemann<FN, NS>(sl, sr, YL, YR, S, F);
   if (DF) {
     // eside: a side's total energy in plane q, theta p + rho (eps + the
@@ -428,33 +427,40 @@ __global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double
       for (int q = 0; q < 2; q++) F[q == 0 ? 4 : NE] = mdot * (Ep[q] + U.p) * rhoinvU;
     }
   }
+}
+
+// F[NE] (NE + 1 rows with DF) of the face of axis A whose high-side cell is R
+template <int NS, int A, int FN, bool RG = false, bool DF = false>
+__global__ void k_riemann(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                          const double *__restrict__ stall, const double *__restrict__ met,
+                          double *__restrict__ Fall, const int lim,
+                          const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS, NF = NE + (DF ? 1 : 0);
+  PGB_WHERE(B, t);
+  int i, j, k;
+  if (!face_at<A>(B, t, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  double F[NF];
+  riemann_face<NS, A, FN, RG, DF>(B, Qall + NE * B.cv, stall + SW * B.cv, met + M_NCOMP * B.cv, lim, R, F);
   double *Fo = Fall + NF * B.cv + R;
 #pragma unroll
-  for (int l = 0; l < NF; l++) Fo[l * v] = F[l];
+  for (int l = 0; l < NF; l++) Fo[l * B.vol] = F[l];
 }
 
 // the diffusive face flux added to F (peregrine/simulator/navstokes/kernels/flux/alpha-damping.mako:3-99);
 // DF: the double flux's faces carry the energy row twice, and the diffusive
 // energy flux adds to both (peregrine/simulator/navstokesdf/kernels/flux/alpha-damping.mako:1-9)
-template <int NS, int A, bool DF = false>
-__global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                           const double *__restrict__ stall, const double *__restrict__ trall,
-                           const double *__restrict__ hall, const double *__restrict__ gall,
-                           const double *__restrict__ met, double *__restrict__ Fall,
-                           const int2 *__restrict__ ctab = nullptr) {
+// the diffusive rows of the face of axis A whose high-side cell is R added
+// to F[NE]; returns the diffusive energy flux (the double flux adds it to its
+// second energy row too).  Q, st, tr, hs, gr and M are the block's own arrays.
+template <int NS, int A>
+__device__ __forceinline__ double diffflux_face(const BlockDev &B, const double *__restrict__ Q,
+                                                const double *__restrict__ st, const double *__restrict__ tr,
+                                                const double *__restrict__ hs, const double *__restrict__ gr,
+                                                const double *__restrict__ M, const long long R, double *F) {
   constexpr int NE = 4 + NS, NGRAD = NE - 1;
-  PGB_WHERE(B, t);
-  int i, j, k;
-  if (!face_at<A>(B, t, i, j, k)) return;
-  const long long R = cell_index(B, i, j, k);
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
-  const double *Q = Qall + NE * B.cv;
-  const double *st = stall + SW * B.cv;
-  const double *tr = trall + (2 + NS) * B.cv;
-  const double *hs = hall + NS * B.cv;
-  const double *gr = gall + 3 * NGRAD * B.cv;
-  const double *M = met + M_NCOMP * B.cv;
   const double S[3] = {M[(M_S + 3 * A) * v + R], M[(M_S + 3 * A + 1) * v + R], M[(M_S + 3 * A + 2) * v + R]};
   const double xf[3] = {M[(M_XF + 3 * A) * v + R], M[(M_XF + 3 * A + 1) * v + R], M[(M_XF + 3 * A + 2) * v + R]};
   const double xL[3] = {M[(M_XCC + 0) * v + L], M[(M_XCC + 1) * v + L], M[(M_XCC + 2) * v + L]};
@@ -470,10 +476,6 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
   const double rhoinvL = sL.rhoinv, rhoinvR = sR.rhoinv;
   const double uL = Q[1 * v + L] * rhoinvL, vL = Q[2 * v + L] * rhoinvL, wL = Q[3 * v + L] * rhoinvL;
   const double uR = Q[1 * v + R] * rhoinvR, vR = Q[2 * v + R] * rhoinvR, wR = Q[3 * v + R] * rhoinvR;
-  double F[NE];
-  double *Fo = Fall + (NE + (DF ? 1 : 0)) * B.cv + R;
-#pragma unroll
-  for (int l = 0; l < NE; l++) F[l] = Fo[l * v];
   double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
   facegrad(g, uL, uR, gL + 0, gRr + 0, dudx, dudy, dudz);
   facegrad(g, vL, vR, gL + 3, gRr + 3, dvdx, dvdy, dvdz);
@@ -529,6 +531,27 @@ __global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const doubl
   const double hns = 0.5 * (hs[(NS - 1) * v + R] + hs[(NS - 1) * v + L]);
   f4 += (-rho * Dk * gradYns + Yns * corr) * hns;
   F[4] += f4;
+  return f4;
+}
+
+template <int NS, int A, bool DF = false>
+__global__ void k_diffflux(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                           const double *__restrict__ stall, const double *__restrict__ trall,
+                           const double *__restrict__ hall, const double *__restrict__ gall,
+                           const double *__restrict__ met, double *__restrict__ Fall,
+                           const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS, NGRAD = NE - 1;
+  PGB_WHERE(B, t);
+  int i, j, k;
+  if (!face_at<A>(B, t, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  const long long v = B.vol;
+  double F[NE];
+  double *Fo = Fall + (NE + (DF ? 1 : 0)) * B.cv + R;
+#pragma unroll
+  for (int l = 0; l < NE; l++) F[l] = Fo[l * v];
+  const double f4 = diffflux_face<NS, A>(B, Qall + NE * B.cv, stall + SW * B.cv, trall + (2 + NS) * B.cv,
+                                         hall + NS * B.cv, gall + 3 * NGRAD * B.cv, met + M_NCOMP * B.cv, R, F);
 #pragma unroll
   for (int l = 0; l < NE; l++) Fo[l * v] = F[l];
   if (DF) Fo[NE * v] += f4;

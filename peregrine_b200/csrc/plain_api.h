@@ -65,6 +65,26 @@ struct PlainCase {
   void *ctx;
 };
 
+// The fused passes' stage (react.cuh): the stage's register, dQ (the
+// coupled source's home and, with write_dq, dQ's), and the combines on
+// physical registers: out = sum_n w[n] X[n] left to right, dt on the last
+// term when step is set, a term's src -1 for dQ and -2 for the first
+// combine's value at the cell; write 0 drops a store no later stage reads.
+struct RCombine {
+  double *out;
+  const double *X[4];
+  double w[4];
+  int src[4];
+  int nterms, step, write;
+};
+struct RStage {
+  const double *Q;
+  double *dQ;
+  int write_dq;
+  int ncomb;
+  RCombine comb[2];
+};
+
 struct PlainOps {
   int (*upload)(const Species *, const Mech *, const MathTables *, cudaStream_t);
   int (*rhs)(const PlainCase *, const double *Q, double *dQ);
@@ -72,6 +92,7 @@ struct PlainOps {
   int (*production)(long long n, const double *rho, const double *Y, const double *T, double *omega, cudaStream_t);
   int (*prestep)(const PlainCase *, double *Q, int first);
   int (*cflmax)(const PlainCase *, const double *Q, double *out);
+  int (*fused)(const PlainCase *, const RStage *);
 };
 
 }  // namespace pgb
@@ -88,4 +109,6 @@ struct PlainOps {
       long long, const double *, const double *, const double *, double *, cudaStream_t);                        \
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_prestep_##N(const pgb::PlainCase *, double *, int); \
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_cflmax_##N(const pgb::PlainCase *, const double *,  \
-                                                                            double *);
+                                                                            double *);                           \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_fused_##N(const pgb::PlainCase *,               \
+                                                                           const pgb::RStage *);

@@ -15,6 +15,7 @@
 #include "substep.cuh"
 #include "plain.cuh"
 #include "plain_api.h"
+#include "react.cuh"
 
 #ifndef PGB_NS
 #define PGB_NS 1
@@ -396,4 +397,84 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
   }
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "double-flux freeze");
+}
+
+// The fused passes' stage (react.cuh): Q's halo, the cell pass (fromQ, the
+// transport and the coupled source), the gradients and their first halo
+// layer, and the tile kernel (every face, the divergence and the combines),
+// each pass one launch over every block
+namespace {
+template <bool VISC>
+void rcell_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RStage &r = *(const RStage *)ctx;
+  k_rcell<NS, VISC><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, pc->tr, pc->hsp, ct);
+}
+void rsource_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RStage &r = *(const RStage *)ctx;
+  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, r.dQ, ct);
+}
+void rgrads_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RStage &r = *(const RStage *)ctx;
+  k_grads<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, pc->met, pc->grads, 0, ct);
+}
+}  // namespace
+
+namespace {
+template <int A>
+void rface_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RStage &r = *(const RStage *)ctx;
+  const int lim = pc->recon == PGB_RECON_MUSCL ? pc->limiter : 0;
+  cudaStream_t s = pc->stream;
+#define PGB_RFACE(FN)                                                                                          \
+  if (pc->visc)                                                                                              \
+    k_rface<NS, A, FN, true><<<g, TH, 0, s>>>(pc->d_blks, b, r.Q, pc->state, pc->tr, pc->hsp, pc->grads,     \
+                                              pc->met, pc->F[A], lim, ct);                                   \
+  else                                                                                                       \
+    k_rface<NS, A, FN, false><<<g, TH, 0, s>>>(pc->d_blks, b, r.Q, pc->state, pc->tr, pc->hsp, pc->grads,    \
+                                               pc->met, pc->F[A], lim, ct);
+  switch (pc->primary) {
+    case PGB_FLUX_KEPAEC: PGB_RFACE(0) break;
+    case PGB_FLUX_HLLC: PGB_RFACE(FN_HLLC) break;
+    case PGB_FLUX_RUSANOV: PGB_RFACE(FN_RUSANOV) break;
+    default: PGB_RFACE(FN_AUSMUP) break;
+  }
+#undef PGB_RFACE
+}
+struct RApplyCtx {
+  RApplyArgs a;
+};
+void rapply_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RApplyCtx &r = *(const RApplyCtx *)ctx;
+  k_rapply<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, r.a, ct);
+}
+}  // namespace
+
+extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs) {
+  cudaStream_t s = pc->stream;
+  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(rs->Q), pc->halo, pc->nhalo, NE, 1, pc->rots);
+  mark(pc, 0);
+  for_blocks(pc, R_VOL, pc->visc ? rcell_launch<true> : rcell_launch<false>, rs, 8);
+  const bool chem = pc->chem == PGB_CHEM_COUPLED;
+  if (chem) for_blocks(pc, R_INNER, rsource_launch, rs, 2);
+  if (pc->visc) {
+    for_blocks(pc, R_INNER, rgrads_launch, rs, 2);
+    k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1), HALO_TENSOR,
+                                                pc->rots);
+    mark(pc, 0);
+  }
+  for_blocks(pc, R_FX, rface_launch<0>, rs, 2);
+  for_blocks(pc, R_FY, rface_launch<1>, rs, 2);
+  for_blocks(pc, R_FZ, rface_launch<2>, rs, 2);
+  RApplyCtx ra{};
+  RApplyArgs &a = ra.a;
+  a.dQ = rs->dQ;
+  a.dt = pc->dt;
+  a.chem = chem ? 1 : 0;
+  a.write_dq = rs->write_dq;
+  a.ncomb = rs->ncomb;
+  a.comb[0] = rs->comb[0];
+  a.comb[1] = rs->comb[1];
+  for_blocks(pc, R_INNER, rapply_launch, &ra, 1);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PGB_OK : cuda_fail(e, "fused passes");
 }

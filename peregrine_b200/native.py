@@ -245,6 +245,8 @@ SIGNATURES = {
                               ctypes.c_int),
     "pgb_rhs_block_noalloc_max_cells": ([ctypes.c_int], ctypes.c_longlong),
     "pgb_block_uniform": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_case_batched_form": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_fp64_fma_rate": ([ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
 }
 
 _lib = None

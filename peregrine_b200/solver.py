@@ -145,10 +145,11 @@ class Solver:
             native.call("pgb_case_destroy", self.case)
             self.case = None
             raise
-        if self.path == native.PATH_BATCHED and not self.fused_capable():
-            # the batched kernel takes the single-species kepaec case; any other
-            # physics runs the per-block kernels, still on the device, packed
-            # (each pass one launch over every block, the same bits)
+        if self.path == native.PATH_BATCHED and self.batched_form() == 0:
+            # the batched path takes the ideal gases without boundaries (the
+            # fused stage kernel or the fused passes); other physics runs the
+            # per-block kernels, still on the device, packed (each pass one
+            # launch over every block, the same bits)
             self.path = native.PATH_PACKED
         if state is None:
             self._uniform_ics()
@@ -157,10 +158,16 @@ class Solver:
     def has_bcs(self):
         return any(face.nbr is None for blk in self.mesh_blocks for face in blk.intfaces)
 
+    def batched_form(self):
+        """The batched path's form for this case: 1 the fused stage kernel
+        (the single-species calorically perfect kepaec case), 2 the fused
+        passes (the other ideal-gas cases without boundaries), 0 neither."""
+        form = ctypes.c_int()
+        native.call("pgb_case_batched_form", self.case, ctypes.byref(form))
+        return form.value
+
     def fused_capable(self):
-        cfg = self.cfg
-        return (not self.has_bcs and min(min(b.cells) for b in self.mesh_blocks) >= 2 and self.ns == 1 and cfg["adv-flux"]["primary"] == "kepaec" and cfg["adv-flux"]["recon"] == "constant"
-                and cfg["mixture"]["eos"] == "cpg")
+        return self.batched_form() > 0
 
     def species_tables(self):
         """The named species tables the case takes (pgb_case_set_table), from
