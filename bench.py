@@ -539,6 +539,54 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def shard_leg(args, dist, rank, world, local):
+    """The workload's blocks over the ranks (peregrine_b200/shard.py), Q's halo
+    traded between stages on the device (NCCL), timed by CUDA events on every
+    rank, the max taken; strong scaling of the one grid."""
+    import torch
+
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases, shard
+    from peregrine_b200.replicas import max_over_ranks
+
+    cfg = cases.tgv_config("navier-stokes", "rk4", "batched")
+    mesh = cases.tgv_mesh(CELLS, BLOCKS, seed=SEED, low=CUT_LOW, high=CUT_HIGH)
+    blocks = mesh.make_blocks(2)
+    owner = shard.partition(blocks, world)
+    sh = shard.ShardedSolver(cfg, mesh, pg.get_backend("cuda", cfg, device=local), owner, rank, exchange="device")
+    every = cases.tgv_prims(*_every_field(mesh))
+    sh.solver.set_prims([every[g] for g in sh.plan.local])
+    dt = stable_dt()
+    sh.step(dt, args.warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sh.step(dt, args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, device=f"cuda:{local}")
+    ncells = sum(b.ncells for b in blocks)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": ncells * STAGES * args.steps / (ms / 1e3), "unit": "cell-stage/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": ncells, "blocks": len(blocks),
+                       "parallelism": f"blocks over {world} ranks, Q halo traded each stage (NCCL)",
+                       "blocks_per_rank": np.bincount(owner, minlength=world).tolist()}}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def _every_field(mesh):
+    from peregrine_b200.grid import metrics as make_metrics
+
+    blocks = mesh.make_blocks(2)
+    return blocks, [make_metrics(b.nodes, 2) for b in blocks]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -561,6 +609,9 @@ def main():
     ap.add_argument("--substep-only", action="store_true", help="the sub-stepped chemistry leg alone")
     ap.add_argument("--no-substep", action="store_true", help="skip the sub-stepped chemistry leg")
     ap.add_argument("--no-boundary", action="store_true", help="skip the bounded channel leg")
+    ap.add_argument("--shard", action="store_true",
+                    help="with N > 1 ranks: the workload's blocks over the ranks, halos traded each stage (strong "
+                         "scaling) instead of a replica per rank")
     args = ap.parse_args()
     set_cells(args.cells)
     args.warmup = max(3, args.warmup)
@@ -595,6 +646,10 @@ def main():
 
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.shard and world > 1:
+        shard_leg(args, dist, rank, world, local)
+        return
 
     mb, mesh, prims = build_case("batched", device=local)
     dt = stable_dt()

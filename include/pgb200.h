@@ -258,6 +258,33 @@ int pgb_case_connect_oriented(pgb_case *c, int blk, int nface, int nbr, const ch
  * vectors of a rotationally periodic face turned (the reference's exchange
  * of a bank, peregrine/multiblock/collections/exchange/collection.py) */
 int pgb_exchange(pgb_case *c, int reg);
+/* Every halo cell the case's interfaces fill, six long longs each: the
+ * block and cell index (full layout) it fills, the block and cell index it
+ * copies, the rotation it turns by (0 none, else 1 + its index) and 0 for
+ * the first face layer, 1 for the rest; n is how many, up to cap written.
+ * A host computation, before or after finalize (the reference's interior
+ * exchange windows, peregrine/multiblock/collections/exchange/collection.py:63-96).
+ * A partitioner lists a whole grid's entries on a case it never finalizes. */
+int pgb_case_halo_entries(pgb_case *c, long long cap, long long *out, long long *n);
+/* A shard's exchange with the blocks other ranks hold: the cells it sends
+ * (packs) and the halo cells it receives (unpacks), each a block and a cell
+ * index, in the order the two sides agree on (the reference's message pools,
+ * peregrine/multiblock/collections/exchange/pool.py:9-71).  After finalize. */
+int pgb_case_set_exchange(pgb_case *c, long long nsend, const int *send_blk, const int *send_idx, long long nrecv,
+                          const int *recv_blk, const int *recv_idx);
+/* The register stage s of the current step reads on path, its send cells
+ * packed into buf (device, ne x nsend doubles, component-major), or its
+ * receive cells filled from buf (ne x nrecv); queued on the case's stream
+ * (the reference's pack and place, buffer.py:7-33, place.mako). */
+int pgb_exchange_pack(pgb_case *c, int stage, int path, double *buf);
+int pgb_exchange_unpack(pgb_case *c, int stage, int path, const double *buf);
+/* Stage s of a step on path, dt the last set (pgb_set_dt): the local halo
+ * fill, the right-hand side and the combines; stages run in order, so a
+ * shard exchanges its halos between them (the reference's Solver.rhs and
+ * Solver.advance per stage, peregrine/integrators/rungekutta.py:33-39).
+ * For cases without boundaries, double flux or sub-stepped chemistry. */
+int pgb_step_stage(pgb_case *c, int s, int path);
+
 /* the case's clock, the t boundary values read at a step's start
  * (peregrine/multiblock/solver.py:35, 355-364); a step moves it on by dt */
 int pgb_set_time(pgb_case *c, double t);

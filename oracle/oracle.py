@@ -655,7 +655,10 @@ class Oracle:
         assert Q.flags["C_CONTIGUOUS"] and rec.flags["C_CONTIGUOUS"]
         self.lib.oracle_freeze(ctypes.byref(self.case), ctypes.c_long(len(Q)), _ptr(Q), _ptr(rec))
 
-    def step(self, dt):
+    def step(self, dt, before_stage=None):
+        """One step; before_stage(register), when given, runs before each
+        stage's right-hand side on the register it reads (a shard's halo
+        trade, tests/test_shard_cpu.py)."""
         names = list(range(self.nregs))
         stages, dQ = stage_combines(self.integrator, names)
         start = self.tme
@@ -666,6 +669,8 @@ class Oracle:
                 self.prestep(self.regs[stages[0][0]])
             self.prestep(self.regs[stages[0][0]])
         for n, (Q, combines) in enumerate(stages):
+            if before_stage is not None:
+                before_stage(self.regs[Q])
             self.rhs(self.regs[Q], self.regs[dQ], t=start + fracs[n] * dt)
             for out, own, reads, step in combines:
                 for b, blk in enumerate(self.blocks):

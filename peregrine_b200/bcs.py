@@ -165,7 +165,8 @@ def check_faces(blocks, bcvals):
     (peregrine/multiblock/solver.py:157-173)."""
     for blk in blocks:
         for face in blk.intfaces:
-            if face.nbr is not None:
+            # a face joined to another rank's block is traded, not a boundary
+            if face.nbr is not None or getattr(face, "remote", None) is not None:
                 continue
             where = f"block {blk.nblki} interface {face.nface}"
             if face.bcname is None:

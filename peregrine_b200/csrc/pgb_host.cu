@@ -69,6 +69,18 @@ int fail(int code, const std::string &msg) {
   } while (0)
 
 static __global__ void k_setscalar(double *p, double v) { *p = v; }
+// a shard's halo cells to and from a buffer [component][cell]: cell e's
+// component c at R[at[e] + c vol[e]]
+static __global__ void k_xpack(const double *__restrict__ R, const long long *__restrict__ at,
+                               const int *__restrict__ vol, long long n, int ne, double *__restrict__ buf) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    for (int c = 0; c < ne; c++) buf[c * n + e] = R[at[e] + (long long)c * vol[e]];
+}
+static __global__ void k_xunpack(double *__restrict__ R, const long long *__restrict__ at,
+                                 const int *__restrict__ vol, long long n, int ne, const double *__restrict__ buf) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    for (int c = 0; c < ne; c++) R[at[e] + (long long)c * vol[e]] = buf[c * n + e];
+}
 // the clock at a step's end: start + dt (peregrine/multiblock/solver.py:355-364)
 static __global__ void k_clock(double *clock, const double *dt) { *clock = *clock + *dt; }
 // the cfl controller's step: min(cfl / the combined CFL number per unit step,
@@ -138,6 +150,12 @@ struct pgb_case {
   bool uniform_done = false;
   bool use_v2 = false;  // every block uniform: the uniform-metric fused kernel
   int form = 0;         // the batched path's form: 1 the fused stage kernel, 2 the fused passes
+  // a shard's exchange with the other ranks' blocks: the cells it packs and
+  // unpacks, each its component 0's offset in a register and its component stride
+  long long *d_xsend = nullptr, *d_xrecv = nullptr;
+  int *d_xsvol = nullptr, *d_xrvol = nullptr;
+  long long nxsend = 0, nxrecv = 0;
+  int stage_next = 0;  // the next stage pgb_step_stage runs
 
   int v2_ctas = 1;      // its resident CTAs per SM
   int v2 = 0;           // its instance: threads per CTA, launch bound, tile layout
@@ -405,6 +423,22 @@ int set_current(pgb_case *c) {
   return PGB_OK;
 }
 
+// each block's extents and its cells' offset in a register, blocks end to
+// end; returns the cells of them all
+long long layout_blocks(pgb_case *c) {
+  long long cv = 0;
+  for (auto &B : c->blocks) {
+    BlockDev &D = B.dev;
+    D = BlockDev{};
+    D.nx = B.nx, D.ny = B.ny, D.nz = B.nz;
+    D.X = B.nx + 2 * NG, D.Y = B.ny + 2 * NG, D.Z = B.nz + 2 * NG;
+    D.vol = (long long)D.X * D.Y * D.Z;
+    D.cv = cv;
+    cv += D.vol;
+  }
+  return cv;
+}
+
 // where a cell outside a block lies: step across the face of the first axis
 // it lies outside of, into the neighbour's own axes by the face's
 // orientation (the reference's digits, peregrine/multiblock/interface/base.py:96-160),
@@ -463,8 +497,9 @@ bool locate(pgb_case *c, int b, int ijk[3], int &sb, int &rot) {
 // every halo cell a stage reads: the face halos two deep (layer 0 of every
 // face first, as the gradients' one-plane exchange reads only those), then
 // the edge cells one deep in both axes
-void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0) {
+void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0, std::vector<int2> *blocks = nullptr) {
   out.clear();
+  if (blocks) blocks->clear();
   auto add = [&](int b, int i, int j, int k) {
     int ijk[3] = {i, j, k};
     int sb, rot;
@@ -477,6 +512,7 @@ void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0) {
     h.dvol = (int)D.vol, h.svol = (int)S.vol;
     h.rot = rot;
     out.push_back(h);
+    if (blocks) blocks->push_back(make_int2(b, sb));
   };
   for (int layer = 0; layer < NG; layer++) {
     for (int b = 0; b < (int)c->blocks.size(); b++) {
@@ -1332,9 +1368,8 @@ int pgb_case_create(const pgb_physics *phys, pgb_case **out) {
   c->uid = ++g_next_uid;
   c->phys = *phys;
   c->ne = 4 + phys->ns;
-  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-  CK(cudaEventCreate(&c->ev0));
-  CK(cudaEventCreate(&c->ev1));
+  // the stream and events are made at finalize: until then a case is host
+  // data alone (a partitioner lists a grid's halo on a machine without a GPU)
   *out = c.release();
   return PGB_OK;
 }
@@ -1346,7 +1381,7 @@ int pgb_case_destroy(pgb_case *c) {
     if (g) cudaGraphExecDestroy(g);
   for (auto &r : c->d_reg)
     if (r) cudaFree(r);
-  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_one, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
+  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_one, c->d_xsend, c->d_xrecv, c->d_xsvol, c->d_xrvol, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
                   c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots};
@@ -1556,6 +1591,127 @@ int pgb_exchange(pgb_case *c, int reg) {
   return PGB_OK;
 }
 
+int pgb_case_halo_entries(pgb_case *c, long long cap, long long *out, long long *n) {
+  if (!c || !n || (cap > 0 && !out)) return fail(PGB_ERR_ARG, "null argument");
+  if (c->blocks.empty()) return fail(PGB_ERR_STATE, "no blocks");
+  // the blocks' layout is a host computation; finalize repeats it
+  if (!c->finalized) layout_blocks(c);
+  std::vector<HaloEntry> halo;
+  std::vector<int2> blk;
+  long long l0 = 0;
+  build_halo(c, halo, l0, &blk);
+  *n = (long long)halo.size();
+  for (long long e = 0; e < *n && e < cap; e++) {
+    long long *r = out + 6 * e;
+    r[0] = blk[e].x, r[1] = halo[e].didx, r[2] = blk[e].y, r[3] = halo[e].sidx, r[4] = halo[e].rot;
+    r[5] = e < l0 ? 0 : 1;
+  }
+  return PGB_OK;
+}
+
+int pgb_case_set_exchange(pgb_case *c, long long nsend, const int *send_blk, const int *send_idx, long long nrecv,
+                          const int *recv_blk, const int *recv_idx) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->finalized) return fail(PGB_ERR_STATE, "finalize the case before its exchange");
+  if (nsend < 0 || nrecv < 0 || (nsend && (!send_blk || !send_idx)) || (nrecv && (!recv_blk || !recv_idx)))
+    return fail(PGB_ERR_ARG, "bad exchange lists");
+  auto table = [&](long long n, const int *blk, const int *idx, long long *&d_at, int *&d_vol) -> int {
+    if (d_at) cudaFree(d_at), d_at = nullptr;
+    if (d_vol) cudaFree(d_vol), d_vol = nullptr;
+    if (!n) return PGB_OK;
+    std::vector<long long> at(n);
+    std::vector<int> vol(n);
+    for (long long e = 0; e < n; e++) {
+      if (blk[e] < 0 || blk[e] >= (int)c->blocks.size()) return fail(PGB_ERR_ARG, "exchange cell: no such block");
+      const BlockDev &D = c->blocks[blk[e]].dev;
+      if (idx[e] < 0 || idx[e] >= D.vol) return fail(PGB_ERR_ARG, "exchange cell: index outside its block");
+      at[e] = (long long)c->ne * D.cv + idx[e];
+      vol[e] = (int)D.vol;
+    }
+    CK(cudaMalloc(&d_at, sizeof(long long) * n));
+    CK(cudaMalloc(&d_vol, sizeof(int) * n));
+    CK(cudaMemcpy(d_at, at.data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_vol, vol.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    return PGB_OK;
+  };
+  RET(table(nsend, send_blk, send_idx, c->d_xsend, c->d_xsvol));
+  RET(table(nrecv, recv_blk, recv_idx, c->d_xrecv, c->d_xrvol));
+  c->nxsend = nsend, c->nxrecv = nrecv;
+  return PGB_OK;
+}
+
+// the physical register stage s of the current step reads
+static int stage_register(pgb_case *c, int s, int path, int &phys) {
+  if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
+  if (path < PGB_PATH_BATCHED || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "no such path");
+  if (s < 0 || s >= (int)c->stages.size()) return fail(PGB_ERR_ARG, "no such stage");
+  if (path == PGB_PATH_BATCHED) phys = c->plans[c->phase][s].qin;
+  else phys = c->phys_of[c->stages[s].q];
+  return PGB_OK;
+}
+
+int pgb_exchange_pack(pgb_case *c, int stage, int path, double *buf) {
+  if (!c || (c->nxsend && !buf)) return fail(PGB_ERR_ARG, "null argument");
+  int r = 0;
+  RET(stage_register(c, stage, path, r));
+  if (c->nxsend)
+    k_xpack<<<grid_for(c->nxsend, 256), 256, 0, c->stream>>>(c->d_reg[r], c->d_xsend, c->d_xsvol, c->nxsend, c->ne,
+                                                             buf);
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int pgb_exchange_unpack(pgb_case *c, int stage, int path, const double *buf) {
+  if (!c || (c->nxrecv && !buf)) return fail(PGB_ERR_ARG, "null argument");
+  int r = 0;
+  RET(stage_register(c, stage, path, r));
+  if (c->nxrecv)
+    k_xunpack<<<grid_for(c->nxrecv, 256), 256, 0, c->stream>>>(c->d_reg[r], c->d_xrecv, c->d_xrvol, c->nxrecv, c->ne,
+                                                               buf);
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
+int pgb_step_stage(pgb_case *c, int s, int path) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (s != c->stage_next) return fail(PGB_ERR_STATE, "stages run in order, from the step's first");
+  const bool fused = path == PGB_PATH_BATCHED;
+  if (fused && !fused_capable(c)) return fail(PGB_ERR_UNSUPPORTED, "the batched path does not take this case");
+  if (path < PGB_PATH_BATCHED || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "no such path");
+  if (c->nbcface[0] || sim_df(c->phys.simulator) || c->phys.chemistry == PGB_CHEM_SUBSTEPPED)
+    return fail(PGB_ERR_UNSUPPORTED, "a stage at a time takes the cases without boundaries, double flux or substeps");
+  // a shard trades Q's halo between stages; the per-block kernels and the
+  // fused passes exchange the gradients' first halo layer inside the stage,
+  // which a trade of Q does not give them: their viscous shards are refused
+  if ((c->nxsend || c->nxrecv) && sim_visc(c->phys.simulator) && !(fused && batched_form(c) == 1))
+    return fail(PGB_ERR_UNSUPPORTED, "a viscous shard steps on the batched path's fused stage kernel alone: it "
+                                     "forms its gradients from Q's two-deep halo, the others trade them mid-stage");
+  RET(prepare(c, fused));
+  if (!fused) RET(ensure_scratch(c));
+  int count = 0;
+  struct Packed {
+    pgb_case *c;
+    ~Packed() { c->packed = false; }
+  } unpack{c};
+  c->packed = path == PGB_PATH_PACKED;
+  if (fused) {
+    const auto &plan = c->plans[c->phase];
+    if (s == 0) CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int) * plan.size(), c->stream));
+    RET(c->form == 2 ? launch_react(c, plan[s], count) : launch_fused(c, plan[s], s, count));
+    if (s + 1 == (int)plan.size()) {
+      c->phase = (c->phase + 1) % c->period;
+      c->phys_of = c->maps[c->phase];
+    }
+  } else {
+    const pgb_stage &st = c->stages[s];
+    RET(rhs_plain(c, c->phys_of[st.q], c->phys_of[st.dq], count, st.tfrac));
+    combine_stage(c, st, count);
+  }
+  c->stage_next = (s + 1) % (int)c->stages.size();
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
 int pgb_case_set_substeps(pgb_case *c, int cap, int bulk, int bins, double eqtol) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
   if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
@@ -1693,20 +1849,13 @@ int pgb_case_finalize(pgb_case *c) {
   if (c->blocks.empty()) return fail(PGB_ERR_STATE, "no blocks");
   if (c->stages.empty()) return fail(PGB_ERR_STATE, "no stages");
   RET(build_species(c));
-  long long cv = 0;
-  for (auto &B : c->blocks) {
-    BlockDev &D = B.dev;
-    D = BlockDev{};
-    D.nx = B.nx, D.ny = B.ny, D.nz = B.nz;
-    D.X = B.nx + 2 * NG, D.Y = B.ny + 2 * NG, D.Z = B.nz + 2 * NG;
-    D.vol = (long long)D.X * D.Y * D.Z;
-    D.cv = cv;
-    cv += D.vol;
-  }
-  c->cells = cv;
+  if (!c->stream) CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  if (!c->ev0) CK(cudaEventCreate(&c->ev0));
+  if (!c->ev1) CK(cudaEventCreate(&c->ev1));
+  c->cells = layout_blocks(c);
   c->interior_cells = 0;
   for (auto &B : c->blocks) c->interior_cells += (long long)B.nx * B.ny * B.nz;
-  const size_t n = (size_t)cv;
+  const size_t n = (size_t)c->cells;
   for (int r = 0; r < c->phys.nregs; r++) {
     CK(cudaMalloc(&c->d_reg[r], sizeof(double) * c->ne * n));
     CK(cudaMemsetAsync(c->d_reg[r], 0, sizeof(double) * c->ne * n, c->stream));
@@ -1992,6 +2141,7 @@ static int step_loop(pgb_case *c, int nsteps, int path, int graph) {
 
 static int step_begin(pgb_case *c, int nsteps, int path) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->stage_next != 0) return fail(PGB_ERR_STATE, "a step taken stage by stage is not finished");
   if (nsteps < 0) return fail(PGB_ERR_ARG, "negative step count");
   if (path < PGB_PATH_BATCHED || path > PGB_PATH_PACKED) return fail(PGB_ERR_ARG, "no such path");
   const bool fused = path == PGB_PATH_BATCHED;

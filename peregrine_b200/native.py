@@ -247,6 +247,14 @@ SIGNATURES = {
     "pgb_block_uniform": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_case_batched_form": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_fp64_fma_rate": ([ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "pgb_case_halo_entries": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong),
+                               ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "pgb_case_set_exchange": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
+                               ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
+                               ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_exchange_pack": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "pgb_exchange_unpack": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "pgb_step_stage": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
 }
 
 _lib = None

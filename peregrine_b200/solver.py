@@ -156,7 +156,9 @@ class Solver:
 
     @property
     def has_bcs(self):
-        return any(face.nbr is None for blk in self.mesh_blocks for face in blk.intfaces)
+        # a face joined to another rank's block (a shard's, peregrine_b200/shard.py) is traded, not a boundary
+        return any(face.nbr is None and getattr(face, "remote", None) is None
+                   for blk in self.mesh_blocks for face in blk.intfaces)
 
     def batched_form(self):
         """The batched path's form for this case: 1 the fused stage kernel
@@ -248,7 +250,7 @@ class Solver:
             ids[name] = out.value
         for blk in self.mesh_blocks:
             for face in blk.intfaces:
-                if face.nbr is None:
+                if face.nbr is None and getattr(face, "remote", None) is None:
                     native.call("pgb_case_set_face_bc", self.case, blk.nblki, face.nface, ids[face.bcname])
 
     def __del__(self):
