@@ -358,30 +358,41 @@ def packed_leg(mb, dt, steps, ncells, stages):
 
 
 def realgas_leg(steps, cpu=True):
-    """Cell-stage/s of the transcritical mixing layer on the per-block path."""
+    """Cell-stage/s of the transcritical mixing layer: the batched path (the
+    double flux's fused stage), with the per-block and packed paths beside it."""
     import peregrine_b200 as pg
-    from peregrine_b200 import cases
+    from peregrine_b200 import cases, native
 
-    cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3")
+    cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3", launch="batched")
     mesh = cases.mixing_layer_mesh(256, 128, 4, 8, seed=SEED)
     mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
     prims = cases.mixing_layer_prims(mb.metrics, 128, seed=SEED)
-    mb.set_prims(prims)
     dt = 2e-9
-    mb.step(dt, 3)
-    mb.backend.sync()
-    ms = time_graph(mb, dt, steps)
     ncells = mb.ncells
-    value = ncells * 3 * steps / (ms / 1e3)
+    legs = {}
+    for path, name in ((native.PATH_PER_BLOCK, "per_block"), (native.PATH_PACKED, "packed"),
+                       (native.PATH_BATCHED, "batched")):
+        mb.set_prims(prims)
+        mb.path = path
+        mb.step(dt, 3)
+        mb.backend.sync()
+        ms = time_graph(mb, dt, steps)
+        legs[name] = {"value": ncells * 3 * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                      "launches_per_step": mb.launches_per_step()}
+    b = legs["batched"]
     # RK3 registers (8/3 of 6 doubles) and the frozen plane's 4 doubles read
     nbytes = 8 * 6 * 8 / 3 + 8 * 4
-    out = {"value": value, "unit": "cell-stage/s", "steps": steps, "ms_per_step": ms / steps,
-           "launches_per_step": mb.launches_per_step(), "dt": dt,
+    peak, peak_kind = peaks()
+    achieved = b["value"] * nbytes / 1e9
+    out = {"value": b["value"], "unit": "cell-stage/s", "steps": steps, "ms_per_step": b["ms_per_step"],
+           "launches_per_step": b["launches_per_step"], "dt": dt,
            "workload": "mixing-layer-256x128x4-8-uneven-blocks-o2-h2-60bar-peng-robinson-double-flux-kepaec-euler-rk3",
-           "path": "per-block kernels, one launch per block and pass",
-           "blocks": [b.cells[0] for b in mb.mesh_blocks],
-           "algorithmic_bytes_per_cell_stage": nbytes, "hbm_gbs_of_algorithmic_bytes": value * nbytes / 1e9}
-    out["packed"] = packed_leg(mb, dt, steps, ncells, 3)
+           "path": "batched: the planes frozen each step (a launch a pass over every block), then per stage Q's "
+                   "halo, the state off the planes and one kernel of each cell's six faces, divergence and combines",
+           "blocks": [b_.cells[0] for b_ in mb.mesh_blocks], "per_block": legs["per_block"], "packed": legs["packed"],
+           "speedup_vs_per_block": legs["per_block"]["ms_per_step"] / b["ms_per_step"],
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_kind": peak_kind, "algorithmic_bytes_per_cell_stage": nbytes}}
     if cpu:
         from oracle.oracle import Oracle
 

@@ -230,6 +230,9 @@ int batched_form(const pgb_case *c) {
     for (int f = 0; f < 6; f++)
       if (B.bc[f] >= 0) return 0;
   }
+  // the double flux's inviscid kepaec case: the fused passes' cell-centric stage
+  if (p.simulator == PGB_EULER_DF)
+    return p.eos == PGB_EOS_REALGAS_DF && p.primary == PGB_FLUX_KEPAEC && p.recon == PGB_RECON_CONSTANT ? 2 : 0;
   if (p.simulator != PGB_EULER && p.simulator != PGB_NAVIER_STOKES) return 0;
   if (p.eos != PGB_EOS_CPG && p.eos != PGB_EOS_TPG) return 0;
   if (p.chemistry == PGB_CHEM_SUBSTEPPED) return 0;
@@ -960,6 +963,7 @@ int fused_attrs(pgb_case *c) {
 
 // one step of the fused path at the current phase
 PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb);
+int prestep_plain(pgb_case *c, int qphys, int &count, int first);
 struct MarkCtx {
   pgb_case *c;
   int *count;
@@ -1012,6 +1016,16 @@ int step_fused(pgb_case *c, int &count) {
   const auto &plan = c->plans[c->phase];
   if (c->form != 2) c->state_stale = true;
   RET(cfl_prologue(c, plan[0].qin, count));
+  if (c->form == 2 && sim_df(c->phys.simulator)) {
+    // the double flux's step start, each pass one launch over every block
+    struct Packed {
+      pgb_case *c;
+      bool was;
+      ~Packed() { c->packed = was; }
+    } keep{c, c->packed};
+    c->packed = true;
+    RET(prestep_plain(c, plan[0].qin, count, 0));
+  }
   CK(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int) * plan.size(), c->stream));
   for (int s = 0; s < (int)plan.size(); s++)
     RET(c->form == 2 ? launch_react(c, plan[s], count) : launch_fused(c, plan[s], s, count));
@@ -2078,6 +2092,7 @@ int pgb_rhs_path(pgb_case *c, int q, int dq, int path) {
   if (q < 0 || q >= c->phys.nregs || dq < 0 || dq >= c->phys.nregs || q == dq)
     return fail(PGB_ERR_ARG, "bad registers");
   RET(prepare(c, true));
+  if (c->form == 2) RET(df_settle(c, c->phys_of[q]));
   int count = 0;
   RET(rhs_fused(c, c->phys_of[q], c->phys_of[dq], count));
   CK(cudaGetLastError());
@@ -2149,7 +2164,7 @@ static int step_begin(pgb_case *c, int nsteps, int path) {
     return fail(PGB_ERR_UNSUPPORTED, "the batched path takes the single-species cpg kepaec case; use the per-block path");
   RET(prepare(c, fused));
   if (!fused) RET(ensure_scratch(c));
-  if (!fused && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
+  if ((!fused || c->form == 2) && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
   return PGB_OK;
 }
 
@@ -2207,7 +2222,7 @@ int pgb_step_timed(pgb_case *c, double dt, int nsteps, int path, float *ms, int 
   if (fused && !fused_capable(c)) return fail(PGB_ERR_UNSUPPORTED, "the batched path does not take this case");
   RET(prepare(c, fused));
   if (!fused) RET(ensure_scratch(c));
-  if (!fused && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
+  if ((!fused || c->form == 2) && !c->stages.empty()) RET(df_settle(c, c->phys_of[c->stages[0].q]));
   k_setscalar<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
   CK(cudaGetLastError());
   c->timing = true;

@@ -276,19 +276,13 @@ __global__ void k_advflux(const BlockDev *__restrict__ blks, int b, const double
 // cell's at F[ne] (peregrine/simulator/eulerdf/kernels/flux/function/kepaec.mako:1-21,
 // the plain flux function/kepaec.mako:2-20); NE + 1 rows per face
 template <int NS, int A>
-__global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
-                             const double *__restrict__ stall, const double *__restrict__ met,
-                             double *__restrict__ Fall, const int2 *__restrict__ ctab = nullptr) {
-  constexpr int NE = 4 + NS, NF = NE + 1;
-  PGB_WHERE(B, t);
-  int i, j, k;
-  if (!face_at<A>(B, t, i, j, k)) return;
-  const long long R = cell_index(B, i, j, k);
+__device__ __forceinline__ void advflux_df_face(const BlockDev &B, const double *__restrict__ Q,
+                                                const double *__restrict__ st, const double *__restrict__ met,
+                                                const long long R, double *F) {
+  constexpr int NE = 4 + NS;
   const long long L = R - (A == 0 ? 1 : A == 1 ? B.X : (long long)B.X * B.Y);
   const long long v = B.vol;
-  const double *Q = Qall + NE * B.cv;
-  const double *st = stall + SW * B.cv;
-  const double *Sp = met + M_NCOMP * B.cv + (M_S + 3 * A) * v + R;
+  const double *Sp = met + (M_S + 3 * A) * v + R;
   const double S0 = Sp[0], S1 = Sp[v], S2 = Sp[2 * v];
   const double uL = Q[1 * v + L] / Q[L], vL = Q[2 * v + L] / Q[L], wL = Q[3 * v + L] / Q[L];
   const double uR = Q[1 * v + R] / Q[R], vR = Q[2 * v + R] / Q[R], wR = Q[3 * v + R] / Q[R];
@@ -298,7 +292,6 @@ __global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const dou
   const double pf = 0.5 * (pR + pL);
   const double rho = 0.5 * (rhoR + rhoL);
   const double C = rho * U;
-  double F[NF];
   F[0] = C;
   F[1] = C * uf + pf * S0;
   F[2] = C * vf + pf * S1;
@@ -328,9 +321,22 @@ __global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const dou
     const double tL = (theta * pL + kappa) * rhoinvL, tR = (theta * pR + kappa) * rhoinvR;
     F[q == 0 ? 4 : NE] = (eps + 0.5 * (cL[q] + cR[q]) + 2.0 * tL * tR / (tL + tR)) * C + Kj + Pj;
   }
+}
+
+template <int NS, int A>
+__global__ void k_advflux_df(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
+                             const double *__restrict__ stall, const double *__restrict__ met,
+                             double *__restrict__ Fall, const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS, NF = NE + 1;
+  PGB_WHERE(B, t);
+  int i, j, k;
+  if (!face_at<A>(B, t, i, j, k)) return;
+  const long long R = cell_index(B, i, j, k);
+  double F[NF];
+  advflux_df_face<NS, A>(B, Qall + NE * B.cv, stall + SW * B.cv, met + M_NCOMP * B.cv, R, F);
   double *Fo = Fall + NF * B.cv + R;
 #pragma unroll
-  for (int l = 0; l < NF; l++) Fo[l * v] = F[l];
+  for (int l = 0; l < NF; l++) Fo[l * B.vol] = F[l];
 }
 
 // the advective face flux of a Riemann solver FN on the cells as they are

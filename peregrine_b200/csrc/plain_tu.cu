@@ -371,6 +371,21 @@ extern "C" int PGB_ENTRY(pgb_plain_production_)(long long n, const double *rho, 
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "production");
 }
 
+namespace {
+struct PrestepArgs {
+  double *Q;
+  int first;
+};
+void prestep_fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const PrestepArgs &a = *(const PrestepArgs *)ctx;
+  k_fromQ<NS, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, a.first ? 0 : 1);
+}
+void prestep_freeze_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const PrestepArgs &a = *(const PrestepArgs *)ctx;
+  k_freeze<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct);
+}
+}  // namespace
+
 // the double flux's step start: the state of Q (the eos's fromrhoE on the
 // first step, the frozen planes' after), the planes frozen anew on the
 // interior with the energy reset to the eos's, then Q and the state (planes
@@ -378,12 +393,19 @@ extern "C" int PGB_ENTRY(pgb_plain_production_)(long long n, const double *rho, 
 // (peregrine/simulator/eulerdf/simulator.py:58-66)
 extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int first) {
   cudaStream_t s = pc->stream;
-  for (int b = 0; b < pc->nblocks; b++) {
-    const BlockDev &D = pc->h_blks[b];
-    k_fromQ<NS, true><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, nullptr, first ? 0 : 1);
-    mark(pc, 2);
-    k_freeze<NS><<<grid_of(range_size(D, R_INNER)), TH, 0, s>>>(pc->d_blks, b, Q, pc->state);
-    mark(pc, 2);
+  if (pc->packed) {
+    // each pass one launch over every block
+    const PrestepArgs pa{Q, first};
+    for_blocks(pc, R_VOL, prestep_fromQ_launch, &pa, 2);
+    for_blocks(pc, R_INNER, prestep_freeze_launch, &pa, 2);
+  } else {
+    for (int b = 0; b < pc->nblocks; b++) {
+      const BlockDev &D = pc->h_blks[b];
+      k_fromQ<NS, true><<<grid_of(D.vol), TH, 0, s>>>(pc->d_blks, b, Q, pc->state, nullptr, first ? 0 : 1);
+      mark(pc, 2);
+      k_freeze<NS><<<grid_of(range_size(D, R_INNER)), TH, 0, s>>>(pc->d_blks, b, Q, pc->state);
+      mark(pc, 2);
+    }
   }
   k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(Q, pc->halo, pc->nhalo, NE, 1, pc->rots);
   mark(pc, 0);
@@ -447,12 +469,39 @@ void rapply_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const voi
   const RApplyCtx &r = *(const RApplyCtx *)ctx;
   k_rapply<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, pc->F[0], pc->F[1], pc->F[2], pc->met, r.a, ct);
 }
+struct RCellFluxCtx {
+  const double *Q;
+  RApplyArgs a;
+};
+void rcellflux_df_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RCellFluxCtx &r = *(const RCellFluxCtx *)ctx;
+  k_rcellflux_df<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, pc->met, r.a, ct);
+}
 }  // namespace
 
 extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs) {
   cudaStream_t s = pc->stream;
   k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(rs->Q), pc->halo, pc->nhalo, NE, 1, pc->rots);
   mark(pc, 0);
+  if (pc->df) {
+    // the double flux, inviscid, kepaec: the state off each cell's frozen
+    // plane (halo included), then a cell a thread of its six faces, the
+    // divergence and the combines
+    const RhsArgs q{rs->Q, rs->dQ};
+    for_blocks(pc, R_VOL, fromQ_launch, &q, 8);
+    RCellFluxCtx cf{};
+    cf.Q = rs->Q;
+    RApplyArgs &a = cf.a;
+    a.dQ = rs->dQ;
+    a.dt = pc->dt;
+    a.write_dq = rs->write_dq;
+    a.ncomb = rs->ncomb;
+    a.comb[0] = rs->comb[0];
+    a.comb[1] = rs->comb[1];
+    for_blocks(pc, R_INNER, rcellflux_df_launch, &cf, 1);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PGB_OK : cuda_fail(e, "fused double-flux stage");
+  }
   for_blocks(pc, R_VOL, pc->visc ? rcell_launch<true> : rcell_launch<false>, rs, 8);
   const bool chem = pc->chem == PGB_CHEM_COUPLED;
   if (chem) for_blocks(pc, R_INNER, rsource_launch, rs, 2);

@@ -168,4 +168,58 @@ __global__ void __launch_bounds__(256) k_rapply(const BlockDev *__restrict__ blk
   }
 }
 
+// The double flux's stage for an inviscid gas with kepaec, a cell a thread:
+// its six faces' two-point fluxes (each face formed by both cells it joins;
+// kepaec reads the two cells alone), the divergence in the per-block
+// applyflux_df's order (the energy row takes the second energy row on the
+// cell's low faces, where it is the right cell, the first on its high
+// faces), and the stage's combines
+// (peregrine/simulator/eulerdf/kernels/flux/function/kepaec.mako:1-21,
+//  peregrine/simulator/eulerdf/kernels/applyflux.mako:2-14)
+template <int NS>
+__global__ void __launch_bounds__(256) k_rcellflux_df(const BlockDev *__restrict__ blks, int b,
+                                                      const double *__restrict__ Qall,
+                                                      const double *__restrict__ stall,
+                                                      const double *__restrict__ met, const RApplyArgs a,
+                                                      const int2 *__restrict__ ctab = nullptr) {
+  constexpr int NE = 4 + NS, NF = NE + 1;
+  PGB_WHERE(B, t);
+  if (t >= (long long)B.nx * B.ny * B.nz) return;
+  const int i = (int)(t % B.nx) + NG, j = (int)((t / B.nx) % B.ny) + NG, k = (int)(t / ((long long)B.nx * B.ny)) + NG;
+  const long long c = cell_index(B, i, j, k), v = B.vol;
+  const long long sJ = B.X, sK = (long long)B.X * B.Y;
+  const double *Q = Qall + NE * B.cv, *st = stall + SW * B.cv, *M = met + M_NCOMP * B.cv;
+  double fi[NF], fj[NF], fk[NF], gi[NF], gj[NF], gk[NF];
+  advflux_df_face<NS, 0>(B, Q, st, M, c, fi);
+  advflux_df_face<NS, 1>(B, Q, st, M, c, fj);
+  advflux_df_face<NS, 2>(B, Q, st, M, c, fk);
+  advflux_df_face<NS, 0>(B, Q, st, M, c + 1, gi);
+  advflux_df_face<NS, 1>(B, Q, st, M, c + sJ, gj);
+  advflux_df_face<NS, 2>(B, Q, st, M, c + sK, gk);
+  const double detJinv = M[M_DETJINV * v + c];
+  const long long at = NE * B.cv + c;
+  const double dt = *a.dt;
+  double first[NE];
+#pragma unroll
+  for (int l = 0; l < NE; l++) {
+    const int lo = l == 4 ? NE : l;
+    const double dq = (fi[lo] + fj[lo] + fk[lo] - gi[l] - gj[l] - gk[l]) * detJinv;
+    if (a.write_dq) a.dQ[at + l * v] = dq;
+    for (int m = 0; m < a.ncomb; m++) {
+      const RCombine &cb = a.comb[m];
+      auto val = [&](int n) {
+        const int s = cb.src[n];
+        return s == -1 ? dq : s == -2 ? first[l] : cb.X[n][at + l * v];
+      };
+      auto term = [&](int n) {
+        return (cb.step && n == cb.nterms - 1) ? cb.w[n] * dt * val(n) : cb.w[n] * val(n);
+      };
+      double acc = term(0);
+      for (int n = 1; n < cb.nterms; n++) acc = acc + term(n);
+      if (m == 0) first[l] = acc;
+      if (cb.write) cb.out[at + l * v] = acc;
+    }
+  }
+}
+
 }  // namespace pgb

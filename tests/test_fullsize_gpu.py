@@ -148,16 +148,18 @@ def test_one_step_of_the_benchmark_reacting_field_matches_the_oracle():
     assert rowmax(b.Q.get()[b.mesh.interior], w[b.mesh.interior]).max() < 1e-9
 
 
-def test_three_steps_of_the_benchmark_mixing_layer_match_the_oracle():
+@pytest.mark.parametrize("launch", ["batched", "per-block"])
+def test_three_steps_of_the_benchmark_mixing_layer_match_the_oracle(launch):
     import peregrine_b200 as pg
     from oracle.oracle import Oracle
 
-    cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3")
+    cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3", launch=launch)
     mesh = cases.mixing_layer_mesh(256, 128, 4, 8, seed=bench.SEED)
     mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
     prims = cases.mixing_layer_prims(mb.metrics, 128, seed=bench.SEED)
     mb.set_prims(prims)
     assert len(mb.blocks) == 8 and sum(b.ncells for b in mb.mesh_blocks) == 256 * 128 * 4
+    assert mb.path == (native.PATH_BATCHED if launch == "batched" else native.PATH_PER_BLOCK)
     adv = cfg["adv-flux"]
     orc = Oracle(mb.mixture.constants(), mb.ns, "euler-df", mb.mesh_blocks, mb.metrics, "tvd-rk3",
                  eos=cfg["mixture"]["eos"], trans=cfg["mixture"]["trans"], primary=adv["primary"],

@@ -65,7 +65,11 @@ def test_the_batched_forms():
     mb, _ = reacting("batched")
     assert mb.batched_form() == 2 and mb.path == native.PATH_BATCHED
     cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3", launch="batched")
-    rg = pg.get_solver(cfg, cases.mixing_layer_mesh(16, 8, 2, 2, seed=0, low=6, high=10), pg.get_backend("cuda", cfg))
+    mesh = cases.mixing_layer_mesh(16, 8, 2, 2, seed=0, low=6, high=10)
+    df = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    assert df.batched_form() == 2 and df.path == native.PATH_BATCHED
+    cfg = cases.mixing_layer_config("pr", "navier-stokes-df", "tvd-rk3", launch="batched")
+    rg = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
     assert rg.batched_form() == 0 and rg.path == native.PATH_PACKED
 
 

@@ -141,3 +141,46 @@ def test_the_packed_path_steps_as_the_per_block_path(simulator):
     assert mb.launches_per_step() < ref.launches_per_step()
     for a, b in zip(mb.blocks, ref.blocks):
         assert np.array_equal(a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior])
+
+
+def test_the_double_flux_batched_path_is_the_per_block_paths():
+    # the inviscid double flux with kepaec on the batched path: the frozen
+    # planes each step (each pass one launch over every block), then per
+    # stage Q's halo, the state off the planes and one kernel of a cell's six
+    # faces, divergence and combines
+    from peregrine_b200 import native
+
+    mb, orc = build("pr", "euler-df", nx=24, ny=16, blocks=3)
+    ref, _ = build("pr", "euler-df", nx=24, ny=16, blocks=3)
+    mb.path = native.PATH_BATCHED
+    assert mb.batched_form() == 2
+    dt = 2e-9
+    mb.step(dt, 3)
+    ref.step(dt, 3)
+    for _ in range(3):
+        orc.step(dt)
+    # the freeze (4 launches: fromQ, freeze, Q's and the state's halo) and three stages of three
+    assert mb.launches_per_step() == 4 + 3 * 3
+    for a, b, w in zip(mb.blocks, ref.blocks, orc.regs[0]):
+        got, same = a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior]
+        scale = np.abs(same).reshape(-1, same.shape[-1]).max(axis=0)
+        assert np.all(np.abs(got - same).reshape(-1, same.shape[-1]).max(axis=0) <= 1e-12 * scale)
+        want = w[a.mesh.interior]
+        scale = np.abs(want).reshape(-1, want.shape[-1]).max(axis=0)
+        scale[1:4] = scale[1:4].max()
+        assert np.all(np.abs(got - want).reshape(-1, want.shape[-1]).max(axis=0) <= 1e-9 * scale)
+
+
+def test_the_double_flux_batched_rhs_is_the_per_block_rhs():
+    from peregrine_b200 import native
+
+    mb, _ = build("pr", "euler-df")
+    ref, _ = build("pr", "euler-df")
+    mb.path = native.PATH_BATCHED
+    dq = mb.regs[-1]
+    mb.rhs(Q="Q", dQ=dq)
+    ref.rhs(Q="Q", dQ=dq)
+    for a, b in zip(mb.blocks, ref.blocks):
+        got, want = getattr(a, dq).get()[a.mesh.interior], getattr(b, dq).get()[b.mesh.interior]
+        scale = np.abs(want).reshape(-1, want.shape[-1]).max(axis=0)
+        assert np.all(np.abs(got - want).reshape(-1, want.shape[-1]).max(axis=0) <= 1e-12 * scale)
