@@ -466,9 +466,11 @@ def boundary_leg(steps, cpu=True):
     return out
 
 
-def serving_leg(n=300, rate=60.0, steps=100):
+def serving_leg(n=300, rate=60.0, steps=100, sweep=(30.0, 120.0, 480.0, 1920.0), nsweep=200):
     """The serving stream: Poisson arrivals of H2/air closed reactors and
-    periodic 1-D domains, admitted into one pool while others run."""
+    periodic 1-D domains, admitted into one pool while others run; then the
+    same mix at other arrival rates (nsweep requests each), for the latency
+    against the load."""
     import ctypes
 
     import peregrine_b200 as pg
@@ -495,11 +497,25 @@ def serving_leg(n=300, rate=60.0, steps=100):
     t0 = time.perf_counter()
     srv.run(reqs, 3)
     wall = time.perf_counter() - t0
-    pool.close()
     st = serving.latency_stats(reqs)
     zero = [r for r in reqs if r.kind == "0d"]
     one = [r for r in reqs if r.kind == "1d"]
-    return {"requests": n, "arrival_rate_per_s": rate, "steps_per_request": steps, "dt": dt,
+    loads = []
+    for k, lam in enumerate(sweep):
+        more = serving.requests(nsweep, lam, proto.mixture.spnames, consts["MW"], seed=SEED + 2 + k, steps=steps)
+        for r in more:
+            serving.box_metrics(r.cells, r.lengths)
+        sv = serving.Server(pool, dt)
+        ta = time.perf_counter()
+        sv.run(more, 3)
+        w = time.perf_counter() - ta
+        ls = serving.latency_stats(more)
+        loads.append({"arrival_rate_per_s": lam, "requests": nsweep, "requests_per_s": nsweep / w,
+                      "p50_ms": ls["p50_ms"], "p99_ms": ls["p99_ms"],
+                      "mean_running": sv.running_sum / max(sv.steps, 1), "pool_steps": sv.steps,
+                      "device_ms": sv.device_ms, "admit_s": sv.admit_s})
+    pool.close()
+    return {"requests": n, "arrival_rate_per_s": rate, "steps_per_request": steps, "dt": dt, "sweep": loads,
             "cell_stages_per_s": srv.cell_stages / wall, "requests_per_s": n / wall, "wall_s": wall,
             "device_ms": srv.device_ms, "pool_steps": srv.steps, "launches": srv.launches,
             "mean_running": srv.running_sum / max(srv.steps, 1), "admit_s": srv.admit_s,

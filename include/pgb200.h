@@ -466,6 +466,13 @@ int pgb_pool_destroy(pgb_pool *p);
 /* a slot for an ni x nj x nk block; PGB_ERR_NOMEM when no slot or arena
  * range is free (queue the case and admit it once another is released) */
 int pgb_pool_admit(pgb_pool *p, int ni, int nj, int nk, int *slot);
+/* A slot for a closed constant-volume reactor (the reference's auto-ignition
+ * box, examples/autoIgnition.py:33-56): a uniform closed box has no flux
+ * divergence, so the pool keeps it as one cell with no grid and steps it by
+ * its eos, its finite-rate source and the stage's combines alone; its
+ * primitives and register are ne values (pgb_pool_set_prims, pgb_pool_get).
+ * For the coupled chemistry on the thermally perfect gas. */
+int pgb_pool_admit_reactor(pgb_pool *p, int *slot);
 /* the slot's metrics and primitives, laid out as pgb_metric_set's and pgb_set_prims' */
 int pgb_pool_metric_set(pgb_pool *p, int slot, int which, const double *host, long count);
 int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count);

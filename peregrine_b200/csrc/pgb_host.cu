@@ -38,7 +38,7 @@ PGB_PLAIN_DECL(12)
 namespace {
 #define PGB_OPS(N)                                                                                          \
   {pgb_plain_upload_##N, pgb_plain_rhs_##N, pgb_plain_fromprims_##N, pgb_plain_production_##N, pgb_plain_prestep_##N, \
-   pgb_plain_cflmax_##N, pgb_plain_fused_##N}
+   pgb_plain_cflmax_##N, pgb_plain_fused_##N, pgb_plain_reactors_##N, pgb_plain_reactor_prims_##N}
 // the per-block path of each species count, 1 to MAXNS
 const PlainOps kPlain[MAXNS] = {PGB_OPS(1), PGB_OPS(2), PGB_OPS(3), PGB_OPS(4),  PGB_OPS(5),  PGB_OPS(6),
                                 PGB_OPS(7), PGB_OPS(8), PGB_OPS(9), PGB_OPS(10), PGB_OPS(11), PGB_OPS(12)};
@@ -2425,7 +2425,8 @@ struct PoolSlot {
   int nx = 0, ny = 0, nz = 0;
   long long cv = 0, vol = 0;
   int steps_left = 0;
-  int active = -1;  // its row in the running table
+  int active = -1;   // its row in the running table
+  int reactor = -1;  // a closed reactor's row in the reactor table (no block)
 };
 
 struct pgb_pool {
@@ -2451,6 +2452,16 @@ struct pgb_pool {
   long long halo_cap = 0, nhalo = 0, nhalo_l0 = 0;
   int2 *d_ctab = nullptr;  // the running blocks' tile tables, one per range, end to end
   long long ctab_cap = 0, ctab_off[5] = {}, nctab[5] = {};
+  // closed constant-volume reactors, a cell each: registers [component][rcap]
+  // per register, each reactor's last T, the free rows, the running rows
+  long long rcap = 0;
+  double *d_rq[MAXREGS] = {};
+  double *d_rT = nullptr;
+  std::vector<int> rfree;
+  std::vector<int> rrun;
+  int *d_rrun = nullptr;
+  // the fused passes take the blocks' stages (the case's batched form 2)
+  bool fused = false;
   std::vector<PoolSlot> slots;
   std::map<long long, long long> free_;  // arena ranges: start -> cells
   std::vector<BlockDev> run;             // running blocks, host copy
@@ -2491,11 +2502,16 @@ BlockDev slot_dev(const PoolSlot &s) {
 // halos NG deep, every block's first layer before any second layer
 int pool_rebuild(pgb_pool *p) {
   p->run.clear();
+  p->rrun.clear();
   std::vector<HaloEntry> l0, l1;
   for (size_t q = 0; q < p->slots.size(); q++) {
     PoolSlot &s = p->slots[q];
     s.active = -1;
     if (s.state != 2) continue;
+    if (s.reactor >= 0) {
+      p->rrun.push_back(s.reactor);
+      continue;
+    }
     s.active = (int)p->run.size();
     const BlockDev D = slot_dev(s);
     p->run.push_back(D);
@@ -2536,6 +2552,8 @@ int pool_rebuild(pgb_pool *p) {
     CK(cudaMemcpyAsync(p->d_halo, l0.data(), sizeof(HaloEntry) * p->nhalo, cudaMemcpyHostToDevice, p->stream));
   if (!p->run.empty())
     CK(cudaMemcpyAsync(p->d_run, p->run.data(), sizeof(BlockDev) * p->run.size(), cudaMemcpyHostToDevice, p->stream));
+  if (!p->rrun.empty())
+    CK(cudaMemcpyAsync(p->d_rrun, p->rrun.data(), sizeof(int) * p->rrun.size(), cudaMemcpyHostToDevice, p->stream));
   // each range's tiles: as many 256-thread CTAs as each block needs, no more
   std::vector<int2> tiles;
   for (int r = 0; r < 5; r++) {
@@ -2595,6 +2613,7 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.chem = p->phys.chemistry == PGB_CHEM_COUPLED;
   pc.realgas = p->phys.eos == PGB_EOS_REALGAS || p->phys.eos == PGB_EOS_REALGAS_DF;
   pc.packed = 1;
+  pc.dt = p->d_dt;
   pc.stream = p->stream;
   return pc;
 }
@@ -2666,6 +2685,20 @@ int pgb_pool_create(const pgb_case *proto, long long max_cells, int max_blocks, 
   CK(cudaMalloc(&p->d_dt, sizeof(double)));
   CK(cudaMalloc(&p->d_blks, sizeof(BlockDev) * max_blocks));
   CK(cudaMalloc(&p->d_run, sizeof(BlockDev) * max_blocks));
+  // a closed reactor a slot at most
+  p->rcap = max_blocks;
+  for (int r = 0; r < p->phys.nregs; r++) {
+    CK(cudaMalloc(&p->d_rq[r], sizeof(double) * ne * p->rcap));
+    CK(cudaMemsetAsync(p->d_rq[r], 0, sizeof(double) * ne * p->rcap, p->stream));
+  }
+  CK(cudaMalloc(&p->d_rT, sizeof(double) * p->rcap));
+  CK(cudaMalloc(&p->d_rrun, sizeof(int) * p->rcap));
+  for (int r = (int)p->rcap - 1; r >= 0; r--) p->rfree.push_back(r);
+  // the blocks step on the fused passes where the physics takes them: the
+  // ideal gases (every pool block is periodic onto itself, of two cells or
+  // more per axis, so neither a boundary nor a block's size bars them)
+  p->fused = (p->phys.simulator == PGB_EULER || p->phys.simulator == PGB_NAVIER_STOKES) &&
+             (p->phys.eos == PGB_EOS_CPG || p->phys.eos == PGB_EOS_TPG);
   *out = p.release();
   return PGB_OK;
 }
@@ -2675,8 +2708,10 @@ int pgb_pool_destroy(pgb_pool *p) {
   if (p->stream) cudaStreamSynchronize(p->stream);
   for (auto &r : p->d_reg)
     if (r) cudaFree(r);
+  for (auto &r : p->d_rq)
+    if (r) cudaFree(r);
   void *ptrs[] = {p->d_met, p->d_state, p->d_tr, p->d_hsp, p->d_grads, p->d_F[0], p->d_F[1], p->d_F[2],
-                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo, p->d_ctab};
+                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo, p->d_ctab, p->d_rT, p->d_rrun};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->ev0) cudaEventDestroy(p->ev0);
@@ -2725,9 +2760,32 @@ int pgb_pool_admit(pgb_pool *p, int ni, int nj, int nk, int *slot) {
   return PGB_OK;
 }
 
+// a slot for a closed constant-volume reactor: a cell, no grid
+int pgb_pool_admit_reactor(pgb_pool *p, int *slot) {
+  if (!p || !slot) return fail(PGB_ERR_ARG, "null argument");
+  if (p->phys.chemistry != PGB_CHEM_COUPLED) return fail(PGB_ERR_UNSUPPORTED, "a reactor takes the coupled chemistry");
+  if (p->phys.eos != PGB_EOS_TPG) return fail(PGB_ERR_UNSUPPORTED, "a reactor takes the thermally perfect gas");
+  int id = -1;
+  for (int q = 0; q < (int)p->slots.size(); q++)
+    if (p->slots[q].state == 0) {
+      id = q;
+      break;
+    }
+  if (id < 0 || p->rfree.empty()) return fail(PGB_ERR_NOMEM, "every slot of the pool is taken");
+  PoolSlot &s = p->slots[id];
+  s = PoolSlot{};
+  s.state = 1;
+  s.nx = s.ny = s.nz = 1;
+  s.reactor = p->rfree.back();
+  p->rfree.pop_back();
+  *slot = id;
+  return PGB_OK;
+}
+
 // a slot's metric array, laid out as pgb_metric_set's
 int pgb_pool_metric_set(pgb_pool *p, int slot, int which, const double *host, long count) {
   RET(pool_slot(p, slot, 1));
+  if (p->slots[slot].reactor >= 0) return fail(PGB_ERR_ARG, "a reactor has no grid");
   if (!host || which < 0 || which >= PGB_NMETRICS) return fail(PGB_ERR_ARG, "no such metric");
   const BlockDev D = slot_dev(p->slots[slot]);
   static const int comps[PGB_NMETRICS] = {3, 1, 9, 3, 3, 3, 3, 3, 3};
@@ -2765,6 +2823,8 @@ int pgb_pool_set_prims(pgb_pool *p, int slot, const double *host, long count) {
   RET(pool_current(p));
   RET(pool_stage_host(p, count));
   CK(cudaMemcpyAsync(p->d_host, host, sizeof(double) * count, cudaMemcpyHostToDevice, p->stream));
+  if (s.reactor >= 0)
+    return kPlain[p->phys.ns - 1].reactor_prims(p->d_host, p->d_rq[0], p->d_rT, s.reactor, p->rcap, p->stream);
   // the unit reads the launch size from the host table at the slot's index
   std::vector<BlockDev> hb((size_t)slot + 1);
   hb[slot] = slot_dev(s);
@@ -2797,15 +2857,63 @@ int pgb_pool_step(pgb_pool *p, double dt, int nsteps) {
   CK(cudaEventRecord(p->ev0, p->stream));
   for (int it = 0; it < nsteps; it++) {
     if (p->dirty) RET(pool_rebuild(p));
-    const int nrun = (int)p->run.size();
-    if (nrun == 0) break;
+    const int nrun = (int)p->run.size(), nreac = (int)p->rrun.size();
+    if (nrun == 0 && nreac == 0) break;
     PlainCase pc = pool_plain(p, p->d_run, p->run.data(), nrun);
     pool_tiles(p, pc);
     pc.mark = count_cb;
     pc.ctx = &launches;
     const dim3 g((unsigned)p->nctab[R_INNER], 1, 1);
     const int2 *inner_tiles = pc.ctab[R_INNER];
+    // a stage's combines on a register table, in place: own first, dQ as
+    // src -1, the first combine's value (already in the thread) as src -2
+    auto combines = [&](const pgb_stage &st, double *const *reg, RCombine *out) {
+      int written0 = -1;
+      auto term = [&](RCombine &rc, int n, int r, double w) {
+        const bool dq = r < 0 || r == st.dq;
+        rc.src[n] = dq ? -1 : r == written0 ? -2 : 0;
+        rc.X[n] = rc.src[n] < 0 ? nullptr : reg[r];
+        rc.w[n] = w;
+      };
+      for (int m = 0; m < st.ncombine; m++) {
+        const pgb_combine &cb = st.combine[m];
+        RCombine &rc = out[m];
+        rc = RCombine{};
+        rc.out = reg[cb.out];
+        rc.step = cb.step;
+        rc.write = 1;
+        int n = 0;
+        if (cb.own) term(rc, n++, cb.out, cb.wout);
+        for (int q = 0; q < cb.nterms; q++) term(rc, n++, cb.reg[q], cb.w[q]);
+        rc.nterms = n;
+        if (m == 0) written0 = cb.out;
+      }
+    };
     for (const pgb_stage &st : p->stages) {
+      if (nreac) {
+        ReactorStage rs{};
+        rs.Q = p->d_rq[st.q];
+        rs.T = p->d_rT;
+        rs.rows = p->d_rrun;
+        rs.n = nreac;
+        rs.cap = p->rcap;
+        rs.dt = p->d_dt;
+        rs.ncomb = st.ncombine;
+        combines(st, p->d_rq, rs.comb);
+        RET(kPlain[p->phys.ns - 1].reactors(&rs, p->stream));
+        launches++;
+      }
+      if (nrun == 0) continue;
+      if (p->fused) {
+        // the fused passes: the divergence and the combines in one pass
+        RStage r{};
+        r.Q = p->d_reg[st.q];
+        r.dQ = p->d_reg[st.dq];
+        r.ncomb = st.ncombine;
+        combines(st, p->d_reg, r.comb);
+        RET(kPlain[p->phys.ns - 1].fused(&pc, &r));
+        continue;
+      }
       RET(kPlain[p->phys.ns - 1].rhs(&pc, p->d_reg[st.q], p->d_reg[st.dq]));
       for (int m = 0; m < st.ncombine; m++) {
         const pgb_combine &cb = st.combine[m];
@@ -2853,6 +2961,13 @@ int pgb_pool_get(pgb_pool *p, int slot, int reg, double *host, long count) {
   const PoolSlot &s = p->slots[slot];
   if (reg < 0 || reg >= p->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
   if (!host || count != (long)s.nx * s.ny * s.nz * p->ne) return fail(PGB_ERR_ARG, "host array of the wrong size");
+  if (s.reactor >= 0) {
+    // the reactor's column of the [component][capacity] table
+    CK(cudaMemcpy2DAsync(host, sizeof(double), p->d_rq[reg] + s.reactor, sizeof(double) * p->rcap, sizeof(double),
+                         (size_t)p->ne, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    return PGB_OK;
+  }
   RET(pool_stage_host(p, count));
   k_pack<<<grid_for((long long)s.nx * s.ny * s.nz, 256), 256, 0, p->stream>>>(p->d_blks, slot, p->ne, p->d_reg[reg],
                                                                                p->d_host);
@@ -2867,6 +2982,11 @@ int pgb_pool_release(pgb_pool *p, int slot) {
   RET(pool_slot(p, slot, -1));
   PoolSlot &s = p->slots[slot];
   if (s.state == 2) p->dirty = true;
+  if (s.reactor >= 0) {
+    p->rfree.push_back(s.reactor);
+    s = PoolSlot{};
+    return PGB_OK;
+  }
   // give the range back, merged with free neighbours
   long long cv = s.cv, vol = s.vol;
   auto nx = p->free_.lower_bound(cv);

@@ -85,6 +85,20 @@ struct RStage {
   RCombine comb[2];
 };
 
+// the serving pool's reactors' stage (react.cuh, k_reactors): the stage's
+// register and each reactor's last T, the running rows, the table's
+// capacity, the step size and the stage's combines on the reactor registers
+struct ReactorStage {
+  const double *Q;
+  double *T;
+  const int *rows;
+  int n;
+  long long cap;
+  const double *dt;
+  int ncomb;
+  RCombine comb[2];
+};
+
 struct PlainOps {
   int (*upload)(const Species *, const Mech *, const MathTables *, cudaStream_t);
   int (*rhs)(const PlainCase *, const double *Q, double *dQ);
@@ -93,6 +107,8 @@ struct PlainOps {
   int (*prestep)(const PlainCase *, double *Q, int first);
   int (*cflmax)(const PlainCase *, const double *Q, double *out);
   int (*fused)(const PlainCase *, const RStage *);
+  int (*reactors)(const ReactorStage *, cudaStream_t);
+  int (*reactor_prims)(const double *prims, double *Q, double *T, int row, long long cap, cudaStream_t);
 };
 
 }  // namespace pgb
@@ -111,4 +127,8 @@ struct PlainOps {
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_cflmax_##N(const pgb::PlainCase *, const double *,  \
                                                                             double *);                           \
   extern "C" __attribute__((visibility("hidden"))) int pgb_plain_fused_##N(const pgb::PlainCase *,               \
-                                                                           const pgb::RStage *);
+                                                                           const pgb::RStage *);                 \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_reactors_##N(const pgb::ReactorStage *,         \
+                                                                              cudaStream_t);                     \
+  extern "C" __attribute__((visibility("hidden"))) int pgb_plain_reactor_prims_##N(                              \
+      const double *, double *, double *, int, long long, cudaStream_t);

@@ -527,3 +527,18 @@ extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "fused passes");
 }
+
+// the serving pool's reactors: one stage of every running reactor, and a
+// reactor's state from its primitives
+extern "C" int PGB_ENTRY(pgb_plain_reactors_)(const ReactorStage *rs, cudaStream_t s) {
+  if (rs->n > 0) k_reactors<NS><<<grid_of(rs->n), TH, 0, s>>>(*rs);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PGB_OK : cuda_fail(e, "reactors");
+}
+
+extern "C" int PGB_ENTRY(pgb_plain_reactor_prims_)(const double *prims, double *Q, double *T, int row,
+                                                   long long cap, cudaStream_t s) {
+  k_reactor_prims<NS><<<1, 1, 0, s>>>(prims, Q, T, row, cap);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PGB_OK : cuda_fail(e, "reactor primitives");
+}

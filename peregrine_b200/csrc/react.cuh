@@ -222,4 +222,60 @@ __global__ void __launch_bounds__(256) k_rcellflux_df(const BlockDev *__restrict
   }
 }
 
+// Closed constant-volume reactors, a cell each, for the serving pool: a
+// uniform closed box has no flux divergence, so a reactor's stage is fromQ
+// (the Newton from its last T), the finite-rate source and the stage's
+// combines, in one thread (the reference's auto-ignition case, a closed
+// box of Euler and chemistry, examples/autoIgnition.py:33-56; the coupled
+// source, peregrine/simulator/chemint/kernels/source.mako:3-10).  A
+// reactor's registers hold it at row r of a [component][capacity] table.
+template <int NS>
+__global__ void __launch_bounds__(256) k_reactors(const ReactorStage a) {
+  constexpr int NE = 4 + NS;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const long long r = a.rows[t], cap = a.cap;
+  auto Qf = [&](int c) { return a.Q[c * cap + r]; };
+  const State s = fromQ<NS>(Qf, a.T[r]);
+  a.T[r] = s.T;
+  double omega[NS];
+  cellrates<NS>(Qf, s.T, omega);
+  const double dt = *a.dt;
+  double first[NE];
+#pragma unroll
+  for (int l = 0; l < NE; l++) {
+    const double dq = l < 5 ? 0.0 : omega[l - 5];
+    const long long at = l * cap + r;
+    for (int m = 0; m < a.ncomb; m++) {
+      const RCombine &cb = a.comb[m];
+      auto val = [&](int n) {
+        const int src = cb.src[n];
+        return src == -1 ? dq : src == -2 ? first[l] : cb.X[n][at];
+      };
+      auto term = [&](int n) {
+        return (cb.step && n == cb.nterms - 1) ? cb.w[n] * dt * val(n) : cb.w[n] * val(n);
+      };
+      double acc = term(0);
+      for (int n = 1; n < cb.nterms; n++) acc = acc + term(n);
+      if (m == 0) first[l] = acc;
+      if (cb.write) cb.out[at] = acc;
+    }
+  }
+}
+
+// a reactor's Q and starting T from its primitives p, u, v, w, T, Y...
+// (the reference's fromprims, peregrine/simulator/euler/kernels/state/fromprims.mako)
+template <int NS>
+__global__ void k_reactor_prims(const double *__restrict__ prims, double *__restrict__ Q, double *__restrict__ T,
+                                const int row, const long long cap) {
+  constexpr int NE = 4 + NS;
+  double q[NE], Qc[NE];
+#pragma unroll
+  for (int l = 0; l < NE; l++) q[l] = prims[l];
+  const State th = fromprims<NS>(q, Qc);
+#pragma unroll
+  for (int l = 0; l < NE; l++) Q[l * cap + row] = Qc[l];
+  T[row] = th.T;
+}
+
 }  // namespace pgb

@@ -4,8 +4,12 @@ A request is one small case, a single block periodic onto itself: a
 uniform 2 x 2 x 2 box (a closed constant-volume reactor, as the reference's
 auto-ignition example builds one, examples/autoIgnition.py:33-56) or an
 N x 2 x 2 periodic 1-D domain.  The ``Pool`` keeps every admitted case's
-state in one device arena (pgb_pool_* in include/pgb200.h); each step
-advances every running case in the same launches, at one shared dt.  The
+state on the device (pgb_pool_* in include/pgb200.h); each step advances
+every running case in the same launches, at one shared dt.  A closed
+reactor's box is uniform and has no flux divergence, so the pool holds it
+as one cell of a reactor table, stepped by its eos, its source and the
+stage's combines (pgb_pool_admit_reactor); a 1-D domain is a block of the
+arena, stepped by the fused passes.  The
 ``Server`` loop admits arrivals in order whenever the arena has room,
 steps, and reads each case out when its step count is done, so requests
 that arrive while others are on the GPU join them at the next step
@@ -84,6 +88,18 @@ class Pool:
     def admit(self, req):
         """The request's slot, or None when the arena has no room for it now."""
         slot = ctypes.c_int()
+        if req.kind == "0d":
+            q = np.asarray(req.prims, dtype=np.float64).reshape(-1, self.ne)
+            if np.any(q != q[:1]):
+                raise ValueError(f"request {req.rid}: a closed reactor's box is uniform")
+            rc = native.load().pgb_pool_admit_reactor(self.handle, ctypes.byref(slot))
+            if rc == native.ERR_NOMEM:
+                return None
+            native.check(rc)
+            q0 = np.ascontiguousarray(q[0])
+            native.call("pgb_pool_set_prims", self.handle, slot.value, _fptr(q0), q0.size)
+            native.call("pgb_pool_start", self.handle, slot.value, int(req.steps))
+            return slot.value
         rc = native.load().pgb_pool_admit(self.handle, *req.cells, ctypes.byref(slot))
         if rc == native.ERR_NOMEM:
             return None
@@ -110,8 +126,14 @@ class Pool:
         native.call("pgb_pool_done", self.handle, buf, cap, ctypes.byref(n))
         return list(buf[: min(n.value, cap)])
 
-    def take(self, slot, cells):
-        """The slot's Q over its interior, then the slot is free."""
+    def take(self, slot, cells, kind="1d"):
+        """The slot's Q over its interior (a reactor's over its box), then the
+        slot is free."""
+        if kind == "0d":
+            one = np.zeros(self.ne)
+            native.call("pgb_pool_get", self.handle, slot, 0, _fptr(one), one.size)
+            native.call("pgb_pool_release", self.handle, slot)
+            return np.asfortranarray(np.broadcast_to(one, tuple(cells) + (self.ne,)))
         out = np.zeros(tuple(cells) + (self.ne,), order="F")
         native.call("pgb_pool_get", self.handle, slot, 0, _fptr(out), out.size)
         native.call("pgb_pool_release", self.handle, slot)
@@ -166,10 +188,12 @@ class Server:
             self.launches += launches
             self.steps += 1
             self.running_sum += len(running)
-            self.cell_stages += stages_per_step * sum(int(np.prod(r.cells)) for r in running.values())
+            # a reactor is one cell
+            self.cell_stages += stages_per_step * sum(1 if r.kind == "0d" else int(np.prod(r.cells))
+                                                      for r in running.values())
             for slot in self.pool.done():
                 req = running.pop(slot)
-                req.result = self.pool.take(slot, req.cells)
+                req.result = self.pool.take(slot, req.cells, req.kind)
                 req.finished = clock() - t0
                 left -= 1
         return requests

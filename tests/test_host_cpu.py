@@ -206,8 +206,9 @@ class _FakePool:
     def done(self):
         return [s for s, v in self.slots.items() if v[1] <= 0]
 
-    def take(self, slot, cells):
+    def take(self, slot, cells, kind="1d"):
         req, _, need = self.slots.pop(slot)
+        assert kind == req.kind
         self.used -= need
         return np.full(cells, float(req.rid))
 

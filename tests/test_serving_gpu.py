@@ -30,7 +30,7 @@ def run_alone(pool, req):
     while True:
         pool.step(DT, 1)
         if slot in pool.done():
-            return pool.take(slot, req.cells)
+            return pool.take(slot, req.cells, req.kind)
 
 
 def test_a_case_is_the_same_alone_and_in_the_mix():
@@ -54,7 +54,7 @@ def test_a_case_is_the_same_alone_and_in_the_mix():
         step += 1
         for slot in pool.done():
             k = running.pop(slot)
-            mixed[k] = pool.take(slot, reqs[k].cells)
+            mixed[k] = pool.take(slot, reqs[k].cells, reqs[k].kind)
     for k, a in enumerate(alone):
         assert np.array_equal(a, mixed[k]), k
     assert any(r.kind == "0d" for r in reqs) and any(r.kind == "1d" for r in reqs)
@@ -104,3 +104,44 @@ def test_a_closed_reactor_matches_the_oracle():
     # a uniform closed box: the state stays uniform, the chemistry moves it
     assert np.abs(got - got[:1, :1, :1]).max() == 0.0
     assert np.abs(got - req.prims).max() > 0.0
+
+
+def test_a_reactor_equals_its_box_on_the_per_block_path():
+    """The pool's reactor (one cell, no flux) against the 2 x 2 x 2 closed box
+    stepped on the ordinary per-block path, whose fluxes of a uniform state
+    cancel."""
+    import peregrine_b200 as pg
+    from peregrine_b200.mesher import CubeMesher
+
+    mb = proto()
+    reqs = [r for r in some_requests(mb, n=16, steps=15, seed=5) if r.kind == "0d"][:3]
+    pool = serving.Pool(mb, 100_000, 8)
+    for req in reqs:
+        got = run_alone(pool, req)
+        cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True, launch="per-block")
+        mesh = CubeMesher(cells=[[c] for c in req.cells], lengths=list(req.lengths), periodic=[True] * 3)
+        one = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+        one.set_prims([req.prims])
+        one.step(DT, req.steps)
+        want = one.blocks[0].Q.get()[one.mesh_blocks[0].interior]
+        scale = np.abs(want).reshape(-1, want.shape[-1]).max(axis=0)
+        err = np.abs(got - want).reshape(-1, want.shape[-1]).max(axis=0)
+        assert np.all(err <= 1e-13 * np.maximum(scale, 1e-300)), err / scale
+    pool.close()
+
+
+def test_reactors_and_blocks_share_the_slots_and_come_back_free():
+    mb = proto()
+    reqs = some_requests(mb, n=10, steps=4, seed=7)
+    pool = serving.Pool(mb, 400_000, 5)
+    free0, _, _ = pool.info()
+    slots = [pool.admit(r) for r in reqs[:5]]
+    assert None not in slots and len(set(slots)) == 5
+    # every slot taken: a sixth case, reactor or block, waits
+    assert pool.admit(reqs[5]) is None
+    while pool.info()[1]:
+        pool.step(DT, 1)
+    for s, r in zip(slots, reqs[:5]):
+        pool.take(s, r.cells, r.kind)
+    assert pool.info() == (free0, 0, 0)
+    pool.close()
