@@ -513,12 +513,13 @@ def serving_leg(n=300, rate=60.0, steps=100, sweep=(30.0, 120.0, 480.0, 1920.0),
         loads.append({"arrival_rate_per_s": lam, "requests": nsweep, "requests_per_s": nsweep / w,
                       "p50_ms": ls["p50_ms"], "p99_ms": ls["p99_ms"],
                       "mean_running": sv.running_sum / max(sv.steps, 1), "pool_steps": sv.steps,
-                      "device_ms": sv.device_ms, "admit_s": sv.admit_s})
+                      "device_ms": sv.device_ms, "admit_s": sv.admit_s, "admit_max_ms": sv.admit_max_s * 1e3})
     pool.close()
     return {"requests": n, "arrival_rate_per_s": rate, "steps_per_request": steps, "dt": dt, "sweep": loads,
             "cell_stages_per_s": srv.cell_stages / wall, "requests_per_s": n / wall, "wall_s": wall,
             "device_ms": srv.device_ms, "pool_steps": srv.steps, "launches": srv.launches,
             "mean_running": srv.running_sum / max(srv.steps, 1), "admit_s": srv.admit_s,
+            "admit_max_ms": srv.admit_max_s * 1e3,
             "latency_ms": st, "latency_0d_ms": serving.latency_stats(zero) if zero else None,
             "latency_1d_ms": serving.latency_stats(one) if one else None,
             "arena_cells": cap, "per_cell_bytes": per_cell,

@@ -2468,6 +2468,9 @@ struct pgb_pool {
   bool dirty = true;
   float last_ms = 0.0f;
   int last_launches = 0;
+  // one step of the running set, captured; replayed until the set changes
+  cudaGraphExec_t step_graph = nullptr;
+  int step_graph_launches = 0;
 };
 
 namespace {
@@ -2647,6 +2650,87 @@ int pool_stage_host(pgb_pool *p, long long n) {
   return PGB_OK;
 }
 
+// one RK step of the running set's launches on the pool's stream: per stage
+// the reactors' kernel, then the blocks' fused passes (or the right-hand side
+// and the combines)
+int pool_launch_step(pgb_pool *p, int &launches) {
+  const int nrun = (int)p->run.size(), nreac = (int)p->rrun.size();
+  PlainCase pc = pool_plain(p, p->d_run, p->run.data(), nrun);
+  pool_tiles(p, pc);
+  pc.mark = count_cb;
+  pc.ctx = &launches;
+  const dim3 g((unsigned)p->nctab[R_INNER], 1, 1);
+  const int2 *inner_tiles = pc.ctab[R_INNER];
+  // a stage's combines on a register table, in place: own first, dQ as
+  // src -1, the first combine's value (already in the thread) as src -2
+  auto combines = [&](const pgb_stage &st, double *const *reg, RCombine *out) {
+    int written0 = -1;
+    auto term = [&](RCombine &rc, int n, int r, double w) {
+      const bool dq = r < 0 || r == st.dq;
+      rc.src[n] = dq ? -1 : r == written0 ? -2 : 0;
+      rc.X[n] = rc.src[n] < 0 ? nullptr : reg[r];
+      rc.w[n] = w;
+    };
+    for (int m = 0; m < st.ncombine; m++) {
+      const pgb_combine &cb = st.combine[m];
+      RCombine &rc = out[m];
+      rc = RCombine{};
+      rc.out = reg[cb.out];
+      rc.step = cb.step;
+      rc.write = 1;
+      int n = 0;
+      if (cb.own) term(rc, n++, cb.out, cb.wout);
+      for (int q = 0; q < cb.nterms; q++) term(rc, n++, cb.reg[q], cb.w[q]);
+      rc.nterms = n;
+      if (m == 0) written0 = cb.out;
+    }
+  };
+  for (const pgb_stage &st : p->stages) {
+    if (nreac) {
+      ReactorStage rs{};
+      rs.Q = p->d_rq[st.q];
+      rs.T = p->d_rT;
+      rs.rows = p->d_rrun;
+      rs.n = nreac;
+      rs.cap = p->rcap;
+      rs.dt = p->d_dt;
+      rs.ncomb = st.ncombine;
+      combines(st, p->d_rq, rs.comb);
+      RET(kPlain[p->phys.ns - 1].reactors(&rs, p->stream));
+      launches++;
+    }
+    if (nrun == 0) continue;
+    if (p->fused) {
+      // the fused passes: the divergence and the combines in one pass
+      RStage r{};
+      r.Q = p->d_reg[st.q];
+      r.dQ = p->d_reg[st.dq];
+      r.ncomb = st.ncombine;
+      combines(st, p->d_reg, r.comb);
+      RET(kPlain[p->phys.ns - 1].fused(&pc, &r));
+      continue;
+    }
+    RET(kPlain[p->phys.ns - 1].rhs(&pc, p->d_reg[st.q], p->d_reg[st.dq]));
+    for (int m = 0; m < st.ncombine; m++) {
+      const pgb_combine &cb = st.combine[m];
+      CombineDev cd{};
+      cd.out = p->d_reg[cb.out];
+      cd.own = cb.own;
+      cd.wout = cb.wout;
+      cd.nterms = cb.nterms;
+      cd.step = cb.step;
+      for (int n = 0; n < cb.nterms; n++) {
+        cd.X[n] = p->d_reg[cb.reg[n] < 0 ? st.dq : cb.reg[n]];
+        cd.w[n] = cb.w[n];
+      }
+      k_combine<<<g, 256, 0, p->stream>>>(p->d_run, 0, p->ne, cd, p->d_dt, inner_tiles);
+      launches++;
+    }
+  }
+  CK(cudaGetLastError());
+  return PGB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2714,6 +2798,7 @@ int pgb_pool_destroy(pgb_pool *p) {
                   p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo, p->d_ctab, p->d_rT, p->d_rrun};
   for (void *q : ptrs)
     if (q) cudaFree(q);
+  if (p->step_graph) cudaGraphExecDestroy(p->step_graph);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   if (p->stream) forget_stream(p->stream), cudaStreamDestroy(p->stream);
@@ -2847,7 +2932,10 @@ int pgb_pool_start(pgb_pool *p, int slot, int nsteps) {
 }
 
 // nsteps RK steps of every running case at dt; a case whose count runs out
-// is done and leaves the running set after that step
+// is done and leaves the running set after that step.  A step's launches
+// depend on the running set alone (dt is read on the device), so the step is
+// captured once per set and replayed until an admission, a release or a case
+// finishing changes it.
 int pgb_pool_step(pgb_pool *p, double dt, int nsteps) {
   if (!p) return fail(PGB_ERR_ARG, "null pool");
   if (nsteps < 1) return fail(PGB_ERR_ARG, "at least one step");
@@ -2856,82 +2944,29 @@ int pgb_pool_step(pgb_pool *p, double dt, int nsteps) {
   int launches = 0;
   CK(cudaEventRecord(p->ev0, p->stream));
   for (int it = 0; it < nsteps; it++) {
-    if (p->dirty) RET(pool_rebuild(p));
-    const int nrun = (int)p->run.size(), nreac = (int)p->rrun.size();
-    if (nrun == 0 && nreac == 0) break;
-    PlainCase pc = pool_plain(p, p->d_run, p->run.data(), nrun);
-    pool_tiles(p, pc);
-    pc.mark = count_cb;
-    pc.ctx = &launches;
-    const dim3 g((unsigned)p->nctab[R_INNER], 1, 1);
-    const int2 *inner_tiles = pc.ctab[R_INNER];
-    // a stage's combines on a register table, in place: own first, dQ as
-    // src -1, the first combine's value (already in the thread) as src -2
-    auto combines = [&](const pgb_stage &st, double *const *reg, RCombine *out) {
-      int written0 = -1;
-      auto term = [&](RCombine &rc, int n, int r, double w) {
-        const bool dq = r < 0 || r == st.dq;
-        rc.src[n] = dq ? -1 : r == written0 ? -2 : 0;
-        rc.X[n] = rc.src[n] < 0 ? nullptr : reg[r];
-        rc.w[n] = w;
-      };
-      for (int m = 0; m < st.ncombine; m++) {
-        const pgb_combine &cb = st.combine[m];
-        RCombine &rc = out[m];
-        rc = RCombine{};
-        rc.out = reg[cb.out];
-        rc.step = cb.step;
-        rc.write = 1;
-        int n = 0;
-        if (cb.own) term(rc, n++, cb.out, cb.wout);
-        for (int q = 0; q < cb.nterms; q++) term(rc, n++, cb.reg[q], cb.w[q]);
-        rc.nterms = n;
-        if (m == 0) written0 = cb.out;
-      }
-    };
-    for (const pgb_stage &st : p->stages) {
-      if (nreac) {
-        ReactorStage rs{};
-        rs.Q = p->d_rq[st.q];
-        rs.T = p->d_rT;
-        rs.rows = p->d_rrun;
-        rs.n = nreac;
-        rs.cap = p->rcap;
-        rs.dt = p->d_dt;
-        rs.ncomb = st.ncombine;
-        combines(st, p->d_rq, rs.comb);
-        RET(kPlain[p->phys.ns - 1].reactors(&rs, p->stream));
-        launches++;
-      }
-      if (nrun == 0) continue;
-      if (p->fused) {
-        // the fused passes: the divergence and the combines in one pass
-        RStage r{};
-        r.Q = p->d_reg[st.q];
-        r.dQ = p->d_reg[st.dq];
-        r.ncomb = st.ncombine;
-        combines(st, p->d_reg, r.comb);
-        RET(kPlain[p->phys.ns - 1].fused(&pc, &r));
-        continue;
-      }
-      RET(kPlain[p->phys.ns - 1].rhs(&pc, p->d_reg[st.q], p->d_reg[st.dq]));
-      for (int m = 0; m < st.ncombine; m++) {
-        const pgb_combine &cb = st.combine[m];
-        CombineDev cd{};
-        cd.out = p->d_reg[cb.out];
-        cd.own = cb.own;
-        cd.wout = cb.wout;
-        cd.nterms = cb.nterms;
-        cd.step = cb.step;
-        for (int n = 0; n < cb.nterms; n++) {
-          cd.X[n] = p->d_reg[cb.reg[n] < 0 ? st.dq : cb.reg[n]];
-          cd.w[n] = cb.w[n];
-        }
-        k_combine<<<g, 256, 0, p->stream>>>(p->d_run, 0, p->ne, cd, p->d_dt, inner_tiles);
-        launches++;
-      }
+    if (p->dirty) {
+      RET(pool_rebuild(p));
+      if (p->step_graph) cudaGraphExecDestroy(p->step_graph);
+      p->step_graph = nullptr;
     }
-    CK(cudaGetLastError());
+    if (p->run.empty() && p->rrun.empty()) break;
+    if (!p->step_graph) {
+      int n = 0;
+      CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = pool_launch_step(p, n);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+      if (rc != PGB_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc != PGB_OK ? rc : fail(PGB_ERR_CUDA, std::string("pool step capture: ") + cudaGetErrorString(e));
+      }
+      const cudaError_t ei = cudaGraphInstantiate(&p->step_graph, g, 0);
+      cudaGraphDestroy(g);
+      CK(ei);
+      p->step_graph_launches = n;
+    }
+    CK(cudaGraphLaunch(p->step_graph, p->stream));
+    launches += p->step_graph_launches;
     for (auto &s : p->slots)
       if (s.state == 2 && --s.steps_left == 0) s.state = 3, p->dirty = true;
   }

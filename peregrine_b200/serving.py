@@ -157,6 +157,7 @@ class Server:
         self.cell_stages = 0
         self.running_sum = 0
         self.admit_s = 0.0
+        self.admit_max_s = 0.0
 
     def run(self, requests, stages_per_step, clock=time.perf_counter, sleep=time.sleep):
         """Serve every request; arrival times are seconds from the start.
@@ -173,7 +174,9 @@ class Server:
             while q < len(pending) and pending[q].arrival <= now:
                 ta = clock()
                 slot = self.pool.admit(pending[q])
-                self.admit_s += clock() - ta
+                took = clock() - ta
+                self.admit_s += took
+                self.admit_max_s = max(self.admit_max_s, took)
                 if slot is None:
                     break
                 pending[q].admitted = clock() - t0
