@@ -266,6 +266,18 @@ int pgb_exchange(pgb_case *c, int reg);
  * exchange windows, peregrine/multiblock/collections/exchange/collection.py:63-96).
  * A partitioner lists a whole grid's entries on a case it never finalizes. */
 int pgb_case_halo_entries(pgb_case *c, long long cap, long long *out, long long *n);
+/* The same halo cells as the boxes the fill launches over: each face's halo
+ * NG deep and each edge line one deep, as one box wherever one block holds
+ * every cell's source at an index affine in the cell's.  Fourteen long longs
+ * a box: the block it fills, the first cell's index there (full layout), the
+ * index steps along the box's three axes (the filled block's i, j, k), the
+ * extents along them, the block it copies, the first source index, the
+ * source index steps along the same three axes, and the rotation (as
+ * pgb_case_halo_entries').  rest is how many halo cells no box holds (the
+ * fill lists those one by one).  A host computation, before or after
+ * finalize; nboxes is how many there are, up to cap written.  No
+ * counterpart in the reference, whose exchange copies interface windows. */
+int pgb_case_halo_boxes(pgb_case *c, long long cap, long long *out, long long *nboxes, long long *rest);
 /* A shard's exchange with the blocks other ranks hold: the cells it sends
  * (packs) and the halo cells it receives (unpacks), each a block and a cell
  * index, in the order the two sides agree on (the reference's message pools,

@@ -73,6 +73,20 @@ struct HaloEntry {
   int rot;
 };
 
+// A box of halo cells of one block whose sources all lie in one block, the
+// source index an affine map of the destination cell: a face's halo NG deep,
+// an edge line one deep.  The box runs i fastest in the destination, so a
+// warp's threads write neighbouring cells; t = x0 + n0 (x1 + n1 x2) is the
+// thread's cell in it, the indices d0 + x . dst and s0 + x . sst.
+struct HaloPatch {
+  long long dcv, scv;
+  int dvol, svol;
+  int d0, s0;
+  int dst[3], sst[3];
+  int n0, n1, cells;
+  int rot;
+};
+
 // what k_halo turns with an entry's rotation: nothing, the vector at a
 // component (Q's momentum at 1), or the gradients' tensor (each row's three
 // directions, and the velocity rows u, v, w down every direction)

@@ -133,6 +133,12 @@ struct pgb_case {
   double *d_one = nullptr;  // 1.0: the step size of a right-hand side on the fused path
   HaloEntry *d_halo = nullptr;
   long long nhalo = 0, nhalo_l0 = 0;  // all entries; face layer 0 only (first)
+  // the same halo as boxes (k_halo_boxes): the boxes, the CTA table and the
+  // cells no box holds, listed one by one
+  HaloPatch *d_boxes = nullptr;
+  int2 *d_boxcta = nullptr;
+  HaloEntry *d_boxrest = nullptr;
+  long long nboxcta = 0, nboxrest = 0;
   // the rotationally periodic faces' rotations, then the products a halo
   // cell reached across two of them needs, 3 x 3 each
   std::vector<double> rots;
@@ -556,6 +562,101 @@ void build_halo(pgb_case *c, std::vector<HaloEntry> &out, long long &n_l0, std::
   }
 }
 
+// The halo as boxes: each face's halo NG deep and each edge line one deep,
+// the cells build_halo lists, as a box wherever one block holds every cell's
+// source and the source index is affine in the cell's (a face whose
+// neighbour is at least NG cells thick, an edge line along a block); the
+// cells of any other box are listed one by one in rest.
+void build_boxes(pgb_case *c, std::vector<HaloPatch> &boxes, std::vector<HaloEntry> &rest) {
+  boxes.clear();
+  rest.clear();
+  auto box = [&](int b, const int lo[3], const int hi[3]) {
+    const BlockDev &D = c->blocks[b].dev;
+    const int n[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+    std::vector<HaloEntry> es;
+    bool all = true;
+    for (int k = lo[2]; k < hi[2]; k++)
+      for (int j = lo[1]; j < hi[1]; j++)
+        for (int i = lo[0]; i < hi[0]; i++) {
+          int ijk[3] = {i, j, k};
+          int sb, rot;
+          if (!locate(c, b, ijk, sb, rot)) {
+            all = false;
+            continue;
+          }
+          const BlockDev &S = c->blocks[sb].dev;
+          HaloEntry h;
+          h.dcv = D.cv, h.scv = S.cv;
+          h.didx = (int)cell_index(D, i + NG, j + NG, k + NG);
+          h.sidx = (int)cell_index(S, ijk[0] + NG, ijk[1] + NG, ijk[2] + NG);
+          h.dvol = (int)D.vol, h.svol = (int)S.vol;
+          h.rot = rot;
+          es.push_back(h);
+        }
+    if (es.empty()) return;
+    bool affine = all;
+    HaloPatch P{};
+    if (affine) {
+      const HaloEntry &e0 = es[0];
+      P.dcv = e0.dcv, P.scv = e0.scv, P.dvol = e0.dvol, P.svol = e0.svol, P.rot = e0.rot;
+      P.d0 = e0.didx, P.s0 = e0.sidx;
+      const int step[3] = {1, n[0], n[0] * n[1]};
+      for (int d = 0; d < 3; d++) {
+        P.dst[d] = n[d] > 1 ? es[step[d]].didx - e0.didx : 0;
+        P.sst[d] = n[d] > 1 ? es[step[d]].sidx - e0.sidx : 0;
+      }
+      P.n0 = n[0], P.n1 = n[1], P.cells = n[0] * n[1] * n[2];
+      size_t e = 0;
+      for (int k = 0; k < n[2] && affine; k++)
+        for (int j = 0; j < n[1] && affine; j++)
+          for (int i = 0; i < n[0] && affine; i++, e++) {
+            const HaloEntry &h = es[e];
+            affine = h.scv == P.scv && h.svol == P.svol && h.rot == P.rot &&
+                     h.didx == P.d0 + i * P.dst[0] + j * P.dst[1] + k * P.dst[2] &&
+                     h.sidx == P.s0 + i * P.sst[0] + j * P.sst[1] + k * P.sst[2];
+          }
+    }
+    if (affine)
+      boxes.push_back(P);
+    else
+      rest.insert(rest.end(), es.begin(), es.end());
+  };
+  for (int b = 0; b < (int)c->blocks.size(); b++) {
+    const HostBlock &B = c->blocks[b];
+    const int n[3] = {B.nx, B.ny, B.nz};
+    for (int f = 0; f < 6; f++) {
+      const int a = f / 2;
+      int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+      lo[a] = f % 2 == 0 ? -NG : n[a];
+      hi[a] = lo[a] + NG;
+      box(b, lo, hi);
+    }
+    for (int a = 0; a < 3; a++) {
+      const int a1 = (a + 1) % 3, a2 = (a + 2) % 3;
+      for (int s1 = 0; s1 < 2; s1++)
+        for (int s2 = 0; s2 < 2; s2++) {
+          int lo[3], hi[3];
+          lo[a] = 0, hi[a] = n[a];
+          lo[a1] = s1 ? n[a1] : -1, hi[a1] = lo[a1] + 1;
+          lo[a2] = s2 ? n[a2] : -1, hi[a2] = lo[a2] + 1;
+          box(b, lo, hi);
+        }
+    }
+  }
+}
+
+int grid_for(long long n, int threads);
+
+// the full halo of a register, comps components, vec the component its
+// rotations turn: by the boxes when the case has them, else by entries
+void halo_fill_case(pgb_case *c, double *base, int comps, int vec) {
+  if (c->nboxcta > 0)
+    halo_boxes_launch<5, SW>((unsigned)c->nboxcta, c->stream, base, c->d_boxes, c->d_boxcta, c->d_boxrest,
+                               c->nboxrest, comps, vec, c->d_rots);
+  else
+    k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(base, c->d_halo, c->nhalo, comps, vec, c->d_rots);
+}
+
 // the default tile of a block: a width that cuts i evenly in pieces of at
 // most 32, as many rows as 128 threads allow, k cut in two runs
 void default_tile(HostBlock &B) {
@@ -912,7 +1013,7 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
   for (int q = 0; q < 2; q++) a.prep[q] = q < a.npre ? c->d_reg[a.pre[q]] : nullptr;
   a.dt = dtp ? dtp : c->d_dt;
   // the stencil register's halo first
-  k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[p.qin], c->d_halo, c->nhalo, c->ne, 1, c->d_rots);
+  halo_fill_case(c, c->d_reg[p.qin], c->ne, 1);
   mark(c, K_HALO, count);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -1116,6 +1217,8 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.met = c->d_met;
   pc.halo = c->d_halo;
   pc.nhalo = c->nhalo, pc.nhalo_l0 = c->nhalo_l0;
+  pc.boxes = c->d_boxes, pc.boxcta = c->d_boxcta, pc.nboxcta = c->nboxcta;
+  pc.boxrest = c->d_boxrest, pc.nboxrest = c->nboxrest;
   pc.rots = c->d_rots;
   pc.visc = sim_visc(c->phys.simulator);
   pc.packed = c->packed ? 1 : 0;
@@ -1395,7 +1498,7 @@ int pgb_case_destroy(pgb_case *c) {
     if (g) cudaGraphExecDestroy(g);
   for (auto &r : c->d_reg)
     if (r) cudaFree(r);
-  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_one, c->d_xsend, c->d_xrecv, c->d_xsvol, c->d_xrvol, c->d_halo, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
+  void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_one, c->d_xsend, c->d_xrecv, c->d_xsvol, c->d_xrvol, c->d_halo, c->d_boxes, c->d_boxcta, c->d_boxrest, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
                   c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots};
@@ -1597,11 +1700,30 @@ int pgb_exchange(pgb_case *c, int reg) {
   if (!c->finalized) return fail(PGB_ERR_STATE, "the case is not finalized");
   if (reg < 0 || reg >= c->phys.nregs) return fail(PGB_ERR_ARG, "no such register");
   RET(set_current(c));
-  if (c->nhalo)
-    k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_reg[c->phys_of[reg]], c->d_halo, c->nhalo, c->ne, 1,
-                                                           c->d_rots);
+  if (c->nhalo) halo_fill_case(c, c->d_reg[c->phys_of[reg]], c->ne, 1);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
+  return PGB_OK;
+}
+
+int pgb_case_halo_boxes(pgb_case *c, long long cap, long long *out, long long *nboxes, long long *rest) {
+  if (!c || !nboxes || !rest || (cap > 0 && !out)) return fail(PGB_ERR_ARG, "null argument");
+  if (c->blocks.empty()) return fail(PGB_ERR_STATE, "no blocks");
+  // the blocks' layout is a host computation; finalize repeats it
+  if (!c->finalized) layout_blocks(c);
+  std::vector<HaloPatch> boxes;
+  std::vector<HaloEntry> left;
+  build_boxes(c, boxes, left);
+  std::map<long long, int> blk_of;
+  for (int b = 0; b < (int)c->blocks.size(); b++) blk_of[c->blocks[b].dev.cv] = b;
+  *nboxes = (long long)boxes.size();
+  *rest = (long long)left.size();
+  for (long long q = 0; q < *nboxes && q < cap; q++) {
+    const HaloPatch &P = boxes[q];
+    const long long v[14] = {blk_of[P.dcv], P.d0,     P.dst[0], P.dst[1], P.dst[2], P.n0, P.n1, P.cells / (P.n0 * P.n1),
+                             blk_of[P.scv], P.s0,     P.sst[0], P.sst[1], P.sst[2], P.rot};
+    for (int e = 0; e < 14; e++) out[14 * q + e] = v[e];
+  }
   return PGB_OK;
 }
 
@@ -1899,6 +2021,30 @@ int pgb_case_finalize(pgb_case *c) {
   c->nhalo = (long long)halo.size();
   CK(cudaMalloc(&c->d_halo, sizeof(HaloEntry) * std::max<size_t>(1, halo.size())));
   CK(cudaMemcpy(c->d_halo, halo.data(), sizeof(HaloEntry) * halo.size(), cudaMemcpyHostToDevice));
+  {
+    // the boxes, used only when they hold exactly the listed cells
+    std::vector<HaloPatch> boxes;
+    std::vector<HaloEntry> rest;
+    build_boxes(c, boxes, rest);
+    long long cells = (long long)rest.size();
+    for (const HaloPatch &P : boxes) cells += P.cells;
+    if (!boxes.empty() && cells == c->nhalo) {
+      std::vector<int2> cta;
+      for (int q = 0; q < (int)boxes.size(); q++)
+        for (int t = 0; t < (boxes[q].cells + 255) / 256; t++) cta.push_back(make_int2(q, t));
+      for (int t = 0; t < (int)((rest.size() + 255) / 256); t++) cta.push_back(make_int2(-1, t));
+      CK(cudaMalloc(&c->d_boxes, sizeof(HaloPatch) * boxes.size()));
+      CK(cudaMemcpy(c->d_boxes, boxes.data(), sizeof(HaloPatch) * boxes.size(), cudaMemcpyHostToDevice));
+      CK(cudaMalloc(&c->d_boxcta, sizeof(int2) * cta.size()));
+      CK(cudaMemcpy(c->d_boxcta, cta.data(), sizeof(int2) * cta.size(), cudaMemcpyHostToDevice));
+      if (!rest.empty()) {
+        CK(cudaMalloc(&c->d_boxrest, sizeof(HaloEntry) * rest.size()));
+        CK(cudaMemcpy(c->d_boxrest, rest.data(), sizeof(HaloEntry) * rest.size(), cudaMemcpyHostToDevice));
+      }
+      c->nboxcta = (long long)cta.size();
+      c->nboxrest = (long long)rest.size();
+    }
+  }
   if (!c->rots.empty()) {
     CK(cudaMalloc(&c->d_rots, sizeof(double) * c->rots.size()));
     CK(cudaMemcpy(c->d_rots, c->rots.data(), sizeof(double) * c->rots.size(), cudaMemcpyHostToDevice));
@@ -2048,7 +2194,7 @@ int pgb_set_prims(pgb_case *c, int blk, int reg, const double *host, long count)
   RET(kPlain[c->phys.ns - 1].fromprims(&pc, blk, c->d_prims, c->d_reg[c->phys_of[reg]]));
   c->state_stale = false;
   // a halo cell's first Newton starts from the stored T of the cell it copies
-  if (c->nhalo) k_halo<<<grid_for(c->nhalo, 256), 256, 0, c->stream>>>(c->d_state, c->d_halo, c->nhalo, SW);
+  if (c->nhalo) halo_fill_case(c, c->d_state, SW, HALO_SCALARS);
   c->df_fresh = true;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));

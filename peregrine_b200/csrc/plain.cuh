@@ -24,25 +24,104 @@ __device__ __forceinline__ void rotate3(double *x, const long long st, const dou
 // vectors an entry's rotation turns given by vec (a component, or
 // HALO_TENSOR for the gradients), rots the case's rotations, 3 x 3 each
 // (the reference's place kernel, peregrine/multiblock/collections/exchange/kernels/place.mako:3-36)
+// one halo cell: C components (comps of them when C is 0) copied from the
+// source cell, then the vectors its rotation turns.  A source is an interior
+// cell, which no thread of the fill writes, so all of a chunk's components
+// are loaded (read-only path) before any is stored: the loads are in flight
+// together, not one round trip each.
+template <int C, bool ROT = true>
+__device__ __forceinline__ void halo_copy(double *__restrict__ base, const int comps, const int vec,
+                                          const double *__restrict__ rots, const long long dcv, const int didx,
+                                          const int dvol, const long long scv, const int sidx, const int svol,
+                                          const int rot) {
+  double *d = base + comps * dcv + didx;
+  const double *s = base + comps * scv + sidx;
+  if constexpr (C > 0) {
+    double v[C];
+#pragma unroll
+    for (int q = 0; q < C; q++) v[q] = __ldg(s + (long long)q * svol);
+#pragma unroll
+    for (int q = 0; q < C; q++) d[(long long)q * dvol] = v[q];
+  } else {
+    constexpr int CH = 4;
+    for (int c0 = 0; c0 < comps; c0 += CH) {
+      double v[CH];
+#pragma unroll
+      for (int q = 0; q < CH; q++)
+        if (c0 + q < comps) v[q] = __ldg(s + (long long)(c0 + q) * svol);
+#pragma unroll
+      for (int q = 0; q < CH; q++)
+        if (c0 + q < comps) d[(long long)(c0 + q) * dvol] = v[q];
+    }
+  }
+  if (ROT && rot && rots && vec != HALO_SCALARS) {
+    const double *R = rots + 9 * (rot - 1);
+    const long long st = dvol;
+    if (vec >= 0) {
+      rotate3(d + vec * st, st, R);
+    } else {
+      // each row's directions, then the velocity rows down every direction
+      for (int r = 0; r < comps / 3; r++) rotate3(d + 3 * r * st, st, R);
+      for (int m = 0; m < 3; m++) rotate3(d + m * st, 3 * st, R);
+    }
+  }
+}
+
 static __global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps,
                               int vec = HALO_SCALARS, const double *__restrict__ rots = nullptr) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const HaloEntry h = tab[e];
-    double *d = base + comps * h.dcv + h.didx;
-    const double *s = base + comps * h.scv + h.sidx;
-    for (int c = 0; c < comps; c++) d[(long long)c * h.dvol] = s[(long long)c * h.svol];
-    if (h.rot && rots && vec != HALO_SCALARS) {
-      const double *R = rots + 9 * (h.rot - 1);
-      const long long st = h.dvol;
-      if (vec >= 0) {
-        rotate3(d + vec * st, st, R);
-      } else {
-        // each row's directions, then the velocity rows down every direction
-        for (int r = 0; r < comps / 3; r++) rotate3(d + 3 * r * st, st, R);
-        for (int m = 0; m < 3; m++) rotate3(d + m * st, 3 * st, R);
-      }
-    }
+    halo_copy<0>(base, comps, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot);
   }
+}
+
+// the same fill over boxes: CTA x (256 threads) fills chunk cta[x].y of box
+// cta[x].x, or, where cta[x].x is -1, entries 256 cta[x].y .. of the cells no
+// box holds; no per-cell record is read for a box's cells
+template <int C, bool ROT>
+static __global__ void __launch_bounds__(256) k_halo_boxes(double *__restrict__ base,
+                                                           const HaloPatch *__restrict__ boxes,
+                                                           const int2 *__restrict__ cta,
+                                                           const HaloEntry *__restrict__ rest, long long nrest,
+                                                           int comps, int vec = HALO_SCALARS,
+                                                           const double *__restrict__ rots = nullptr) {
+  const int2 w = cta[blockIdx.x];
+  const int t = w.y * 256 + (int)threadIdx.x;
+  if (w.x < 0) {
+    if (t >= nrest) return;
+    const HaloEntry h = rest[t];
+    halo_copy<C, ROT>(base, comps, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot);
+    return;
+  }
+  const HaloPatch &p = boxes[w.x];
+  if (t >= p.cells) return;
+  const int x0 = t % p.n0, r = t / p.n0, x1 = r % p.n1, x2 = r / p.n1;
+  const int didx = p.d0 + x0 * p.dst[0] + x1 * p.dst[1] + x2 * p.dst[2];
+  const int sidx = p.s0 + x0 * p.sst[0] + x1 * p.sst[1] + x2 * p.sst[2];
+  halo_copy<C, ROT>(base, comps, vec, rots, p.dcv, didx, p.dvol, p.scv, sidx, p.svol, p.rot);
+}
+
+// the box fill of a register of comps components: the kernel built for that
+// count where there is one (a stage's Q), else the loop; the rotation code
+// only where the case has rotations and the register has vectors
+template <bool ROT, int... Cs>
+inline void halo_boxes_rot(unsigned grid, cudaStream_t st, double *base, const HaloPatch *boxes, const int2 *cta,
+                           const HaloEntry *rest, long long nrest, int comps, int vec, const double *rots) {
+  bool done = false;
+  ((!done && comps == Cs
+        ? (k_halo_boxes<Cs, ROT><<<grid, 256, 0, st>>>(base, boxes, cta, rest, nrest, comps, vec, rots), done = true)
+        : false),
+   ...);
+  if (!done) k_halo_boxes<0, ROT><<<grid, 256, 0, st>>>(base, boxes, cta, rest, nrest, comps, vec, rots);
+}
+
+template <int... Cs>
+inline void halo_boxes_launch(unsigned grid, cudaStream_t st, double *base, const HaloPatch *boxes, const int2 *cta,
+                              const HaloEntry *rest, long long nrest, int comps, int vec, const double *rots) {
+  if (rots && vec != HALO_SCALARS)
+    halo_boxes_rot<true, Cs...>(grid, st, base, boxes, cta, rest, nrest, comps, vec, rots);
+  else
+    halo_boxes_rot<false, Cs...>(grid, st, base, boxes, cta, rest, nrest, comps, vec, rots);
 }
 
 __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi, int &fj, int &fk) {

@@ -33,6 +33,13 @@ struct PlainCase {
   const double *met;
   const HaloEntry *halo;
   long long nhalo, nhalo_l0;  // every halo entry; the first layer's
+  // the same halo as boxes (k_halo_boxes), when the case has them: the
+  // boxes, the CTA table, its length, the cells no box holds
+  const HaloPatch *boxes;
+  const int2 *boxcta;
+  long long nboxcta;
+  const HaloEntry *boxrest;
+  long long nboxrest;
   const double *rots;         // the rotationally periodic interfaces' rotations, 3 x 3 each
   int visc, primary, recon, limiter;
   int chem;  // 0 none, 1 coupled source, 2 sub-stepped (PGB_CHEM_*)

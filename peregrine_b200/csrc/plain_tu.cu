@@ -46,6 +46,16 @@ void mark(const PlainCase *pc, int kind) {
   if (pc->mark) pc->mark(pc->ctx, kind);
 }
 
+// the full halo of a register (comps components, vec the component its
+// rotations turn): by boxes when the case has them, else by entries
+void halo_fill(const PlainCase *pc, double *base, int comps, int vec) {
+  if (pc->boxcta && pc->nboxcta > 0)
+    halo_boxes_launch<NE, SW>((unsigned)pc->nboxcta, pc->stream, base, pc->boxes, pc->boxcta, pc->boxrest, pc->nboxrest,
+                          comps, vec, pc->rots);
+  else
+    k_halo<<<grid_of(pc->nhalo), TH, 0, pc->stream>>>(base, pc->halo, pc->nhalo, comps, vec, pc->rots);
+}
+
 // a pass over every block: one launch per block, or packed, one launch over
 // them all, by the range's tile table when there is one, else a grid row per
 // block as long as the largest block needs
@@ -248,7 +258,7 @@ static void substep_passes(const PlainCase *pc, const RhsArgs &a) {
 extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, double *dQ) {
   cudaStream_t s = pc->stream;
   const RhsArgs a{Q, dQ};
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(Q), pc->halo, pc->nhalo, NE, 1, pc->rots);
+  halo_fill(pc, const_cast<double *>(Q), NE, 1);
   mark(pc, 0);
   if (pc->packed) {
     for_blocks(pc, R_VOL, fromQ_launch, &a, 2);
@@ -407,9 +417,9 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
       mark(pc, 2);
     }
   }
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(Q, pc->halo, pc->nhalo, NE, 1, pc->rots);
+  halo_fill(pc, Q, NE, 1);
   mark(pc, 0);
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(pc->state, pc->halo, pc->nhalo, SW);
+  halo_fill(pc, pc->state, SW, HALO_SCALARS);
   mark(pc, 0);
   // the boundaries' halo cells from the state just formed, then their planes
   if (pc->nbchalo) {
@@ -481,7 +491,7 @@ void rcellflux_df_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, con
 
 extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs) {
   cudaStream_t s = pc->stream;
-  k_halo<<<grid_of(pc->nhalo), TH, 0, s>>>(const_cast<double *>(rs->Q), pc->halo, pc->nhalo, NE, 1, pc->rots);
+  halo_fill(pc, const_cast<double *>(rs->Q), NE, 1);
   mark(pc, 0);
   if (pc->df) {
     // the double flux, inviscid, kepaec: the state off each cell's frozen

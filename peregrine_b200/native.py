@@ -250,6 +250,8 @@ SIGNATURES = {
     "pgb_fp64_fma_rate": ([ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "pgb_case_halo_entries": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong),
                                ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "pgb_case_halo_boxes": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong),
+                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "pgb_case_set_exchange": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
                                ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
                                ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
