@@ -5,6 +5,7 @@ them, to an .npz that peregrine_b200 loads.
         [--keep H2,H,O,...] [--eos tpg] [--trans kinetic-theory] \\
         [--chemistry finite-rate] [--trange 300 3500] [--cubic srk|pr] \\
         [--diffusion lewis|binary] [--oneway]
+    python -m peregrine_b200.data.export_mixture --integrals REFERENCE OUT.npz
 
 MECHANISM is a mechanism file, or species of the reference's library
 separated by commas.
@@ -192,7 +193,26 @@ def tables(mix):
     return out
 
 
+def integrals(reference):
+    """The collision-integral table the kinetic theory reads (Monchick and
+    Mason's Stockmayer Omega(2,2)* and A* against T* and delta*, as the
+    reference's database carries it), for peregrine_b200.mixgen."""
+    import yaml
+
+    path = os.path.join(reference, "peregrine", "simulator", "mixture", "database", "integrals.yaml")
+    with open(path) as f:
+        ci = yaml.safe_load(f)
+    return {k: np.array(ci[k], dtype=np.float64) for k in ("delta", "tstar22", "omega22", "tstar", "astar")}
+
+
 def main(argv=None):
+    if argv is None:
+        argv = sys.argv[1:]
+    if argv and argv[0] == "--integrals":
+        # python -m peregrine_b200.data.export_mixture --integrals REFERENCE OUT.npz
+        np.savez(argv[2], **integrals(argv[1]))
+        print(argv[2])
+        return
     ap = argparse.ArgumentParser()
     ap.add_argument("reference")
     ap.add_argument("out")

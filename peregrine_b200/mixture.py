@@ -15,13 +15,14 @@ its kernels as hex literals (peregrine/codegen/constants.py:13-20):
 * Lewis diffusion ``lewis``, one unless a species states its own
   (simulator/mixture/diffusion/lewis.py).
 
-A thermally perfect gas, kinetic-theory transport and finite-rate chemistry
-take tables the reference's own mixture code works out from its species
-database and mechanism files (polynomial refits in ln T, collision-integral
-fits, reaction columns).  Those are not restated here: they are read from an
-.npz that peregrine_b200/data/export_mixture.py wrote by running the
-reference's mixture once, offline.  Name such a table set (a file under
-peregrine_b200/data, or a path) as ``mixture.species``.
+A thermally perfect gas, kinetic-theory transport, finite-rate chemistry and
+the cubic real gas take tables worked out from a mechanism's species and
+reactions (polynomial refits in ln T, collision-integral fits, reaction
+columns).  Name as ``mixture.species`` either a Cantera-format mechanism file
+(``.yaml``/``.yml``), whose tables peregrine_b200.mixgen works out here as the
+reference's mixture models do (the case states its ``T-range``), or a table
+set: a file under peregrine_b200/data, or a path to an .npz, as
+peregrine_b200/data/export_mixture.py or mixgen writes one.
 """
 
 import os
@@ -49,10 +50,35 @@ def load_tables(name):
         return {k: z[k] for k in z.files}
 
 
+def mechanism_tables(cfgsect):
+    """The tables of the mechanism file cfgsect names, for its eos,
+    transport, diffusion, mixing rule and chemistry, fitted over its T-range."""
+    from peregrine_b200 import mixgen
+
+    path = cfgsect["species"]
+    if not os.path.isfile(path):
+        raise FileNotFoundError(f"mixture.species: no mechanism file {path!r}")
+    eos = cfgsect["eos"]
+    trange = cfgsect.get("T-range")
+    if trange is None and eos != "cpg":
+        raise ValueError(f"mixture.T-range: the {eos} fits are made over the case's temperatures; state them")
+    # the double flux's real gas is the real gas's, same tables
+    tables = mixgen.make_tables(
+        mechanism=path, eos="real-gas" if eos == "real-gas-df" else eos, trans=cfgsect.get("trans"),
+        diffusion=cfgsect.get("diffusion") or "lewis", mixing_rule=cfgsect.get("mixing-rule") or "wilke",
+        chemistry=cfgsect.get("chemistry"), trange=tuple(trange) if trange is not None else (300.0, 3500.0),
+        refit_tol=cfgsect.get("refit-tol", 1e-3), refit_max_deg=cfgsect.get("refit-max-deg", 6),
+        bath=cfgsect.get("bath"))
+    return tables
+
+
 class Mixture:
     def __init__(self, cfgsect):
         species = cfgsect["species"]
         self.tables = None
+        if isinstance(species, str) and species.lower().endswith((".yaml", ".yml")):
+            self._from_tables(cfgsect, mechanism_tables(cfgsect))
+            return
         if isinstance(species, str):
             self._from_tables(cfgsect, load_tables(species))
             return
