@@ -215,6 +215,22 @@ int pgb_case_set_table(pgb_case *c, const char *name, const double *values, long
  * "cubicdaMW", "vshiftMW" (ns each; peregrine/simulator/mixture/eos/realgas/model.py:43-98) */
 /* the case's finite-rate mechanism, copied; before finalize */
 int pgb_case_set_mechanism(pgb_case *c, const pgb_mechanism *m);
+/* The coupled chemistry's source kernel generated for the case's mechanism:
+ * every reaction straight-line code with its species indices and constants as
+ * literals, compiled for the device at pgb_case_finalize (NVRTC), as the
+ * reference renders its finite-rate kernels
+ * (peregrine/simulator/mixture/chemistry/kernels/finiterate.mako).  On by
+ * default; off (before finalize) keeps the table-driven kernel, which walks
+ * the mechanism's columns at run time.  Where NVRTC cannot be opened the
+ * table-driven kernel stays in use; pgb_case_generated_chemistry says which
+ * runs and, when it is not the generated one, why (up to cap bytes). */
+int pgb_case_set_generated_chemistry(pgb_case *c, int on);
+int pgb_case_generated_chemistry(const pgb_case *c, int *on, char *why, long long cap);
+/* The generated source itself (len its length, up to cap bytes written), and
+ * its compilation for sm_100a with nothing loaded (the compiler's log on
+ * failure): host computations, before or after finalize. */
+int pgb_case_rates_source(pgb_case *c, char *buf, long long cap, long long *len);
+int pgb_case_rates_compile(pgb_case *c, char *log, long long cap);
 /* the sub-stepped chemistry's options (the reference's chem-integration
  * section, peregrine/simulator/chemint/substepped.py:14-33): max-substeps
  * cap >= 1, bulk-substeps 1 <= bulk <= cap (bulk < cap compacts the stiff

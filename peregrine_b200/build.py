@@ -20,7 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 MAXNS = 12
-SOURCES = [os.path.join(CSRC, f) for f in ("pgb_host.cu", "pgb_noalloc.cu", "plain_tu.cu", "fp64_peak.cu")]
+SOURCES = [os.path.join(CSRC, f) for f in ("pgb_host.cu", "pgb_noalloc.cu", "plain_tu.cu", "fp64_peak.cu", "rategen.cu")]
 HEADERS = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cuh", ".h"))] + \
           [os.path.join(ROOT, "include", "pgb200.h")]
 TARGET = os.path.join(HERE, "libpgb200.so")
@@ -33,7 +33,8 @@ def units():
     """(source, object, extra flags) of every translation unit."""
     out = [(os.path.join(CSRC, "pgb_host.cu"), os.path.join(OBJ, "pgb_host.o"), []),
            (os.path.join(CSRC, "pgb_noalloc.cu"), os.path.join(OBJ, "pgb_noalloc.o"), []),
-           (os.path.join(CSRC, "fp64_peak.cu"), os.path.join(OBJ, "fp64_peak.o"), [])]
+           (os.path.join(CSRC, "fp64_peak.cu"), os.path.join(OBJ, "fp64_peak.o"), []),
+           (os.path.join(CSRC, "rategen.cu"), os.path.join(OBJ, "rategen.o"), [])]
     for n in range(1, MAXNS + 1):
         out.append((os.path.join(CSRC, "plain_tu.cu"), os.path.join(OBJ, f"plain_ns{n}.o"), [f"-DPGB_NS={n}"]))
     return out
@@ -63,7 +64,7 @@ def build(force=False, verbose=False, jobs=None):
 
     with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as pool:
         objs = list(pool.map(compile_one, units()))
-    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", TARGET, *objs]
+    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", TARGET, *objs, "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -80,7 +80,7 @@ _DEFAULTS = {
     # this build's device path: "batched" is the fused persistent kernel over
     # every block, "per-block" the unfused launches per block and kernel;
     # "metrics" picks the uniform-block form where a block's metrics allow it
-    "backend-b200": {"launch": "batched", "metrics": "auto", "graph": True},
+    "backend-b200": {"launch": "batched", "metrics": "auto", "graph": True, "chemistry-kernel": "generated"},
     "halo-exchange": {"kind": "device"},
 }
 
@@ -189,4 +189,6 @@ class Config(dict):
         launch = self["backend-b200"]["launch"]
         if launch not in ("batched", "per-block", "packed"):
             raise ConfigError("backend-b200.launch", "batched, per-block or packed")
+        if self["backend-b200"]["chemistry-kernel"] not in ("generated", "tables"):
+            raise ConfigError("backend-b200.chemistry-kernel", "generated or tables")
         return self

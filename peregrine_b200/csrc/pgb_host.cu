@@ -1,8 +1,10 @@
 // The host side of pgb200: cases, device arrays, halo tables, the stage plans
 // and the launches, behind the C ABI of include/pgb200.h.
 #include "pgb200.h"
+#include "rategen.h"
 
 #include <algorithm>
+#include <cstddef>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -186,6 +188,14 @@ struct pgb_case {
   long long stage_cap = 0;
   // finite-rate chemistry: the mechanism's device tables
   std::unique_ptr<Mech> mech;
+  // the finite-rate source generated for the mechanism (rategen.cu): wanted
+  // (the default), its loaded library and kernel, the table log's and exp's
+  // tables it reads, and why it is not in use when it is not
+  bool gen_want = true;
+  cudaLibrary_t gen_lib = nullptr;
+  const void *gen_src = nullptr;
+  MathTables *d_math = nullptr;
+  std::string gen_why;
   unsigned long long uid = 0;  // unique over the process, never reused
   unsigned version = 0;        // bumped when the species or mechanism tables change
   bool df_fresh = true;        // the double flux has no frozen planes for the state yet
@@ -1234,6 +1244,7 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.bchalo_n = c->bcthreads[0], pc.bcgrad_n = c->bcthreads[1], pc.bcwall_n = c->bcthreads[2];
   pc.bcent = c->d_bcent, pc.bcops = c->d_bcops;
   pc.clock = c->d_clock, pc.dt = c->d_dt;
+  pc.gensrc = c->gen_src, pc.genmath = c->d_math, pc.blkstride = (int)sizeof(BlockDev);
   pc.tfrac = 0.0;
   pc.stream = c->stream;
   return pc;
@@ -1412,6 +1423,38 @@ int prepare(pgb_case *c, bool fused) {
   return PGB_OK;
 }
 
+// the generated kernel reads a block record's leading fields by these offsets
+static_assert(offsetof(BlockDev, nx) == 0 && offsetof(BlockDev, Z) == 20 && offsetof(BlockDev, vol) == 24 &&
+                  offsetof(BlockDev, cv) == 32,
+              "the generated source's block record");
+
+// The coupled chemistry's source generated for the case's mechanism and
+// compiled for the device (rategen.cu); where NVRTC is missing or the case
+// asks for the table-driven kernel, that kernel stays in use
+int build_generated(pgb_case *c) {
+  c->gen_src = nullptr;
+  if (c->phys.chemistry != PGB_CHEM_COUPLED || !c->mech) {
+    c->gen_why = "the case has no coupled chemistry";
+    return PGB_OK;
+  }
+  if (!c->gen_want) {
+    c->gen_why = "the case asked for the table-driven kernel";
+    return PGB_OK;
+  }
+  std::string cubin;
+  if (!rates_compile(rates_source(*c->mech, c->sp, c->phys.ns), cubin, c->gen_why)) return PGB_OK;
+  CK(cudaLibraryLoadData(&c->gen_lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  cudaKernel_t k = nullptr;
+  CK(cudaLibraryGetKernel(&k, c->gen_lib, "pgb_gen_source"));
+  MathTables mt;
+  math_tables_fill(mt);
+  CK(cudaMalloc(&c->d_math, sizeof(MathTables)));
+  CK(cudaMemcpy(c->d_math, &mt, sizeof(MathTables), cudaMemcpyHostToDevice));
+  c->gen_src = (const void *)k;
+  c->gen_why.clear();
+  return PGB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1502,6 +1545,8 @@ int pgb_case_destroy(pgb_case *c) {
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
                   c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots};
+  if (c->gen_lib) cudaLibraryUnload(c->gen_lib);
+  if (c->d_math) cudaFree(c->d_math);
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1979,6 +2024,52 @@ int pgb_case_set_stages(pgb_case *c, const pgb_stage *stages, int nstages) {
   return PGB_OK;
 }
 
+int pgb_case_set_generated_chemistry(pgb_case *c, int on) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
+  c->gen_want = on != 0;
+  return PGB_OK;
+}
+
+int pgb_case_generated_chemistry(const pgb_case *c, int *on, char *why, long long cap) {
+  if (!c || !on) return fail(PGB_ERR_ARG, "null argument");
+  *on = c->gen_src != nullptr;
+  if (why && cap > 0) {
+    const size_t n = std::min<size_t>((size_t)cap - 1, c->gen_why.size());
+    std::memcpy(why, c->gen_why.data(), n);
+    why[n] = 0;
+  }
+  return PGB_OK;
+}
+
+int pgb_case_rates_source(pgb_case *c, char *buf, long long cap, long long *len) {
+  if (!c || !len || (cap > 0 && !buf)) return fail(PGB_ERR_ARG, "null argument");
+  if (!c->mech) return fail(PGB_ERR_STATE, "the case has no mechanism");
+  if (!c->finalized) RET(build_species(c));
+  const std::string src = rates_source(*c->mech, c->sp, c->phys.ns);
+  *len = (long long)src.size();
+  if (buf && cap > 0) {
+    const size_t n = std::min<size_t>((size_t)cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = 0;
+  }
+  return PGB_OK;
+}
+
+int pgb_case_rates_compile(pgb_case *c, char *log, long long cap) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  if (!c->mech) return fail(PGB_ERR_STATE, "the case has no mechanism");
+  if (!c->finalized) RET(build_species(c));
+  std::string cubin, err;
+  const bool ok = rates_compile(rates_source(*c->mech, c->sp, c->phys.ns), cubin, err);
+  if (log && cap > 0) {
+    const size_t n = std::min<size_t>((size_t)cap - 1, err.size());
+    std::memcpy(log, err.data(), n);
+    log[n] = 0;
+  }
+  return ok ? PGB_OK : fail(PGB_ERR_UNSUPPORTED, err);
+}
+
 int pgb_case_finalize(pgb_case *c) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
   if (c->finalized) return PGB_OK;
@@ -1986,6 +2077,7 @@ int pgb_case_finalize(pgb_case *c) {
   if (c->stages.empty()) return fail(PGB_ERR_STATE, "no stages");
   RET(build_species(c));
   if (!c->stream) CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  RET(build_generated(c));
   if (!c->ev0) CK(cudaEventCreate(&c->ev0));
   if (!c->ev1) CK(cudaEventCreate(&c->ev1));
   c->cells = layout_blocks(c);

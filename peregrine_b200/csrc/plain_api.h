@@ -66,6 +66,11 @@ struct PlainCase {
   const BcEntry *bcent;
   const BcOp *bcops;
   const double *clock, *dt;
+  // the coupled source generated for the mechanism (a kernel handle for
+  // cudaLaunchKernel; null for the table-driven kernel), the table log's and
+  // exp's tables it reads, and the block record's size
+  const void *gensrc, *genmath;
+  int blkstride;
   double tfrac;
   cudaStream_t stream;
   void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block, 4 boundary, 5 CFL

@@ -152,9 +152,23 @@ void grads_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void
   const RhsArgs &a = *(const RhsArgs *)ctx;
   k_grads<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->met, pc->grads, 0, ct);
 }
+// the coupled source: the kernel generated for the case's mechanism where it
+// has one (rategen.cu), else the table-driven k_source
+void launch_source(const PlainCase *pc, int b, dim3 g, const int2 *ct, const double *Q, double *dQ) {
+  if (pc->gensrc) {
+    const char *blks = reinterpret_cast<const char *>(pc->d_blks);
+    int stride = pc->blkstride, blk = b;
+    const double *st = pc->state;
+    const void *mt = pc->genmath;
+    void *args[] = {&blks, &stride, &blk, &Q, &st, &dQ, &ct, &mt};
+    cudaLaunchKernel(pc->gensrc, g, dim3(TH), args, 0, pc->stream);
+    return;
+  }
+  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, Q, pc->state, dQ, ct);
+}
 void source_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
-  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, a.dQ, ct);
+  launch_source(pc, b, g, ct, a.Q, a.dQ);
 }
 void bulk_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
@@ -443,7 +457,7 @@ void rcell_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void
 }
 void rsource_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RStage &r = *(const RStage *)ctx;
-  k_source<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, r.dQ, ct);
+  launch_source(pc, b, g, ct, r.Q, r.dQ);
 }
 void rgrads_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RStage &r = *(const RStage *)ctx;

@@ -185,6 +185,12 @@ SIGNATURES = {
     "pgb_pool_create": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "pgb_pool_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "pgb_pool_admit_reactor": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_case_set_generated_chemistry": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "pgb_case_generated_chemistry": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                      ctypes.c_longlong], ctypes.c_int),
+    "pgb_case_rates_source": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong,
+                               ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "pgb_case_rates_compile": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong], ctypes.c_int),
     "pgb_pool_admit": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_pool_metric_set": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),
     "pgb_pool_set_prims": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_long], ctypes.c_int),

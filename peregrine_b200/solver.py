@@ -160,6 +160,13 @@ class Solver:
         return any(face.nbr is None and getattr(face, "remote", None) is None
                    for blk in self.mesh_blocks for face in blk.intfaces)
 
+    def generated_chemistry(self):
+        """Whether the coupled source runs the kernel generated for the
+        mechanism, and why not when it does not."""
+        on, why = ctypes.c_int(), ctypes.create_string_buffer(512)
+        native.call("pgb_case_generated_chemistry", self.case, ctypes.byref(on), why, 512)
+        return bool(on.value), why.value.decode()
+
     def batched_form(self):
         """The batched path's form for this case: 1 the fused stage kernel
         (the single-species calorically perfect kepaec case), 2 the fused
@@ -225,6 +232,9 @@ class Solver:
             native.call("pgb_case_set_substeps", self.case, chem["max-substeps"], chem["bulk-substeps"],
                         chem["stiff-bins"], float(chem["equilibrium-tolerance"]))
         native.call("pgb_case_set_stages", self.case, records, len(records))
+        # the coupled source generated for the mechanism, or the table-driven kernel
+        generated = self.cfg["backend-b200"]["chemistry-kernel"] == "generated"
+        native.call("pgb_case_set_generated_chemistry", self.case, 1 if generated else 0)
         native.call("pgb_case_finalize", self.case)
         self.metrics = []
         for blk in self.mesh_blocks:
