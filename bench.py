@@ -301,6 +301,27 @@ def reacting_leg(steps, cpu=True):
     return out
 
 
+def reacting_profile(kernel):
+    """The reacting case's batched step twice (a warm-up and one more), its
+    launches plain (no graph), so a profiler sees each pass on its own: the
+    stage's seven launches after a halo fill (cell pass, source, gradients,
+    gradient halo, three face passes, divergence and combines)."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases
+
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True, launch="batched")
+    cfg["backend-b200"]["chemistry-kernel"] = kernel
+    mesh = cases.reacting_mesh(REACT_CELLS, (1, 1, 1))
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    consts = mb.mixture.constants()
+    mb.set_prims(cases.reacting_prims(mb.metrics, mb.mixture.spnames, consts["MW"], REACT_CELLS, seed=SEED))
+    mb.graph = False
+    mb.step(2e-8, 1)
+    mb.step(2e-8, 1)
+    mb.backend.sync()
+    print(json.dumps({"reacting_profile": kernel, "generated": mb.generated_chemistry()[0]}), flush=True)
+
+
 # the sub-stepped leg's timed steps, fixed: the hot spots burn through in a
 # few microseconds, so the stiff cells a step lists depend on how far the
 # field has run (three warm-up steps, then these)
@@ -642,6 +663,9 @@ def main():
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
     ap.add_argument("--no-reacting", action="store_true", help="skip the reacting leg")
     ap.add_argument("--reacting-only", action="store_true", help="the reacting leg alone (profiling)")
+    ap.add_argument("--reacting-profile", default=None, choices=("generated", "tables"),
+                    help="one warm-up and one RK3 step of the 96^3 reacting case on the batched path, no graph, "
+                         "with the named source kernel: the command an ncu capture of its passes runs")
     ap.add_argument("--serving-only", action="store_true", help="the serving leg alone")
     ap.add_argument("--realgas-only", action="store_true", help="the real-gas leg alone")
     ap.add_argument("--no-realgas", action="store_true", help="skip the real-gas leg")
@@ -673,6 +697,9 @@ def main():
         return
     if args.reacting_only:
         print(json.dumps({"reacting": reacting_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)
+        return
+    if args.reacting_profile:
+        reacting_profile(args.reacting_profile)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
