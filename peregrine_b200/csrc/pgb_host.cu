@@ -1245,6 +1245,10 @@ PlainCase plain_case(pgb_case *c, std::vector<BlockDev> &hb) {
   pc.bcent = c->d_bcent, pc.bcops = c->d_bcops;
   pc.clock = c->d_clock, pc.dt = c->d_dt;
   pc.gensrc = c->gen_src, pc.genmath = c->d_math, pc.blkstride = (int)sizeof(BlockDev);
+  // blocks whose halo is a large share of their cells take the interior cell
+  // pass, where the case's own halo table fills every halo cell (a shard's
+  // traded halo cells get Q alone, so their fields are formed in place)
+  pc.rcell_inner = c->nxrecv == 0 && c->cells > (long long)(1.3 * (double)c->interior_cells) ? 1 : 0;
   pc.tfrac = 0.0;
   pc.stream = c->stream;
   return pc;
@@ -2855,6 +2859,8 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.realgas = p->phys.eos == PGB_EOS_REALGAS || p->phys.eos == PGB_EOS_REALGAS_DF;
   pc.packed = 1;
   pc.dt = p->d_dt;
+  // the pool's blocks are thin (a 1-D domain's halo is most of its cells)
+  pc.rcell_inner = 1;
   pc.stream = p->stream;
   return pc;
 }

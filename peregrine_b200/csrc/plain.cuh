@@ -33,9 +33,11 @@ template <int C, bool ROT = true>
 __device__ __forceinline__ void halo_copy(double *__restrict__ base, const int comps, const int vec,
                                           const double *__restrict__ rots, const long long dcv, const int didx,
                                           const int dvol, const long long scv, const int sidx, const int svol,
-                                          const int rot) {
-  double *d = base + comps * dcv + didx;
-  const double *s = base + comps * scv + sidx;
+                                          const int rot, const int stride) {
+  // a block's array starts stride x its cell offset in (its component
+  // count, or more where the first comps of wider records are copied)
+  double *d = base + stride * dcv + didx;
+  const double *s = base + stride * scv + sidx;
   if constexpr (C > 0) {
     double v[C];
 #pragma unroll
@@ -68,10 +70,11 @@ __device__ __forceinline__ void halo_copy(double *__restrict__ base, const int c
 }
 
 static __global__ void k_halo(double *__restrict__ base, const HaloEntry *__restrict__ tab, long long n, int comps,
-                              int vec = HALO_SCALARS, const double *__restrict__ rots = nullptr) {
+                              int vec = HALO_SCALARS, const double *__restrict__ rots = nullptr, int stride = 0) {
+  if (stride == 0) stride = comps;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const HaloEntry h = tab[e];
-    halo_copy<0>(base, comps, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot);
+    halo_copy<0>(base, comps, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot, stride);
   }
 }
 
@@ -84,13 +87,15 @@ static __global__ void __launch_bounds__(256) k_halo_boxes(double *__restrict__ 
                                                            const int2 *__restrict__ cta,
                                                            const HaloEntry *__restrict__ rest, long long nrest,
                                                            int comps, int vec = HALO_SCALARS,
-                                                           const double *__restrict__ rots = nullptr) {
+                                                           const double *__restrict__ rots = nullptr,
+                                                           int stride = 0) {
+  if (stride == 0) stride = comps;
   const int2 w = cta[blockIdx.x];
   const int t = w.y * 256 + (int)threadIdx.x;
   if (w.x < 0) {
     if (t >= nrest) return;
     const HaloEntry h = rest[t];
-    halo_copy<C, ROT>(base, comps, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot);
+    halo_copy<C, ROT>(base, comps, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot, stride);
     return;
   }
   const HaloPatch &p = boxes[w.x];
@@ -98,7 +103,7 @@ static __global__ void __launch_bounds__(256) k_halo_boxes(double *__restrict__ 
   const int x0 = t % p.n0, r = t / p.n0, x1 = r % p.n1, x2 = r / p.n1;
   const int didx = p.d0 + x0 * p.dst[0] + x1 * p.dst[1] + x2 * p.dst[2];
   const int sidx = p.s0 + x0 * p.sst[0] + x1 * p.sst[1] + x2 * p.sst[2];
-  halo_copy<C, ROT>(base, comps, vec, rots, p.dcv, didx, p.dvol, p.scv, sidx, p.svol, p.rot);
+  halo_copy<C, ROT>(base, comps, vec, rots, p.dcv, didx, p.dvol, p.scv, sidx, p.svol, p.rot, stride);
 }
 
 // the box fill of a register of comps components: the kernel built for that
@@ -106,22 +111,25 @@ static __global__ void __launch_bounds__(256) k_halo_boxes(double *__restrict__ 
 // only where the case has rotations and the register has vectors
 template <bool ROT, int... Cs>
 inline void halo_boxes_rot(unsigned grid, cudaStream_t st, double *base, const HaloPatch *boxes, const int2 *cta,
-                           const HaloEntry *rest, long long nrest, int comps, int vec, const double *rots) {
+                           const HaloEntry *rest, long long nrest, int comps, int vec, const double *rots,
+                           int stride) {
   bool done = false;
   ((!done && comps == Cs
-        ? (k_halo_boxes<Cs, ROT><<<grid, 256, 0, st>>>(base, boxes, cta, rest, nrest, comps, vec, rots), done = true)
+        ? (k_halo_boxes<Cs, ROT><<<grid, 256, 0, st>>>(base, boxes, cta, rest, nrest, comps, vec, rots, stride),
+           done = true)
         : false),
    ...);
-  if (!done) k_halo_boxes<0, ROT><<<grid, 256, 0, st>>>(base, boxes, cta, rest, nrest, comps, vec, rots);
+  if (!done) k_halo_boxes<0, ROT><<<grid, 256, 0, st>>>(base, boxes, cta, rest, nrest, comps, vec, rots, stride);
 }
 
 template <int... Cs>
 inline void halo_boxes_launch(unsigned grid, cudaStream_t st, double *base, const HaloPatch *boxes, const int2 *cta,
-                              const HaloEntry *rest, long long nrest, int comps, int vec, const double *rots) {
+                              const HaloEntry *rest, long long nrest, int comps, int vec, const double *rots,
+                              int stride = 0) {
   if (rots && vec != HALO_SCALARS)
-    halo_boxes_rot<true, Cs...>(grid, st, base, boxes, cta, rest, nrest, comps, vec, rots);
+    halo_boxes_rot<true, Cs...>(grid, st, base, boxes, cta, rest, nrest, comps, vec, rots, stride);
   else
-    halo_boxes_rot<false, Cs...>(grid, st, base, boxes, cta, rest, nrest, comps, vec, rots);
+    halo_boxes_rot<false, Cs...>(grid, st, base, boxes, cta, rest, nrest, comps, vec, rots, stride);
 }
 
 __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi, int &fj, int &fk) {

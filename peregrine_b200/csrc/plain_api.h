@@ -71,6 +71,9 @@ struct PlainCase {
   // exp's tables it reads, and the block record's size
   const void *gensrc, *genmath;
   int blkstride;
+  // the fused passes' cell pass over the interior cells, its fields then
+  // copied into the halo (blocks whose halo is a large share of their cells)
+  int rcell_inner;
   double tfrac;
   cudaStream_t stream;
   void (*mark)(void *ctx, int kind);  // called after each launch, kind 0 halo, 2 block, 4 boundary, 5 CFL

@@ -48,12 +48,12 @@ void mark(const PlainCase *pc, int kind) {
 
 // the full halo of a register (comps components, vec the component its
 // rotations turn): by boxes when the case has them, else by entries
-void halo_fill(const PlainCase *pc, double *base, int comps, int vec) {
+void halo_fill(const PlainCase *pc, double *base, int comps, int vec, int stride = 0) {
   if (pc->boxcta && pc->nboxcta > 0)
     halo_boxes_launch<NE, SW>((unsigned)pc->nboxcta, pc->stream, base, pc->boxes, pc->boxcta, pc->boxrest, pc->nboxrest,
-                          comps, vec, pc->rots);
+                              comps, vec, pc->rots, stride);
   else
-    k_halo<<<grid_of(pc->nhalo), TH, 0, pc->stream>>>(base, pc->halo, pc->nhalo, comps, vec, pc->rots);
+    k_halo<<<grid_of(pc->nhalo), TH, 0, pc->stream>>>(base, pc->halo, pc->nhalo, comps, vec, pc->rots, stride);
 }
 
 // a pass over every block: one launch per block, or packed, one launch over
@@ -455,6 +455,11 @@ void rcell_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void
   const RStage &r = *(const RStage *)ctx;
   k_rcell<NS, VISC><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, pc->tr, pc->hsp, ct);
 }
+template <bool VISC>
+void rcell_inner_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RStage &r = *(const RStage *)ctx;
+  k_rcell<NS, VISC, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, r.Q, pc->state, pc->tr, pc->hsp, ct);
+}
 void rsource_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RStage &r = *(const RStage *)ctx;
   launch_source(pc, b, g, ct, r.Q, r.dQ);
@@ -526,7 +531,21 @@ extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PGB_OK : cuda_fail(e, "fused double-flux stage");
   }
-  for_blocks(pc, R_VOL, pc->visc ? rcell_launch<true> : rcell_launch<false>, rs, 8);
+  if (pc->rcell_inner) {
+    // the interior cells, then each halo cell's fields from its source's:
+    // the same values, as a halo cell's Q and last T are its source's
+    for_blocks(pc, R_INNER, pc->visc ? rcell_inner_launch<true> : rcell_inner_launch<false>, rs, 8);
+    halo_fill(pc, pc->state, 8, HALO_SCALARS, SW);
+    mark(pc, 0);
+    if (pc->visc) {
+      halo_fill(pc, pc->tr, 2 + NS, HALO_SCALARS);
+      mark(pc, 0);
+      halo_fill(pc, pc->hsp, NS, HALO_SCALARS);
+      mark(pc, 0);
+    }
+  } else {
+    for_blocks(pc, R_VOL, pc->visc ? rcell_launch<true> : rcell_launch<false>, rs, 8);
+  }
   const bool chem = pc->chem == PGB_CHEM_COUPLED;
   if (chem) for_blocks(pc, R_INNER, rsource_launch, rs, 2);
   if (pc->visc) {

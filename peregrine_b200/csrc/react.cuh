@@ -47,15 +47,24 @@
 namespace pgb {
 
 // fromQ and the transport of one cell (k_fromQ then k_transport); t over the
-// block's full extents
-template <int NS, bool VISC>
+// block's full extents, or, with INNER, over its interior cells (a halo
+// cell's values are then its source's, copied after)
+template <int NS, bool VISC, bool INNER = false>
 __global__ void __launch_bounds__(256) k_rcell(const BlockDev *__restrict__ blks, int b,
                                                const double *__restrict__ Qall, double *__restrict__ stall,
                                                double *__restrict__ trall, double *__restrict__ hall,
                                                const int2 *__restrict__ ctab = nullptr) {
   constexpr int NE = 4 + NS;
-  PGB_WHERE(B, t);
-  if (t >= B.vol) return;
+  PGB_WHERE(B, tt);
+  long long t = tt;
+  if (INNER) {
+    if (tt >= (long long)B.nx * B.ny * B.nz) return;
+    const int i = (int)(tt % B.nx) + NG, j = (int)((tt / B.nx) % B.ny) + NG;
+    const int k = (int)(tt / ((long long)B.nx * B.ny)) + NG;
+    t = cell_index(B, i, j, k);
+  } else if (t >= B.vol) {
+    return;
+  }
   const long long v = B.vol;
   const double *Q = Qall + NE * B.cv + t;
   double *st = stall + SW * B.cv + t;

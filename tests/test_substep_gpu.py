@@ -37,6 +37,9 @@ def config(kind, cap=200, bulk=1, bins=8, eqtol=1e-7, simulator="euler"):
     cfg["chem-integration"].update({"max-substeps": cap, "bulk-substeps": bulk, "stiff-bins": bins,
                                     "equilibrium-tolerance": eqtol})
     cfg["backend-b200"]["launch"] = "per-block"
+    # the substeps' fold walks the mechanism's tables; the coupled source held
+    # to it bit for bit walks them too
+    cfg["backend-b200"]["chemistry-kernel"] = "tables"
     cfg["bcvals"]["walls"] = {"kind": "slp-adia-wall"}
     return cfg.validate()
 
