@@ -561,6 +561,29 @@ def serving_leg(n=300, rate=60.0, steps=100, sweep=(30.0, 120.0, 480.0, 1920.0),
                         "periodic 1-D domains of 64-2048 cells, Poisson arrivals, one pool, continuous batching"}
 
 
+def serving_profile(n=200):
+    """A saturated pool: n seeded requests (closed reactors and 1-D domains)
+    admitted at once, then a step (its graph captured) and two more."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases, serving
+
+    cfg = cases.reacting_config("navier-stokes", "tvd-rk3", "hllc", "muscl", "koren", True)
+    proto = pg.get_solver(cfg, cases.reacting_mesh(4), pg.get_backend("cuda", cfg))
+    consts = proto.mixture.constants()
+    reqs = serving.requests(n, 0.0, proto.mixture.spnames, consts["MW"], seed=SEED + 7, steps=100)
+    pool = serving.Pool(proto, 8_000_000, 4096)
+    slots = [pool.admit(r) for r in reqs]
+    assert None not in slots
+    pool.step(2e-8, 1)
+    ms, launches = pool.step(2e-8, 2)
+    free, run, done = pool.info()
+    cells = sum(1 if r.kind == "0d" else int(np.prod(r.cells)) for r in reqs)
+    print(json.dumps({"serving_profile": {"requests": n, "running": run, "reactors": sum(r.kind == "0d" for r in reqs),
+                                          "cells": cells, "ms_per_step": ms / 2, "launches_per_step": launches / 2}}),
+          flush=True)
+    pool.close()
+
+
 def reference_arm(args):
     """The reference CPU restatement's throughput on the same workload; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -667,6 +690,9 @@ def main():
                     help="one warm-up and one RK3 step of the 96^3 reacting case on the batched path, no graph, "
                          "with the named source kernel: the command an ncu capture of its passes runs")
     ap.add_argument("--serving-only", action="store_true", help="the serving leg alone")
+    ap.add_argument("--serving-profile", action="store_true",
+                    help="200 seeded requests admitted into one pool at once, then three pool steps: the command an "
+                         "ncu launch list of a saturated pool step runs")
     ap.add_argument("--realgas-only", action="store_true", help="the real-gas leg alone")
     ap.add_argument("--no-realgas", action="store_true", help="skip the real-gas leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
@@ -694,6 +720,9 @@ def main():
         return
     if args.serving_only:
         print(json.dumps({"serving": serving_leg()}), flush=True)
+        return
+    if args.serving_profile:
+        serving_profile()
         return
     if args.reacting_only:
         print(json.dumps({"reacting": reacting_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)

@@ -2692,6 +2692,11 @@ struct pgb_pool {
   BlockDev *d_run = nullptr;   // the running table, by row
   HaloEntry *d_halo = nullptr;
   long long halo_cap = 0, nhalo = 0, nhalo_l0 = 0;
+  // the same halo as boxes (k_halo_boxes): each running block's six face
+  // halos, NG deep, periodic onto itself, and their CTA table
+  HaloPatch *d_boxes = nullptr;
+  int2 *d_boxcta = nullptr;
+  long long box_cap = 0, boxcta_cap = 0, nboxcta = 0;
   int2 *d_ctab = nullptr;  // the running blocks' tile tables, one per range, end to end
   long long ctab_cap = 0, ctab_off[5] = {}, nctab[5] = {};
   // closed constant-volume reactors, a cell each: registers [component][rcap]
@@ -2767,7 +2772,9 @@ int pool_rebuild(pgb_pool *p) {
           // the halo plane at distance layer + 1 beyond the interior on this side
           const int h = side == 0 ? NG - 1 - layer : NG + n[a] + layer;
           const int src = side == 0 ? h + n[a] : h - n[a];
-          const int e1 = (a + 1) % 3, e2 = (a + 2) % 3;
+          // the lower tangential axis fastest, so neighbouring entries touch
+          // neighbouring cells (i on the j- and k-faces)
+          const int e1 = a == 0 ? 1 : 0, e2 = a == 2 ? 1 : 2;
           for (int u = NG; u < NG + n[e2]; u++)
             for (int v = NG; v < NG + n[e1]; v++) {
               int di[3], si[3];
@@ -2783,6 +2790,45 @@ int pool_rebuild(pgb_pool *p) {
             }
         }
   }
+  // the boxes: for each running block and face, the NG halo planes, i
+  // fastest, each cell's source n cells across along the face's axis
+  std::vector<HaloPatch> boxes;
+  for (const BlockDev &D : p->run) {
+    const int n[3] = {D.nx, D.ny, D.nz};
+    const int step[3] = {1, D.X, D.X * D.Y};
+    for (int a = 0; a < 3; a++)
+      for (int side = 0; side < 2; side++) {
+        int lo[3] = {NG, NG, NG}, ext[3] = {n[0], n[1], n[2]};
+        lo[a] = side == 0 ? 0 : NG + n[a];
+        ext[a] = NG;
+        HaloPatch P{};
+        P.dcv = P.scv = D.cv;
+        P.dvol = P.svol = (int)D.vol;
+        P.d0 = (int)cell_index(D, lo[0], lo[1], lo[2]);
+        P.s0 = P.d0 + (side == 0 ? 1 : -1) * n[a] * step[a];
+        for (int d = 0; d < 3; d++) P.dst[d] = P.sst[d] = step[d];
+        P.n0 = ext[0], P.n1 = ext[1], P.cells = ext[0] * ext[1] * ext[2];
+        boxes.push_back(P);
+      }
+  }
+  std::vector<int2> bcta;
+  for (int q = 0; q < (int)boxes.size(); q++)
+    for (int t = 0; t < (boxes[q].cells + 255) / 256; t++) bcta.push_back(make_int2(q, t));
+  if ((long long)boxes.size() > p->box_cap || (long long)bcta.size() > p->boxcta_cap) {
+    CK(cudaStreamSynchronize(p->stream));
+    if (p->d_boxes) CK(cudaFree(p->d_boxes));
+    if (p->d_boxcta) CK(cudaFree(p->d_boxcta));
+    p->d_boxes = nullptr, p->d_boxcta = nullptr;
+    p->box_cap = std::max<long long>((long long)boxes.size(), 2 * p->box_cap);
+    p->boxcta_cap = std::max<long long>((long long)bcta.size(), 2 * p->boxcta_cap);
+    CK(cudaMalloc(&p->d_boxes, sizeof(HaloPatch) * std::max<long long>(1, p->box_cap)));
+    CK(cudaMalloc(&p->d_boxcta, sizeof(int2) * std::max<long long>(1, p->boxcta_cap)));
+  }
+  if (!boxes.empty()) {
+    CK(cudaMemcpyAsync(p->d_boxes, boxes.data(), sizeof(HaloPatch) * boxes.size(), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(p->d_boxcta, bcta.data(), sizeof(int2) * bcta.size(), cudaMemcpyHostToDevice, p->stream));
+  }
+  p->nboxcta = (long long)bcta.size();
   p->nhalo_l0 = (long long)l0.size();
   p->nhalo = (long long)(l0.size() + l1.size());
   l0.insert(l0.end(), l1.begin(), l1.end());
@@ -2853,6 +2899,8 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.met = p->d_met;
   pc.halo = p->d_halo;
   pc.nhalo = p->nhalo, pc.nhalo_l0 = p->nhalo_l0;
+  // the boxes describe the running table's blocks, built with it
+  if (d_blks == p->d_run) pc.boxes = p->d_boxes, pc.boxcta = p->d_boxcta, pc.nboxcta = p->nboxcta;
   pc.visc = sim_visc(p->phys.simulator);
   pc.primary = p->phys.primary, pc.recon = p->phys.recon, pc.limiter = p->phys.limiter;
   pc.chem = p->phys.chemistry == PGB_CHEM_COUPLED;
@@ -3039,7 +3087,7 @@ int pgb_pool_destroy(pgb_pool *p) {
   for (auto &r : p->d_rq)
     if (r) cudaFree(r);
   void *ptrs[] = {p->d_met, p->d_state, p->d_tr, p->d_hsp, p->d_grads, p->d_F[0], p->d_F[1], p->d_F[2],
-                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo, p->d_ctab, p->d_rT, p->d_rrun};
+                  p->d_dt, p->d_host, p->d_blks, p->d_run, p->d_halo, p->d_ctab, p->d_rT, p->d_rrun, p->d_boxes, p->d_boxcta};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->step_graph) cudaGraphExecDestroy(p->step_graph);
