@@ -823,8 +823,19 @@ def main():
         pb_launches = mb.launches_per_step()
         mb.path = native.PATH_BATCHED
         value_pb = ncells * STAGES * pb_steps / (ms_pb / 1e3)
+        # the same kernels packed, each pass one launch over every block: the
+        # un-fused device baseline without the per-block launch count
+        mb.path = native.PATH_PACKED
+        mb.step(dt, 2)
+        mb.backend.sync()
+        ms_pk = time_graph(mb, dt, pb_steps)
+        pk_launches = mb.launches_per_step()
+        mb.path = native.PATH_BATCHED
+        value_pk = ncells * STAGES * pb_steps / (ms_pk / 1e3)
         per_block = {"value": value_pb, "ms_per_step": ms_pb / pb_steps, "launches_per_step": pb_launches,
-                     "speedup_batched": value / world / value_pb}
+                     "speedup_batched": value / world / value_pb,
+                     "packed": {"value": value_pk, "ms_per_step": ms_pk / pb_steps, "launches_per_step": pk_launches,
+                                "speedup_batched": value / world / value_pk}}
         # end to end: state in from pinned host, a step, state out, every step
         e2e_steps = max(3, min(args.steps // 4, 20))
         wall, nbytes = e2e_leg(mb, dt, e2e_steps)

@@ -230,6 +230,29 @@ def trade(plan, packed, group=None):
     return out
 
 
+CFL_KEYS = ("acoustic", "convective", "combined")
+
+
+def reduce_cfl(local, group=None, device=None):
+    """The CFL numbers over every rank's blocks: each rank's own maxima, then
+    a MAX over the ranks (the reference's Allreduce of its cflmax speeds,
+    peregrine/multiblock/solver.py:292-296).  device: a CUDA device for the
+    tensor (NCCL), None for a host tensor (gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(local[k]) for k in CFL_KEYS], dtype=torch.float64)
+    if device is not None:
+        t = t.to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return dict(zip(CFL_KEYS, t.cpu().tolist()))
+
+
+def cfl_stepsize(cfl, dtmax, cflmax):
+    """The cfl controller's step (peregrine/integrators/controllers.py:21-26)."""
+    return min(cfl / cflmax["combined"], dtmax)
+
+
 class LocalMesh:
     """A rank's blocks of a mesh, numbered 0 .. n-1 in global order; a face
     joined to another rank's block is left unjoined (its halo is traded)."""
@@ -315,6 +338,22 @@ class ShardedSolver:
                 off += self.nrecv[q]
             stream.synchronize()
         native.call("pgb_exchange_unpack", mb.case, s, mb.path, ctypes.c_void_p(rbuf.data_ptr()))
+
+    def cflmax(self):
+        """The CFL numbers over every rank's blocks."""
+        import torch
+
+        dev = torch.device("cuda", torch.cuda.current_device()) if self.mode == "device" else None
+        return reduce_cfl(self.solver.cflmax(), self.group, dev)
+
+    def step_cfl(self, cfl, dtmax, nsteps=1):
+        """nsteps steps under the cfl controller, each step's size from the
+        CFL numbers over every rank's blocks; returns the last step's size."""
+        dt = None
+        for _ in range(nsteps):
+            dt = cfl_stepsize(cfl, dtmax, self.cflmax())
+            self.step(dt, 1)
+        return dt
 
     def step(self, dt, nsteps=1):
         mb = self.solver

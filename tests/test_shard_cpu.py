@@ -147,3 +147,36 @@ def test_two_ranks_step_as_one_rank_to_the_bit():
     assert sorted(got) == list(range(len(blocks)))
     for b, blk in enumerate(blocks):
         assert np.array_equal(got[b], one.regs[0][b][blk.interior]), b
+
+
+def _cfl_rank(rank, world, port, out):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    mesh, blocks = tgv_blocks()
+    owner = shard.partition(blocks, world)
+    plan = shard.ExchangePlan(blocks, owner, rank)
+    local = shard.LocalMesh(mesh, owner, rank).make_blocks(2)
+    orc = _oracle(local, plan.local)
+    mine = {k: float(v) for k, v in orc.cflmax().items()}
+    out[rank] = (mine, shard.reduce_cfl(mine))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_the_cfl_numbers_reduce_over_the_ranks():
+    # each rank's own blocks' maxima, a MAX over the ranks: the one-rank
+    # maxima over every block, and so the cfl controller's step, to the bit
+    import torch.multiprocessing as mp
+
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.spawn(_cfl_rank, args=(2, _free_port(), out), nprocs=2, join=True)
+    _, blocks = tgv_blocks()
+    whole = {k: float(v) for k, v in _oracle(blocks).cflmax().items()}
+    for r in range(2):
+        mine, reduced = out[r]
+        assert reduced == whole
+        assert all(mine[k] <= whole[k] for k in shard.CFL_KEYS)
+    assert shard.cfl_stepsize(0.8, 1.0, out[0][1]) == min(0.8 / whole["combined"], 1.0)

@@ -135,3 +135,20 @@ def test_a_viscous_shard_off_the_fused_stage_kernel_is_refused():
     native.call("pgb_set_dt", mb.case, 1e-6)
     with pytest.raises(native.PgbUnsupported):
         native.call("pgb_step_stage", mb.case, 0, mb.path)
+
+
+def test_the_shards_cfl_numbers_make_the_whole_grids():
+    # each shard's own blocks' maxima, a MAX over the shards: the whole grid's
+    # numbers, and so the cfl controller's step, to the bit (the MAX across
+    # ranks itself is shard.reduce_cfl, checked over gloo ranks on the CPU)
+    import peregrine_b200 as pg
+
+    cfg, mesh = build("tgv", "batched")
+    whole = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    allprims = prims_of("tgv", whole.mesh_blocks, whole.metrics)
+    whole.set_prims(allprims)
+    parts = shards(cfg, mesh, allprims)
+    mine = [mb.cflmax() for _, mb in parts]
+    got = {k: max(m[k] for m in mine) for k in shard.CFL_KEYS}
+    assert got == whole.cflmax()
+    assert shard.cfl_stepsize(0.8, 1.0, got) == min(0.8 / whole.cflmax()["combined"], 1.0)
