@@ -2697,6 +2697,9 @@ struct pgb_pool {
   HaloPatch *d_boxes = nullptr;
   int2 *d_boxcta = nullptr;
   long long box_cap = 0, boxcta_cap = 0, nboxcta = 0;
+  // the first face layer's boxes (the gradients' fill): the last
+  // 6 x blocks boxes of d_boxes, their CTA table after the full one's
+  long long nboxcta0 = 0;
   int2 *d_ctab = nullptr;  // the running blocks' tile tables, one per range, end to end
   long long ctab_cap = 0, ctab_off[5] = {}, nctab[5] = {};
   // closed constant-volume reactors, a cell each: registers [component][rcap]
@@ -2753,7 +2756,6 @@ BlockDev slot_dev(const PoolSlot &s) {
 int pool_rebuild(pgb_pool *p) {
   p->run.clear();
   p->rrun.clear();
-  std::vector<HaloEntry> l0, l1;
   for (size_t q = 0; q < p->slots.size(); q++) {
     PoolSlot &s = p->slots[q];
     s.active = -1;
@@ -2763,57 +2765,40 @@ int pool_rebuild(pgb_pool *p) {
       continue;
     }
     s.active = (int)p->run.size();
-    const BlockDev D = slot_dev(s);
-    p->run.push_back(D);
-    const int n[3] = {s.nx, s.ny, s.nz};
-    for (int a = 0; a < 3; a++)
-      for (int layer = 0; layer < NG; layer++)
-        for (int side = 0; side < 2; side++) {
-          // the halo plane at distance layer + 1 beyond the interior on this side
-          const int h = side == 0 ? NG - 1 - layer : NG + n[a] + layer;
-          const int src = side == 0 ? h + n[a] : h - n[a];
-          // the lower tangential axis fastest, so neighbouring entries touch
-          // neighbouring cells (i on the j- and k-faces)
-          const int e1 = a == 0 ? 1 : 0, e2 = a == 2 ? 1 : 2;
-          for (int u = NG; u < NG + n[e2]; u++)
-            for (int v = NG; v < NG + n[e1]; v++) {
-              int di[3], si[3];
-              di[a] = h, si[a] = src;
-              di[e1] = si[e1] = v;
-              di[e2] = si[e2] = u;
-              HaloEntry e{};
-              e.dcv = e.scv = D.cv;
-              e.dvol = e.svol = D.vol;
-              e.didx = cell_index(D, di[0], di[1], di[2]);
-              e.sidx = cell_index(D, si[0], si[1], si[2]);
-              (layer == 0 ? l0 : l1).push_back(e);
-            }
-        }
+    p->run.push_back(slot_dev(s));
   }
   // the boxes: for each running block and face, the NG halo planes, i
   // fastest, each cell's source n cells across along the face's axis
+  // and, after them, the first layer alone (depth 1, next to the interior),
+  // the gradients' fill; no per-cell list is built
   std::vector<HaloPatch> boxes;
-  for (const BlockDev &D : p->run) {
-    const int n[3] = {D.nx, D.ny, D.nz};
-    const int step[3] = {1, D.X, D.X * D.Y};
-    for (int a = 0; a < 3; a++)
-      for (int side = 0; side < 2; side++) {
-        int lo[3] = {NG, NG, NG}, ext[3] = {n[0], n[1], n[2]};
-        lo[a] = side == 0 ? 0 : NG + n[a];
-        ext[a] = NG;
-        HaloPatch P{};
-        P.dcv = P.scv = D.cv;
-        P.dvol = P.svol = (int)D.vol;
-        P.d0 = (int)cell_index(D, lo[0], lo[1], lo[2]);
-        P.s0 = P.d0 + (side == 0 ? 1 : -1) * n[a] * step[a];
-        for (int d = 0; d < 3; d++) P.dst[d] = P.sst[d] = step[d];
-        P.n0 = ext[0], P.n1 = ext[1], P.cells = ext[0] * ext[1] * ext[2];
-        boxes.push_back(P);
-      }
-  }
+  for (int depth : {NG, 1})
+    for (const BlockDev &D : p->run) {
+      const int n[3] = {D.nx, D.ny, D.nz};
+      const int step[3] = {1, D.X, D.X * D.Y};
+      for (int a = 0; a < 3; a++)
+        for (int side = 0; side < 2; side++) {
+          int lo[3] = {NG, NG, NG}, ext[3] = {n[0], n[1], n[2]};
+          lo[a] = side == 0 ? NG - depth : NG + n[a];
+          ext[a] = depth;
+          HaloPatch P{};
+          P.dcv = P.scv = D.cv;
+          P.dvol = P.svol = (int)D.vol;
+          P.d0 = (int)cell_index(D, lo[0], lo[1], lo[2]);
+          P.s0 = P.d0 + (side == 0 ? 1 : -1) * n[a] * step[a];
+          for (int d = 0; d < 3; d++) P.dst[d] = P.sst[d] = step[d];
+          P.n0 = ext[0], P.n1 = ext[1], P.cells = ext[0] * ext[1] * ext[2];
+          boxes.push_back(P);
+        }
+    }
   std::vector<int2> bcta;
-  for (int q = 0; q < (int)boxes.size(); q++)
+  const int nfull = (int)boxes.size() / 2;
+  for (int q = 0; q < (int)boxes.size(); q++) {
+    if (q == nfull) p->nboxcta = (long long)bcta.size();
     for (int t = 0; t < (boxes[q].cells + 255) / 256; t++) bcta.push_back(make_int2(q, t));
+  }
+  if (boxes.empty()) p->nboxcta = 0;
+  p->nboxcta0 = (long long)bcta.size() - p->nboxcta;
   if ((long long)boxes.size() > p->box_cap || (long long)bcta.size() > p->boxcta_cap) {
     CK(cudaStreamSynchronize(p->stream));
     if (p->d_boxes) CK(cudaFree(p->d_boxes));
@@ -2828,19 +2813,7 @@ int pool_rebuild(pgb_pool *p) {
     CK(cudaMemcpyAsync(p->d_boxes, boxes.data(), sizeof(HaloPatch) * boxes.size(), cudaMemcpyHostToDevice, p->stream));
     CK(cudaMemcpyAsync(p->d_boxcta, bcta.data(), sizeof(int2) * bcta.size(), cudaMemcpyHostToDevice, p->stream));
   }
-  p->nboxcta = (long long)bcta.size();
-  p->nhalo_l0 = (long long)l0.size();
-  p->nhalo = (long long)(l0.size() + l1.size());
-  l0.insert(l0.end(), l1.begin(), l1.end());
-  if (p->nhalo > p->halo_cap) {
-    if (p->d_halo) CK(cudaFree(p->d_halo));
-    p->d_halo = nullptr;
-    const long long cap = std::max<long long>(p->nhalo, 2 * p->halo_cap);
-    CK(cudaMalloc(&p->d_halo, sizeof(HaloEntry) * cap));
-    p->halo_cap = cap;
-  }
-  if (p->nhalo)
-    CK(cudaMemcpyAsync(p->d_halo, l0.data(), sizeof(HaloEntry) * p->nhalo, cudaMemcpyHostToDevice, p->stream));
+  p->nhalo_l0 = p->nhalo = 0;
   if (!p->run.empty())
     CK(cudaMemcpyAsync(p->d_run, p->run.data(), sizeof(BlockDev) * p->run.size(), cudaMemcpyHostToDevice, p->stream));
   if (!p->rrun.empty())
@@ -2900,7 +2873,10 @@ PlainCase pool_plain(pgb_pool *p, const BlockDev *d_blks, const BlockDev *h_blks
   pc.halo = p->d_halo;
   pc.nhalo = p->nhalo, pc.nhalo_l0 = p->nhalo_l0;
   // the boxes describe the running table's blocks, built with it
-  if (d_blks == p->d_run) pc.boxes = p->d_boxes, pc.boxcta = p->d_boxcta, pc.nboxcta = p->nboxcta;
+  if (d_blks == p->d_run) {
+    pc.boxes = p->d_boxes, pc.boxcta = p->d_boxcta, pc.nboxcta = p->nboxcta;
+    pc.boxes0 = p->d_boxes, pc.boxcta0 = p->d_boxcta + p->nboxcta, pc.nboxcta0 = p->nboxcta0;
+  }
   pc.visc = sim_visc(p->phys.simulator);
   pc.primary = p->phys.primary, pc.recon = p->phys.recon, pc.limiter = p->phys.limiter;
   pc.chem = p->phys.chemistry == PGB_CHEM_COUPLED;

@@ -40,6 +40,11 @@ struct PlainCase {
   long long nboxcta;
   const HaloEntry *boxrest;
   long long nboxrest;
+  // the first face layer alone as boxes (the gradients' fill), when the case
+  // lists its halo only as boxes
+  const HaloPatch *boxes0;
+  const int2 *boxcta0;
+  long long nboxcta0;
   const double *rots;         // the rotationally periodic interfaces' rotations, 3 x 3 each
   int visc, primary, recon, limiter;
   int chem;  // 0 none, 1 coupled source, 2 sub-stepped (PGB_CHEM_*)

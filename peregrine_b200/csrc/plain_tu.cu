@@ -48,6 +48,18 @@ void mark(const PlainCase *pc, int kind) {
 
 // the full halo of a register (comps components, vec the component its
 // rotations turn): by boxes when the case has them, else by entries
+// the gradients' fill: the first face layer, each row's directions and the
+// velocity rows turned across a rotational periodic
+void grads_fill(const PlainCase *pc) {
+  constexpr int NG3 = 3 * (NE - 1);
+  if (pc->boxcta0 && pc->nboxcta0 > 0)
+    halo_boxes_launch<NG3>((unsigned)pc->nboxcta0, pc->stream, pc->grads, pc->boxes0, pc->boxcta0, nullptr, 0, NG3,
+                           HALO_TENSOR, pc->rots);
+  else
+    k_halo<<<grid_of(pc->nhalo_l0), TH, 0, pc->stream>>>(pc->grads, pc->halo, pc->nhalo_l0, NG3, HALO_TENSOR,
+                                                        pc->rots);
+}
+
 void halo_fill(const PlainCase *pc, double *base, int comps, int vec, int stride = 0) {
   if (pc->boxcta && pc->nboxcta > 0)
     halo_boxes_launch<NE, SW>((unsigned)pc->nboxcta, pc->stream, base, pc->boxes, pc->boxcta, pc->boxrest, pc->nboxrest,
@@ -298,8 +310,7 @@ extern "C" int PGB_ENTRY(pgb_plain_rhs_)(const PlainCase *pc, const double *Q, d
     }
   }
   if (pc->visc) {
-    k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1), HALO_TENSOR,
-                                                pc->rots);
+    grads_fill(pc);
     mark(pc, 0);
     bc_grads_launch(pc);
   }
@@ -550,8 +561,7 @@ extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs
   if (chem) for_blocks(pc, R_INNER, rsource_launch, rs, 2);
   if (pc->visc) {
     for_blocks(pc, R_INNER, rgrads_launch, rs, 2);
-    k_halo<<<grid_of(pc->nhalo_l0), TH, 0, s>>>(pc->grads, pc->halo, pc->nhalo_l0, 3 * (NE - 1), HALO_TENSOR,
-                                                pc->rots);
+    grads_fill(pc);
     mark(pc, 0);
   }
   for_blocks(pc, R_FX, rface_launch<0>, rs, 2);
