@@ -690,9 +690,9 @@ def main():
                     help="one warm-up and one RK3 step of the 96^3 reacting case on the batched path, no graph, "
                          "with the named source kernel: the command an ncu capture of its passes runs")
     ap.add_argument("--serving-only", action="store_true", help="the serving leg alone")
-    ap.add_argument("--serving-profile", action="store_true",
-                    help="200 seeded requests admitted into one pool at once, then three pool steps: the command an "
-                         "ncu launch list of a saturated pool step runs")
+    ap.add_argument("--serving-profile", type=int, default=0, metavar="N",
+                    help="N seeded requests admitted into one pool at once, then three pool steps: the command an "
+                         "ncu launch list of a pool step runs (200: saturated)")
     ap.add_argument("--realgas-only", action="store_true", help="the real-gas leg alone")
     ap.add_argument("--no-realgas", action="store_true", help="skip the real-gas leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
@@ -722,7 +722,7 @@ def main():
         print(json.dumps({"serving": serving_leg()}), flush=True)
         return
     if args.serving_profile:
-        serving_profile()
+        serving_profile(args.serving_profile)
         return
     if args.reacting_only:
         print(json.dumps({"reacting": reacting_leg(max(1, min(args.steps, 20)), cpu=not args.no_cpu)}), flush=True)

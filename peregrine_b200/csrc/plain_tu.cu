@@ -584,7 +584,8 @@ extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs
 // the serving pool's reactors: one stage of every running reactor, and a
 // reactor's state from its primitives
 extern "C" int PGB_ENTRY(pgb_plain_reactors_)(const ReactorStage *rs, cudaStream_t s) {
-  if (rs->n > 0) k_reactors<NS><<<grid_of(rs->n), TH, 0, s>>>(*rs);
+  // a warp a reactor, eight a CTA
+  if (rs->n > 0) k_reactors_warp<NS><<<(unsigned)((rs->n + 7) / 8), 256, 0, s>>>(*rs);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PGB_OK : cuda_fail(e, "reactors");
 }

@@ -272,6 +272,77 @@ __global__ void __launch_bounds__(256) k_reactors(const ReactorStage a) {
   }
 }
 
+// A warp per reactor: every lane forms the same clipped mass fractions, state
+// and rate state; the lanes take the reactions' rates of progress k, k + 32,
+// ... (the mechanism's global copy, lanes reading different reactions),
+// staged in shared memory; then every lane sums the fold in reaction order,
+// as cellrates' fold does (the same products and sums in the same order: the
+// same bits), and lane l writes component l's combines.
+template <int NS>
+__global__ void __launch_bounds__(256) k_reactors_warp(const ReactorStage a) {
+  constexpr int NE = 4 + NS;
+  __shared__ double sh[8][MAXRXN];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 8 + w;
+  if (t >= a.n) return;  // a warp's lanes alike
+  const long long r = a.rows[t], cap = a.cap;
+  auto Qf = [&](int c) { return a.Q[c * cap + r]; };
+  const State st = fromQ<NS>(Qf, a.T[r]);
+  // cellrates: the clipped mass fractions and the rate state
+  const double rho = Qf(0), rhoinv = 1.0 / rho;
+  double Ylast = 1.0, Ysum = 0.0;
+#pragma unroll
+  for (int n = 0; n < NS - 1; n++) {
+    const double Yn = fmax(fmin(Qf(5 + n) * rhoinv, 1.0), 0.0);
+    Ylast -= Yn;
+    Ysum += Yn;
+  }
+  const double Yscale = 1.0 / fmax(Ysum, 1.0);
+  Ylast = fmax(Ylast, 0.0);
+  auto Y = [&](int n) { return n < NS - 1 ? fmax(fmin(Qf(5 + n) * rhoinv, 1.0), 0.0) * Yscale : Ylast; };
+  RateState<NS> s;
+  ratestate<NS>(s, rho, Y, st.T);
+  const int nr = kMech.nr;
+  for (int k = lane; k < nr; k += 32) {
+    const Rxn &rx = gMech.rxn[k];
+    double fwd, rev;
+    oneway<NS>(rx, s, fwd, rev);
+    sh[w][k] = rx.reversible ? fwd - rev : fwd;
+  }
+  __syncwarp();
+  double omega[NS];
+#pragma unroll
+  for (int n = 0; n < NS; n++) omega[n] = 0.0;
+  for (int k = 0; k < nr; k++) {
+    const Rxn &rx = kMech.rxn[k];
+    const double rp = sh[w][k];
+    for (int j = 0; j < rx.nnet; j++) omega[rx.netsp[j]] += rx.netnuMW[j] * rp;
+  }
+  // every lane has read T above; one writes the new guess
+  if (lane == 0) a.T[r] = st.T;
+  if (lane >= NE) return;
+  const int l = lane;
+  const double dt = *a.dt;
+  double dq = 0.0;
+#pragma unroll
+  for (int n = 0; n < NS; n++)
+    if (l == 5 + n) dq = omega[n];
+  const long long at = l * cap + r;
+  double first = 0.0;
+  for (int m = 0; m < a.ncomb; m++) {
+    const RCombine &cb = a.comb[m];
+    auto val = [&](int n) {
+      const int src = cb.src[n];
+      return src == -1 ? dq : src == -2 ? first : cb.X[n][at];
+    };
+    auto term = [&](int n) { return (cb.step && n == cb.nterms - 1) ? cb.w[n] * dt * val(n) : cb.w[n] * val(n); };
+    double acc = term(0);
+    for (int n = 1; n < cb.nterms; n++) acc = acc + term(n);
+    if (m == 0) first = acc;
+    if (cb.write) cb.out[at] = acc;
+  }
+}
+
 // a reactor's Q and starting T from its primitives p, u, v, w, T, Y...
 // (the reference's fromprims, peregrine/simulator/euler/kernels/state/fromprims.mako)
 template <int NS>
