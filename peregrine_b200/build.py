@@ -40,6 +40,24 @@ def units():
     return out
 
 
+def shared_kernels(objs=None):
+    """The library's symbols (namespace pgb) that more than one object
+    defines.  Each unit holds its own constant memory (species, mechanism),
+    so a template instantiated by two units is two kernels reading different
+    constants; the linker keeps a single host launch stub for them, and a
+    launch may then run either unit's copy.  Empty when every unit's kernels
+    are its own."""
+    objs = objs if objs is not None else [o for _, o, _ in units()]
+    seen = {}
+    for obj in objs:
+        r = subprocess.run(["nm", "--defined-only", obj], capture_output=True, text=True, check=True)
+        for line in r.stdout.splitlines():
+            parts = line.split()
+            if len(parts) == 3 and parts[1] in ("W", "T") and parts[2].startswith("_ZN3pgb"):
+                seen.setdefault(parts[2], []).append(os.path.basename(obj))
+    return sorted(f"{name} ({', '.join(where)})" for name, where in seen.items() if len(where) > 1)
+
+
 def stale():
     if not os.path.exists(TARGET):
         return True
@@ -64,6 +82,10 @@ def build(force=False, verbose=False, jobs=None):
 
     with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as pool:
         objs = list(pool.map(compile_one, units()))
+    shared = shared_kernels(objs)
+    if shared:
+        raise RuntimeError("kernels defined by more than one unit (the linker would keep one launch stub for "
+                           "copies that read different constant memory):\n  " + "\n  ".join(shared[:20]))
     cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", TARGET, *objs, "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)

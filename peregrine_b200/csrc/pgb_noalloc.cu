@@ -26,6 +26,13 @@
 #include <string>
 
 #include "pgb200.h"
+
+// This unit's kernels under a name of their own.  The per-species units
+// instantiate the same templates (k_fromQ<1>, k_advflux<2, 0>, ...), each
+// against its own unit's constant memory; under one name the linker keeps
+// one host launch stub for both, and a launch from either unit may run the
+// other's copy, which reads the other unit's species constants.
+#define pgb pgb_noalloc_unit
 #include "plain.cuh"
 
 using namespace pgb;

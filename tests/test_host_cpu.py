@@ -32,6 +32,17 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert set(names) <= set(native.SIGNATURES), set(names) - set(native.SIGNATURES)
 
 
+def test_no_kernel_is_defined_by_two_units():
+    # every unit keeps its own constant memory, so a kernel template two units
+    # instantiate is two kernels behind one linked launch stub
+    from peregrine_b200 import build
+
+    objs = [o for _, o, _ in build.units()]
+    if not all(os.path.exists(o) for o in objs):
+        pytest.skip("the library's objects are not built here")
+    assert build.shared_kernels(objs) == []
+
+
 def test_errors_carry_the_library_message():
     lib = native.load()
     rc = lib.pgb_case_create(None, None)
