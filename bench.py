@@ -105,6 +105,11 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: the region opens once it
+            # samples (within 5 s), so a short region is not left unsampled
+            t0 = time.monotonic()
+            while not self.samples and self.proc.poll() is None and time.monotonic() - t0 < 5.0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -681,6 +686,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-extra", action="store_true", help="skip the per-block and end-to-end legs")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape and tiles")
+    ap.add_argument("--halo-fill", action="store_true",
+                    help="fill each stage's halo before it instead of reading across the blocks' faces")
     ap.add_argument("--shape", default=None, help="force the fused kernel's THREADSxMINBLOCKSxWIDTH (no tuning)")
     ap.add_argument("--ksplit", type=int, default=3, help="k runs per block with --shape")
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
@@ -749,6 +756,10 @@ def main():
         return
 
     mb, mesh, prims = build_case("batched", device=local)
+    if args.halo_fill:
+        from peregrine_b200 import native
+
+        native.call("pgb_case_set_halo_pull", mb.case, 0)
     dt = stable_dt()
     ncells = mb.ncells
     mb.step(dt, 1)

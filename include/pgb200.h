@@ -428,6 +428,18 @@ int pgb_get_tile(const pgb_case *c, int blk, int *tw, int *th, int *kchunk);
  * ints each (threads, minblocks, width, height) */
 int pgb_set_fused_shape(pgb_case *c, int threads, int minblocks, int width);
 int pgb_fused_shapes(int *shapes, int cap, int *n);
+/* Whether a uniform-metric stage reads the cells past its blocks' faces
+ * straight from the neighbouring blocks in place of a halo fill before it
+ * (on by default).  It does so only where every face of every block is joined
+ * to a neighbour low face to high face in the identity orientation, without
+ * rotation, both blocks at least two cells thick across it, no exchange with
+ * another case fills a halo, and the 256- or 128-thread instances run; the
+ * result is the same either way.  pgb_case_halo_pull reports whether stages
+ * of the finalized case read that way.  Other readers of a halo still get it
+ * from pgb_exchange (the reference's exchange before a right-hand side,
+ * peregrine/multiblock/collections/exchange/collection.py). */
+int pgb_case_set_halo_pull(pgb_case *c, int on);
+int pgb_case_halo_pull(const pgb_case *c, int *on);
 
 /* The batched path's form for the case: 1 the fused stage kernel (the
  * calorically perfect single-species gas with kepaec on the cells as they

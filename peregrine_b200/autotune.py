@@ -15,7 +15,7 @@ import numpy as np
 
 from peregrine_b200 import native
 
-KSPLITS = (2, 3, 4)
+KSPLITS = (1, 2, 3, 4)
 
 
 def shapes():

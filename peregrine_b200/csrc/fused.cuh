@@ -65,6 +65,13 @@ struct FusedArgs {
   const double *prep[2];
   int write[2];
   const double *dt;
+  // 1: the uniform kernel reads its tiles' ring and the planes beyond a
+  // block's k ends from the neighbouring blocks' cells (every face joined,
+  // unrotated, in the identity orientation, the neighbour at least NG cells
+  // thick), and no halo fill precedes it; nbr27[27 b + q] is then the block
+  // one step away from b along each axis, q = (dk + 1) 9 + (dj + 1) 3 + di + 1
+  int pull;
+  const int *nbr27;
 };
 
 // fields of a cell plane in shared memory

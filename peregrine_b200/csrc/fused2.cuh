@@ -21,6 +21,17 @@
 //            the k-face between k and k+1; dQ, combines and stores for the
 //            tile's cells of plane k.
 //
+// Where a tile's ring or a plane beyond its block's k ends lies past a face,
+// the cell comes either from the block's halo, filled by a launch before the
+// stage, or (a.pull) straight from the neighbouring block's own cells, with
+// no fill: every face of the case joined low face to high face in the
+// identity orientation, unrotated, both blocks at least NG cells thick.  The
+// block a cell comes from is the one a halo cell's source is located in
+// (across i first, then j, then k), so the values, and the results, are the
+// fill's to the bit.  Each thread works out its two cells' sources at tile
+// start: the planes inside the block in registers, the planes below and
+// above it in shared memory.
+//
 // Measured and set aside: one barrier a plane, with three plane slots, two
 // gradient planes and two face-flux planes standing in for the second (the
 // gradients of plane k+1 formed before the barrier, plane k+3's values after
@@ -167,17 +178,21 @@ __device__ __forceinline__ void cp_wait() {
 // a cell's twelve contiguous in a record of GS (14 doubles, for the same
 // reason), Fi[5][LN1], Fj[5][LN1]
 // low-face fluxes, raw[3][5][NT + LNR] the Q copies of three planes in
-// flight, pre[3][2][5][LNT] the combines' registers of three planes.
+// flight, pre[3][2][5][LNT] the combines' registers of three planes, and the
+// sources of a thread's two fetched cells in the planes below and above the
+// block (those inside it a thread keeps in registers): src[2][NT + LNR]
+// pointers to the source cell's plane 0, then vol[2][NT + LNR] and
+// plane[2][NT + LNR] its block's component and plane strides.
 template <int NT, int TW, int TH>
 struct F2L {
   static constexpr int LW1 = TW + 2, LH1 = TH + 2, LN1 = LW1 * LH1;
   static constexpr int LW2 = TW + 4, LN2 = LW2 * (TH + 4), LNR = 2 * (TW + TH), LNT = TW * TH;
-  static constexpr int RAW = 5 * (NT + LNR), PRE = 2 * 5 * LNT;
+  static constexpr int RAW = 5 * (NT + LNR), PRE = 2 * 5 * LNT, SRC = 2 * (NT + LNR);
   static constexpr int GS = 14;  // a gradient record: twelve values and two of padding
   static_assert(LN1 <= NT, "the tile and its ring fit the CTA");
   static_assert(LNR <= NT, "the outer ring fits the CTA");
   __host__ __device__ static constexpr size_t doubles(bool visc) {
-    return (size_t)2 * P_N * LN2 + (visc ? GS * LN1 : 0) + 10 * LN1 + 3 * RAW + 3 * PRE;
+    return (size_t)2 * P_N * LN2 + (visc ? GS * LN1 : 0) + 10 * LN1 + 3 * RAW + 3 * PRE + 2 * SRC;
   }
 };
 
@@ -194,6 +209,8 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
   double *Fj = Fi + 5 * LN1;
   double *raw = Fj + 5 * LN1;  // [3][5][NT] own cells then [5][LNR] ring cells, per slot
   double *pre = raw + 3 * L::RAW;  // [3][2][5][LNT]
+  const double **src = reinterpret_cast<const double **>(pre + 3 * L::PRE);  // [2][NT + LNR]
+  int *svol = reinterpret_cast<int *>(src + L::SRC), *splane = svol + L::SRC;
   for (;;) {
     if (tid == 0) s_tile = (int)atomicAdd(a.counter, 1u);
     __syncthreads();
@@ -207,7 +224,6 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
     const int nring = 2 * (tw + th);
     const int v = (int)B.vol;
     const int sJ = B.X, sK = B.X * B.Y;
-    const double *Q = a.R[a.qin] + 5 * B.cv;
     const bool col = tid < N1;
     // the columns in warp order: the tile's first, then the ring's high edges
     // (the i-faces of its last column and the j-faces of its top row are the
@@ -241,7 +257,40 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
       r2 = x2 + LW2 * y2;
     }
     const int o1 = (T.j0 + jj + 1) * sJ + (T.i0 + ii + 1);
-    const int o2 = (T.j0 + y2) * sJ + (T.i0 + x2);
+    // where each of this thread's fetched cells comes from, per k region:
+    // the block's own cell (its halo beyond a face) or, when the stage pulls,
+    // the cell of the block one step across each face it lies past (the
+    // block a halo cell's source is located in, i first, then j, then k).
+    // The planes inside the block (region 1) come back in q, sv, sk; those
+    // below and above it (regions 0, 2) go to entry e of the shared table:
+    // tid for the column, NT + tid for the outer ring cell.
+    const double *Rq = a.R[a.qin];
+    auto source_of = [&](int I, int J, int e, const double *&q, int &sv, int &sk) {
+      const int di = I < 0 ? -1 : I < B.nx ? 0 : 1, dj = J < 0 ? -1 : J < B.ny ? 0 : 1;
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const int sb = a.pull ? a.nbr27[27 * T.blk + 9 * r + 3 * (dj + 1) + di + 1] : T.blk;
+        const BlockDev &S = a.blks[sb];
+        int i = I, j = J, dk = 0;
+        if (a.pull) {
+          i = di < 0 ? I + S.nx : di > 0 ? I - B.nx : I;
+          j = dj < 0 ? J + S.ny : dj > 0 ? J - B.ny : J;
+          dk = r == 0 ? S.nz : r == 2 ? -B.nz : 0;
+        }
+        const int plane = S.X * S.Y;
+        const double *at = Rq + 5 * S.cv + (long long)(dk + NG) * plane + (j + NG) * S.X + (i + NG);
+        if (r == 1) {
+          q = at, sv = (int)S.vol, sk = plane;
+        } else {
+          const int x = (r >> 1) * (NT + LNR) + e;
+          src[x] = at, svol[x] = (int)S.vol, splane[x] = plane;
+        }
+      }
+    };
+    const double *qc = nullptr, *qr = nullptr;
+    int vc = 0, kc = 0, vr = 0, kr = 0;
+    if (col) source_of(T.i0 + ii - 1, T.j0 + jj - 1, tid, qc, vc, kc);
+    if (r2 >= 0) source_of(T.i0 + x2 - 2, T.j0 + y2 - 2, NT + tid, qr, vr, kr);
     auto slot = [](int p) { return p & 1; };
     auto ring3 = [](int p) { return (p + 6) % 3; };
     auto getP = [&](int s, int r) {
@@ -256,16 +305,22 @@ __global__ void __launch_bounds__(NT, MINB) k_fused2(const FusedArgs a) {
       Ps[0] = make_double2(c.rho, c.u), Ps[1] = make_double2(c.v, c.w), Ps[2] = make_double2(c.T, c.e);
     };
     // plane p's Q copies for this thread's cells, into raw slot p mod 3
+    const int nzb = B.nz;
     auto fetch = [&](int p) {
       double *rs = raw + ring3(p) * L::RAW;
-      const int z = (p + NG) * sK;
+      const bool inside = p >= 0 && p < nzb;
+      const int r = (p < 0 ? 0 : 1) * (NT + LNR);
       if (col) {
+        const double *q = inside ? qc + p * kc : src[r + tid] + p * splane[r + tid];
+        const int sv = inside ? vc : svol[r + tid];
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(rs + l * NT + tid, Q + l * v + z + o1);
+        for (int l = 0; l < 5; l++) cp8(rs + l * NT + tid, q + l * sv);
       }
       if (r2 >= 0) {
+        const double *q = inside ? qr + p * kr : src[r + NT + tid] + p * splane[r + NT + tid];
+        const int sv = inside ? vr : svol[r + NT + tid];
 #pragma unroll
-        for (int l = 0; l < 5; l++) cp8(rs + 5 * NT + l * LNR + tid, Q + l * v + z + o2);
+        for (int l = 0; l < 5; l++) cp8(rs + 5 * NT + l * LNR + tid, q + l * sv);
       }
     };
     // plane p's combine registers for a tile cell, into pre slot p mod 3

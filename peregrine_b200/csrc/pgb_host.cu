@@ -167,6 +167,10 @@ struct pgb_case {
 
   int v2_ctas = 1;      // its resident CTAs per SM
   int v2 = 0;           // its instance: threads per CTA, launch bound, tile layout
+  // the uniform stage reads across faces from the neighbours' cells in place
+  // of a halo fill: wanted (the default), and whether every face allows it
+  bool pull_want = true, pull_faces = false;
+  int *d_nbr27 = nullptr;  // per block, the block one step away along each axis
   // register mapping: logical -> physical
   std::vector<int> phys_of, canonical;
   int period = 1, phase = 0;
@@ -686,16 +690,17 @@ struct V2Inst {
   int nt, minb, tw, th;
   const void *fvisc, *feuler;
   size_t smvisc, smeuler;
+  bool pull;  // reads across faces from the neighbours' cells when the case allows
 };
 #define PGB_V2(NT, MB, TW, TH)                                                                    \
   V2Inst{NT, MB, TW, TH, (const void *)k_fused2<true, NT, MB, TW, TH>,                             \
          (const void *)k_fused2<false, NT, MB, TW, TH>, fused2_smem<NT, TW, TH>(true),             \
-         fused2_smem<NT, TW, TH>(false)}
+         fused2_smem<NT, TW, TH>(false), true}
 // the warp-specialised form: sixteen warps of 128 registers
 #define PGB_V3(NT, MB, TW, TH)                                                                    \
   V2Inst{NT, MB, TW, TH, (const void *)k_fused3<true, NT, MB, TW, TH>,                             \
          (const void *)k_fused3<false, NT, MB, TW, TH>, fused3_smem<NT, TW, TH>(true),             \
-         fused3_smem<NT, TW, TH>(false)}
+         fused3_smem<NT, TW, TH>(false), false}
 const V2Inst kV2[] = {PGB_V2(256, 1, 24, 7), PGB_V2(256, 1, 30, 6), PGB_V2(128, 2, 14, 6), PGB_V3(512, 1, 14, 8),
                       PGB_V3(512, 1, 16, 7)};
 #undef PGB_V2
@@ -958,6 +963,38 @@ void mark(pgb_case *c, int kind, int &count) {
   c->tkind.push_back(kind);
 }
 
+// Whether every face of every block lets a stage read across it from the
+// neighbour's cells in place of its halo: joined to a neighbour low face to
+// high face in the identity orientation, unrotated, with both blocks at least
+// NG cells thick along the axis, so a halo cell's source lies one face away
+// along each axis it is outside (what locate finds, axis by axis).
+bool faces_pullable(const pgb_case *c) {
+  for (const HostBlock &B : c->blocks) {
+    const int n[3] = {B.nx, B.ny, B.nz};
+    for (int f = 0; f < 6; f++) {
+      const int a = f / 2, nb = B.nbr[f];
+      if (nb < 0 || B.rot[f] || B.bc[f] >= 0 || n[a] < NG) return false;
+      if (B.nbrface[f] != (f % 2 ? f : f + 2)) return false;
+      for (int d = 0; d < 3; d++)
+        if (B.orient[f][d] != d + 1) return false;
+      const HostBlock &N = c->blocks[nb];
+      const int m[3] = {N.nx, N.ny, N.nz};
+      if (m[a] < NG) return false;
+      for (int d = 0; d < 3; d++)
+        if (d != a && m[d] != n[d]) return false;
+    }
+  }
+  return true;
+}
+
+// whether the case's uniform stages pull across faces: wanted, the faces
+// allow it, the instance reads that way, and no face's halo comes from an
+// exchange with another case
+bool pulls(const pgb_case *c) {
+  return c->pull_want && c->pull_faces && c->use_v2 && c->v2 >= 0 && c->v2 < kNV2 && kV2[c->v2].pull &&
+         c->nxrecv == 0;
+}
+
 // the uniform kernel of the case's instance
 const void *v2_kernel(const pgb_case *c) {
   if (c->v2 < 0 || c->v2 >= kNV2) return nullptr;
@@ -1022,9 +1059,13 @@ int launch_fused(pgb_case *c, const FusedStagePlan &p, int stage_index, int &cou
   }
   for (int q = 0; q < 2; q++) a.prep[q] = q < a.npre ? c->d_reg[a.pre[q]] : nullptr;
   a.dt = dtp ? dtp : c->d_dt;
-  // the stencil register's halo first
-  halo_fill_case(c, c->d_reg[p.qin], c->ne, 1);
-  mark(c, K_HALO, count);
+  // the stencil register's halo first, unless the stage reads across faces
+  a.pull = pulls(c) ? 1 : 0;
+  a.nbr27 = c->d_nbr27;
+  if (!a.pull) {
+    halo_fill_case(c, c->d_reg[p.qin], c->ne, 1);
+    mark(c, K_HALO, count);
+  }
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1548,7 +1589,7 @@ int pgb_case_destroy(pgb_case *c) {
   void *ptrs[] = {c->d_blks, c->d_met, c->d_dt, c->d_one, c->d_xsend, c->d_xrecv, c->d_xsvol, c->d_xrvol, c->d_halo, c->d_boxes, c->d_boxcta, c->d_boxrest, c->d_state, c->d_tr, c->d_hsp, c->d_grads,
                   c->d_F[0], c->d_F[1], c->d_F[2], c->d_prims, c->d_tiles, c->d_counter, c->d_stage,
                   c->d_bcent, c->d_bcops, c->d_bcface[0], c->d_bcface[1], c->d_bcface[2], c->d_clock,
-                  c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots};
+                  c->d_cfl, c->d_ctrl, c->d_subs, c->d_stiffhead, c->d_stiffcells, c->d_rots, c->d_nbr27};
   if (c->gen_lib) cudaLibraryUnload(c->gen_lib);
   if (c->d_math) cudaFree(c->d_math);
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
@@ -1822,6 +1863,9 @@ int pgb_case_set_exchange(pgb_case *c, long long nsend, const int *send_blk, con
   RET(table(nsend, send_blk, send_idx, c->d_xsend, c->d_xsvol));
   RET(table(nrecv, recv_blk, recv_idx, c->d_xrecv, c->d_xrvol));
   c->nxsend = nsend, c->nxrecv = nrecv;
+  // a stage reads halo copies once another case fills some of them
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
   return PGB_OK;
 }
 
@@ -2028,6 +2072,20 @@ int pgb_case_set_stages(pgb_case *c, const pgb_stage *stages, int nstages) {
   return PGB_OK;
 }
 
+int pgb_case_set_halo_pull(pgb_case *c, int on) {
+  if (!c) return fail(PGB_ERR_ARG, "null case");
+  c->pull_want = on != 0;
+  for (auto &g : c->graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
+  return PGB_OK;
+}
+
+int pgb_case_halo_pull(const pgb_case *c, int *on) {
+  if (!c || !on) return fail(PGB_ERR_ARG, "null argument");
+  *on = c->finalized && pulls(c) ? 1 : 0;
+  return PGB_OK;
+}
+
 int pgb_case_set_generated_chemistry(pgb_case *c, int on) {
   if (!c) return fail(PGB_ERR_ARG, "null case");
   if (c->finalized) return fail(PGB_ERR_STATE, "the case is finalized");
@@ -2085,6 +2143,24 @@ int pgb_case_finalize(pgb_case *c) {
   if (!c->ev0) CK(cudaEventCreate(&c->ev0));
   if (!c->ev1) CK(cudaEventCreate(&c->ev1));
   c->cells = layout_blocks(c);
+  c->pull_faces = faces_pullable(c);
+  if (c->pull_faces) {
+    // the block reached from b by a step of (di, dj, dk), i first, then j,
+    // then k, as a halo cell's source is located
+    std::vector<int> t(27 * c->blocks.size());
+    for (int b = 0; b < (int)c->blocks.size(); b++)
+      for (int dk = -1; dk <= 1; dk++)
+        for (int dj = -1; dj <= 1; dj++)
+          for (int di = -1; di <= 1; di++) {
+            int s = b;
+            if (di) s = c->blocks[s].nbr[di < 0 ? 0 : 1];
+            if (dj) s = c->blocks[s].nbr[dj < 0 ? 2 : 3];
+            if (dk) s = c->blocks[s].nbr[dk < 0 ? 4 : 5];
+            t[27 * b + 9 * (dk + 1) + 3 * (dj + 1) + di + 1] = s;
+          }
+    CK(cudaMalloc(&c->d_nbr27, sizeof(int) * t.size()));
+    CK(cudaMemcpy(c->d_nbr27, t.data(), sizeof(int) * t.size(), cudaMemcpyHostToDevice));
+  }
   c->interior_cells = 0;
   for (auto &B : c->blocks) c->interior_cells += (long long)B.nx * B.ny * B.nz;
   const size_t n = (size_t)c->cells;

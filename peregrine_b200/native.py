@@ -247,6 +247,8 @@ SIGNATURES = {
                         ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_set_fused_shape": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pgb_fused_shapes": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "pgb_case_set_halo_pull": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "pgb_case_halo_pull": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "pgb_rhs_block_noalloc": ([ctypes.POINTER(Physics), ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
                                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                               ctypes.c_int),

@@ -204,3 +204,64 @@ def test_the_stages_by_hand_are_a_step(integrator):
     for a, b in zip(mb.blocks, ref.blocks):
         assert np.array_equal(a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior])
     assert mb.dt.get() == dt
+
+
+def _pull_case(simulator, mesh, seed=5):
+    import peregrine_b200 as pg
+
+    cfg = cases.tgv_config(simulator, "tvd-rk3", "batched")
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    mb.set_prims(cases.tgv_prims(mb.mesh_blocks, mb.metrics, seed=seed, noise=1e-3))
+    return mb
+
+
+def _pulls(mb):
+    import ctypes
+
+    on = ctypes.c_int(-1)
+    native.call("pgb_case_halo_pull", mb.case, ctypes.byref(on))
+    return on.value
+
+
+@pytest.mark.parametrize("shape", [(256, 1, 24), (256, 1, 30), (128, 2, 14)])
+@pytest.mark.parametrize("blocks,low,high", [((3, 3, 3), 6, 11), ((2, 1, 2), 5, 19), ((1, 3, 1), 2, 14)])
+@pytest.mark.parametrize("simulator", ["euler", "navier-stokes"])
+def test_reading_across_faces_gives_the_halo_fills_bits(simulator, blocks, low, high, shape):
+    # the uniform stage reading its tiles' ring and the planes past a block's
+    # k ends straight from the neighbouring blocks (i first, then j, then k:
+    # the order a halo cell's source is found in) gives the bits the halo fill
+    # before each stage gives, on uneven blocks two cells thick and up, tiles
+    # of several k runs, a block that is its own neighbour across j
+    runs = []
+    for pull in (1, 0):
+        mb = _pull_case(simulator, cases.tgv_mesh(24, blocks, seed=7, low=low, high=high))
+        native.call("pgb_case_set_halo_pull", mb.case, pull)
+        mb.step(1e-6)
+        native.call("pgb_set_fused_shape", mb.case, *shape)
+        mb.step(2e-5, 3)
+        assert all(mb.uniform(n) for n in range(len(mb.blocks)))
+        assert _pulls(mb) == pull
+        runs.append([b.Q.get()[b.mesh.interior] for b in mb.blocks])
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
+
+
+def test_a_block_thinner_than_the_halo_keeps_the_fill():
+    # a halo cell past a block one cell thick comes from two faces away, so
+    # the stage keeps the halo fill, and matches the oracle
+    from oracle.oracle import Oracle
+    from peregrine_b200.mesher import CubeMesher
+
+    mesh = CubeMesher(mbdims=[3, 1, 1], cells=[[10, 1, 13], [16], [16]], lengths=[2 * np.pi] * 3,
+                      periodic=[True] * 3)
+    mb = _pull_case("navier-stokes", mesh)
+    prims = cases.tgv_prims(mb.mesh_blocks, mb.metrics, seed=5, noise=1e-3)
+    mb.set_prims(prims)
+    orc = Oracle(mb.mixture.constants(), 1, "navier-stokes", mb.mesh_blocks, mb.metrics, "tvd-rk3")
+    orc.set_prims(prims)
+    mb.step(2e-5, 2)
+    orc.step(2e-5)
+    orc.step(2e-5)
+    assert _pulls(mb) == 0
+    for b, w in zip(mb.blocks, orc.regs[0]):
+        assert rowmax_err(b.Q.get()[b.mesh.interior], w[b.mesh.interior]) < STATE_TOL
