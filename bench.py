@@ -426,8 +426,9 @@ def realgas_leg(steps, cpu=True):
     out = {"value": b["value"], "unit": "cell-stage/s", "steps": steps, "ms_per_step": b["ms_per_step"],
            "launches_per_step": b["launches_per_step"], "dt": dt,
            "workload": "mixing-layer-256x128x4-8-uneven-blocks-o2-h2-60bar-peng-robinson-double-flux-kepaec-euler-rk3",
-           "path": "batched: the planes frozen each step (a launch a pass over every block), then per stage Q's "
-                   "halo, the state off the planes and one kernel of each cell's six faces, divergence and combines",
+           "path": "batched: the planes frozen each step (a launch a pass over every block), then per stage the "
+                   "interior's state off the planes, Q's halo with the state's copy in one pass, and one kernel "
+                   "of each cell's six faces, divergence and combines",
            "blocks": [b_.cells[0] for b_ in mb.mesh_blocks], "per_block": legs["per_block"], "packed": legs["packed"],
            "speedup_vs_per_block": legs["per_block"]["ms_per_step"] / b["ms_per_step"],
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

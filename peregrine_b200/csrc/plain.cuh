@@ -106,6 +106,37 @@ static __global__ void __launch_bounds__(256) k_halo_boxes(double *__restrict__ 
   halo_copy<C, ROT>(base, comps, vec, rots, p.dcv, didx, p.dvol, p.scv, sidx, p.svol, p.rot, stride);
 }
 
+// two registers' halos in one pass over the boxes: C1 components of the
+// first (its vector at vec turned by a cell's rotation), then C2 scalar
+// components of the second; each with its own stride (0: its component
+// count).  A CTA fills 256 cells of one box, or 256 leftover entries.
+template <int C1, int C2, bool ROT>
+static __global__ void __launch_bounds__(256) k_halo_boxes2(double *__restrict__ base1, int vec, int stride1,
+                                                            double *__restrict__ base2, int stride2,
+                                                            const HaloPatch *__restrict__ boxes,
+                                                            const int2 *__restrict__ cta,
+                                                            const HaloEntry *__restrict__ rest, long long nrest,
+                                                            const double *__restrict__ rots) {
+  if (stride1 == 0) stride1 = C1;
+  if (stride2 == 0) stride2 = C2;
+  const int2 w = cta[blockIdx.x];
+  const int t = w.y * 256 + (int)threadIdx.x;
+  if (w.x < 0) {
+    if (t >= nrest) return;
+    const HaloEntry h = rest[t];
+    halo_copy<C1, ROT>(base1, C1, vec, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, h.rot, stride1);
+    halo_copy<C2, false>(base2, C2, HALO_SCALARS, rots, h.dcv, h.didx, h.dvol, h.scv, h.sidx, h.svol, 0, stride2);
+    return;
+  }
+  const HaloPatch &p = boxes[w.x];
+  if (t >= p.cells) return;
+  const int x0 = t % p.n0, r = t / p.n0, x1 = r % p.n1, x2 = r / p.n1;
+  const int didx = p.d0 + x0 * p.dst[0] + x1 * p.dst[1] + x2 * p.dst[2];
+  const int sidx = p.s0 + x0 * p.sst[0] + x1 * p.sst[1] + x2 * p.sst[2];
+  halo_copy<C1, ROT>(base1, C1, vec, rots, p.dcv, didx, p.dvol, p.scv, sidx, p.svol, p.rot, stride1);
+  halo_copy<C2, false>(base2, C2, HALO_SCALARS, rots, p.dcv, didx, p.dvol, p.scv, sidx, p.svol, 0, stride2);
+}
+
 // the box fill of a register of comps components: the kernel built for that
 // count where there is one (a stage's Q), else the loop; the rotation code
 // only where the case has rotations and the register has vectors
@@ -144,12 +175,19 @@ __device__ __forceinline__ void unravel(const BlockDev &B, long long t, int &fi,
 // (peregrine/simulator/euler/kernels/state/fromQ.mako:5-19); for the real
 // gas its fromrhoE and root Z; with plane set, the double flux's fromplane:
 // p off the cell's frozen plane, then the state at rho and p
-// (peregrine/simulator/eulerdf/kernels/fromplane.mako:3-17)
-template <int NS, bool RG = false>
+// (peregrine/simulator/eulerdf/kernels/fromplane.mako:3-17).  With INNER a
+// thread a cell of the interior alone (a launch over R_INNER).
+template <int NS, bool RG = false, bool INNER = false>
 __global__ void k_fromQ(const BlockDev *__restrict__ blks, int b, const double *__restrict__ Qall,
                         double *__restrict__ stall, const int2 *__restrict__ ctab = nullptr, const int plane = 0) {
-  PGB_WHERE(B, t);
-  if (t >= B.vol) return;
+  PGB_WHERE(B, u);
+  long long t = u;
+  if (INNER) {
+    if (u >= (long long)B.nx * B.ny * B.nz) return;
+    t = cell_index(B, (int)(u % B.nx) + NG, (int)((u / B.nx) % B.ny) + NG, (int)(u / ((long long)B.nx * B.ny)) + NG);
+  } else if (t >= B.vol) {
+    return;
+  }
   const double *Q = Qall + (4 + NS) * B.cv + t;
   double *st = stall + SW * B.cv + t;
   const long long v = B.vol;

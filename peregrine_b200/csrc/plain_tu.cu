@@ -146,6 +146,11 @@ void diff_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void 
     k_diffflux<NS, A><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, pc->tr, pc->hsp, pc->grads, pc->met, pc->F[A], ct);
 }
 
+// the double flux's state off the frozen planes on the interior alone (R_INNER)
+void fromplane_inner_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const RhsArgs &a = *(const RhsArgs *)ctx;
+  k_fromQ<NS, true, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, 1);
+}
 void fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const RhsArgs &a = *(const RhsArgs *)ctx;
   if (pc->realgas)
@@ -415,6 +420,10 @@ void prestep_fromQ_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, co
   const PrestepArgs &a = *(const PrestepArgs *)ctx;
   k_fromQ<NS, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, a.first ? 0 : 1);
 }
+void prestep_fromQ_inner_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
+  const PrestepArgs &a = *(const PrestepArgs *)ctx;
+  k_fromQ<NS, true, true><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct, a.first ? 0 : 1);
+}
 void prestep_freeze_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, const void *ctx) {
   const PrestepArgs &a = *(const PrestepArgs *)ctx;
   k_freeze<NS><<<g, TH, 0, pc->stream>>>(pc->d_blks, b, a.Q, pc->state, ct);
@@ -424,14 +433,20 @@ void prestep_freeze_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, c
 // the double flux's step start: the state of Q (the eos's fromrhoE on the
 // first step, the frozen planes' after), the planes frozen anew on the
 // interior with the energy reset to the eos's, then Q and the state (planes
-// included) copied into the halos, so a halo's plane is its image's
+// included) copied into the halos, so a halo's plane is its image's (one
+// pass for both where the halo goes by boxes)
 // (peregrine/simulator/eulerdf/simulator.py:58-66)
 extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int first) {
   cudaStream_t s = pc->stream;
   if (pc->packed) {
     // each pass one launch over every block
     const PrestepArgs pa{Q, first};
-    for_blocks(pc, R_VOL, prestep_fromQ_launch, &pa, 2);
+    // the halo's state is the copy below, so with rcell_inner only the
+    // interior's is formed (a boundary's halo cells keep the whole pass)
+    if (pc->rcell_inner && !pc->nbchalo)
+      for_blocks(pc, R_INNER, prestep_fromQ_inner_launch, &pa, 2);
+    else
+      for_blocks(pc, R_VOL, prestep_fromQ_launch, &pa, 2);
     for_blocks(pc, R_INNER, prestep_freeze_launch, &pa, 2);
   } else {
     for (int b = 0; b < pc->nblocks; b++) {
@@ -442,10 +457,21 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
       mark(pc, 2);
     }
   }
-  halo_fill(pc, Q, NE, 1);
-  mark(pc, 0);
-  halo_fill(pc, pc->state, SW, HALO_SCALARS);
-  mark(pc, 0);
+  if (pc->boxcta && pc->nboxcta > 0) {
+    // Q's halo and the state's (planes included) in one pass over the boxes
+    if (pc->rots)
+      k_halo_boxes2<NE, SW, true><<<(unsigned)pc->nboxcta, 256, 0, s>>>(Q, 1, 0, pc->state, SW, pc->boxes, pc->boxcta,
+                                                                        pc->boxrest, pc->nboxrest, pc->rots);
+    else
+      k_halo_boxes2<NE, SW, false><<<(unsigned)pc->nboxcta, 256, 0, s>>>(Q, 1, 0, pc->state, SW, pc->boxes, pc->boxcta,
+                                                                         pc->boxrest, pc->nboxrest, pc->rots);
+    mark(pc, 0);
+  } else {
+    halo_fill(pc, Q, NE, 1);
+    mark(pc, 0);
+    halo_fill(pc, pc->state, SW, HALO_SCALARS);
+    mark(pc, 0);
+  }
   // the boundaries' halo cells from the state just formed, then their planes
   if (pc->nbchalo) {
     bc_halo_launch(pc, Q);
@@ -521,14 +547,35 @@ void rcellflux_df_launch(const PlainCase *pc, int b, dim3 g, const int2 *ct, con
 
 extern "C" int PGB_ENTRY(pgb_plain_fused_)(const PlainCase *pc, const RStage *rs) {
   cudaStream_t s = pc->stream;
-  halo_fill(pc, const_cast<double *>(rs->Q), NE, 1);
-  mark(pc, 0);
+  // the double flux's interior state pass reads no halo cell: its stage
+  // fills Q's halo after that pass, in the state's copy
+  const bool df_inner = pc->df && pc->rcell_inner && pc->boxcta && pc->nboxcta > 0;
+  if (!df_inner) {
+    halo_fill(pc, const_cast<double *>(rs->Q), NE, 1);
+    mark(pc, 0);
+  }
   if (pc->df) {
     // the double flux, inviscid, kepaec: the state off each cell's frozen
     // plane (halo included), then a cell a thread of its six faces, the
     // divergence and the combines
     const RhsArgs q{rs->Q, rs->dQ};
-    for_blocks(pc, R_VOL, fromQ_launch, &q, 8);
+    if (df_inner) {
+      // the interior's state, then in one pass over the halo Q's halo and
+      // each halo cell's state (p .. c and Z) copied from its source's: the
+      // values the pass would form there, as a halo cell's Q, frozen plane
+      // and last T are its source's
+      for_blocks(pc, R_INNER, fromplane_inner_launch, &q, 8);
+      constexpr int CS = ST_Z + 1;
+      if (pc->rots)
+        k_halo_boxes2<NE, CS, true><<<(unsigned)pc->nboxcta, 256, 0, s>>>(
+            const_cast<double *>(rs->Q), 1, 0, pc->state, SW, pc->boxes, pc->boxcta, pc->boxrest, pc->nboxrest, pc->rots);
+      else
+        k_halo_boxes2<NE, CS, false><<<(unsigned)pc->nboxcta, 256, 0, s>>>(
+            const_cast<double *>(rs->Q), 1, 0, pc->state, SW, pc->boxes, pc->boxcta, pc->boxrest, pc->nboxrest, pc->rots);
+      mark(pc, 0);
+    } else {
+      for_blocks(pc, R_VOL, fromQ_launch, &q, 8);
+    }
     RCellFluxCtx cf{};
     cf.Q = rs->Q;
     RApplyArgs &a = cf.a;

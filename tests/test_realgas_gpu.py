@@ -159,8 +159,11 @@ def test_the_double_flux_batched_path_is_the_per_block_paths():
     ref.step(dt, 3)
     for _ in range(3):
         orc.step(dt)
-    # the freeze (4 launches: fromQ, freeze, Q's and the state's halo) and three stages of three
-    assert mb.launches_per_step() == 4 + 3 * 3
+    # the freeze (3 launches: the interior's state, the freeze, then Q's and
+    # the state's halo in one pass) and three stages of three (the
+    # interior's state off the planes, Q's halo with the state's copy, and
+    # the faces, divergence and combines)
+    assert mb.launches_per_step() == 3 + 3 * 3
     for a, b, w in zip(mb.blocks, ref.blocks, orc.regs[0]):
         got, same = a.Q.get()[a.mesh.interior], b.Q.get()[b.mesh.interior]
         scale = np.abs(same).reshape(-1, same.shape[-1]).max(axis=0)
