@@ -198,21 +198,53 @@ __global__ void __launch_bounds__(256) k_rcellflux_df(const BlockDev *__restrict
   const long long c = cell_index(B, i, j, k), v = B.vol;
   const long long sJ = B.X, sK = (long long)B.X * B.Y;
   const double *Q = Qall + NE * B.cv, *st = stall + SW * B.cv, *M = met + M_NCOMP * B.cv;
-  double fi[NF], fj[NF], fk[NF], gi[NF], gj[NF], gk[NF];
-  advflux_df_face<NS, 0>(B, Q, st, M, c, fi);
-  advflux_df_face<NS, 1>(B, Q, st, M, c, fj);
-  advflux_df_face<NS, 2>(B, Q, st, M, c, fk);
-  advflux_df_face<NS, 0>(B, Q, st, M, c + 1, gi);
-  advflux_df_face<NS, 1>(B, Q, st, M, c + sJ, gj);
-  advflux_df_face<NS, 2>(B, Q, st, M, c + sK, gk);
+  // the six faces one after another, each summed in as it is formed, in
+  // the divergence's order (low i, j, k faces added, high ones taken off):
+  // one face's rows live at a time
+  double acc[NE];
+  {
+    double f[NF];
+    advflux_df_face<NS, 0>(B, Q, st, M, c, f);
+#pragma unroll
+    for (int l = 0; l < NE; l++) acc[l] = f[l == 4 ? NE : l];
+  }
+  {
+    double f[NF];
+    advflux_df_face<NS, 1>(B, Q, st, M, c, f);
+#pragma unroll
+    for (int l = 0; l < NE; l++) acc[l] = acc[l] + f[l == 4 ? NE : l];
+  }
+  {
+    double f[NF];
+    advflux_df_face<NS, 2>(B, Q, st, M, c, f);
+#pragma unroll
+    for (int l = 0; l < NE; l++) acc[l] = acc[l] + f[l == 4 ? NE : l];
+  }
+  {
+    double f[NF];
+    advflux_df_face<NS, 0>(B, Q, st, M, c + 1, f);
+#pragma unroll
+    for (int l = 0; l < NE; l++) acc[l] = acc[l] - f[l];
+  }
+  {
+    double f[NF];
+    advflux_df_face<NS, 1>(B, Q, st, M, c + sJ, f);
+#pragma unroll
+    for (int l = 0; l < NE; l++) acc[l] = acc[l] - f[l];
+  }
+  {
+    double f[NF];
+    advflux_df_face<NS, 2>(B, Q, st, M, c + sK, f);
+#pragma unroll
+    for (int l = 0; l < NE; l++) acc[l] = acc[l] - f[l];
+  }
   const double detJinv = M[M_DETJINV * v + c];
   const long long at = NE * B.cv + c;
   const double dt = *a.dt;
   double first[NE];
 #pragma unroll
   for (int l = 0; l < NE; l++) {
-    const int lo = l == 4 ? NE : l;
-    const double dq = (fi[lo] + fj[lo] + fk[lo] - gi[l] - gj[l] - gk[l]) * detJinv;
+    const double dq = acc[l] * detJinv;
     if (a.write_dq) a.dQ[at + l * v] = dq;
     for (int m = 0; m < a.ncomb; m++) {
       const RCombine &cb = a.comb[m];
