@@ -105,6 +105,16 @@ def test_two_shards_step_as_one_case(kind, launch, simulator):
             a = mb.blocks[n].Q.get()[mb.mesh_blocks[n].interior]
             b = whole.blocks[g].Q.get()[whole.mesh_blocks[g].interior]
             assert np.array_equal(a, b), (g, np.abs(a - b).max())
+    if kind == "tgv" and launch == "batched":
+        # the whole grid's stage reads across its blocks' faces; a shard,
+        # whose halo at the cut comes from the exchange, fills its halo
+        def pulls(mb):
+            on = ctypes.c_int(-1)
+            native.call("pgb_case_halo_pull", mb.case, ctypes.byref(on))
+            return on.value
+
+        assert pulls(whole) == 1
+        assert all(pulls(mb) == 0 for _, mb in parts)
 
 
 def test_a_stage_out_of_order_is_refused():
