@@ -327,6 +327,26 @@ def reacting_profile(kernel):
     print(json.dumps({"reacting_profile": kernel, "generated": mb.generated_chemistry()[0]}), flush=True)
 
 
+def realgas_profile():
+    """The mixing layer's batched step three times (two warm-ups and one
+    more), its launches plain (no graph), so a profiler sees each pass on its
+    own: the step start's two passes and halo pass, then per stage the
+    interior's state, the halo pass and the faces, divergence and combines."""
+    import peregrine_b200 as pg
+    from peregrine_b200 import cases, native
+
+    cfg = cases.mixing_layer_config("pr", "euler-df", "tvd-rk3", launch="batched")
+    mesh = cases.mixing_layer_mesh(256, 128, 4, 8, seed=SEED)
+    mb = pg.get_solver(cfg, mesh, pg.get_backend("cuda", cfg))
+    mb.set_prims(cases.mixing_layer_prims(mb.metrics, 128, seed=SEED))
+    mb.path = native.PATH_BATCHED
+    mb.graph = False
+    for _ in range(3):
+        mb.step(2e-9, 1)
+    mb.backend.sync()
+    print(json.dumps({"realgas_profile": "batched", "launches_per_step": mb.launches_per_step()}), flush=True)
+
+
 # the sub-stepped leg's timed steps, fixed: the hot spots burn through in a
 # few microseconds, so the stiff cells a step lists depend on how far the
 # field has run (three warm-up steps, then these)
@@ -694,6 +714,8 @@ def main():
     ap.add_argument("--cells", type=int, default=CELLS, help="cells per axis of the cube (a smaller case for profiling)")
     ap.add_argument("--no-reacting", action="store_true", help="skip the reacting leg")
     ap.add_argument("--reacting-only", action="store_true", help="the reacting leg alone (profiling)")
+    ap.add_argument("--realgas-profile", action="store_true",
+                    help="three plain batched steps of the mixing layer (for a profiler)")
     ap.add_argument("--reacting-profile", default=None, choices=("generated", "tables"),
                     help="one warm-up and one RK3 step of the 96^3 reacting case on the batched path, no graph, "
                          "with the named source kernel: the command an ncu capture of its passes runs")
@@ -737,6 +759,9 @@ def main():
         return
     if args.reacting_profile:
         reacting_profile(args.reacting_profile)
+        return
+    if args.realgas_profile:
+        realgas_profile()
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
