@@ -457,19 +457,22 @@ extern "C" int PGB_ENTRY(pgb_plain_prestep_)(const PlainCase *pc, double *Q, int
       mark(pc, 2);
     }
   }
+  // the state's record up to its last plane field (p .. c, Z, theta, eps,
+  // kappa and the NS - 1 zetas), the rest of its stride unused here
+  constexpr int CS = ST_ZETA + NS - 1;
   if (pc->boxcta && pc->nboxcta > 0) {
     // Q's halo and the state's (planes included) in one pass over the boxes
     if (pc->rots)
-      k_halo_boxes2<NE, SW, true><<<(unsigned)pc->nboxcta, 256, 0, s>>>(Q, 1, 0, pc->state, SW, pc->boxes, pc->boxcta,
+      k_halo_boxes2<NE, CS, true><<<(unsigned)pc->nboxcta, 256, 0, s>>>(Q, 1, 0, pc->state, SW, pc->boxes, pc->boxcta,
                                                                         pc->boxrest, pc->nboxrest, pc->rots);
     else
-      k_halo_boxes2<NE, SW, false><<<(unsigned)pc->nboxcta, 256, 0, s>>>(Q, 1, 0, pc->state, SW, pc->boxes, pc->boxcta,
+      k_halo_boxes2<NE, CS, false><<<(unsigned)pc->nboxcta, 256, 0, s>>>(Q, 1, 0, pc->state, SW, pc->boxes, pc->boxcta,
                                                                          pc->boxrest, pc->nboxrest, pc->rots);
     mark(pc, 0);
   } else {
     halo_fill(pc, Q, NE, 1);
     mark(pc, 0);
-    halo_fill(pc, pc->state, SW, HALO_SCALARS);
+    halo_fill(pc, pc->state, CS, HALO_SCALARS, SW);
     mark(pc, 0);
   }
   // the boundaries' halo cells from the state just formed, then their planes
