@@ -435,7 +435,8 @@ int pgb_fused_shapes(int *shapes, int cap, int *n);
  * rotation, both blocks at least two cells thick across it, no exchange with
  * another case fills a halo, and the 256- or 128-thread instances run; the
  * result is the same either way.  pgb_case_halo_pull reports whether stages
- * of the finalized case read that way.  Other readers of a halo still get it
+ * of the finalized case read that way; before finalize, with no device
+ * work, whether the wish and the blocks' faces allow it.  Other readers of a halo still get it
  * from pgb_exchange (the reference's exchange before a right-hand side,
  * peregrine/multiblock/collections/exchange/collection.py). */
 int pgb_case_set_halo_pull(pgb_case *c, int on);

@@ -2082,7 +2082,8 @@ int pgb_case_set_halo_pull(pgb_case *c, int on) {
 
 int pgb_case_halo_pull(const pgb_case *c, int *on) {
   if (!c || !on) return fail(PGB_ERR_ARG, "null argument");
-  *on = c->finalized && pulls(c) ? 1 : 0;
+  // before finalize a host computation: whether the wish and the faces allow it
+  *on = c->finalized ? (pulls(c) ? 1 : 0) : (c->pull_want && faces_pullable(c) ? 1 : 0);
   return PGB_OK;
 }
 

@@ -113,3 +113,42 @@ def test_blocks_thinner_than_the_halo():
     mesh = cases.tgv_mesh(8, (4, 3, 1), seed=1, low=1, high=4)
     ent, box, rest = check(mesh.make_blocks(2))
     assert rest > 0 and len(box) > 0
+
+
+def pull_allowed(blocks, want=True):
+    h = scratch(blocks)
+    try:
+        native.call("pgb_case_set_halo_pull", h, 1 if want else 0)
+        on = ctypes.c_int(-1)
+        native.call("pgb_case_halo_pull", h, ctypes.byref(on))
+        return on.value
+    finally:
+        native.call("pgb_case_destroy", h)
+
+
+def test_reading_across_faces_is_allowed_only_where_every_face_joins_unrotated():
+    # the uniform stage reads past a face from the neighbour's own cells only
+    # where every face of every block is joined low face to high face in the
+    # identity orientation, unrotated, both blocks two cells thick or more
+    from peregrine_b200.mesher import CubeMesher, fill_node_halos, reorient
+
+    tgv = cases.tgv_mesh(128, (3, 3, 3), seed=0, low=30, high=56).make_blocks(2)
+    assert pull_allowed(tgv) == 1
+    assert pull_allowed(tgv, want=False) == 0
+    thin = cases.tgv_mesh(8, (4, 3, 1), seed=1, low=1, high=4).make_blocks(2)
+    assert min(b.cells[0] for b in thin) < 2
+    assert pull_allowed(thin) == 0
+    # a periodic pair: in the identity orientation, then with the second
+    # block laid out along other axes
+    for S, want in (("123", 1), ("213", 0), ("456", 0)):
+        blocks = CubeMesher(mbdims=[2, 1, 1], blkdims=[6, 4, 4], lengths=[2, 1, 1],
+                            periodic=[True] * 3).make_blocks(2)
+        if S != "123":
+            reorient(blocks, 1, S)
+            fill_node_halos(blocks)
+        assert pull_allowed(blocks) == want, S
+    # a wall (a face with no neighbour), and a rotational periodic
+    assert pull_allowed(pair("123")) == 0
+    mesher = AnnulusMesher(mbdims=[1, 1, 2], blkdims=[5, 5, 6], p1=[0, 0, 0], p2=[1, 0, 0], p3=[0, 0.5, 0],
+                           sweep=90, thickness=0.5, periodic=True, defaultbc="wall")
+    assert pull_allowed(mesher.make_blocks(2)) == 0
